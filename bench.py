@@ -1,0 +1,383 @@
+#!/usr/bin/env python
+"""Benchmark of the harmonic-conversion hot path on B200.
+
+Workload (one "step"): sph2fourier('N') followed by fourier2sph('N') on one
+field of degree 4095 (n = 4096 rows, M = 8191 columns, column-major), FP64,
+seeded U(-1,1) in the reference's triangular sph layout.  Metric: coefficients
+per second, coeffs/s = fields * n^2 / (t_fwd + t_bwd).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n 4096]
+
+Under torchrun (N > 1) every rank runs an independent replica on its own
+field (the path has no exchange step); the step time is the max over ranks.
+
+Arms:
+  ours       the CUDA library: device-resident timing (value), roofline of the
+             dominant kernel from CUDA events recorded around each launch on its
+             stream, end-to-end timing through the host drop-in API (e2e), and the
+             reference's CPU build timed on a sample of the same workload.
+  reference  the reference FastTransforms library compiled from its own sources
+             (oracle/_ref/libft_ref.so, OpenMP + its AVX kernels + OpenBLAS), run
+             on the host cores for the same workload and metric.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "sph2fourier fwd+bwd coeffs/s: batched mixed-prec vs plain FP64 GPU, ε₂≤1e-6"
+UNIT = "coeffs/s"
+SEED = 20261203
+
+
+def rotations_sph(n: int) -> int:
+    """Givens rotations of one sph hi2lo (or lo2hi) over all orders (src/drivers.c:94-101)."""
+    tot = 0
+    for m in range(2, n):
+        c = m // 2                       # sweeps j = m-2, m-4, ..., m % 2
+        sum_j = c * (m % 2 + m - 2) // 2
+        tot += 2 * (c * (n - 2) - sum_j)  # sweep j rotates rows k = 0 .. n-3-j, both columns
+    return tot
+
+
+def trmm_flops(n: int, M: int) -> int:
+    """Upper-triangular multiply of all M columns: n(n+1)/2 multiply-adds per column."""
+    return n * (n + 1) * M
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return json.load(open(path))
+    except Exception:
+        return {}
+
+
+def fp64_peak_tflops(torch) -> float:
+    """cuBLAS DGEMM 8192^3 burst (best of 5), the FP64 counterpart of the bf16 GEMM peak."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    c = a @ b
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        c = a @ b
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b, c
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", gpu_id], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_sample(n: int, reps: int) -> dict:
+    """Reference CPU build on this host's cores: one plan, `reps` timed fwd+bwd after one warm-up."""
+    threads = os.cpu_count() or 1
+    from oracle.bind import Reference, Oracle, fill
+    A = fill("sph", n, SEED)
+    if Reference.available():
+        R = Reference()
+        kind = "reference"
+        try:
+            ob = C.CDLL(None)
+            for name in ("scipy_openblas_set_num_threads", "openblas_set_num_threads"):
+                if hasattr(ob, name):
+                    getattr(ob, name)(threads)
+        except Exception:
+            pass
+        R.set_num_threads(threads)
+        P = R.plan("sph", n)
+        run = lambda fwd, B: R.execute("sph", P, fwd, "N", B)
+    else:
+        R = Oracle()
+        kind = "port"
+        P = R.plan("sph", n)
+        run = lambda fwd, B: R.execute(P, fwd, "N", B)
+    B = A.copy(order="F")
+    run(True, B)
+    run(False, B)
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        run(True, B)
+        run(False, B)
+        ts.append(time.perf_counter() - t0)
+    R.destroy(P)
+    t = statistics.median(ts)
+    return {"value": n * n / t, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"sph n={n} (degree {n - 1}), 1 field, fwd+bwd 'N', median of {reps} after 1 warm-up, "
+                      f"OMP threads = BLAS threads = {threads}", "sec_per_step": t}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    from oracle.bind import Reference, fill
+    if not Reference.available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref/libft_ref.so was not built"}))
+        return
+    n = args.n
+    M = 2 * n - 1
+    R = Reference()
+    R.set_num_threads(threads)
+    P = R.plan("sph", n)
+    A = fill("sph", n, SEED)
+    for _ in range(args.warmup):
+        R.execute("sph", P, True, "N", A)
+        R.execute("sph", P, False, "N", A)
+    ts = []
+    budget = 240.0
+    t_all = time.perf_counter()
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        R.execute("sph", P, True, "N", A)
+        R.execute("sph", P, False, "N", A)
+        ts.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_all > budget:
+            break
+    R.destroy(P)
+    tot = sum(ts)
+    value = n * n * len(ts) / tot
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": len(ts), "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(ts),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded U(-1,1) in the sph triangular layout",
+            "config": {"workload": f"sph2fourier+fourier2sph FP64, degree {n - 1} (n={n}, M={M}), 1 field, host CPU",
+                       "n": n, "fields": 1},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": f"{len(ts)} steps of the full workload, OMP threads = BLAS threads = {threads}"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_ours(args, rank, world, local_rank, dist):
+    import numpy as np
+    import torch
+    import fasttransforms_b200 as ft
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.cuda.current_device()
+    props = torch.cuda.get_device_properties(dev)
+    n = args.n
+    M = 2 * n - 1
+    A = ft.sphrand(n, SEED + rank)
+    P = ft.plan_sph2fourier(n)
+    d = torch.from_numpy(A.ravel(order="F").copy()).cuda()
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+
+    def step():
+        ft.execute_dev(P, True, "N", d.data_ptr(), n, M, sptr)
+        ft.execute_dev(P, False, "N", d.data_ptr(), n, M, sptr)
+
+    # accuracy of one fwd+bwd from the seeded input
+    step()
+    back = d.cpu().numpy().reshape((n, M), order="F")
+    eps2 = float(np.linalg.norm(back - A) / np.linalg.norm(A))
+    epsinf = float(np.abs(back - A).max() / np.abs(A).max())
+    d.copy_(torch.from_numpy(A.ravel(order="F").copy()))
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    uuid = getattr(props, "uuid", None)
+    gpu_id = ("GPU-" + str(uuid)) if uuid is not None else str(local_rank)
+    sampler = ClockSampler(gpu_id)
+    time.sleep(0.3)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = ft.kernel_launches()
+    ft.profile(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clocks = sampler.stop()
+    launches = ft.kernel_launches() - launches0
+    rot_ms, rot_n = ft.profile_read(0)
+    trmm_ms, trmm_n = ft.profile_read(1)
+    ft.profile(False)
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * n * n * args.steps / (ms * 1e-3)
+
+    # end to end through the drop-in host API: each call stages its input from
+    # pinned host memory and reads its result back
+    hbuf = torch.empty(n * M, dtype=torch.float64, pin_memory=True)
+    hbuf.copy_(torch.from_numpy(A.ravel(order="F")))
+    Ah = hbuf.numpy().reshape((M, n)).T
+    assert Ah.flags.f_contiguous
+    ft.execute_sph2fourier("N", P, Ah)
+    ft.execute_fourier2sph("N", P, Ah)
+    e2e_steps = max(1, min(args.steps, 10))
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ft.execute_sph2fourier("N", P, Ah)
+        ft.execute_fourier2sph("N", P, Ah)
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * n * n * e2e_steps / e2e_s
+    bytes_mat = n * M * 8
+
+    if rank != 0:
+        P.close()
+        return
+    # roofline of the dominant kernel family
+    peaks = measured_peaks()
+    fp64 = fp64_peak_tflops(torch)
+    rot_flops = 6 * rotations_sph(n)
+    tr_flops = trmm_flops(n, M)
+    fam = "rotations" if rot_ms >= trmm_ms else "trmm"
+    per_launch_ms = (rot_ms / max(rot_n, 1)) if fam == "rotations" else (trmm_ms / max(trmm_n, 1))
+    flops = rot_flops if fam == "rotations" else tr_flops
+    achieved = flops / (per_launch_ms * 1e-3) / 1e12
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(f"sph_n{n}", {}).get(fam)
+        except Exception:
+            traffic = None
+    total_flops = 2 * (rot_flops + tr_flops)
+    roofline = {
+        "bound": "fp64", "kernel": "rot_kernel (Givens sweeps)" if fam == "rotations" else "gemm_tri_kernel (DMMA trmm)",
+        "achieved": achieved, "peak": fp64, "unit": "TFLOP/s", "frac": achieved / fp64, "traffic": traffic,
+        "peak_source": "measured in bench.py: cuBLAS DGEMM 8192^3 burst (MEASURED_PEAKS.json has no FP64 entry)",
+        "flops_per_launch": flops, "ms_per_launch": per_launch_ms,
+        "families_ms_per_step": {"rotations": rot_ms / args.steps, "trmm": trmm_ms / args.steps},
+        "step_fp64_frac": total_flops / (ms / args.steps * 1e-3) / 1e12 / fp64 if ms > 0 else None,
+        "hbm_peak_gbs": peaks.get("hbm_gbs"),
+    }
+    P.close()
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        try:
+            out = subprocess.run([sys.executable, os.path.abspath(__file__), "--cpu-sample", "--n", str(args.n)],
+                                 capture_output=True, text=True, timeout=900)
+            cpu = json.loads(out.stdout.strip().splitlines()[-1])
+        except Exception as exc:  # the line still carries the GPU numbers
+            cpu = {"value": None, "error": repr(exc)[:200]}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: seeded U(-1,1) in the sph triangular layout (splitmix64, seed 20261203 + rank)",
+        "config": {"workload": f"plain FP64 sph2fourier+fourier2sph, degree {n - 1} (n={n}, M={M}), "
+                               f"1 field per GPU, device-resident plan",
+                   "n": n, "M": M, "fields_per_gpu": 1, "parallelism": f"replicas x{world}",
+                   "l2": f"inputs larger than L2: A {bytes_mat / 1e6:.0f} MB, rotation table "
+                         f"{16 * n * (n + 1) // 2 / 1e6:.0f} MB, connection matrices {4 * 8 * n * n / 1e6:.0f} MB"},
+        "accuracy": {"roundtrip_eps2": eps2, "roundtrip_epsinf": epsinf},
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * bytes_mat, "d2h_bytes_per_step": 2 * bytes_mat,
+                "api": "ft_execute_sph2fourier + ft_execute_fourier2sph on pinned host arrays", "steps": e2e_steps},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=4096)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-sample", action="store_true", help=argparse.SUPPRESS)
+    args = ap.parse_args()
+    if args.cpu_sample:
+        print(json.dumps(cpu_sample(args.n, 2)))
+        return
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1 and args.impl == "ours":
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = tdist
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, local_rank, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

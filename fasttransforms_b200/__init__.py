@@ -1,0 +1,251 @@
+"""B200-native (sm_100a) harmonic-conversion path of FastTransforms.
+
+Python mirror of the reference's C API for sph2fourier / fourier2sph,
+tri2cheb / cheb2tri and disk2cxf / cxf2disk (src/fasttransforms.h:370-415),
+over the C ABI in include/ft_b200.h.  The compute runs in hand-written CUDA
+kernels in ``_lib/libft_b200.so``; there is no CPU fallback: importing this
+package fails if the library is missing, and planning fails without an sm_100
+device.
+
+Host arrays are numpy float64 in Fortran (column-major) order, N x M, exactly
+the reference's layout; transforms run in place like the reference's.
+Device entry points take raw device pointers (e.g. ``tensor.data_ptr()``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Sequence
+
+import numpy as np
+
+from .utilities import diskrand, layout_cols, rand_layout, sphrand, trirand
+
+__all__ = [
+    "FTB200Error", "HarmonicPlan", "RotationPlan", "library_path", "lib",
+    "plan_sph2fourier", "plan_tri2cheb", "plan_disk2cxf",
+    "execute_sph2fourier", "execute_fourier2sph", "execute_tri2cheb", "execute_cheb2tri",
+    "execute_disk2cxf", "execute_cxf2disk",
+    "plan_rotsphere", "plan_rottriangle", "plan_rotdisk",
+    "execute_sph_hi2lo", "execute_sph_lo2hi", "execute_tri_hi2lo", "execute_tri_lo2hi",
+    "execute_disk_hi2lo", "execute_disk_lo2hi",
+    "execute_dev", "execute_batched_dev", "rotations_dev", "kernel_launches", "profile", "profile_read",
+    "layout_cols", "rand_layout", "sphrand", "trirand", "diskrand",
+    "SPH", "TRI", "DISK",
+]
+
+SPH, TRI, DISK = 0, 1, 2
+_KINDS = {"sph": SPH, "tri": TRI, "disk": DISK}
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+library_path = os.path.join(_HERE, "_lib", "libft_b200.so")
+
+
+class FTB200Error(RuntimeError):
+    """A call into the CUDA library failed; ``status`` is the ft_b200 status code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"ft_b200 status {status}: {message}")
+        self.status = status
+
+
+def _load() -> C.CDLL:
+    if not os.path.exists(library_path):
+        raise ImportError(f"{library_path} is not built (python -m fasttransforms_b200.build)")
+    L = C.CDLL(library_path)
+    vp, dp, i, d, ch = C.c_void_p, C.POINTER(C.c_double), C.c_int, C.c_double, C.c_char
+    sig = {
+        "ft_b200_last_status": (i, []), "ft_b200_last_error": (C.c_char_p, []),
+        "ft_b200_kernel_launches": (C.c_ulonglong, []),
+        "ft_plan_sph2fourier": (vp, [i]), "ft_plan_tri2cheb": (vp, [i, d, d, d]), "ft_plan_disk2cxf": (vp, [i, d, d]),
+        "ft_destroy_harmonic_plan": (None, [vp]),
+        "ft_plan_rotsphere": (vp, [i]), "ft_plan_rottriangle": (vp, [i, d, d, d]), "ft_plan_rotdisk": (vp, [i, d, d]),
+        "ft_destroy_rotation_plan": (None, [vp]),
+        "ft_b200_execute_dev": (i, [vp, i, ch, vp, i, i, vp]),
+        "ft_b200_rotations_dev": (i, [vp, i, vp, i, vp]),
+        "ft_b200_execute_batched_dev": (i, [C.POINTER(vp), i, ch, C.POINTER(vp), C.POINTER(i), C.POINTER(i), i, vp]),
+        "ft_b200_plan_kind": (i, [vp]), "ft_b200_plan_device": (i, [vp]),
+        "ft_b200_profile": (i, [i]), "ft_b200_profile_read": (i, [i, C.POINTER(C.c_double), C.POINTER(i)]),
+    }
+    for name in ("sph2fourier", "fourier2sph", "tri2cheb", "cheb2tri", "disk2cxf", "cxf2disk"):
+        sig["ft_execute_" + name] = (None, [ch, vp, dp, i, i])
+    for fam in ("sph", "tri", "disk"):
+        for d_ in ("hi2lo", "lo2hi"):
+            sig[f"ft_execute_{fam}_{d_}"] = (None, [vp, dp, dp, i])
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    return L
+
+
+lib = _load()
+
+
+def _check():
+    st = lib.ft_b200_last_status()
+    if st != 0:
+        raise FTB200Error(st, lib.ft_b200_last_error().decode())
+
+
+def profile(enable: bool) -> None:
+    """Turn per-launch CUDA-event timing on (resetting the record) or off."""
+    lib.ft_b200_profile(1 if enable else 0)
+
+
+def profile_read(family: int):
+    """(total ms, launches) recorded for a kernel family: 0 rotations, 1 trmm, 2 other."""
+    ms = C.c_double(0)
+    cnt = C.c_int(0)
+    if lib.ft_b200_profile_read(family, C.byref(ms), C.byref(cnt)) != 0:
+        _check()
+    return ms.value, cnt.value
+
+
+def kernel_launches() -> int:
+    """Kernels this library has launched since it was loaded."""
+    return int(lib.ft_b200_kernel_launches())
+
+
+class HarmonicPlan:
+    """Owns an ``ft_harmonic_plan *`` of the CUDA library (reference: src/drivers.c:793-1021)."""
+
+    def __init__(self, ptr: int, kind: str, n: int, params=()):
+        self.ptr = ptr
+        self.kind = kind
+        self.n = n
+        self.params = tuple(params)
+
+    @property
+    def M(self) -> int:
+        return layout_cols(self.kind, self.n)
+
+    def close(self):
+        if self.ptr:
+            lib.ft_destroy_harmonic_plan(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class RotationPlan(HarmonicPlan):
+    """Owns an ``ft_rotation_plan *`` (reference: src/rotations.c:116-190)."""
+
+    def close(self):
+        if self.ptr:
+            lib.ft_destroy_rotation_plan(self.ptr)
+            self.ptr = None
+
+
+def _plan(kind, n, ptr, params=()):
+    if not ptr:
+        _check()
+        raise FTB200Error(-1, "plan creation failed")
+    return HarmonicPlan(ptr, kind, n, params)
+
+
+def plan_sph2fourier(n: int) -> HarmonicPlan:
+    return _plan("sph", n, lib.ft_plan_sph2fourier(n))
+
+
+def plan_tri2cheb(n: int, alpha: float, beta: float, gamma: float) -> HarmonicPlan:
+    return _plan("tri", n, lib.ft_plan_tri2cheb(n, alpha, beta, gamma), (alpha, beta, gamma))
+
+
+def plan_disk2cxf(n: int, alpha: float, beta: float) -> HarmonicPlan:
+    return _plan("disk", n, lib.ft_plan_disk2cxf(n, alpha, beta), (alpha, beta))
+
+
+def _host_matrix(A: np.ndarray) -> np.ndarray:
+    if not (isinstance(A, np.ndarray) and A.dtype == np.float64 and A.ndim == 2 and A.flags.f_contiguous and A.flags.writeable):
+        raise TypeError("A must be a writeable 2-D float64 numpy array in Fortran order")
+    return A
+
+
+def _exec_host(fname: str, trans: str, P: HarmonicPlan, A: np.ndarray, N=None, M=None):
+    A = _host_matrix(A)
+    N = A.shape[0] if N is None else N
+    M = A.shape[1] if M is None else M
+    if N * M > A.size:
+        raise ValueError("N x M exceeds the array")
+    getattr(lib, fname)(trans.encode(), P.ptr, A.ctypes.data_as(C.POINTER(C.c_double)), N, M)
+    _check()
+
+
+def execute_sph2fourier(trans, P, A, N=None, M=None): _exec_host("ft_execute_sph2fourier", trans, P, A, N, M)
+def execute_fourier2sph(trans, P, A, N=None, M=None): _exec_host("ft_execute_fourier2sph", trans, P, A, N, M)
+def execute_tri2cheb(trans, P, A, N=None, M=None): _exec_host("ft_execute_tri2cheb", trans, P, A, N, M)
+def execute_cheb2tri(trans, P, A, N=None, M=None): _exec_host("ft_execute_cheb2tri", trans, P, A, N, M)
+def execute_disk2cxf(trans, P, A, N=None, M=None): _exec_host("ft_execute_disk2cxf", trans, P, A, N, M)
+def execute_cxf2disk(trans, P, A, N=None, M=None): _exec_host("ft_execute_cxf2disk", trans, P, A, N, M)
+
+
+def plan_rotsphere(n: int) -> RotationPlan:
+    p = lib.ft_plan_rotsphere(n)
+    if not p:
+        _check()
+    return RotationPlan(p, "sph", n)
+
+
+def plan_rottriangle(n: int, alpha: float, beta: float, gamma: float) -> RotationPlan:
+    p = lib.ft_plan_rottriangle(n, alpha, beta, gamma)
+    if not p:
+        _check()
+    return RotationPlan(p, "tri", n, (alpha, beta, gamma))
+
+
+def plan_rotdisk(n: int, alpha: float, beta: float) -> RotationPlan:
+    p = lib.ft_plan_rotdisk(n, alpha, beta)
+    if not p:
+        _check()
+    return RotationPlan(p, "disk", n, (alpha, beta))
+
+
+def _exec_rot(fname, RP, A, M=None):
+    A = _host_matrix(A)
+    M = A.shape[1] if M is None else M
+    getattr(lib, fname)(RP.ptr, A.ctypes.data_as(C.POINTER(C.c_double)), None, M)
+    _check()
+
+
+def execute_sph_hi2lo(RP, A, M=None): _exec_rot("ft_execute_sph_hi2lo", RP, A, M)
+def execute_sph_lo2hi(RP, A, M=None): _exec_rot("ft_execute_sph_lo2hi", RP, A, M)
+def execute_tri_hi2lo(RP, A, M=None): _exec_rot("ft_execute_tri_hi2lo", RP, A, M)
+def execute_tri_lo2hi(RP, A, M=None): _exec_rot("ft_execute_tri_lo2hi", RP, A, M)
+def execute_disk_hi2lo(RP, A, M=None): _exec_rot("ft_execute_disk_hi2lo", RP, A, M)
+def execute_disk_lo2hi(RP, A, M=None): _exec_rot("ft_execute_disk_lo2hi", RP, A, M)
+
+
+def execute_dev(P: HarmonicPlan, forward: bool, trans: str, ptr: int, N: int, M: int, stream: int = 0) -> None:
+    """Full transform on a device matrix (N x M, column-major) enqueued on ``stream``."""
+    st = lib.ft_b200_execute_dev(P.ptr, 1 if forward else 0, trans.encode(), C.c_void_p(ptr), N, M, C.c_void_p(stream))
+    if st != 0:
+        _check()
+
+
+def rotations_dev(RP: RotationPlan, hi2lo: bool, ptr: int, M: int, stream: int = 0) -> None:
+    st = lib.ft_b200_rotations_dev(RP.ptr, 1 if hi2lo else 0, C.c_void_p(ptr), M, C.c_void_p(stream))
+    if st != 0:
+        _check()
+
+
+def execute_batched_dev(plans: Sequence[HarmonicPlan], forward: bool, trans: str, ptrs: Sequence[int],
+                        N: Sequence[int], M: Sequence[int], stream: int = 0) -> None:
+    nf = len(plans)
+    pa = (C.c_void_p * nf)(*[p.ptr for p in plans])
+    aa = (C.c_void_p * nf)(*ptrs)
+    na = (C.c_int * nf)(*N)
+    ma = (C.c_int * nf)(*M)
+    st = lib.ft_b200_execute_batched_dev(pa, 1 if forward else 0, trans.encode(), aa, na, ma, nf, C.c_void_p(stream))
+    if st != 0:
+        _check()

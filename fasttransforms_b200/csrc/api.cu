@@ -1,0 +1,566 @@
+// C ABI: plans, device residency, execute sequences, error reporting.
+//
+// Every transform is the reference's sequence (src/drivers.c:833-1021): a
+// rotation stage and one or two triangular multiplies (plus the Chebyshev
+// normalisation for tri).  The triangular multiplies run out of place between
+// the caller's matrix and the plan's device scratch; the rotation stage is
+// placed so that the result always lands back in the caller's matrix.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "ft_internal.h"
+
+namespace ftb {
+
+namespace {
+thread_local int t_status = FT_B200_OK;
+thread_local std::string t_message;
+std::atomic<unsigned long long> g_launches{0};
+constexpr int kPlanMagic = 0x46544232;   // "FTB2"
+}  // namespace
+
+namespace {
+struct ProfRec { int family; cudaEvent_t a, b; };
+std::mutex g_prof_mu;
+bool g_prof_on = false;
+std::vector<ProfRec> g_prof;
+std::vector<cudaEvent_t> g_prof_pool;
+thread_local int t_prof_family = -1;
+thread_local cudaEvent_t t_prof_a = nullptr;
+cudaEvent_t prof_event() {
+    if (!g_prof_pool.empty()) { cudaEvent_t e = g_prof_pool.back(); g_prof_pool.pop_back(); return e; }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+}  // namespace
+
+void prof_begin(int family, cudaStream_t st) {
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    if (!g_prof_on) { t_prof_family = -1; return; }
+    t_prof_family = family;
+    t_prof_a = prof_event();
+    cudaEventRecord(t_prof_a, st);
+}
+
+void prof_end(cudaStream_t st) {
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    if (!g_prof_on || t_prof_family < 0) return;
+    cudaEvent_t b = prof_event();
+    cudaEventRecord(b, st);
+    g_prof.push_back({t_prof_family, t_prof_a, b});
+    t_prof_family = -1;
+}
+
+void set_error(int status, const std::string & msg) { t_status = status; t_message = msg; }
+void clear_error() { t_status = FT_B200_OK; t_message.clear(); }
+void count_launch(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+namespace {
+
+bool cuda_ok(cudaError_t e, const char * what) {
+    if (e == cudaSuccess) return true;
+    set_error(e == cudaErrorMemoryAllocation ? FT_B200_ENOMEM : FT_B200_ECUDA,
+              std::string(what) + ": " + cudaGetErrorString(e));
+    return false;
+}
+
+bool check_device(int * dev_out) {
+    int dev = 0;
+    if (!cuda_ok(cudaGetDevice(&dev), "cudaGetDevice")) { t_status = FT_B200_ENODEV; return false; }
+    int major = 0;
+    if (!cuda_ok(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev), "cudaDeviceGetAttribute")) return false;
+    if (major != 10) {
+        set_error(FT_B200_ENODEV, "device " + std::to_string(dev) + " is not an sm_100 (B200) device");
+        return false;
+    }
+    *dev_out = dev;
+    return true;
+}
+
+struct HarmonicPlan {
+    ft_harmonic_plan pub;       // must stay the first member
+    int magic;
+    int kind, n, Mdef;
+    ft_rotation_plan * rp_arr[1];
+    double * hostP[2];
+    double * hostPinv[2];
+    double * dP[2];
+    double * dPinv[2];
+    double * d_scratch;
+    size_t scratch_elems;
+    double * d_stage;           // device copy of A for host-pointer calls
+    size_t stage_elems;
+    cudaStream_t stream;
+    int device;
+};
+
+HarmonicPlan * as_plan(const ft_harmonic_plan * P) {
+    if (!P) return nullptr;
+    HarmonicPlan * H = reinterpret_cast<HarmonicPlan *>(const_cast<ft_harmonic_plan *>(P));
+    return H->magic == kPlanMagic ? H : nullptr;
+}
+
+int default_cols(int kind, int n) { return kind == SPH ? 2 * n - 1 : kind == TRI ? n : 4 * n - 3; }
+
+// ---------------------------------------------------------------------------
+// rotation plans
+// ---------------------------------------------------------------------------
+ft_rotation_plan * make_rotation_plan(int kind, int n, double alpha, double beta, double gamma) {
+    clear_error();
+    if (n < 1) { set_error(FT_B200_EINVAL, "n must be positive"); return nullptr; }
+    int dev = 0;
+    if (!check_device(&dev)) return nullptr;
+    const long long len = Geo::table_len(kind, n);
+    ft_rotation_plan * RP = new (std::nothrow) ft_rotation_plan_s();
+    if (!RP) { set_error(FT_B200_ENOMEM, "host allocation"); return nullptr; }
+    RP->n = n; RP->kind = kind; RP->alpha = alpha; RP->beta = beta; RP->gamma = gamma; RP->device = dev;
+    RP->s = static_cast<double *>(std::calloc(len, sizeof(double)));
+    RP->c = static_cast<double *>(std::calloc(len, sizeof(double)));
+    RP->mu = new std::mutex();
+    RP->tasks = new std::map<int, std::pair<RotTask *, int>>();
+    if (!RP->s || !RP->c) { set_error(FT_B200_ENOMEM, "host allocation"); ft_destroy_rotation_plan(RP); return nullptr; }
+    rotation_tables(kind, n, alpha, beta, gamma, RP->s, RP->c);
+    std::vector<double2> sc(len);
+    for (long long i = 0; i < len; i++) sc[i] = make_double2(RP->s[i], RP->c[i]);
+    if (!cuda_ok(cudaMalloc(&RP->d_sc, sizeof(double2) * len), "cudaMalloc(table)") ||
+        !cuda_ok(cudaMemcpy(RP->d_sc, sc.data(), sizeof(double2) * len, cudaMemcpyHostToDevice), "cudaMemcpy(table)") ||
+        !cuda_ok(cudaMalloc(&RP->d_counter, sizeof(int)), "cudaMalloc(counter)")) {
+        ft_destroy_rotation_plan(RP);
+        return nullptr;
+    }
+    return RP;
+}
+
+// Device task list for an N x M matrix, longest first (cached per M).
+bool get_tasks(ft_rotation_plan * RP, int M, RotTask ** d_tasks, int * ntasks) {
+    std::lock_guard<std::mutex> lk(*RP->mu);
+    auto it = RP->tasks->find(M);
+    if (it != RP->tasks->end()) { *d_tasks = it->second.first; *ntasks = it->second.second; return true; }
+    std::vector<RotTask> t = build_tasks(RP->kind, RP->n, M, 0);
+    std::stable_sort(t.begin(), t.end(), [&](const RotTask & a, const RotTask & b) {
+        return task_cost(RP->kind, RP->n, M, a.mbase) > task_cost(RP->kind, RP->n, M, b.mbase);
+    });
+    RotTask * d = nullptr;
+    if (!t.empty()) {
+        if (!cuda_ok(cudaMalloc(&d, sizeof(RotTask) * t.size()), "cudaMalloc(tasks)")) return false;
+        if (!cuda_ok(cudaMemcpy(d, t.data(), sizeof(RotTask) * t.size(), cudaMemcpyHostToDevice), "cudaMemcpy(tasks)")) return false;
+    }
+    (*RP->tasks)[M] = {d, (int) t.size()};
+    *d_tasks = d; *ntasks = (int) t.size();
+    return true;
+}
+
+// Columns the rotation stage leaves alone (orders 0 and 1): copied when the
+// stage runs out of place.
+int untouched_cols(int kind, int M) { return std::min(M, kind == TRI ? 1 : 3); }
+
+bool rotations(ft_rotation_plan * RP, bool hi2lo, const double * in, double * out, int M, long long lda, cudaStream_t st) {
+    RotTask * d_tasks = nullptr;
+    int ntasks = 0;
+    if (!get_tasks(RP, M, &d_tasks, &ntasks)) return false;
+    if (in != out) {
+        const int nc = untouched_cols(RP->kind, M);
+        if (!cuda_ok(cudaMemcpy2DAsync(out, lda * sizeof(double), in, lda * sizeof(double), RP->n * sizeof(double), nc,
+                                       cudaMemcpyDeviceToDevice, st), "cudaMemcpy2DAsync")) return false;
+    }
+    if (ntasks == 0) return true;
+    static thread_local RotLaunch L;   // large parameter block; kept off the stack
+    L.nfields = 1;
+    L.fields[0] = RotField{in, out, RP->d_sc, RP->n, M, RP->kind, lda};
+    L.tasks = d_tasks;
+    L.ntasks = ntasks;
+    L.counter = RP->d_counter;
+    prof_begin(FAM_ROT, st);
+    const cudaError_t e = launch_rotations(RP->kind, hi2lo, L, 0, st);
+    prof_end(st);
+    return cuda_ok(e, "rotation kernel");
+}
+
+bool valid_MN(int kind, int n, int N, int M) {
+    if (N != n) { set_error(FT_B200_EINVAL, "N does not match the plan's n"); return false; }
+    if (M < 1) { set_error(FT_B200_EINVAL, "M must be positive"); return false; }
+    if (kind == TRI && M != N) { set_error(FT_B200_EINVAL, "tri transforms need M == N"); return false; }
+    return true;
+}
+
+// sph / disk: four stride-4N column classes, P[0] on classes 0 and 3, P[1] on 1 and 2
+bool trmm4(HarmonicPlan * H, bool inverse, bool trans, const double * in, double * out, int M, cudaStream_t st) {
+    const int N = H->n;
+    TrmmLaunch L{};
+    L.n = N;
+    L.ld_in = L.ld_out = 4LL * N;
+    L.trans = trans;
+    const int ncols[4] = {(M + 3) / 4, (M + 2) / 4, (M + 1) / 4, M / 4};
+    double * const * U = inverse ? H->dPinv : H->dP;
+    int c = 0;
+    for (int r = 0; r < 4; r++) {
+        if (ncols[r] <= 0) continue;
+        L.cls[c].U = (r == 0 || r == 3) ? U[0] : U[1];
+        L.cls[c].in = in + (long long) r * N;
+        L.cls[c].out = out + (long long) r * N;
+        L.cls[c].ncols = ncols[r];
+        c++;
+    }
+    L.nclasses = c;
+    prof_begin(FAM_TRMM, st);
+    const cudaError_t e = launch_trmm(L, st);
+    prof_end(st);
+    return cuda_ok(e, "trmm kernel");
+}
+
+bool trmm_left1(HarmonicPlan * H, const double * U, bool trans, const double * in, double * out, int M, cudaStream_t st) {
+    TrmmLaunch L{};
+    L.n = H->n;
+    L.ld_in = L.ld_out = H->n;
+    L.trans = trans;
+    L.nclasses = 1;
+    L.cls[0] = TrmmClass{U, in, out, M};
+    prof_begin(FAM_TRMM, st);
+    const cudaError_t e = launch_trmm(L, st);
+    prof_end(st);
+    return cuda_ok(e, "trmm kernel");
+}
+
+bool trmm_right(const double * U, const double * in, double * out, int N, long long lda, bool trans, cudaStream_t st) {
+    prof_begin(FAM_TRMM, st);
+    const cudaError_t e = launch_trmm_right(U, in, out, N, N, lda, trans, st);
+    prof_end(st);
+    return cuda_ok(e, "trmm kernel");
+}
+
+bool normalize(double * A, int N, int M, long long lda, bool transposed, cudaStream_t st) {
+    prof_begin(FAM_OTHER, st);
+    const cudaError_t e = launch_cheb_normalize(A, N, M, lda, transposed, st);
+    prof_end(st);
+    return cuda_ok(e, "normalize");
+}
+
+bool ensure_scratch(HarmonicPlan * H, size_t elems) {
+    if (elems <= H->scratch_elems) return true;
+    if (H->d_scratch) cudaFree(H->d_scratch);
+    H->d_scratch = nullptr;
+    H->scratch_elems = 0;
+    if (!cuda_ok(cudaMalloc(&H->d_scratch, elems * sizeof(double)), "cudaMalloc(scratch)")) return false;
+    H->scratch_elems = elems;
+    H->pub.B = H->d_scratch;
+    return true;
+}
+
+int execute_dev_impl(HarmonicPlan * H, bool forward, char TRANS, double * A, int N, int M, cudaStream_t st) {
+    if (TRANS != 'N' && TRANS != 'T') { set_error(FT_B200_EINVAL, "TRANS must be 'N' or 'T'"); return t_status; }
+    if (!A) { set_error(FT_B200_EINVAL, "NULL matrix"); return t_status; }
+    if (!valid_MN(H->kind, H->n, N, M)) return t_status;
+    if (!ensure_scratch(H, (size_t) N * M)) return t_status;
+    double * S = H->d_scratch;
+    ft_rotation_plan * RP = H->rp_arr[0];
+    const bool tN = TRANS == 'N';
+    const long long lda = N;
+    if (H->kind != TRI) {
+        // rotations (out of place) then trmm back, or trmm out then rotations back
+        if (forward && tN) {            // hi2lo, P
+            if (!rotations(RP, true, A, S, M, lda, st)) return t_status;
+            if (!trmm4(H, false, false, S, A, M, st)) return t_status;
+        } else if (forward) {           // P^T, lo2hi
+            if (!trmm4(H, false, true, A, S, M, st)) return t_status;
+            if (!rotations(RP, false, S, A, M, lda, st)) return t_status;
+        } else if (tN) {                // Pinv, lo2hi
+            if (!trmm4(H, true, false, A, S, M, st)) return t_status;
+            if (!rotations(RP, false, S, A, M, lda, st)) return t_status;
+        } else {                        // hi2lo, Pinv^T
+            if (!rotations(RP, true, A, S, M, lda, st)) return t_status;
+            if (!trmm4(H, true, true, S, A, M, st)) return t_status;
+        }
+        return FT_B200_OK;
+    }
+    // tri: src/drivers.c:921-957
+    const double a = H->pub.alpha, b = H->pub.beta, g = H->pub.gamma;
+    const bool left = (b + g != -1.5) || (a != -0.5);
+    const bool right = (g != -0.5) || (b != -0.5);
+    const int k = (left ? 1 : 0) + (right ? 1 : 0);
+    double * U0 = forward ? H->dP[0] : H->dPinv[0];
+    double * U1 = forward ? H->dP[1] : H->dPinv[1];
+    double * cur = A;
+    double * oth = S;
+    auto flip = [&]() { std::swap(cur, oth); };
+    const bool rot_hi2lo_first = (forward && tN) || (!forward && !tN);
+    if (rot_hi2lo_first) {
+        // rotation, then left / right, then normalisation; the rotation goes out of place iff k is odd
+        double * rot_out = (k % 2) ? S : A;
+        if (!rotations(RP, true, A, rot_out, M, lda, st)) return t_status;
+        cur = rot_out; oth = (rot_out == A) ? S : A;
+        if (forward) {   // tri2cheb 'N': left N P0, right T P1
+            if (left) { if (!trmm_left1(H, U0, false, cur, oth, M, st)) return t_status; flip(); }
+            if (right) { if (!trmm_right(U1, cur, oth, N, lda, true, st)) return t_status; flip(); }
+            if (!normalize(cur, N, M, lda, false, st)) return t_status;
+        } else {         // cheb2tri 'T': left T Pinv0, right N Pinv1
+            if (left) { if (!trmm_left1(H, U0, true, cur, oth, M, st)) return t_status; flip(); }
+            if (right) { if (!trmm_right(U1, cur, oth, N, lda, false, st)) return t_status; flip(); }
+            if (!normalize(cur, N, M, lda, true, st)) return t_status;
+        }
+    } else {
+        // normalisation, right / left, then the rotation back into A
+        if (!normalize(A, N, M, lda, !forward, st)) return t_status;
+        if (forward) {   // tri2cheb 'T': right N P1, left T P0
+            if (right) { if (!trmm_right(U1, cur, oth, N, lda, false, st)) return t_status; flip(); }
+            if (left) { if (!trmm_left1(H, U0, true, cur, oth, M, st)) return t_status; flip(); }
+        } else {         // cheb2tri 'N': right T Pinv1, left N Pinv0
+            if (right) { if (!trmm_right(U1, cur, oth, N, lda, true, st)) return t_status; flip(); }
+            if (left) { if (!trmm_left1(H, U0, false, cur, oth, M, st)) return t_status; flip(); }
+        }
+        if (!rotations(RP, false, cur, A, M, lda, st)) return t_status;
+    }
+    return FT_B200_OK;
+}
+
+HarmonicPlan * make_harmonic_plan(int kind, int n, double alpha, double beta, double gamma) {
+    clear_error();
+    if (n < 1) { set_error(FT_B200_EINVAL, "n must be positive"); return nullptr; }
+    int dev = 0;
+    if (!check_device(&dev)) return nullptr;
+    HarmonicPlan * H = new (std::nothrow) HarmonicPlan();
+    if (!H) { set_error(FT_B200_ENOMEM, "host allocation"); return nullptr; }
+    std::memset(&H->pub, 0, sizeof(H->pub));
+    H->magic = kPlanMagic;
+    H->kind = kind; H->n = n; H->Mdef = default_cols(kind, n); H->device = dev;
+    H->pub.alpha = alpha; H->pub.beta = beta; H->pub.gamma = gamma;
+    H->pub.RP = H->rp_arr;
+    H->pub.P = H->hostP;
+    H->pub.Pinv = H->hostPinv;
+    H->pub.NRP = 1; H->pub.NMP = 0; H->pub.NP = 2;
+    auto fail = [&]() { ft_destroy_harmonic_plan(&H->pub); return (HarmonicPlan *) nullptr; };
+    H->rp_arr[0] = make_rotation_plan(kind, n, alpha, beta, gamma);
+    if (!H->rp_arr[0]) return fail();
+    if (kind == SPH) {   // src/drivers.c:816-831
+        H->hostP[0] = connection_legendre_to_chebyshev(1, 0, n);
+        H->hostP[1] = connection_ultraspherical(1, 0, n, 1.5, 1.0);
+        H->hostPinv[0] = connection_chebyshev_to_legendre(0, 1, n);
+        H->hostPinv[1] = connection_ultraspherical(0, 1, n, 1.0, 1.5);
+    } else if (kind == TRI) {   // src/drivers.c:901-919
+        H->hostP[0] = connection_jacobi(n, beta + gamma + 1.0, alpha, -0.5, -0.5);
+        H->hostP[1] = connection_jacobi(n, gamma, beta, -0.5, -0.5);
+        H->hostPinv[0] = connection_jacobi(n, -0.5, -0.5, beta + gamma + 1.0, alpha);
+        H->hostPinv[1] = connection_jacobi(n, -0.5, -0.5, gamma, beta);
+    } else {   // src/drivers.c:959-987 with src/transforms.c:157-180 inlined
+        H->hostP[0] = connection_jacobi(n, beta, alpha, -0.5, -0.5);
+        H->hostP[1] = connection_jacobi(n, beta, alpha + 1.0, -0.5, 0.5);
+        H->hostPinv[0] = connection_jacobi(n, -0.5, -0.5, beta, alpha);
+        H->hostPinv[1] = connection_jacobi(n, -0.5, 0.5, beta, alpha + 1.0);
+        if (H->hostP[0] && H->hostPinv[0]) {
+            std::vector<double> sclrow(n), sclcol(n);
+            for (int i = 0; i < n; i++) {
+                sclrow[i] = i ? std::sqrt((long double) M_2_PIl) : std::sqrt((long double) M_1_PIl);
+                sclcol[i] = i ? std::sqrt((long double) M_PI_2l) : std::sqrt((long double) M_PIl);
+            }
+            for (int j = 0; j < n; j++)
+                for (int i = 0; i <= j; i++) {
+                    H->hostP[0][i + (size_t) j * n] *= sclrow[i];
+                    H->hostPinv[0][i + (size_t) j * n] *= sclcol[j];
+                }
+            const double cst0 = std::pow(2.0, 0.5 * (alpha + beta + 2.0));
+            const double cst1 = cst0 * 0.797884560802865355;       // sqrt(2/pi), src/ftinternal.h:66
+            const double cst0inv = std::pow(2.0, -0.5 * (alpha + beta + 2.0));
+            const double cst1inv = cst0inv * 1.253314137315500251; // sqrt(pi/2), src/ftinternal.h:65
+            for (int j = 0; j < n; j++)
+                for (int i = 0; i <= j; i++) {
+                    H->hostP[0][i + (size_t) j * n] *= cst0;
+                    H->hostP[1][i + (size_t) j * n] *= cst1;
+                    H->hostPinv[0][i + (size_t) j * n] *= cst0inv;
+                    H->hostPinv[1][i + (size_t) j * n] *= cst1inv;
+                }
+        }
+    }
+    for (int i = 0; i < 2; i++)
+        if (!H->hostP[i] || !H->hostPinv[i]) { set_error(FT_B200_ENOMEM, "host allocation (connection matrices)"); return fail(); }
+    const size_t nn = (size_t) n * n * sizeof(double);
+    for (int i = 0; i < 2; i++) {
+        if (!cuda_ok(cudaMalloc(&H->dP[i], nn), "cudaMalloc(P)") ||
+            !cuda_ok(cudaMemcpy(H->dP[i], H->hostP[i], nn, cudaMemcpyHostToDevice), "cudaMemcpy(P)") ||
+            !cuda_ok(cudaMalloc(&H->dPinv[i], nn), "cudaMalloc(Pinv)") ||
+            !cuda_ok(cudaMemcpy(H->dPinv[i], H->hostPinv[i], nn, cudaMemcpyHostToDevice), "cudaMemcpy(Pinv)"))
+            return fail();
+    }
+    if (!ensure_scratch(H, (size_t) n * H->Mdef)) return fail();
+    if (!cuda_ok(cudaStreamCreateWithFlags(&H->stream, cudaStreamNonBlocking), "cudaStreamCreate")) return fail();
+    // build the default task list now, outside any later stream capture
+    RotTask * dt; int nt;
+    if (!get_tasks(H->rp_arr[0], H->Mdef, &dt, &nt)) return fail();
+    return H;
+}
+
+// host-pointer execution: stage A on the device, run, copy back, wait
+void execute_host(const ft_harmonic_plan * P, bool forward, char TRANS, double * A, int N, int M) {
+    clear_error();
+    HarmonicPlan * H = as_plan(P);
+    if (!H) { set_error(FT_B200_EINVAL, "not a plan created by this library"); return; }
+    if (TRANS != 'N' && TRANS != 'T') { set_error(FT_B200_EINVAL, "TRANS must be 'N' or 'T'"); return; }
+    if (!A) { set_error(FT_B200_EINVAL, "NULL matrix"); return; }
+    if (!valid_MN(H->kind, H->n, N, M)) return;
+    const size_t elems = (size_t) N * M;
+    if (elems > H->stage_elems) {
+        if (H->d_stage) cudaFree(H->d_stage);
+        H->d_stage = nullptr; H->stage_elems = 0;
+        if (!cuda_ok(cudaMalloc(&H->d_stage, elems * sizeof(double)), "cudaMalloc(stage)")) return;
+        H->stage_elems = elems;
+    }
+    if (!cuda_ok(cudaMemcpyAsync(H->d_stage, A, elems * sizeof(double), cudaMemcpyHostToDevice, H->stream), "cudaMemcpyAsync(H2D)")) return;
+    if (execute_dev_impl(H, forward, TRANS, H->d_stage, N, M, H->stream) != FT_B200_OK) { cudaStreamSynchronize(H->stream); return; }
+    if (!cuda_ok(cudaMemcpyAsync(A, H->d_stage, elems * sizeof(double), cudaMemcpyDeviceToHost, H->stream), "cudaMemcpyAsync(D2H)")) return;
+    cuda_ok(cudaStreamSynchronize(H->stream), "cudaStreamSynchronize");
+}
+
+void rotations_host(const ft_rotation_plan * RPc, bool hi2lo, double * A, int M, int kind) {
+    clear_error();
+    ft_rotation_plan * RP = const_cast<ft_rotation_plan *>(RPc);
+    if (!RP || !A) { set_error(FT_B200_EINVAL, "NULL argument"); return; }
+    if (RP->kind != kind) { set_error(FT_B200_EINVAL, "rotation plan of another family"); return; }
+    const size_t elems = (size_t) RP->n * M;
+    double * d = nullptr;
+    if (!cuda_ok(cudaMalloc(&d, elems * sizeof(double)), "cudaMalloc")) return;
+    if (cuda_ok(cudaMemcpy(d, A, elems * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy(H2D)") &&
+        rotations(RP, hi2lo, d, d, M, RP->n, 0) &&
+        cuda_ok(cudaDeviceSynchronize(), "cudaDeviceSynchronize"))
+        cuda_ok(cudaMemcpy(A, d, elems * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy(D2H)");
+    cudaFree(d);
+}
+
+}  // namespace
+}  // namespace ftb
+
+using namespace ftb;
+
+extern "C" {
+
+int ft_b200_last_status(void) { return t_status; }
+const char * ft_b200_last_error(void) { return t_message.c_str(); }
+unsigned long long ft_b200_kernel_launches(void) { return g_launches.load(); }
+
+int ft_b200_profile(int enable) {
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    for (auto & r : g_prof) { g_prof_pool.push_back(r.a); g_prof_pool.push_back(r.b); }
+    g_prof.clear();
+    g_prof_on = enable != 0;
+    return FT_B200_OK;
+}
+
+int ft_b200_profile_read(int family, double * ms, int * launches) {
+    clear_error();
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    double tot = 0;
+    int cnt = 0;
+    for (auto & r : g_prof) {
+        if (r.family != family) continue;
+        if (!cuda_ok(cudaEventSynchronize(r.b), "cudaEventSynchronize")) return t_status;
+        float t = 0;
+        if (!cuda_ok(cudaEventElapsedTime(&t, r.a, r.b), "cudaEventElapsedTime")) return t_status;
+        tot += t;
+        cnt++;
+    }
+    if (ms) *ms = tot;
+    if (launches) *launches = cnt;
+    return FT_B200_OK;
+}
+
+ft_harmonic_plan * ft_plan_sph2fourier(const int n) {
+    HarmonicPlan * H = make_harmonic_plan(SPH, n, 0, 0, 0);
+    return H ? &H->pub : nullptr;
+}
+ft_harmonic_plan * ft_plan_tri2cheb(const int n, const double alpha, const double beta, const double gamma) {
+    HarmonicPlan * H = make_harmonic_plan(TRI, n, alpha, beta, gamma);
+    return H ? &H->pub : nullptr;
+}
+ft_harmonic_plan * ft_plan_disk2cxf(const int n, const double alpha, const double beta) {
+    HarmonicPlan * H = make_harmonic_plan(DISK, n, alpha, beta, 0);
+    return H ? &H->pub : nullptr;
+}
+
+void ft_destroy_harmonic_plan(ft_harmonic_plan * P) {
+    HarmonicPlan * H = as_plan(P);
+    if (!H) return;
+    if (H->stream) { cudaStreamSynchronize(H->stream); cudaStreamDestroy(H->stream); }
+    if (H->rp_arr[0]) ft_destroy_rotation_plan(H->rp_arr[0]);
+    for (int i = 0; i < 2; i++) {
+        std::free(H->hostP[i]); std::free(H->hostPinv[i]);
+        if (H->dP[i]) cudaFree(H->dP[i]);
+        if (H->dPinv[i]) cudaFree(H->dPinv[i]);
+    }
+    if (H->d_scratch) cudaFree(H->d_scratch);
+    if (H->d_stage) cudaFree(H->d_stage);
+    H->magic = 0;
+    delete H;
+}
+
+void ft_execute_sph2fourier(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M) { execute_host(P, true, TRANS, A, N, M); }
+void ft_execute_fourier2sph(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M) { execute_host(P, false, TRANS, A, N, M); }
+void ft_execute_tri2cheb(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M) { execute_host(P, true, TRANS, A, N, M); }
+void ft_execute_cheb2tri(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M) { execute_host(P, false, TRANS, A, N, M); }
+void ft_execute_disk2cxf(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M) { execute_host(P, true, TRANS, A, N, M); }
+void ft_execute_cxf2disk(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M) { execute_host(P, false, TRANS, A, N, M); }
+
+ft_rotation_plan * ft_plan_rotsphere(const int n) { return make_rotation_plan(SPH, n, 0, 0, 0); }
+ft_rotation_plan * ft_plan_rottriangle(const int n, const double alpha, const double beta, const double gamma) { return make_rotation_plan(TRI, n, alpha, beta, gamma); }
+ft_rotation_plan * ft_plan_rotdisk(const int n, const double alpha, const double beta) { return make_rotation_plan(DISK, n, alpha, beta, 0); }
+
+void ft_destroy_rotation_plan(ft_rotation_plan * RP) {
+    if (!RP) return;
+    if (RP->tasks) {
+        for (auto & kv : *RP->tasks) if (kv.second.first) cudaFree(kv.second.first);
+        delete RP->tasks;
+    }
+    delete RP->mu;
+    if (RP->d_sc) cudaFree(RP->d_sc);
+    if (RP->d_counter) cudaFree(RP->d_counter);
+    std::free(RP->s);
+    std::free(RP->c);
+    delete RP;
+}
+
+void ft_execute_sph_hi2lo(const ft_rotation_plan * RP, double * A, double *, const int M) { rotations_host(RP, true, A, M, SPH); }
+void ft_execute_sph_lo2hi(const ft_rotation_plan * RP, double * A, double *, const int M) { rotations_host(RP, false, A, M, SPH); }
+void ft_execute_tri_hi2lo(const ft_rotation_plan * RP, double * A, double *, const int M) { rotations_host(RP, true, A, M, TRI); }
+void ft_execute_tri_lo2hi(const ft_rotation_plan * RP, double * A, double *, const int M) { rotations_host(RP, false, A, M, TRI); }
+void ft_execute_disk_hi2lo(const ft_rotation_plan * RP, double * A, double *, const int M) { rotations_host(RP, true, A, M, DISK); }
+void ft_execute_disk_lo2hi(const ft_rotation_plan * RP, double * A, double *, const int M) { rotations_host(RP, false, A, M, DISK); }
+
+int ft_b200_execute_dev(const ft_harmonic_plan * P, int forward, char TRANS, double * dA, int N, int M, void * stream) {
+    clear_error();
+    HarmonicPlan * H = as_plan(P);
+    if (!H) { set_error(FT_B200_EINVAL, "not a plan created by this library"); return t_status; }
+    return execute_dev_impl(H, forward != 0, TRANS, dA, N, M, static_cast<cudaStream_t>(stream));
+}
+
+int ft_b200_rotations_dev(const ft_rotation_plan * RP, int hi2lo, double * dA, int M, void * stream) {
+    clear_error();
+    if (!RP || !dA || M < 1) { set_error(FT_B200_EINVAL, "bad argument"); return t_status; }
+    rotations(const_cast<ft_rotation_plan *>(RP), hi2lo != 0, dA, dA, M, RP->n, static_cast<cudaStream_t>(stream));
+    return t_status;
+}
+
+int ft_b200_plan_kind(const ft_harmonic_plan * P) {
+    HarmonicPlan * H = as_plan(P);
+    return H ? H->kind : -1;
+}
+int ft_b200_plan_device(const ft_harmonic_plan * P) {
+    HarmonicPlan * H = as_plan(P);
+    return H ? H->device : -1;
+}
+
+int ft_b200_execute_batched_dev(const ft_harmonic_plan * const * plans, int forward, char TRANS,
+                                double * const * dA, const int * N, const int * M, int nfields, void * stream) {
+    clear_error();
+    if (!plans || !dA || !N || !M || nfields < 0) { set_error(FT_B200_EINVAL, "bad argument"); return t_status; }
+    for (int f = 0; f < nfields; f++) {
+        if (execute_dev_impl(as_plan(plans[f]), forward != 0, TRANS, dA[f], N[f], M[f], static_cast<cudaStream_t>(stream)) != FT_B200_OK)
+            return t_status;
+    }
+    return FT_B200_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,151 @@
+// Internal declarations shared by the host plan code and the CUDA kernels.
+#pragma once
+
+#include <algorithm>
+#include <cstddef>
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/ft_b200.h"
+
+namespace ftb {
+
+enum Kind { SPH = 0, TRI = 1, DISK = 2 };
+
+// ---------------------------------------------------------------------------
+// Rotation geometry.
+//
+// A column of the coefficient matrix is swept by Givens rotations G(k, k+d)
+// (d = 2 for sph: rows of equal parity; d = 1 for tri and disk).  Splitting a
+// sph column into its even and odd rows gives two independent "chains" in
+// which every rotation couples neighbouring chain positions (i, i+1); tri and
+// disk columns are a single chain.  Chain position i of chain c is row
+// 2i + c (sph) or row i (tri, disk).
+//
+// Sweep j rotates positions (i, i+1) for i = 0 .. top(j, c).  Consecutive
+// sweeps of one column differ by STEP in j (2 for sph and disk: orders keep
+// their parity; 1 for tri) and their tops by exactly one position, the fact
+// the wavefront schedule in rotations.cu is built on.
+//   sph  (src/rotations/rotations_default.c:31-43):  top = floor((N-3-j-c)/2)
+//   tri  (src/rotations/rotations_default.c:45-57):  top = N-2-j
+//   disk (src/rotations/rotations_default.c:59-71):  top = N-2-floor((j+1)/2)
+// Sine/cosine tables use the reference packings (src/rotations/rotations.h:6-10).
+// ---------------------------------------------------------------------------
+struct Geo {
+    __host__ __device__ static inline int floordiv2(int x) { return x >= 0 ? x / 2 : -((1 - x) / 2); }
+    __host__ __device__ static inline int chains(int kind) { return kind == SPH ? 2 : 1; }
+    __host__ __device__ static inline int step(int kind) { return kind == TRI ? 1 : 2; }
+    __host__ __device__ static inline int top(int kind, int N, int j, int c) {
+        if (kind == SPH) return floordiv2(N - 3 - j - c);
+        if (kind == TRI) return N - 2 - j;
+        return N - 2 - (j + 1) / 2;
+    }
+    // number of positions of chain c in a column of N rows
+    __host__ __device__ static inline int chain_len(int kind, int N, int c) {
+        return kind == SPH ? (N - c + 1) / 2 : N;
+    }
+    // packed table offset of column j (entry l of sweep j is at offset + l)
+    __host__ __device__ static inline long long table_base(int kind, int N, int j) {
+        if (kind == DISK) return (long long) j * N - (long long) (j / 2) * ((j + 1) / 2);
+        return (long long) j * (2 * N + 1 - j) / 2;
+    }
+    __host__ __device__ static inline long long table_len(int kind, int N) {
+        return kind == DISK ? (long long) N * N : (long long) N * (N + 1) / 2;
+    }
+    // number of order columns the rotation stage visits for an N x M matrix
+    // sph / disk: pairs (2m-1, 2m), m = 2 .. M/2; tri: column m, m = 1 .. M-1
+    __host__ __device__ static inline int first_order(int kind) { return kind == TRI ? 1 : 2; }
+    __host__ __device__ static inline int last_order(int kind, int M) { return kind == TRI ? M - 1 : M / 2; }
+};
+
+// A unit of work of the rotation kernel: up to 32 columns that share their
+// sweeps.  sph / disk: 16 orders of one parity, m = mbase + 2*o (o < 16), two
+// columns each; tri: 32 consecutive orders m = mbase + o.
+struct RotTask {
+    int field;   // index into the field table of the launch
+    int mbase;   // lowest order of the group
+};
+
+// One coefficient matrix of a launch.
+struct RotField {
+    const double * in;      // first pass reads here
+    double * out;           // every pass writes here (in == out allowed)
+    const double2 * sc;     // interleaved (sin, cos) table in the reference packing
+    int N, M, kind;
+    long long lda;
+};
+
+// Kernel launchers (rotations.cu).  The field table travels by value in the
+// kernel parameters (CUDA 12 allows up to 32 KB of parameters).
+constexpr int kMaxFields = 128;
+struct RotLaunch {
+    RotField fields[kMaxFields];
+    int nfields;
+    const RotTask * tasks;     // device, longest first
+    int ntasks;
+    int * counter;             // device work counter (reset by the launcher)
+};
+cudaError_t launch_rotations(int kind, bool hi2lo, const RotLaunch & L, int max_ctas, cudaStream_t st);
+int rotation_ctas_per_sm(int kind);
+
+// Triangular multiplies (trmm.cu).  Out = op(U) * In on column classes.
+struct TrmmClass {
+    const double * U;     // n x n upper triangular, column-major, ld = n
+    const double * in;    // first column of the class
+    double * out;
+    int ncols;            // columns in the class
+};
+struct TrmmLaunch {
+    TrmmClass cls[4];
+    int nclasses;
+    int n;
+    long long ld_in, ld_out;   // column stride within a class (4N for sph/disk, N for tri)
+    bool trans;                // op(U) = U^T
+};
+cudaError_t launch_trmm(const TrmmLaunch & L, cudaStream_t st);
+// Right multiply for tri: Out = In * op(U) (rows of In are independent).
+cudaError_t launch_trmm_right(const double * U, const double * in, double * out, int n, int nrows,
+                              long long ld, bool trans, cudaStream_t st);
+// tri normalisation (src/drivers.c:6-24), in place
+cudaError_t launch_cheb_normalize(double * A, int N, int M, long long lda, bool transposed, cudaStream_t st);
+
+// Host plan generation (plan.cpp).
+void rotation_tables(int kind, int n, double alpha, double beta, double gamma, double * s, double * c);
+double * connection_legendre_to_chebyshev(int normleg, int normcheb, int n);
+double * connection_chebyshev_to_legendre(int normcheb, int normleg, int n);
+double * connection_ultraspherical(int norm1, int norm2, int n, double lambda, double mu);
+double * connection_jacobi(int n, double alpha, double beta, double gamma, double delta);
+std::vector<RotTask> build_tasks(int kind, int N, int M, int field);
+double task_cost(int kind, int N, int M, int mbase);
+
+// Error state (api.cu).
+void set_error(int status, const std::string & msg);
+void clear_error();
+void count_launch(unsigned long long n = 1);
+// measurement hook: bracket a launch with events on its stream when profiling is on
+enum { FAM_ROT = 0, FAM_TRMM = 1, FAM_OTHER = 2 };
+void prof_begin(int family, cudaStream_t st);
+void prof_end(cudaStream_t st);
+
+}  // namespace ftb
+
+// The rotation plan behind the public opaque type.  The first three members
+// mirror the reference's struct so code that reads RP->s / RP->c / RP->n works.
+struct ft_rotation_plan_s {
+    double * s;
+    double * c;
+    int n;
+    // ---- B200 state ----
+    int kind;
+    double alpha, beta, gamma;
+    int device;
+    double2 * d_sc;            // interleaved table
+    int * d_counter;           // work counter for the persistent kernel
+    std::mutex * mu;
+    std::map<int, std::pair<ftb::RotTask *, int>> * tasks;   // M -> device task list (longest first)
+};

@@ -1,0 +1,49 @@
+"""Seeded fills in the reference's coefficient layouts.
+
+The reference's test utilities fill the triangular layouts with unseeded
+``rand()`` (src/ftutilities.c:75-113).  These fills use a counter-based
+splitmix64 generator instead, so the same (kind, n, seed) gives the same
+matrix on every machine: the value at column-major linear index idx is
+2u - 1 with u the top 53 bits of mix(seed + (idx + 1) * 0x9E3779B97F4A7C15)
+divided by 2^53; entries outside the layout's triangle are zero.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+__all__ = ["layout_cols", "sphrand", "trirand", "diskrand", "rand_layout"]
+
+_STEP = {"sph": 2, "tri": 1, "disk": 4}
+
+
+def layout_cols(kind: str, n: int) -> int:
+    """Columns M of the layout for n rows: 2n-1 (sph), n (tri), 4n-3 (disk)."""
+    return {"sph": 2 * n - 1, "tri": n, "disk": 4 * n - 3}[kind]
+
+
+def rand_layout(kind: str, n: int, seed: int) -> np.ndarray:
+    """n x M float64 matrix, Fortran order, U(-1, 1) inside the layout's triangle."""
+    M = layout_cols(kind, n)
+    i = np.arange(n, dtype=np.int64)[:, None]
+    j = np.arange(M, dtype=np.int64)[None, :]
+    on = j < M - _STEP[kind] * i
+    idx = (i + j * n).astype(np.uint64)
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed) + (idx + np.uint64(1)) * np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    u = (z >> np.uint64(11)).astype(np.float64) * 2.0 ** -53
+    return np.asfortranarray(np.where(on, 2.0 * u - 1.0, 0.0))
+
+
+def sphrand(n: int, seed: int) -> np.ndarray:
+    return rand_layout("sph", n, seed)
+
+
+def trirand(n: int, seed: int) -> np.ndarray:
+    return rand_layout("tri", n, seed)
+
+
+def diskrand(n: int, seed: int) -> np.ndarray:
+    return rand_layout("disk", n, seed)

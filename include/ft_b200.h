@@ -1,0 +1,164 @@
+/*
+ * ft_b200.h -- C ABI of the B200 (sm_100a) harmonic-conversion library.
+ *
+ * Drop-in for FastTransforms' harmonic-conversion path: the Givens-rotation
+ * sweeps behind sph2fourier / fourier2sph and the same kernel family used by
+ * tri2cheb / cheb2tri and disk2cxf / cxf2disk.  Link with -lft_b200 instead of
+ * -lfasttransforms; existing callers of the functions below need no change.
+ *
+ * Conventions (identical to the reference):
+ *   - A is column-major with leading dimension N (host memory for the drop-in
+ *     entry points, device memory for the *_dev entry points);
+ *     M = 2N-1 (sph), N (tri), 4N-3 (disk).
+ *   - Column pair (2m-1, 2m) carries order m for sph and disk; column m for tri.
+ *   - TRANS 'N' applies the operator, 'T' its transpose; any other character
+ *     is a no-op (the reference silently ignores it; here the status is
+ *     FT_B200_EINVAL and A is left untouched).
+ *   - In place on A.  The plan owns its device scratch, so two concurrent
+ *     executes on ONE plan are not reentrant (as in the reference, whose plan
+ *     owns P->B).  Different plans may run concurrently on different streams.
+ *
+ * Everything runs on the current CUDA device.  There is no CPU fallback: if no
+ * sm_100 device is present, plan creation fails (NULL) and the status says why.
+ */
+#ifndef FT_B200_H
+#define FT_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes and errors (the reference has none: it prints and exits).   */
+/* ------------------------------------------------------------------------ */
+#define FT_B200_OK          0
+#define FT_B200_EINVAL      1   /* bad TRANS, sizes that do not match the plan, NULL pointers */
+#define FT_B200_ECUDA       2   /* a CUDA runtime call failed (message has the CUDA error) */
+#define FT_B200_ENOMEM      3   /* device or host allocation failed */
+#define FT_B200_ENODEV      4   /* no usable sm_100 device */
+#define FT_B200_ETIMEOUT    5   /* a bounded device-side wait ran out (queue stalled) */
+#define FT_B200_EUNSUPPORTED 6  /* option not supported for this plan kind */
+
+/* Status of the last call made on this host thread (0 = success). */
+int ft_b200_last_status(void);
+/* Human-readable message for the last failure on this host thread ("" if none). */
+const char * ft_b200_last_error(void);
+
+/* ------------------------------------------------------------------------ */
+/* Plan structures.                                                         */
+/* ------------------------------------------------------------------------ */
+
+/* Rotation plan.  The first three members are layout-compatible with the
+ * reference's struct (src/ftinternal.h:370-374): host copies of the sine and
+ * cosine tables in the reference's packing, and n.  The rest is device state. */
+typedef struct ft_rotation_plan_s ft_rotation_plan;
+
+/* Harmonic plan.  Layout-compatible prefix with the reference's public struct
+ * (src/fasttransforms.h:370-385): RP, MP, B, P, Pinv, alpha..rho, NRP, NMP, NP,
+ * with host copies of the connection matrices in P / Pinv and NULL MP.  B is a
+ * device pointer to the plan's scratch (the reference's host scratch). */
+typedef struct {
+    ft_rotation_plan ** RP;
+    void ** MP;
+    double * B;
+    double ** P;
+    double ** Pinv;
+    double alpha;
+    double beta;
+    double gamma;
+    double delta;
+    double rho;
+    int NRP;
+    int NMP;
+    int NP;
+} ft_harmonic_plan;
+
+/* ------------------------------------------------------------------------ */
+/* Drop-in entry points: same names, signatures and meaning as the          */
+/* reference (src/fasttransforms.h:297-415).  Host pointers.  Errors are    */
+/* reported through ft_b200_last_status() / ft_b200_last_error().           */
+/* ------------------------------------------------------------------------ */
+
+/* replaces ft_plan_sph2fourier, src/drivers.c:816-831 */
+ft_harmonic_plan * ft_plan_sph2fourier(const int n);
+/* replaces ft_execute_sph2fourier, src/drivers.c:833-848 */
+void ft_execute_sph2fourier(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M);
+/* replaces ft_execute_fourier2sph, src/drivers.c:850-865 */
+void ft_execute_fourier2sph(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M);
+
+/* replaces ft_plan_tri2cheb, src/drivers.c:901-919 */
+ft_harmonic_plan * ft_plan_tri2cheb(const int n, const double alpha, const double beta, const double gamma);
+/* replaces ft_execute_tri2cheb, src/drivers.c:921-938 */
+void ft_execute_tri2cheb(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M);
+/* replaces ft_execute_cheb2tri, src/drivers.c:940-957 */
+void ft_execute_cheb2tri(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M);
+
+/* replaces ft_plan_disk2cxf, src/drivers.c:959-987 */
+ft_harmonic_plan * ft_plan_disk2cxf(const int n, const double alpha, const double beta);
+/* replaces ft_execute_disk2cxf, src/drivers.c:989-1004 */
+void ft_execute_disk2cxf(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M);
+/* replaces ft_execute_cxf2disk, src/drivers.c:1006-1021 */
+void ft_execute_cxf2disk(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M);
+
+/* replaces ft_destroy_harmonic_plan, src/drivers.c:793-814 */
+void ft_destroy_harmonic_plan(ft_harmonic_plan * P);
+
+/* Rotation level. */
+/* replaces ft_plan_rotsphere, src/rotations.c:116-133 */
+ft_rotation_plan * ft_plan_rotsphere(const int n);
+/* replaces ft_plan_rottriangle, src/rotations.c:143-160 */
+ft_rotation_plan * ft_plan_rottriangle(const int n, const double alpha, const double beta, const double gamma);
+/* replaces ft_plan_rotdisk, src/rotations.c:173-190 */
+ft_rotation_plan * ft_plan_rotdisk(const int n, const double alpha, const double beta);
+/* replaces ft_destroy_rotation_plan, src/rotations.c:6-10 */
+void ft_destroy_rotation_plan(ft_rotation_plan * RP);
+/* replace ft_execute_{sph,tri,disk}_{hi2lo,lo2hi}, src/drivers.c:58-92, 278-312, 378-412.
+ * B is the reference's host scratch argument; it is accepted and not used. */
+void ft_execute_sph_hi2lo(const ft_rotation_plan * RP, double * A, double * B, const int M);
+void ft_execute_sph_lo2hi(const ft_rotation_plan * RP, double * A, double * B, const int M);
+void ft_execute_tri_hi2lo(const ft_rotation_plan * RP, double * A, double * B, const int M);
+void ft_execute_tri_lo2hi(const ft_rotation_plan * RP, double * A, double * B, const int M);
+void ft_execute_disk_hi2lo(const ft_rotation_plan * RP, double * A, double * B, const int M);
+void ft_execute_disk_lo2hi(const ft_rotation_plan * RP, double * A, double * B, const int M);
+
+/* ------------------------------------------------------------------------ */
+/* Device-pointer entry points (no host copies).  A is a device pointer     */
+/* (N x M, leading dimension N); stream is a cudaStream_t (NULL = legacy    */
+/* default stream).  Asynchronous: they return once the work is enqueued.   */
+/* Return FT_B200_OK or an error code.                                      */
+/* ------------------------------------------------------------------------ */
+enum { FT_B200_SPH = 0, FT_B200_TRI = 1, FT_B200_DISK = 2 };
+
+/* Full transform.  forward = 1: sph2fourier / tri2cheb / disk2cxf;
+ * forward = 0: fourier2sph / cheb2tri / cxf2disk. */
+int ft_b200_execute_dev(const ft_harmonic_plan * P, int forward, char TRANS, double * dA, int N, int M, void * stream);
+/* Rotation stage alone (hi2lo = 1: ft_execute_*_hi2lo; 0: *_lo2hi). */
+int ft_b200_rotations_dev(const ft_rotation_plan * RP, int hi2lo, double * dA, int M, void * stream);
+
+/* Batched drop-in: nfields fields, each with its own plan (plans may repeat,
+ * degrees may differ), all in one persistent launch per stage.  dA[f] is the
+ * device pointer of field f, N[f] x M[f].  Same transform and TRANS for all. */
+int ft_b200_execute_batched_dev(const ft_harmonic_plan * const * plans, int forward, char TRANS,
+                                double * const * dA, const int * N, const int * M, int nfields, void * stream);
+
+/* Kind of a plan (FT_B200_SPH / TRI / DISK), or -1. */
+int ft_b200_plan_kind(const ft_harmonic_plan * P);
+/* Device id the plan lives on. */
+int ft_b200_plan_device(const ft_harmonic_plan * P);
+
+/* Number of kernels this library launched since load (all entry points). */
+unsigned long long ft_b200_kernel_launches(void);
+
+/* Measurement hook.  While enabled, every kernel launch is bracketed by a pair
+ * of CUDA events recorded on its launch stream.  ft_b200_profile(1) resets the
+ * record; ft_b200_profile_read waits for the recorded events and returns, for
+ * one kernel family (0 = rotation sweeps, 1 = triangular multiplies, 2 = other),
+ * the summed device time in ms and the launch count.  Off by default. */
+int ft_b200_profile(int enable);
+int ft_b200_profile_read(int family, double * ms, int * launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,213 @@
+"""ctypes bindings for the two CPU oracles -- TEST INFRASTRUCTURE ONLY.
+
+* ``Oracle``: the plain-C restatement in ``oracle/ft_oracle.c`` (built into
+  ``oracle/_build/libft_oracle.so``).
+* ``Reference``: the reference FastTransforms library compiled from its own
+  sources by ``oracle/ref_build/Makefile`` into ``oracle/_ref/libft_ref.so``;
+  absent when the reference sources were not available at build time.
+
+Only tests, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg use
+this module.  Arrays are numpy float64 in Fortran (column-major) order, N x M,
+exactly the reference's layout (``src/fasttransforms.h:370-415``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "libft_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libft_ref.so")
+
+SPH, TRI, DISK = 0, 1, 2
+KIND = {"sph": SPH, "tri": TRI, "disk": DISK}
+
+
+def layout_cols(kind: str, n: int) -> int:
+    """Number of columns M of the reference layout for degree n-1."""
+    return {"sph": 2 * n - 1, "tri": n, "disk": 4 * n - 3}[kind]
+
+
+def fill(kind: str, n: int, seed: int) -> np.ndarray:
+    """Seeded U(-1,1) fill in the reference's triangular layouts (src/ftutilities.c:75-113).
+
+    Counter-based splitmix64 on the column-major linear index; identical to
+    ``oracle_fill`` in ft_oracle.c and to ``fasttransforms_b200.utilities``.
+    """
+    M = layout_cols(kind, n)
+    i = np.arange(n, dtype=np.int64)[:, None]
+    j = np.arange(M, dtype=np.int64)[None, :]
+    step = {"sph": 2, "tri": 1, "disk": 4}[kind]
+    on = j < M - step * i
+    idx = (i + j * n).astype(np.uint64)
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed) + (idx + np.uint64(1)) * np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    u = (z >> np.uint64(11)).astype(np.float64) * 2.0 ** -53
+    A = np.where(on, 2.0 * u - 1.0, 0.0)
+    return np.asfortranarray(A)
+
+
+def _ptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.f_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class _OraclePlan(C.Structure):
+    _fields_ = [("kind", C.c_int), ("n", C.c_int), ("s", C.POINTER(C.c_double)),
+                ("c", C.POINTER(C.c_double)), ("P", C.POINTER(C.c_double) * 2),
+                ("Pinv", C.POINTER(C.c_double) * 2), ("alpha", C.c_double),
+                ("beta", C.c_double), ("gamma", C.c_double)]
+
+
+class Oracle:
+    """The C restatement."""
+
+    def __init__(self, path: str = ORACLE_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"oracle library not built: {path} (run make -C oracle)")
+        L = self.lib = C.CDLL(path)
+        PP = C.POINTER(_OraclePlan)
+        L.oracle_plan_sph2fourier.restype = PP
+        L.oracle_plan_sph2fourier.argtypes = [C.c_int]
+        L.oracle_plan_tri2cheb.restype = PP
+        L.oracle_plan_tri2cheb.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double]
+        L.oracle_plan_disk2cxf.restype = PP
+        L.oracle_plan_disk2cxf.argtypes = [C.c_int, C.c_double, C.c_double]
+        L.oracle_plan_rotations.restype = PP
+        L.oracle_plan_rotations.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
+        L.oracle_destroy_plan.argtypes = [PP]
+        L.oracle_execute.argtypes = [PP, C.c_int, C.c_char, C.POINTER(C.c_double), C.c_int, C.c_int]
+        for f in ("oracle_execute_hi2lo", "oracle_execute_lo2hi"):
+            getattr(L, f).argtypes = [PP, C.POINTER(C.c_double), C.c_int]
+        for f in ("oracle_kernel_hi2lo", "oracle_kernel_lo2hi"):
+            getattr(L, f).argtypes = [PP, C.c_int, C.c_int, C.POINTER(C.c_double), C.c_int]
+        L.oracle_set_fused.argtypes = [C.c_int]
+        L.oracle_fill.argtypes = [C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.POINTER(C.c_double)]
+        dp = C.POINTER(C.c_double)
+        L.oracle_plan_legendre_to_chebyshev.restype = dp
+        L.oracle_plan_legendre_to_chebyshev.argtypes = [C.c_int, C.c_int, C.c_int]
+        L.oracle_plan_chebyshev_to_legendre.restype = dp
+        L.oracle_plan_chebyshev_to_legendre.argtypes = [C.c_int, C.c_int, C.c_int]
+        L.oracle_plan_ultraspherical_to_ultraspherical.restype = dp
+        L.oracle_plan_ultraspherical_to_ultraspherical.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double]
+        L.oracle_plan_jacobi_to_jacobi.restype = dp
+        L.oracle_plan_jacobi_to_jacobi.argtypes = [C.c_int, C.c_int, C.c_int] + [C.c_double] * 4
+        self._libc = C.CDLL(None)
+        self._libc.free.argtypes = [C.c_void_p]
+
+    def set_fused(self, fused: bool):
+        self.lib.oracle_set_fused(1 if fused else 0)
+
+    def plan(self, kind: str, n: int, alpha=0.0, beta=0.0, gamma=0.0, rotations_only=False):
+        L = self.lib
+        if rotations_only:
+            return L.oracle_plan_rotations(KIND[kind], n, alpha, beta, gamma)
+        if kind == "sph":
+            return L.oracle_plan_sph2fourier(n)
+        if kind == "tri":
+            return L.oracle_plan_tri2cheb(n, alpha, beta, gamma)
+        return L.oracle_plan_disk2cxf(n, alpha, beta)
+
+    def destroy(self, P):
+        self.lib.oracle_destroy_plan(P)
+
+    def execute(self, P, forward: bool, trans: str, A: np.ndarray):
+        N, M = A.shape
+        self.lib.oracle_execute(P, 1 if forward else 0, trans.encode(), _ptr(A), N, M)
+
+    def hi2lo(self, P, A):
+        self.lib.oracle_execute_hi2lo(P, _ptr(A), A.shape[1])
+
+    def lo2hi(self, P, A):
+        self.lib.oracle_execute_lo2hi(P, _ptr(A), A.shape[1])
+
+    def kernel(self, P, hi2lo: bool, m1: int, m2: int, col: np.ndarray):
+        a = np.asfortranarray(col.reshape(-1, 1))
+        f = self.lib.oracle_kernel_hi2lo if hi2lo else self.lib.oracle_kernel_lo2hi
+        f(P, m1, m2, _ptr(a), 1)
+        return a.ravel()
+
+    def tables(self, P):
+        p = P.contents
+        n = p.n
+        ln = n * n if p.kind == DISK else n * (n + 1) // 2
+        s = np.ctypeslib.as_array(p.s, shape=(ln,)).copy()
+        c = np.ctypeslib.as_array(p.c, shape=(ln,)).copy()
+        return s, c
+
+    def connection(self, P):
+        p = P.contents
+        n = p.n
+        get = lambda q: np.ctypeslib.as_array(q, shape=(n * n,)).reshape(n, n, order="F").copy()
+        return [get(p.P[0]), get(p.P[1])], [get(p.Pinv[0]), get(p.Pinv[1])]
+
+    def fill(self, kind: str, n: int, seed: int) -> np.ndarray:
+        M = layout_cols(kind, n)
+        A = np.zeros((n, M), order="F")
+        self.lib.oracle_fill(KIND[kind], n, M, seed, _ptr(A))
+        return A
+
+
+class _RefHarmonicPlan(C.Structure):
+    # src/fasttransforms.h:370-385
+    _fields_ = [("RP", C.c_void_p), ("MP", C.c_void_p), ("B", C.c_void_p),
+                ("P", C.POINTER(C.POINTER(C.c_double))), ("Pinv", C.POINTER(C.POINTER(C.c_double))),
+                ("alpha", C.c_double), ("beta", C.c_double), ("gamma", C.c_double),
+                ("delta", C.c_double), ("rho", C.c_double),
+                ("NRP", C.c_int), ("NMP", C.c_int), ("NP", C.c_int)]
+
+
+class Reference:
+    """The reference library compiled from its own sources (oracle/_ref)."""
+
+    _FWD = {"sph": "ft_execute_sph2fourier", "tri": "ft_execute_tri2cheb", "disk": "ft_execute_disk2cxf"}
+    _BWD = {"sph": "ft_execute_fourier2sph", "tri": "ft_execute_cheb2tri", "disk": "ft_execute_cxf2disk"}
+
+    @staticmethod
+    def available(path: str = REF_SO) -> bool:
+        return os.path.exists(path)
+
+    def __init__(self, path: str = REF_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"reference library not built: {path}")
+        L = self.lib = C.CDLL(path)
+        HP = C.POINTER(_RefHarmonicPlan)
+        L.ft_plan_sph2fourier.restype = HP
+        L.ft_plan_sph2fourier.argtypes = [C.c_int]
+        L.ft_plan_tri2cheb.restype = HP
+        L.ft_plan_tri2cheb.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double]
+        L.ft_plan_disk2cxf.restype = HP
+        L.ft_plan_disk2cxf.argtypes = [C.c_int, C.c_double, C.c_double]
+        L.ft_destroy_harmonic_plan.argtypes = [HP]
+        for f in list(self._FWD.values()) + list(self._BWD.values()):
+            getattr(L, f).argtypes = [C.c_char, HP, C.POINTER(C.c_double), C.c_int, C.c_int]
+        L.ft_set_num_threads.argtypes = [C.c_int]
+
+    def set_num_threads(self, t: int):
+        self.lib.ft_set_num_threads(t)
+
+    def plan(self, kind: str, n: int, alpha=0.0, beta=0.0, gamma=0.0):
+        L = self.lib
+        if kind == "sph":
+            return L.ft_plan_sph2fourier(n)
+        if kind == "tri":
+            return L.ft_plan_tri2cheb(n, alpha, beta, gamma)
+        return L.ft_plan_disk2cxf(n, alpha, beta)
+
+    def destroy(self, P):
+        self.lib.ft_destroy_harmonic_plan(P)
+
+    def execute(self, kind: str, P, forward: bool, trans: str, A: np.ndarray):
+        N, M = A.shape
+        f = getattr(self.lib, (self._FWD if forward else self._BWD)[kind])
+        f(trans.encode(), P, _ptr(A), N, M)
+
+    def connection(self, P, n: int):
+        p = P.contents
+        get = lambda q: np.ctypeslib.as_array(q, shape=(n * n,)).reshape(n, n, order="F").copy()
+        return [get(p.P[0]), get(p.P[1])], [get(p.Pinv[0]), get(p.Pinv[1])]

@@ -1,0 +1,709 @@
+/*
+ * ft_oracle.c -- TEST INFRASTRUCTURE ONLY (see ft_oracle.h).
+ *
+ * CPU restatement of FastTransforms' harmonic-conversion path.  Every function
+ * names the reference file:line it restates (paths relative to the reference
+ * project root).  Where bit-for-bit agreement with the reference's plans is
+ * wanted (the connection matrices are built in long double and rounded), the
+ * arithmetic expressions keep the reference's association order.
+ *
+ * Build: make -C oracle  ->  oracle/_build/libft_oracle.so
+ */
+#define _GNU_SOURCE
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include "ft_oracle.h"
+
+#define MIN(a, b) ((a) < (b) ? (a) : (b))
+#define MAX(a, b) ((a) > (b) ? (a) : (b))
+
+static int g_fused = 1;
+void oracle_set_fused(int fused) { g_fused = fused ? 1 : 0; }
+
+/* ---------------------------------------------------------------------------
+ * Rotation tables.
+ * ------------------------------------------------------------------------- */
+
+/* packed triangle index for sph / tri: src/rotations/rotations.h:6-7 */
+static inline size_t tri_idx(int n, int l, int m) { return (size_t) l + (size_t) m * (2 * n + 1 - m) / 2; }
+/* disk packing: src/rotations/rotations.h:9-10 */
+static inline size_t disk_idx(int n, int l, int m) { return (size_t) l + (size_t) m * n - (size_t) (m / 2) * ((m + 1) / 2); }
+
+/* src/rotations.c:116-133 (ft_plan_rotsphere) */
+static void plan_rotsphere(int n, double * s, double * c) {
+    for (int m = 0; m < n; m++)
+        for (int l = 0; l < n - m; l++) {
+            double nums = (l + 1) * (l + 2);
+            double numc = (2 * m + 2) * (2 * l + 2 * m + 5);
+            double den = (l + 2 * m + 3) * (l + 2 * m + 4);
+            s[tri_idx(n, l, m)] = sqrt(nums / den);
+            c[tri_idx(n, l, m)] = sqrt(numc / den);
+        }
+}
+
+/* src/rotations.c:143-160 (ft_plan_rottriangle) */
+static void plan_rottriangle(int n, double alpha, double beta, double gamma, double * s, double * c) {
+    for (int m = 0; m < n; m++)
+        for (int l = 0; l < n - m; l++) {
+            double nums = (l + 1) * (l + alpha + 1);
+            double numc = (2 * m + beta + gamma + 2) * (2 * l + 2 * m + alpha + beta + gamma + 4);
+            double den = (l + 2 * m + beta + gamma + 3) * (l + 2 * m + alpha + beta + gamma + 3);
+            s[tri_idx(n, l, m)] = sqrt(nums / den);
+            c[tri_idx(n, l, m)] = sqrt(numc / den);
+        }
+}
+
+/* src/rotations.c:173-190 (ft_plan_rotdisk); note the negated sine */
+static void plan_rotdisk(int n, double alpha, double beta, double * s, double * c) {
+    for (int m = 0; m < 2 * n - 1; m++)
+        for (int l = 0; l < n - (m + 1) / 2; l++) {
+            double nums = (l + 1) * (l + beta + 1);
+            double numc = (m + alpha + 1) * (2 * l + m + alpha + beta + 3);
+            double den = (l + m + alpha + 2) * (l + m + alpha + beta + 2);
+            s[disk_idx(n, l, m)] = -sqrt(nums / den);
+            c[disk_idx(n, l, m)] = sqrt(numc / den);
+        }
+}
+
+/* ---------------------------------------------------------------------------
+ * Givens rotations: src/rotations/rotations_default.c:3-15 (scalar form) and
+ * src/rotations/rotations_AVX512F.c:4-15 (fused form).
+ * ------------------------------------------------------------------------- */
+
+static inline void givens(double S, double C, double * X, double * Y) {
+    double x0 = *X, y0 = *Y;
+    if (g_fused) {
+        double sy = S * y0, sx = S * x0;
+        *X = fma(C, x0, sy);
+        *Y = fma(C, y0, -sx);
+    } else {
+        double cx = C * x0, sy = S * y0, cy = C * y0, sx = S * x0;
+        *X = cx + sy;
+        *Y = cy - sx;
+    }
+}
+
+static inline void givens_t(double S, double C, double * X, double * Y) {
+    double x0 = *X, y0 = *Y;
+    if (g_fused) {
+        double sy = S * y0, sx = S * x0;
+        *X = fma(C, x0, -sy);
+        *Y = fma(C, y0, sx);
+    } else {
+        double cx = C * x0, sy = S * y0, cy = C * y0, sx = S * x0;
+        *X = cx - sy;
+        *Y = cy + sx;
+    }
+}
+
+/* src/rotations/rotations_default.c:31-36 (sph), :45-50 (tri), :59-64 (disk) */
+void oracle_kernel_hi2lo(const oracle_plan * P, int m1, int m2, double * A, int S) {
+    int n = P->n;
+    const double * s = P->s, * c = P->c;
+    if (P->kind == ORACLE_SPH) {
+        for (int j = m2 - 2; j >= m1; j -= 2)
+            for (int k = n - 3 - j; k >= 0; k--)
+                givens(s[tri_idx(n, k, j)], c[tri_idx(n, k, j)], A + k * S, A + (k + 2) * S);
+    } else if (P->kind == ORACLE_TRI) {
+        for (int j = m2 - 1; j >= m1; j--)
+            for (int k = n - 2 - j; k >= 0; k--)
+                givens(s[tri_idx(n, k, j)], c[tri_idx(n, k, j)], A + k * S, A + (k + 1) * S);
+    } else {
+        for (int j = m2 - 2; j >= m1; j -= 2)
+            for (int k = n - 2 - (j + 1) / 2; k >= 0; k--)
+                givens(s[disk_idx(n, k, j)], c[disk_idx(n, k, j)], A + k * S, A + (k + 1) * S);
+    }
+}
+
+/* src/rotations/rotations_default.c:38-43 (sph), :52-57 (tri), :66-71 (disk) */
+void oracle_kernel_lo2hi(const oracle_plan * P, int m1, int m2, double * A, int S) {
+    int n = P->n;
+    const double * s = P->s, * c = P->c;
+    if (P->kind == ORACLE_SPH) {
+        for (int j = m1; j < m2; j += 2)
+            for (int k = 0; k <= n - 3 - j; k++)
+                givens_t(s[tri_idx(n, k, j)], c[tri_idx(n, k, j)], A + k * S, A + (k + 2) * S);
+    } else if (P->kind == ORACLE_TRI) {
+        for (int j = m1; j < m2; j++)
+            for (int k = 0; k <= n - 2 - j; k++)
+                givens_t(s[tri_idx(n, k, j)], c[tri_idx(n, k, j)], A + k * S, A + (k + 1) * S);
+    } else {
+        for (int j = m1; j < m2; j += 2)
+            for (int k = 0; k <= n - 2 - (j + 1) / 2; k++)
+                givens_t(s[disk_idx(n, k, j)], c[disk_idx(n, k, j)], A + k * S, A + (k + 1) * S);
+    }
+}
+
+/* Execute loops over orders: src/drivers.c:94-110 (sph), :314-326 (tri), :414-430 (disk).
+ * Column pair (2m-1, 2m) carries order m for sph and disk; column m carries order m for tri. */
+static void execute_rot(const oracle_plan * P, double * A, int M, int hi2lo) {
+    int N = P->n;
+    if (P->kind == ORACLE_TRI) {
+        #pragma omp parallel for schedule(dynamic, 1)
+        for (int m = 1; m < M; m++) {
+            if (hi2lo) oracle_kernel_hi2lo(P, 0, m, A + (size_t) N * m, 1);
+            else       oracle_kernel_lo2hi(P, 0, m, A + (size_t) N * m, 1);
+        }
+    } else {
+        #pragma omp parallel for schedule(dynamic, 1)
+        for (int m = 2; m <= M / 2; m++) {
+            for (int h = 0; h < 2; h++) {
+                double * col = A + (size_t) N * (2 * m - 1 + h);
+                if (hi2lo) oracle_kernel_hi2lo(P, m % 2, m, col, 1);
+                else       oracle_kernel_lo2hi(P, m % 2, m, col, 1);
+            }
+        }
+    }
+}
+
+void oracle_execute_hi2lo(const oracle_plan * P, double * A, int M) { execute_rot(P, A, M, 1); }
+void oracle_execute_lo2hi(const oracle_plan * P, double * A, int M) { execute_rot(P, A, M, 0); }
+
+/* ---------------------------------------------------------------------------
+ * Triangular multiplies (the reference calls cblas_dtrmm with ColMajor, Upper,
+ * NonUnit, alpha = 1; src/drivers.c:836-863, 924-956, 992-1019).
+ * ------------------------------------------------------------------------- */
+void oracle_trmm(char side, char trans, int n, const double * U, int nb, double * B, int ldb) {
+    #define Uij(i, j) U[(size_t) (i) + (size_t) (j) * n]
+    if (side == 'L') {
+        /* B is n x nb: column by column */
+        #pragma omp parallel
+        {
+            double * t = malloc(sizeof(double) * n);
+            #pragma omp for schedule(static)
+            for (int col = 0; col < nb; col++) {
+                double * b = B + (size_t) col * ldb;
+                for (int i = 0; i < n; i++) {
+                    double acc = 0.0;
+                    if (trans == 'N') for (int k = i; k < n; k++) acc += Uij(i, k) * b[k];
+                    else              for (int k = 0; k <= i; k++) acc += Uij(k, i) * b[k];
+                    t[i] = acc;
+                }
+                memcpy(b, t, sizeof(double) * n);
+            }
+            free(t);
+        }
+    } else {
+        /* B is nb x n: row by row, B <- B op(U) */
+        #pragma omp parallel
+        {
+            double * t = malloc(sizeof(double) * n);
+            #pragma omp for schedule(static)
+            for (int row = 0; row < nb; row++) {
+                for (int j = 0; j < n; j++) {
+                    double acc = 0.0;
+                    if (trans == 'N') for (int k = 0; k <= j; k++) acc += B[row + (size_t) k * ldb] * Uij(k, j);
+                    else              for (int k = j; k < n; k++) acc += B[row + (size_t) k * ldb] * Uij(j, k);
+                    t[j] = acc;
+                }
+                for (int j = 0; j < n; j++) B[row + (size_t) j * ldb] = t[j];
+            }
+            free(t);
+        }
+    }
+    #undef Uij
+}
+
+/* ---------------------------------------------------------------------------
+ * Connection matrices in long double, rounded to double.
+ * The triangular-banded generalised eigenvector method of the reference:
+ * src/banded_source.c:779-800 (eigenvectors), :2024-2170 (diagonals),
+ * :2316-2456 (A and B operators), :1774-1903 (Jacobi operators),
+ * :288-343 (banded products and sums); planners in src/transforms.c:50-180.
+ * A banded matrix here stores entry (i, j) for -l <= j - i <= u.
+ * ------------------------------------------------------------------------- */
+
+typedef long double ld;
+#define LD_EPS 0x1p-64L   /* src/ftinternal.h:83 (M_EPSl) */
+
+typedef struct { int n, l, u; ld * d; } bnd;
+
+static bnd bnd_new(int n, int l, int u) {
+    bnd A = { n, l, u, calloc((size_t) n * (l + u + 1), sizeof(ld)) };
+    return A;
+}
+static inline ld bget(const bnd * A, int i, int j) {
+    if (0 <= i && 0 <= j && -A->l <= j - i && j - i <= A->u && i < A->n && j < A->n)
+        return A->d[(size_t) (A->u + i - j) + (size_t) j * (A->l + A->u + 1)];
+    return 0;
+}
+static inline void bset(bnd * A, ld v, int i, int j) {
+    if (0 <= i && 0 <= j && -A->l <= j - i && j - i <= A->u && i < A->n && j < A->n)
+        A->d[(size_t) (A->u + i - j) + (size_t) j * (A->l + A->u + 1)] = v;
+}
+
+/* C <- alpha*A*B + beta*C: src/banded_source.c:288-305 */
+static void bmm(ld alpha, const bnd * A, const bnd * B, ld beta, bnd * C) {
+    int n = A->n;
+    for (int j = 0; j < n; j++)
+        for (int i = MAX(0, j - C->u); i < MIN(n, j + C->l + 1); i++) {
+            ld ab = 0;
+            for (int k = MAX(MAX(0, i - A->l), j - B->u); k < MIN(MIN(n, i + A->u + 1), j + B->l + 1); k++)
+                ab += bget(A, i, k) * bget(B, k, j);
+            ld c = bget(C, i, j);
+            bset(C, alpha * ab + beta * c, i, j);
+        }
+}
+
+/* C <- alpha*A + beta*B: src/banded_source.c:333-343 */
+static void badd(ld alpha, const bnd * A, ld beta, const bnd * B, bnd * C) {
+    int n = C->n;
+    for (int j = 0; j < n; j++)
+        for (int i = MAX(0, j - C->u); i < MIN(n, j + C->l + 1); i++)
+            bset(C, alpha * bget(A, i, j) + beta * bget(B, i, j), i, j);
+}
+
+/* Generalised eigenvectors of upper-triangular banded (A, B), V pre-loaded with its diagonal:
+ * src/banded_source.c:779-800 */
+static void tb_eigenvectors(const bnd * A, const bnd * B, ld * V, int n) {
+    int b = MAX(A->u, B->u);
+    for (int j = 1; j < n; j++) {
+        ld lam = bget(A, j, j) / bget(B, j, j);
+        for (int i = j - 1; i >= 0; i--) {
+            ld t = 0, kt = 0;
+            for (int k = i + 1; k < MIN(i + b + 1, n); k++) {
+                t += (bget(A, i, k) - lam * bget(B, i, k)) * V[k + (size_t) j * n];
+                kt += (fabsl(bget(A, i, k)) + fabsl(lam * bget(B, i, k))) * fabsl(V[k + (size_t) j * n]);
+            }
+            ld d = lam * bget(B, i, i) - bget(A, i, i);
+            ld kd = fabsl(lam * bget(B, i, i)) + fabsl(bget(A, i, i));
+            if (fabsl(d) < 4 * kd * LD_EPS || fabsl(t) < 4 * kt * LD_EPS)
+                V[i + (size_t) j * n] = 0;
+            else
+                V[i + (size_t) j * n] = t / d;
+        }
+    }
+}
+
+static double * finish_plan(bnd * A, bnd * B, ld * Vl, int n) {
+    tb_eigenvectors(A, B, Vl, n);
+    double * V = malloc(sizeof(double) * (size_t) n * n);
+    for (size_t i = 0; i < (size_t) n * n; i++) V[i] = (double) Vl[i];
+    free(A->d); free(B->d); free(Vl);
+    return V;
+}
+
+#define ONE ((ld) 1)
+#define TWO ((ld) 2)
+
+/* src/banded_source.c:2316-2338 and :2024-2061; planner src/transforms.c:50-63 */
+double * oracle_plan_legendre_to_chebyshev(int normleg, int normcheb, int n) {
+    bnd A = bnd_new(n, 0, 2), B = bnd_new(n, 0, 2);
+    if (n > 1) bset(&A, 2, 1, 1);
+    for (int i = 2; i < n; i++) {
+        bset(&A, -i * (i - ONE), i - 2, i);
+        bset(&A, i * (i + ONE), i, i);
+    }
+    if (n > 0) bset(&B, normcheb ? sqrtl(2) : 2, 0, 0);
+    if (n > 1) bset(&B, 1, 1, 1);
+    for (int i = 2; i < n; i++) {
+        bset(&B, -1, i - 2, i);
+        bset(&B, 1, i, i);
+    }
+    ld * D = calloc((size_t) n * n, sizeof(ld));
+    int inc = n + 1;
+    if (normleg) {
+        if (normcheb) {
+            if (n > 0) D[0] = sqrtl(0.5) * tgammal(0.5);
+            if (n > 1) D[inc] = sqrtl(1.5) * D[0];
+            for (int i = 2; i < n; i++) D[i * inc] = sqrtl((2 * i + 1) * (2 * i - ONE)) * D[(i - 1) * inc] / (2 * i);
+        } else {
+            if (n > 0) D[0] = sqrtl(0.5);
+            if (n > 1) D[inc] = sqrtl(1.5);
+            for (int i = 2; i < n; i++) D[i * inc] = sqrtl((2 * i + 1) * (2 * i - ONE)) * D[(i - 1) * inc] / (2 * i);
+        }
+    } else {
+        if (normcheb) {
+            if (n > 0) D[0] = tgammal(0.5);
+            if (n > 1) D[inc] = D[0] / sqrtl(2);
+            for (int i = 2; i < n; i++) D[i * inc] = (2 * i - 1) * D[(i - 1) * inc] / (2 * i);
+        } else {
+            if (n > 0) D[0] = 1;
+            if (n > 1) D[inc] = 1;
+            for (int i = 2; i < n; i++) D[i * inc] = (2 * i - 1) * D[(i - 1) * inc] / (2 * i);
+        }
+    }
+    return finish_plan(&A, &B, D, n);
+}
+
+/* src/banded_source.c:2340-2384 and :2063-2100; planner src/transforms.c:65-78 */
+double * oracle_plan_chebyshev_to_legendre(int normcheb, int normleg, int n) {
+    bnd A = bnd_new(n, 0, 2), B = bnd_new(n, 0, 2);
+    if (normleg) {
+        if (n > 1) bset(&A, sqrtl(TWO / 5), 1, 1);
+        for (int i = 2; i < n; i++) {
+            bset(&A, -(i + 1) * sqrtl(((i - ONE) * i) / ((2 * i - ONE) * (2 * i + 1))) * (i + 1), i - 2, i);
+            bset(&A, i * sqrtl(((i + ONE) * (i + 2)) / ((2 * i + ONE) * (2 * i + 3))) * i, i, i);
+        }
+        if (n > 0) bset(&B, sqrtl(TWO / 3), 0, 0);
+        if (n > 1) bset(&B, sqrtl(TWO / 5), 1, 1);
+        for (int i = 2; i < n; i++) {
+            bset(&B, -sqrtl(((i - ONE) * i) / ((2 * i - ONE) * (2 * i + 1))), i - 2, i);
+            bset(&B, sqrtl(((i + ONE) * (i + 2)) / ((2 * i + ONE) * (2 * i + 3))), i, i);
+        }
+    } else {
+        if (n > 1) bset(&A, ONE / 3, 1, 1);
+        for (int i = 2; i < n; i++) {
+            bset(&A, -(i + 1) / (2 * i + ONE) * (i + 1), i - 2, i);
+            bset(&A, i / (2 * i + ONE) * i, i, i);
+        }
+        if (n > 0) bset(&B, 1, 0, 0);
+        if (n > 1) bset(&B, ONE / 3, 1, 1);
+        for (int i = 2; i < n; i++) {
+            bset(&B, -1 / (2 * i + ONE), i - 2, i);
+            bset(&B, 1 / (2 * i + ONE), i, i);
+        }
+    }
+    ld * D = calloc((size_t) n * n, sizeof(ld));
+    int inc = n + 1;
+    if (normcheb) {
+        if (normleg) {
+            if (n > 0) D[0] = sqrtl(2) / tgammal(0.5);
+            if (n > 1) D[inc] = D[0] / sqrtl(1.5);
+            for (int i = 2; i < n; i++) D[i * inc] = (2 * i) / sqrtl((2 * i + 1) * (2 * i - ONE)) * D[(i - 1) * inc];
+        } else {
+            if (n > 0) D[0] = 1 / tgammal(0.5);
+            if (n > 1) D[inc] = sqrtl(2) * D[0];
+            for (int i = 2; i < n; i++) D[i * inc] = (2 * i) * D[(i - 1) * inc] / (2 * i - 1);
+        }
+    } else {
+        if (normleg) {
+            if (n > 0) D[0] = sqrtl(2);
+            if (n > 1) D[inc] = 1 / sqrtl(1.5);
+            for (int i = 2; i < n; i++) D[i * inc] = (2 * i) / sqrtl((2 * i + 1) * (2 * i - ONE)) * D[(i - 1) * inc];
+        } else {
+            if (n > 0) D[0] = 1;
+            if (n > 1) D[inc] = 1;
+            for (int i = 2; i < n; i++) D[i * inc] = (2 * i) * D[(i - 1) * inc] / (2 * i - 1);
+        }
+    }
+    return finish_plan(&A, &B, D, n);
+}
+
+/* src/banded_source.c:2386-2430 and :2102-2131; planner src/transforms.c:80-93 */
+double * oracle_plan_ultraspherical_to_ultraspherical(int norm1, int norm2, int n, double lambda_d, double mu_d) {
+    ld lambda = lambda_d, mu = mu_d;
+    bnd A = bnd_new(n, 0, 2), B = bnd_new(n, 0, 2);
+    if (norm2) {
+        if (n > 1) bset(&A, (1 + 2 * lambda) * copysignl(sqrtl((2 * mu + 1) / (2 * mu + 4)), mu), 1, 1);
+        for (int i = 2; i < n; i++) {
+            bset(&A, -(i + 2 * mu) * (i + 2 * (mu - lambda)) * copysignl(sqrtl((i * (i - ONE)) / (4 * (i + mu) * (i + mu - 1))), mu), i - 2, i);
+            bset(&A, i * (i + 2 * lambda) * copysignl(sqrtl(((i + 2 * mu) * (i + 2 * mu + 1)) / (4 * (i + mu) * (i + mu + 1))), mu), i, i);
+        }
+        if (n > 0) bset(&B, sqrtl((2 * mu + 1) / (2 * mu + 2)), 0, 0);
+        if (n > 1) bset(&B, copysignl(sqrtl((2 * mu + 1) / (2 * mu + 4)), mu), 1, 1);
+        for (int i = 2; i < n; i++) {
+            bset(&B, -copysignl(sqrtl((i * (i - ONE)) / (4 * (i + mu) * (i + mu - 1))), mu), i - 2, i);
+            bset(&B, copysignl(sqrtl(((i + 2 * mu) * (i + 2 * mu + 1)) / (4 * (i + mu) * (i + mu + 1))), mu), i, i);
+        }
+    } else {
+        if (n > 1) bset(&A, (1 + 2 * lambda) * mu / (1 + mu), 1, 1);
+        for (int i = 2; i < n; i++) {
+            bset(&A, -(i + 2 * mu) * (i + 2 * (mu - lambda)) * mu / (i + mu), i - 2, i);
+            bset(&A, i * (i + 2 * lambda) * mu / (i + mu), i, i);
+        }
+        if (n > 0) bset(&B, 1, 0, 0);
+        if (n > 1) bset(&B, mu / (1 + mu), 1, 1);
+        for (int i = 2; i < n; i++) {
+            bset(&B, -mu / (i + mu), i - 2, i);
+            bset(&B, mu / (i + mu), i, i);
+        }
+    }
+    ld * D = calloc((size_t) n * n, sizeof(ld));
+    int inc = n + 1;
+    if (norm1) {
+        if (norm2) {
+            if (n > 0) D[0] = sqrtl(tgammal(lambda + 1) / (tgammal(0.5) * tgammal(lambda + 0.5))) * sqrtl(tgammal(0.5) * tgammal(mu + 0.5) / tgammal(mu + 1));
+            for (int i = 1; i < n; i++)
+                D[i * inc] = sqrtl((i - 1 + mu) / i * (i - 1 + 2 * mu) / (i + mu)) * sqrtl(i / (i - 1 + lambda) * (i + lambda) / (i - 1 + 2 * lambda)) * (i - 1 + lambda) / (i - 1 + mu) * D[(i - 1) * inc];
+        } else {
+            if (n > 0) D[0] = sqrtl(tgammal(lambda + 1) / (tgammal(0.5) * tgammal(lambda + 0.5)));
+            for (int i = 1; i < n; i++)
+                D[i * inc] = sqrtl(i / (i - 1 + lambda) * (i + lambda) / (i - 1 + 2 * lambda)) * (i - 1 + lambda) / (i - 1 + mu) * D[(i - 1) * inc];
+        }
+    } else {
+        if (norm2) {
+            if (n > 0) D[0] = sqrtl(tgammal(0.5) * tgammal(mu + 0.5) / tgammal(mu + 1));
+            for (int i = 1; i < n; i++)
+                D[i * inc] = sqrtl((i - 1 + mu) / i * (i - 1 + 2 * mu) / (i + mu)) * (i - 1 + lambda) / (i - 1 + mu) * D[(i - 1) * inc];
+        } else {
+            if (n > 0) D[0] = 1;
+            for (int i = 1; i < n; i++) D[i * inc] = (i - 1 + lambda) / (i - 1 + mu) * D[(i - 1) * inc];
+        }
+    }
+    return finish_plan(&A, &B, D, n);
+}
+
+/* Jacobi operators (normalized forms used by the harmonic planners: norm = 1).
+ * derivative: src/banded_source.c:1774-1795 */
+static bnd jacobi_derivative(int norm, int n, int order, ld alpha, ld beta) {
+    bnd A = bnd_new(n, -order, order);
+    for (int j = order; j < n; j++) {
+        ld v = 1;
+        if (norm) {
+            for (int k = 0; k < order; k++) v *= (j - k) * (j + alpha + beta + k + 1);
+            v = sqrtl(v);
+        } else {
+            for (int k = 0; k < order; k++) v *= (j + alpha + beta + k + 1) / 2;
+        }
+        bset(&A, v, j - order, j);
+    }
+    return A;
+}
+
+/* multiplication by x: src/banded_source.c:1797-1841 (norm = 1 branch) */
+static bnd jacobi_multiplication(int n, ld alpha, ld beta) {
+    bnd A = bnd_new(n, 1, 1);
+    for (int j = 0; j < n; j++) {
+        ld v;
+        if (j == 1)
+            v = 2 * sqrtl(((alpha + 1) * (beta + 1)) / ((alpha + beta + 2) * (alpha + beta + 2) * (alpha + beta + 3)));
+        else
+            v = 2 * sqrtl((j * (j + alpha) * (j + beta) * (j + alpha + beta)) / ((2 * j + alpha + beta - 1) * (2 * j + alpha + beta) * (2 * j + alpha + beta) * (2 * j + alpha + beta + 1)));
+        bset(&A, v, j - 1, j);
+        if (j == 0) {
+            v = (beta - alpha) / (alpha + beta + 2);
+            bset(&A, v, 0, 0);
+            v = 2 * sqrtl(((alpha + 1) * (beta + 1)) / ((alpha + beta + 2) * (alpha + beta + 2) * (alpha + beta + 3)));
+            bset(&A, v, 1, 0);
+        } else {
+            v = ((beta - alpha) * (alpha + beta)) / ((2 * j + alpha + beta) * (2 * j + alpha + beta + 2));
+            bset(&A, v, j, j);
+            v = 2 * sqrtl(((j + 1) * (j + alpha + 1) * (j + beta + 1) * (j + alpha + beta + 1)) / ((2 * j + alpha + beta + 1) * (2 * j + alpha + beta + 2) * (2 * j + alpha + beta + 2) * (2 * j + alpha + beta + 3)));
+            bset(&A, v, j + 1, j);
+        }
+    }
+    return A;
+}
+
+/* raising: src/banded_source.c:1843-1873 (norm = 1 branch) */
+static bnd jacobi_raising(int n, ld alpha, ld beta) {
+    bnd A = bnd_new(n, 0, 2);
+    for (int j = 0; j < n; j++) {
+        ld v = -2 * sqrtl(((j - 1) * j * (j + alpha) * (j + beta)) / ((2 * j + alpha + beta - 1) * (2 * j + alpha + beta) * (2 * j + alpha + beta) * (2 * j + alpha + beta + 1)));
+        bset(&A, v, j - 2, j);
+        v = 2 * (alpha - beta) * sqrtl(j * (j + alpha + beta + 1)) / ((2 * j + alpha + beta) * (2 * j + alpha + beta + 2));
+        bset(&A, v, j - 1, j);
+        if (j == 0)
+            v = 2 * sqrtl(((alpha + 1) * (beta + 1)) / ((alpha + beta + 2) * (alpha + beta + 3)));
+        else
+            v = 2 * sqrtl(((j + alpha + 1) * (j + beta + 1) * (j + alpha + beta + 1) * (j + alpha + beta + 2)) / ((2 * j + alpha + beta + 1) * (2 * j + alpha + beta + 2) * (2 * j + alpha + beta + 2) * (2 * j + alpha + beta + 3)));
+        bset(&A, v, j, j);
+    }
+    return A;
+}
+
+/* lowering: src/banded_source.c:1875-1903 (norm = 1 branch) */
+static bnd jacobi_lowering(int n, ld alpha, ld beta) {
+    bnd A = bnd_new(n, 2, 0);
+    for (int j = 0; j < n; j++) {
+        ld v;
+        if (j == 0)
+            v = 2 * sqrtl(((alpha + 1) * (beta + 1)) / ((alpha + beta + 2) * (alpha + beta + 3)));
+        else
+            v = 2 * sqrtl(((j + alpha + 1) * (j + beta + 1) * (j + alpha + beta + 1) * (j + alpha + beta + 2)) / ((2 * j + alpha + beta + 1) * (2 * j + alpha + beta + 2) * (2 * j + alpha + beta + 2) * (2 * j + alpha + beta + 3)));
+        bset(&A, v, j, j);
+        v = 2 * (alpha - beta) * sqrtl((j + 1) * (j + alpha + beta + 2)) / ((2 * j + alpha + beta + 2) * (2 * j + alpha + beta + 4));
+        bset(&A, v, j + 1, j);
+        v = -2 * sqrtl(((j + 1) * (j + 2) * (j + alpha + 2) * (j + beta + 2)) / ((2 * j + alpha + beta + 3) * (2 * j + alpha + beta + 4) * (2 * j + alpha + beta + 4) * (2 * j + alpha + beta + 5)));
+        bset(&A, v, j + 2, j);
+    }
+    return A;
+}
+
+/* A = sigma D^2 + tau D for the Jacobi-Jacobi problem: src/banded_source.c:2432-2451;
+ * B = raising: :2453-2456; diagonal: :2133-2142 (norm1 = norm2 = 1);
+ * planner src/transforms.c:95-108.  Only the normalized-to-normalized form is
+ * used by the tri and disk planners (src/drivers.c:905-910, 963-968). */
+double * oracle_plan_jacobi_to_jacobi(int norm1, int norm2, int n, double alpha_d, double beta_d, double gamma_d, double delta_d) {
+    (void) norm1; (void) norm2;  /* harmonic planners pass norm1 = norm2 = 1 */
+    ld alpha = alpha_d, beta = beta_d, gamma = gamma_d, delta = delta_d;
+    bnd A = bnd_new(n, 0, 2);
+    bnd D1 = jacobi_derivative(1, n, 1, gamma, delta);
+    bnd D2 = jacobi_derivative(1, n, 2, gamma, delta);
+    bnd L1 = jacobi_lowering(n, gamma + 1, delta + 1);
+    bnd M1 = jacobi_multiplication(n, gamma + 1, delta + 1);
+    bmm(-1, &L1, &D2, 0, &A);
+    badd(1, &A, alpha - beta, &D1, &A);
+    bmm(alpha + beta + 2, &M1, &D1, 1, &A);
+    free(D1.d); free(D2.d); free(L1.d); free(M1.d);
+    bnd B = jacobi_raising(n, gamma, delta);
+    ld * D = calloc((size_t) n * n, sizeof(ld));
+    int inc = n + 1;
+    if (n > 0)
+        D[0] = sqrtl(tgammal(alpha + beta + 2) / (powl(2, alpha + beta + 1) * tgammal(alpha + 1) * tgammal(beta + 1)) * (powl(2, gamma + delta + 1) * tgammal(gamma + 1) * tgammal(delta + 1)) / tgammal(gamma + delta + 2));
+    if (n > 1)
+        D[inc] = (alpha + beta + 2) / (gamma + delta + 2) * sqrtl((alpha + beta + 3) / ((alpha + 1) * (beta + 1)) * ((gamma + 1) * (delta + 1)) / (gamma + delta + 3)) * D[0];
+    for (int i = 2; i < n; i++)
+        D[i * inc] = (2 * i + alpha + beta) / (2 * i + gamma + delta) * sqrtl(((2 * i + alpha + beta - 1) * (2 * i + alpha + beta + 1)) / ((i + alpha) * (i + beta) * (i + alpha + beta)) * ((i + gamma) * (i + delta) * (i + gamma + delta)) / ((2 * i + gamma + delta - 1) * (2 * i + gamma + delta + 1))) * D[(i - 1) * inc];
+    return finish_plan(&A, &B, D, n);
+}
+
+/* ---------------------------------------------------------------------------
+ * Plans and full transforms.
+ * ------------------------------------------------------------------------- */
+
+oracle_plan * oracle_plan_rotations(int kind, int n, double alpha, double beta, double gamma) {
+    oracle_plan * P = calloc(1, sizeof(oracle_plan));
+    P->kind = kind; P->n = n;
+    P->alpha = alpha; P->beta = beta; P->gamma = gamma;
+    size_t len = kind == ORACLE_DISK ? (size_t) n * n : (size_t) n * (n + 1) / 2;
+    P->s = calloc(len ? len : 1, sizeof(double));
+    P->c = calloc(len ? len : 1, sizeof(double));
+    if (kind == ORACLE_SPH) plan_rotsphere(n, P->s, P->c);
+    else if (kind == ORACLE_TRI) plan_rottriangle(n, alpha, beta, gamma, P->s, P->c);
+    else plan_rotdisk(n, alpha, beta, P->s, P->c);
+    return P;
+}
+
+/* src/drivers.c:816-831 */
+oracle_plan * oracle_plan_sph2fourier(int n) {
+    oracle_plan * P = oracle_plan_rotations(ORACLE_SPH, n, 0, 0, 0);
+    P->P[0] = oracle_plan_legendre_to_chebyshev(1, 0, n);
+    P->P[1] = oracle_plan_ultraspherical_to_ultraspherical(1, 0, n, 1.5, 1.0);
+    P->Pinv[0] = oracle_plan_chebyshev_to_legendre(0, 1, n);
+    P->Pinv[1] = oracle_plan_ultraspherical_to_ultraspherical(0, 1, n, 1.0, 1.5);
+    return P;
+}
+
+/* src/drivers.c:901-919 */
+oracle_plan * oracle_plan_tri2cheb(int n, double alpha, double beta, double gamma) {
+    oracle_plan * P = oracle_plan_rotations(ORACLE_TRI, n, alpha, beta, gamma);
+    P->P[0] = oracle_plan_jacobi_to_jacobi(1, 1, n, beta + gamma + 1.0, alpha, -0.5, -0.5);
+    P->P[1] = oracle_plan_jacobi_to_jacobi(1, 1, n, gamma, beta, -0.5, -0.5);
+    P->Pinv[0] = oracle_plan_jacobi_to_jacobi(1, 1, n, -0.5, -0.5, beta + gamma + 1.0, alpha);
+    P->Pinv[1] = oracle_plan_jacobi_to_jacobi(1, 1, n, -0.5, -0.5, gamma, beta);
+    return P;
+}
+
+/* src/drivers.c:959-987, with plan_jacobi_to_chebyshev / plan_chebyshev_to_jacobi
+ * (src/transforms.c:157-180) inlined: row / column scalings by sqrt(2/pi), sqrt(1/pi) etc. */
+oracle_plan * oracle_plan_disk2cxf(int n, double alpha, double beta) {
+    oracle_plan * P = oracle_plan_rotations(ORACLE_DISK, n, alpha, beta, 0);
+    P->P[0] = oracle_plan_jacobi_to_jacobi(1, 1, n, beta, alpha, -0.5, -0.5);
+    P->P[1] = oracle_plan_jacobi_to_jacobi(1, 1, n, beta, alpha + 1.0, -0.5, 0.5);
+    P->Pinv[0] = oracle_plan_jacobi_to_jacobi(1, 1, n, -0.5, -0.5, beta, alpha);
+    P->Pinv[1] = oracle_plan_jacobi_to_jacobi(1, 1, n, -0.5, 0.5, beta, alpha + 1.0);
+    double * sclrow = malloc(sizeof(double) * (n ? n : 1));
+    double * sclcol = malloc(sizeof(double) * (n ? n : 1));
+    for (int i = 0; i < n; i++) {
+        sclrow[i] = i ? sqrtl(M_2_PIl) : sqrtl(M_1_PIl);
+        sclcol[i] = i ? sqrtl(M_PI_2l) : sqrtl(M_PIl);
+    }
+    for (int j = 0; j < n; j++)
+        for (int i = 0; i <= j; i++) {
+            P->P[0][i + (size_t) j * n] *= sclrow[i];
+            P->Pinv[0][i + (size_t) j * n] *= sclcol[j];
+        }
+    free(sclrow); free(sclcol);
+    double cst0 = pow(2.0, 0.5 * (alpha + beta + 2.0));
+    double cst1 = cst0 * 0.797884560802865355;      /* sqrt(2/pi), src/ftinternal.h:66 */
+    double cst0inv = pow(2.0, -0.5 * (alpha + beta + 2.0));
+    double cst1inv = cst0inv * 1.253314137315500251; /* sqrt(pi/2), src/ftinternal.h:65 */
+    for (int j = 0; j < n; j++)
+        for (int i = 0; i <= j; i++) {
+            P->P[0][i + (size_t) j * n] *= cst0;
+            P->P[1][i + (size_t) j * n] *= cst1;
+            P->Pinv[0][i + (size_t) j * n] *= cst0inv;
+            P->Pinv[1][i + (size_t) j * n] *= cst1inv;
+        }
+    return P;
+}
+
+void oracle_destroy_plan(oracle_plan * P) {
+    if (!P) return;
+    free(P->s); free(P->c);
+    for (int i = 0; i < 2; i++) { free(P->P[i]); free(P->Pinv[i]); }
+    free(P);
+}
+
+/* src/drivers.c:6-24 */
+static void cheb_normalize(double * A, int N, int M, int transposed) {
+    double r = transposed ? M_SQRT2 : M_SQRT1_2;
+    double g = transposed ? M_PI_2 : M_2_PI;
+    for (int i = 0; i < N; i++) A[i] *= r;
+    for (int j = 0; j < M; j++) {
+        A[(size_t) j * N] *= r;
+        for (int i = 0; i < N; i++) A[i + (size_t) j * N] *= g;
+    }
+}
+
+/* Four stride-4N column classes: j = 0,3 (mod 4) use U0; j = 1,2 (mod 4) use U1.
+ * src/drivers.c:836-839 */
+static void trmm4(char trans, int N, int M, const double * U0, const double * U1, double * A) {
+    oracle_trmm('L', trans, N, U0, (M + 3) / 4, A, 4 * N);
+    oracle_trmm('L', trans, N, U1, (M + 2) / 4, A + N, 4 * N);
+    oracle_trmm('L', trans, N, U1, (M + 1) / 4, A + 2 * N, 4 * N);
+    oracle_trmm('L', trans, N, U0, M / 4, A + 3 * N, 4 * N);
+}
+
+/* src/drivers.c:833-865 (sph), :921-957 (tri), :989-1021 (disk) */
+void oracle_execute(const oracle_plan * P, int forward, char TRANS, double * A, int N, int M) {
+    if (TRANS != 'N' && TRANS != 'T') return;
+    int tN = TRANS == 'N';
+    if (P->kind == ORACLE_TRI) {
+        double a = P->alpha, b = P->beta, g = P->gamma;
+        int left = (b + g != -1.5) || (a != -0.5);
+        int right = (g != -0.5) || (b != -0.5);
+        if (forward && tN) {
+            oracle_execute_hi2lo(P, A, M);
+            if (left) oracle_trmm('L', 'N', N, P->P[0], M, A, N);
+            if (right) oracle_trmm('R', 'T', N, P->P[1], N, A, N);
+            cheb_normalize(A, N, M, 0);
+        } else if (forward) {
+            cheb_normalize(A, N, M, 0);
+            if (right) oracle_trmm('R', 'N', N, P->P[1], N, A, N);
+            if (left) oracle_trmm('L', 'T', N, P->P[0], M, A, N);
+            oracle_execute_lo2hi(P, A, M);
+        } else if (tN) {
+            cheb_normalize(A, N, M, 1);
+            if (right) oracle_trmm('R', 'T', N, P->Pinv[1], N, A, N);
+            if (left) oracle_trmm('L', 'N', N, P->Pinv[0], M, A, N);
+            oracle_execute_lo2hi(P, A, M);
+        } else {
+            oracle_execute_hi2lo(P, A, M);
+            if (left) oracle_trmm('L', 'T', N, P->Pinv[0], M, A, N);
+            if (right) oracle_trmm('R', 'N', N, P->Pinv[1], N, A, N);
+            cheb_normalize(A, N, M, 1);
+        }
+        return;
+    }
+    /* sph and disk share the execute structure */
+    if (forward && tN) {
+        oracle_execute_hi2lo(P, A, M);
+        trmm4('N', N, M, P->P[0], P->P[1], A);
+    } else if (forward) {
+        trmm4('T', N, M, P->P[0], P->P[1], A);
+        oracle_execute_lo2hi(P, A, M);
+    } else if (tN) {
+        trmm4('N', N, M, P->Pinv[0], P->Pinv[1], A);
+        oracle_execute_lo2hi(P, A, M);
+    } else {
+        oracle_execute_hi2lo(P, A, M);
+        trmm4('T', N, M, P->Pinv[0], P->Pinv[1], A);
+    }
+}
+
+/* ---------------------------------------------------------------------------
+ * Seeded fills.  Counter-based splitmix64: value(idx) for the entry at linear
+ * column-major index idx = i + j*N is 2*u - 1 with u the top 53 bits of
+ * mix(seed + (idx + 1) * 0x9E3779B97F4A7C15) / 2^53.  Entries outside the
+ * layout's triangle are zero (src/ftutilities.c:75-113).
+ * ------------------------------------------------------------------------- */
+static inline double u_pm1(unsigned long long seed, unsigned long long idx) {
+    unsigned long long z = seed + (idx + 1ULL) * 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    z = z ^ (z >> 31);
+    return 2.0 * ((double) (z >> 11) * 0x1p-53) - 1.0;
+}
+
+void oracle_fill(int kind, int N, int M, unsigned long long seed, double * A) {
+    for (int j = 0; j < M; j++)
+        for (int i = 0; i < N; i++) {
+            int on = kind == ORACLE_SPH ? (j < M - 2 * i) : kind == ORACLE_TRI ? (j < M - i) : (j < M - 4 * i);
+            size_t idx = (size_t) i + (size_t) j * N;
+            A[idx] = on ? u_pm1(seed, idx) : 0.0;
+        }
+}

@@ -1,0 +1,76 @@
+/*
+ * ft_oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * A plain-C, single-source restatement of FastTransforms' harmonic-conversion
+ * path (sph2fourier / fourier2sph, tri2cheb / cheb2tri, disk2cxf / cxf2disk):
+ * rotation tables, scalar Givens sweeps, the execute loops over orders, the
+ * dense connection matrices and the triangular multiplies.  It is the checker
+ * for the CUDA library: only tests, the smoke check and bench.py's CPU
+ * baseline may load it.  The product never calls into it.
+ *
+ * Pinned against the reference library compiled from its own sources
+ * (oracle/_ref, built by oracle/ref_build/Makefile): see tests/test_oracle_pin.py.
+ */
+#ifndef FT_ORACLE_H
+#define FT_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ORACLE_SPH = 0, ORACLE_TRI = 1, ORACLE_DISK = 2 };
+
+typedef struct {
+    int kind;          /* ORACLE_SPH / ORACLE_TRI / ORACLE_DISK */
+    int n;             /* degree + 1 (rows of the coefficient matrix) */
+    double * s;        /* rotation sines, packed triangle (sph, tri) or disk packing */
+    double * c;        /* rotation cosines, same packing */
+    double * P[2];     /* dense n x n upper-triangular connection matrices, column-major */
+    double * Pinv[2];  /* their inverses */
+    double alpha, beta, gamma;
+} oracle_plan;
+
+/* Rotation arithmetic.  fused = 1: x' = fma(c, x, s*y), y' = fma(c, y, -(s*x)), the form of
+ * the reference's FMA SIMD kernels (src/rotations/rotations_AVX512F.c:4-15).  fused = 0:
+ * x' = c*x + s*y with every product rounded, the form of the scalar kernels
+ * (src/rotations/rotations_default.c:3-15) when compiled without FMA contraction. */
+void oracle_set_fused(int fused);
+
+oracle_plan * oracle_plan_sph2fourier(int n);
+oracle_plan * oracle_plan_tri2cheb(int n, double alpha, double beta, double gamma);
+oracle_plan * oracle_plan_disk2cxf(int n, double alpha, double beta);
+/* Rotation tables only (no connection matrices): cheap, for rotation-stage checks. */
+oracle_plan * oracle_plan_rotations(int kind, int n, double alpha, double beta, double gamma);
+void oracle_destroy_plan(oracle_plan * P);
+
+/* Rotation stage over all orders of an N x M matrix (in place). */
+void oracle_execute_hi2lo(const oracle_plan * P, double * A, int M);
+void oracle_execute_lo2hi(const oracle_plan * P, double * A, int M);
+
+/* Single-column kernels (reference ft_kernel_*_{hi2lo,lo2hi}): orders m1 <- m2 on column A with stride S. */
+void oracle_kernel_hi2lo(const oracle_plan * P, int m1, int m2, double * A, int S);
+void oracle_kernel_lo2hi(const oracle_plan * P, int m1, int m2, double * A, int S);
+
+/* B <- op(U) B (side 'L') or B <- B op(U) (side 'R'); U upper triangular n x n (ld n);
+ * B has n rows (side 'L') or n columns (side 'R'), leading dimension ldb. */
+void oracle_trmm(char side, char trans, int n, const double * U, int nb, double * B, int ldb);
+
+/* Full transforms, in place on the N x M column-major matrix A.
+ * forward = 1: sph2fourier / tri2cheb / disk2cxf; forward = 0: fourier2sph / cheb2tri / cxf2disk.
+ * TRANS 'N' or 'T'; any other character leaves A untouched (as the reference does). */
+void oracle_execute(const oracle_plan * P, int forward, char TRANS, double * A, int N, int M);
+
+/* Connection-matrix planners (n x n, column-major, caller frees with free()). */
+double * oracle_plan_legendre_to_chebyshev(int normleg, int normcheb, int n);
+double * oracle_plan_chebyshev_to_legendre(int normcheb, int normleg, int n);
+double * oracle_plan_ultraspherical_to_ultraspherical(int norm1, int norm2, int n, double lambda, double mu);
+double * oracle_plan_jacobi_to_jacobi(int norm1, int norm2, int n, double alpha, double beta, double gamma, double delta);
+
+/* Seeded fills in the reference layouts (src/ftutilities.c:75-113), U(-1,1) from splitmix64. */
+void oracle_fill(int kind, int N, int M, unsigned long long seed, double * A);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,79 @@
+"""Generate the golden fixtures in this directory from the reference library.
+
+The reference FastTransforms library is compiled from its own sources by
+oracle/ref_build/Makefile into oracle/_ref/libft_ref.so; this script runs it on
+seeded inputs and stores inputs and outputs as compressed .npz files:
+
+  * full transforms: forward and backward, TRANS 'N' and 'T', each applied to
+    the same seeded input (sph, tri and disk families, small degrees, even and
+    odd n, several Jacobi parameters);
+  * rotation stages alone (ft_execute_*_hi2lo / _lo2hi);
+  * the four dense connection matrices of each plan.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+from oracle.bind import Reference, _ptr, fill  # noqa: E402
+
+CASES = [
+    ("sph", 8, ()), ("sph", 17, ()), ("sph", 33, ()),
+    ("tri", 16, (0.0, 0.0, 0.0)), ("tri", 17, (-0.5, -0.5, -0.5)), ("tri", 16, (0.5, 1.0, -0.25)),
+    ("disk", 9, (0.0, 0.0)), ("disk", 16, (0.0, 0.0)), ("disk", 12, (0.5, -0.25)),
+]
+SEED = 20261203
+
+
+def case_name(kind, n, params):
+    tag = "_".join(f"{p:+.2f}".replace(".", "p").replace("+", "p").replace("-", "m") for p in params)
+    return f"{kind}_n{n}" + (f"_{tag}" if tag else "")
+
+
+def main():
+    R = Reference()
+    R.set_num_threads(1)
+    L = R.lib
+    planner = {"sph": ("ft_plan_rotsphere", [C.c_int]), "tri": ("ft_plan_rottriangle", [C.c_int] + [C.c_double] * 3),
+               "disk": ("ft_plan_rotdisk", [C.c_int] + [C.c_double] * 2)}
+    for name, args in planner.values():
+        getattr(L, name).restype = C.c_void_p
+        getattr(L, name).argtypes = args
+    for fam in ("sph", "tri", "disk"):
+        for d in ("hi2lo", "lo2hi"):
+            getattr(L, f"ft_execute_{fam}_{d}").argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int]
+    L.ft_destroy_rotation_plan.argtypes = [C.c_void_p]
+    for kind, n, params in CASES:
+        A = fill(kind, n, SEED)
+        P = R.plan(kind, n, *params)
+        out = {"A": A, "params": np.array(params, dtype=np.float64)}
+        for fwd in (True, False):
+            for tr in "NT":
+                B = A.copy(order="F")
+                R.execute(kind, P, fwd, tr, B)
+                out[("fwd" if fwd else "bwd") + "_" + tr] = B
+        Ps, Pinvs = R.connection(P, n)
+        out["P0"], out["P1"], out["Pinv0"], out["Pinv1"] = Ps[0], Ps[1], Pinvs[0], Pinvs[1]
+        R.destroy(P)
+        pname, _ = planner[kind]
+        RP = getattr(L, pname)(n, *params[: 3 if kind == "tri" else 2]) if params else getattr(L, pname)(n)
+        for d in ("hi2lo", "lo2hi"):
+            B = A.copy(order="F")
+            scratch = np.zeros_like(B, order="F")
+            getattr(L, f"ft_execute_{kind}_{d}")(RP, _ptr(B), _ptr(scratch), A.shape[1])
+            out["rot_" + d] = B
+        L.ft_destroy_rotation_plan(RP)
+        path = os.path.join(HERE, case_name(kind, n, params) + ".npz")
+        np.savez_compressed(path, **out)
+        print("wrote", os.path.relpath(path), A.shape)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,52 @@
+"""The C-ABI library loads, exports every declared entry point, and fails
+cleanly (no crash, an error status) when there is no sm_100 device.  CPU only:
+no compute call is made here."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from conftest import ROOT, has_gpu
+
+HEADER = os.path.join(ROOT, "include", "ft_b200.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = re.findall(r"^[A-Za-z_][\w \*]*?\b(ft_\w+)\s*\(", text, flags=re.M)
+    return sorted(set(names))
+
+
+def test_header_declares_the_reference_api():
+    names = set(declared_functions())
+    for f in ("ft_plan_sph2fourier", "ft_execute_sph2fourier", "ft_execute_fourier2sph", "ft_destroy_harmonic_plan",
+              "ft_plan_tri2cheb", "ft_execute_tri2cheb", "ft_execute_cheb2tri", "ft_plan_disk2cxf",
+              "ft_execute_disk2cxf", "ft_execute_cxf2disk", "ft_plan_rotsphere", "ft_execute_sph_hi2lo",
+              "ft_execute_sph_lo2hi", "ft_destroy_rotation_plan"):
+        assert f in names
+
+
+def test_library_exports_every_declared_symbol():
+    import fasttransforms_b200 as ft
+    lib = C.CDLL(ft.library_path)
+    missing = [f for f in declared_functions() if not hasattr(lib, f)]
+    assert not missing, missing
+
+
+def test_plan_struct_prefix_matches_reference():
+    # src/fasttransforms.h:370-385: 5 pointers, 5 doubles, 3 ints
+    from oracle.bind import _RefHarmonicPlan
+    assert _RefHarmonicPlan.NRP.offset == 5 * 8 + 5 * 8
+    assert C.sizeof(_RefHarmonicPlan) == 5 * 8 + 5 * 8 + 3 * 4 + 4
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-device path")
+def test_no_device_fails_cleanly():
+    import fasttransforms_b200 as ft
+    p = ft.lib.ft_plan_sph2fourier(16)
+    assert not p
+    assert ft.lib.ft_b200_last_status() in (2, 4)
+    with pytest.raises(ft.FTB200Error):
+        ft.plan_sph2fourier(16)
