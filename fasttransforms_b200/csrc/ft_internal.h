@@ -60,12 +60,15 @@ struct Geo {
     // number of order columns the rotation stage visits for an N x M matrix
     // sph / disk: pairs (2m-1, 2m), m = 2 .. M/2; tri: column m, m = 1 .. M-1
     __host__ __device__ static inline int first_order(int kind) { return kind == TRI ? 1 : 2; }
+    // orders per rotation task: one lane per (order, chain) of a 32-lane warp
+    __host__ __device__ static inline int task_orders(int kind) { return kind == SPH ? 16 : 32; }
     __host__ __device__ static inline int last_order(int kind, int M) { return kind == TRI ? M - 1 : M / 2; }
 };
 
-// A unit of work of the rotation kernel: up to 32 columns that share their
-// sweeps.  sph / disk: 16 orders of one parity, m = mbase + 2*o (o < 16), two
-// columns each; tri: 32 consecutive orders m = mbase + o.
+// A unit of work of the rotation kernel: the columns of task_orders(kind)
+// orders that share their sweeps.  sph: 16 orders of one parity, m = mbase + 2*o,
+// two columns each; disk: 32 orders of one parity, two columns each; tri: 32
+// consecutive orders m = mbase + o.
 struct RotTask {
     int field;   // index into the field table of the launch
     int mbase;   // lowest order of the group
@@ -81,8 +84,8 @@ struct RotField {
 };
 
 // Kernel launchers (rotations.cu).  The field table travels by value in the
-// kernel parameters (CUDA 12 allows up to 32 KB of parameters).
-constexpr int kMaxFields = 128;
+// kernel parameters (kept under the classic 4 KB parameter limit).
+constexpr int kMaxFields = 64;
 struct RotLaunch {
     RotField fields[kMaxFields];
     int nfields;

@@ -402,7 +402,7 @@ double * connection_jacobi(int n, double alpha_d, double beta_d, double gamma_d,
 // ---------------------------------------------------------------------------
 double task_cost(int kind, int N, int M, int mbase) {
     const int step = Geo::step(kind);
-    const int ord = kind == TRI ? 32 : 16;
+    const int ord = Geo::task_orders(kind);
     const int mlast = Geo::last_order(kind, M);
     int omax = mbase + step * (ord - 1);
     if (omax > mlast) omax = mbase + step * ((mlast - mbase) / step);
@@ -415,12 +415,13 @@ double task_cost(int kind, int N, int M, int mbase) {
 std::vector<RotTask> build_tasks(int kind, int N, int M, int field) {
     std::vector<RotTask> t;
     const int mfirst = Geo::first_order(kind), mlast = Geo::last_order(kind, M);
+    const int span = Geo::step(kind) * Geo::task_orders(kind);
     if (kind == TRI) {
-        for (int m = mfirst; m <= mlast; m += 32) t.push_back({field, m});
+        for (int m = mfirst; m <= mlast; m += span) t.push_back({field, m});
     } else {
         for (int p = 0; p < 2; p++) {
             const int m0 = p == 0 ? 2 : 3;
-            for (int m = m0; m <= mlast; m += 32) t.push_back({field, m});
+            for (int m = m0; m <= mlast; m += span) t.push_back({field, m});
         }
     }
     return t;

@@ -6,27 +6,34 @@
 //
 // Work decomposition
 // ------------------
-// A task is a group of 32 columns that receive the same sweeps (sph / disk:
-// 16 orders of one parity, cos and sin column each; tri: 32 consecutive
-// orders).  Orders in a group differ, so a sweep j is applied to the columns
+// A task is a group of columns that receive the same sweeps (sph: 16 orders
+// of one parity, cos and sin column each; disk: 32 orders of one parity, cos
+// and sin each; tri: 32 consecutive orders).  Orders in a group differ, so a sweep j is applied to the columns
 // whose order m satisfies j <= m - STEP and is an exact no-op (sin 0, cos 1)
 // for the others.  Tasks are pulled from a longest-first queue by persistent
 // CTAs (one per SM), which balances the triangular cost over orders.
 //
 // Inside a CTA the sweeps of a task run as a wavefront.  Warp q (a "stage")
-// owns B consecutive sweeps.  Each lane owns one column; per chain it keeps a
-// window of 2B consecutive chain positions in registers.  At every step the
+// owns B consecutive sweeps.  Each lane owns one chain of the columns of one
+// order and keeps, per column, a window of 2B consecutive chain positions in
+// registers.  At every step the
 // window slides by one position: one element enters, B independent rotations
 // are applied (sweep b at window slots 2b, 2b+1), one element leaves.  The
 // element leaving stage q is the element entering stage q+1 at the same step,
-// passed through a shared-memory ring buffer.  A loader warp streams the
-// column segments of the next chunk from global memory into the first buffer
-// and a storer warp writes the last buffer back, so one pass of W*B sweeps
-// reads and writes each column once.  All lanes of a warp use the same
-// (sin, cos) pair at each rotation, read as a warp-broadcast 16-byte load.
+// passed through a shared-memory ring buffer.  All W warps share the global
+// traffic: during each iteration every warp loads its share of the next
+// chunk's column segments into registers (latency hidden behind the sweeps)
+// and writes its share of the last stage's finished chunk back, so one pass of
+// W*B sweeps reads and writes each column once.  All lanes of a warp use the
+// same (sin, cos) pair at each rotation, read as a warp-broadcast 16-byte load.
+// With W = 8 warps every SM sub-partition holds two warps and the register
+// budget per thread is the full 255.
 //
 // No thread waits on another except through __syncthreads; there are no spin
 // loops.  Every global access is bounds-checked against the field's N, M.
+
+#include <cstdio>
+#include <type_traits>
 
 #include "ft_internal.h"
 
@@ -37,47 +44,64 @@ template <int KIND>
 struct KT {
     static constexpr int CH = KIND == SPH ? 2 : 1;        // chains per column
     static constexpr int STEP = KIND == TRI ? 1 : 2;      // order step between sweeps
-    static constexpr int ORDERS = KIND == TRI ? 32 : 16;  // orders per task
+    static constexpr int NCOL = KIND == TRI ? 1 : 2;      // columns per order (cos, sin)
+    static constexpr int ORD = 32 / CH;                   // orders per task (one lane per order and chain)
+    static constexpr int COLS = ORD * NCOL;               // columns per task
+    static constexpr int CPAD = COLS + 1;                 // padded column dimension of the stage buffers
 };
 
-constexpr int PAD = 33;   // padded lane dimension of the stage buffers (bank spread)
-
 struct SweepInfo {
-    long long tbase;   // packed-table offset of the sweep's column
-    int j;             // order of the sweep
+    long long tbase;      // packed-table offset of the sweep's column
+    int j;                // order of the sweep
     int tlo[2], thi[2];   // steps at which the sweep has a valid position, per chain
 };
 
+__device__ __forceinline__ void cp_async16(void * smem, const void * gmem) {
+    const unsigned sa = (unsigned) __cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" :: "r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 __device__ __forceinline__ void rot_hi2lo(double & x, double & y, double s, double c) {
-    double sy = __dmul_rn(s, y), sx = __dmul_rn(s, x);
-    double xn = __fma_rn(c, x, sy);
-    double yn = __fma_rn(c, y, -sx);
+    const double sy = __dmul_rn(s, y), sx = __dmul_rn(s, x);
+    const double xn = __fma_rn(c, x, sy);
+    const double yn = __fma_rn(c, y, -sx);
     x = xn; y = yn;
 }
 __device__ __forceinline__ void rot_lo2hi(double & x, double & y, double s, double c) {
-    double sy = __dmul_rn(s, y), sx = __dmul_rn(s, x);
-    double xn = __fma_rn(c, x, -sy);
-    double yn = __fma_rn(c, y, sx);
+    const double sy = __dmul_rn(s, y), sx = __dmul_rn(s, x);
+    const double xn = __fma_rn(c, x, -sy);
+    const double yn = __fma_rn(c, y, sx);
     x = xn; y = yn;
 }
 
+// Lane layout: lane = o * CH + c owns chain c of the NCOL columns of order
+// mbase + STEP * o (sph: cos and sin columns 2m-1, 2m; disk: the same pair;
+// tri: column m).  The NCOL columns of a lane share every (sin, cos) pair, so
+// one shared-memory load feeds NCOL rotations.
 template <int KIND, bool HI2LO, int W, int B, int E>
-__global__ void __maxnreg__(200)
+__global__ void __launch_bounds__(W * 32, 1)
 rot_kernel(const __grid_constant__ RotLaunch L) {
-    constexpr int CH = KT<KIND>::CH, STEP = KT<KIND>::STEP, ORD = KT<KIND>::ORDERS;
+    using T = KT<KIND>;
+    constexpr int CH = T::CH, STEP = T::STEP, NCOL = T::NCOL, ORD = T::ORD, COLS = T::COLS, CPAD = T::CPAD;
     constexpr int WB = W * B;
     static_assert(E % (2 * B) == 0, "chunk must be a multiple of the window");
     extern __shared__ double smem[];
-    // buffer q (0..W): input of stage q (q = W: output of the last stage), 2 slots
+    // buffer q (0..W): input of stage q (q = W: output of the last stage), 2 slots,
+    // element (step u, chain c, task column cl)
     auto buf = [&](int q, int slot, int u, int c) -> double * {
-        return smem + ((((q * 2 + slot) * E + u) * CH + c) * PAD);
+        return smem + ((((q * 2 + slot) * E + u) * CH + c) * CPAD);
     };
+    // (sin, cos) pairs of the chunk a stage works on, staged one iteration ahead
+    double2 * const sc_stage_base = reinterpret_cast<double2 *>(smem + (W + 1) * 2 * E * CH * CPAD);
+    auto sc_stage = [&](int q, int slot) -> double2 * { return sc_stage_base + ((q * 2 + slot) * B) * (E * CH); };
     __shared__ int s_task;
     __shared__ SweepInfo sweep_info[W * B];
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const bool is_loader = warp == 0, is_storer = warp == W + 1;
-    const int q = warp - 1;   // stage index for stage warps
+    const int q = warp;                       // stage index
+    const int o_lane = lane / CH, c_lane = lane % CH;
 
     for (;;) {
         if (threadIdx.x == 0) s_task = atomicAdd(L.counter, 1);
@@ -97,11 +121,7 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
         const int jhi = omax - STEP;
         const int nsw = (jhi - jlo) / STEP + 1;
         const int npass = (nsw + WB - 1) / WB;
-
-        // this lane's column (for the loader and storer, the lane index is a column too)
-        const int m_lane = KIND == TRI ? mbase + lane : mbase + 2 * (lane >> 1);
-        const int col_lane = KIND == TRI ? m_lane : 2 * m_lane - 1 + (lane & 1);
-        const bool lane_ok = m_lane <= mlast;
+        const int m_lane = mbase + STEP * o_lane;
         const int L0 = Geo::chain_len(KIND, N, 0);
 
         for (int r = 0; r < npass; ++r) {
@@ -122,40 +142,73 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
             const int tend = HI2LO ? ref + 2 * WB : emax + 2 * WB - 1;
             const int K = (tend - tstart + 1 + E - 1) / E;
 
-            // ---- stage state ----
-            double win[CH][2 * B];
+            // ---- stage state: per column a window of 2B chain positions ----
+            double win[NCOL][2 * B];
 #pragma unroll
-            for (int c = 0; c < CH; ++c)
+            for (int h = 0; h < NCOL; ++h)
 #pragma unroll
-                for (int x = 0; x < 2 * B; ++x) win[c][x] = 0.0;
-            // per sweep of this stage (lane b < B computes sweep q*B + b): order j,
-            // table column base and valid step range per chain, kept in shared memory
-            SweepInfo * const my = sweep_info + (is_loader || is_storer ? 0 : q * B);
-            bool full_lanes = false;
-            if (!is_loader && !is_storer) {
-                if (lane < B) {
-                    const int s = q * B + lane;
-                    SweepInfo si;
-                    si.j = HI2LO ? jfirst - STEP * s : jfirst + STEP * s;
-                    const bool sv = s < S;
-                    si.tbase = sv ? Geo::table_base(KIND, N, si.j) : 0;
+                for (int x = 0; x < 2 * B; ++x) win[h][x] = 0.0;
+            // per sweep of this stage (lane b < B computes sweep q*B + b)
+            SweepInfo * const my = sweep_info + q * B;
+            if (lane < B) {
+                const int s = q * B + lane;
+                SweepInfo si;
+                si.j = HI2LO ? jfirst - STEP * s : jfirst + STEP * s;
+                const bool sv = s < S;
+                si.tbase = sv ? Geo::table_base(KIND, N, si.j) : 0;
 #pragma unroll
-                    for (int c = 0; c < CH; ++c) {
-                        const int ts = HI2LO ? topc[c] + s : topc[c] - s;
-                        if (HI2LO) { si.tlo[c] = ref + 2 * s - ts; si.thi[c] = ref + 2 * s; }
-                        else       { si.tlo[c] = 2 * s;            si.thi[c] = 2 * s + ts; }
-                        if (!sv || ts < 0) { si.tlo[c] = 1; si.thi[c] = 0; }   // empty
-                    }
-                    my[lane] = si;
+                for (int c = 0; c < 2; ++c) {
+                    const int ts = HI2LO ? Geo::top(KIND, N, jfirst, c < CH ? c : 0) + s : Geo::top(KIND, N, jfirst, c < CH ? c : 0) - s;
+                    if (HI2LO) { si.tlo[c] = ref + 2 * s - ts; si.thi[c] = ref + 2 * s; }
+                    else       { si.tlo[c] = 2 * s;            si.thi[c] = 2 * s + ts; }
+                    if (!sv || ts < 0) { si.tlo[c] = 1; si.thi[c] = 0; }   // empty
                 }
-                __syncwarp();
-                const int jmax = HI2LO ? jfirst - STEP * (q * B) : jfirst + STEP * (q * B + B - 1);
-                full_lanes = jmax <= mbase - STEP;
+                my[lane] = si;
+            }
+            __syncwarp();
+            const int jmax = HI2LO ? jfirst - STEP * (q * B) : jfirst + STEP * (q * B + B - 1);
+            const bool full_lanes = jmax <= mbase - STEP;   // every sweep of this stage applies to every order
+            unsigned lane_mask = 0;                          // sweeps that apply to this lane's order
+#pragma unroll
+            for (int b = 0; b < B; ++b) {
+                const int sg = q * B + b;
+                const int j = HI2LO ? jfirst - STEP * sg : jfirst + STEP * sg;
+                if (j <= m_lane - STEP) lane_mask |= 1u << b;
             }
 
-            // ---- loader: chunk k goes to slot k & 1 one iteration before stage 0 reads it ----
-            constexpr int PER = (E * CH * 32) / 32;   // elements per lane per chunk
-            double pre[PER];
+            // Stage the (sin, cos) pairs of a chunk: entry (b, jj) is the pair sweep b
+            // uses at step u of the chunk on chain c; where the sweep has no valid
+            // position at that step the entry is the identity (sin 0, cos 1), so every
+            // chunk runs the same straight-line code and those rotations are exact no-ops.
+            auto prefetch_sc = [&](int kp) {
+                const int t0p = tstart + kp * E;
+                double2 * const d = sc_stage(q, kp & 1);
+#pragma unroll
+                for (int rr = 0; rr < (B * E * CH) / 32; ++rr) {
+                    const int f = rr * 32 + lane;
+                    const int b = f / (E * CH), jj = f % (E * CH);
+                    const int c = CH == 2 ? (jj & 1) : 0;
+                    const int u = HI2LO ? (E - 1 - (CH == 2 ? (jj >> 1) : jj)) : (CH == 2 ? (jj >> 1) : jj);
+                    const int t = t0p + u;
+                    const int s = q * B + b;
+                    const SweepInfo & si = my[b];
+                    if (t >= si.tlo[c] && t <= si.thi[c]) {
+                        const int i = HI2LO ? ref + 2 * s - t : t - 2 * s;
+                        cp_async16(d + f, F.sc + si.tbase + (CH == 2 ? 2 * i + c : i));
+                    } else {
+                        d[f] = make_double2(0.0, 1.0);
+                    }
+                }
+                cp_async_commit();
+            };
+
+            // ---- global traffic, shared by all warps: warp w moves elements
+            //      v in [w*PER_W, (w+1)*PER_W) of each chunk (f = v*32 + lane) ----
+            constexpr int RPC = E * CH;                // rows of one column segment per chunk
+            constexpr int PER = COLS * RPC / 32;       // elements per lane per chunk (all warps)
+            constexpr int PER_W = PER / W;             // this warp's share
+            static_assert(PER % W == 0, "chunk must split evenly over the warps");
+            double pre[PER_W];
             auto chunk_row = [&](int k, int rr, int & row, int & u, int & c, bool storer) -> bool {
                 // rr: row offset within the chunk's contiguous row range; returns validity
                 const int t0 = tstart + k * E;
@@ -168,150 +221,113 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
                 u = HI2LO ? (pmin + E - 1 - p) : (p - pmin);
                 return p >= 0 && p <= emax && row < N;
             };
-            auto load_chunk = [&](int k, double * dstv) {
+            auto column_of = [&](int cl, int & mcl) -> long long {
+                const int o = cl / NCOL, h = cl % NCOL;
+                mcl = mbase + STEP * o;
+                return KIND == TRI ? mcl : 2 * mcl - 1 + h;
+            };
+            auto load_chunk = [&](int k) {
 #pragma unroll
-                for (int v = 0; v < PER; ++v) {
-                    const int f = v * 32 + lane;
-                    const int cl = f / (E * CH), rr = f % (E * CH);
-                    int row, u, c;
+                for (int v = 0; v < PER_W; ++v) {
+                    const int f = (q * PER_W + v) * 32 + lane;
+                    const int cl = f / RPC, rr = f % RPC;
+                    int row, u, c, mcl;
                     const bool ok = chunk_row(k, rr, row, u, c, false);
-                    const int mcl = KIND == TRI ? mbase + cl : mbase + 2 * (cl >> 1);
-                    const int colc = KIND == TRI ? mcl : 2 * mcl - 1 + (cl & 1);
+                    const long long colc = column_of(cl, mcl);
                     double val = 0.0;
-                    if (ok && k < K && mcl <= mlast) val = __ldcg(src + (long long) colc * lda + row);
-                    dstv[v] = val;
+                    if (ok && k < K && mcl <= mlast) val = __ldcg(src + colc * lda + row);
+                    pre[v] = val;
                 }
             };
-            auto store_pre = [&](int k, const double * v_) {
+            auto stash_chunk = [&](int k) {
 #pragma unroll
-                for (int v = 0; v < PER; ++v) {
-                    const int f = v * 32 + lane;
-                    const int cl = f / (E * CH), rr = f % (E * CH);
+                for (int v = 0; v < PER_W; ++v) {
+                    const int f = (q * PER_W + v) * 32 + lane;
+                    const int cl = f / RPC, rr = f % RPC;
                     int row, u, c;
                     chunk_row(k, rr, row, u, c, false);
-                    buf(0, k & 1, u, c)[cl] = v_[v];
+                    buf(0, k & 1, u, c)[cl] = pre[v];
                 }
             };
-            if (is_loader) {
-                load_chunk(0, pre);
-                store_pre(0, pre);
-            }
+            auto store_chunk = [&](int k) {
+#pragma unroll
+                for (int v = 0; v < PER_W; ++v) {
+                    const int f = (q * PER_W + v) * 32 + lane;
+                    const int cl = f / RPC, rr = f % RPC;
+                    int row, u, c, mcl;
+                    const bool ok = chunk_row(k, rr, row, u, c, true);
+                    const long long colc = column_of(cl, mcl);
+                    const double val = buf(W, k & 1, u, c)[cl];
+                    if (ok && mcl <= mlast) __stcg(dst + colc * lda + row, val);
+                }
+            };
+            load_chunk(0);
+            stash_chunk(0);
+            if (q == 0) prefetch_sc(0);
+            cp_async_wait_all();
             __syncthreads();
 
             for (int it = 0; it < K + W; ++it) {
-                if (is_loader) {
-                    // chunk it+1: its loads are in flight while the stages work on chunk it
-                    if (it + 1 < K) {
-                        load_chunk(it + 1, pre);
-                        store_pre(it + 1, pre);
-                    }
-                } else if (is_storer) {
-                    const int k = it - W;
-                    if (k >= 0 && k < K) {
+                // chunk it+1: loads in flight while the stages work on their chunks
+                if (it + 1 < K) load_chunk(it + 1);
+                // the last stage finished chunk it-W in the previous iteration
+                if (it - W >= 0 && it - W < K) store_chunk(it - W);
+                // (sin, cos) of the chunk this stage works on next iteration
+                if (it + 1 - q >= 0 && it + 1 - q < K) prefetch_sc(it + 1 - q);
+                const int k = it - q;
+                if (k >= 0 && k < K) {
+                    const int slot = k & 1;
+                    const double2 * const scb = sc_stage(q, slot);
+                    const bool masked = !full_lanes;
+                    // two copies of the step loop: all sweeps apply to all lanes, or per-lane masks
+                    auto run = [&](auto masked_tag) {
+                        constexpr bool MASKED = decltype(masked_tag)::value;
 #pragma unroll
-                        for (int v = 0; v < PER; ++v) {
-                            const int f = v * 32 + lane;
-                            const int cl = f / (E * CH), rr = f % (E * CH);
-                            int row, u, c;
-                            const bool ok = chunk_row(k, rr, row, u, c, true);
-                            const int mcl = KIND == TRI ? mbase + cl : mbase + 2 * (cl >> 1);
-                            const int colc = KIND == TRI ? mcl : 2 * mcl - 1 + (cl & 1);
-                            const double val = buf(W, k & 1, u, c)[cl];
-                            if (ok && mcl <= mlast) __stcg(dst + (long long) colc * lda + row, val);
-                        }
-                    }
-                } else {
-                    const int k = it - q;
-                    if (k >= 0 && k < K) {
-                        const int t0 = tstart + k * E;
-                        const int slot = k & 1;
-                        bool mine = true;
-                        const double2 * tpl = F.sc;
-                        if (lane < B) {
-                            const SweepInfo si = my[lane];
+                        for (int u = 0; u < E; ++u) {
+                            const double * bin = buf(q, slot, u, c_lane) + o_lane * NCOL;
+                            double * bout = buf(q + 1, slot, u, c_lane) + o_lane * NCOL;
 #pragma unroll
-                            for (int c = 0; c < CH; ++c) mine = mine && t0 >= si.tlo[c] && t0 + E - 1 <= si.thi[c];
-                            const int s = q * B + lane;
-                            long long off;
-                            if (HI2LO) off = (CH == 2) ? 2LL * (ref + 2 * s - t0) : (long long) (ref + 2 * s - t0);
-                            else       off = (CH == 2) ? 2LL * (t0 - 2 * s) : (long long) (t0 - 2 * s);
-                            tpl = F.sc + si.tbase + off;
-                        }
-                        const bool interior = full_lanes && __all_sync(0xffffffffu, mine);
-                        if (interior) {
-                            // table pointers at step t0 for every sweep of the stage
-                            const double2 * tp[B];
+                            for (int h = 0; h < NCOL; ++h) {
+                                const double in = bin[h];
+                                const double out = win[h][2 * B - 1];
 #pragma unroll
-                            for (int b = 0; b < B; ++b)
-                                tp[b] = reinterpret_cast<const double2 *>(__shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(tpl), b));
-#pragma unroll
-                            for (int u = 0; u < E; ++u) {
-#pragma unroll
-                                for (int c = 0; c < CH; ++c) {
-                                    const double in = buf(q, slot, u, c)[lane];
-                                    const double out = win[c][2 * B - 1];
-#pragma unroll
-                                    for (int x = 2 * B - 1; x > 0; --x) win[c][x] = win[c][x - 1];
-                                    win[c][0] = in;
-                                    buf(q + 1, slot, u, c)[lane] = out;
-                                }
-#pragma unroll
-                                for (int b = 0; b < B; ++b) {
-#pragma unroll
-                                    for (int c = 0; c < CH; ++c) {
-                                        const int o = HI2LO ? (CH == 2 ? -2 * u + c : -u) : (CH == 2 ? 2 * u + c : u);
-                                        const double2 sc = __ldg(tp[b] + o);
-                                        if (HI2LO) rot_hi2lo(win[c][2 * b], win[c][2 * b + 1], sc.x, sc.y);
-                                        else       rot_lo2hi(win[c][2 * b + 1], win[c][2 * b], sc.x, sc.y);
-                                    }
-                                }
+                                for (int x = 2 * B - 1; x > 0; --x) win[h][x] = win[h][x - 1];
+                                win[h][0] = in;
+                                bout[h] = out;
                             }
-                        } else {
+                            const int obase = HI2LO ? (CH == 2 ? 2 * (E - 1 - u) : E - 1 - u) : (CH == 2 ? 2 * u : u);
 #pragma unroll
-                            for (int u = 0; u < E; ++u) {
-                                const int t = t0 + u;
-#pragma unroll
-                                for (int c = 0; c < CH; ++c) {
-                                    const double in = buf(q, slot, u, c)[lane];
-                                    const double out = win[c][2 * B - 1];
-#pragma unroll
-                                    for (int x = 2 * B - 1; x > 0; --x) win[c][x] = win[c][x - 1];
-                                    win[c][0] = in;
-                                    buf(q + 1, slot, u, c)[lane] = out;
+                            for (int b = 0; b < B; ++b) {
+                                const double2 sc = scb[b * (E * CH) + obase + (CH == 2 ? c_lane : 0)];
+                                double sn = sc.x, cs = sc.y;
+                                if (MASKED) {
+                                    const bool on = (lane_mask >> b) & 1u;
+                                    sn = on ? sn : 0.0;
+                                    cs = on ? cs : 1.0;
                                 }
 #pragma unroll
-                                for (int b = 0; b < B; ++b) {
-                                    const int s = q * B + b;
-                                    const SweepInfo si = my[b];
-                                    const bool lane_on = si.j <= m_lane - STEP;
-#pragma unroll
-                                    for (int c = 0; c < CH; ++c) {
-                                        if (t >= si.tlo[c] && t <= si.thi[c]) {
-                                            const int i = HI2LO ? ref + 2 * s - t : t - 2 * s;
-                                            const int krow = CH == 2 ? 2 * i + c : i;
-                                            const double2 sc = __ldg(F.sc + si.tbase + krow);
-                                            const double sn = lane_on ? sc.x : 0.0;
-                                            const double cs = lane_on ? sc.y : 1.0;
-                                            if (HI2LO) rot_hi2lo(win[c][2 * b], win[c][2 * b + 1], sn, cs);
-                                            else       rot_lo2hi(win[c][2 * b + 1], win[c][2 * b], sn, cs);
-                                        }
-                                    }
+                                for (int h = 0; h < NCOL; ++h) {
+                                    if (HI2LO) rot_hi2lo(win[h][2 * b], win[h][2 * b + 1], sn, cs);
+                                    else       rot_lo2hi(win[h][2 * b + 1], win[h][2 * b], sn, cs);
                                 }
                             }
                         }
-                    }
+                    };
+                    if (masked) run(std::true_type{});
+                    else        run(std::false_type{});
                 }
+                if (it + 1 < K) stash_chunk(it + 1);
+                cp_async_wait_all();
                 __syncthreads();
             }
         }
-        (void) lane_ok; (void) col_lane;
     }
 }
 
 template <int KIND, bool HI2LO, int W, int B, int E>
 cudaError_t launch_cfg(const RotLaunch & L, int max_ctas, cudaStream_t st) {
-    constexpr int CH = KT<KIND>::CH;
-    const size_t shm = sizeof(double) * (size_t) (W + 1) * 2 * E * CH * PAD;
+    constexpr int CH = KT<KIND>::CH, CPAD = KT<KIND>::CPAD;
+    const size_t shm = sizeof(double) * (size_t) (W + 1) * 2 * E * CH * CPAD + sizeof(double2) * (size_t) W * 2 * B * E * CH;
     auto kern = rot_kernel<KIND, HI2LO, W, B, E>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) shm);
     if (e != cudaSuccess) return e;
@@ -324,9 +340,16 @@ cudaError_t launch_cfg(const RotLaunch & L, int max_ctas, cudaStream_t st) {
     if (ctas <= 0) return cudaSuccess;
     e = cudaMemsetAsync(L.counter, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
-    kern<<<ctas, (W + 2) * 32, shm, st>>>(L);
+    kern<<<ctas, W * 32, shm, st>>>(L);
     count_launch();
-    return cudaGetLastError();
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        cudaFuncAttributes fa{};
+        cudaFuncGetAttributes(&fa, kern);
+        std::fprintf(stderr, "rot_kernel launch failed (%s): regs %d, static smem %zu, dyn smem %zu, max threads %d, params %zu B\n",
+                     cudaGetErrorString(e), fa.numRegs, fa.sharedSizeBytes, shm, fa.maxThreadsPerBlock, sizeof(RotLaunch));
+    }
+    return e;
 }
 
 }  // namespace
