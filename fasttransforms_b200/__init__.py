@@ -29,7 +29,7 @@ __all__ = [
     "plan_rotsphere", "plan_rottriangle", "plan_rotdisk",
     "execute_sph_hi2lo", "execute_sph_lo2hi", "execute_tri_hi2lo", "execute_tri_lo2hi",
     "execute_disk_hi2lo", "execute_disk_lo2hi",
-    "execute_dev", "execute_batched_dev", "rotations_dev", "kernel_launches", "profile", "profile_read",
+    "execute_dev", "execute_noalloc_dev", "NOALLOC_MAX_ELEMS", "execute_batched_dev", "rotations_dev", "kernel_launches", "profile", "profile_read",
     "layout_cols", "rand_layout", "sphrand", "trirand", "diskrand",
     "SPH", "TRI", "DISK",
 ]
@@ -51,7 +51,7 @@ class FTB200Error(RuntimeError):
 
 def _load() -> C.CDLL:
     if not os.path.exists(library_path):
-        raise ImportError(f"{library_path} is not built (python -m fasttransforms_b200.build)")
+        raise ImportError(f"{library_path} is not built (python fasttransforms_b200/build.py)")
     L = C.CDLL(library_path)
     vp, dp, i, d, ch = C.c_void_p, C.POINTER(C.c_double), C.c_int, C.c_double, C.c_char
     sig = {
@@ -65,6 +65,7 @@ def _load() -> C.CDLL:
         "ft_b200_rotations_dev": (i, [vp, i, vp, i, vp]),
         "ft_b200_execute_batched_dev": (i, [C.POINTER(vp), i, ch, C.POINTER(vp), C.POINTER(i), C.POINTER(i), i, vp]),
         "ft_b200_plan_kind": (i, [vp]), "ft_b200_plan_device": (i, [vp]),
+        "ft_b200_execute_noalloc_dev": (i, [vp, i, ch, vp, i, i, vp]),
         "ft_b200_profile": (i, [i]), "ft_b200_profile_read": (i, [i, C.POINTER(C.c_double), C.POINTER(i)]),
     }
     for name in ("sph2fourier", "fourier2sph", "tri2cheb", "cheb2tri", "disk2cxf", "cxf2disk"):
@@ -229,6 +230,23 @@ def execute_disk_lo2hi(RP, A, M=None): _exec_rot("ft_execute_disk_lo2hi", RP, A,
 def execute_dev(P: HarmonicPlan, forward: bool, trans: str, ptr: int, N: int, M: int, stream: int = 0) -> None:
     """Full transform on a device matrix (N x M, column-major) enqueued on ``stream``."""
     st = lib.ft_b200_execute_dev(P.ptr, 1 if forward else 0, trans.encode(), C.c_void_p(ptr), N, M, C.c_void_p(stream))
+    if st != 0:
+        _check()
+
+
+NOALLOC_MAX_ELEMS = 1 << 20
+
+
+def execute_noalloc_dev(P: HarmonicPlan, forward: bool, trans: str, ptr: int, N: int, M: int, stream: int = 0) -> None:
+    """Like execute_dev, but the library allocates no device memory for the call.
+
+    For callers that manage all device memory themselves and cannot let a
+    library call cudaMalloc: the intermediate matrix lives in a fixed 8 MiB
+    device array inside the library, so N*M is limited to NOALLOC_MAX_ELEMS and
+    M must be the plan's default.  The array is shared by every call: calls that
+    overlap on the GPU race and must be serialised by the caller.
+    """
+    st = lib.ft_b200_execute_noalloc_dev(P.ptr, 1 if forward else 0, trans.encode(), C.c_void_p(ptr), N, M, C.c_void_p(stream))
     if st != 0:
         _check()
 

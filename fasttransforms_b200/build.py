@@ -1,6 +1,6 @@
 """Build the sm_100a library in-tree: fasttransforms_b200/_lib/libft_b200.so.
 
-    python -m fasttransforms_b200.build
+    python fasttransforms_b200/build.py      (by path: the package import loads the library)
 
 nvcc compiles the CUDA kernels and the host plan code for sm_100a only and
 links a shared library with a static CUDA runtime that exports only the C ABI
@@ -19,7 +19,7 @@ OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libft_b200.so")
 BUILD_DIR = os.path.join(HERE, "_build")
 
-SOURCES = ["rotations.cu", "trmm.cu", "api.cu", "plan.cpp"]
+SOURCES = ["rotations.cu", "trmm.cu", "api.cu", "noalloc.cu", "plan.cpp"]
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "-ccbin", "/usr/bin/g++"]

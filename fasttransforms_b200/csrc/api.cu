@@ -23,7 +23,6 @@ namespace {
 thread_local int t_status = FT_B200_OK;
 thread_local std::string t_message;
 std::atomic<unsigned long long> g_launches{0};
-constexpr int kPlanMagic = 0x46544232;   // "FTB2"
 }  // namespace
 
 namespace {
@@ -85,28 +84,24 @@ bool check_device(int * dev_out) {
     return true;
 }
 
-struct HarmonicPlan {
-    ft_harmonic_plan pub;       // must stay the first member
-    int magic;
-    int kind, n, Mdef;
-    ft_rotation_plan * rp_arr[1];
-    double * hostP[2];
-    double * hostPinv[2];
-    double * dP[2];
-    double * dPinv[2];
-    double * d_scratch;
-    size_t scratch_elems;
-    double * d_stage;           // device copy of A for host-pointer calls
-    size_t stage_elems;
-    cudaStream_t stream;
-    int device;
-};
+}  // namespace
 
 HarmonicPlan * as_plan(const ft_harmonic_plan * P) {
     if (!P) return nullptr;
     HarmonicPlan * H = reinterpret_cast<HarmonicPlan *>(const_cast<ft_harmonic_plan *>(P));
     return H->magic == kPlanMagic ? H : nullptr;
 }
+
+bool find_tasks(ft_rotation_plan * RP, int M, const RotTask ** d_tasks, int * ntasks) {
+    std::lock_guard<std::mutex> lk(*RP->mu);
+    auto it = RP->tasks->find(M);
+    if (it == RP->tasks->end()) return false;
+    *d_tasks = it->second.first;
+    *ntasks = it->second.second;
+    return true;
+}
+
+namespace {
 
 int default_cols(int kind, int n) { return kind == SPH ? 2 * n - 1 : kind == TRI ? n : 4 * n - 3; }
 

@@ -126,6 +126,29 @@ double * connection_jacobi(int n, double alpha, double beta, double gamma, doubl
 std::vector<RotTask> build_tasks(int kind, int N, int M, int field);
 double task_cost(int kind, int N, int M, int mbase);
 
+// The harmonic plan behind ft_harmonic_plan * (the public struct is its first member).
+constexpr int kPlanMagic = 0x46544232;   // "FTB2"
+struct HarmonicPlan {
+    ft_harmonic_plan pub;       // must stay the first member
+    int magic;
+    int kind, n, Mdef;
+    ft_rotation_plan * rp_arr[1];
+    double * hostP[2];
+    double * hostPinv[2];
+    double * dP[2];
+    double * dPinv[2];
+    double * d_scratch;
+    size_t scratch_elems;
+    double * d_stage;           // device copy of A for host-pointer calls
+    size_t stage_elems;
+    cudaStream_t stream;
+    int device;
+};
+// NULL unless P is a live plan of this library (api.cu)
+HarmonicPlan * as_plan(const ft_harmonic_plan * P);
+// device task list already built for (RP, M), without building one (api.cu)
+bool find_tasks(ft_rotation_plan * RP, int M, const RotTask ** d_tasks, int * ntasks);
+
 // Error state (api.cu).
 void set_error(int status, const std::string & msg);
 void clear_error();

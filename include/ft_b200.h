@@ -141,6 +141,34 @@ int ft_b200_rotations_dev(const ft_rotation_plan * RP, int hi2lo, double * dA, i
 int ft_b200_execute_batched_dev(const ft_harmonic_plan * const * plans, int forward, char TRANS,
                                 double * const * dA, const int * N, const int * M, int nfields, void * stream);
 
+/* Allocation-free variant of ft_b200_execute_dev.  No counterpart in the
+ * reference (whose plans own host scratch).
+ *
+ * For callers that cannot let a library allocate device memory: frameworks
+ * that own all device memory through their own pool and hand a library only
+ * the arrays it works on, and long-running services that reserve memory at
+ * start-up and must not allocate afterwards, because cudaMalloc / cudaFree can
+ * block or synchronise the device and can fail under memory pressure.
+ *
+ * Same transform and arguments as ft_b200_execute_dev; A is the caller's
+ * device matrix (input and output).  The intermediate matrix and the rotation
+ * kernel's work counter live in a fixed device array compiled into the library
+ * (FT_B200_NOALLOC_MAX_ELEMS doubles, 8 MiB, plus 256 bytes), which every GPU
+ * that loads the library holds until the process exits.  The call makes no
+ * cudaMalloc / cudaFree and no allocating library call.
+ *   - N*M above FT_B200_NOALLOC_MAX_ELEMS is rejected with FT_B200_EINVAL.
+ *   - M must be the plan's default (2N-1, N, 4N-3); other M return
+ *     FT_B200_EUNSUPPORTED, since their task list would have to be allocated.
+ *   - The first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress) with that device current; make that first call
+ *     before any stream capture.
+ *   - All calls share the one array, which keeps the last call's contents; the
+ *     work counter is cleared by every call.  Calls that overlap on the GPU
+ *     (concurrent streams, or several host threads) race on the array and must
+ *     be serialised by the caller. */
+#define FT_B200_NOALLOC_MAX_ELEMS (1 << 20)
+int ft_b200_execute_noalloc_dev(const ft_harmonic_plan * P, int forward, char TRANS, double * dA, int N, int M, void * stream);
+
 /* Kind of a plan (FT_B200_SPH / TRI / DISK), or -1. */
 int ft_b200_plan_kind(const ft_harmonic_plan * P);
 /* Device id the plan lives on. */
