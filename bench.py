@@ -345,6 +345,22 @@ def run_ours(args, rank, world, local_rank, dist):
     print(json.dumps(line))
 
 
+def profile_case(n: int) -> None:
+    """Small fixed program for ncu captures: plan, seeded field, two forward transforms."""
+    import torch
+    import fasttransforms_b200 as ft
+    M = 2 * n - 1
+    P = ft.plan_sph2fourier(n)
+    A = ft.sphrand(n, SEED)
+    d = torch.from_numpy(A.ravel(order="F").copy()).cuda()
+    s = torch.cuda.current_stream().cuda_stream
+    for _ in range(2):
+        ft.execute_dev(P, True, "N", d.data_ptr(), n, M, s)
+    torch.cuda.synchronize()
+    P.close()
+    print(json.dumps({"profile_case": f"sph n={n}", "max_abs": float(d.abs().max())}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -354,7 +370,12 @@ def main():
     ap.add_argument("--n", type=int, default=4096)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-sample", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--profile-case", action="store_true",
+                    help="run one plan and two forward transforms (for ncu), no timing")
     args = ap.parse_args()
+    if args.profile_case:
+        profile_case(args.n)
+        return
     if args.cpu_sample:
         print(json.dumps(cpu_sample(args.n, 2)))
         return

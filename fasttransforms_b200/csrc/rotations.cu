@@ -33,6 +33,7 @@
 // loops.  Every global access is bounds-checked against the field's N, M.
 
 #include <cstdio>
+#include <cstdlib>
 #include <type_traits>
 
 #include "ft_internal.h"
@@ -87,6 +88,7 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
     constexpr int CH = T::CH, STEP = T::STEP, NCOL = T::NCOL, ORD = T::ORD, COLS = T::COLS, CPAD = T::CPAD;
     constexpr int WB = W * B;
     static_assert(E % (2 * B) == 0, "chunk must be a multiple of the window");
+    static_assert((B * E * CH) % 32 == 0, "a chunk's (sin, cos) entries must split evenly over the lanes");
     extern __shared__ double smem[];
     // buffer q (0..W): input of stage q (q = W: output of the last stage), 2 slots,
     // element (step u, chain c, task column cl)
@@ -128,8 +130,14 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
             const double * src = r == 0 ? F.in : F.out;
             double * dst = F.out;
             const bool copy_all = r == 0 && F.in != F.out;
-            const int s0 = r * WB;
-            const int S = min(WB, nsw - s0);
+            // Passes of W*B sweeps; the one partial pass is the one with the shortest
+            // sweeps (the first in hi2lo order, the last in lo2hi order), and only its
+            // first WA stages run, so its cost scales with its sweeps.
+            const int rem = nsw - (npass - 1) * WB;   // sweeps of the partial pass (1..WB)
+            const int s0 = HI2LO ? (r == 0 ? 0 : rem + (r - 1) * WB) : r * WB;
+            const int S = HI2LO ? (r == 0 ? rem : WB) : min(WB, nsw - s0);
+            const int WA = (S + B - 1) / B;            // active stages
+            const int WAB = WA * B;
             const int jfirst = HI2LO ? jhi - STEP * s0 : jlo + STEP * s0;
             int topc[CH];
 #pragma unroll
@@ -139,7 +147,7 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
             if (copy_all || emax > L0 - 1) emax = L0 - 1;
             if (emax < 0) emax = 0;
             const int tstart = HI2LO ? ref - emax : -1;
-            const int tend = HI2LO ? ref + 2 * WB : emax + 2 * WB - 1;
+            const int tend = HI2LO ? ref + 2 * WAB : emax + 2 * WAB - 1;
             const int K = (tend - tstart + 1 + E - 1) / E;
 
             // ---- stage state: per column a window of 2B chain positions ----
@@ -209,57 +217,59 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
             constexpr int PER_W = PER / W;             // this warp's share
             static_assert(PER % W == 0, "chunk must split evenly over the warps");
             double pre[PER_W];
-            auto chunk_row = [&](int k, int rr, int & row, int & u, int & c, bool storer) -> bool {
-                // rr: row offset within the chunk's contiguous row range; returns validity
-                const int t0 = tstart + k * E;
-                int pmin;
-                if (HI2LO) pmin = ref - t0 - E + 1 + (storer ? 2 * WB : 0);
-                else       pmin = t0 + 1 - (storer ? 2 * WB : 0);
-                int p;
-                if (CH == 2) { p = pmin + (rr >> 1); c = rr & 1; row = 2 * p + c; }
-                else         { p = pmin + rr; c = 0; row = p; }
-                u = HI2LO ? (pmin + E - 1 - p) : (p - pmin);
-                return p >= 0 && p <= emax && row < N;
-            };
-            auto column_of = [&](int cl, int & mcl) -> long long {
+            // Element v of this lane's share: task column cl and row offset rr inside
+            // the chunk's contiguous row range (row = CH * pmin + rr).  Everything but
+            // pmin is fixed for the pass, so it is computed once here.
+            const double * gsrc[PER_W];
+            double * gdst[PER_W];
+            int ioff[PER_W];     // rr >> (CH - 1): position offset from pmin
+            int rro[PER_W];      // rr: row offset from CH * pmin
+            int soff[PER_W];     // shared-memory offset inside a slot
+            bool colok[PER_W];
+#pragma unroll
+            for (int v = 0; v < PER_W; ++v) {
+                const int f = (q * PER_W + v) * 32 + lane;
+                const int cl = f / RPC, rr = f % RPC;
                 const int o = cl / NCOL, h = cl % NCOL;
-                mcl = mbase + STEP * o;
-                return KIND == TRI ? mcl : 2 * mcl - 1 + h;
+                const int mcl = mbase + STEP * o;
+                const long long colc = KIND == TRI ? mcl : 2 * mcl - 1 + h;
+                colok[v] = mcl <= mlast;
+                const long long coff = colok[v] ? colc * lda + rr : 0;
+                gsrc[v] = src + coff;
+                gdst[v] = dst + coff;
+                ioff[v] = CH == 2 ? (rr >> 1) : rr;
+                rro[v] = rr;
+                const int c = CH == 2 ? (rr & 1) : 0;
+                const int u = HI2LO ? E - 1 - ioff[v] : ioff[v];
+                soff[v] = (u * CH + c) * CPAD + cl;
+            }
+            // lowest chain position of chunk k entering stage 0 (storer: leaving stage W-1)
+            auto pmin_of = [&](int k, bool storer) -> int {
+                const int t0 = tstart + k * E;
+                return HI2LO ? ref - t0 - E + 1 + (storer ? 2 * WAB : 0) : t0 + 1 - (storer ? 2 * WAB : 0);
+            };
+            auto row_ok = [&](int pmin, int v) -> bool {
+                const int p = pmin + ioff[v];
+                const int row = CH * pmin + rro[v];
+                return colok[v] && p >= 0 && p <= emax && row < N;
             };
             auto load_chunk = [&](int k) {
+                const int pmin = pmin_of(k, false);
 #pragma unroll
-                for (int v = 0; v < PER_W; ++v) {
-                    const int f = (q * PER_W + v) * 32 + lane;
-                    const int cl = f / RPC, rr = f % RPC;
-                    int row, u, c, mcl;
-                    const bool ok = chunk_row(k, rr, row, u, c, false);
-                    const long long colc = column_of(cl, mcl);
-                    double val = 0.0;
-                    if (ok && k < K && mcl <= mlast) val = __ldcg(src + colc * lda + row);
-                    pre[v] = val;
-                }
+                for (int v = 0; v < PER_W; ++v)
+                    pre[v] = (k < K && row_ok(pmin, v)) ? __ldcg(gsrc[v] + (long long) CH * pmin) : 0.0;
             };
             auto stash_chunk = [&](int k) {
+                double * const b0 = buf(0, k & 1, 0, 0);
 #pragma unroll
-                for (int v = 0; v < PER_W; ++v) {
-                    const int f = (q * PER_W + v) * 32 + lane;
-                    const int cl = f / RPC, rr = f % RPC;
-                    int row, u, c;
-                    chunk_row(k, rr, row, u, c, false);
-                    buf(0, k & 1, u, c)[cl] = pre[v];
-                }
+                for (int v = 0; v < PER_W; ++v) b0[soff[v]] = pre[v];
             };
             auto store_chunk = [&](int k) {
+                const int pmin = pmin_of(k, true);
+                const double * const bw = buf(WA, k & 1, 0, 0);
 #pragma unroll
-                for (int v = 0; v < PER_W; ++v) {
-                    const int f = (q * PER_W + v) * 32 + lane;
-                    const int cl = f / RPC, rr = f % RPC;
-                    int row, u, c, mcl;
-                    const bool ok = chunk_row(k, rr, row, u, c, true);
-                    const long long colc = column_of(cl, mcl);
-                    const double val = buf(W, k & 1, u, c)[cl];
-                    if (ok && mcl <= mlast) __stcg(dst + colc * lda + row, val);
-                }
+                for (int v = 0; v < PER_W; ++v)
+                    if (row_ok(pmin, v)) __stcg(gdst[v] + (long long) CH * pmin, bw[soff[v]]);
             };
             load_chunk(0);
             stash_chunk(0);
@@ -267,15 +277,15 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
             cp_async_wait_all();
             __syncthreads();
 
-            for (int it = 0; it < K + W; ++it) {
+            for (int it = 0; it < K + WA; ++it) {
                 // chunk it+1: loads in flight while the stages work on their chunks
                 if (it + 1 < K) load_chunk(it + 1);
-                // the last stage finished chunk it-W in the previous iteration
-                if (it - W >= 0 && it - W < K) store_chunk(it - W);
+                // the last active stage finished chunk it-WA in the previous iteration
+                if (it - WA >= 0 && it - WA < K) store_chunk(it - WA);
                 // (sin, cos) of the chunk this stage works on next iteration
-                if (it + 1 - q >= 0 && it + 1 - q < K) prefetch_sc(it + 1 - q);
+                if (q < WA && it + 1 - q >= 0 && it + 1 - q < K) prefetch_sc(it + 1 - q);
                 const int k = it - q;
-                if (k >= 0 && k < K) {
+                if (q < WA && k >= 0 && k < K) {
                     const int slot = k & 1;
                     const double2 * const scb = sc_stage(q, slot);
                     const bool masked = !full_lanes;
@@ -284,16 +294,20 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
                         constexpr bool MASKED = decltype(masked_tag)::value;
 #pragma unroll
                         for (int u = 0; u < E; ++u) {
+                            // The window is circular: at step u, window position x lives in
+                            // register slot (u - x) mod 2B.  The element leaving (position
+                            // 2B-1 of the previous step) sits in slot u mod 2B, which the
+                            // entering element (position 0) takes over.  E is a multiple of
+                            // 2B, so the mapping is the same at every chunk boundary.
+                            constexpr int W2 = 2 * B;
+                            const int pn = u % W2;
                             const double * bin = buf(q, slot, u, c_lane) + o_lane * NCOL;
                             double * bout = buf(q + 1, slot, u, c_lane) + o_lane * NCOL;
 #pragma unroll
                             for (int h = 0; h < NCOL; ++h) {
                                 const double in = bin[h];
-                                const double out = win[h][2 * B - 1];
-#pragma unroll
-                                for (int x = 2 * B - 1; x > 0; --x) win[h][x] = win[h][x - 1];
-                                win[h][0] = in;
-                                bout[h] = out;
+                                bout[h] = win[h][pn];
+                                win[h][pn] = in;
                             }
                             const int obase = HI2LO ? (CH == 2 ? 2 * (E - 1 - u) : E - 1 - u) : (CH == 2 ? 2 * u : u);
 #pragma unroll
@@ -305,10 +319,12 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
                                     sn = on ? sn : 0.0;
                                     cs = on ? cs : 1.0;
                                 }
+                                const int xl = (u - 2 * b + 2 * W2) % W2;       // window position 2b
+                                const int xu = (u - 2 * b - 1 + 2 * W2) % W2;   // window position 2b+1
 #pragma unroll
                                 for (int h = 0; h < NCOL; ++h) {
-                                    if (HI2LO) rot_hi2lo(win[h][2 * b], win[h][2 * b + 1], sn, cs);
-                                    else       rot_lo2hi(win[h][2 * b + 1], win[h][2 * b], sn, cs);
+                                    if (HI2LO) rot_hi2lo(win[h][xl], win[h][xu], sn, cs);
+                                    else       rot_lo2hi(win[h][xu], win[h][xl], sn, cs);
                                 }
                             }
                         }
@@ -354,13 +370,38 @@ cudaError_t launch_cfg(const RotLaunch & L, int max_ctas, cudaStream_t st) {
 
 }  // namespace
 
-// Tuned configuration per family: W stage warps x B sweeps per warp, chunk E.
+// Configurations: W stage warps x B sweeps per warp, chunk E.
+//   0: W = 8,  B = 8, E = 16 (255 registers, two warps per sub-partition)
+//   1: W = 16, B = 4, E = 8  (128 registers, four warps per sub-partition)
+//   2: W = 8,  B = 4, E = 8  (fewer sweeps per warp: lighter register pressure)
+//   3: W = 8,  B = 4, E = 16
+template <int KIND, bool HI2LO>
+cudaError_t launch_kind(int cfg, const RotLaunch & L, int max_ctas, cudaStream_t st) {
+    if constexpr (KIND != TRI) {
+        if (cfg == 1) return launch_cfg<KIND, HI2LO, 16, 4, 8>(L, max_ctas, st);
+    }
+    if (cfg == 2) return launch_cfg<KIND, HI2LO, 8, 4, 8>(L, max_ctas, st);
+    if (cfg == 3) return launch_cfg<KIND, HI2LO, 8, 4, 16>(L, max_ctas, st);
+    return launch_cfg<KIND, HI2LO, 8, 8, 16>(L, max_ctas, st);
+}
+
+int g_rot_cfg = -1;
+
+int rotation_config() {
+    if (g_rot_cfg < 0) {
+        const char * e = std::getenv("FT_B200_ROT_CFG");
+        g_rot_cfg = (e && e[0] >= '0' && e[0] <= '3') ? e[0] - '0' : 0;
+    }
+    return g_rot_cfg;
+}
+
 cudaError_t launch_rotations(int kind, bool hi2lo, const RotLaunch & L, int max_ctas, cudaStream_t st) {
     if (L.ntasks <= 0) return cudaSuccess;
+    const int cfg = rotation_config();
     switch (kind) {
-        case SPH:  return hi2lo ? launch_cfg<SPH, true, 8, 8, 16>(L, max_ctas, st) : launch_cfg<SPH, false, 8, 8, 16>(L, max_ctas, st);
-        case TRI:  return hi2lo ? launch_cfg<TRI, true, 8, 8, 16>(L, max_ctas, st) : launch_cfg<TRI, false, 8, 8, 16>(L, max_ctas, st);
-        case DISK: return hi2lo ? launch_cfg<DISK, true, 8, 8, 16>(L, max_ctas, st) : launch_cfg<DISK, false, 8, 8, 16>(L, max_ctas, st);
+        case SPH:  return hi2lo ? launch_kind<SPH, true>(cfg, L, max_ctas, st) : launch_kind<SPH, false>(cfg, L, max_ctas, st);
+        case TRI:  return hi2lo ? launch_kind<TRI, true>(cfg, L, max_ctas, st) : launch_kind<TRI, false>(cfg, L, max_ctas, st);
+        case DISK: return hi2lo ? launch_kind<DISK, true>(cfg, L, max_ctas, st) : launch_kind<DISK, false>(cfg, L, max_ctas, st);
     }
     return cudaErrorInvalidValue;
 }
