@@ -316,6 +316,12 @@ def run_ours(args, rank, world, local_rank, dist):
         "hbm_peak_gbs": peaks.get("hbm_gbs"),
     }
     P.close()
+    extra = None
+    if not args.no_extra:
+        try:
+            extra = extra_workloads(args, torch, ft)
+        except Exception as exc:
+            extra = {"error": repr(exc)[:300]}
     cpu = None
     if world == 1 and not args.no_cpu:
         try:
@@ -341,6 +347,7 @@ def run_ours(args, rank, world, local_rank, dist):
                 "api": "ft_execute_sph2fourier + ft_execute_fourier2sph on pinned host arrays", "steps": e2e_steps},
         "gpu_launches": launches,
         "clocks": clocks,
+        "workloads": extra,
     }
     print(json.dumps(line))
 
@@ -361,6 +368,81 @@ def profile_case(n: int) -> None:
     print(json.dumps({"profile_case": f"sph n={n}", "max_abs": float(d.abs().max())}))
 
 
+def extra_workloads(args, torch, ft):
+    """Secondary workloads (reported beside the headline, same device timing rules)."""
+    import numpy as np
+    out = {}
+    st = torch.cuda.current_stream()
+    sp = st.cuda_stream
+
+    def timed(fn, steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        for _ in range(steps):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    # 64 FP64 sph fields, degrees drawn from {127, 255, 511, 1023, 2047}, one launch per stage,
+    # fwd+bwd captured in one CUDA graph
+    rng = np.random.default_rng(SEED)
+    degs = [int(d) + 1 for d in rng.choice([127, 255, 511, 1023, 2047], size=64)]
+    plans = {n: ft.plan_sph2fourier(n) for n in sorted(set(degs))}
+    P = [plans[n] for n in degs]
+    Ns = [p.n for p in P]
+    Ms = [p.M for p in P]
+    data = [torch.from_numpy(ft.sphrand(n, SEED + f).ravel(order="F").copy()).cuda() for f, n in enumerate(degs)]
+    ptrs = [d.data_ptr() for d in data]
+    side = torch.cuda.Stream()
+    side.wait_stream(st)
+    with torch.cuda.stream(side):
+        for _ in range(max(1, args.warmup)):
+            ft.execute_batched_dev(P, True, "N", ptrs, Ns, Ms, side.cuda_stream)
+            ft.execute_batched_dev(P, False, "N", ptrs, Ns, Ms, side.cuda_stream)
+    st.wait_stream(side)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        cs = torch.cuda.current_stream().cuda_stream
+        ft.execute_batched_dev(P, True, "N", ptrs, Ns, Ms, cs)
+        ft.execute_batched_dev(P, False, "N", ptrs, Ns, Ms, cs)
+    ms = timed(g.replay, max(3, args.steps // 2))
+    coeffs = sum(n * n for n in degs)
+    # same fields one plan call after another, eager, for comparison
+    ms_loop = timed(lambda: [ft.execute_dev(p, fw, "N", d.data_ptr(), p.n, p.M, sp)
+                             for fw in (True, False) for p, d in zip(P, data)], max(3, args.steps // 4))
+    out["batched_uneven_64"] = {"coeffs_per_s": coeffs / (ms * 1e-3), "ms_per_step": ms,
+                                "per_field_loop_coeffs_per_s": coeffs / (ms_loop * 1e-3),
+                                "degrees": "64 fields, U{127,255,511,1023,2047} seed 20261203",
+                                "graph": "fwd+bwd captured in one CUDA graph"}
+    del g, data
+    for p in plans.values():
+        p.close()
+    # sibling families at degree 2047, 8 fields per transform
+    for name, kind, params in (("tri_000", "tri", (0.0, 0.0, 0.0)), ("tri_hhh", "tri", (-0.5, -0.5, -0.5)),
+                               ("disk_00", "disk", (0.0, 0.0))):
+        n = 2048
+        planner = ft.plan_tri2cheb if kind == "tri" else ft.plan_disk2cxf
+        p = planner(n, *params)
+        M = p.M
+        fields = [torch.from_numpy(ft.rand_layout(kind, n, SEED + f).ravel(order="F").copy()).cuda() for f in range(8)]
+        fptr = [f.data_ptr() for f in fields]
+
+        def step():
+            ft.execute_batched_dev([p] * 8, True, "N", fptr, [n] * 8, [M] * 8, sp)
+            ft.execute_batched_dev([p] * 8, False, "N", fptr, [n] * 8, [M] * 8, sp)
+        for _ in range(max(1, args.warmup)):
+            step()
+        ms = timed(step, max(3, args.steps // 4))
+        per_field = n * (n + 1) // 2 if kind == "tri" else 2 * n * n - n
+        out[name] = {"coeffs_per_s": 8 * per_field / (ms * 1e-3), "ms_per_step": ms,
+                     "workload": f"{kind}{params}, degree {n - 1}, 8 fields, fwd+bwd 'N'"}
+        del fields
+        p.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -369,6 +451,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=4096)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the secondary workloads")
     ap.add_argument("--cpu-sample", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--profile-case", action="store_true",
                     help="run one plan and two forward transforms (for ncu), no timing")

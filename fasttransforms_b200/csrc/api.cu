@@ -426,6 +426,154 @@ void rotations_host(const ft_rotation_plan * RPc, bool hi2lo, double * A, int M,
     cudaFree(d);
 }
 
+// ---------------------------------------------------------------------------
+// batches: many fields in one launch per stage
+// ---------------------------------------------------------------------------
+struct BatchCtx {
+    RotTask * d_tasks = nullptr;
+    int ntasks = 0;
+    TrmmBatchClass * d_classes = nullptr;
+    TrmmTile * d_tiles[2] = {nullptr, nullptr};   // tile order for op(U) = U and U^T
+    int ntiles = 0;
+    double * d_work = nullptr;                     // one scratch matrix per field
+    std::vector<size_t> work_off;
+    int * d_counter = nullptr;
+};
+std::mutex g_batch_mu;
+std::map<std::string, BatchCtx *> g_batches;
+
+std::string batch_key(HarmonicPlan * const * H, const int * N, const int * M, int nf) {
+    std::string k;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    k += std::to_string(dev) + ":";
+    for (int f = 0; f < nf; f++) k += std::to_string((uintptr_t) H[f]) + "," + std::to_string(N[f]) + "," + std::to_string(M[f]) + ";";
+    return k;
+}
+
+BatchCtx * get_batch(HarmonicPlan * const * H, const int * N, const int * M, int nf) {
+    std::lock_guard<std::mutex> lk(g_batch_mu);
+    const std::string key = batch_key(H, N, M, nf);
+    auto it = g_batches.find(key);
+    if (it != g_batches.end()) return it->second;
+    BatchCtx * B = new BatchCtx();
+    const int kind = H[0]->kind;
+    // rotation tasks of every field, longest first
+    std::vector<std::pair<double, RotTask>> tv;
+    for (int f = 0; f < nf; f++)
+        for (const RotTask & t : build_tasks(kind, N[f], M[f], f))
+            tv.push_back({task_cost(kind, N[f], M[f], t.mbase), t});
+    std::stable_sort(tv.begin(), tv.end(), [](const auto & a, const auto & b) { return a.first > b.first; });
+    std::vector<RotTask> tasks;
+    for (auto & p : tv) tasks.push_back(p.second);
+    // trmm classes and tiles (four stride-4N classes per field), longest K first
+    std::vector<TrmmBatchClass> cls;
+    struct TK { long long klen; TrmmTile t; };
+    std::vector<TK> tN, tT;
+    const int bm = trmm_tile_rows(), bn = trmm_tile_cols();
+    for (int f = 0; f < nf; f++) {
+        const int n = N[f];
+        const int nc[4] = {(M[f] + 3) / 4, (M[f] + 2) / 4, (M[f] + 1) / 4, M[f] / 4};
+        for (int r = 0; r < 4; r++) {
+            if (nc[r] <= 0) continue;
+            const int c = (int) cls.size();
+            cls.push_back(TrmmBatchClass{f, (r == 0 || r == 3) ? 0 : 1, r, n, nc[r], 4LL * n});
+            for (int tm = 0; tm * bm < n; tm++)
+                for (int tn = 0; tn * bn < nc[r]; tn++) {
+                    tN.push_back({(long long) (n - tm * bm), TrmmTile{c, tm, tn}});
+                    tT.push_back({(long long) std::min(n, (tm + 1) * bm), TrmmTile{c, tm, tn}});
+                }
+        }
+    }
+    auto order = [](std::vector<TK> & v) {
+        std::stable_sort(v.begin(), v.end(), [](const TK & a, const TK & b) { return a.klen > b.klen; });
+        std::vector<TrmmTile> o;
+        for (auto & x : v) o.push_back(x.t);
+        return o;
+    };
+    const std::vector<TrmmTile> oN = order(tN), oT = order(tT);
+    size_t work = 0;
+    for (int f = 0; f < nf; f++) { B->work_off.push_back(work); work += (size_t) N[f] * M[f]; work = (work + 1) & ~(size_t) 1; }
+    bool ok = cuda_ok(cudaMalloc(&B->d_tasks, sizeof(RotTask) * std::max<size_t>(1, tasks.size())), "cudaMalloc(batch tasks)") &&
+              cuda_ok(cudaMalloc(&B->d_classes, sizeof(TrmmBatchClass) * std::max<size_t>(1, cls.size())), "cudaMalloc(batch classes)") &&
+              cuda_ok(cudaMalloc(&B->d_tiles[0], sizeof(TrmmTile) * std::max<size_t>(1, oN.size())), "cudaMalloc(batch tiles)") &&
+              cuda_ok(cudaMalloc(&B->d_tiles[1], sizeof(TrmmTile) * std::max<size_t>(1, oT.size())), "cudaMalloc(batch tiles)") &&
+              cuda_ok(cudaMalloc(&B->d_work, sizeof(double) * std::max<size_t>(1, work)), "cudaMalloc(batch workspace)") &&
+              cuda_ok(cudaMalloc(&B->d_counter, sizeof(int)), "cudaMalloc(batch counter)");
+    ok = ok && (tasks.empty() || cuda_ok(cudaMemcpy(B->d_tasks, tasks.data(), sizeof(RotTask) * tasks.size(), cudaMemcpyHostToDevice), "cudaMemcpy"));
+    ok = ok && (cls.empty() || cuda_ok(cudaMemcpy(B->d_classes, cls.data(), sizeof(TrmmBatchClass) * cls.size(), cudaMemcpyHostToDevice), "cudaMemcpy"));
+    ok = ok && (oN.empty() || cuda_ok(cudaMemcpy(B->d_tiles[0], oN.data(), sizeof(TrmmTile) * oN.size(), cudaMemcpyHostToDevice), "cudaMemcpy"));
+    ok = ok && (oT.empty() || cuda_ok(cudaMemcpy(B->d_tiles[1], oT.data(), sizeof(TrmmTile) * oT.size(), cudaMemcpyHostToDevice), "cudaMemcpy"));
+    if (!ok) {
+        cudaFree(B->d_tasks); cudaFree(B->d_classes); cudaFree(B->d_tiles[0]); cudaFree(B->d_tiles[1]);
+        cudaFree(B->d_work); cudaFree(B->d_counter);
+        delete B;
+        return nullptr;
+    }
+    B->ntasks = (int) tasks.size();
+    B->ntiles = (int) oN.size();
+    g_batches[key] = B;
+    return B;
+}
+
+// one launch per stage over up to kMaxFields fields of the sph or disk family
+int execute_batch_chunk(HarmonicPlan * const * H, bool forward, char TRANS, double * const * A, const int * N,
+                        const int * M, int nf, cudaStream_t st) {
+    BatchCtx * B = get_batch(H, N, M, nf);
+    if (!B) return t_status;
+    const bool tN = TRANS == 'N';
+    std::vector<double *> S(nf);
+    for (int f = 0; f < nf; f++) S[f] = B->d_work + B->work_off[f];
+    auto rot = [&](bool hi2lo, bool from_A) -> bool {
+        static thread_local RotLaunch L;
+        L.nfields = nf;
+        for (int f = 0; f < nf; f++) {
+            const double * in = from_A ? A[f] : S[f];
+            double * out = from_A ? S[f] : A[f];
+            L.fields[f] = RotField{in, out, H[f]->rp_arr[0]->d_sc, N[f], M[f], H[f]->kind, (long long) N[f]};
+            const int nc = untouched_cols(H[f]->kind, M[f]);
+            if (!cuda_ok(cudaMemcpy2DAsync(out, N[f] * sizeof(double), in, N[f] * sizeof(double), N[f] * sizeof(double), nc,
+                                           cudaMemcpyDeviceToDevice, st), "cudaMemcpy2DAsync")) return false;
+        }
+        L.tasks = B->d_tasks;
+        L.ntasks = B->ntasks;
+        L.counter = B->d_counter;
+        prof_begin(FAM_ROT, st);
+        const cudaError_t e = launch_rotations(H[0]->kind, hi2lo, L, 0, st);
+        prof_end(st);
+        return cuda_ok(e, "rotation kernel");
+    };
+    auto trmm = [&](bool inverse, bool trans, bool from_A) -> bool {
+        static thread_local TrmmBatch P;
+        bool vec = true;
+        for (int f = 0; f < nf; f++) {
+            double * const * U = inverse ? H[f]->dPinv : H[f]->dP;
+            P.U[f][0] = U[0];
+            P.U[f][1] = U[1];
+            P.in[f] = from_A ? A[f] : S[f];
+            P.out[f] = from_A ? S[f] : A[f];
+            vec = vec && (N[f] % 2 == 0) && ((reinterpret_cast<uintptr_t>(A[f]) & 15) == 0) && ((reinterpret_cast<uintptr_t>(S[f]) & 15) == 0);
+        }
+        P.classes = B->d_classes;
+        P.tiles = B->d_tiles[trans ? 1 : 0];
+        P.trans = trans;
+        prof_begin(FAM_TRMM, st);
+        const cudaError_t e = launch_trmm_batched(P, B->ntiles, vec, st);
+        prof_end(st);
+        return cuda_ok(e, "trmm kernel");
+    };
+    bool good;
+    if (forward && tN)  good = rot(true, true) && trmm(false, false, false);
+    else if (forward)   good = trmm(false, true, true) && rot(false, false);
+    else if (tN)        good = trmm(true, false, true) && rot(false, false);
+    else                good = rot(true, true) && trmm(true, true, false);
+    return good ? FT_B200_OK : t_status;
+}
+
+int execute_batch_tri_field(HarmonicPlan * H, bool forward, char TRANS, double * A, int N, int M, cudaStream_t st) {
+    return execute_dev_impl(H, forward, TRANS, A, N, M, st);
+}
+
 }  // namespace
 }  // namespace ftb
 
@@ -551,8 +699,26 @@ int ft_b200_execute_batched_dev(const ft_harmonic_plan * const * plans, int forw
                                 double * const * dA, const int * N, const int * M, int nfields, void * stream) {
     clear_error();
     if (!plans || !dA || !N || !M || nfields < 0) { set_error(FT_B200_EINVAL, "bad argument"); return t_status; }
+    if (TRANS != 'N' && TRANS != 'T') { set_error(FT_B200_EINVAL, "TRANS must be 'N' or 'T'"); return t_status; }
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    std::vector<HarmonicPlan *> H(nfields);
     for (int f = 0; f < nfields; f++) {
-        if (execute_dev_impl(as_plan(plans[f]), forward != 0, TRANS, dA[f], N[f], M[f], static_cast<cudaStream_t>(stream)) != FT_B200_OK)
+        H[f] = as_plan(plans[f]);
+        if (!H[f]) { set_error(FT_B200_EINVAL, "field " + std::to_string(f) + ": not a plan created by this library"); return t_status; }
+        if (!dA[f]) { set_error(FT_B200_EINVAL, "field " + std::to_string(f) + ": NULL matrix"); return t_status; }
+        if (!valid_MN(H[f]->kind, H[f]->n, N[f], M[f])) return t_status;
+        if (H[f]->kind != H[0]->kind) { set_error(FT_B200_EINVAL, "all fields of a batch must be of one family"); return t_status; }
+    }
+    if (nfields == 0) return FT_B200_OK;
+    if (H[0]->kind == TRI) {
+        // tri: the stage sequence depends on each plan's parameters; fields run one after another
+        for (int f = 0; f < nfields; f++)
+            if (execute_batch_tri_field(H[f], forward != 0, TRANS, dA[f], N[f], M[f], st) != FT_B200_OK) return t_status;
+        return FT_B200_OK;
+    }
+    for (int f0 = 0; f0 < nfields; f0 += kMaxFields) {
+        const int nf = std::min(kMaxFields, nfields - f0);
+        if (execute_batch_chunk(H.data() + f0, forward != 0, TRANS, dA + f0, N + f0, M + f0, nf, st) != FT_B200_OK)
             return t_status;
     }
     return FT_B200_OK;

@@ -111,6 +111,28 @@ struct TrmmLaunch {
     bool trans;                // op(U) = U^T
 };
 cudaError_t launch_trmm(const TrmmLaunch & L, cudaStream_t st);
+// Batched left multiplies (many fields, one launch).  A class is one column
+// class of one field: columns r, r + cstride, ... of that field's matrix.
+struct TrmmBatchClass {
+    int field;       // index into the pointer tables
+    int u;           // which of the field's two matrices
+    int r;           // first column of the class (column offset r * n)
+    int n;           // order of the triangular matrix (= rows)
+    int ncols;       // columns in the class
+    long long ld;    // column stride inside the class (4n for sph / disk, n for tri)
+};
+struct TrmmTile { int cls, tm, tn; };
+struct TrmmBatch {
+    const double * U[kMaxFields][2];
+    const double * in[kMaxFields];
+    double * out[kMaxFields];
+    const TrmmBatchClass * classes;   // device
+    const TrmmTile * tiles;           // device, longest K first
+    bool trans;
+};
+cudaError_t launch_trmm_batched(const TrmmBatch & P, int ntiles, bool vec16, cudaStream_t st);
+int trmm_tile_rows();
+int trmm_tile_cols();
 // Right multiply for tri: Out = In * op(U) (rows of In are independent).
 cudaError_t launch_trmm_right(const double * U, const double * in, double * out, int n, int nrows,
                               long long ld, bool trans, cudaStream_t st);

@@ -53,9 +53,9 @@ struct GemmParams {
     int mode;           // 0: left N (k >= i), 1: left T (k <= i), 2: right N (k <= j), 3: right T (k >= j)
 };
 
+// One 128 x 64 output tile of class C: rows [tm*BM, ...), columns [tn*BN, ...).
 template <bool A_MC, bool B_KC, bool VEC16>
-__global__ void __launch_bounds__(NTHREADS, 2)
-gemm_tri_kernel(const __grid_constant__ GemmParams P) {
+__device__ __forceinline__ void tri_tile(const GemmClass & C, const int n, const int mode, const int tm, const int tn) {
     constexpr int LDA = A_MC ? BM + 4 : BK + 4;   // [k][m] or [m][k]
     constexpr int LDB = B_KC ? BK + 4 : BN + 4;   // [n][k] or [k][n]
     constexpr int ASZ = A_MC ? BK * LDA : BM * LDA;
@@ -63,26 +63,13 @@ gemm_tri_kernel(const __grid_constant__ GemmParams P) {
     extern __shared__ double sm[];
     double * As = sm;
     double * Bs = sm + NSTAGE * ASZ;
-
-    // block -> (class, tile m, tile n); tiles with the most K work first
-    int bid = blockIdx.x;
-    const int per_class = P.tiles_m * P.tiles_n;
-    const int cl = bid / per_class;
-    bid -= cl * per_class;
-    int tm, tn;
-    if (P.mode == 0)      { tm = bid / P.tiles_n; tn = bid % P.tiles_n; }                 // small i: long K
-    else if (P.mode == 1) { tm = P.tiles_m - 1 - bid / P.tiles_n; tn = bid % P.tiles_n; } // large i: long K
-    else if (P.mode == 2) { tn = P.tiles_n - 1 - bid / P.tiles_m; tm = bid % P.tiles_m; } // large j
-    else                  { tn = bid / P.tiles_m; tm = bid % P.tiles_m; }                 // small j
-    const GemmClass & C = P.cls[cl];
     const int i0 = tm * BM, j0 = tn * BN;
     if (i0 >= C.mrows || j0 >= C.ncols) return;
-    const int n = P.n;
     int klo, khi;
-    if (P.mode == 0)      { klo = i0; khi = n; }
-    else if (P.mode == 1) { klo = 0; khi = min(i0 + BM, n); }
-    else if (P.mode == 2) { klo = 0; khi = min(j0 + BN, n); }
-    else                  { klo = j0; khi = n; }
+    if (mode == 0)      { klo = i0; khi = n; }
+    else if (mode == 1) { klo = 0; khi = min(i0 + BM, n); }
+    else if (mode == 2) { klo = 0; khi = min(j0 + BN, n); }
+    else                { klo = j0; khi = n; }
     klo = (klo / BK) * BK;
     const int nslab = (khi - klo + BK - 1) / BK;
 
@@ -204,6 +191,41 @@ gemm_tri_kernel(const __grid_constant__ GemmParams P) {
     }
 }
 
+template <bool A_MC, bool B_KC, bool VEC16>
+__global__ void __launch_bounds__(NTHREADS, 2)
+gemm_tri_kernel(const __grid_constant__ GemmParams P) {
+    // block -> (class, tile m, tile n); tiles with the most K work first
+    int bid = blockIdx.x;
+    const int per_class = P.tiles_m * P.tiles_n;
+    const int cl = bid / per_class;
+    bid -= cl * per_class;
+    int tm, tn;
+    if (P.mode == 0)      { tm = bid / P.tiles_n; tn = bid % P.tiles_n; }                 // small i: long K
+    else if (P.mode == 1) { tm = P.tiles_m - 1 - bid / P.tiles_n; tn = bid % P.tiles_n; } // large i: long K
+    else if (P.mode == 2) { tn = P.tiles_n - 1 - bid / P.tiles_m; tm = bid % P.tiles_m; } // large j
+    else                  { tn = bid / P.tiles_m; tm = bid % P.tiles_m; }                 // small j
+    tri_tile<A_MC, B_KC, VEC16>(P.cls[cl], P.n, P.mode, tm, tn);
+}
+
+// Batched left multiplies over many fields: the tile list (longest K first) and
+// the pointer-free class table live in device memory; pointers come by value.
+template <bool VEC16>
+__global__ void __launch_bounds__(NTHREADS, 2)
+gemm_tri_batched_kernel(const __grid_constant__ TrmmBatch P) {
+    const TrmmTile t = P.tiles[blockIdx.x];
+    const TrmmBatchClass c = P.classes[t.cls];
+    GemmClass C;
+    C.a = P.U[c.field][c.u];
+    C.b = P.in[c.field] + (long long) c.r * c.n;
+    C.c = P.out[c.field] + (long long) c.r * c.n;
+    C.a_ld = c.n;
+    C.b_ld = C.c_ld = c.ld;
+    C.mrows = c.n;
+    C.ncols = c.ncols;
+    if (P.trans) tri_tile<false, true, VEC16>(C, c.n, 1, t.tm, t.tn);
+    else         tri_tile<true, true, VEC16>(C, c.n, 0, t.tm, t.tn);
+}
+
 template <bool A_MC, bool B_KC>
 cudaError_t run_gemm(const GemmParams & P, bool vec16, cudaStream_t st) {
     constexpr int LDA = A_MC ? BM + 4 : BK + 4;
@@ -264,6 +286,31 @@ cudaError_t launch_trmm(const TrmmLaunch & L, cudaStream_t st) {
     P.mode = L.trans ? 1 : 0;
     return L.trans ? run_gemm<false, true>(P, vec, st) : run_gemm<true, true>(P, vec, st);
 }
+
+cudaError_t launch_trmm_batched(const TrmmBatch & P, int ntiles, bool vec16, cudaStream_t st) {
+    if (ntiles == 0) return cudaSuccess;
+    // both operand layouts of the left multiply share one shared-memory size bound
+    constexpr size_t shmN = sizeof(double) * NSTAGE * (BK * (BM + 4) + BN * (BK + 4));
+    constexpr size_t shmT = sizeof(double) * NSTAGE * (BM * (BK + 4) + BN * (BK + 4));
+    constexpr size_t shm = shmN > shmT ? shmN : shmT;
+    cudaError_t e;
+    if (vec16) {
+        auto k = gemm_tri_batched_kernel<true>;
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) shm);
+        if (e != cudaSuccess) return e;
+        k<<<ntiles, NTHREADS, shm, st>>>(P);
+    } else {
+        auto k = gemm_tri_batched_kernel<false>;
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) shm);
+        if (e != cudaSuccess) return e;
+        k<<<ntiles, NTHREADS, shm, st>>>(P);
+    }
+    count_launch();
+    return cudaGetLastError();
+}
+
+int trmm_tile_rows() { return BM; }
+int trmm_tile_cols() { return BN; }
 
 cudaError_t launch_trmm_right(const double * U, const double * in, double * out, int n, int nrows,
                               long long ld, bool trans, cudaStream_t st) {
