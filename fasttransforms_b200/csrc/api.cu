@@ -429,15 +429,19 @@ void rotations_host(const ft_rotation_plan * RPc, bool hi2lo, double * A, int M,
 // ---------------------------------------------------------------------------
 // batches: many fields in one launch per stage
 // ---------------------------------------------------------------------------
+struct TrmmSet {
+    TrmmBatchClass * d_classes = nullptr;
+    TrmmTile * d_tiles[4] = {nullptr, nullptr, nullptr, nullptr};   // tile order per multiply mode
+    int ntiles = 0;
+};
 struct BatchCtx {
     RotTask * d_tasks = nullptr;
     int ntasks = 0;
-    TrmmBatchClass * d_classes = nullptr;
-    TrmmTile * d_tiles[2] = {nullptr, nullptr};   // tile order for op(U) = U and U^T
-    int ntiles = 0;
+    TrmmSet left, right;                           // right: tri only
     double * d_work = nullptr;                     // one scratch matrix per field
     std::vector<size_t> work_off;
     int * d_counter = nullptr;
+    std::vector<void *> allocs;
 };
 std::mutex g_batch_mu;
 std::map<std::string, BatchCtx *> g_batches;
@@ -449,6 +453,39 @@ std::string batch_key(HarmonicPlan * const * H, const int * N, const int * M, in
     k += std::to_string(dev) + ":";
     for (int f = 0; f < nf; f++) k += std::to_string((uintptr_t) H[f]) + "," + std::to_string(N[f]) + "," + std::to_string(M[f]) + ";";
     return k;
+}
+
+template <class T>
+bool upload(BatchCtx * B, const std::vector<T> & v, T ** d) {
+    if (!cuda_ok(cudaMalloc(d, sizeof(T) * std::max<size_t>(1, v.size())), "cudaMalloc(batch table)")) return false;
+    B->allocs.push_back(*d);
+    return v.empty() || cuda_ok(cudaMemcpy(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice), "cudaMemcpy(batch table)");
+}
+
+// tiles of every class, ordered longest K first for each multiply mode
+bool build_trmm_set(BatchCtx * B, const std::vector<TrmmBatchClass> & cls, TrmmSet * T) {
+    const int bm = trmm_tile_rows(), bn = trmm_tile_cols();
+    std::vector<std::pair<long long, TrmmTile>> t[4];
+    for (int c = 0; c < (int) cls.size(); c++) {
+        const TrmmBatchClass & k = cls[c];
+        for (int tm = 0; tm * bm < k.mrows; tm++)
+            for (int tn = 0; tn * bn < k.ncols; tn++) {
+                const TrmmTile x{c, tm, tn};
+                t[0].push_back({(long long) (k.n - tm * bm), x});
+                t[1].push_back({(long long) std::min(k.n, (tm + 1) * bm), x});
+                t[2].push_back({(long long) std::min(k.n, (tn + 1) * bn), x});
+                t[3].push_back({(long long) (k.n - tn * bn), x});
+            }
+    }
+    if (!upload(B, cls, &T->d_classes)) return false;
+    for (int m = 0; m < 4; m++) {
+        std::stable_sort(t[m].begin(), t[m].end(), [](const auto & a, const auto & b) { return a.first > b.first; });
+        std::vector<TrmmTile> o;
+        for (auto & x : t[m]) o.push_back(x.second);
+        if (!upload(B, o, &T->d_tiles[m])) return false;
+        T->ntiles = (int) o.size();
+    }
+    return true;
 }
 
 BatchCtx * get_batch(HarmonicPlan * const * H, const int * N, const int * M, int nf) {
@@ -466,84 +503,68 @@ BatchCtx * get_batch(HarmonicPlan * const * H, const int * N, const int * M, int
     std::stable_sort(tv.begin(), tv.end(), [](const auto & a, const auto & b) { return a.first > b.first; });
     std::vector<RotTask> tasks;
     for (auto & p : tv) tasks.push_back(p.second);
-    // trmm classes and tiles (four stride-4N classes per field), longest K first
-    std::vector<TrmmBatchClass> cls;
-    struct TK { long long klen; TrmmTile t; };
-    std::vector<TK> tN, tT;
-    const int bm = trmm_tile_rows(), bn = trmm_tile_cols();
+    std::vector<TrmmBatchClass> left, right;
     for (int f = 0; f < nf; f++) {
         const int n = N[f];
-        const int nc[4] = {(M[f] + 3) / 4, (M[f] + 2) / 4, (M[f] + 1) / 4, M[f] / 4};
-        for (int r = 0; r < 4; r++) {
-            if (nc[r] <= 0) continue;
-            const int c = (int) cls.size();
-            cls.push_back(TrmmBatchClass{f, (r == 0 || r == 3) ? 0 : 1, r, n, nc[r], 4LL * n});
-            for (int tm = 0; tm * bm < n; tm++)
-                for (int tn = 0; tn * bn < nc[r]; tn++) {
-                    tN.push_back({(long long) (n - tm * bm), TrmmTile{c, tm, tn}});
-                    tT.push_back({(long long) std::min(n, (tm + 1) * bm), TrmmTile{c, tm, tn}});
-                }
+        if (kind == TRI) {   // one class per field: left with U0, right with U1 (src/drivers.c:921-957)
+            left.push_back(TrmmBatchClass{f, 0, 0, n, n, M[f], (long long) n});
+            right.push_back(TrmmBatchClass{f, 1, 0, n, n, M[f], (long long) n});
+        } else {             // four stride-4N classes per field (src/drivers.c:836-839)
+            const int nc[4] = {(M[f] + 3) / 4, (M[f] + 2) / 4, (M[f] + 1) / 4, M[f] / 4};
+            for (int r = 0; r < 4; r++)
+                if (nc[r] > 0) left.push_back(TrmmBatchClass{f, (r == 0 || r == 3) ? 0 : 1, r, n, n, nc[r], 4LL * n});
         }
     }
-    auto order = [](std::vector<TK> & v) {
-        std::stable_sort(v.begin(), v.end(), [](const TK & a, const TK & b) { return a.klen > b.klen; });
-        std::vector<TrmmTile> o;
-        for (auto & x : v) o.push_back(x.t);
-        return o;
-    };
-    const std::vector<TrmmTile> oN = order(tN), oT = order(tT);
     size_t work = 0;
     for (int f = 0; f < nf; f++) { B->work_off.push_back(work); work += (size_t) N[f] * M[f]; work = (work + 1) & ~(size_t) 1; }
-    bool ok = cuda_ok(cudaMalloc(&B->d_tasks, sizeof(RotTask) * std::max<size_t>(1, tasks.size())), "cudaMalloc(batch tasks)") &&
-              cuda_ok(cudaMalloc(&B->d_classes, sizeof(TrmmBatchClass) * std::max<size_t>(1, cls.size())), "cudaMalloc(batch classes)") &&
-              cuda_ok(cudaMalloc(&B->d_tiles[0], sizeof(TrmmTile) * std::max<size_t>(1, oN.size())), "cudaMalloc(batch tiles)") &&
-              cuda_ok(cudaMalloc(&B->d_tiles[1], sizeof(TrmmTile) * std::max<size_t>(1, oT.size())), "cudaMalloc(batch tiles)") &&
+    bool ok = upload(B, tasks, &B->d_tasks) && build_trmm_set(B, left, &B->left) &&
+              (kind != TRI || build_trmm_set(B, right, &B->right)) &&
               cuda_ok(cudaMalloc(&B->d_work, sizeof(double) * std::max<size_t>(1, work)), "cudaMalloc(batch workspace)") &&
               cuda_ok(cudaMalloc(&B->d_counter, sizeof(int)), "cudaMalloc(batch counter)");
-    ok = ok && (tasks.empty() || cuda_ok(cudaMemcpy(B->d_tasks, tasks.data(), sizeof(RotTask) * tasks.size(), cudaMemcpyHostToDevice), "cudaMemcpy"));
-    ok = ok && (cls.empty() || cuda_ok(cudaMemcpy(B->d_classes, cls.data(), sizeof(TrmmBatchClass) * cls.size(), cudaMemcpyHostToDevice), "cudaMemcpy"));
-    ok = ok && (oN.empty() || cuda_ok(cudaMemcpy(B->d_tiles[0], oN.data(), sizeof(TrmmTile) * oN.size(), cudaMemcpyHostToDevice), "cudaMemcpy"));
-    ok = ok && (oT.empty() || cuda_ok(cudaMemcpy(B->d_tiles[1], oT.data(), sizeof(TrmmTile) * oT.size(), cudaMemcpyHostToDevice), "cudaMemcpy"));
+    if (B->d_work) B->allocs.push_back(B->d_work);
+    if (B->d_counter) B->allocs.push_back(B->d_counter);
     if (!ok) {
-        cudaFree(B->d_tasks); cudaFree(B->d_classes); cudaFree(B->d_tiles[0]); cudaFree(B->d_tiles[1]);
-        cudaFree(B->d_work); cudaFree(B->d_counter);
+        for (void * p : B->allocs) cudaFree(p);
         delete B;
         return nullptr;
     }
     B->ntasks = (int) tasks.size();
-    B->ntiles = (int) oN.size();
     g_batches[key] = B;
     return B;
 }
 
-// one launch per stage over up to kMaxFields fields of the sph or disk family
+// one launch per stage over up to kMaxFields fields of one family
 int execute_batch_chunk(HarmonicPlan * const * H, bool forward, char TRANS, double * const * A, const int * N,
                         const int * M, int nf, cudaStream_t st) {
     BatchCtx * B = get_batch(H, N, M, nf);
     if (!B) return t_status;
+    const int kind = H[0]->kind;
     const bool tN = TRANS == 'N';
     std::vector<double *> S(nf);
     for (int f = 0; f < nf; f++) S[f] = B->d_work + B->work_off[f];
-    auto rot = [&](bool hi2lo, bool from_A) -> bool {
+    // cur_is_A: which buffer holds the current data (all fields move together)
+    auto rot = [&](bool hi2lo, bool from_A, bool to_A) -> bool {
         static thread_local RotLaunch L;
         L.nfields = nf;
         for (int f = 0; f < nf; f++) {
             const double * in = from_A ? A[f] : S[f];
-            double * out = from_A ? S[f] : A[f];
+            double * out = to_A ? A[f] : S[f];
             L.fields[f] = RotField{in, out, H[f]->rp_arr[0]->d_sc, N[f], M[f], H[f]->kind, (long long) N[f]};
-            const int nc = untouched_cols(H[f]->kind, M[f]);
-            if (!cuda_ok(cudaMemcpy2DAsync(out, N[f] * sizeof(double), in, N[f] * sizeof(double), N[f] * sizeof(double), nc,
-                                           cudaMemcpyDeviceToDevice, st), "cudaMemcpy2DAsync")) return false;
+            if (in != out) {
+                const int nc = untouched_cols(H[f]->kind, M[f]);
+                if (!cuda_ok(cudaMemcpy2DAsync(out, N[f] * sizeof(double), in, N[f] * sizeof(double), N[f] * sizeof(double), nc,
+                                               cudaMemcpyDeviceToDevice, st), "cudaMemcpy2DAsync")) return false;
+            }
         }
         L.tasks = B->d_tasks;
         L.ntasks = B->ntasks;
         L.counter = B->d_counter;
         prof_begin(FAM_ROT, st);
-        const cudaError_t e = launch_rotations(H[0]->kind, hi2lo, L, 0, st);
+        const cudaError_t e = launch_rotations(kind, hi2lo, L, 0, st);
         prof_end(st);
         return cuda_ok(e, "rotation kernel");
     };
-    auto trmm = [&](bool inverse, bool trans, bool from_A) -> bool {
+    auto trmm = [&](const TrmmSet & T, int mode, bool inverse, bool from_A) -> bool {
         static thread_local TrmmBatch P;
         bool vec = true;
         for (int f = 0; f < nf; f++) {
@@ -554,24 +575,62 @@ int execute_batch_chunk(HarmonicPlan * const * H, bool forward, char TRANS, doub
             P.out[f] = from_A ? S[f] : A[f];
             vec = vec && (N[f] % 2 == 0) && ((reinterpret_cast<uintptr_t>(A[f]) & 15) == 0) && ((reinterpret_cast<uintptr_t>(S[f]) & 15) == 0);
         }
-        P.classes = B->d_classes;
-        P.tiles = B->d_tiles[trans ? 1 : 0];
-        P.trans = trans;
+        P.classes = T.d_classes;
+        P.tiles = T.d_tiles[mode];
         prof_begin(FAM_TRMM, st);
-        const cudaError_t e = launch_trmm_batched(P, B->ntiles, vec, st);
+        const cudaError_t e = launch_trmm_batched(P, T.ntiles, vec, mode, st);
         prof_end(st);
         return cuda_ok(e, "trmm kernel");
     };
-    bool good;
-    if (forward && tN)  good = rot(true, true) && trmm(false, false, false);
-    else if (forward)   good = trmm(false, true, true) && rot(false, false);
-    else if (tN)        good = trmm(true, false, true) && rot(false, false);
-    else                good = rot(true, true) && trmm(true, true, false);
-    return good ? FT_B200_OK : t_status;
+    auto norm = [&](bool on_A, bool transposed) -> bool {
+        for (int f = 0; f < nf; f++) {
+            prof_begin(FAM_OTHER, st);
+            const cudaError_t e = launch_cheb_normalize(on_A ? A[f] : S[f], N[f], M[f], N[f], transposed, st);
+            prof_end(st);
+            if (!cuda_ok(e, "normalize")) return false;
+        }
+        return true;
+    };
+    if (kind != TRI) {   // src/drivers.c:833-865, 989-1021
+        bool good;
+        if (forward && tN)  good = rot(true, true, false) && trmm(B->left, 0, false, false);
+        else if (forward)   good = trmm(B->left, 1, false, true) && rot(false, false, true);
+        else if (tN)        good = trmm(B->left, 0, true, true) && rot(false, false, true);
+        else                good = rot(true, true, false) && trmm(B->left, 1, true, false);
+        return good ? FT_B200_OK : t_status;
+    }
+    // tri (src/drivers.c:921-957); all plans share the left / right flags
+    const double a = H[0]->pub.alpha, b = H[0]->pub.beta, g = H[0]->pub.gamma;
+    const bool left = (b + g != -1.5) || (a != -0.5);
+    const bool right = (g != -0.5) || (b != -0.5);
+    const int k = (left ? 1 : 0) + (right ? 1 : 0);
+    bool cur_A = true;
+    if ((forward && tN) || (!forward && !tN)) {
+        const bool rot_to_A = (k % 2) == 0;
+        if (!rot(true, true, rot_to_A)) return t_status;
+        cur_A = rot_to_A;
+        const int lm = forward ? 0 : 1, rm = forward ? 3 : 2;
+        if (left) { if (!trmm(B->left, lm, !forward, cur_A)) return t_status; cur_A = !cur_A; }
+        if (right) { if (!trmm(B->right, rm, !forward, cur_A)) return t_status; cur_A = !cur_A; }
+        if (!norm(cur_A, !forward)) return t_status;
+    } else {
+        if (!norm(true, !forward)) return t_status;
+        const int rm = forward ? 2 : 3, lm = forward ? 1 : 0;
+        if (right) { if (!trmm(B->right, rm, !forward, cur_A)) return t_status; cur_A = !cur_A; }
+        if (left) { if (!trmm(B->left, lm, !forward, cur_A)) return t_status; cur_A = !cur_A; }
+        if (!rot(false, cur_A, true)) return t_status;
+    }
+    return FT_B200_OK;
 }
 
-int execute_batch_tri_field(HarmonicPlan * H, bool forward, char TRANS, double * A, int N, int M, cudaStream_t st) {
-    return execute_dev_impl(H, forward, TRANS, A, N, M, st);
+bool same_tri_flags(HarmonicPlan * const * H, int nf) {
+    auto flags = [](HarmonicPlan * h) {
+        const double a = h->pub.alpha, b = h->pub.beta, g = h->pub.gamma;
+        return ((b + g != -1.5) || (a != -0.5) ? 1 : 0) + ((g != -0.5) || (b != -0.5) ? 2 : 0);
+    };
+    for (int f = 1; f < nf; f++)
+        if (flags(H[f]) != flags(H[0])) return false;
+    return true;
 }
 
 }  // namespace
@@ -710,10 +769,10 @@ int ft_b200_execute_batched_dev(const ft_harmonic_plan * const * plans, int forw
         if (H[f]->kind != H[0]->kind) { set_error(FT_B200_EINVAL, "all fields of a batch must be of one family"); return t_status; }
     }
     if (nfields == 0) return FT_B200_OK;
-    if (H[0]->kind == TRI) {
-        // tri: the stage sequence depends on each plan's parameters; fields run one after another
+    if (H[0]->kind == TRI && !same_tri_flags(H.data(), nfields)) {
+        // tri plans whose parameters call for different multiplies run one after another
         for (int f = 0; f < nfields; f++)
-            if (execute_batch_tri_field(H[f], forward != 0, TRANS, dA[f], N[f], M[f], st) != FT_B200_OK) return t_status;
+            if (execute_dev_impl(H[f], forward != 0, TRANS, dA[f], N[f], M[f], st) != FT_B200_OK) return t_status;
         return FT_B200_OK;
     }
     for (int f0 = 0; f0 < nfields; f0 += kMaxFields) {

@@ -117,8 +117,9 @@ struct TrmmBatchClass {
     int field;       // index into the pointer tables
     int u;           // which of the field's two matrices
     int r;           // first column of the class (column offset r * n)
-    int n;           // order of the triangular matrix (= rows)
-    int ncols;       // columns in the class
+    int n;           // order of the triangular matrix
+    int mrows;       // rows of the product
+    int ncols;       // columns of the product
     long long ld;    // column stride inside the class (4n for sph / disk, n for tri)
 };
 struct TrmmTile { int cls, tm, tn; };
@@ -128,9 +129,9 @@ struct TrmmBatch {
     double * out[kMaxFields];
     const TrmmBatchClass * classes;   // device
     const TrmmTile * tiles;           // device, longest K first
-    bool trans;
 };
-cudaError_t launch_trmm_batched(const TrmmBatch & P, int ntiles, bool vec16, cudaStream_t st);
+// mode 0 / 1: Out = U In / U^T In; mode 2 / 3: Out = In U / In U^T
+cudaError_t launch_trmm_batched(const TrmmBatch & P, int ntiles, bool vec16, int mode, cudaStream_t st);
 int trmm_tile_rows();
 int trmm_tile_cols();
 // Right multiply for tri: Out = In * op(U) (rows of In are independent).

@@ -207,23 +207,51 @@ gemm_tri_kernel(const __grid_constant__ GemmParams P) {
     tri_tile<A_MC, B_KC, VEC16>(P.cls[cl], P.n, P.mode, tm, tn);
 }
 
-// Batched left multiplies over many fields: the tile list (longest K first) and
-// the pointer-free class table live in device memory; pointers come by value.
-template <bool VEC16>
+// Batched multiplies over many fields: the tile list (longest K first) and the
+// pointer-free class table live in device memory; pointers come by value.
+// MODE 0/1: left, op(U) = U / U^T; MODE 2/3: right, op(U) = U / U^T.
+template <int MODE, bool VEC16>
 __global__ void __launch_bounds__(NTHREADS, 2)
 gemm_tri_batched_kernel(const __grid_constant__ TrmmBatch P) {
     const TrmmTile t = P.tiles[blockIdx.x];
     const TrmmBatchClass c = P.classes[t.cls];
     GemmClass C;
-    C.a = P.U[c.field][c.u];
-    C.b = P.in[c.field] + (long long) c.r * c.n;
+    const double * X = P.in[c.field] + (long long) c.r * c.n;
+    const double * U = P.U[c.field][c.u];
     C.c = P.out[c.field] + (long long) c.r * c.n;
-    C.a_ld = c.n;
-    C.b_ld = C.c_ld = c.ld;
-    C.mrows = c.n;
+    C.c_ld = c.ld;
+    C.mrows = c.mrows;
     C.ncols = c.ncols;
-    if (P.trans) tri_tile<false, true, VEC16>(C, c.n, 1, t.tm, t.tn);
-    else         tri_tile<true, true, VEC16>(C, c.n, 0, t.tm, t.tn);
+    if (MODE < 2) { C.a = U; C.a_ld = c.n; C.b = X; C.b_ld = c.ld; }
+    else          { C.a = X; C.a_ld = c.ld; C.b = U; C.b_ld = c.n; }
+    constexpr bool A_MC = MODE != 1;
+    constexpr bool B_KC = MODE != 3;
+    tri_tile<A_MC, B_KC, VEC16>(C, c.n, MODE, t.tm, t.tn);
+}
+
+template <int MODE>
+cudaError_t run_batched(const TrmmBatch & P, int ntiles, bool vec16, cudaStream_t st) {
+    constexpr bool A_MC = MODE != 1;
+    constexpr bool B_KC = MODE != 3;
+    constexpr int LDA = A_MC ? BM + 4 : BK + 4;
+    constexpr int LDB = B_KC ? BK + 4 : BN + 4;
+    constexpr int ASZ = A_MC ? BK * LDA : BM * LDA;
+    constexpr int BSZ = B_KC ? BN * LDB : BK * LDB;
+    const size_t shm = sizeof(double) * NSTAGE * (ASZ + BSZ);
+    cudaError_t e;
+    if (vec16) {
+        auto k = gemm_tri_batched_kernel<MODE, true>;
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) shm);
+        if (e != cudaSuccess) return e;
+        k<<<ntiles, NTHREADS, shm, st>>>(P);
+    } else {
+        auto k = gemm_tri_batched_kernel<MODE, false>;
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) shm);
+        if (e != cudaSuccess) return e;
+        k<<<ntiles, NTHREADS, shm, st>>>(P);
+    }
+    count_launch();
+    return cudaGetLastError();
 }
 
 template <bool A_MC, bool B_KC>
@@ -287,26 +315,15 @@ cudaError_t launch_trmm(const TrmmLaunch & L, cudaStream_t st) {
     return L.trans ? run_gemm<false, true>(P, vec, st) : run_gemm<true, true>(P, vec, st);
 }
 
-cudaError_t launch_trmm_batched(const TrmmBatch & P, int ntiles, bool vec16, cudaStream_t st) {
+cudaError_t launch_trmm_batched(const TrmmBatch & P, int ntiles, bool vec16, int mode, cudaStream_t st) {
     if (ntiles == 0) return cudaSuccess;
-    // both operand layouts of the left multiply share one shared-memory size bound
-    constexpr size_t shmN = sizeof(double) * NSTAGE * (BK * (BM + 4) + BN * (BK + 4));
-    constexpr size_t shmT = sizeof(double) * NSTAGE * (BM * (BK + 4) + BN * (BK + 4));
-    constexpr size_t shm = shmN > shmT ? shmN : shmT;
-    cudaError_t e;
-    if (vec16) {
-        auto k = gemm_tri_batched_kernel<true>;
-        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) shm);
-        if (e != cudaSuccess) return e;
-        k<<<ntiles, NTHREADS, shm, st>>>(P);
-    } else {
-        auto k = gemm_tri_batched_kernel<false>;
-        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) shm);
-        if (e != cudaSuccess) return e;
-        k<<<ntiles, NTHREADS, shm, st>>>(P);
+    switch (mode) {
+        case 0: return run_batched<0>(P, ntiles, vec16, st);
+        case 1: return run_batched<1>(P, ntiles, vec16, st);
+        case 2: return run_batched<2>(P, ntiles, vec16, st);
+        case 3: return run_batched<3>(P, ntiles, vec16, st);
     }
-    count_launch();
-    return cudaGetLastError();
+    return cudaErrorInvalidValue;
 }
 
 int trmm_tile_rows() { return BM; }

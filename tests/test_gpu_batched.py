@@ -38,6 +38,8 @@ def make_fields(ft, torch, kind, degrees, params, seed0=500):
     ("sph", (), [15, 64, 33, 127, 64, 8, 2, 3]),
     ("disk", (0.0, 0.0), [9, 40, 40, 17]),
     ("tri", (0.0, 0.0, 0.0), [12, 30, 30]),
+    ("tri", (-0.5, -0.5, -0.5), [7, 64, 33]),
+    ("tri", (0.5, 1.0, -0.25), [16, 16]),
 ])
 def test_batched_equals_per_field(env, kind, params, degrees):
     ft, torch, O = env
@@ -105,4 +107,23 @@ def test_batched_fwd_bwd_in_cuda_graph(env):
         assert torch.equal(w, e)
     del g
     for p in plans.values():
+        p.close()
+
+
+def test_batched_tri_mixed_parameters(env):
+    """tri plans whose parameters call for different multiplies in one batch."""
+    ft, torch, O = env
+    st = torch.cuda.current_stream().cuda_stream
+    specs = [((0.0, 0.0, 0.0), 20), ((-0.5, -0.5, -0.5), 24), ((0.0, 0.0, 0.0), 9)]
+    plans = [ft.plan_tri2cheb(n, *p) for p, n in specs]
+    As = [ft.trirand(n, 7 + i) for i, (_, n) in enumerate(specs)]
+    ts = [torch.from_numpy(A.ravel(order="F").copy()).cuda() for A in As]
+    ft.execute_batched_dev(plans, True, "N", [t.data_ptr() for t in ts], [p.n for p in plans], [p.M for p in plans], st)
+    for (params, n), A, t in zip(specs, As, ts):
+        ref = A.copy(order="F")
+        PO = O.plan("tri", n, *params)
+        O.execute(PO, True, "N", ref)
+        O.destroy(PO)
+        assert rel2(t.cpu().numpy().reshape(A.shape, order="F"), ref) <= 1e-14
+    for p in plans:
         p.close()
