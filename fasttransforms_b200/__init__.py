@@ -29,7 +29,7 @@ __all__ = [
     "plan_rotsphere", "plan_rottriangle", "plan_rotdisk",
     "execute_sph_hi2lo", "execute_sph_lo2hi", "execute_tri_hi2lo", "execute_tri_lo2hi",
     "execute_disk_hi2lo", "execute_disk_lo2hi",
-    "execute_dev", "execute_noalloc_dev", "NOALLOC_MAX_ELEMS", "execute_batched_dev", "rotations_dev", "kernel_launches", "profile", "profile_read",
+    "execute_dev", "execute_shared_dev", "FP64", "FP64_BLOCKED", "execute_noalloc_dev", "NOALLOC_MAX_ELEMS", "execute_batched_dev", "rotations_dev", "kernel_launches", "profile", "profile_read",
     "layout_cols", "rand_layout", "sphrand", "trirand", "diskrand",
     "SPH", "TRI", "DISK",
 ]
@@ -66,6 +66,7 @@ def _load() -> C.CDLL:
         "ft_b200_execute_batched_dev": (i, [C.POINTER(vp), i, ch, C.POINTER(vp), C.POINTER(i), C.POINTER(i), i, vp]),
         "ft_b200_plan_kind": (i, [vp]), "ft_b200_plan_device": (i, [vp]),
         "ft_b200_execute_noalloc_dev": (i, [vp, i, ch, vp, i, i, vp]),
+        "ft_b200_execute_shared_dev": (i, [vp, i, ch, C.POINTER(vp), i, i, vp]),
         "ft_b200_profile": (i, [i]), "ft_b200_profile_read": (i, [i, C.POINTER(C.c_double), C.POINTER(i)]),
     }
     for name in ("sph2fourier", "fourier2sph", "tri2cheb", "cheb2tri", "disk2cxf", "cxf2disk"):
@@ -247,6 +248,24 @@ def execute_noalloc_dev(P: HarmonicPlan, forward: bool, trans: str, ptr: int, N:
     overlap on the GPU race and must be serialised by the caller.
     """
     st = lib.ft_b200_execute_noalloc_dev(P.ptr, 1 if forward else 0, trans.encode(), C.c_void_p(ptr), N, M, C.c_void_p(stream))
+    if st != 0:
+        _check()
+
+
+FP64, FP64_BLOCKED = 0, 1
+
+
+def execute_shared_dev(P: HarmonicPlan, forward: bool, trans: str, ptrs: Sequence[int], precision: int = FP64,
+                       stream: int = 0) -> None:
+    """Transform every field of ``ptrs`` (device matrices sharing plan ``P``) in one call.
+
+    precision FP64: the direct sweeps; FP64_BLOCKED (sph only): whole blocks of
+    32 sweeps applied as pre-multiplied 64 x 64 tile matrices on the FP64 tensor
+    pipe (rounds differently from the direct sweeps, ~1e-14 relative).
+    """
+    nf = len(ptrs)
+    aa = (C.c_void_p * nf)(*ptrs)
+    st = lib.ft_b200_execute_shared_dev(P.ptr, 1 if forward else 0, trans.encode(), aa, nf, precision, C.c_void_p(stream))
     if st != 0:
         _check()
 

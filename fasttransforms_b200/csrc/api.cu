@@ -169,7 +169,7 @@ bool rotations(ft_rotation_plan * RP, bool hi2lo, const double * in, double * ou
     if (ntasks == 0) return true;
     static thread_local RotLaunch L;   // large parameter block; kept off the stack
     L.nfields = 1;
-    L.fields[0] = RotField{in, out, RP->d_sc, RP->n, M, RP->kind, lda};
+    L.fields[0] = RotField{in, out, RP->d_sc, RP->n, M, RP->kind, lda, 0};
     L.tasks = d_tasks;
     L.ntasks = ntasks;
     L.counter = RP->d_counter;
@@ -442,6 +442,8 @@ struct BatchCtx {
     std::vector<size_t> work_off;
     int * d_counter = nullptr;
     std::vector<void *> allocs;
+    BlkTaskList blk_tasks;                         // blocked-sweep tasks (built on first blocked call)
+    bool blk_ready = false;
 };
 std::mutex g_batch_mu;
 std::map<std::string, BatchCtx *> g_batches;
@@ -535,9 +537,15 @@ BatchCtx * get_batch(HarmonicPlan * const * H, const int * N, const int * M, int
 
 // one launch per stage over up to kMaxFields fields of one family
 int execute_batch_chunk(HarmonicPlan * const * H, bool forward, char TRANS, double * const * A, const int * N,
-                        const int * M, int nf, cudaStream_t st) {
+                        const int * M, int nf, cudaStream_t st, bool blocked = false) {
     BatchCtx * B = get_batch(H, N, M, nf);
     if (!B) return t_status;
+    const int blk = blocked ? blocked_block_size() : 0;
+    if (blocked && !B->blk_ready) {
+        if (!blocked_tasks(H[0]->blocked, nf, N[0], M[0], &B->blk_tasks)) return t_status;
+        if (B->blk_tasks.d_tasks) B->allocs.push_back(B->blk_tasks.d_tasks);
+        B->blk_ready = true;
+    }
     const int kind = H[0]->kind;
     const bool tN = TRANS == 'N';
     std::vector<double *> S(nf);
@@ -549,7 +557,7 @@ int execute_batch_chunk(HarmonicPlan * const * H, bool forward, char TRANS, doub
         for (int f = 0; f < nf; f++) {
             const double * in = from_A ? A[f] : S[f];
             double * out = to_A ? A[f] : S[f];
-            L.fields[f] = RotField{in, out, H[f]->rp_arr[0]->d_sc, N[f], M[f], H[f]->kind, (long long) N[f]};
+            L.fields[f] = RotField{in, out, H[f]->rp_arr[0]->d_sc, N[f], M[f], H[f]->kind, (long long) N[f], blk};
             if (in != out) {
                 const int nc = untouched_cols(H[f]->kind, M[f]);
                 if (!cuda_ok(cudaMemcpy2DAsync(out, N[f] * sizeof(double), in, N[f] * sizeof(double), N[f] * sizeof(double), nc,
@@ -591,12 +599,20 @@ int execute_batch_chunk(HarmonicPlan * const * H, bool forward, char TRANS, doub
         }
         return true;
     };
+    // blocked products of the whole blocks, in place on the scratch matrices
+    auto blocks = [&](bool hi2lo) -> bool {
+        if (!blocked) return true;
+        prof_begin(FAM_ROT, st);
+        const cudaError_t e = launch_blocked(H[0]->blocked, hi2lo, S.data(), nf, N[0], M[0], B->blk_tasks, B->d_counter, st);
+        prof_end(st);
+        return cuda_ok(e, "blocked kernel");
+    };
     if (kind != TRI) {   // src/drivers.c:833-865, 989-1021
         bool good;
-        if (forward && tN)  good = rot(true, true, false) && trmm(B->left, 0, false, false);
-        else if (forward)   good = trmm(B->left, 1, false, true) && rot(false, false, true);
-        else if (tN)        good = trmm(B->left, 0, true, true) && rot(false, false, true);
-        else                good = rot(true, true, false) && trmm(B->left, 1, true, false);
+        if (forward && tN)  good = rot(true, true, false) && blocks(true) && trmm(B->left, 0, false, false);
+        else if (forward)   good = trmm(B->left, 1, false, true) && blocks(false) && rot(false, false, true);
+        else if (tN)        good = trmm(B->left, 0, true, true) && blocks(false) && rot(false, false, true);
+        else                good = rot(true, true, false) && blocks(true) && trmm(B->left, 1, true, false);
         return good ? FT_B200_OK : t_status;
     }
     // tri (src/drivers.c:921-957); all plans share the left / right flags
@@ -695,6 +711,7 @@ void ft_destroy_harmonic_plan(ft_harmonic_plan * P) {
     }
     if (H->d_scratch) cudaFree(H->d_scratch);
     if (H->d_stage) cudaFree(H->d_stage);
+    if (H->blocked) blocked_plan_free(H->blocked);
     H->magic = 0;
     delete H;
 }
@@ -743,6 +760,38 @@ int ft_b200_rotations_dev(const ft_rotation_plan * RP, int hi2lo, double * dA, i
     if (!RP || !dA || M < 1) { set_error(FT_B200_EINVAL, "bad argument"); return t_status; }
     rotations(const_cast<ft_rotation_plan *>(RP), hi2lo != 0, dA, dA, M, RP->n, static_cast<cudaStream_t>(stream));
     return t_status;
+}
+
+int ft_b200_execute_shared_dev(const ft_harmonic_plan * P, int forward, char TRANS, double * const * dA, int nfields,
+                               int precision, void * stream) {
+    clear_error();
+    HarmonicPlan * H = as_plan(P);
+    if (!H) { set_error(FT_B200_EINVAL, "not a plan created by this library"); return t_status; }
+    if (!dA || nfields < 0) { set_error(FT_B200_EINVAL, "bad argument"); return t_status; }
+    if (TRANS != 'N' && TRANS != 'T') { set_error(FT_B200_EINVAL, "TRANS must be 'N' or 'T'"); return t_status; }
+    if (precision != FT_B200_FP64 && precision != FT_B200_FP64_BLOCKED) { set_error(FT_B200_EINVAL, "unknown precision"); return t_status; }
+    if (precision == FT_B200_FP64_BLOCKED && H->kind != SPH) {
+        set_error(FT_B200_EUNSUPPORTED, "the blocked sweeps are built for sph plans");
+        return t_status;
+    }
+    for (int f = 0; f < nfields; f++)
+        if (!dA[f]) { set_error(FT_B200_EINVAL, "NULL matrix"); return t_status; }
+    if (nfields == 0) return FT_B200_OK;
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (precision == FT_B200_FP64_BLOCKED && !H->blocked) {
+        H->blocked = blocked_plan_build(H);
+        if (!H->blocked) return t_status;
+    }
+    const int M = H->Mdef;
+    for (int f0 = 0; f0 < nfields; f0 += kMaxFields) {
+        const int nf = std::min(kMaxFields, nfields - f0);
+        std::vector<HarmonicPlan *> Hs(nf, H);
+        std::vector<int> Ns(nf, H->n), Ms(nf, M);
+        if (execute_batch_chunk(Hs.data(), forward != 0, TRANS, dA + f0, Ns.data(), Ms.data(), nf, st,
+                                precision == FT_B200_FP64_BLOCKED) != FT_B200_OK)
+            return t_status;
+    }
+    return FT_B200_OK;
 }
 
 int ft_b200_plan_kind(const ft_harmonic_plan * P) {

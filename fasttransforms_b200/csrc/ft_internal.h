@@ -81,6 +81,8 @@ struct RotField {
     const double2 * sc;     // interleaved (sin, cos) table in the reference packing
     int N, M, kind;
     long long lda;
+    int blk;                // 0: all sweeps; > 0: only each column's sweeps above the last
+                            // whole block of blk sweeps (the rest run as blocked products)
 };
 
 // Kernel launchers (rotations.cu).  The field table travels by value in the
@@ -166,11 +168,21 @@ struct HarmonicPlan {
     size_t stage_elems;
     cudaStream_t stream;
     int device;
+    void * blocked;             // tile matrices of the blocked sweeps (built on first use)
 };
 // NULL unless P is a live plan of this library (api.cu)
 HarmonicPlan * as_plan(const ft_harmonic_plan * P);
 // device task list already built for (RP, M), without building one (api.cu)
 bool find_tasks(ft_rotation_plan * RP, int M, const RotTask ** d_tasks, int * ntasks);
+
+// Blocked sweeps for fields sharing one sph plan (blocked.cu).
+struct BlkTaskList { void * d_tasks = nullptr; int ntasks = 0; };
+void * blocked_plan_build(HarmonicPlan * H);
+void blocked_plan_free(void * p);
+int blocked_block_size();
+bool blocked_tasks(void * plan, int nf, int N, int M, BlkTaskList * out);
+cudaError_t launch_blocked(void * plan, bool hi2lo, double * const * A, int nf, int N, int M, const BlkTaskList & tl,
+                           int * counter, cudaStream_t st);
 
 // Error state (api.cu).
 void set_error(int status, const std::string & msg);

@@ -119,11 +119,32 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
         const int mbase = task.mbase;
         int omax = mbase + STEP * (ORD - 1);
         if (omax > mlast) omax = mbase + STEP * ((mlast - mbase) / STEP);
-        const int jlo = KIND == TRI ? 0 : (mbase & 1);
+        const int jpar = KIND == TRI ? 0 : (mbase & 1);   // lowest sweep of every column
+        // With F.blk > 0 a column of order m runs only its sweeps j >= jcut(m): the
+        // (m - jpar)/STEP mod blk sweeps above its last whole block of blk sweeps.
+        auto jcut = [&](int m) -> int {
+            return F.blk > 0 ? m - STEP * (((m - jpar) / STEP) % F.blk) : jpar;
+        };
+        int jlo = jpar;
+        if (F.blk > 0) {
+            jlo = jcut(mbase);
+            for (int o = 1; o < ORD; ++o) {
+                const int m = mbase + STEP * o;
+                if (m <= mlast) jlo = min(jlo, jcut(m));
+            }
+        }
         const int jhi = omax - STEP;
+        if (jhi < jlo) continue;   // nothing to do for this task (uniform)
         const int nsw = (jhi - jlo) / STEP + 1;
         const int npass = (nsw + WB - 1) / WB;
         const int m_lane = mbase + STEP * o_lane;
+        const int jcut_lane = jcut(m_lane);
+        int jlo_all_max = jpar;   // highest first sweep over the task's columns
+        if (F.blk > 0)
+            for (int o = 0; o < ORD; ++o) {
+                const int m = mbase + STEP * o;
+                if (m <= mlast) jlo_all_max = max(jlo_all_max, jcut(m));
+            }
         const int L0 = Geo::chain_len(KIND, N, 0);
 
         for (int r = 0; r < npass; ++r) {
@@ -175,13 +196,15 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
             }
             __syncwarp();
             const int jmax = HI2LO ? jfirst - STEP * (q * B) : jfirst + STEP * (q * B + B - 1);
-            const bool full_lanes = jmax <= mbase - STEP;   // every sweep of this stage applies to every order
+            const int jmin = HI2LO ? jfirst - STEP * (q * B + B - 1) : jfirst + STEP * (q * B);
+            // every sweep of this stage applies to every order of the task
+            const bool full_lanes = jmax <= mbase - STEP && (F.blk == 0 || jmin >= jlo_all_max);
             unsigned lane_mask = 0;                          // sweeps that apply to this lane's order
 #pragma unroll
             for (int b = 0; b < B; ++b) {
                 const int sg = q * B + b;
                 const int j = HI2LO ? jfirst - STEP * sg : jfirst + STEP * sg;
-                if (j <= m_lane - STEP) lane_mask |= 1u << b;
+                if (j <= m_lane - STEP && j >= jcut_lane) lane_mask |= 1u << b;
             }
 
             // Stage the (sin, cos) pairs of a chunk: entry (b, jj) is the pair sweep b

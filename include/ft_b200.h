@@ -169,6 +169,21 @@ int ft_b200_execute_batched_dev(const ft_harmonic_plan * const * plans, int forw
 #define FT_B200_NOALLOC_MAX_ELEMS (1 << 20)
 int ft_b200_execute_noalloc_dev(const ft_harmonic_plan * P, int forward, char TRANS, double * dA, int N, int M, void * stream);
 
+/* Fields sharing one plan (same n, same M, same family), in one call.
+ * precision FT_B200_FP64: the direct sweeps, as ft_b200_execute_batched_dev.
+ * precision FT_B200_FP64_BLOCKED (sph only): blocks of 32 consecutive sweeps
+ * are cut into tiles whose rotations are pre-multiplied (in FP64, once per
+ * plan) into dense orthogonal 64 x 64 matrices, applied to every field's
+ * columns as FP64 tensor-core (DMMA) products; a column's sweeps above its
+ * last whole block stay direct.  Not bit-identical to the direct sweeps (the
+ * products round differently); the relative 2-norm difference is of the order
+ * of 1e-14.  The first call on a plan builds its tile matrices (device memory,
+ * about 550 MB at n = 4096); make it before any stream capture. */
+#define FT_B200_FP64 0
+#define FT_B200_FP64_BLOCKED 1
+int ft_b200_execute_shared_dev(const ft_harmonic_plan * P, int forward, char TRANS, double * const * dA, int nfields,
+                               int precision, void * stream);
+
 /* Kind of a plan (FT_B200_SPH / TRI / DISK), or -1. */
 int ft_b200_plan_kind(const ft_harmonic_plan * P);
 /* Device id the plan lives on. */
