@@ -419,6 +419,34 @@ def extra_workloads(args, torch, ft):
     del g, data
     for p in plans.values():
         p.close()
+    # 16 fields of degree 4095 sharing one plan: direct FP64 vs blocked FP64 (tensor-core products)
+    n = 4096
+    Pn = ft.plan_sph2fourier(n)
+    M = Pn.M
+    fields = [torch.from_numpy(ft.sphrand(n, SEED + 100 + f).ravel(order="F").copy()).cuda() for f in range(16)]
+    fptr = [f.data_ptr() for f in fields]
+    res = {}
+    ref_out = None
+    for name, prec in (("fp64_direct", ft.FP64), ("fp64_blocked", ft.FP64_BLOCKED)):
+        x0 = fields[0].clone()
+        ft.execute_shared_dev(Pn, True, "N", [x0.data_ptr()], prec, sp)   # builds tables outside timing
+        torch.cuda.synchronize()
+        if ref_out is None:
+            ref_out = x0
+            err = 0.0
+        else:
+            err = float(torch.linalg.norm(x0 - ref_out) / torch.linalg.norm(ref_out))
+
+        def step(prec=prec):
+            ft.execute_shared_dev(Pn, True, "N", fptr, prec, sp)
+            ft.execute_shared_dev(Pn, False, "N", fptr, prec, sp)
+        step()
+        ms = timed(step, 3)
+        res[name] = {"coeffs_per_s": 16 * n * n / (ms * 1e-3), "ms_per_step": ms,
+                     "eps2_fwd_vs_fp64_direct": err}
+    out["shared_16_n4096"] = res
+    del fields
+    Pn.close()
     # sibling families at degree 2047, 8 fields per transform
     for name, kind, params in (("tri_000", "tri", (0.0, 0.0, 0.0)), ("tri_hhh", "tri", (-0.5, -0.5, -0.5)),
                                ("disk_00", "disk", (0.0, 0.0))):
