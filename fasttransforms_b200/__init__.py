@@ -29,7 +29,7 @@ __all__ = [
     "plan_rotsphere", "plan_rottriangle", "plan_rotdisk",
     "execute_sph_hi2lo", "execute_sph_lo2hi", "execute_tri_hi2lo", "execute_tri_lo2hi",
     "execute_disk_hi2lo", "execute_disk_lo2hi",
-    "execute_dev", "execute_shared_dev", "FP64", "FP64_BLOCKED", "execute_noalloc_dev", "NOALLOC_MAX_ELEMS", "execute_batched_dev", "rotations_dev", "kernel_launches", "profile", "profile_read",
+    "execute_dev", "execute_shared_dev", "FP64", "FP64_BLOCKED", "MIXED_BF16", "MIXED_BF16X4", "device_status", "execute_noalloc_dev", "NOALLOC_MAX_ELEMS", "execute_batched_dev", "rotations_dev", "kernel_launches", "profile", "profile_read",
     "layout_cols", "rand_layout", "sphrand", "trirand", "diskrand",
     "SPH", "TRI", "DISK",
 ]
@@ -67,6 +67,7 @@ def _load() -> C.CDLL:
         "ft_b200_plan_kind": (i, [vp]), "ft_b200_plan_device": (i, [vp]),
         "ft_b200_execute_noalloc_dev": (i, [vp, i, ch, vp, i, i, vp]),
         "ft_b200_execute_shared_dev": (i, [vp, i, ch, C.POINTER(vp), i, i, vp]),
+        "ft_b200_device_status": (i, [vp]),
         "ft_b200_profile": (i, [i]), "ft_b200_profile_read": (i, [i, C.POINTER(C.c_double), C.POINTER(i)]),
     }
     for name in ("sph2fourier", "fourier2sph", "tri2cheb", "cheb2tri", "disk2cxf", "cxf2disk"):
@@ -96,7 +97,7 @@ def profile(enable: bool) -> None:
 
 
 def profile_read(family: int):
-    """(total ms, launches) recorded for a kernel family: 0 rotations, 1 trmm, 2 other."""
+    """(total ms, launches) recorded for a kernel family: 0 rotations, 1 trmm, 2 other, 3 blocked sweeps."""
     ms = C.c_double(0)
     cnt = C.c_int(0)
     if lib.ft_b200_profile_read(family, C.byref(ms), C.byref(cnt)) != 0:
@@ -252,7 +253,7 @@ def execute_noalloc_dev(P: HarmonicPlan, forward: bool, trans: str, ptr: int, N:
         _check()
 
 
-FP64, FP64_BLOCKED = 0, 1
+FP64, FP64_BLOCKED, MIXED_BF16, MIXED_BF16X4 = 0, 1, 2, 3
 
 
 def execute_shared_dev(P: HarmonicPlan, forward: bool, trans: str, ptrs: Sequence[int], precision: int = FP64,
@@ -261,13 +262,24 @@ def execute_shared_dev(P: HarmonicPlan, forward: bool, trans: str, ptrs: Sequenc
 
     precision FP64: the direct sweeps; FP64_BLOCKED (sph only): whole blocks of
     32 sweeps applied as pre-multiplied 64 x 64 tile matrices on the FP64 tensor
-    pipe (rounds differently from the direct sweeps, ~1e-14 relative).
+    pipe (rounds differently from the direct sweeps, ~1e-14 relative);
+    MIXED_BF16 (sph only): the same tile products on the BF16 tensor cores from
+    three fixed-point BF16 slices per operand (~1e-6 .. 1e-5 relative);
+    MIXED_BF16X4: four slices (~1e-7 relative).
     """
     nf = len(ptrs)
     aa = (C.c_void_p * nf)(*ptrs)
     st = lib.ft_b200_execute_shared_dev(P.ptr, 1 if forward else 0, trans.encode(), aa, nf, precision, C.c_void_p(stream))
     if st != 0:
         _check()
+
+
+def device_status(P: HarmonicPlan) -> int:
+    """Read and clear the plan's device status word (nonzero: a tensor-core wait gave up)."""
+    v = lib.ft_b200_device_status(P.ptr)
+    if v < 0:
+        _check()
+    return v
 
 
 def rotations_dev(RP: RotationPlan, hi2lo: bool, ptr: int, M: int, stream: int = 0) -> None:

@@ -444,6 +444,10 @@ struct BatchCtx {
     std::vector<void *> allocs;
     BlkTaskList blk_tasks;                         // blocked-sweep tasks (built on first blocked call)
     bool blk_ready = false;
+    BlkTaskList mx_tasks;                          // the same for the split-BF16 products (pairs of fields)
+    bool mx_ready = false;
+    float * d_T = nullptr;                         // their task-major copy of the columns
+    void * mx_trmm = nullptr;                      // sliced inputs and tile lists of the tensor-core multiply
 };
 std::mutex g_batch_mu;
 std::map<std::string, BatchCtx *> g_batches;
@@ -488,6 +492,24 @@ bool build_trmm_set(BatchCtx * B, const std::vector<TrmmBatchClass> & cls, TrmmS
         T->ntiles = (int) o.size();
     }
     return true;
+}
+
+// Frees every batch context that names plan H (called when H is destroyed).
+void release_batches(HarmonicPlan * H) {
+    std::lock_guard<std::mutex> lk(g_batch_mu);
+    const std::string tag = std::to_string((uintptr_t) H) + ",";
+    for (auto it = g_batches.begin(); it != g_batches.end();) {
+        const std::string & k = it->first;
+        bool hit = false;
+        for (size_t pos = k.find(tag); pos != std::string::npos; pos = k.find(tag, pos + 1))
+            if (pos > 0 && (k[pos - 1] == ':' || k[pos - 1] == ';')) { hit = true; break; }
+        if (!hit) { ++it; continue; }
+        BatchCtx * B = it->second;
+        for (void * p : B->allocs) cudaFree(p);
+        mixed_trmm_work_free(B->mx_trmm);
+        delete B;
+        it = g_batches.erase(it);
+    }
 }
 
 BatchCtx * get_batch(HarmonicPlan * const * H, const int * N, const int * M, int nf) {
@@ -537,14 +559,25 @@ BatchCtx * get_batch(HarmonicPlan * const * H, const int * N, const int * M, int
 
 // one launch per stage over up to kMaxFields fields of one family
 int execute_batch_chunk(HarmonicPlan * const * H, bool forward, char TRANS, double * const * A, const int * N,
-                        const int * M, int nf, cudaStream_t st, bool blocked = false) {
+                        const int * M, int nf, cudaStream_t st, int precision = FT_B200_FP64) {
     BatchCtx * B = get_batch(H, N, M, nf);
     if (!B) return t_status;
+    const bool blocked = precision != FT_B200_FP64;
+    const bool mixed = precision == FT_B200_MIXED_BF16 || precision == FT_B200_MIXED_BF16X4;
+    const int ns = precision == FT_B200_MIXED_BF16X4 ? 4 : 3;
     const int blk = blocked ? blocked_block_size() : 0;
-    if (blocked && !B->blk_ready) {
+    if (blocked && !mixed && !B->blk_ready) {
         if (!blocked_tasks(H[0]->blocked, nf, N[0], M[0], &B->blk_tasks)) return t_status;
         if (B->blk_tasks.d_tasks) B->allocs.push_back(B->blk_tasks.d_tasks);
         B->blk_ready = true;
+    }
+    if (mixed && !B->mx_ready) {
+        if (!blocked_tasks_mixed(H[0]->blocked, nf, N[0], M[0], &B->mx_tasks)) return t_status;
+        if (B->mx_tasks.d_tasks) B->allocs.push_back(B->mx_tasks.d_tasks);
+        const size_t te = blocked_mixed_T_elems(H[0]->blocked, nf, N[0]);
+        if (!cuda_ok(cudaMalloc(&B->d_T, te * sizeof(float)), "cudaMalloc(blocked task copy)")) return t_status;
+        B->allocs.push_back(B->d_T);
+        B->mx_ready = true;
     }
     const int kind = H[0]->kind;
     const bool tN = TRANS == 'N';
@@ -573,6 +606,15 @@ int execute_batch_chunk(HarmonicPlan * const * H, bool forward, char TRANS, doub
         return cuda_ok(e, "rotation kernel");
     };
     auto trmm = [&](const TrmmSet & T, int mode, bool inverse, bool from_A) -> bool {
+        if (mixed) {   // sph only: the left multiplies, mode 0 (U In) or 1 (U^T In)
+            std::vector<double *> in(nf), out(nf);
+            for (int f = 0; f < nf; f++) { in[f] = from_A ? A[f] : S[f]; out[f] = from_A ? S[f] : A[f]; }
+            prof_begin(FAM_TRMM, st);
+            const cudaError_t e = launch_trmm_mixed(H[0], &H[0]->mixed_trmm, &B->mx_trmm, ns, inverse, mode == 1,
+                                                    in.data(), out.data(), nf, M[0], st);
+            prof_end(st);
+            return cuda_ok(e, "tensor-core trmm");
+        }
         static thread_local TrmmBatch P;
         bool vec = true;
         for (int f = 0; f < nf; f++) {
@@ -602,10 +644,17 @@ int execute_batch_chunk(HarmonicPlan * const * H, bool forward, char TRANS, doub
     // blocked products of the whole blocks, in place on the scratch matrices
     auto blocks = [&](bool hi2lo) -> bool {
         if (!blocked) return true;
-        prof_begin(FAM_ROT, st);
-        const cudaError_t e = launch_blocked(H[0]->blocked, hi2lo, S.data(), nf, N[0], M[0], B->blk_tasks, B->d_counter, st);
+        prof_begin(FAM_BLOCK, st);
+        if (!mixed) {
+            const cudaError_t e = launch_blocked(H[0]->blocked, hi2lo, S.data(), nf, N[0], M[0], B->blk_tasks, B->d_counter, st);
+            prof_end(st);
+            return cuda_ok(e, "blocked kernel");
+        }
+        cudaError_t e = launch_blocked_transpose(H[0]->blocked, true, S.data(), nf, N[0], M[0], B->d_T, B->mx_tasks, st);
+        if (e == cudaSuccess) e = launch_blocked_mixed(H[0]->blocked, ns, hi2lo, B->d_T, N[0], M[0], B->mx_tasks, B->d_counter, st);
+        if (e == cudaSuccess) e = launch_blocked_transpose(H[0]->blocked, false, S.data(), nf, N[0], M[0], B->d_T, B->mx_tasks, st);
         prof_end(st);
-        return cuda_ok(e, "blocked kernel");
+        return cuda_ok(e, "blocked kernels");
     };
     if (kind != TRI) {   // src/drivers.c:833-865, 989-1021
         bool good;
@@ -712,6 +761,8 @@ void ft_destroy_harmonic_plan(ft_harmonic_plan * P) {
     if (H->d_scratch) cudaFree(H->d_scratch);
     if (H->d_stage) cudaFree(H->d_stage);
     if (H->blocked) blocked_plan_free(H->blocked);
+    if (H->mixed_trmm) mixed_trmm_plan_free(H->mixed_trmm);
+    release_batches(H);
     H->magic = 0;
     delete H;
 }
@@ -769,8 +820,12 @@ int ft_b200_execute_shared_dev(const ft_harmonic_plan * P, int forward, char TRA
     if (!H) { set_error(FT_B200_EINVAL, "not a plan created by this library"); return t_status; }
     if (!dA || nfields < 0) { set_error(FT_B200_EINVAL, "bad argument"); return t_status; }
     if (TRANS != 'N' && TRANS != 'T') { set_error(FT_B200_EINVAL, "TRANS must be 'N' or 'T'"); return t_status; }
-    if (precision != FT_B200_FP64 && precision != FT_B200_FP64_BLOCKED) { set_error(FT_B200_EINVAL, "unknown precision"); return t_status; }
-    if (precision == FT_B200_FP64_BLOCKED && H->kind != SPH) {
+    if (precision != FT_B200_FP64 && precision != FT_B200_FP64_BLOCKED && precision != FT_B200_MIXED_BF16 &&
+        precision != FT_B200_MIXED_BF16X4) {
+        set_error(FT_B200_EINVAL, "unknown precision");
+        return t_status;
+    }
+    if (precision != FT_B200_FP64 && H->kind != SPH) {
         set_error(FT_B200_EUNSUPPORTED, "the blocked sweeps are built for sph plans");
         return t_status;
     }
@@ -778,20 +833,31 @@ int ft_b200_execute_shared_dev(const ft_harmonic_plan * P, int forward, char TRA
         if (!dA[f]) { set_error(FT_B200_EINVAL, "NULL matrix"); return t_status; }
     if (nfields == 0) return FT_B200_OK;
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
-    if (precision == FT_B200_FP64_BLOCKED && !H->blocked) {
+    if (precision != FT_B200_FP64 && !H->blocked) {
         H->blocked = blocked_plan_build(H);
         if (!H->blocked) return t_status;
     }
+    if ((precision == FT_B200_MIXED_BF16 || precision == FT_B200_MIXED_BF16X4) &&
+        !blocked_mixed_prepare(H->blocked, precision == FT_B200_MIXED_BF16X4 ? 4 : 3))
+        return t_status;
     const int M = H->Mdef;
     for (int f0 = 0; f0 < nfields; f0 += kMaxFields) {
         const int nf = std::min(kMaxFields, nfields - f0);
         std::vector<HarmonicPlan *> Hs(nf, H);
         std::vector<int> Ns(nf, H->n), Ms(nf, M);
-        if (execute_batch_chunk(Hs.data(), forward != 0, TRANS, dA + f0, Ns.data(), Ms.data(), nf, st,
-                                precision == FT_B200_FP64_BLOCKED) != FT_B200_OK)
+        if (execute_batch_chunk(Hs.data(), forward != 0, TRANS, dA + f0, Ns.data(), Ms.data(), nf, st, precision) != FT_B200_OK)
             return t_status;
     }
     return FT_B200_OK;
+}
+
+int ft_b200_device_status(const ft_harmonic_plan * P) {
+    clear_error();
+    HarmonicPlan * H = as_plan(P);
+    if (!H) { set_error(FT_B200_EINVAL, "not a plan created by this library"); return -1; }
+    const int a = H->blocked ? blocked_device_error(H->blocked) : 0;
+    const int b = H->mixed_trmm ? mixed_trmm_device_error(H->mixed_trmm) : 0;
+    return a ? a : b;
 }
 
 int ft_b200_plan_kind(const ft_harmonic_plan * P) {

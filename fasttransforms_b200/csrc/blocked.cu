@@ -23,7 +23,10 @@
 #include <algorithm>
 #include <cstdio>
 
+#include <cuda_bf16.h>
+
 #include "ft_internal.h"
+#include "tc05.h"
 
 namespace ftb {
 namespace {
@@ -205,6 +208,358 @@ __global__ void __launch_bounds__(NT, 1) blocked_kernel(const __grid_constant__ 
     }
 }
 
+// ---------------------------------------------------------------------------
+// Split-BF16 products on the tensor cores (tcgen05)
+//
+// The same block / tile decomposition, with every product computed from NS
+// BF16 pieces per operand on the tensor cores with FP32 accumulation.  The
+// pieces are fixed-point slices (the Ozaki splitting), not floating ones: a
+// window column x (64 positions) is scaled by a power of two s so that
+// |s x| < 2^7, and
+//   s x = i_0 + i_1 2^-8 + ... + i_{NS-1} 2^-8(NS-1),   integers |i_a| <= 2^7,
+// each rounded to nearest; a tile matrix entry (|q| <= 1) likewise with the
+// fixed scale 2^7 (slices j_b).  Integers of that size are exact in BF16,
+// every product i_a j_b is an integer below 2^14, and the products of one
+// order level L = a + b go to their own FP32 accumulator in tensor memory.
+// Levels L <= NS - 1 are kept (NS (NS + 1) / 2 products: 6 for NS = 3, 10 for
+// NS = 4); a level sums at most 4 x 64 such products, below 2^22, so the
+// accumulation is exact whatever rounding the tensor core applies.  The
+// epilogue recombines
+//   y = (A_0 + 2^-8 A_1 + ... ) 2^-7 / s
+// in FP32 with round-to-nearest.  The errors are the slicing and the dropped
+// levels (relative order 2^-8 NS of the window's largest entry and of the
+// tile matrix entries, summed over the 64 products of a row) and the FP32
+// rounding of y, all unbiased; a window position is carried between tiles as
+// FP32, in global memory the matrix stays FP64.
+//
+// A task is 128 columns: one band (BLK orders x cos, sin) of two fields.  The
+// product is D^T = X^T op(Q)^T with M = 128 (columns), N = WIN (output
+// positions), K = WIN (input positions), so each thread of the epilogue owns
+// one column (its TMEM lane) and half of the window.  Warps 0-7 carry chain 0,
+// warps 8-15 chain 1, warp 16 issues the MMAs (one thread) and owns the TMEM
+// allocation, warp 17 streams the tile images into shared memory, one buffer
+// per chain.  The
+// chains alternate on the tensor cores, so one chain's epilogue runs while the
+// other chain's products are in flight.
+// ---------------------------------------------------------------------------
+constexpr int MX_COLS = 128;                          // columns per task
+constexpr int MX_PIECE = MX_COLS * WIN * 2;           // bytes of one BF16 piece of one chain's window
+constexpr int MX_QPIECE = WIN * WIN * 2;              // bytes of one BF16 piece of one tile matrix
+constexpr int MX_THREADS = 576;                       // 16 epilogue warps, MMA warp, loader warp
+constexpr uint32_t MX_IDESC = tc::idesc_bf16(MX_COLS, WIN);
+constexpr int MX_TMEM_COLS = 512;                     // 2 chains x NS levels x WIN accumulator columns
+
+template <int NS> struct MxCfg {
+    static constexpr int QCHAIN = NS * MX_QPIECE;     // one chain's tile image
+    static constexpr size_t SMEM = 2 * NS * (size_t) MX_PIECE + 2 * (size_t) QCHAIN + 1024;
+    static_assert(2 * NS * WIN <= MX_TMEM_COLS, "accumulators exceed tensor memory");
+    static_assert(SMEM <= 227 * 1024, "shared memory");
+};
+
+// The blocked stage works on its own copy of the columns, task-major and
+// column-fastest: task (pair of fields, parity, band) -> 128 columns, and
+// element (chain c, position pos, column i) at ((c * Lmax + pos) * 128 + i),
+// in FP32.  A warp then reads or writes one position of 32 adjacent columns as
+// 128 contiguous bytes.
+__host__ __device__ __forceinline__ long long task_index(const BlkTask & t, int nbeta) {
+    return ((long long) (t.field >> 1) * 2 + t.p) * nbeta + (t.band - 1);
+}
+
+struct MixedLaunch {
+    float * T;                     // task-major copy of the columns (in place)
+    int Lmax;                      // positions per chain in T
+    const __nv_bfloat16 * img;     // tile images of the direction: [tile][chain][piece][WIN x WIN swizzled]
+    const long long * qbase;       // [2][nbeta], as for the FP64 tiles (2 chains per tile)
+    const int * kmax;
+    int nbeta;
+    const BlkTask * tasks;         // field: first field of the pair
+    int ntasks;
+    int * counter;
+    int * err;
+    int N, M;
+};
+
+// Q of one (parity, block): every tile and chain into its NS-slice BF16 image
+// (B[o][w] = Q[o][w] for hi2lo, Q[w][o] for lo2hi; rows o K-major, swizzled).
+template <int NS>
+__global__ void build_img_kernel(const double * __restrict__ Q, long long qb, int nk, bool transpose,
+                                 __nv_bfloat16 * __restrict__ img) {
+    const int k1 = blockIdx.x, c = blockIdx.y;    // tile k = k1 - 1
+    const double * q = Q + (qb + (long long) c * nk + k1) * WIN * WIN;
+    unsigned char * out = reinterpret_cast<unsigned char *>(img) + ((qb / 2 + k1) * 2 + c) * (long long) MxCfg<NS>::QCHAIN;
+    for (int e = threadIdx.x; e < WIN * WIN; e += blockDim.x) {
+        const int o = e / WIN, w = e % WIN;
+        // 128 q = j_0 + j_1 2^-8 + ..., integers |j| <= 2^7
+        double t = (transpose ? q[(long long) w * WIN + o] : q[e]) * 128.0;
+        const uint32_t off = tc::sw128_offset(o, w);
+        for (int b = 0; b < NS; ++b) {
+            const double j = rint(t);
+            *reinterpret_cast<__nv_bfloat16 *>(out + b * MX_QPIECE + off) = __float2bfloat16_rn((float) j);
+            t = (t - j) * 256.0;
+        }
+    }
+}
+
+// Power-of-two scale s with |s x| < 2^7 for every |x| <= amax (s = 1 for amax = 0).
+__device__ __forceinline__ float slice_scale(float amax) {
+    int E = (int) ((__float_as_uint(amax) >> 23) & 0xFF);   // amax < 2^(E - 126)
+    if (E < 8) E = 8;                                         // tiny or zero windows
+    return __uint_as_float((uint32_t) (260 - E) << 23);       // 2^(7 - (E - 126))
+}
+
+// eight consecutive window positions, scaled by s, -> NS 16-byte chunks of
+// integer-valued BF16 slices: s x = i_0 + i_1 2^-8 + ...
+template <int NS>
+__device__ __forceinline__ void slice8(const float * v, float s, uint4 * out) {
+    uint32_t w[NS][4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        float t0 = v[2 * q] * s, t1 = v[2 * q + 1] * s;
+#pragma unroll
+        for (int a = 0; a < NS; ++a) {
+            const float i0 = rintf(t0), i1 = rintf(t1);
+            const __nv_bfloat162 b = __floats2bfloat162_rn(i0, i1);
+            w[a][q] = *reinterpret_cast<const uint32_t *>(&b);
+            t0 = (t0 - i0) * 256.0f;
+            t1 = (t1 - i1) * 256.0f;
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < NS; ++a) out[a] = make_uint4(w[a][0], w[a][1], w[a][2], w[a][3]);
+}
+
+template <bool HI2LO, int NS>
+__global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __grid_constant__ MixedLaunch L) {
+    constexpr int QCHAIN = MxCfg<NS>::QCHAIN;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char * const sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t) 1023);
+    unsigned char * const Xs = sm;                        // [chain][piece]: MX_COLS rows x WIN slots
+    unsigned char * const Qs = sm + 2 * NS * MX_PIECE;    // [chain]: the chain's tile image
+    __shared__ __align__(8) uint64_t bar_qfull[2], bar_qempty[2], bar_xready[2], bar_acc[2], bar_pmax[2], bar_done;
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_task;
+    __shared__ volatile int s_abort;
+    __shared__ float s_pmax[2][2][MX_COLS];             // [chain][half][column]: largest window entry
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int N = L.N;
+
+    if (tid == 0) {
+        for (int i = 0; i < 2; ++i) {
+            tc::mbar_init(&bar_qfull[i], 1);
+            tc::mbar_init(&bar_qempty[i], 1);
+            tc::mbar_init(&bar_xready[i], 256);
+            tc::mbar_init(&bar_pmax[i], 256);
+            tc::mbar_init(&bar_acc[i], 1);
+        }
+        tc::mbar_init(&bar_done, 1);
+        s_abort = 0;
+    }
+    if (warp == 16) tc::tmem_alloc(&s_tmem, MX_TMEM_COLS);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = s_tmem;
+
+    auto fail = [&]() {
+        s_abort = 1;
+        atomicExch(L.err, 1);
+    };
+    // per-role pipeline counters (identical traversal in every role)
+    unsigned qt = 0;                 // tiles issued (loader) / consumed (MMA)
+    unsigned xr[2] = {0, 0};         // x-ready phases consumed (MMA)
+    unsigned ac = 0;                 // accumulator phases consumed (epilogue, own chain)
+    unsigned pp = 0;                 // window-maximum exchanges (epilogue, own chain)
+    int last_u = -1;                 // loader: last use of the chain buffers
+
+    for (;;) {
+        if (tid == 0) s_task = atomicAdd(L.counter, 1);
+        __syncthreads();
+        const int t_id = s_task;
+        __syncthreads();
+        if (t_id >= L.ntasks || s_abort) break;
+        const BlkTask T = L.tasks[t_id];
+        const int p = T.p, band = T.band;
+
+        if (warp == 17) {
+            // ---- tile images into shared memory, one buffer per chain ----
+            if (lane == 0) {
+                for (int bi = 0; bi < band && !s_abort; ++bi) {
+                    const int beta = HI2LO ? band - 1 - bi : bi;
+                    const int kmax = L.kmax[p * L.nbeta + beta];
+                    const long long tb = L.qbase[p * L.nbeta + beta] / 2;
+                    const unsigned char * const img0 = reinterpret_cast<const unsigned char *>(L.img) + tb * 2LL * QCHAIN;
+                    // the block's first tiles into L2 ahead of their copies
+                    for (int ki = 0; ki < 2 && ki < kmax + 2; ++ki)
+                        tc::prefetch_l2(img0 + (HI2LO ? kmax - ki + 1 : ki) * 2LL * QCHAIN, 2 * QCHAIN);
+                    for (int ki = 0; ki < kmax + 2 && !s_abort; ++ki, ++qt) {
+                        const int k = HI2LO ? kmax - ki : ki - 1;
+                        const int u = (int) qt;
+                        const unsigned char * src = img0 + (k + 1) * 2LL * QCHAIN;
+                        if (ki + 2 < kmax + 2)   // two tiles ahead
+                            tc::prefetch_l2(img0 + (HI2LO ? k - 2 + 1 : k + 2 + 1) * 2LL * QCHAIN, 2 * QCHAIN);
+                        for (int c = 0; c < 2; ++c) {
+                            if (!tc::mbar_wait(&bar_qempty[c], (u & 1) ^ 1, &s_abort)) { fail(); break; }
+                            tc::mbar_arrive_expect_tx(&bar_qfull[c], QCHAIN);
+                            tc::bulk_g2s(Qs + c * QCHAIN, src + c * QCHAIN, QCHAIN, &bar_qfull[c]);
+                        }
+                        last_u = u;
+                    }
+                }
+            }
+            __syncwarp();
+        } else if (warp == 16) {
+            // ---- MMA issue ----
+            if (lane == 0) {
+                const uint32_t xs0 = tc::smem_addr(Xs), qs0 = tc::smem_addr(Qs);
+                for (int bi = 0; bi < band && !s_abort; ++bi) {
+                    const int beta = HI2LO ? band - 1 - bi : bi;
+                    const int kmax = L.kmax[p * L.nbeta + beta];
+                    for (int ki = 0; ki < kmax + 2 && !s_abort; ++ki, ++qt) {
+                        const int k = HI2LO ? kmax - ki : ki - 1;
+                        const int lo = k * TL;
+                        const unsigned u = qt;
+                        for (int c = 0; c < 2; ++c) {
+                            if (!tc::mbar_wait(&bar_qfull[c], u & 1, &s_abort)) { fail(); break; }
+                            if (!tc::mbar_wait(&bar_xready[c], xr[c] & 1, &s_abort)) { fail(); break; }
+                            xr[c]++;
+                            tc::fence_after_sync();
+                            for (int kk = 0; kk < WIN / 16; ++kk) {
+                                const uint32_t sc = (uint32_t) (((lo + 16 * kk) & (WIN - 1)) >> 4);
+#pragma unroll
+                                for (int a = 0; a < NS; ++a)
+#pragma unroll
+                                    for (int b = 0; a + b < NS; ++b) {
+                                        const uint64_t ad = tc::desc_sw128(xs0 + (c * NS + a) * MX_PIECE + sc * 32);
+                                        const uint64_t bd = tc::desc_sw128(qs0 + c * QCHAIN + b * MX_QPIECE + kk * 32);
+                                        // level a + b; its first product (kk = 0, a = 0) starts the accumulator
+                                        tc::mma_bf16(tmem + (c * NS + a + b) * WIN, ad, bd, MX_IDESC, !(kk == 0 && a == 0));
+                                    }
+                            }
+                            tc::commit(&bar_acc[c]);
+                            tc::commit(&bar_qempty[c]);
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+        } else {
+            // ---- epilogue: one column (TMEM lane) and half a window per thread ----
+            // warps 8c .. 8c + 7 carry chain c; warp 8c + 4 hf + q owns TMEM lanes 32 q ..
+            // and window offsets 32 hf .. 32 hf + 31
+            const int c = warp >> 3;
+            const int quarter = warp & 3, hf = (warp >> 2) & 1;
+            const int r = 32 * quarter + lane;
+            const int fh = HI2LO ? 1 : 0;                 // the half whose outputs leave the window
+            float * const Tc = L.T + task_index(T, L.nbeta) * (2LL * L.Lmax * MX_COLS) + (long long) c * L.Lmax * MX_COLS + r;
+            unsigned char * const xrow = Xs + c * NS * MX_PIECE;
+            const uint32_t tacc = tmem + ((uint32_t) (quarter * 32) << 16) + c * NS * WIN + 32 * hf;
+            float scale = 1.0f;   // slicing scale of the window the products in flight were computed from
+            auto valid = [&](int pos) -> bool { return pos >= 0 && 2 * pos + c < N; };
+            auto load32 = [&](int pos0, float * v) {
+#pragma unroll
+                for (int e = 0; e < TL; ++e) v[e] = valid(pos0 + e) ? __ldcg(Tc + (long long) (pos0 + e) * MX_COLS) : 0.0f;
+            };
+            // 32 positions from pos0 (a multiple of 32) into their window slots, with one
+            // scale for the whole window: the two halves exchange their largest entries
+            auto put32 = [&](int pos0, const float * v) -> bool {
+                float m0 = 0.0f, m1 = 0.0f, m2 = 0.0f, m3 = 0.0f;
+#pragma unroll
+                for (int e = 0; e < TL; e += 4) {
+                    m0 = fmaxf(m0, fabsf(v[e]));
+                    m1 = fmaxf(m1, fabsf(v[e + 1]));
+                    m2 = fmaxf(m2, fabsf(v[e + 2]));
+                    m3 = fmaxf(m3, fabsf(v[e + 3]));
+                }
+                const float pm = fmaxf(fmaxf(m0, m1), fmaxf(m2, m3));
+                s_pmax[c][hf][r] = pm;
+                tc::mbar_arrive(&bar_pmax[c]);
+                if (!tc::mbar_wait(&bar_pmax[c], pp & 1, &s_abort)) { fail(); return false; }
+                pp++;
+                const float sc = slice_scale(fmaxf(pm, s_pmax[c][hf ^ 1][r]));
+                scale = sc;
+#pragma unroll
+                for (int g = 0; g < TL / 8; ++g) {
+                    uint4 ch[NS];
+                    slice8<NS>(v + 8 * g, sc, ch);
+                    const uint32_t off = tc::sw128_offset(r, (pos0 + 8 * g) & (WIN - 1));
+#pragma unroll
+                    for (int a = 0; a < NS; ++a) *reinterpret_cast<uint4 *>(xrow + a * MX_PIECE + off) = ch[a];
+                }
+                tc::fence_async_smem();
+                tc::fence_before_sync();
+                tc::mbar_arrive(&bar_xready[c]);
+                return true;
+            };
+            for (int bi = 0; bi < band && !s_abort; ++bi) {
+                const int beta = HI2LO ? band - 1 - bi : bi;
+                const int kmax = L.kmax[p * L.nbeta + beta];
+                const int nk = kmax + 2;
+                float src[TL];
+                {   // first tile: the whole window
+                    const int pos0 = (HI2LO ? kmax : -1) * TL + TL * hf;
+                    load32(pos0, src);
+                    if (!put32(pos0, src)) break;
+                }
+                for (int ki = 0; ki < nk; ++ki) {
+                    const int k = HI2LO ? kmax - ki : ki - 1;
+                    const int lo = k * TL;
+                    const bool last = ki == nk - 1;
+                    const bool fin = last || hf == fh;    // this half's outputs leave the window
+                    const int npos = HI2LO ? lo - TL : lo + WIN;
+                    // the finishing half brings the positions entering the next tile
+                    if (!last && hf == fh) load32(npos, src);
+                    if (!tc::mbar_wait(&bar_acc[c], ac & 1, &s_abort)) { fail(); break; }
+                    ac++;
+                    __syncwarp();
+                    tc::fence_after_sync();
+                    const float unscale = 0.0078125f / scale;     // 2^-7 / s, a power of two
+#pragma unroll
+                    for (int g = 0; g < TL / 8; ++g) {             // 8 window positions at a time
+                        uint32_t a[NS][8];
+#pragma unroll
+                        for (int lv = 0; lv < NS; ++lv) tc::tmem_ld8_async(tacc + lv * WIN + 8 * g, a[lv]);
+                        tc::tmem_wait_ld();
+#pragma unroll
+                        for (int e = 0; e < 8; ++e) {
+                            float y = __uint_as_float(a[NS - 1][e]);
+#pragma unroll
+                            for (int lv = NS - 2; lv >= 0; --lv) y = fmaf(y, 0.00390625f, __uint_as_float(a[lv][e]));
+                            const float v = y * unscale;
+                            const int pos = lo + TL * hf + 8 * g + e;
+                            if (fin) {
+                                if (valid(pos)) __stcg(Tc + (long long) pos * MX_COLS, v);
+                            } else {
+                                src[8 * g + e] = v;
+                            }
+                        }
+                    }
+                    // next window: the overlap stays in its slots, the entering positions take
+                    // the finished ones' slots
+                    if (!last && !put32(hf == fh ? npos : lo + TL * hf, src)) break;
+                }
+            }
+        }
+    }
+
+    // ---- teardown: nothing of this CTA may be in flight when TMEM is freed ----
+    __syncthreads();
+    __shared__ volatile int s_never;
+    if (tid == 0) s_never = 0;
+    __syncthreads();
+    if (warp == 17 && lane == 0 && s_abort && last_u >= 0) {
+        for (int c = 0; c < 2; ++c) (void) tc::mbar_wait(&bar_qfull[c], last_u & 1, &s_never);
+    }
+    if (warp == 16) {
+        if (lane == 0) {
+            tc::commit(&bar_done);
+            if (!tc::mbar_wait(&bar_done, 0, &s_never)) atomicExch(L.err, 2);
+        }
+        __syncwarp();
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tmem, MX_TMEM_COLS);
+    }
+}
+
 struct BlockedPlan {
     int n = 0;
     int nbeta = 0;
@@ -212,7 +567,11 @@ struct BlockedPlan {
     long long * d_qbase = nullptr;
     int * d_kmax = nullptr;
     std::vector<int> kmax;      // [2][nbeta]
+    std::vector<long long> qbase;
+    long long ntiles = 0;       // tile-chain pairs x 2
     size_t bytes = 0;
+    __nv_bfloat16 * d_img[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // tile images [3 or 4 slices][hi2lo, lo2hi]
+    int * d_err = nullptr;      // set by a tensor-core kernel whose wait ran out
 };
 
 int kmax_of(int N, int p, int beta) {
@@ -248,6 +607,8 @@ void * blocked_plan_build(HarmonicPlan * H) {
             tiles += 2LL * (km + 2);
         }
     B->bytes = (size_t) std::max(1LL, tiles) * WIN * WIN * sizeof(double);
+    B->qbase = qbase;
+    B->ntiles = tiles;
     const double2 * sc = H->rp_arr[0]->d_sc;
     bool ok = cuda_fine(cudaMalloc(&B->d_Q, B->bytes), "cudaMalloc(blocked Q)") &&
               cuda_fine(cudaMalloc(&B->d_qbase, sizeof(long long) * qbase.size()), "cudaMalloc") &&
@@ -277,6 +638,8 @@ void blocked_plan_free(void * p) {
     BlockedPlan * B = static_cast<BlockedPlan *>(p);
     if (!B) return;
     cudaFree(B->d_Q); cudaFree(B->d_qbase); cudaFree(B->d_kmax);
+    for (auto & im : B->d_img) { cudaFree(im[0]); cudaFree(im[1]); }
+    cudaFree(B->d_err);
     delete B;
 }
 
@@ -339,6 +702,188 @@ bool blocked_tasks(void * plan, int nf, int N, int M, BlkTaskList * out) {
     if (t.empty()) return true;
     if (!cuda_fine(cudaMalloc(&out->d_tasks, sizeof(BlkTask) * t.size()), "cudaMalloc(blocked tasks)")) return false;
     return cuda_fine(cudaMemcpy(out->d_tasks, t.data(), sizeof(BlkTask) * t.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
+}
+
+// Split-BF16 tile images with ns (3 or 4) slices, both directions (built once
+// per plan and slice count, from the FP64 tiles).
+bool blocked_mixed_prepare(void * plan, int ns) {
+    BlockedPlan * B = static_cast<BlockedPlan *>(plan);
+    if (ns != 3 && ns != 4) { set_error(FT_B200_EINVAL, "slice count must be 3 or 4"); return false; }
+    __nv_bfloat16 ** img = B->d_img[ns - 3];
+    if (!B->d_err) {
+        if (!cuda_fine(cudaMalloc(&B->d_err, sizeof(int)), "cudaMalloc")) return false;
+        if (!cuda_fine(cudaMemset(B->d_err, 0, sizeof(int)), "cudaMemset")) return false;
+    }
+    if (img[0] && img[1]) return true;
+    const size_t bytes = (size_t) std::max(1LL, B->ntiles / 2) * 2 * (size_t) ns * MX_QPIECE;
+    for (int d = 0; d < 2; d++) {
+        if (img[d]) continue;
+        void * p = nullptr;
+        if (!cuda_fine(cudaMalloc(&p, bytes), "cudaMalloc(split tile images)")) return false;
+        img[d] = static_cast<__nv_bfloat16 *>(p);
+        for (int par = 0; par < 2; par++)
+            for (int beta = 0; beta < B->nbeta; beta++) {
+                const int nk = B->kmax[par * B->nbeta + beta] + 2;
+                const long long qb = B->qbase[par * B->nbeta + beta];
+                if (ns == 3) build_img_kernel<3><<<dim3(nk, 2), 256>>>(B->d_Q, qb, nk, d == 1, img[d]);
+                else         build_img_kernel<4><<<dim3(nk, 2), 256>>>(B->d_Q, qb, nk, d == 1, img[d]);
+                count_launch();
+            }
+        if (!cuda_fine(cudaGetLastError(), "build_img_kernel")) return false;
+    }
+    return cuda_fine(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+}
+
+// Tasks (pair of fields, parity, band >= 1), longest first.
+bool blocked_tasks_mixed(void * plan, int nf, int N, int M, BlkTaskList * out) {
+    BlockedPlan * B = static_cast<BlockedPlan *>(plan);
+    const int mlast = M / 2;
+    (void) N;
+    std::vector<std::pair<long long, BlkTask>> v;
+    for (int f = 0; f < nf; f += 2)
+        for (int p = 0; p < 2; p++) {
+            const int m0 = p == 0 ? 2 : 3;
+            for (int band = 1; p + 2 * BLK * band <= mlast; band++) {
+                if (p + 2 * BLK * band < m0) continue;
+                if (band > B->nbeta) {
+                    set_error(FT_B200_EINVAL, "column band beyond the plan's blocks");
+                    return false;
+                }
+                long long cost = 0;
+                for (int beta = 0; beta < band; beta++) cost += B->kmax[p * B->nbeta + beta] + 2;
+                v.push_back({cost, BlkTask{f, p, band}});
+            }
+        }
+    std::stable_sort(v.begin(), v.end(), [](const auto & a, const auto & b) { return a.first > b.first; });
+    std::vector<BlkTask> t;
+    for (auto & x : v) t.push_back(x.second);
+    out->ntasks = (int) t.size();
+    if (t.empty()) return true;
+    if (!cuda_fine(cudaMalloc(&out->d_tasks, sizeof(BlkTask) * t.size()), "cudaMalloc(blocked tasks)")) return false;
+    return cuda_fine(cudaMemcpy(out->d_tasks, t.data(), sizeof(BlkTask) * t.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
+}
+
+cudaError_t launch_blocked_mixed(void * plan, int ns, bool hi2lo, float * T, int N, int M, const BlkTaskList & tl,
+                                 int * counter, cudaStream_t st) {
+    BlockedPlan * B = static_cast<BlockedPlan *>(plan);
+    if (tl.ntasks == 0) return cudaSuccess;
+    static thread_local MixedLaunch L;
+    L.T = T;
+    L.Lmax = (N + 1) / 2;
+    L.img = B->d_img[ns - 3][hi2lo ? 0 : 1];
+    L.qbase = B->d_qbase;
+    L.kmax = B->d_kmax;
+    L.nbeta = B->nbeta;
+    L.tasks = reinterpret_cast<const BlkTask *>(tl.d_tasks);
+    L.ntasks = tl.ntasks;
+    L.counter = counter;
+    L.err = B->d_err;
+    L.N = N;
+    L.M = M;
+    auto kern = ns == 3 ? (hi2lo ? blocked_mixed_kernel<true, 3> : blocked_mixed_kernel<false, 3>)
+                        : (hi2lo ? blocked_mixed_kernel<true, 4> : blocked_mixed_kernel<false, 4>);
+    const size_t smem = ns == 3 ? MxCfg<3>::SMEM : MxCfg<4>::SMEM;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(counter, 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int ctas = std::min(sms, tl.ntasks);
+    kern<<<ctas, MX_THREADS, smem, st>>>(L);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// Elements of the task-major copy used by the split-BF16 products.
+size_t blocked_mixed_T_elems(void * plan, int nf, int N) {
+    BlockedPlan * B = static_cast<BlockedPlan *>(plan);
+    const long long npairs = (nf + 1) / 2;
+    return (size_t) (npairs * 2 * std::max(1, B->nbeta)) * 2 * (size_t) ((N + 1) / 2) * MX_COLS;
+}
+
+// S (the fields' FP64 matrices) <-> T (task-major FP32 copy of the columns the
+// blocks apply to); one CTA per (task, 32 positions of both chains).
+struct TransLaunch {
+    double * A[kMaxFields];
+    int nf, N, M, nbeta, Lmax;
+    float * T;
+    const BlkTask * tasks;
+};
+
+template <bool TO_T>
+__global__ void __launch_bounds__(256) transpose_kernel(const __grid_constant__ TransLaunch L) {
+    __shared__ float tile[64][MX_COLS + 1];             // [row in the chunk][column]
+    const BlkTask t = L.tasks[blockIdx.x];
+    const int q = blockIdx.y;                           // positions 32q .. 32q + 31
+    const int tid = threadIdx.x;
+    const int N = L.N, mlast = L.M / 2;
+    float * const Tt = L.T + task_index(t, L.nbeta) * (2LL * L.Lmax * MX_COLS);
+    // column i of the task: field, matrix column, or -1
+    auto column = [&](int i, int & f) -> long long {
+        f = t.field + (i >> 6);
+        const int n = i & 63;
+        const int m = t.p + 2 * BLK * t.band + 2 * (n >> 1);
+        return (f < L.nf && m <= mlast) ? 2LL * m - 1 + (n & 1) : -1;
+    };
+    const int rr = tid & 63;                            // row of the chunk: 2 * (pos - 32q) + chain
+    const int row = 64 * q + rr;
+    if (TO_T) {
+        for (int i = tid >> 6; i < MX_COLS; i += 4) {
+            int f;
+            const long long col = column(i, f);
+            tile[rr][i] = (col >= 0 && row < N) ? (float) __ldcg(L.A[f] + col * N + row) : 0.0f;
+        }
+        __syncthreads();
+        const int i = tid & (MX_COLS - 1);
+        for (int e = tid >> 7; e < 64; e += 2) {       // e = 2 * (pos - 32q) + c
+            const int c = e & 1, pos = 32 * q + (e >> 1);
+            if (pos < L.Lmax) __stcg(Tt + ((long long) c * L.Lmax + pos) * MX_COLS + i, tile[e][i]);
+        }
+    } else {
+        const int i = tid & (MX_COLS - 1);
+        for (int e = tid >> 7; e < 64; e += 2) {
+            const int c = e & 1, pos = 32 * q + (e >> 1);
+            tile[e][i] = pos < L.Lmax ? __ldcg(Tt + ((long long) c * L.Lmax + pos) * MX_COLS + i) : 0.0f;
+        }
+        __syncthreads();
+        for (int i2 = tid >> 6; i2 < MX_COLS; i2 += 4) {
+            int f;
+            const long long col = column(i2, f);
+            if (col >= 0 && row < N) __stcg(L.A[f] + col * N + row, (double) tile[rr][i2]);
+        }
+    }
+}
+
+cudaError_t launch_blocked_transpose(void * plan, bool to_T, double * const * A, int nf, int N, int M, float * T,
+                                     const BlkTaskList & tl, cudaStream_t st) {
+    BlockedPlan * B = static_cast<BlockedPlan *>(plan);
+    if (tl.ntasks == 0) return cudaSuccess;
+    static thread_local TransLaunch L;
+    for (int f = 0; f < nf; f++) L.A[f] = A[f];
+    L.nf = nf;
+    L.N = N;
+    L.M = M;
+    L.nbeta = B->nbeta;
+    L.Lmax = (N + 1) / 2;
+    L.T = T;
+    L.tasks = reinterpret_cast<const BlkTask *>(tl.d_tasks);
+    const dim3 grid(tl.ntasks, (L.Lmax + 31) / 32);
+    if (to_T) transpose_kernel<true><<<grid, 256, 0, st>>>(L);
+    else      transpose_kernel<false><<<grid, 256, 0, st>>>(L);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// Reads and clears the flag a tensor-core kernel sets when one of its waits ran out.
+int blocked_device_error(void * plan) {
+    BlockedPlan * B = static_cast<BlockedPlan *>(plan);
+    if (!B || !B->d_err) return 0;
+    int v = 0;
+    if (cudaMemcpy(&v, B->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    if (v) cudaMemset(B->d_err, 0, sizeof(int));
+    return v;
 }
 
 }  // namespace ftb

@@ -169,6 +169,7 @@ struct HarmonicPlan {
     cudaStream_t stream;
     int device;
     void * blocked;             // tile matrices of the blocked sweeps (built on first use)
+    void * mixed_trmm;          // sliced images of the connection matrices (built on first use)
 };
 // NULL unless P is a live plan of this library (api.cu)
 HarmonicPlan * as_plan(const ft_harmonic_plan * P);
@@ -183,13 +184,28 @@ int blocked_block_size();
 bool blocked_tasks(void * plan, int nf, int N, int M, BlkTaskList * out);
 cudaError_t launch_blocked(void * plan, bool hi2lo, double * const * A, int nf, int N, int M, const BlkTaskList & tl,
                            int * counter, cudaStream_t st);
+// split-BF16 tensor-core products of the same blocks
+bool blocked_mixed_prepare(void * plan, int ns);
+bool blocked_tasks_mixed(void * plan, int nf, int N, int M, BlkTaskList * out);
+cudaError_t launch_blocked_mixed(void * plan, int ns, bool hi2lo, float * T, int N, int M, const BlkTaskList & tl,
+                                 int * counter, cudaStream_t st);
+size_t blocked_mixed_T_elems(void * plan, int nf, int N);
+cudaError_t launch_blocked_transpose(void * plan, bool to_T, double * const * A, int nf, int N, int M, float * T,
+                                     const BlkTaskList & tl, cudaStream_t st);
+int blocked_device_error(void * plan);
+// connection multiply of the sph family on the tensor cores from BF16 slices (trmm_mixed.cu)
+cudaError_t launch_trmm_mixed(HarmonicPlan * H, void ** plan_slot, void ** work_slot, int nu, bool inverse, bool trans,
+                              double * const * in, double * const * out, int nf, int M, cudaStream_t st);
+void mixed_trmm_plan_free(void * p);
+void mixed_trmm_work_free(void * p);
+int mixed_trmm_device_error(void * p);
 
 // Error state (api.cu).
 void set_error(int status, const std::string & msg);
 void clear_error();
 void count_launch(unsigned long long n = 1);
 // measurement hook: bracket a launch with events on its stream when profiling is on
-enum { FAM_ROT = 0, FAM_TRMM = 1, FAM_OTHER = 2 };
+enum { FAM_ROT = 0, FAM_TRMM = 1, FAM_OTHER = 2, FAM_BLOCK = 3 };
 void prof_begin(int family, cudaStream_t st);
 void prof_end(cudaStream_t st);
 

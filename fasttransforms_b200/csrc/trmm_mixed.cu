@@ -1,0 +1,490 @@
+// The sph connection multiply (src/drivers.c:833-865: four column classes j = 0,1,2,3 mod 4,
+// class j multiplied by U[0] for j = 0, 3 and U[1] for j = 1, 2, U upper triangular)
+// on the tcgen05 tensor cores, from fixed-point BF16 slices.
+//
+// Slicing (the Ozaki splitting).  A row i of op(U) is scaled by a power of two
+// sU_i with |sU_i U| < 2^7 and cut into NU slices of integers |j_b| <= 2^7:
+// sU_i U = j_0 + j_1 2^-8 + ...; a column x of the input is cut the same way
+// in chunks of 256 rows, each chunk with its own scale sX (NX slices).  The
+// products j_b i_a of one order level L = a + b <= NL - 1 are integers below
+// 2^14 and a level sums at most 3 x 256 of them per chunk, below 2^24, so the
+// level accumulators in tensor memory are exact whatever rounding the tensor
+// core applies.  After each chunk the epilogue folds
+//   (A_0 + 2^-8 A_1 + ...) / sX
+// into an FP32 running sum per output element; at the end it scales by
+// 1 / sU_i and writes FP64.  Configurations: NU = 3 slices of U (levels <= 2,
+// six products) and NU = 4 (levels <= 3, nine products), both with NX = 3.
+//
+// Work: output tiles of 128 rows x 128 columns of one class of one field,
+// longest K first, strided over persistent CTAs.  The operands come as
+// pre-sliced images in the tensor cores' K-major 128-byte swizzled layout:
+// U's once per plan, the input's by a slicing pass before each multiply.
+// Warp 8 issues the MMAs (one thread) and owns the TMEM allocation, warp 9
+// streams the K-tiles into a two-stage buffer with bulk copies, warps 0-7
+// fold the chunks (two warps per TMEM lane quarter, 64 columns each).
+#include <algorithm>
+#include <cstdio>
+#include <vector>
+
+#include <cuda_bf16.h>
+
+#include "ft_internal.h"
+#include "tc05.h"
+
+namespace ftb {
+namespace {
+
+constexpr int TB = 128;                     // output tile rows and columns
+constexpr int KT = 64;                      // K per tile of the images
+constexpr int CHUNK_KT = 4;                 // K-tiles per exact chunk (256 rows)
+constexpr int PIECE = TB * KT * 2;          // bytes of one slice of one K-tile (16 KB)
+constexpr int THREADS = 320;
+constexpr uint32_t IDESC = tc::idesc_bf16(TB, TB);
+
+template <int NU, int NX> struct Cfg {
+    static constexpr int NL = NU;                           // levels kept: 0 .. NU - 1
+    static constexpr int STAGE = (NU + NX) * PIECE;
+    static constexpr size_t SMEM = 2 * (size_t) STAGE + 1024;
+    static_assert(NL * TB <= 512, "accumulators exceed tensor memory");
+    static_assert(SMEM <= 227 * 1024, "shared memory");
+};
+
+struct MixTile { int field, cls, it, jt, k0, k1; };   // K-tiles k0 .. k1 inclusive
+
+struct MixLaunch {
+    double * out[kMaxFields];
+    const unsigned char * Uimg[2];      // per class matrix: [it][kt][NU slices]
+    const float * Uinv[2];              // 1 / sU per row
+    const unsigned char * Ximg;         // [field][cls][jt][kt][NX slices]
+    const float * Xinv;                 // [field][cls][jt][chunk][128]: 1 / sX
+    const MixTile * tiles;
+    int ntiles;
+    int n, M, nkt, njt;                 // njt: column tiles per class (max over classes)
+    int * err;
+};
+
+__host__ __device__ __forceinline__ int class_cols(int M, int r) { return (M - r + 3) / 4; }
+__host__ __device__ __forceinline__ int class_matrix(int r) { return (r == 0 || r == 3) ? 0 : 1; }
+
+// ---------------------------------------------------------------------------
+// slicing passes
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float pow2_scale(float amax) {
+    int E = (int) ((__float_as_uint(amax) >> 23) & 0xFF);   // amax < 2^(E - 126)
+    if (E < 8) E = 8;
+    return __uint_as_float((uint32_t) (260 - E) << 23);       // 2^(7 - (E - 126))
+}
+
+// 8 consecutive K values (already scaled) -> NS 16-byte chunks of integer slices
+template <int NS>
+__device__ __forceinline__ void slice8(const float * t_in, uint4 * out) {
+    uint32_t w[NS][4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        float t0 = t_in[2 * q], t1 = t_in[2 * q + 1];
+#pragma unroll
+        for (int a = 0; a < NS; ++a) {
+            const float i0 = rintf(t0), i1 = rintf(t1);
+            const __nv_bfloat162 b = __floats2bfloat162_rn(i0, i1);
+            w[a][q] = *reinterpret_cast<const uint32_t *>(&b);
+            t0 = (t0 - i0) * 256.0f;
+            t1 = (t1 - i1) * 256.0f;
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < NS; ++a) out[a] = make_uint4(w[a][0], w[a][1], w[a][2], w[a][3]);
+}
+
+// One warp per row of op(U): scale over the whole row, then every K-tile's slices.
+// The FP64 row is sliced in double precision (exact residuals).
+template <int NS>
+__global__ void slice_matrix_kernel(const double * __restrict__ U, int n, bool trans, int nkt,
+                                    unsigned char * __restrict__ img, float * __restrict__ inv) {
+    const int row = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+    const int lane = threadIdx.x & 31;
+    if (row >= TB * ((n + TB - 1) / TB)) return;
+    auto at = [&](int k) -> double {
+        if (row >= n || k >= n) return 0.0;
+        return trans ? U[(long long) row * n + k] : U[row + (long long) k * n];
+    };
+    double amax = 0.0;
+    for (int k = lane; k < n; k += 32) amax = fmax(amax, fabs(at(k)));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+    // power of two s with |s U| < 2^7
+    int ex = 0;
+    if (amax > 0) (void) frexp(amax, &ex);                      // amax < 2^ex
+    const double s = amax > 0 ? ldexp(1.0, 7 - ex) : 1.0;
+    if (lane == 0) inv[row] = (float) (1.0 / s);
+    const int it = row / TB, rr = row % TB;
+    for (int kt = 0; kt < nkt; ++kt) {
+        if (lane >= 8) continue;                                // 8 lanes x 8 values = one K-tile row
+        const int k0 = kt * KT + 8 * lane;
+        uint32_t w[NS][4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            double t0 = at(k0 + 2 * q) * s, t1 = at(k0 + 2 * q + 1) * s;
+#pragma unroll
+            for (int a = 0; a < NS; ++a) {
+                const double i0 = rint(t0), i1 = rint(t1);
+                const __nv_bfloat162 b = __floats2bfloat162_rn((float) i0, (float) i1);
+                w[a][q] = *reinterpret_cast<const uint32_t *>(&b);
+                t0 = (t0 - i0) * 256.0;
+                t1 = (t1 - i1) * 256.0;
+            }
+        }
+        unsigned char * base = img + ((long long) it * nkt + kt) * NS * PIECE;
+        const uint32_t off = tc::sw128_offset(rr, 8 * lane);
+#pragma unroll
+        for (int a = 0; a < NS; ++a) *reinterpret_cast<uint4 *>(base + a * PIECE + off) = make_uint4(w[a][0], w[a][1], w[a][2], w[a][3]);
+    }
+}
+
+struct SliceXLaunch {
+    const double * in[kMaxFields];
+    int n, M, nkt, njt;
+    unsigned char * img;
+    float * inv;
+};
+
+// One CTA per (field, class, column tile, chunk), one warp per column at a time:
+// the chunk's 256 rows are read coalesced into shared memory, then each lane
+// slices 8 consecutive rows.
+template <int NS>
+__global__ void __launch_bounds__(256) slice_input_kernel(const __grid_constant__ SliceXLaunch L) {
+    __shared__ float buf[8][256];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nch = (L.nkt + CHUNK_KT - 1) / CHUNK_KT;
+    int b = blockIdx.x;
+    const int q = b % nch; b /= nch;
+    const int jt = b % L.njt; b /= L.njt;
+    const int r = b % 4;
+    const int f = b / 4;
+    const int ncols = class_cols(L.M, r);
+    const long long tile_base = ((long long) (f * 4 + r) * L.njt + jt);
+    for (int ci = warp; ci < TB; ci += 8) {
+        const int j = jt * TB + ci;
+        const bool cok = j < ncols;
+        const double * col = L.in[f] + (long long) (r + 4LL * j) * L.n;
+        float amax = 0.0f;
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const int row = q * (KT * CHUNK_KT) + 32 * e + lane;
+            const float v = (cok && row < L.n) ? (float) __ldcg(col + row) : 0.0f;
+            buf[warp][32 * e + lane] = v;
+            amax = fmaxf(amax, fabsf(v));
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+        const float s = pow2_scale(amax);
+        __syncwarp();
+        float t[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) t[e] = buf[warp][8 * lane + e] * s;
+        __syncwarp();
+        const int kt = q * CHUNK_KT + lane / 8;
+        if (kt < L.nkt) {
+            uint4 ch[NS];
+            slice8<NS>(t, ch);
+            unsigned char * base = L.img + (tile_base * L.nkt + kt) * NS * PIECE;
+            const uint32_t off = tc::sw128_offset(ci, 8 * (lane % 8));
+#pragma unroll
+            for (int a = 0; a < NS; ++a) *reinterpret_cast<uint4 *>(base + a * PIECE + off) = ch[a];
+        }
+        if (lane == 0) L.inv[(tile_base * nch + q) * TB + ci] = 1.0f / s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// the multiply
+// ---------------------------------------------------------------------------
+template <int NU, int NX>
+__global__ void __launch_bounds__(THREADS, 1) trmm_mixed_kernel(const __grid_constant__ MixLaunch L) {
+    using C = Cfg<NU, NX>;
+    constexpr int NL = C::NL;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char * const sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t) 1023);
+    __shared__ __align__(8) uint64_t bar_full[2], bar_empty[2], bar_accf, bar_acce, bar_done;
+    __shared__ uint32_t s_tmem;
+    __shared__ volatile int s_abort;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nch = (L.nkt + CHUNK_KT - 1) / CHUNK_KT;
+
+    if (tid == 0) {
+        for (int i = 0; i < 2; ++i) { tc::mbar_init(&bar_full[i], 1); tc::mbar_init(&bar_empty[i], 1); }
+        tc::mbar_init(&bar_accf, 1);
+        tc::mbar_init(&bar_acce, 256);
+        tc::mbar_init(&bar_done, 1);
+        s_abort = 0;
+    }
+    if (warp == 8) tc::tmem_alloc(&s_tmem, 512);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = s_tmem;
+    auto fail = [&]() { s_abort = 1; atomicExch(L.err, 1); };
+    // chunk index of a K-tile, and whether kt starts / ends a chunk of tile range [k0, k1]
+    auto chunk_start = [&](int kt, int k0) { return kt == k0 || kt % CHUNK_KT == 0; };
+    auto chunk_end = [&](int kt, int k1) { return kt == k1 || kt % CHUNK_KT == CHUNK_KT - 1; };
+
+    if (warp == 9) {
+        if (lane == 0) {
+            unsigned q = 0;
+            for (int t = blockIdx.x; t < L.ntiles && !s_abort; t += gridDim.x) {
+                const MixTile T = L.tiles[t];
+                const unsigned char * ua = L.Uimg[class_matrix(T.cls)] + (long long) T.it * L.nkt * NU * PIECE;
+                const unsigned char * xb = L.Ximg + (((long long) (T.field * 4 + T.cls) * L.njt + T.jt) * L.nkt) * NX * PIECE;
+                for (int kt = T.k0; kt <= T.k1; ++kt, ++q) {
+                    const int st = q & 1, u = q >> 1;
+                    if (!tc::mbar_wait(&bar_empty[st], (u & 1) ^ 1, &s_abort)) { fail(); break; }
+                    tc::mbar_arrive_expect_tx(&bar_full[st], C::STAGE);
+                    tc::bulk_g2s(sm + st * C::STAGE, ua + (long long) kt * NU * PIECE, NU * PIECE, &bar_full[st]);
+                    tc::bulk_g2s(sm + st * C::STAGE + NU * PIECE, xb + (long long) kt * NX * PIECE, NX * PIECE, &bar_full[st]);
+                }
+            }
+        }
+        __syncwarp();
+    } else if (warp == 8) {
+        if (lane == 0) {
+            unsigned q = 0, nacc = 0;
+            const uint32_t s0 = tc::smem_addr(sm);
+            for (int t = blockIdx.x; t < L.ntiles && !s_abort; t += gridDim.x) {
+                const MixTile T = L.tiles[t];
+                for (int kt = T.k0; kt <= T.k1 && !s_abort; ++kt, ++q) {
+                    const int st = q & 1, u = q >> 1;
+                    const bool cs = chunk_start(kt, T.k0);
+                    if (cs) {   // the epilogue has read the previous chunk
+                        if (!tc::mbar_wait(&bar_acce, (nacc & 1) ^ 1, &s_abort)) { fail(); break; }
+                        nacc++;
+                    }
+                    if (!tc::mbar_wait(&bar_full[st], u & 1, &s_abort)) { fail(); break; }
+                    tc::fence_after_sync();
+                    const uint32_t ua = s0 + st * C::STAGE, xb = ua + NU * PIECE;
+#pragma unroll
+                    for (int kk = 0; kk < KT / 16; ++kk)
+#pragma unroll
+                        for (int lv = 0; lv < NL; ++lv) {
+                            const int bmin = lv - (NX - 1) > 0 ? lv - (NX - 1) : 0;
+                            const int bmax = lv < NU - 1 ? lv : NU - 1;
+#pragma unroll
+                            for (int b = bmin; b <= bmax; ++b) {
+                                const int a = lv - b;
+                                // level lv starts afresh with its first product of the chunk
+                                const bool fresh = cs && kk == 0 && b == bmin;
+                                tc::mma_bf16(tmem + lv * TB, tc::desc_sw128(ua + b * PIECE + kk * 32),
+                                             tc::desc_sw128(xb + a * PIECE + kk * 32), IDESC, !fresh);
+                            }
+                        }
+                    tc::commit(&bar_empty[st]);
+                    if (chunk_end(kt, T.k1)) tc::commit(&bar_accf);
+                }
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---- epilogue: lane quarter q4, columns 64 h .. 64 h + 63 of the tile ----
+        const int q4 = warp & 3, h = warp >> 2;
+        const int row_in = 32 * q4 + lane;
+        const uint32_t tbase = tmem + ((uint32_t) (32 * q4) << 16) + 64 * h;
+        unsigned nacc = 0;
+        for (int t = blockIdx.x; t < L.ntiles && !s_abort; t += gridDim.x) {
+            const MixTile T = L.tiles[t];
+            float acc[64];
+#pragma unroll
+            for (int j = 0; j < 64; ++j) acc[j] = 0.0f;
+            const float * xinv = L.Xinv + ((long long) (T.field * 4 + T.cls) * L.njt + T.jt) * nch * TB + 64 * h;
+            for (int kt = T.k0; kt <= T.k1; ++kt) {
+                if (!chunk_end(kt, T.k1)) continue;
+                if (!tc::mbar_wait(&bar_accf, nacc & 1, &s_abort)) { fail(); break; }
+                nacc++;
+                __syncwarp();
+                tc::fence_after_sync();
+                const float * xi = xinv + (long long) (kt / CHUNK_KT) * TB;
+#pragma unroll
+                for (int g = 0; g < 8; ++g) {
+                    uint32_t a[NL][8];
+#pragma unroll
+                    for (int lv = 0; lv < NL; ++lv) tc::tmem_ld8_async(tbase + lv * TB + 8 * g, a[lv]);
+                    tc::tmem_wait_ld();
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) {
+                        float y = __uint_as_float(a[NL - 1][e]);
+#pragma unroll
+                        for (int lv = NL - 2; lv >= 0; --lv) y = fmaf(y, 0.00390625f, __uint_as_float(a[lv][e]));
+                        acc[8 * g + e] = fmaf(y, __ldg(xi + 8 * g + e), acc[8 * g + e]);
+                    }
+                }
+                tc::fence_before_sync();
+                tc::mbar_arrive(&bar_acce);
+            }
+            if (s_abort) break;
+            // out = acc 2^-14 / sU_i
+            const int row = T.it * TB + row_in;
+            if (row < L.n) {
+                const double sc = (double) __ldg(L.Uinv[class_matrix(T.cls)] + row);
+                double * const o = L.out[T.field];
+                const int ncols = class_cols(L.M, T.cls);
+#pragma unroll
+                for (int j = 0; j < 64; ++j) {
+                    const int jj = T.jt * TB + 64 * h + j;
+                    if (jj < ncols) __stcg(o + (long long) (T.cls + 4LL * jj) * L.n + row, (double) acc[j] * sc);
+                }
+            }
+        }
+    }
+
+    __syncthreads();
+    if (warp == 8) {
+        if (lane == 0) {
+            tc::commit(&bar_done);
+            __shared__ volatile int s_never;
+            s_never = 0;
+            if (!tc::mbar_wait(&bar_done, 0, &s_never)) atomicExch(L.err, 2);
+        }
+        __syncwarp();
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tmem, 512);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+struct MixedTrmmPlan {
+    // [slices of U - 3][inverse][trans][matrix]
+    unsigned char * img[2][2][2][2] = {};
+    float * inv[2][2][2][2] = {};
+    int * d_err = nullptr;
+};
+
+struct MixedTrmmWork {
+    int nf = 0, n = 0, M = 0, nkt = 0, njt = 0, nch = 0;
+    unsigned char * ximg = nullptr;      // sliced input (NX = 4 size, either slice count fits)
+    float * xinv = nullptr;
+    MixTile * tiles[2] = {nullptr, nullptr};   // [trans], longest K first
+    int ntiles = 0;
+};
+
+}  // namespace
+
+void mixed_trmm_plan_free(void * p) {
+    MixedTrmmPlan * T = static_cast<MixedTrmmPlan *>(p);
+    if (!T) return;
+    for (auto & a : T->img) for (auto & b : a) for (auto & c : b) for (auto & d : c) cudaFree(d);
+    for (auto & a : T->inv) for (auto & b : a) for (auto & c : b) for (auto & d : c) cudaFree(d);
+    cudaFree(T->d_err);
+    delete T;
+}
+
+void mixed_trmm_work_free(void * p) {
+    MixedTrmmWork * W = static_cast<MixedTrmmWork *>(p);
+    if (!W) return;
+    cudaFree(W->ximg); cudaFree(W->xinv); cudaFree(W->tiles[0]); cudaFree(W->tiles[1]);
+    delete W;
+}
+
+int mixed_trmm_device_error(void * p) {
+    MixedTrmmPlan * T = static_cast<MixedTrmmPlan *>(p);
+    if (!T || !T->d_err) return 0;
+    int v = 0;
+    if (cudaMemcpy(&v, T->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    if (v) cudaMemset(T->d_err, 0, sizeof(int));
+    return v;
+}
+
+// Out = op(U) In for the four column classes of every field (sph), U = P or Pinv of the
+// plan, with nu slices of U (3 or 4) and 3 of the input.  Builds the plan's slice
+// images of op(U) on first use (into *plan_slot) and the batch's work buffers (*work_slot).
+cudaError_t launch_trmm_mixed(HarmonicPlan * H, void ** plan_slot, void ** work_slot, int nu, bool inverse, bool trans,
+                              double * const * in, double * const * out, int nf, int M, cudaStream_t st) {
+    const int n = H->n;
+    const int nkt = (n + KT - 1) / KT, nit = (n + TB - 1) / TB;
+    if (!*plan_slot) *plan_slot = new MixedTrmmPlan();
+    MixedTrmmPlan * T = static_cast<MixedTrmmPlan *>(*plan_slot);
+    if (!T->d_err) {
+        cudaError_t e = cudaMalloc(&T->d_err, sizeof(int));
+        if (e == cudaSuccess) e = cudaMemset(T->d_err, 0, sizeof(int));
+        if (e != cudaSuccess) return e;
+    }
+    const int ui = nu - 3, ii = inverse ? 1 : 0, ti = trans ? 1 : 0;
+    for (int u = 0; u < 2; ++u) {
+        if (T->img[ui][ii][ti][u]) continue;
+        const size_t bytes = (size_t) nit * nkt * nu * PIECE;
+        cudaError_t e = cudaMalloc(&T->img[ui][ii][ti][u], bytes);
+        if (e == cudaSuccess) e = cudaMalloc(&T->inv[ui][ii][ti][u], sizeof(float) * (size_t) nit * TB);
+        if (e != cudaSuccess) return e;
+        const double * U = inverse ? H->dPinv[u] : H->dP[u];
+        const int rows = nit * TB;
+        if (nu == 3) slice_matrix_kernel<3><<<(rows + 7) / 8, 256, 0, st>>>(U, n, trans, nkt, T->img[ui][ii][ti][u], T->inv[ui][ii][ti][u]);
+        else         slice_matrix_kernel<4><<<(rows + 7) / 8, 256, 0, st>>>(U, n, trans, nkt, T->img[ui][ii][ti][u], T->inv[ui][ii][ti][u]);
+        count_launch();
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    MixedTrmmWork * W = static_cast<MixedTrmmWork *>(*work_slot);
+    if (!W) {
+        W = new MixedTrmmWork();
+        *work_slot = W;
+        W->nf = nf; W->n = n; W->M = M; W->nkt = nkt;
+        W->njt = (class_cols(M, 0) + TB - 1) / TB;
+        W->nch = (nkt + CHUNK_KT - 1) / CHUNK_KT;
+        const size_t xbytes = (size_t) nf * 4 * W->njt * nkt * 4 * PIECE;
+        cudaError_t e = cudaMalloc(&W->ximg, xbytes);
+        if (e == cudaSuccess) e = cudaMalloc(&W->xinv, sizeof(float) * (size_t) nf * 4 * W->njt * W->nch * TB);
+        if (e != cudaSuccess) return e;
+        for (int tr = 0; tr < 2; ++tr) {
+            std::vector<std::pair<int, MixTile>> v;
+            for (int f = 0; f < nf; ++f)
+                for (int r = 0; r < 4; ++r)
+                    for (int it = 0; it < nit; ++it)
+                        for (int jt = 0; jt * TB < class_cols(M, r); ++jt) {
+                            const int k0 = tr ? 0 : 2 * it, k1 = tr ? std::min(nkt - 1, 2 * it + 1) : nkt - 1;
+                            v.push_back({k1 - k0 + 1, MixTile{f, r, it, jt, k0, k1}});
+                        }
+            std::stable_sort(v.begin(), v.end(), [](const auto & a, const auto & b) { return a.first > b.first; });
+            std::vector<MixTile> tl;
+            for (auto & x : v) tl.push_back(x.second);
+            W->ntiles = (int) tl.size();
+            e = cudaMalloc(&W->tiles[tr], sizeof(MixTile) * std::max<size_t>(1, tl.size()));
+            if (e == cudaSuccess && !tl.empty()) e = cudaMemcpy(W->tiles[tr], tl.data(), sizeof(MixTile) * tl.size(), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    if (W->nf != nf || W->n != n || W->M != M) return cudaErrorInvalidValue;
+    // slice the input
+    static thread_local SliceXLaunch SX;
+    for (int f = 0; f < nf; ++f) SX.in[f] = in[f];
+    SX.n = n; SX.M = M; SX.nkt = nkt; SX.njt = W->njt;
+    SX.img = W->ximg; SX.inv = W->xinv;
+    const int sgrid = nf * 4 * W->njt * W->nch;
+    slice_input_kernel<3><<<sgrid, 256, 0, st>>>(SX);
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    // multiply
+    static thread_local MixLaunch L;
+    for (int f = 0; f < nf; ++f) L.out[f] = out[f];
+    for (int u = 0; u < 2; ++u) { L.Uimg[u] = T->img[ui][ii][ti][u]; L.Uinv[u] = T->inv[ui][ii][ti][u]; }
+    L.Ximg = W->ximg; L.Xinv = W->xinv;
+    L.tiles = W->tiles[ti]; L.ntiles = W->ntiles;
+    L.n = n; L.M = M; L.nkt = nkt; L.njt = W->njt;
+    L.err = T->d_err;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int ctas = std::min(sms, W->ntiles);
+    if (ctas <= 0) return cudaSuccess;
+    if (nu == 3) {
+        auto kern = trmm_mixed_kernel<3, 3>;
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) Cfg<3, 3>::SMEM);
+        if (e == cudaSuccess) { kern<<<ctas, THREADS, Cfg<3, 3>::SMEM, st>>>(L); e = cudaGetLastError(); }
+    } else {
+        auto kern = trmm_mixed_kernel<4, 3>;
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) Cfg<4, 3>::SMEM);
+        if (e == cudaSuccess) { kern<<<ctas, THREADS, Cfg<4, 3>::SMEM, st>>>(L); e = cudaGetLastError(); }
+    }
+    count_launch();
+    return e;
+}
+
+}  // namespace ftb

@@ -178,11 +178,28 @@ int ft_b200_execute_noalloc_dev(const ft_harmonic_plan * P, int forward, char TR
  * last whole block stay direct.  Not bit-identical to the direct sweeps (the
  * products round differently); the relative 2-norm difference is of the order
  * of 1e-14.  The first call on a plan builds its tile matrices (device memory,
- * about 550 MB at n = 4096); make it before any stream capture. */
+ * about 550 MB at n = 4096); make it before any stream capture.
+ * precision FT_B200_MIXED_BF16 (sph only): the same blocks, each tile product
+ * computed on the tcgen05 tensor cores from three BF16 fixed-point slices per
+ * operand (six slice products, exact FP32 accumulation per order level); a
+ * value is carried between tiles at FP32 accuracy, in global memory the
+ * matrices stay FP64.  The connection multiply stays FP64.  Relative 2-norm
+ * error against the FP64 transform about 1e-6 at n = 256, 8e-6 at n = 4096.
+ * precision FT_B200_MIXED_BF16X4: four slices per operand, ten products;
+ * relative error about 1e-7 at n = 4096.  The first call of either builds
+ * its slice images of the tiles (about 400 / 550 MB at n = 4096). */
 #define FT_B200_FP64 0
 #define FT_B200_FP64_BLOCKED 1
+#define FT_B200_MIXED_BF16 2
+#define FT_B200_MIXED_BF16X4 3
 int ft_b200_execute_shared_dev(const ft_harmonic_plan * P, int forward, char TRANS, double * const * dA, int nfields,
                                int precision, void * stream);
+
+/* Reads and clears the plan's device status word: 0 normally; nonzero when a
+ * wait inside one of its tensor-core kernels gave up (the kernel then stops
+ * early and its output is not valid).  Synchronises with the device.  No
+ * counterpart in the reference, whose kernels have no device waits. */
+int ft_b200_device_status(const ft_harmonic_plan * P);
 
 /* Kind of a plan (FT_B200_SPH / TRI / DISK), or -1. */
 int ft_b200_plan_kind(const ft_harmonic_plan * P);
