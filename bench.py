@@ -1,24 +1,30 @@
 #!/usr/bin/env python
 """Benchmark of the harmonic-conversion hot path on B200.
 
-Workload (one "step"): sph2fourier('N') followed by fourier2sph('N') on one
-field of degree 4095 (n = 4096 rows, M = 8191 columns, column-major), FP64,
-seeded U(-1,1) in the reference's triangular sph layout.  Metric: coefficients
-per second, coeffs/s = fields * n^2 / (t_fwd + t_bwd).
+Headline workload (one "step"): sph2fourier('N') followed by fourier2sph('N') on
+16 fields of degree 4095 sharing one plan (n = 4096 rows, M = 8191 columns each,
+column-major), seeded U(-1,1) in the reference's triangular sph layout, through
+ft_b200_execute_shared_dev with the four-slice split-BF16 tensor-core path
+(MIXED_BF16X4).  Metric: coefficients per second, fields * n^2 / (t_fwd + t_bwd),
+reported beside the plain FP64 GPU path on the same fields (their ratio) and the
+relative 2-norm / max errors of the mixed result against the FP64 transform.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n 4096]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n 4096] [--fields 16]
 
 Under torchrun (N > 1) every rank runs an independent replica on its own
-field (the path has no exchange step); the step time is the max over ranks.
+fields (the path has no exchange step); the step time is the max over ranks.
 
 Arms:
   ours       the CUDA library: device-resident timing (value), roofline of the
              dominant kernel from CUDA events recorded around each launch on its
-             stream, end-to-end timing through the host drop-in API (e2e), and the
-             reference's CPU build timed on a sample of the same workload.
+             stream, end-to-end timing with the fields copied from and to pinned
+             host memory inside the timed region (e2e), and the reference's CPU
+             build timed on a sample of the same workload; the secondary
+             workloads (plain FP64 single field, uneven batch, every precision of
+             the shared-plan call, tri / disk) follow under "workloads".
   reference  the reference FastTransforms library compiled from its own sources
              (oracle/_ref/libft_ref.so, OpenMP + its AVX kernels + OpenBLAS), run
-             on the host cores for the same workload and metric.
+             on the host cores, one field of the workload per step.
 """
 from __future__ import annotations
 
@@ -195,12 +201,50 @@ def run_reference(args, rank, world):
             "steps": len(ts), "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(ts),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic: seeded U(-1,1) in the sph triangular layout",
-            "config": {"workload": f"sph2fourier+fourier2sph FP64, degree {n - 1} (n={n}, M={M}), 1 field, host CPU",
-                       "n": n, "fields": 1},
+            "config": {"workload": f"sph2fourier+fourier2sph FP64, degree {n - 1} (n={n}, M={M}), host CPU; "
+                                   f"each step is one of the {args.fields} fields of the shared-plan workload",
+                       "n": n, "fields_per_step": 1},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
-                             "sample": f"{len(ts)} steps of the full workload, OMP threads = BLAS threads = {threads}"},
+                             "sample": f"{len(ts)} steps of one field each (the reference has no batch call; a field "
+                                       f"is the workload's unit), OMP threads = BLAS threads = {threads}"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+def block_split_rotations(n: int, blk: int = 32):
+    """Rotations of one sph hi2lo over all orders, split into those of whole blocks of
+    `blk` sweeps (the tensor-core products) and the heads above them (direct kernel)."""
+    heads = blocks = 0
+    for m in range(2, n):
+        p = m % 2
+        h = ((m - p) // 2) % blk                 # head sweeps j = m-2, ..., m - 2h
+        for j in range(m - 2, p - 1, -2):
+            r = 2 * (n - 2 - j)
+            if j >= m - 2 * h:
+                heads += r
+            else:
+                blocks += r
+    return blocks, heads
+
+
+def block_tiles(n: int, nf: int, blk: int = 32, tl: int = 32) -> int:
+    """Tile products (128 columns x both chains each) of the blocked stage for nf fields."""
+    mlast = n - 1
+    nbeta = (n - 1) // (2 * blk)
+
+    def kmax(p, beta):
+        j0 = p + 2 * blk * beta + 2 * blk - 2
+        x = n - 3 - j0
+        t0 = x // 2 if x >= 0 else -((1 - x) // 2)
+        return t0 // tl if t0 >= 0 else -1
+    tiles = 0
+    for p in range(2):
+        band = 1
+        while p + 2 * blk * band <= mlast:
+            if band <= nbeta:
+                tiles += sum(kmax(p, b) + 2 for b in range(band))
+            band += 1
+    return tiles * ((nf + 1) // 2)
 
 
 def run_ours(args, rank, world, local_rank, dist):
@@ -211,24 +255,43 @@ def run_ours(args, rank, world, local_rank, dist):
     torch.cuda.set_device(local_rank)
     dev = torch.cuda.current_device()
     props = torch.cuda.get_device_properties(dev)
-    n = args.n
+    n, nf = args.n, args.fields
     M = 2 * n - 1
-    A = ft.sphrand(n, SEED + rank)
+    prec = ft.MIXED_BF16X4
     P = ft.plan_sph2fourier(n)
-    d = torch.from_numpy(A.ravel(order="F").copy()).cuda()
+    host = [ft.sphrand(n, SEED + rank * nf + f) for f in range(nf)]
+    d = [torch.from_numpy(A.ravel(order="F").copy()).cuda() for A in host]
+    ptrs = [t.data_ptr() for t in d]
     stream = torch.cuda.current_stream()
     sptr = stream.cuda_stream
 
-    def step():
-        ft.execute_dev(P, True, "N", d.data_ptr(), n, M, sptr)
-        ft.execute_dev(P, False, "N", d.data_ptr(), n, M, sptr)
+    def step(pr=prec):
+        ft.execute_shared_dev(P, True, "N", ptrs, pr, sptr)
+        ft.execute_shared_dev(P, False, "N", ptrs, pr, sptr)
 
-    # accuracy of one fwd+bwd from the seeded input
-    step()
-    back = d.cpu().numpy().reshape((n, M), order="F")
-    eps2 = float(np.linalg.norm(back - A) / np.linalg.norm(A))
-    epsinf = float(np.abs(back - A).max() / np.abs(A).max())
-    d.copy_(torch.from_numpy(A.ravel(order="F").copy()))
+    def reset():
+        for t, A in zip(d, host):
+            t.copy_(torch.from_numpy(A.ravel(order="F")))
+
+    # accuracy against the FP64 transform (the direct FP64 path, parity-pinned to the
+    # oracle at 1e-14): forward and round trip, all fields (builds every table first)
+    ft.execute_shared_dev(P, True, "N", ptrs, ft.FP64, sptr)
+    ref_fwd = [t.clone() for t in d]
+    reset()
+    ft.execute_shared_dev(P, True, "N", ptrs, prec, sptr)
+    fw = torch.cat(d)
+    rf = torch.cat(ref_fwd)
+    eps2 = float(torch.linalg.norm(fw - rf) / torch.linalg.norm(rf))
+    epsinf = float((fw - rf).abs().max() / rf.abs().max())
+    del fw, rf, ref_fwd
+    ft.execute_shared_dev(P, False, "N", ptrs, prec, sptr)
+    back = torch.cat(d)
+    src = torch.cat([torch.from_numpy(A.ravel(order="F")) for A in host]).cuda()
+    rt2 = float(torch.linalg.norm(back - src) / torch.linalg.norm(src))
+    rtinf = float((back - src).abs().max() / src.abs().max())
+    del back, src
+    status = ft.device_status(P)
+    reset()
 
     for _ in range(args.warmup):
         step()
@@ -253,68 +316,102 @@ def run_ours(args, rank, world, local_rank, dist):
         dist.barrier()
     clocks = sampler.stop()
     launches = ft.kernel_launches() - launches0
-    rot_ms, rot_n = ft.profile_read(0)
-    trmm_ms, trmm_n = ft.profile_read(1)
+    fam = {name: ft.profile_read(i) for i, name in enumerate(("heads", "trmm", "transposes", "blocks"))}
     ft.profile(False)
     ms = e0.elapsed_time(e1)
     if dist is not None:
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    value = world * n * n * args.steps / (ms * 1e-3)
+    coeffs = nf * n * n
+    value = world * coeffs * args.steps / (ms * 1e-3)
 
-    # end to end through the drop-in host API: each call stages its input from
-    # pinned host memory and reads its result back
-    hbuf = torch.empty(n * M, dtype=torch.float64, pin_memory=True)
-    hbuf.copy_(torch.from_numpy(A.ravel(order="F")))
-    Ah = hbuf.numpy().reshape((M, n)).T
-    assert Ah.flags.f_contiguous
-    ft.execute_sph2fourier("N", P, Ah)
-    ft.execute_fourier2sph("N", P, Ah)
-    e2e_steps = max(1, min(args.steps, 10))
+    # the same fields through the plain FP64 path
+    psteps = max(2, args.steps // 3)
+    for _ in range(2):
+        step(ft.FP64)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    e0.record(stream)
+    for _ in range(psteps):
+        step(ft.FP64)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    pms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([pms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        pms = float(t.item())
+    plain_value = world * coeffs * psteps / (pms * 1e-3)
+
+    # end to end through the C-ABI call: every step copies the fields in from pinned
+    # host memory, runs forward and backward, and copies the results back
+    hb = [torch.from_numpy(A.ravel(order="F").copy()).pin_memory() for A in host]
+    e2e_steps = max(1, min(args.steps, 3))
+    for t, h in zip(d, hb):
+        t.copy_(h, non_blocking=True)
+    step()
+    for t, h in zip(d, hb):
+        h.copy_(t, non_blocking=True)
+    torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        ft.execute_sph2fourier("N", P, Ah)
-        ft.execute_fourier2sph("N", P, Ah)
+        for t, h in zip(d, hb):
+            t.copy_(h, non_blocking=True)
+        step()
+        for t, h in zip(d, hb):
+            h.copy_(t, non_blocking=True)
+        torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     if dist is not None:
         t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e_value = world * n * n * e2e_steps / e2e_s
+    e2e_value = world * coeffs * e2e_steps / e2e_s
     bytes_mat = n * M * 8
+    del hb
 
     if rank != 0:
+        del d
         P.close()
         return
-    # roofline of the dominant kernel family
+    # roofline of the dominant kernel: the split-BF16 tile products of the blocked sweeps
     peaks = measured_peaks()
     fp64 = fp64_peak_tflops(torch)
-    rot_flops = 6 * rotations_sph(n)
-    tr_flops = trmm_flops(n, M)
-    fam = "rotations" if rot_ms >= trmm_ms else "trmm"
-    per_launch_ms = (rot_ms / max(rot_n, 1)) if fam == "rotations" else (trmm_ms / max(trmm_n, 1))
-    flops = rot_flops if fam == "rotations" else tr_flops
-    achieved = flops / (per_launch_ms * 1e-3) / 1e12
+    bf16 = peaks.get("bf16_tflops") or 1590.0
+    rb, rh = block_split_rotations(n)
+    blk_ms, blk_n = fam["blocks"]
+    per_launch = blk_ms / max(blk_n, 1)
+    alg_flops = 6 * rb * nf                                     # algorithmic: the rotations the blocks apply
+    tiles = block_tiles(n, nf)
+    products = 10                                               # four slices, levels <= 3
+    issued = tiles * 2 * products * 2 * 128 * 64 * 64           # MMA flops the kernel issues
+    achieved = alg_flops / (per_launch * 1e-3) / 1e12
+    # the algorithmic rate at which the tensor pipe is saturated: BF16 peak over the ten
+    # slice products and the 4/3 of a 64 x 64 tile product over its 32 x 32 rotations
+    alg_peak = bf16 / (products * 4.0 / 3.0)
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get(f"sph_n{n}", {}).get(fam)
+            traffic = json.load(open(tpath)).get(f"shared{nf}_n{n}", {}).get("blocked_mixed_kernel")
         except Exception:
             traffic = None
-    total_flops = 2 * (rot_flops + tr_flops)
     roofline = {
-        "bound": "fp64", "kernel": "rot_kernel (Givens sweeps)" if fam == "rotations" else "gemm_tri_kernel (DMMA trmm)",
-        "achieved": achieved, "peak": fp64, "unit": "TFLOP/s", "frac": achieved / fp64, "traffic": traffic,
-        "peak_source": "measured in bench.py: cuBLAS DGEMM 8192^3 burst (MEASURED_PEAKS.json has no FP64 entry)",
-        "flops_per_launch": flops, "ms_per_launch": per_launch_ms,
-        "families_ms_per_step": {"rotations": rot_ms / args.steps, "trmm": trmm_ms / args.steps},
-        "step_fp64_frac": total_flops / (ms / args.steps * 1e-3) / 1e12 / fp64 if ms > 0 else None,
+        "bound": "tensor", "kernel": "blocked_mixed_kernel (tcgen05 split-BF16 tile products, 4 slices)",
+        "achieved": achieved, "peak": alg_peak, "unit": "TFLOP/s", "frac": achieved / alg_peak, "traffic": traffic,
+        "peak_source": f"MEASURED_PEAKS.json bf16_tflops {bf16} (burst) / (10 products x 4/3 tile overhead)",
+        "algorithmic_flops_per_launch": alg_flops, "ms_per_launch": per_launch,
+        "tensor_flops_issued_per_launch": issued,
+        "tensor_pipe_frac": issued / (per_launch * 1e-3) / 1e12 / bf16,
+        "fp64_equivalent_frac": achieved / fp64, "fp64_peak_tflops": fp64,
+        "families_ms_per_step": {k: v[0] / args.steps for k, v in fam.items()},
         "hbm_peak_gbs": peaks.get("hbm_gbs"),
     }
+    del d
     P.close()
     extra = None
     if not args.no_extra:
@@ -333,23 +430,101 @@ def run_ours(args, rank, world, local_rank, dist):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic: seeded U(-1,1) in the sph triangular layout (splitmix64, seed 20261203 + rank)",
-        "config": {"workload": f"plain FP64 sph2fourier+fourier2sph, degree {n - 1} (n={n}, M={M}), "
-                               f"1 field per GPU, device-resident plan",
-                   "n": n, "M": M, "fields_per_gpu": 1, "parallelism": f"replicas x{world}",
-                   "l2": f"inputs larger than L2: A {bytes_mat / 1e6:.0f} MB, rotation table "
-                         f"{16 * n * (n + 1) // 2 / 1e6:.0f} MB, connection matrices {4 * 8 * n * n / 1e6:.0f} MB"},
-        "accuracy": {"roundtrip_eps2": eps2, "roundtrip_epsinf": epsinf},
+        "vs_baseline": None, "dtype": "bf16x4 slices / f32 acc (f64 in and out)",
+        "data": "synthetic: seeded U(-1,1) in the sph triangular layout (splitmix64, seed 20261203 + field)",
+        "config": {"workload": f"batched mixed-precision sph2fourier+fourier2sph: {nf} fields of degree {n - 1} "
+                               f"(n={n}, M={M}) sharing one plan, MIXED_BF16X4, per GPU",
+                   "n": n, "M": M, "fields_per_gpu": nf, "precision": "MIXED_BF16X4", "parallelism": f"replicas x{world}",
+                   "l2": f"inputs larger than L2: {nf} fields x {bytes_mat / 1e6:.0f} MB"},
+        "vs_plain_fp64": {"plain_fp64_value": plain_value, "plain_fp64_ms_per_step": pms / psteps,
+                          "ratio": value / plain_value, "plain": "FT_B200_FP64 direct sweeps + DMMA trmm, same fields"},
+        "accuracy": {"fwd_eps2_vs_fp64": eps2, "fwd_epsinf_vs_fp64": epsinf, "roundtrip_eps2": rt2,
+                     "roundtrip_epsinf": rtinf, "device_status": status,
+                     "reference": "FT_B200_FP64 output (matches the oracle to 1e-14)"},
         "roofline": roofline,
         "cpu_baseline": cpu,
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * bytes_mat, "d2h_bytes_per_step": 2 * bytes_mat,
-                "api": "ft_execute_sph2fourier + ft_execute_fourier2sph on pinned host arrays", "steps": e2e_steps},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nf * bytes_mat, "d2h_bytes_per_step": nf * bytes_mat,
+                "api": "ft_b200_execute_shared_dev (fwd, bwd) with the fields copied in from and out to pinned host memory",
+                "steps": e2e_steps},
         "gpu_launches": launches,
         "clocks": clocks,
         "workloads": extra,
     }
     print(json.dumps(line))
+
+
+def plain_single(args, torch, ft):
+    """Plain FP64 drop-in, one field of degree n - 1 (device-resident), with the FP64
+    roofline of its dominant kernel family."""
+    import numpy as np
+    n = args.n
+    M = 2 * n - 1
+    A = ft.sphrand(n, SEED)
+    P = ft.plan_sph2fourier(n)
+    d = torch.from_numpy(A.ravel(order="F").copy()).cuda()
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+
+    def step():
+        ft.execute_dev(P, True, "N", d.data_ptr(), n, M, sptr)
+        ft.execute_dev(P, False, "N", d.data_ptr(), n, M, sptr)
+    step()
+    back = d.cpu().numpy().reshape((n, M), order="F")
+    eps2 = float(np.linalg.norm(back - A) / np.linalg.norm(A))
+    epsinf = float(np.abs(back - A).max() / np.abs(A).max())
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    steps = max(5, args.steps // 2)
+    ft.profile(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    rot_ms, rot_n = ft.profile_read(0)
+    trmm_ms, trmm_n = ft.profile_read(1)
+    ft.profile(False)
+    ms = e0.elapsed_time(e1)
+    # end to end through the drop-in host API (pinned host array)
+    hbuf = torch.empty(n * M, dtype=torch.float64, pin_memory=True)
+    hbuf.copy_(torch.from_numpy(A.ravel(order="F")))
+    Ah = hbuf.numpy().reshape((M, n)).T
+    ft.execute_sph2fourier("N", P, Ah)
+    ft.execute_fourier2sph("N", P, Ah)
+    t0 = time.perf_counter()
+    for _ in range(3):
+        ft.execute_sph2fourier("N", P, Ah)
+        ft.execute_fourier2sph("N", P, Ah)
+    e2e = n * n * 3 / (time.perf_counter() - t0)
+    P.close()
+    fp64 = fp64_peak_tflops(torch)
+    rot_flops = 6 * rotations_sph(n)
+    tr_flops = trmm_flops(n, M)
+    famname = "rotations" if rot_ms >= trmm_ms else "trmm"
+    per_launch = (rot_ms / max(rot_n, 1)) if famname == "rotations" else (trmm_ms / max(trmm_n, 1))
+    flops = rot_flops if famname == "rotations" else tr_flops
+    achieved = flops / (per_launch * 1e-3) / 1e12
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(f"sph_n{n}", {}).get(famname)
+        except Exception:
+            traffic = None
+    total = 2 * (rot_flops + tr_flops)
+    return {
+        "coeffs_per_s": n * n * steps / (ms * 1e-3), "ms_per_step": ms / steps,
+        "workload": f"plain FP64 sph2fourier+fourier2sph, degree {n - 1}, 1 field, device-resident plan",
+        "roundtrip_eps2": eps2, "roundtrip_epsinf": epsinf,
+        "e2e_coeffs_per_s": e2e, "e2e_api": "ft_execute_sph2fourier + ft_execute_fourier2sph on a pinned host array",
+        "roofline": {"bound": "fp64", "kernel": "rot_kernel (Givens sweeps)" if famname == "rotations" else "gemm_tri_kernel (DMMA trmm)",
+                     "achieved": achieved, "peak": fp64, "unit": "TFLOP/s", "frac": achieved / fp64, "traffic": traffic,
+                     "peak_source": "measured in bench.py: cuBLAS DGEMM 8192^3 burst",
+                     "flops_per_launch": flops, "ms_per_launch": per_launch,
+                     "families_ms_per_step": {"rotations": rot_ms / steps, "trmm": trmm_ms / steps},
+                     "step_fp64_frac": total / (ms / steps * 1e-3) / 1e12 / fp64}}
 
 
 def profile_case(n: int) -> None:
@@ -371,7 +546,7 @@ def profile_case(n: int) -> None:
 def extra_workloads(args, torch, ft):
     """Secondary workloads (reported beside the headline, same device timing rules)."""
     import numpy as np
-    out = {}
+    out = {"plain_fp64_n%d" % args.n: plain_single(args, torch, ft)}
     st = torch.cuda.current_stream()
     sp = st.cuda_stream
 
@@ -419,7 +594,7 @@ def extra_workloads(args, torch, ft):
     del g, data
     for p in plans.values():
         p.close()
-    # 16 fields of degree 4095 sharing one plan: direct FP64 vs blocked FP64 (tensor-core products)
+    # 16 fields of degree 4095 sharing one plan: every precision of ft_b200_execute_shared_dev
     n = 4096
     Pn = ft.plan_sph2fourier(n)
     M = Pn.M
@@ -427,8 +602,10 @@ def extra_workloads(args, torch, ft):
     fptr = [f.data_ptr() for f in fields]
     res = {}
     ref_out = None
-    for name, prec in (("fp64_direct", ft.FP64), ("fp64_blocked", ft.FP64_BLOCKED)):
-        x0 = fields[0].clone()
+    field0 = fields[0].clone()   # the fields below are transformed in place; errors start from this copy
+    for name, prec in (("fp64_direct", ft.FP64), ("fp64_blocked", ft.FP64_BLOCKED), ("mixed_bf16_3slices", ft.MIXED_BF16),
+                       ("mixed_bf16_4slices", ft.MIXED_BF16X4)):
+        x0 = field0.clone()
         ft.execute_shared_dev(Pn, True, "N", [x0.data_ptr()], prec, sp)   # builds tables outside timing
         torch.cuda.synchronize()
         if ref_out is None:
@@ -443,7 +620,7 @@ def extra_workloads(args, torch, ft):
         step()
         ms = timed(step, 3)
         res[name] = {"coeffs_per_s": 16 * n * n / (ms * 1e-3), "ms_per_step": ms,
-                     "eps2_fwd_vs_fp64_direct": err}
+                     "eps2_fwd_vs_fp64_direct": err, "fields": "seeds 20261303 + f (field 0 for the error)"}
     out["shared_16_n4096"] = res
     del fields
     Pn.close()
@@ -474,10 +651,11 @@ def extra_workloads(args, torch, ft):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=12)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=4096)
+    ap.add_argument("--fields", type=int, default=16, help="fields sharing one plan in the headline workload")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the secondary workloads")
     ap.add_argument("--cpu-sample", action="store_true", help=argparse.SUPPRESS)

@@ -644,14 +644,19 @@ int execute_batch_chunk(HarmonicPlan * const * H, bool forward, char TRANS, doub
     // blocked products of the whole blocks, in place on the scratch matrices
     auto blocks = [&](bool hi2lo) -> bool {
         if (!blocked) return true;
-        prof_begin(FAM_BLOCK, st);
         if (!mixed) {
+            prof_begin(FAM_BLOCK, st);
             const cudaError_t e = launch_blocked(H[0]->blocked, hi2lo, S.data(), nf, N[0], M[0], B->blk_tasks, B->d_counter, st);
             prof_end(st);
             return cuda_ok(e, "blocked kernel");
         }
+        prof_begin(FAM_OTHER, st);
         cudaError_t e = launch_blocked_transpose(H[0]->blocked, true, S.data(), nf, N[0], M[0], B->d_T, B->mx_tasks, st);
+        prof_end(st);
+        prof_begin(FAM_BLOCK, st);
         if (e == cudaSuccess) e = launch_blocked_mixed(H[0]->blocked, ns, hi2lo, B->d_T, N[0], M[0], B->mx_tasks, B->d_counter, st);
+        prof_end(st);
+        prof_begin(FAM_OTHER, st);
         if (e == cudaSuccess) e = launch_blocked_transpose(H[0]->blocked, false, S.data(), nf, N[0], M[0], B->d_T, B->mx_tasks, st);
         prof_end(st);
         return cuda_ok(e, "blocked kernels");
