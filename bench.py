@@ -4,8 +4,8 @@
 Headline workload (one "step"): sph2fourier('N') followed by fourier2sph('N') on
 16 fields of degree 4095 sharing one plan (n = 4096 rows, M = 8191 columns each,
 column-major), seeded U(-1,1) in the reference's triangular sph layout, through
-ft_b200_execute_shared_dev with the four-slice split-BF16 tensor-core path
-(MIXED_BF16X4).  Metric: coefficients per second, fields * n^2 / (t_fwd + t_bwd),
+ft_b200_execute_shared_dev with the split-BF16 tensor-core path (MIXED_BF16:
+three 9-bit slices per operand in the blocked sweeps).  Metric: coefficients per second, fields * n^2 / (t_fwd + t_bwd),
 reported beside the plain FP64 GPU path on the same fields (their ratio) and the
 relative 2-norm / max errors of the mixed result against the FP64 transform.
 
@@ -257,7 +257,7 @@ def run_ours(args, rank, world, local_rank, dist):
     props = torch.cuda.get_device_properties(dev)
     n, nf = args.n, args.fields
     M = 2 * n - 1
-    prec = ft.MIXED_BF16X4
+    prec = ft.MIXED_BF16
     P = ft.plan_sph2fourier(n)
     host = [ft.sphrand(n, SEED + rank * nf + f) for f in range(nf)]
     d = [torch.from_numpy(A.ravel(order="F").copy()).cuda() for A in host]
@@ -387,10 +387,10 @@ def run_ours(args, rank, world, local_rank, dist):
     per_launch = blk_ms / max(blk_n, 1)
     alg_flops = 6 * rb * nf                                     # algorithmic: the rotations the blocks apply
     tiles = block_tiles(n, nf)
-    products = 10                                               # four slices, levels <= 3
+    products = 8                                                # three slices, levels <= 3
     issued = tiles * 2 * products * 2 * 128 * 64 * 64           # MMA flops the kernel issues
     achieved = alg_flops / (per_launch * 1e-3) / 1e12
-    # the algorithmic rate at which the tensor pipe is saturated: BF16 peak over the ten
+    # the algorithmic rate at which the tensor pipe is saturated: BF16 peak over the eight
     # slice products and the 4/3 of a 64 x 64 tile product over its 32 x 32 rotations
     alg_peak = bf16 / (products * 4.0 / 3.0)
     traffic = None
@@ -401,9 +401,9 @@ def run_ours(args, rank, world, local_rank, dist):
         except Exception:
             traffic = None
     roofline = {
-        "bound": "tensor", "kernel": "blocked_mixed_kernel (tcgen05 split-BF16 tile products, 4 slices)",
+        "bound": "tensor", "kernel": "blocked_mixed_kernel (tcgen05 split-BF16 tile products, 3 slices)",
         "achieved": achieved, "peak": alg_peak, "unit": "TFLOP/s", "frac": achieved / alg_peak, "traffic": traffic,
-        "peak_source": f"MEASURED_PEAKS.json bf16_tflops {bf16} (burst) / (10 products x 4/3 tile overhead)",
+        "peak_source": f"MEASURED_PEAKS.json bf16_tflops {bf16} (burst) / (8 products x 4/3 tile overhead)",
         "algorithmic_flops_per_launch": alg_flops, "ms_per_launch": per_launch,
         "tensor_flops_issued_per_launch": issued,
         "tensor_pipe_frac": issued / (per_launch * 1e-3) / 1e12 / bf16,
@@ -430,11 +430,11 @@ def run_ours(args, rank, world, local_rank, dist):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "bf16x4 slices / f32 acc (f64 in and out)",
+        "vs_baseline": None, "dtype": "bf16 slices (3 per operand) / f32 exact acc (f64 in and out)",
         "data": "synthetic: seeded U(-1,1) in the sph triangular layout (splitmix64, seed 20261203 + field)",
         "config": {"workload": f"batched mixed-precision sph2fourier+fourier2sph: {nf} fields of degree {n - 1} "
-                               f"(n={n}, M={M}) sharing one plan, MIXED_BF16X4, per GPU",
-                   "n": n, "M": M, "fields_per_gpu": nf, "precision": "MIXED_BF16X4", "parallelism": f"replicas x{world}",
+                               f"(n={n}, M={M}) sharing one plan, MIXED_BF16, per GPU",
+                   "n": n, "M": M, "fields_per_gpu": nf, "precision": "MIXED_BF16", "parallelism": f"replicas x{world}",
                    "l2": f"inputs larger than L2: {nf} fields x {bytes_mat / 1e6:.0f} MB"},
         "vs_plain_fp64": {"plain_fp64_value": plain_value, "plain_fp64_ms_per_step": pms / psteps,
                           "ratio": value / plain_value, "plain": "FT_B200_FP64 direct sweeps + DMMA trmm, same fields"},

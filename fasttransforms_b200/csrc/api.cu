@@ -610,7 +610,9 @@ int execute_batch_chunk(HarmonicPlan * const * H, bool forward, char TRANS, doub
             std::vector<double *> in(nf), out(nf);
             for (int f = 0; f < nf; f++) { in[f] = from_A ? A[f] : S[f]; out[f] = from_A ? S[f] : A[f]; }
             prof_begin(FAM_TRMM, st);
-            const cudaError_t e = launch_trmm_mixed(H[0], &H[0]->mixed_trmm, &B->mx_trmm, ns, inverse, mode == 1,
+            // four slices of the connection matrix for both block precisions: its K runs over all
+            // n rows, where three slices would cost about 2e-6 at n = 4096
+            const cudaError_t e = launch_trmm_mixed(H[0], &H[0]->mixed_trmm, &B->mx_trmm, 4, inverse, mode == 1,
                                                     in.data(), out.data(), nf, M[0], st);
             prof_end(st);
             return cuda_ok(e, "tensor-core trmm");

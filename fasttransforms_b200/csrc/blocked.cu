@@ -215,19 +215,19 @@ __global__ void __launch_bounds__(NT, 1) blocked_kernel(const __grid_constant__ 
 // BF16 pieces per operand on the tensor cores with FP32 accumulation.  The
 // pieces are fixed-point slices (the Ozaki splitting), not floating ones: a
 // window column x (64 positions) is scaled by a power of two s so that
-// |s x| < 2^7, and
-//   s x = i_0 + i_1 2^-8 + ... + i_{NS-1} 2^-8(NS-1),   integers |i_a| <= 2^7,
+// |s x| < 2^8, and
+//   s x = i_0 + i_1 2^-9 + ... + i_{NS-1} 2^-9(NS-1),   integers |i_a| <= 2^8,
 // each rounded to nearest; a tile matrix entry (|q| <= 1) likewise with the
-// fixed scale 2^7 (slices j_b).  Integers of that size are exact in BF16,
-// every product i_a j_b is an integer below 2^14, and the products of one
-// order level L = a + b go to their own FP32 accumulator in tensor memory.
-// Levels L <= NS - 1 are kept (NS (NS + 1) / 2 products: 6 for NS = 3, 10 for
-// NS = 4); a level sums at most 4 x 64 such products, below 2^22, so the
-// accumulation is exact whatever rounding the tensor core applies.  The
-// epilogue recombines
-//   y = (A_0 + 2^-8 A_1 + ... ) 2^-7 / s
+// fixed scale 2^8 (slices j_b).  Integers up to 2^8 are exact in BF16 (eight
+// significant bits), every product i_a j_b is an integer of magnitude at most
+// 2^16, and the products of one order level L = a + b go to their own FP32
+// accumulator in tensor memory.  Levels L <= 3 are kept (NS = 3: eight
+// products, NS = 4: ten); a level sums at most 4 x 64 such products, at most
+// 2^24 in magnitude, so the accumulation is exact whatever rounding the tensor
+// core applies.  The epilogue recombines
+//   y = (A_0 + 2^-9 A_1 + ... ) 2^-8 / s
 // in FP32 with round-to-nearest.  The errors are the slicing and the dropped
-// levels (relative order 2^-8 NS of the window's largest entry and of the
+// levels (relative order 2^-9 NS of the window's largest entry and of the
 // tile matrix entries, summed over the 64 products of a row) and the FP32
 // rounding of y, all unbiased; a window position is carried between tiles as
 // FP32, in global memory the matrix stays FP64.
@@ -247,12 +247,11 @@ constexpr int MX_PIECE = MX_COLS * WIN * 2;           // bytes of one BF16 piece
 constexpr int MX_QPIECE = WIN * WIN * 2;              // bytes of one BF16 piece of one tile matrix
 constexpr int MX_THREADS = 576;                       // 16 epilogue warps, MMA warp, loader warp
 constexpr uint32_t MX_IDESC = tc::idesc_bf16(MX_COLS, WIN);
-constexpr int MX_TMEM_COLS = 512;                     // 2 chains x NS levels x WIN accumulator columns
+constexpr int MX_TMEM_COLS = 512;                     // 2 chains x 4 levels x WIN accumulator columns
 
 template <int NS> struct MxCfg {
     static constexpr int QCHAIN = NS * MX_QPIECE;     // one chain's tile image
     static constexpr size_t SMEM = 2 * NS * (size_t) MX_PIECE + 2 * (size_t) QCHAIN + 1024;
-    static_assert(2 * NS * WIN <= MX_TMEM_COLS, "accumulators exceed tensor memory");
     static_assert(SMEM <= 227 * 1024, "shared memory");
 };
 
@@ -289,26 +288,26 @@ __global__ void build_img_kernel(const double * __restrict__ Q, long long qb, in
     unsigned char * out = reinterpret_cast<unsigned char *>(img) + ((qb / 2 + k1) * 2 + c) * (long long) MxCfg<NS>::QCHAIN;
     for (int e = threadIdx.x; e < WIN * WIN; e += blockDim.x) {
         const int o = e / WIN, w = e % WIN;
-        // 128 q = j_0 + j_1 2^-8 + ..., integers |j| <= 2^7
-        double t = (transpose ? q[(long long) w * WIN + o] : q[e]) * 128.0;
+        // 256 q = j_0 + j_1 2^-9 + ..., integers |j| <= 2^8
+        double t = (transpose ? q[(long long) w * WIN + o] : q[e]) * 256.0;
         const uint32_t off = tc::sw128_offset(o, w);
         for (int b = 0; b < NS; ++b) {
             const double j = rint(t);
             *reinterpret_cast<__nv_bfloat16 *>(out + b * MX_QPIECE + off) = __float2bfloat16_rn((float) j);
-            t = (t - j) * 256.0;
+            t = (t - j) * 512.0;
         }
     }
 }
 
-// Power-of-two scale s with |s x| < 2^7 for every |x| <= amax (s = 1 for amax = 0).
+// Power-of-two scale s with |s x| < 2^8 for every |x| <= amax (s = 1 for amax = 0).
 __device__ __forceinline__ float slice_scale(float amax) {
     int E = (int) ((__float_as_uint(amax) >> 23) & 0xFF);   // amax < 2^(E - 126)
     if (E < 8) E = 8;                                         // tiny or zero windows
-    return __uint_as_float((uint32_t) (260 - E) << 23);       // 2^(7 - (E - 126))
+    return __uint_as_float((uint32_t) (261 - E) << 23);       // 2^(8 - (E - 126))
 }
 
 // eight consecutive window positions, scaled by s, -> NS 16-byte chunks of
-// integer-valued BF16 slices: s x = i_0 + i_1 2^-8 + ...
+// integer-valued BF16 slices: s x = i_0 + i_1 2^-9 + ...
 template <int NS>
 __device__ __forceinline__ void slice8(const float * v, float s, uint4 * out) {
     uint32_t w[NS][4];
@@ -320,22 +319,25 @@ __device__ __forceinline__ void slice8(const float * v, float s, uint4 * out) {
             const float i0 = rintf(t0), i1 = rintf(t1);
             const __nv_bfloat162 b = __floats2bfloat162_rn(i0, i1);
             w[a][q] = *reinterpret_cast<const uint32_t *>(&b);
-            t0 = (t0 - i0) * 256.0f;
-            t1 = (t1 - i1) * 256.0f;
+            t0 = (t0 - i0) * 512.0f;
+            t1 = (t1 - i1) * 512.0f;
         }
     }
 #pragma unroll
     for (int a = 0; a < NS; ++a) out[a] = make_uint4(w[a][0], w[a][1], w[a][2], w[a][3]);
 }
 
-template <bool HI2LO, int NS>
+// NS slices per operand; products of levels 0 .. LV, one accumulator per level
+template <bool HI2LO, int NS, int LV>
 __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __grid_constant__ MixedLaunch L) {
     constexpr int QCHAIN = MxCfg<NS>::QCHAIN;
+    constexpr int NL = LV + 1;                            // accumulators per chain
+    static_assert(2 * NL * WIN <= MX_TMEM_COLS, "accumulators exceed tensor memory");
     extern __shared__ unsigned char smem_raw[];
     unsigned char * const sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t) 1023);
     unsigned char * const Xs = sm;                        // [chain][piece]: MX_COLS rows x WIN slots
     unsigned char * const Qs = sm + 2 * NS * MX_PIECE;    // [chain]: the chain's tile image
-    __shared__ __align__(8) uint64_t bar_qfull[2], bar_qempty[2], bar_xready[2], bar_acc[2], bar_pmax[2], bar_done;
+    __shared__ __align__(8) uint64_t bar_qfull[2], bar_qempty[2], bar_xready[2], bar_acc[2], bar_pmax[2], bar_block[2], bar_done;
     __shared__ uint32_t s_tmem;
     __shared__ int s_task;
     __shared__ volatile int s_abort;
@@ -349,6 +351,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
             tc::mbar_init(&bar_qempty[i], 1);
             tc::mbar_init(&bar_xready[i], 256);
             tc::mbar_init(&bar_pmax[i], 256);
+            tc::mbar_init(&bar_block[i], 256);
             tc::mbar_init(&bar_acc[i], 1);
         }
         tc::mbar_init(&bar_done, 1);
@@ -369,6 +372,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
     unsigned xr[2] = {0, 0};         // x-ready phases consumed (MMA)
     unsigned ac = 0;                 // accumulator phases consumed (epilogue, own chain)
     unsigned pp = 0;                 // window-maximum exchanges (epilogue, own chain)
+    unsigned bs = 0;                 // block boundaries passed (epilogue, own chain)
     int last_u = -1;                 // loader: last use of the chain buffers
 
     for (;;) {
@@ -426,14 +430,18 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
                             for (int kk = 0; kk < WIN / 16; ++kk) {
                                 const uint32_t sc = (uint32_t) (((lo + 16 * kk) & (WIN - 1)) >> 4);
 #pragma unroll
-                                for (int a = 0; a < NS; ++a)
+                                for (int lv = 0; lv <= LV; ++lv) {
+                                    const int bmin = lv - (NS - 1) > 0 ? lv - (NS - 1) : 0;
+                                    const int bmax = lv < NS - 1 ? lv : NS - 1;
 #pragma unroll
-                                    for (int b = 0; a + b < NS; ++b) {
+                                    for (int b = bmin; b <= bmax; ++b) {
+                                        const int a = lv - b;
                                         const uint64_t ad = tc::desc_sw128(xs0 + (c * NS + a) * MX_PIECE + sc * 32);
                                         const uint64_t bd = tc::desc_sw128(qs0 + c * QCHAIN + b * MX_QPIECE + kk * 32);
-                                        // level a + b; its first product (kk = 0, a = 0) starts the accumulator
-                                        tc::mma_bf16(tmem + (c * NS + a + b) * WIN, ad, bd, MX_IDESC, !(kk == 0 && a == 0));
+                                        // the level's first product of the tile starts its accumulator
+                                        tc::mma_bf16(tmem + (c * NL + lv) * WIN, ad, bd, MX_IDESC, !(kk == 0 && b == bmin));
                                     }
+                                }
                             }
                             tc::commit(&bar_acc[c]);
                             tc::commit(&bar_qempty[c]);
@@ -452,7 +460,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
             const int fh = HI2LO ? 1 : 0;                 // the half whose outputs leave the window
             float * const Tc = L.T + task_index(T, L.nbeta) * (2LL * L.Lmax * MX_COLS) + (long long) c * L.Lmax * MX_COLS + r;
             unsigned char * const xrow = Xs + c * NS * MX_PIECE;
-            const uint32_t tacc = tmem + ((uint32_t) (quarter * 32) << 16) + c * NS * WIN + 32 * hf;
+            const uint32_t tacc = tmem + ((uint32_t) (quarter * 32) << 16) + c * NL * WIN + 32 * hf;
             float scale = 1.0f;   // slicing scale of the window the products in flight were computed from
             auto valid = [&](int pos) -> bool { return pos >= 0 && 2 * pos + c < N; };
             auto load32 = [&](int pos0, float * v) {
@@ -506,24 +514,32 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
                     const bool last = ki == nk - 1;
                     const bool fin = last || hf == fh;    // this half's outputs leave the window
                     const int npos = HI2LO ? lo - TL : lo + WIN;
+                    // the rows entering the tile after next into L2 (32 positions x 128 columns,
+                    // contiguous in the task-major copy)
+                    if (hf == fh && quarter == 0 && lane == 0 && ki + 2 < nk) {
+                        const int ppos = HI2LO ? npos - TL : npos + TL;
+                        const int plo = ppos < 0 ? 0 : ppos;
+                        const int phi = min(ppos + TL, L.Lmax);
+                        if (phi > plo) tc::prefetch_l2(Tc - r + (long long) plo * MX_COLS, (uint32_t) (phi - plo) * MX_COLS * 4);
+                    }
                     // the finishing half brings the positions entering the next tile
                     if (!last && hf == fh) load32(npos, src);
                     if (!tc::mbar_wait(&bar_acc[c], ac & 1, &s_abort)) { fail(); break; }
                     ac++;
                     __syncwarp();
                     tc::fence_after_sync();
-                    const float unscale = 0.0078125f / scale;     // 2^-7 / s, a power of two
+                    const float unscale = 0.00390625f / scale;    // 2^-8 / s, a power of two
 #pragma unroll
                     for (int g = 0; g < TL / 8; ++g) {             // 8 window positions at a time
-                        uint32_t a[NS][8];
+                        uint32_t a[NL][8];
 #pragma unroll
-                        for (int lv = 0; lv < NS; ++lv) tc::tmem_ld8_async(tacc + lv * WIN + 8 * g, a[lv]);
+                        for (int lv = 0; lv < NL; ++lv) tc::tmem_ld8_async(tacc + lv * WIN + 8 * g, a[lv]);
                         tc::tmem_wait_ld();
 #pragma unroll
                         for (int e = 0; e < 8; ++e) {
-                            float y = __uint_as_float(a[NS - 1][e]);
+                            float y = __uint_as_float(a[NL - 1][e]);
 #pragma unroll
-                            for (int lv = NS - 2; lv >= 0; --lv) y = fmaf(y, 0.00390625f, __uint_as_float(a[lv][e]));
+                            for (int lv = NL - 2; lv >= 0; --lv) y = fmaf(y, 0.001953125f, __uint_as_float(a[lv][e]));
                             const float v = y * unscale;
                             const int pos = lo + TL * hf + 8 * g + e;
                             if (fin) {
@@ -537,6 +553,11 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
                     // the finished ones' slots
                     if (!last && !put32(hf == fh ? npos : lo + TL * hf, src)) break;
                 }
+                // block boundary: the next block's first window reads rows of global memory that
+                // the other half of this chain's threads wrote
+                tc::mbar_arrive(&bar_block[c]);
+                if (!tc::mbar_wait(&bar_block[c], bs & 1, &s_abort)) { fail(); break; }
+                bs++;
             }
         }
     }
@@ -780,8 +801,9 @@ cudaError_t launch_blocked_mixed(void * plan, int ns, bool hi2lo, float * T, int
     L.err = B->d_err;
     L.N = N;
     L.M = M;
-    auto kern = ns == 3 ? (hi2lo ? blocked_mixed_kernel<true, 3> : blocked_mixed_kernel<false, 3>)
-                        : (hi2lo ? blocked_mixed_kernel<true, 4> : blocked_mixed_kernel<false, 4>);
+    // three slices: levels 0 .. 3 (eight products); four slices: levels 0 .. 3 (ten products)
+    auto kern = ns == 3 ? (hi2lo ? blocked_mixed_kernel<true, 3, 3> : blocked_mixed_kernel<false, 3, 3>)
+                        : (hi2lo ? blocked_mixed_kernel<true, 4, 3> : blocked_mixed_kernel<false, 4, 3>);
     const size_t smem = ns == 3 ? MxCfg<3>::SMEM : MxCfg<4>::SMEM;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
     if (e != cudaSuccess) return e;

@@ -408,19 +408,23 @@ cudaError_t launch_kind(int cfg, const RotLaunch & L, int max_ctas, cudaStream_t
     return launch_cfg<KIND, HI2LO, 8, 8, 16>(L, max_ctas, st);
 }
 
-int g_rot_cfg = -1;
+int g_rot_cfg = -2;
 
+// FT_B200_ROT_CFG = 0..3 forces a configuration; otherwise -1 (choose per launch)
 int rotation_config() {
-    if (g_rot_cfg < 0) {
+    if (g_rot_cfg == -2) {
         const char * e = std::getenv("FT_B200_ROT_CFG");
-        g_rot_cfg = (e && e[0] >= '0' && e[0] <= '3') ? e[0] - '0' : 0;
+        g_rot_cfg = (e && e[0] >= '0' && e[0] <= '3') ? e[0] - '0' : -1;
     }
     return g_rot_cfg;
 }
 
 cudaError_t launch_rotations(int kind, bool hi2lo, const RotLaunch & L, int max_ctas, cudaStream_t st) {
     if (L.ntasks <= 0) return cudaSuccess;
-    const int cfg = rotation_config();
+    // Launches that run only the heads above whole blocks (blk > 0: fewer than blk sweeps
+    // per column, 2 blk - 2 per task at most) keep more stages busy with 4 sweeps per warp.
+    int cfg = rotation_config();
+    if (cfg < 0) cfg = (L.nfields > 0 && L.fields[0].blk > 0) ? 3 : 0;
     switch (kind) {
         case SPH:  return hi2lo ? launch_kind<SPH, true>(cfg, L, max_ctas, st) : launch_kind<SPH, false>(cfg, L, max_ctas, st);
         case TRI:  return hi2lo ? launch_kind<TRI, true>(cfg, L, max_ctas, st) : launch_kind<TRI, false>(cfg, L, max_ctas, st);

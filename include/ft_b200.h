@@ -180,14 +180,16 @@ int ft_b200_execute_noalloc_dev(const ft_harmonic_plan * P, int forward, char TR
  * of 1e-14.  The first call on a plan builds its tile matrices (device memory,
  * about 550 MB at n = 4096); make it before any stream capture.
  * precision FT_B200_MIXED_BF16 (sph only): the same blocks, each tile product
- * computed on the tcgen05 tensor cores from three BF16 fixed-point slices per
- * operand (six slice products, exact FP32 accumulation per order level); a
- * value is carried between tiles at FP32 accuracy, in global memory the
- * matrices stay FP64.  The connection multiply stays FP64.  Relative 2-norm
- * error against the FP64 transform about 1e-6 at n = 256, 8e-6 at n = 4096.
- * precision FT_B200_MIXED_BF16X4: four slices per operand, ten products;
- * relative error about 1e-7 at n = 4096.  The first call of either builds
- * its slice images of the tiles (about 400 / 550 MB at n = 4096). */
+ * computed on the tcgen05 tensor cores from three 9-bit fixed-point BF16
+ * slices per operand (eight slice products, exact FP32 accumulation per order
+ * level); a value is carried between tiles at FP32 accuracy, in global memory
+ * the matrices stay FP64.  The connection multiply runs on the tensor cores
+ * too (four 8-bit slices of the matrix, three of the input, exact chunks of
+ * 256 rows, FP32 running sums).  Relative 2-norm error against the FP64
+ * transform about 5e-7 at n = 4096.
+ * precision FT_B200_MIXED_BF16X4: four slices in the blocks (ten products),
+ * about 3.5e-7 at n = 4096.  The first call of either builds its slice images
+ * of the tiles and of the connection matrices (about 1 GB at n = 4096). */
 #define FT_B200_FP64 0
 #define FT_B200_FP64_BLOCKED 1
 #define FT_B200_MIXED_BF16 2
