@@ -211,6 +211,22 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
+def max_over_ranks(x: float, dist, device: str) -> float:
+    """The largest of every rank's x (each rank times its own replica; the job's time is the
+    slowest rank's).  dist None: single process."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(coeffs_per_rank: int, world: int, steps: int, ms: float) -> float:
+    """Whole-job coefficients per second: every rank transforms its own fields each step."""
+    return world * coeffs_per_rank * steps / (ms * 1e-3)
+
+
 def block_split_rotations(n: int, blk: int = 32):
     """Rotations of one sph hi2lo over all orders, split into those of whole blocks of
     `blk` sweeps (the tensor-core products) and the heads above them (direct kernel)."""
@@ -319,12 +335,9 @@ def run_ours(args, rank, world, local_rank, dist):
     fam = {name: ft.profile_read(i) for i, name in enumerate(("heads", "trmm", "transposes", "blocks"))}
     ft.profile(False)
     ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, "cuda")
     coeffs = nf * n * n
-    value = world * coeffs * args.steps / (ms * 1e-3)
+    value = replica_value(coeffs, world, args.steps, ms)
 
     # the same fields through the plain FP64 path
     psteps = max(2, args.steps // 3)
@@ -339,11 +352,8 @@ def run_ours(args, rank, world, local_rank, dist):
     e1.record(stream)
     torch.cuda.synchronize()
     pms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([pms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        pms = float(t.item())
-    plain_value = world * coeffs * psteps / (pms * 1e-3)
+    pms = max_over_ranks(pms, dist, "cuda")
+    plain_value = replica_value(coeffs, world, psteps, pms)
 
     # end to end through the C-ABI call: every step copies the fields in from pinned
     # host memory, runs forward and backward, and copies the results back
@@ -366,10 +376,7 @@ def run_ours(args, rank, world, local_rank, dist):
             h.copy_(t, non_blocking=True)
         torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, dist, "cuda")
     e2e_value = world * coeffs * e2e_steps / e2e_s
     bytes_mat = n * M * 8
     del hb
@@ -527,20 +534,30 @@ def plain_single(args, torch, ft):
                      "step_fp64_frac": total / (ms / steps * 1e-3) / 1e12 / fp64}}
 
 
-def profile_case(n: int) -> None:
-    """Small fixed program for ncu captures: plan, seeded field, two forward transforms."""
+def profile_case(n: int, precision: str, fields: int) -> None:
+    """Small fixed programs for ncu captures (no timing).  fp64: one field through the
+    plain drop-in path, two forward transforms.  mixed / mixed4: `fields` fields sharing
+    a plan through ft_b200_execute_shared_dev (MIXED_BF16 / MIXED_BF16X4), two forward
+    transforms (the first builds the slice images)."""
     import torch
     import fasttransforms_b200 as ft
     M = 2 * n - 1
     P = ft.plan_sph2fourier(n)
-    A = ft.sphrand(n, SEED)
-    d = torch.from_numpy(A.ravel(order="F").copy()).cuda()
     s = torch.cuda.current_stream().cuda_stream
-    for _ in range(2):
-        ft.execute_dev(P, True, "N", d.data_ptr(), n, M, s)
+    if precision == "fp64":
+        d = [torch.from_numpy(ft.sphrand(n, SEED).ravel(order="F").copy()).cuda()]
+        for _ in range(2):
+            ft.execute_dev(P, True, "N", d[0].data_ptr(), n, M, s)
+    else:
+        prec = ft.MIXED_BF16 if precision == "mixed" else ft.MIXED_BF16X4
+        d = [torch.from_numpy(ft.sphrand(n, SEED + f).ravel(order="F").copy()).cuda() for f in range(fields)]
+        for _ in range(2):
+            ft.execute_shared_dev(P, True, "N", [t.data_ptr() for t in d], prec, s)
     torch.cuda.synchronize()
+    status = ft.device_status(P)
     P.close()
-    print(json.dumps({"profile_case": f"sph n={n}", "max_abs": float(d.abs().max())}))
+    print(json.dumps({"profile_case": f"sph n={n}, {precision}, {len(d)} field(s)", "device_status": status,
+                      "max_abs": max(float(t.abs().max()) for t in d)}))
 
 
 def extra_workloads(args, torch, ft):
@@ -661,9 +678,11 @@ def main():
     ap.add_argument("--cpu-sample", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--profile-case", action="store_true",
                     help="run one plan and two forward transforms (for ncu), no timing")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "mixed4"],
+                    help="--profile-case path: plain FP64 (one field) or the shared-plan tensor-core paths")
     args = ap.parse_args()
     if args.profile_case:
-        profile_case(args.n)
+        profile_case(args.n, args.precision, args.fields)
         return
     if args.cpu_sample:
         print(json.dumps(cpu_sample(args.n, 2)))
