@@ -255,18 +255,20 @@ template <int NS> struct MxCfg {
     static_assert(SMEM <= 227 * 1024, "shared memory");
 };
 
-// The blocked stage works on its own copy of the columns, task-major and
-// column-fastest: task (pair of fields, parity, band) -> 128 columns, and
-// element (chain c, position pos, column i) at ((c * Lmax + pos) * 128 + i),
-// in FP32.  A warp then reads or writes one position of 32 adjacent columns as
-// 128 contiguous bytes.
+// The blocked stage works on its own copy of the columns, task-major, in FP32:
+// task (pair of fields, parity, band) -> 128 columns, and element (chain c,
+// position pos, column i) at ((c * Lq + pos / 4) * 128 + i) * 4 + pos % 4, with
+// Lq position quads per chain.  A thread moves four consecutive positions of
+// its column as one 16-byte access, and a warp (32 adjacent columns) 512
+// contiguous bytes.  Positions past a chain's end hold zeros: the tile
+// products never rotate them, so they stay zero.
 __host__ __device__ __forceinline__ long long task_index(const BlkTask & t, int nbeta) {
     return ((long long) (t.field >> 1) * 2 + t.p) * nbeta + (t.band - 1);
 }
 
 struct MixedLaunch {
     float * T;                     // task-major copy of the columns (in place)
-    int Lmax;                      // positions per chain in T
+    int Lq;                        // position quads per chain in T
     const __nv_bfloat16 * img;     // tile images of the direction: [tile][chain][piece][WIN x WIN swizzled]
     const long long * qbase;       // [2][nbeta], as for the FP64 tiles (2 chains per tile)
     const int * kmax;
@@ -343,7 +345,6 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
     __shared__ volatile int s_abort;
     __shared__ float s_pmax[2][2][MX_COLS];             // [chain][half][column]: largest window entry
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int N = L.N;
 
     if (tid == 0) {
         for (int i = 0; i < 2; ++i) {
@@ -458,14 +459,21 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
             const int quarter = warp & 3, hf = (warp >> 2) & 1;
             const int r = 32 * quarter + lane;
             const int fh = HI2LO ? 1 : 0;                 // the half whose outputs leave the window
-            float * const Tc = L.T + task_index(T, L.nbeta) * (2LL * L.Lmax * MX_COLS) + (long long) c * L.Lmax * MX_COLS + r;
+            // this column's quads: quad Q of the chain at Tq[Q * MX_COLS]
+            float4 * const Tq = reinterpret_cast<float4 *>(L.T + task_index(T, L.nbeta) * (8LL * L.Lq * MX_COLS)) +
+                                (long long) c * L.Lq * MX_COLS + r;
+            const int Pend = 4 * L.Lq;                    // positions held in the copy
             unsigned char * const xrow = Xs + c * NS * MX_PIECE;
             const uint32_t tacc = tmem + ((uint32_t) (quarter * 32) << 16) + c * NL * WIN + 32 * hf;
             float scale = 1.0f;   // slicing scale of the window the products in flight were computed from
-            auto valid = [&](int pos) -> bool { return pos >= 0 && 2 * pos + c < N; };
+            // 32 positions from pos0 (a multiple of 32): 8 quads, zero outside the copy
             auto load32 = [&](int pos0, float * v) {
 #pragma unroll
-                for (int e = 0; e < TL; ++e) v[e] = valid(pos0 + e) ? __ldcg(Tc + (long long) (pos0 + e) * MX_COLS) : 0.0f;
+                for (int qd = 0; qd < TL / 4; ++qd) {
+                    const int P = pos0 + 4 * qd;
+                    const float4 x = (P >= 0 && P < Pend) ? __ldcg(Tq + (long long) (P >> 2) * MX_COLS) : make_float4(0.f, 0.f, 0.f, 0.f);
+                    v[4 * qd] = x.x; v[4 * qd + 1] = x.y; v[4 * qd + 2] = x.z; v[4 * qd + 3] = x.w;
+                }
             };
             // 32 positions from pos0 (a multiple of 32) into their window slots, with one
             // scale for the whole window: the two halves exchange their largest entries
@@ -518,9 +526,9 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
                     // contiguous in the task-major copy)
                     if (hf == fh && quarter == 0 && lane == 0 && ki + 2 < nk) {
                         const int ppos = HI2LO ? npos - TL : npos + TL;
-                        const int plo = ppos < 0 ? 0 : ppos;
-                        const int phi = min(ppos + TL, L.Lmax);
-                        if (phi > plo) tc::prefetch_l2(Tc - r + (long long) plo * MX_COLS, (uint32_t) (phi - plo) * MX_COLS * 4);
+                        const int qlo = ppos < 0 ? 0 : ppos >> 2;
+                        const int qhi = min((ppos + TL) >> 2, L.Lq);
+                        if (qhi > qlo) tc::prefetch_l2(Tq - r + (long long) qlo * MX_COLS, (uint32_t) (qhi - qlo) * MX_COLS * 16);
                     }
                     // the finishing half brings the positions entering the next tile
                     if (!last && hf == fh) load32(npos, src);
@@ -536,16 +544,21 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
                         for (int lv = 0; lv < NL; ++lv) tc::tmem_ld8_async(tacc + lv * WIN + 8 * g, a[lv]);
                         tc::tmem_wait_ld();
 #pragma unroll
-                        for (int e = 0; e < 8; ++e) {
-                            float y = __uint_as_float(a[NL - 1][e]);
+                        for (int hq = 0; hq < 2; ++hq) {           // one quad of positions at a time
+                            float v[4];
 #pragma unroll
-                            for (int lv = NL - 2; lv >= 0; --lv) y = fmaf(y, 0.001953125f, __uint_as_float(a[lv][e]));
-                            const float v = y * unscale;
-                            const int pos = lo + TL * hf + 8 * g + e;
+                            for (int e = 0; e < 4; ++e) {
+                                float y = __uint_as_float(a[NL - 1][4 * hq + e]);
+#pragma unroll
+                                for (int lv = NL - 2; lv >= 0; --lv) y = fmaf(y, 0.001953125f, __uint_as_float(a[lv][4 * hq + e]));
+                                v[e] = y * unscale;
+                            }
+                            const int P = lo + TL * hf + 8 * g + 4 * hq;
                             if (fin) {
-                                if (valid(pos)) __stcg(Tc + (long long) pos * MX_COLS, v);
+                                if (P >= 0 && P < Pend) __stcg(Tq + (long long) (P >> 2) * MX_COLS, make_float4(v[0], v[1], v[2], v[3]));
                             } else {
-                                src[8 * g + e] = v;
+#pragma unroll
+                                for (int e = 0; e < 4; ++e) src[8 * g + 4 * hq + e] = v[e];
                             }
                         }
                     }
@@ -790,7 +803,7 @@ cudaError_t launch_blocked_mixed(void * plan, int ns, bool hi2lo, float * T, int
     if (tl.ntasks == 0) return cudaSuccess;
     static thread_local MixedLaunch L;
     L.T = T;
-    L.Lmax = (N + 1) / 2;
+    L.Lq = ((N + 1) / 2 + 3) / 4;
     L.img = B->d_img[ns - 3][hi2lo ? 0 : 1];
     L.qbase = B->d_qbase;
     L.kmax = B->d_kmax;
@@ -822,14 +835,15 @@ cudaError_t launch_blocked_mixed(void * plan, int ns, bool hi2lo, float * T, int
 size_t blocked_mixed_T_elems(void * plan, int nf, int N) {
     BlockedPlan * B = static_cast<BlockedPlan *>(plan);
     const long long npairs = (nf + 1) / 2;
-    return (size_t) (npairs * 2 * std::max(1, B->nbeta)) * 2 * (size_t) ((N + 1) / 2) * MX_COLS;
+    const size_t Lq = (size_t) (((N + 1) / 2 + 3) / 4);
+    return (size_t) (npairs * 2 * std::max(1, B->nbeta)) * 2 * Lq * 4 * MX_COLS;
 }
 
 // S (the fields' FP64 matrices) <-> T (task-major FP32 copy of the columns the
 // blocks apply to); one CTA per (task, 32 positions of both chains).
 struct TransLaunch {
     double * A[kMaxFields];
-    int nf, N, M, nbeta, Lmax;
+    int nf, N, M, nbeta, Lq;
     float * T;
     const BlkTask * tasks;
 };
@@ -841,7 +855,9 @@ __global__ void __launch_bounds__(256) transpose_kernel(const __grid_constant__ 
     const int q = blockIdx.y;                           // positions 32q .. 32q + 31
     const int tid = threadIdx.x;
     const int N = L.N, mlast = L.M / 2;
-    float * const Tt = L.T + task_index(t, L.nbeta) * (2LL * L.Lmax * MX_COLS);
+    float * const Tt = L.T + task_index(t, L.nbeta) * (8LL * L.Lq * MX_COLS);
+    // element (chain c, position pos, column i) of the task's copy
+    auto at = [&](int c, int pos, int i) -> long long { return (((long long) c * L.Lq + (pos >> 2)) * MX_COLS + i) * 4 + (pos & 3); };
     // column i of the task: field, matrix column, or -1
     auto column = [&](int i, int & f) -> long long {
         f = t.field + (i >> 6);
@@ -859,15 +875,19 @@ __global__ void __launch_bounds__(256) transpose_kernel(const __grid_constant__ 
         }
         __syncthreads();
         const int i = tid & (MX_COLS - 1);
-        for (int e = tid >> 7; e < 64; e += 2) {       // e = 2 * (pos - 32q) + c
-            const int c = e & 1, pos = 32 * q + (e >> 1);
-            if (pos < L.Lmax) __stcg(Tt + ((long long) c * L.Lmax + pos) * MX_COLS + i, tile[e][i]);
+        for (int e = tid >> 7; e < 16; e += 2) {       // e = 2 * (quad - 8q) + c
+            const int c = e & 1, qd = e >> 1, Q = 8 * q + qd;
+            if (Q < L.Lq) {
+                const float4 v = make_float4(tile[8 * qd + c][i], tile[8 * qd + 2 + c][i], tile[8 * qd + 4 + c][i], tile[8 * qd + 6 + c][i]);
+                __stcg(reinterpret_cast<float4 *>(Tt + at(c, 4 * Q, i)), v);
+            }
         }
     } else {
         const int i = tid & (MX_COLS - 1);
-        for (int e = tid >> 7; e < 64; e += 2) {
-            const int c = e & 1, pos = 32 * q + (e >> 1);
-            tile[e][i] = pos < L.Lmax ? __ldcg(Tt + ((long long) c * L.Lmax + pos) * MX_COLS + i) : 0.0f;
+        for (int e = tid >> 7; e < 16; e += 2) {       // e = 2 * (quad - 8q) + c
+            const int c = e & 1, qd = e >> 1, Q = 8 * q + qd;
+            const float4 v = Q < L.Lq ? __ldcg(reinterpret_cast<const float4 *>(Tt + at(c, 4 * Q, i))) : make_float4(0.f, 0.f, 0.f, 0.f);
+            tile[8 * qd + c][i] = v.x; tile[8 * qd + 2 + c][i] = v.y; tile[8 * qd + 4 + c][i] = v.z; tile[8 * qd + 6 + c][i] = v.w;
         }
         __syncthreads();
         for (int i2 = tid >> 6; i2 < MX_COLS; i2 += 4) {
@@ -888,10 +908,10 @@ cudaError_t launch_blocked_transpose(void * plan, bool to_T, double * const * A,
     L.N = N;
     L.M = M;
     L.nbeta = B->nbeta;
-    L.Lmax = (N + 1) / 2;
+    L.Lq = ((N + 1) / 2 + 3) / 4;
     L.T = T;
     L.tasks = reinterpret_cast<const BlkTask *>(tl.d_tasks);
-    const dim3 grid(tl.ntasks, (L.Lmax + 31) / 32);
+    const dim3 grid(tl.ntasks, (4 * L.Lq + 31) / 32);
     if (to_T) transpose_kernel<true><<<grid, 256, 0, st>>>(L);
     else      transpose_kernel<false><<<grid, 256, 0, st>>>(L);
     count_launch();
