@@ -25,7 +25,7 @@ __all__ = [
     "FTB200Error", "HarmonicPlan", "RotationPlan", "library_path", "lib",
     "plan_sph2fourier", "plan_tri2cheb", "plan_disk2cxf",
     "execute_sph2fourier", "execute_fourier2sph", "execute_tri2cheb", "execute_cheb2tri",
-    "execute_disk2cxf", "execute_cxf2disk",
+    "execute_disk2cxf", "execute_cxf2disk", "execute_sphv2fourier", "execute_fourier2sphv", "execute_sphv_dev",
     "plan_rotsphere", "plan_rottriangle", "plan_rotdisk",
     "execute_sph_hi2lo", "execute_sph_lo2hi", "execute_tri_hi2lo", "execute_tri_lo2hi",
     "execute_disk_hi2lo", "execute_disk_lo2hi",
@@ -62,6 +62,7 @@ def _load() -> C.CDLL:
         "ft_plan_rotsphere": (vp, [i]), "ft_plan_rottriangle": (vp, [i, d, d, d]), "ft_plan_rotdisk": (vp, [i, d, d]),
         "ft_destroy_rotation_plan": (None, [vp]),
         "ft_b200_execute_dev": (i, [vp, i, ch, vp, i, i, vp]),
+        "ft_b200_execute_sphv_dev": (i, [vp, i, ch, vp, i, i, vp]),
         "ft_b200_rotations_dev": (i, [vp, i, vp, i, vp]),
         "ft_b200_execute_batched_dev": (i, [C.POINTER(vp), i, ch, C.POINTER(vp), C.POINTER(i), C.POINTER(i), i, vp]),
         "ft_b200_plan_kind": (i, [vp]), "ft_b200_plan_device": (i, [vp]),
@@ -70,7 +71,7 @@ def _load() -> C.CDLL:
         "ft_b200_device_status": (i, [vp]),
         "ft_b200_profile": (i, [i]), "ft_b200_profile_read": (i, [i, C.POINTER(C.c_double), C.POINTER(i)]),
     }
-    for name in ("sph2fourier", "fourier2sph", "tri2cheb", "cheb2tri", "disk2cxf", "cxf2disk"):
+    for name in ("sph2fourier", "fourier2sph", "tri2cheb", "cheb2tri", "disk2cxf", "cxf2disk", "sphv2fourier", "fourier2sphv"):
         sig["ft_execute_" + name] = (None, [ch, vp, dp, i, i])
     for fam in ("sph", "tri", "disk"):
         for d_ in ("hi2lo", "lo2hi"):
@@ -191,6 +192,8 @@ def execute_tri2cheb(trans, P, A, N=None, M=None): _exec_host("ft_execute_tri2ch
 def execute_cheb2tri(trans, P, A, N=None, M=None): _exec_host("ft_execute_cheb2tri", trans, P, A, N, M)
 def execute_disk2cxf(trans, P, A, N=None, M=None): _exec_host("ft_execute_disk2cxf", trans, P, A, N, M)
 def execute_cxf2disk(trans, P, A, N=None, M=None): _exec_host("ft_execute_cxf2disk", trans, P, A, N, M)
+def execute_sphv2fourier(trans, P, A, N=None, M=None): _exec_host("ft_execute_sphv2fourier", trans, P, A, N, M)
+def execute_fourier2sphv(trans, P, A, N=None, M=None): _exec_host("ft_execute_fourier2sphv", trans, P, A, N, M)
 
 
 def plan_rotsphere(n: int) -> RotationPlan:
@@ -232,6 +235,13 @@ def execute_disk_lo2hi(RP, A, M=None): _exec_rot("ft_execute_disk_lo2hi", RP, A,
 def execute_dev(P: HarmonicPlan, forward: bool, trans: str, ptr: int, N: int, M: int, stream: int = 0) -> None:
     """Full transform on a device matrix (N x M, column-major) enqueued on ``stream``."""
     st = lib.ft_b200_execute_dev(P.ptr, 1 if forward else 0, trans.encode(), C.c_void_p(ptr), N, M, C.c_void_p(stream))
+    if st != 0:
+        _check()
+
+
+def execute_sphv_dev(P: HarmonicPlan, forward: bool, trans: str, ptr: int, N: int, M: int, stream: int = 0) -> None:
+    """sph vector-field transform (sphv2fourier / fourier2sphv) on a device matrix, sph plan."""
+    st = lib.ft_b200_execute_sphv_dev(P.ptr, 1 if forward else 0, trans.encode(), C.c_void_p(ptr), N, M, C.c_void_p(stream))
     if st != 0:
         _check()
 

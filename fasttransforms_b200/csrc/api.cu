@@ -179,6 +179,18 @@ bool rotations(ft_rotation_plan * RP, bool hi2lo, const double * in, double * ou
     return cuda_ok(e, "rotation kernel");
 }
 
+// Vector-field sweeps (src/drivers.c:168-276): order m's rotations on columns 2m + 1 and
+// 2m + 2 for m = 2 .. M/2 - 1, i.e. the sph sweeps of the matrix that starts two columns
+// later and has M - 2 columns; columns 0 and 1 are left alone.
+bool rotations_sphv(ft_rotation_plan * RP, bool hi2lo, const double * in, double * out, int M, long long lda,
+                    cudaStream_t st) {
+    const int lead = std::min(M, 2);
+    if (in != out && !cuda_ok(cudaMemcpy2DAsync(out, lda * sizeof(double), in, lda * sizeof(double), RP->n * sizeof(double),
+                                                lead, cudaMemcpyDeviceToDevice, st), "cudaMemcpy2DAsync")) return false;
+    if (M <= 2) return true;
+    return rotations(RP, hi2lo, in + 2 * lda, out + 2 * lda, M - 2, lda, st);
+}
+
 bool valid_MN(int kind, int n, int N, int M) {
     if (N != n) { set_error(FT_B200_EINVAL, "N does not match the plan's n"); return false; }
     if (M < 1) { set_error(FT_B200_EINVAL, "M must be positive"); return false; }
@@ -187,7 +199,9 @@ bool valid_MN(int kind, int n, int N, int M) {
 }
 
 // sph / disk: four stride-4N column classes, P[0] on classes 0 and 3, P[1] on 1 and 2
-bool trmm4(HarmonicPlan * H, bool inverse, bool trans, const double * in, double * out, int M, cudaStream_t st) {
+// (swapped for the sph vector-field transforms, src/drivers.c:867-899)
+bool trmm4(HarmonicPlan * H, bool inverse, bool trans, const double * in, double * out, int M, cudaStream_t st,
+           bool swap = false) {
     const int N = H->n;
     TrmmLaunch L{};
     L.n = N;
@@ -198,7 +212,7 @@ bool trmm4(HarmonicPlan * H, bool inverse, bool trans, const double * in, double
     int c = 0;
     for (int r = 0; r < 4; r++) {
         if (ncols[r] <= 0) continue;
-        L.cls[c].U = (r == 0 || r == 3) ? U[0] : U[1];
+        L.cls[c].U = ((r == 0 || r == 3) != swap) ? U[0] : U[1];
         L.cls[c].in = in + (long long) r * N;
         L.cls[c].out = out + (long long) r * N;
         L.cls[c].ncols = ncols[r];
@@ -249,9 +263,11 @@ bool ensure_scratch(HarmonicPlan * H, size_t elems) {
     return true;
 }
 
-int execute_dev_impl(HarmonicPlan * H, bool forward, char TRANS, double * A, int N, int M, cudaStream_t st) {
+int execute_dev_impl(HarmonicPlan * H, bool forward, char TRANS, double * A, int N, int M, cudaStream_t st,
+                     bool vector = false) {
     if (TRANS != 'N' && TRANS != 'T') { set_error(FT_B200_EINVAL, "TRANS must be 'N' or 'T'"); return t_status; }
     if (!A) { set_error(FT_B200_EINVAL, "NULL matrix"); return t_status; }
+    if (vector && H->kind != SPH) { set_error(FT_B200_EINVAL, "vector-field transforms take a sph plan"); return t_status; }
     if (!valid_MN(H->kind, H->n, N, M)) return t_status;
     if (!ensure_scratch(H, (size_t) N * M)) return t_status;
     double * S = H->d_scratch;
@@ -260,18 +276,22 @@ int execute_dev_impl(HarmonicPlan * H, bool forward, char TRANS, double * A, int
     const long long lda = N;
     if (H->kind != TRI) {
         // rotations (out of place) then trmm back, or trmm out then rotations back
+        // (sph vector fields: the shifted sweeps and the swapped matrices, src/drivers.c:867-899)
+        auto rot = [&](bool hi2lo, const double * in, double * out) {
+            return vector ? rotations_sphv(RP, hi2lo, in, out, M, lda, st) : rotations(RP, hi2lo, in, out, M, lda, st);
+        };
         if (forward && tN) {            // hi2lo, P
-            if (!rotations(RP, true, A, S, M, lda, st)) return t_status;
-            if (!trmm4(H, false, false, S, A, M, st)) return t_status;
+            if (!rot(true, A, S)) return t_status;
+            if (!trmm4(H, false, false, S, A, M, st, vector)) return t_status;
         } else if (forward) {           // P^T, lo2hi
-            if (!trmm4(H, false, true, A, S, M, st)) return t_status;
-            if (!rotations(RP, false, S, A, M, lda, st)) return t_status;
+            if (!trmm4(H, false, true, A, S, M, st, vector)) return t_status;
+            if (!rot(false, S, A)) return t_status;
         } else if (tN) {                // Pinv, lo2hi
-            if (!trmm4(H, true, false, A, S, M, st)) return t_status;
-            if (!rotations(RP, false, S, A, M, lda, st)) return t_status;
+            if (!trmm4(H, true, false, A, S, M, st, vector)) return t_status;
+            if (!rot(false, S, A)) return t_status;
         } else {                        // hi2lo, Pinv^T
-            if (!rotations(RP, true, A, S, M, lda, st)) return t_status;
-            if (!trmm4(H, true, true, S, A, M, st)) return t_status;
+            if (!rot(true, A, S)) return t_status;
+            if (!trmm4(H, true, true, S, A, M, st, vector)) return t_status;
         }
         return FT_B200_OK;
     }
@@ -391,7 +411,7 @@ HarmonicPlan * make_harmonic_plan(int kind, int n, double alpha, double beta, do
 }
 
 // host-pointer execution: stage A on the device, run, copy back, wait
-void execute_host(const ft_harmonic_plan * P, bool forward, char TRANS, double * A, int N, int M) {
+void execute_host(const ft_harmonic_plan * P, bool forward, char TRANS, double * A, int N, int M, bool vector = false) {
     clear_error();
     HarmonicPlan * H = as_plan(P);
     if (!H) { set_error(FT_B200_EINVAL, "not a plan created by this library"); return; }
@@ -406,7 +426,7 @@ void execute_host(const ft_harmonic_plan * P, bool forward, char TRANS, double *
         H->stage_elems = elems;
     }
     if (!cuda_ok(cudaMemcpyAsync(H->d_stage, A, elems * sizeof(double), cudaMemcpyHostToDevice, H->stream), "cudaMemcpyAsync(H2D)")) return;
-    if (execute_dev_impl(H, forward, TRANS, H->d_stage, N, M, H->stream) != FT_B200_OK) { cudaStreamSynchronize(H->stream); return; }
+    if (execute_dev_impl(H, forward, TRANS, H->d_stage, N, M, H->stream, vector) != FT_B200_OK) { cudaStreamSynchronize(H->stream); return; }
     if (!cuda_ok(cudaMemcpyAsync(A, H->d_stage, elems * sizeof(double), cudaMemcpyDeviceToHost, H->stream), "cudaMemcpyAsync(D2H)")) return;
     cuda_ok(cudaStreamSynchronize(H->stream), "cudaStreamSynchronize");
 }
@@ -776,6 +796,8 @@ void ft_destroy_harmonic_plan(ft_harmonic_plan * P) {
 
 void ft_execute_sph2fourier(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M) { execute_host(P, true, TRANS, A, N, M); }
 void ft_execute_fourier2sph(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M) { execute_host(P, false, TRANS, A, N, M); }
+void ft_execute_sphv2fourier(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M) { execute_host(P, true, TRANS, A, N, M, true); }
+void ft_execute_fourier2sphv(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M) { execute_host(P, false, TRANS, A, N, M, true); }
 void ft_execute_tri2cheb(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M) { execute_host(P, true, TRANS, A, N, M); }
 void ft_execute_cheb2tri(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M) { execute_host(P, false, TRANS, A, N, M); }
 void ft_execute_disk2cxf(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M) { execute_host(P, true, TRANS, A, N, M); }
@@ -811,6 +833,13 @@ int ft_b200_execute_dev(const ft_harmonic_plan * P, int forward, char TRANS, dou
     HarmonicPlan * H = as_plan(P);
     if (!H) { set_error(FT_B200_EINVAL, "not a plan created by this library"); return t_status; }
     return execute_dev_impl(H, forward != 0, TRANS, dA, N, M, static_cast<cudaStream_t>(stream));
+}
+
+int ft_b200_execute_sphv_dev(const ft_harmonic_plan * P, int forward, char TRANS, double * dA, int N, int M, void * stream) {
+    clear_error();
+    HarmonicPlan * H = as_plan(P);
+    if (!H) { set_error(FT_B200_EINVAL, "not a plan created by this library"); return t_status; }
+    return execute_dev_impl(H, forward != 0, TRANS, dA, N, M, static_cast<cudaStream_t>(stream), true);
 }
 
 int ft_b200_rotations_dev(const ft_rotation_plan * RP, int hi2lo, double * dA, int M, void * stream) {

@@ -86,6 +86,12 @@ void ft_execute_sph2fourier(const char TRANS, const ft_harmonic_plan * P, double
 /* replaces ft_execute_fourier2sph, src/drivers.c:850-865 */
 void ft_execute_fourier2sph(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M);
 
+/* replaces ft_execute_sphv2fourier, src/drivers.c:867-882: vector fields on a sph plan
+ * (order m's sweeps on columns 2m+1, 2m+2; P[0] and P[1] swapped in the column classes) */
+void ft_execute_sphv2fourier(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M);
+/* replaces ft_execute_fourier2sphv, src/drivers.c:884-899 */
+void ft_execute_fourier2sphv(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M);
+
 /* replaces ft_plan_tri2cheb, src/drivers.c:901-919 */
 ft_harmonic_plan * ft_plan_tri2cheb(const int n, const double alpha, const double beta, const double gamma);
 /* replaces ft_execute_tri2cheb, src/drivers.c:921-938 */
@@ -132,6 +138,8 @@ enum { FT_B200_SPH = 0, FT_B200_TRI = 1, FT_B200_DISK = 2 };
 /* Full transform.  forward = 1: sph2fourier / tri2cheb / disk2cxf;
  * forward = 0: fourier2sph / cheb2tri / cxf2disk. */
 int ft_b200_execute_dev(const ft_harmonic_plan * P, int forward, char TRANS, double * dA, int N, int M, void * stream);
+/* The sph vector-field transforms on device memory (forward = 1: sphv2fourier). */
+int ft_b200_execute_sphv_dev(const ft_harmonic_plan * P, int forward, char TRANS, double * dA, int N, int M, void * stream);
 /* Rotation stage alone (hi2lo = 1: ft_execute_*_hi2lo; 0: *_lo2hi). */
 int ft_b200_rotations_dev(const ft_rotation_plan * RP, int hi2lo, double * dA, int M, void * stream);
 

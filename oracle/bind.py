@@ -82,6 +82,7 @@ class Oracle:
         L.oracle_plan_rotations.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
         L.oracle_destroy_plan.argtypes = [PP]
         L.oracle_execute.argtypes = [PP, C.c_int, C.c_char, C.POINTER(C.c_double), C.c_int, C.c_int]
+        L.oracle_execute_sphv.argtypes = [PP, C.c_int, C.c_char, C.POINTER(C.c_double), C.c_int, C.c_int]
         for f in ("oracle_execute_hi2lo", "oracle_execute_lo2hi"):
             getattr(L, f).argtypes = [PP, C.POINTER(C.c_double), C.c_int]
         for f in ("oracle_kernel_hi2lo", "oracle_kernel_lo2hi"):
@@ -119,6 +120,11 @@ class Oracle:
     def execute(self, P, forward: bool, trans: str, A: np.ndarray):
         N, M = A.shape
         self.lib.oracle_execute(P, 1 if forward else 0, trans.encode(), _ptr(A), N, M)
+
+    def execute_sphv(self, P, forward: bool, trans: str, A: np.ndarray):
+        """sph vector fields on a sph plan: sphv2fourier (forward) / fourier2sphv."""
+        N, M = A.shape
+        self.lib.oracle_execute_sphv(P, 1 if forward else 0, trans.encode(), _ptr(A), N, M)
 
     def hi2lo(self, P, A):
         self.lib.oracle_execute_hi2lo(P, _ptr(A), A.shape[1])
@@ -165,8 +171,10 @@ class _RefHarmonicPlan(C.Structure):
 class Reference:
     """The reference library compiled from its own sources (oracle/_ref)."""
 
-    _FWD = {"sph": "ft_execute_sph2fourier", "tri": "ft_execute_tri2cheb", "disk": "ft_execute_disk2cxf"}
-    _BWD = {"sph": "ft_execute_fourier2sph", "tri": "ft_execute_cheb2tri", "disk": "ft_execute_cxf2disk"}
+    _FWD = {"sph": "ft_execute_sph2fourier", "tri": "ft_execute_tri2cheb", "disk": "ft_execute_disk2cxf",
+            "sphv": "ft_execute_sphv2fourier"}
+    _BWD = {"sph": "ft_execute_fourier2sph", "tri": "ft_execute_cheb2tri", "disk": "ft_execute_cxf2disk",
+            "sphv": "ft_execute_fourier2sphv"}
 
     @staticmethod
     def available(path: str = REF_SO) -> bool:
@@ -193,7 +201,7 @@ class Reference:
 
     def plan(self, kind: str, n: int, alpha=0.0, beta=0.0, gamma=0.0):
         L = self.lib
-        if kind == "sph":
+        if kind in ("sph", "sphv"):
             return L.ft_plan_sph2fourier(n)
         if kind == "tri":
             return L.ft_plan_tri2cheb(n, alpha, beta, gamma)

@@ -685,6 +685,38 @@ void oracle_execute(const oracle_plan * P, int forward, char TRANS, double * A, 
     }
 }
 
+/* sph vector fields (src/drivers.c:198-214, 867-899): order m's sweeps on the column pair
+ * (2m+1, 2m+2) for m = 2 .. M/2-1, and P[0] / P[1] swapped in the four column classes. */
+static void execute_rot_sphv(const oracle_plan * P, double * A, int M, int hi2lo) {
+    int N = P->n;
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (int m = 2; m <= M / 2 - 1; m++) {
+        for (int h = 0; h < 2; h++) {
+            double * col = A + (size_t) N * (2 * m + 1 + h);
+            if (hi2lo) oracle_kernel_hi2lo(P, m % 2, m, col, 1);
+            else       oracle_kernel_lo2hi(P, m % 2, m, col, 1);
+        }
+    }
+}
+
+void oracle_execute_sphv(const oracle_plan * P, int forward, char TRANS, double * A, int N, int M) {
+    if (TRANS != 'N' && TRANS != 'T') return;
+    int tN = TRANS == 'N';
+    if (forward && tN) {
+        execute_rot_sphv(P, A, M, 1);
+        trmm4('N', N, M, P->P[1], P->P[0], A);
+    } else if (forward) {
+        trmm4('T', N, M, P->P[1], P->P[0], A);
+        execute_rot_sphv(P, A, M, 0);
+    } else if (tN) {
+        trmm4('N', N, M, P->Pinv[1], P->Pinv[0], A);
+        execute_rot_sphv(P, A, M, 0);
+    } else {
+        execute_rot_sphv(P, A, M, 1);
+        trmm4('T', N, M, P->Pinv[1], P->Pinv[0], A);
+    }
+}
+
 /* ---------------------------------------------------------------------------
  * Seeded fills.  Counter-based splitmix64: value(idx) for the entry at linear
  * column-major index idx = i + j*N is 2*u - 1 with u the top 53 bits of

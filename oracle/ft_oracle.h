@@ -59,6 +59,8 @@ void oracle_trmm(char side, char trans, int n, const double * U, int nb, double 
  * forward = 1: sph2fourier / tri2cheb / disk2cxf; forward = 0: fourier2sph / cheb2tri / cxf2disk.
  * TRANS 'N' or 'T'; any other character leaves A untouched (as the reference does). */
 void oracle_execute(const oracle_plan * P, int forward, char TRANS, double * A, int N, int M);
+/* sph vector-field transforms on a sph plan: sphv2fourier (forward = 1) / fourier2sphv. */
+void oracle_execute_sphv(const oracle_plan * P, int forward, char TRANS, double * A, int N, int M);
 
 /* Connection-matrix planners (n x n, column-major, caller frees with free()). */
 double * oracle_plan_legendre_to_chebyshev(int normleg, int normcheb, int n);

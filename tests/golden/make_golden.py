@@ -6,7 +6,8 @@ seeded inputs and stores inputs and outputs as compressed .npz files:
 
   * full transforms: forward and backward, TRANS 'N' and 'T', each applied to
     the same seeded input (sph, tri and disk families, small degrees, even and
-    odd n, several Jacobi parameters);
+    odd n, several Jacobi parameters); for sph also the vector-field transforms
+    (ft_execute_sphv2fourier / ft_execute_fourier2sphv, keys "v_fwd_N" ...);
   * rotation stages alone (ft_execute_*_hi2lo / _lo2hi);
   * the four dense connection matrices of each plan.
 
@@ -59,6 +60,10 @@ def main():
                 B = A.copy(order="F")
                 R.execute(kind, P, fwd, tr, B)
                 out[("fwd" if fwd else "bwd") + "_" + tr] = B
+                if kind == "sph":
+                    V = A.copy(order="F")
+                    R.execute("sphv", P, fwd, tr, V)
+                    out["v_" + ("fwd" if fwd else "bwd") + "_" + tr] = V
         Ps, Pinvs = R.connection(P, n)
         out["P0"], out["P1"], out["Pinv0"], out["Pinv1"] = Ps[0], Ps[1], Pinvs[0], Pinvs[1]
         R.destroy(P)

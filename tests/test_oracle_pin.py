@@ -54,6 +54,24 @@ def test_transforms_match_reference(O, path):
     O.destroy(P)
 
 
+SPH_GOLDEN = [p for p in GOLDEN if os.path.basename(p).startswith("sph_")]
+
+
+@pytest.mark.parametrize("path", SPH_GOLDEN, ids=[os.path.basename(p)[:-4] for p in SPH_GOLDEN])
+def test_vector_field_transforms_match_reference(O, path):
+    """sphv2fourier / fourier2sphv (src/drivers.c:867-899) on the sph plan."""
+    _, z = _case(path)
+    n = z["A"].shape[0]
+    P = O.plan("sph", n)
+    for fwd in (True, False):
+        for tr in "NT":
+            B = z["A"].copy(order="F")
+            O.execute_sphv(P, fwd, tr, B)
+            ref = z["v_" + ("fwd" if fwd else "bwd") + "_" + tr]
+            assert rel2(B, ref) <= 1e-14, (fwd, tr, rel2(B, ref))
+    O.destroy(P)
+
+
 @pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
 def test_rotation_stage_matches_reference(O, path):
     kind, z = _case(path)
