@@ -191,9 +191,21 @@ bool rotations_sphv(ft_rotation_plan * RP, bool hi2lo, const double * in, double
     return rotations(RP, hi2lo, in + 2 * lda, out + 2 * lda, M - 2, lda, st);
 }
 
+// sph and disk: order m occupies the column pair (2m - 1, 2m) for m = 2 .. M/2
+// (src/drivers.c:94-110, 414-430), so an even M >= 4 would put the last order's
+// second column at index M, past the matrix; such M are rejected.
+bool valid_pairs(int kind, int M) {
+    if (kind != TRI && M >= 4 && M % 2 == 0) {
+        set_error(FT_B200_EINVAL, "sph and disk matrices need an odd number of columns M");
+        return false;
+    }
+    return true;
+}
+
 bool valid_MN(int kind, int n, int N, int M) {
     if (N != n) { set_error(FT_B200_EINVAL, "N does not match the plan's n"); return false; }
     if (M < 1) { set_error(FT_B200_EINVAL, "M must be positive"); return false; }
+    if (!valid_pairs(kind, M)) return false;
     if (kind == TRI && M != N) { set_error(FT_B200_EINVAL, "tri transforms need M == N"); return false; }
     return true;
 }
@@ -436,6 +448,8 @@ void rotations_host(const ft_rotation_plan * RPc, bool hi2lo, double * A, int M,
     ft_rotation_plan * RP = const_cast<ft_rotation_plan *>(RPc);
     if (!RP || !A) { set_error(FT_B200_EINVAL, "NULL argument"); return; }
     if (RP->kind != kind) { set_error(FT_B200_EINVAL, "rotation plan of another family"); return; }
+    if (M < 1) { set_error(FT_B200_EINVAL, "M must be positive"); return; }
+    if (!valid_pairs(kind, M)) return;
     const size_t elems = (size_t) RP->n * M;
     double * d = nullptr;
     if (!cuda_ok(cudaMalloc(&d, elems * sizeof(double)), "cudaMalloc")) return;
@@ -594,7 +608,7 @@ int execute_batch_chunk(HarmonicPlan * const * H, bool forward, char TRANS, doub
     if (mixed && !B->mx_ready) {
         if (!blocked_tasks_mixed(H[0]->blocked, nf, N[0], M[0], &B->mx_tasks)) return t_status;
         if (B->mx_tasks.d_tasks) B->allocs.push_back(B->mx_tasks.d_tasks);
-        const size_t te = blocked_mixed_T_elems(H[0]->blocked, nf, N[0]);
+        const size_t te = blocked_mixed_T_elems(H[0]->blocked, B->mx_tasks.ntasks, N[0]);
         if (!cuda_ok(cudaMalloc(&B->d_T, te * sizeof(float)), "cudaMalloc(blocked task copy)")) return t_status;
         B->allocs.push_back(B->d_T);
         B->mx_ready = true;
@@ -626,7 +640,7 @@ int execute_batch_chunk(HarmonicPlan * const * H, bool forward, char TRANS, doub
         return cuda_ok(e, "rotation kernel");
     };
     auto trmm = [&](const TrmmSet & T, int mode, bool inverse, bool from_A) -> bool {
-        if (mixed) {   // sph only: the left multiplies, mode 0 (U In) or 1 (U^T In)
+        if (mixed && kind != TRI) {   // the left multiplies of sph and disk, mode 0 (U In) or 1 (U^T In)
             std::vector<double *> in(nf), out(nf);
             for (int f = 0; f < nf; f++) { in[f] = from_A ? A[f] : S[f]; out[f] = from_A ? S[f] : A[f]; }
             prof_begin(FAM_TRMM, st);
@@ -663,23 +677,24 @@ int execute_batch_chunk(HarmonicPlan * const * H, bool forward, char TRANS, doub
         }
         return true;
     };
-    // blocked products of the whole blocks, in place on the scratch matrices
-    auto blocks = [&](bool hi2lo) -> bool {
+    // blocked products of the whole blocks, in place on the scratch matrices (on_A: on A)
+    auto blocks = [&](bool hi2lo, bool on_A = false) -> bool {
         if (!blocked) return true;
+        double * const * X = on_A ? A : S.data();
         if (!mixed) {
             prof_begin(FAM_BLOCK, st);
-            const cudaError_t e = launch_blocked(H[0]->blocked, hi2lo, S.data(), nf, N[0], M[0], B->blk_tasks, B->d_counter, st);
+            const cudaError_t e = launch_blocked(H[0]->blocked, hi2lo, X, nf, N[0], M[0], B->blk_tasks, B->d_counter, st);
             prof_end(st);
             return cuda_ok(e, "blocked kernel");
         }
         prof_begin(FAM_OTHER, st);
-        cudaError_t e = launch_blocked_transpose(H[0]->blocked, true, S.data(), nf, N[0], M[0], B->d_T, B->mx_tasks, st);
+        cudaError_t e = launch_blocked_transpose(H[0]->blocked, true, X, nf, N[0], M[0], B->d_T, B->mx_tasks, st);
         prof_end(st);
         prof_begin(FAM_BLOCK, st);
         if (e == cudaSuccess) e = launch_blocked_mixed(H[0]->blocked, ns, hi2lo, B->d_T, N[0], M[0], B->mx_tasks, B->d_counter, st);
         prof_end(st);
         prof_begin(FAM_OTHER, st);
-        if (e == cudaSuccess) e = launch_blocked_transpose(H[0]->blocked, false, S.data(), nf, N[0], M[0], B->d_T, B->mx_tasks, st);
+        if (e == cudaSuccess) e = launch_blocked_transpose(H[0]->blocked, false, X, nf, N[0], M[0], B->d_T, B->mx_tasks, st);
         prof_end(st);
         return cuda_ok(e, "blocked kernels");
     };
@@ -699,7 +714,7 @@ int execute_batch_chunk(HarmonicPlan * const * H, bool forward, char TRANS, doub
     bool cur_A = true;
     if ((forward && tN) || (!forward && !tN)) {
         const bool rot_to_A = (k % 2) == 0;
-        if (!rot(true, true, rot_to_A)) return t_status;
+        if (!rot(true, true, rot_to_A) || !blocks(true, rot_to_A)) return t_status;
         cur_A = rot_to_A;
         const int lm = forward ? 0 : 1, rm = forward ? 3 : 2;
         if (left) { if (!trmm(B->left, lm, !forward, cur_A)) return t_status; cur_A = !cur_A; }
@@ -710,7 +725,7 @@ int execute_batch_chunk(HarmonicPlan * const * H, bool forward, char TRANS, doub
         const int rm = forward ? 2 : 3, lm = forward ? 1 : 0;
         if (right) { if (!trmm(B->right, rm, !forward, cur_A)) return t_status; cur_A = !cur_A; }
         if (left) { if (!trmm(B->left, lm, !forward, cur_A)) return t_status; cur_A = !cur_A; }
-        if (!rot(false, cur_A, true)) return t_status;
+        if (!blocks(false, cur_A) || !rot(false, cur_A, true)) return t_status;
     }
     return FT_B200_OK;
 }
@@ -845,6 +860,7 @@ int ft_b200_execute_sphv_dev(const ft_harmonic_plan * P, int forward, char TRANS
 int ft_b200_rotations_dev(const ft_rotation_plan * RP, int hi2lo, double * dA, int M, void * stream) {
     clear_error();
     if (!RP || !dA || M < 1) { set_error(FT_B200_EINVAL, "bad argument"); return t_status; }
+    if (!valid_pairs(RP->kind, M)) return t_status;
     rotations(const_cast<ft_rotation_plan *>(RP), hi2lo != 0, dA, dA, M, RP->n, static_cast<cudaStream_t>(stream));
     return t_status;
 }
@@ -859,10 +875,6 @@ int ft_b200_execute_shared_dev(const ft_harmonic_plan * P, int forward, char TRA
     if (precision != FT_B200_FP64 && precision != FT_B200_FP64_BLOCKED && precision != FT_B200_MIXED_BF16 &&
         precision != FT_B200_MIXED_BF16X4) {
         set_error(FT_B200_EINVAL, "unknown precision");
-        return t_status;
-    }
-    if (precision != FT_B200_FP64 && H->kind != SPH) {
-        set_error(FT_B200_EUNSUPPORTED, "the blocked sweeps are built for sph plans");
         return t_status;
     }
     for (int f = 0; f < nfields; f++)

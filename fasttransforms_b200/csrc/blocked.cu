@@ -1,25 +1,34 @@
-// Blocked rotation sweeps for fields that share one sph plan.
+// Blocked rotation sweeps for fields that share one plan (sph, disk or tri).
 //
 // The sweeps of a parity are cut into blocks of BLK consecutive sweeps on a
-// fixed grid (block beta holds sweeps j = p + 2*BLK*beta + 2*BLK - 2 - 2s,
-// s = 0 .. BLK-1), and each block into parallelogram tiles: tile k holds the
+// fixed grid (block beta holds sweeps j = p + STEP*BLK*(beta + 1) - STEP - STEP*s,
+// s = 0 .. BLK-1, with STEP = 2 for sph and disk and 1 for tri, whose sweeps
+// have no parity), and each block into parallelogram tiles: tile k holds the
 // rotations of sweep s at chain positions [k*TL + s, k*TL + s + TL), which
-// touch the TL + BLK = WIN positions [k*TL, k*TL + WIN).  The rotations of a
-// tile multiply into one dense orthogonal WIN x WIN matrix Q (built in FP64 at
-// plan time), so a block is a chain of tile products X <- Q X running down the
-// column (hi2lo; Q^T running up for lo2hi), consecutive tiles overlapping in
-// BLK positions.  The X of a product is every column that needs the whole
-// block, across all fields: that is what turns the sweeps into tensor-core
-// work.  A column's sweeps above its last whole block (its "head", fewer than
-// BLK sweeps) run in the direct rotation kernel, before the blocks in hi2lo
-// and after them in lo2hi.
+// touch the TL + BLK = WIN positions [k*TL, k*TL + WIN).  (Every family's
+// sweep j rotates the chain positions 0 .. top(j), and the top rises by one
+// from one sweep of a block to the next.)  The rotations of a tile multiply
+// into one dense orthogonal WIN x WIN matrix Q (built in FP64 at plan time), so
+// a block is a chain of tile products X <- Q X running down the column (hi2lo;
+// Q^T running up for lo2hi), consecutive tiles overlapping in BLK positions.
+// The X of a product is every column that needs the whole block, across all
+// fields: that is what turns the sweeps into tensor-core work.  A column's
+// sweeps above its last whole block (its "head", fewer than BLK sweeps) run in
+// the direct rotation kernel, before the blocks in hi2lo and after them in
+// lo2hi.
 //
-// Kernel: persistent CTAs over tasks (field, parity, band), a band being the
-// 2*BLK columns of BLK consecutive orders that need the same blocks; 8 warps,
-// warps 0-3 do chain 0 (even rows) and 4-7 chain 1 (odd rows) of each tile
-// product as 32 x 32 DMMA (mma.m8n8k4.f64) tiles.  The WIN-position window of
-// both chains stays in shared memory as a circular buffer (slot = position mod
-// WIN), so the overlap rows never move.
+// Chains: a sph column is two chains (even and odd rows, rotations between
+// rows k and k + 2); a disk or tri column is one chain (rows k and k + 1).  A
+// task has two chain slots: the two chains of the same columns for sph, the
+// same band of two groups of fields for disk and tri (whose tiles are the same
+// for both slots and stored once).
+//
+// FP64 kernel: persistent CTAs over tasks (fields, parity, band), a band being
+// the columns of BLK consecutive orders of one parity that need the same
+// blocks; 8 warps, warps 0-3 do slot 0 and 4-7 slot 1 of each tile product as
+// 32 x 32 DMMA (mma.m8n8k4.f64) tiles.  The WIN-position window of both slots
+// stays in shared memory as a circular buffer (slot = position mod WIN), so
+// the overlap rows never move.
 #include <algorithm>
 #include <cstdio>
 
@@ -39,14 +48,53 @@ constexpr int LDQ = WIN + 4;       // padded rows of Q in shared memory
 constexpr int LDX = FT + 1;        // padded rows of the window
 constexpr int NT = 256;
 
-struct BlkTask { int field, p, band; };
+// A task: fields field .. field + fields per task - 1, parity p, band >= 1 (orders of the
+// band need blocks 0 .. band - 1; nb = min(band, blocks of the plan), the blocks above
+// those hold no rotations), and its index in the task-major copy of the split-BF16 path.
+struct BlkTask { int field, p, band, nb, slot; };
+
+// Family-dependent shape of the blocked stage.
+//   sph:  two chains (even / odd rows) of (N + 1) / 2 positions; sweeps j = p, p + 2, ...
+//   disk: one chain (the column) of N positions; sweeps j = p, p + 2, ...
+//   tri:  one chain (the column) of N positions; sweeps j = 0, 1, ...
+// A band of a field: BLK orders of one parity, two columns each (cos, sin) for sph and
+// disk, one for tri (src/drivers.c:94-110, 314-326, 414-430 for the column of an order).
+struct Shape {
+    int kind;
+    __host__ __device__ bool two_chains() const { return kind == SPH; }
+    __host__ __device__ int step() const { return kind == TRI ? 1 : 2; }
+    __host__ __device__ int band_cols() const { return kind == TRI ? BLK : 2 * BLK; }
+    __host__ __device__ int positions(int N) const { return kind == SPH ? (N + 1) / 2 : N; }
+    // matrix row of chain position pos of chain c (also the sweep's table entry)
+    __host__ __device__ int row(int pos, int c) const { return kind == SPH ? 2 * pos + c : pos; }
+    // highest sweep of block beta of parity p
+    __host__ __device__ int block_top(int p, int beta) const { return p + step() * BLK * (beta + 1) - step(); }
+    // fields of one chain slot of a task `width` columns wide, and of the whole task
+    __host__ __device__ int slot_fields(int width) const { return width / band_cols(); }
+    __host__ __device__ int task_fields(int width) const { return slot_fields(width) * (two_chains() ? 1 : 2); }
+    // column i of chain slot c of task t: its field f and matrix column, -1 past the last order
+    __host__ __device__ long long column(const BlkTask & t, int width, int c, int i, int mlast, int & f) const {
+        const int bc = band_cols();
+        f = t.field + (two_chains() ? 0 : c * slot_fields(width)) + i / bc;
+        const int n = i % bc;
+        if (kind == TRI) {
+            const int m = BLK * t.band + n;
+            return m <= mlast ? m : -1;
+        }
+        const int m = t.p + 2 * BLK * t.band + 2 * (n >> 1);
+        return m <= mlast ? 2LL * m - 1 + (n & 1) : -1;
+    }
+};
 
 struct BlockedLaunch {
     double * A[kMaxFields];        // in place
+    int nf;
+    Shape sh;
     const double * Q;              // all tiles, row-major WIN x WIN each
     const long long * qbase;       // [2 parities][nbeta]: index of tile (c = 0, k = -1)
     const int * kmax;              // [2][nbeta]
     int nbeta;                     // blocks per parity slot
+    int cq;                        // 1: one tile chain per slot (sph), 0: both slots share chain 0
     const BlkTask * tasks;
     int ntasks;
     int * counter;
@@ -58,31 +106,28 @@ __device__ __forceinline__ void dmma(double & d0, double & d1, double a, double 
                  : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
 }
 
-__device__ __forceinline__ int top_sph(int N, int j, int c) {
-    const int x = N - 3 - j - c;
-    return x >= 0 ? x / 2 : -((1 - x) / 2);
-}
-
 // ---------------------------------------------------------------------------
 // plan time: Q of every tile.  One CTA per (parity, block, chain, tile); the
 // WIN columns of Q evolve independently under the rotations' row operations,
-// one thread per column.
+// one thread per column.  Rotation (s, c) on positions (i, i + 1) of the chain
+// is the reference's Givens step (src/rotations/rotations_default.c:31-36, 45-50,
+// 59-64), entry Geo::table_base(j) + row(i) of the packed tables.
 // ---------------------------------------------------------------------------
-__global__ void build_q_kernel(const double2 * __restrict__ sc, int N, int p, int beta, int c, int kmax, double * Qout) {
+__global__ void build_q_kernel(const double2 * __restrict__ sc, Shape sh, int N, int p, int beta, int c, double * Qout) {
     __shared__ double Q[WIN][WIN + 1];
     const int k = (int) blockIdx.x - 1;   // tiles k = -1 .. kmax
     const int col = threadIdx.x;
     for (int r = 0; r < WIN; ++r) Q[r][col] = r == col ? 1.0 : 0.0;
-    const int j0 = p + 2 * BLK * beta + 2 * BLK - 2;
-    const int T0 = top_sph(N, j0, c);
+    const int j0 = sh.block_top(p, beta);
+    const int T0 = Geo::top(sh.kind, N, j0, c);
     const int lo = k * TL;
     for (int s = 0; s < BLK; ++s) {
-        const int j = j0 - 2 * s;
-        const long long base = (long long) j * (2 * N + 1 - j) / 2;
+        const int j = j0 - sh.step() * s;
+        const long long base = Geo::table_base(sh.kind, N, j);
         const int Ts = T0 + s;
         const int ihi = min(lo + s + TL - 1, Ts), ilo = max(lo + s, 0);
         for (int i = ihi; i >= ilo; --i) {
-            const double2 v = sc[base + 2 * i + c];
+            const double2 v = sc[base + sh.row(i, c)];
             const int a = i - lo;
             const double x = Q[a][col], y = Q[a + 1][col];
             Q[a][col] = __fma_rn(v.y, x, __dmul_rn(v.x, y));
@@ -90,7 +135,6 @@ __global__ void build_q_kernel(const double2 * __restrict__ sc, int N, int p, in
         }
     }
     __syncthreads();
-    (void) kmax;
     double * out = Qout + (long long) blockIdx.x * WIN * WIN;
     for (int r = 0; r < WIN; ++r) out[(long long) r * WIN + col] = Q[r][col];
 }
@@ -108,7 +152,9 @@ __global__ void __launch_bounds__(NT, 1) blocked_kernel(const __grid_constant__ 
     const int c_w = warp >> 2;                       // chain of this warp
     const int wm = ((warp & 3) >> 1) * 32, wn = (warp & 1) * 32;
     const int fr = lane >> 2, fc = lane & 3;
-    const int N = L.N, mlast = L.M / 2;
+    const int N = L.N, mlast = Geo::last_order(L.sh.kind, L.M);
+    const Shape sh = L.sh;
+    const bool two = sh.two_chains();
 
     for (;;) {
         if (tid == 0) s_task = atomicAdd(L.counter, 1);
@@ -117,16 +163,16 @@ __global__ void __launch_bounds__(NT, 1) blocked_kernel(const __grid_constant__ 
         __syncthreads();
         if (t_id >= L.ntasks) break;
         const BlkTask T = L.tasks[t_id];
-        double * const A = L.A[T.field];
-        const int p = T.p, band = T.band;
-        // task column n: order m = p + 2*BLK*band + 2*(n/2), column 2m - 1 + (n & 1)
-        auto col_of = [&](int n, bool & ok) -> long long {
-            const int m = p + 2 * BLK * band + 2 * (n >> 1);
-            ok = m <= mlast;
-            return 2LL * m - 1 + (n & 1);
+        const int p = T.p;
+        // column n of slot c: its matrix (null past the fields or the last order) and column
+        auto col_of = [&](int c, int n, double *& A) -> long long {
+            int f;
+            const long long col = sh.column(T, FT, c, n, mlast, f);
+            A = (col >= 0 && f < L.nf) ? L.A[f] : nullptr;
+            return col;
         };
-        for (int bi = 0; bi < band; ++bi) {
-            const int beta = HI2LO ? band - 1 - bi : bi;
+        for (int bi = 0; bi < T.nb; ++bi) {
+            const int beta = HI2LO ? T.nb - 1 - bi : bi;
             const int kmax = L.kmax[p * L.nbeta + beta];
             const long long qb = L.qbase[p * L.nbeta + beta];
             const int nk = kmax + 2;
@@ -137,21 +183,22 @@ __global__ void __launch_bounds__(NT, 1) blocked_kernel(const __grid_constant__ 
                 // positions entering the window: all of it for the first tile, else TL of them
                 const int plo = first ? lo : (HI2LO ? lo : lo + BLK);
                 const int pcnt = first ? WIN : TL;
-                // load rows [2*plo, 2*(plo + pcnt)) of the FT columns
+                // load positions [plo, plo + pcnt) of both slots' FT columns
                 for (int f = tid; f < FT * 2 * pcnt; f += NT) {
                     const int n = f / (2 * pcnt), r = f % (2 * pcnt);
-                    const int pos = plo + (r >> 1), c = r & 1;
-                    const int row = 2 * pos + c;
-                    bool ok;
-                    const long long col = col_of(n, ok);
+                    const int c = two ? (r & 1) : r / pcnt;
+                    const int pos = plo + (two ? (r >> 1) : r % pcnt);
+                    const int row = sh.row(pos, c);
+                    double * A;
+                    const long long col = col_of(c, n, A);
                     double v = 0.0;
-                    if (ok && pos >= 0 && row < N) v = __ldcg(A + col * N + row);
+                    if (A && pos >= 0 && row < N) v = __ldcg(A + col * N + row);
                     Xw[((pos & (WIN - 1)) * 2 + c) * LDX + n] = v;
                 }
-                // both chains' Q for this tile
+                // both slots' Q for this tile (the same tile for one-chain families)
                 for (int f = tid; f < 2 * WIN * WIN; f += NT) {
                     const int c = f / (WIN * WIN), e = f % (WIN * WIN);
-                    const double * q = L.Q + (qb + (long long) c * nk + (k + 1)) * WIN * WIN;
+                    const double * q = L.Q + (qb + (long long) c * L.cq * nk + (k + 1)) * WIN * WIN;
                     Qs[(c * WIN + e / WIN) * LDQ + e % WIN] = __ldg(q + e);
                 }
                 __syncthreads();
@@ -187,16 +234,16 @@ __global__ void __launch_bounds__(NT, 1) blocked_kernel(const __grid_constant__ 
                     const int m = wm + a * 8 + fr;
                     const int pos = lo + m;
                     const bool fin = last || (HI2LO ? m >= BLK : m < TL);
-                    const int row = 2 * pos + c_w;
+                    const int row = sh.row(pos, c_w);
 #pragma unroll
                     for (int b = 0; b < 4; ++b)
 #pragma unroll
                         for (int h = 0; h < 2; ++h) {
                             const int n = wn + b * 8 + 2 * fc + h;
                             if (fin) {
-                                bool ok;
-                                const long long col = col_of(n, ok);
-                                if (ok && pos >= 0 && row < N) __stcg(A + col * N + row, acc[a][b][h]);
+                                double * A;
+                                const long long col = col_of(c_w, n, A);
+                                if (A && pos >= 0 && row < N) __stcg(A + col * N + row, acc[a][b][h]);
                             } else {
                                 Xw[((pos & (WIN - 1)) * 2 + c_w) * LDX + n] = acc[a][b][h];
                             }
@@ -232,15 +279,15 @@ __global__ void __launch_bounds__(NT, 1) blocked_kernel(const __grid_constant__ 
 // rounding of y, all unbiased; a window position is carried between tiles as
 // FP32, in global memory the matrix stays FP64.
 //
-// A task is 128 columns: one band (BLK orders x cos, sin) of two fields.  The
-// product is D^T = X^T op(Q)^T with M = 128 (columns), N = WIN (output
-// positions), K = WIN (input positions), so each thread of the epilogue owns
-// one column (its TMEM lane) and half of the window.  Warps 0-7 carry chain 0,
-// warps 8-15 chain 1, warp 16 issues the MMAs (one thread) and owns the TMEM
-// allocation, warp 17 streams the tile images into shared memory, one buffer
-// per chain.  The
-// chains alternate on the tensor cores, so one chain's epilogue runs while the
-// other chain's products are in flight.
+// A task is two chain slots of 128 columns each: one band of two fields (sph,
+// both chains), four fields (disk) or eight (tri).  The product is
+// D^T = X^T op(Q)^T with M = 128 (columns), N = WIN (output positions),
+// K = WIN (input positions), so each thread of the epilogue owns one column
+// (its TMEM lane) and half of the window.  Warps 0-7 carry slot 0, warps 8-15
+// slot 1, warp 16 issues the MMAs (one thread) and owns the TMEM allocation,
+// warp 17 streams the tile images into shared memory, one buffer per slot.
+// The slots alternate on the tensor cores, so one slot's epilogue runs while
+// the other slot's products are in flight.
 // ---------------------------------------------------------------------------
 constexpr int MX_COLS = 128;                          // columns per task
 constexpr int MX_PIECE = MX_COLS * WIN * 2;           // bytes of one BF16 piece of one chain's window
@@ -256,24 +303,21 @@ template <int NS> struct MxCfg {
 };
 
 // The blocked stage works on its own copy of the columns, task-major, in FP32:
-// task (pair of fields, parity, band) -> 128 columns, and element (chain c,
-// position pos, column i) at ((c * Lq + pos / 4) * 128 + i) * 4 + pos % 4, with
-// Lq position quads per chain.  A thread moves four consecutive positions of
-// its column as one 16-byte access, and a warp (32 adjacent columns) 512
-// contiguous bytes.  Positions past a chain's end hold zeros: the tile
-// products never rotate them, so they stay zero.
-__host__ __device__ __forceinline__ long long task_index(const BlkTask & t, int nbeta) {
-    return ((long long) (t.field >> 1) * 2 + t.p) * nbeta + (t.band - 1);
-}
-
+// task (fields, parity, band) -> 2 slots x 128 columns, and element (slot c,
+// position pos, column i) at ((c * Lq + pos / 4) * 128 + i) * 4 + pos % 4 of the
+// task's part, with Lq position quads per slot.  A thread moves four
+// consecutive positions of its column as one 16-byte access, and a warp (32
+// adjacent columns) 512 contiguous bytes.  Positions past a chain's end hold
+// zeros: the tile products never rotate them, so they stay zero.
 struct MixedLaunch {
     float * T;                     // task-major copy of the columns (in place)
-    int Lq;                        // position quads per chain in T
-    const __nv_bfloat16 * img;     // tile images of the direction: [tile][chain][piece][WIN x WIN swizzled]
-    const long long * qbase;       // [2][nbeta], as for the FP64 tiles (2 chains per tile)
+    int Lq;                        // position quads per slot in T
+    const __nv_bfloat16 * img;     // tile images of the direction: [tile][slot chain][piece][WIN x WIN swizzled]
+    const long long * qbase;       // [2][nbeta], as for the FP64 tiles
     const int * kmax;
     int nbeta;
-    const BlkTask * tasks;         // field: first field of the pair
+    int cq;                        // 1: one tile chain per slot (sph), 0: both slots share chain 0
+    const BlkTask * tasks;         // field: first field of the task
     int ntasks;
     int * counter;
     int * err;
@@ -281,13 +325,14 @@ struct MixedLaunch {
 };
 
 // Q of one (parity, block): every tile and chain into its NS-slice BF16 image
-// (B[o][w] = Q[o][w] for hi2lo, Q[w][o] for lo2hi; rows o K-major, swizzled).
+// (B[o][w] = Q[o][w] for hi2lo, Q[w][o] for lo2hi; rows o K-major, swizzled);
+// tile k + 1 of chain c of the block is image qb + (k + 1) * nch + c.
 template <int NS>
-__global__ void build_img_kernel(const double * __restrict__ Q, long long qb, int nk, bool transpose,
+__global__ void build_img_kernel(const double * __restrict__ Q, long long qb, int nk, int nch, bool transpose,
                                  __nv_bfloat16 * __restrict__ img) {
     const int k1 = blockIdx.x, c = blockIdx.y;    // tile k = k1 - 1
     const double * q = Q + (qb + (long long) c * nk + k1) * WIN * WIN;
-    unsigned char * out = reinterpret_cast<unsigned char *>(img) + ((qb / 2 + k1) * 2 + c) * (long long) MxCfg<NS>::QCHAIN;
+    unsigned char * out = reinterpret_cast<unsigned char *>(img) + (qb + (long long) k1 * nch + c) * (long long) MxCfg<NS>::QCHAIN;
     for (int e = threadIdx.x; e < WIN * WIN; e += blockDim.x) {
         const int o = e / WIN, w = e % WIN;
         // 256 q = j_0 + j_1 2^-9 + ..., integers |j| <= 2^8
@@ -383,29 +428,30 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
         __syncthreads();
         if (t_id >= L.ntasks || s_abort) break;
         const BlkTask T = L.tasks[t_id];
-        const int p = T.p, band = T.band;
+        const int p = T.p, nb = T.nb;
 
         if (warp == 17) {
             // ---- tile images into shared memory, one buffer per chain ----
             if (lane == 0) {
-                for (int bi = 0; bi < band && !s_abort; ++bi) {
-                    const int beta = HI2LO ? band - 1 - bi : bi;
+                const int nch = 1 + L.cq;                 // tile chains stored per tile
+                for (int bi = 0; bi < nb && !s_abort; ++bi) {
+                    const int beta = HI2LO ? nb - 1 - bi : bi;
                     const int kmax = L.kmax[p * L.nbeta + beta];
-                    const long long tb = L.qbase[p * L.nbeta + beta] / 2;
-                    const unsigned char * const img0 = reinterpret_cast<const unsigned char *>(L.img) + tb * 2LL * QCHAIN;
+                    const long long tb = L.qbase[p * L.nbeta + beta];
+                    const unsigned char * const img0 = reinterpret_cast<const unsigned char *>(L.img) + tb * QCHAIN;
                     // the block's first tiles into L2 ahead of their copies
                     for (int ki = 0; ki < 2 && ki < kmax + 2; ++ki)
-                        tc::prefetch_l2(img0 + (HI2LO ? kmax - ki + 1 : ki) * 2LL * QCHAIN, 2 * QCHAIN);
+                        tc::prefetch_l2(img0 + (HI2LO ? kmax - ki + 1 : ki) * (long long) nch * QCHAIN, nch * QCHAIN);
                     for (int ki = 0; ki < kmax + 2 && !s_abort; ++ki, ++qt) {
                         const int k = HI2LO ? kmax - ki : ki - 1;
                         const int u = (int) qt;
-                        const unsigned char * src = img0 + (k + 1) * 2LL * QCHAIN;
+                        const unsigned char * src = img0 + (k + 1) * (long long) nch * QCHAIN;
                         if (ki + 2 < kmax + 2)   // two tiles ahead
-                            tc::prefetch_l2(img0 + (HI2LO ? k - 2 + 1 : k + 2 + 1) * 2LL * QCHAIN, 2 * QCHAIN);
+                            tc::prefetch_l2(img0 + (HI2LO ? k - 2 + 1 : k + 2 + 1) * (long long) nch * QCHAIN, nch * QCHAIN);
                         for (int c = 0; c < 2; ++c) {
                             if (!tc::mbar_wait(&bar_qempty[c], (u & 1) ^ 1, &s_abort)) { fail(); break; }
                             tc::mbar_arrive_expect_tx(&bar_qfull[c], QCHAIN);
-                            tc::bulk_g2s(Qs + c * QCHAIN, src + c * QCHAIN, QCHAIN, &bar_qfull[c]);
+                            tc::bulk_g2s(Qs + c * QCHAIN, src + c * L.cq * QCHAIN, QCHAIN, &bar_qfull[c]);
                         }
                         last_u = u;
                     }
@@ -416,8 +462,8 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
             // ---- MMA issue ----
             if (lane == 0) {
                 const uint32_t xs0 = tc::smem_addr(Xs), qs0 = tc::smem_addr(Qs);
-                for (int bi = 0; bi < band && !s_abort; ++bi) {
-                    const int beta = HI2LO ? band - 1 - bi : bi;
+                for (int bi = 0; bi < nb && !s_abort; ++bi) {
+                    const int beta = HI2LO ? nb - 1 - bi : bi;
                     const int kmax = L.kmax[p * L.nbeta + beta];
                     for (int ki = 0; ki < kmax + 2 && !s_abort; ++ki, ++qt) {
                         const int k = HI2LO ? kmax - ki : ki - 1;
@@ -460,7 +506,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
             const int r = 32 * quarter + lane;
             const int fh = HI2LO ? 1 : 0;                 // the half whose outputs leave the window
             // this column's quads: quad Q of the chain at Tq[Q * MX_COLS]
-            float4 * const Tq = reinterpret_cast<float4 *>(L.T + task_index(T, L.nbeta) * (8LL * L.Lq * MX_COLS)) +
+            float4 * const Tq = reinterpret_cast<float4 *>(L.T + T.slot * (8LL * L.Lq * MX_COLS)) +
                                 (long long) c * L.Lq * MX_COLS + r;
             const int Pend = 4 * L.Lq;                    // positions held in the copy
             unsigned char * const xrow = Xs + c * NS * MX_PIECE;
@@ -506,8 +552,8 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
                 tc::mbar_arrive(&bar_xready[c]);
                 return true;
             };
-            for (int bi = 0; bi < band && !s_abort; ++bi) {
-                const int beta = HI2LO ? band - 1 - bi : bi;
+            for (int bi = 0; bi < nb && !s_abort; ++bi) {
+                const int beta = HI2LO ? nb - 1 - bi : bi;
                 const int kmax = L.kmax[p * L.nbeta + beta];
                 const int nk = kmax + 2;
                 float src[TL];
@@ -596,23 +642,37 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
 
 struct BlockedPlan {
     int n = 0;
+    Shape sh{SPH};
+    int nch = 2;                // tile chains per block: 2 (sph), 1 (disk, tri)
+    int npar = 2;               // parity slots: 2 (sph, disk), 1 (tri)
     int nbeta = 0;
     double * d_Q = nullptr;
     long long * d_qbase = nullptr;
     int * d_kmax = nullptr;
-    std::vector<int> kmax;      // [2][nbeta]
+    std::vector<int> kmax;      // [npar][nbeta]
     std::vector<long long> qbase;
-    long long ntiles = 0;       // tile-chain pairs x 2
+    long long ntiles = 0;       // tiles over all blocks and chains
     size_t bytes = 0;
     __nv_bfloat16 * d_img[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // tile images [3 or 4 slices][hi2lo, lo2hi]
     int * d_err = nullptr;      // set by a tensor-core kernel whose wait ran out
 };
 
-int kmax_of(int N, int p, int beta) {
-    const int j0 = p + 2 * BLK * beta + 2 * BLK - 2;
-    const int x = N - 3 - j0;
-    const int T0 = x >= 0 ? x / 2 : -((1 - x) / 2);
+// last tile of block beta of parity p (chain 0, the longer one): tiles k = -1 .. kmax
+int kmax_of(const Shape & sh, int N, int p, int beta) {
+    const int T0 = Geo::top(sh.kind, N, sh.block_top(p, beta), 0);
     return T0 >= 0 ? T0 / TL : -1;
+}
+
+// blocks holding any rotation: block beta of parity p rotates something iff its lowest
+// sweep does (the tops fall as j rises)
+int blocks_of(const Shape & sh, int N, int npar) {
+    int nb = 0;
+    for (int p = 0; p < npar; p++) {
+        int b = 0;
+        while (Geo::top(sh.kind, N, sh.block_top(p, b) - sh.step() * (BLK - 1), 0) >= 0) b++;
+        nb = std::max(nb, b);
+    }
+    return nb;
 }
 
 bool cuda_fine(cudaError_t e, const char * what) {
@@ -621,24 +681,64 @@ bool cuda_fine(cudaError_t e, const char * what) {
     return false;
 }
 
+int quads(const BlockedPlan * B, int N) { return (B->sh.positions(N) + 3) / 4; }
+
+// Tasks (fields, parity, band >= 1) `width` columns per chain slot, longest first.
+bool make_tasks(const BlockedPlan * B, int width, int nf, int M, BlkTaskList * out) {
+    const Shape & sh = B->sh;
+    const int mlast = Geo::last_order(sh.kind, M);
+    const int fpt = sh.task_fields(width);
+    std::vector<std::pair<long long, BlkTask>> v;
+    for (int f = 0; f < nf; f += fpt)
+        for (int p = 0; p < B->npar; p++)
+            // band b holds the orders p + STEP BLK b + STEP o, o < BLK, which need blocks 0 .. b - 1
+            for (int band = 1; p + sh.step() * BLK * band <= mlast; band++) {
+                const int nb = std::min(band, B->nbeta);
+                if (nb == 0) break;
+                long long cost = 0;
+                for (int beta = 0; beta < nb; beta++) cost += B->kmax[p * B->nbeta + beta] + 2;
+                v.push_back({cost, BlkTask{f, p, band, nb, 0}});
+            }
+    std::stable_sort(v.begin(), v.end(), [](const auto & a, const auto & b) { return a.first > b.first; });
+    std::vector<BlkTask> t;
+    for (auto & x : v) {
+        t.push_back(x.second);
+        t.back().slot = (int) t.size() - 1;
+    }
+    out->ntasks = (int) t.size();
+    if (t.empty()) return true;
+    if (!cuda_fine(cudaMalloc(&out->d_tasks, sizeof(BlkTask) * t.size()), "cudaMalloc(blocked tasks)")) return false;
+    return cuda_fine(cudaMemcpy(out->d_tasks, t.data(), sizeof(BlkTask) * t.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
+}
+
+int sm_count() {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
 }  // namespace
 
-// Build (once) the tile matrices of a sph plan.
+// Build (once) the tile matrices of a plan.
 void * blocked_plan_build(HarmonicPlan * H) {
     const int N = H->n;
     BlockedPlan * B = new BlockedPlan();
     B->n = N;
-    // blocks exist for sweeps j <= N - 3: beta with p + 2*BLK*beta + 2*BLK - 2 <= N - 3
-    B->nbeta = std::max(0, (N - 1) / (2 * BLK));
-    std::vector<long long> qbase(2 * std::max(1, B->nbeta));
-    B->kmax.assign(2 * std::max(1, B->nbeta), -1);
+    B->sh = Shape{H->kind};
+    B->nch = B->sh.two_chains() ? 2 : 1;
+    B->npar = B->sh.step();
+    B->nbeta = blocks_of(B->sh, N, B->npar);
+    const int slots = B->npar * std::max(1, B->nbeta);
+    std::vector<long long> qbase(slots);
+    B->kmax.assign(slots, -1);
     long long tiles = 0;
-    for (int p = 0; p < 2; p++)
+    for (int p = 0; p < B->npar; p++)
         for (int beta = 0; beta < B->nbeta; beta++) {
-            const int km = kmax_of(N, p, beta);
+            const int km = kmax_of(B->sh, N, p, beta);
             B->kmax[p * B->nbeta + beta] = km;
             qbase[p * B->nbeta + beta] = tiles;
-            tiles += 2LL * (km + 2);
+            tiles += (long long) B->nch * (km + 2);
         }
     B->bytes = (size_t) std::max(1LL, tiles) * WIN * WIN * sizeof(double);
     B->qbase = qbase;
@@ -649,12 +749,12 @@ void * blocked_plan_build(HarmonicPlan * H) {
               cuda_fine(cudaMalloc(&B->d_kmax, sizeof(int) * B->kmax.size()), "cudaMalloc") &&
               cuda_fine(cudaMemcpy(B->d_qbase, qbase.data(), sizeof(long long) * qbase.size(), cudaMemcpyHostToDevice), "cudaMemcpy") &&
               cuda_fine(cudaMemcpy(B->d_kmax, B->kmax.data(), sizeof(int) * B->kmax.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
-    for (int p = 0; ok && p < 2; p++)
+    for (int p = 0; ok && p < B->npar; p++)
         for (int beta = 0; ok && beta < B->nbeta; beta++) {
             const int km = B->kmax[p * B->nbeta + beta];
-            for (int c = 0; c < 2; c++) {
+            for (int c = 0; c < B->nch; c++) {
                 double * out = B->d_Q + (qbase[p * B->nbeta + beta] + (long long) c * (km + 2)) * WIN * WIN;
-                build_q_kernel<<<km + 2, WIN>>>(sc, N, p, beta, c, km, out);
+                build_q_kernel<<<km + 2, WIN>>>(sc, B->sh, N, p, beta, c, out);
                 count_launch();
             }
             ok = cuda_fine(cudaGetLastError(), "build_q_kernel");
@@ -686,10 +786,13 @@ cudaError_t launch_blocked(void * plan, bool hi2lo, double * const * A, int nf, 
     if (tl.ntasks == 0) return cudaSuccess;
     static thread_local BlockedLaunch L;
     for (int f = 0; f < nf; f++) L.A[f] = A[f];
+    L.nf = nf;
+    L.sh = B->sh;
     L.Q = B->d_Q;
     L.qbase = B->d_qbase;
     L.kmax = B->d_kmax;
     L.nbeta = B->nbeta;
+    L.cq = B->nch - 1;
     L.tasks = reinterpret_cast<const BlkTask *>(tl.d_tasks);
     L.ntasks = tl.ntasks;
     L.counter = counter;
@@ -701,41 +804,15 @@ cudaError_t launch_blocked(void * plan, bool hi2lo, double * const * A, int nf, 
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(counter, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
-    int dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int ctas = std::min(sms, tl.ntasks);
-    kern<<<ctas, NT, shm, st>>>(L);
+    kern<<<std::min(sm_count(), tl.ntasks), NT, shm, st>>>(L);
     count_launch();
     return cudaGetLastError();
 }
 
-// Tasks (field, parity, band >= 1), longest first.
+// FP64 tasks: FT columns per chain slot (one sph field, two disk fields, four tri fields per task).
 bool blocked_tasks(void * plan, int nf, int N, int M, BlkTaskList * out) {
-    BlockedPlan * B = static_cast<BlockedPlan *>(plan);
-    const int mlast = M / 2;
-    std::vector<std::pair<long long, BlkTask>> v;
-    for (int f = 0; f < nf; f++)
-        for (int p = 0; p < 2; p++) {
-            const int m0 = p == 0 ? 2 : 3;
-            for (int band = 1; p + 2 * BLK * band <= mlast; band++) {
-                if (p + 2 * BLK * band < m0) continue;
-                if (band > B->nbeta) {   // cannot happen for M = 2N - 1; guards the tile tables
-                    set_error(FT_B200_EINVAL, "column band beyond the plan's blocks");
-                    return false;
-                }
-                long long cost = 0;
-                for (int beta = 0; beta < band; beta++) cost += B->kmax[p * B->nbeta + beta] + 2;
-                v.push_back({cost, BlkTask{f, p, band}});
-            }
-        }
-    std::stable_sort(v.begin(), v.end(), [](const auto & a, const auto & b) { return a.first > b.first; });
-    std::vector<BlkTask> t;
-    for (auto & x : v) t.push_back(x.second);
-    out->ntasks = (int) t.size();
-    if (t.empty()) return true;
-    if (!cuda_fine(cudaMalloc(&out->d_tasks, sizeof(BlkTask) * t.size()), "cudaMalloc(blocked tasks)")) return false;
-    return cuda_fine(cudaMemcpy(out->d_tasks, t.data(), sizeof(BlkTask) * t.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
+    (void) N;
+    return make_tasks(static_cast<BlockedPlan *>(plan), FT, nf, M, out);
 }
 
 // Split-BF16 tile images with ns (3 or 4) slices, both directions (built once
@@ -749,18 +826,18 @@ bool blocked_mixed_prepare(void * plan, int ns) {
         if (!cuda_fine(cudaMemset(B->d_err, 0, sizeof(int)), "cudaMemset")) return false;
     }
     if (img[0] && img[1]) return true;
-    const size_t bytes = (size_t) std::max(1LL, B->ntiles / 2) * 2 * (size_t) ns * MX_QPIECE;
+    const size_t bytes = (size_t) std::max(1LL, B->ntiles) * (size_t) ns * MX_QPIECE;
     for (int d = 0; d < 2; d++) {
         if (img[d]) continue;
         void * p = nullptr;
         if (!cuda_fine(cudaMalloc(&p, bytes), "cudaMalloc(split tile images)")) return false;
         img[d] = static_cast<__nv_bfloat16 *>(p);
-        for (int par = 0; par < 2; par++)
+        for (int par = 0; par < B->npar; par++)
             for (int beta = 0; beta < B->nbeta; beta++) {
                 const int nk = B->kmax[par * B->nbeta + beta] + 2;
                 const long long qb = B->qbase[par * B->nbeta + beta];
-                if (ns == 3) build_img_kernel<3><<<dim3(nk, 2), 256>>>(B->d_Q, qb, nk, d == 1, img[d]);
-                else         build_img_kernel<4><<<dim3(nk, 2), 256>>>(B->d_Q, qb, nk, d == 1, img[d]);
+                if (ns == 3) build_img_kernel<3><<<dim3(nk, B->nch), 256>>>(B->d_Q, qb, nk, B->nch, d == 1, img[d]);
+                else         build_img_kernel<4><<<dim3(nk, B->nch), 256>>>(B->d_Q, qb, nk, B->nch, d == 1, img[d]);
                 count_launch();
             }
         if (!cuda_fine(cudaGetLastError(), "build_img_kernel")) return false;
@@ -768,33 +845,10 @@ bool blocked_mixed_prepare(void * plan, int ns) {
     return cuda_fine(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
 }
 
-// Tasks (pair of fields, parity, band >= 1), longest first.
+// Split-BF16 tasks: MX_COLS columns per chain slot (two sph, four disk, eight tri fields per task).
 bool blocked_tasks_mixed(void * plan, int nf, int N, int M, BlkTaskList * out) {
-    BlockedPlan * B = static_cast<BlockedPlan *>(plan);
-    const int mlast = M / 2;
     (void) N;
-    std::vector<std::pair<long long, BlkTask>> v;
-    for (int f = 0; f < nf; f += 2)
-        for (int p = 0; p < 2; p++) {
-            const int m0 = p == 0 ? 2 : 3;
-            for (int band = 1; p + 2 * BLK * band <= mlast; band++) {
-                if (p + 2 * BLK * band < m0) continue;
-                if (band > B->nbeta) {
-                    set_error(FT_B200_EINVAL, "column band beyond the plan's blocks");
-                    return false;
-                }
-                long long cost = 0;
-                for (int beta = 0; beta < band; beta++) cost += B->kmax[p * B->nbeta + beta] + 2;
-                v.push_back({cost, BlkTask{f, p, band}});
-            }
-        }
-    std::stable_sort(v.begin(), v.end(), [](const auto & a, const auto & b) { return a.first > b.first; });
-    std::vector<BlkTask> t;
-    for (auto & x : v) t.push_back(x.second);
-    out->ntasks = (int) t.size();
-    if (t.empty()) return true;
-    if (!cuda_fine(cudaMalloc(&out->d_tasks, sizeof(BlkTask) * t.size()), "cudaMalloc(blocked tasks)")) return false;
-    return cuda_fine(cudaMemcpy(out->d_tasks, t.data(), sizeof(BlkTask) * t.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
+    return make_tasks(static_cast<BlockedPlan *>(plan), MX_COLS, nf, M, out);
 }
 
 cudaError_t launch_blocked_mixed(void * plan, int ns, bool hi2lo, float * T, int N, int M, const BlkTaskList & tl,
@@ -803,11 +857,12 @@ cudaError_t launch_blocked_mixed(void * plan, int ns, bool hi2lo, float * T, int
     if (tl.ntasks == 0) return cudaSuccess;
     static thread_local MixedLaunch L;
     L.T = T;
-    L.Lq = ((N + 1) / 2 + 3) / 4;
+    L.Lq = quads(B, N);
     L.img = B->d_img[ns - 3][hi2lo ? 0 : 1];
     L.qbase = B->d_qbase;
     L.kmax = B->d_kmax;
     L.nbeta = B->nbeta;
+    L.cq = B->nch - 1;
     L.tasks = reinterpret_cast<const BlkTask *>(tl.d_tasks);
     L.ntasks = tl.ntasks;
     L.counter = counter;
@@ -822,63 +877,57 @@ cudaError_t launch_blocked_mixed(void * plan, int ns, bool hi2lo, float * T, int
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(counter, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
-    int dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int ctas = std::min(sms, tl.ntasks);
-    kern<<<ctas, MX_THREADS, smem, st>>>(L);
+    kern<<<std::min(sm_count(), tl.ntasks), MX_THREADS, smem, st>>>(L);
     count_launch();
     return cudaGetLastError();
 }
 
-// Elements of the task-major copy used by the split-BF16 products.
-size_t blocked_mixed_T_elems(void * plan, int nf, int N) {
+// Elements of the task-major copy used by the split-BF16 products (ntasks from blocked_tasks_mixed).
+size_t blocked_mixed_T_elems(void * plan, int ntasks, int N) {
     BlockedPlan * B = static_cast<BlockedPlan *>(plan);
-    const long long npairs = (nf + 1) / 2;
-    const size_t Lq = (size_t) (((N + 1) / 2 + 3) / 4);
-    return (size_t) (npairs * 2 * std::max(1, B->nbeta)) * 2 * Lq * 4 * MX_COLS;
+    return (size_t) std::max(1, ntasks) * 2 * (size_t) quads(B, N) * 4 * MX_COLS;
 }
 
 // S (the fields' FP64 matrices) <-> T (task-major FP32 copy of the columns the
-// blocks apply to); one CTA per (task, 32 positions of both chains).
+// blocks apply to); one CTA per (task, 32 positions of both slots).
 struct TransLaunch {
     double * A[kMaxFields];
-    int nf, N, M, nbeta, Lq;
+    int nf, N, M, Lq;
+    Shape sh;
     float * T;
     const BlkTask * tasks;
 };
 
 template <bool TO_T>
 __global__ void __launch_bounds__(256) transpose_kernel(const __grid_constant__ TransLaunch L) {
-    __shared__ float tile[64][MX_COLS + 1];             // [row in the chunk][column]
+    // [row of the chunk][column]; chunk row rr holds position pl = 0 .. 31 of the chunk in
+    // slot c: rr = 2 pl + c (sph: the rows of the matrix in order) or 32 c + pl
+    __shared__ float tile[64][MX_COLS + 1];
     const BlkTask t = L.tasks[blockIdx.x];
     const int q = blockIdx.y;                           // positions 32q .. 32q + 31
     const int tid = threadIdx.x;
-    const int N = L.N, mlast = L.M / 2;
-    float * const Tt = L.T + task_index(t, L.nbeta) * (8LL * L.Lq * MX_COLS);
-    // element (chain c, position pos, column i) of the task's copy
+    const int N = L.N, mlast = Geo::last_order(L.sh.kind, L.M);
+    const bool two = L.sh.two_chains();
+    float * const Tt = L.T + t.slot * (8LL * L.Lq * MX_COLS);
+    // element (slot c, position pos, column i) of the task's copy
     auto at = [&](int c, int pos, int i) -> long long { return (((long long) c * L.Lq + (pos >> 2)) * MX_COLS + i) * 4 + (pos & 3); };
-    // column i of the task: field, matrix column, or -1
-    auto column = [&](int i, int & f) -> long long {
-        f = t.field + (i >> 6);
-        const int n = i & 63;
-        const int m = t.p + 2 * BLK * t.band + 2 * (n >> 1);
-        return (f < L.nf && m <= mlast) ? 2LL * m - 1 + (n & 1) : -1;
-    };
-    const int rr = tid & 63;                            // row of the chunk: 2 * (pos - 32q) + chain
-    const int row = 64 * q + rr;
+    auto chunk_row = [&](int c, int pl) -> int { return two ? 2 * pl + c : 32 * c + pl; };
+    const int rr = tid & 63;
+    const int c_r = two ? (rr & 1) : (rr >> 5), pl_r = two ? (rr >> 1) : (rr & 31);
+    const int row = L.sh.row(32 * q + pl_r, c_r);        // matrix row of chunk row rr
     if (TO_T) {
         for (int i = tid >> 6; i < MX_COLS; i += 4) {
             int f;
-            const long long col = column(i, f);
-            tile[rr][i] = (col >= 0 && row < N) ? (float) __ldcg(L.A[f] + col * N + row) : 0.0f;
+            const long long col = L.sh.column(t, MX_COLS, c_r, i, mlast, f);
+            tile[rr][i] = (col >= 0 && f < L.nf && row < N) ? (float) __ldcg(L.A[f] + col * N + row) : 0.0f;
         }
         __syncthreads();
         const int i = tid & (MX_COLS - 1);
         for (int e = tid >> 7; e < 16; e += 2) {       // e = 2 * (quad - 8q) + c
             const int c = e & 1, qd = e >> 1, Q = 8 * q + qd;
             if (Q < L.Lq) {
-                const float4 v = make_float4(tile[8 * qd + c][i], tile[8 * qd + 2 + c][i], tile[8 * qd + 4 + c][i], tile[8 * qd + 6 + c][i]);
+                const float4 v = make_float4(tile[chunk_row(c, 4 * qd)][i], tile[chunk_row(c, 4 * qd + 1)][i],
+                                             tile[chunk_row(c, 4 * qd + 2)][i], tile[chunk_row(c, 4 * qd + 3)][i]);
                 __stcg(reinterpret_cast<float4 *>(Tt + at(c, 4 * Q, i)), v);
             }
         }
@@ -887,13 +936,14 @@ __global__ void __launch_bounds__(256) transpose_kernel(const __grid_constant__ 
         for (int e = tid >> 7; e < 16; e += 2) {       // e = 2 * (quad - 8q) + c
             const int c = e & 1, qd = e >> 1, Q = 8 * q + qd;
             const float4 v = Q < L.Lq ? __ldcg(reinterpret_cast<const float4 *>(Tt + at(c, 4 * Q, i))) : make_float4(0.f, 0.f, 0.f, 0.f);
-            tile[8 * qd + c][i] = v.x; tile[8 * qd + 2 + c][i] = v.y; tile[8 * qd + 4 + c][i] = v.z; tile[8 * qd + 6 + c][i] = v.w;
+            tile[chunk_row(c, 4 * qd)][i] = v.x; tile[chunk_row(c, 4 * qd + 1)][i] = v.y;
+            tile[chunk_row(c, 4 * qd + 2)][i] = v.z; tile[chunk_row(c, 4 * qd + 3)][i] = v.w;
         }
         __syncthreads();
         for (int i2 = tid >> 6; i2 < MX_COLS; i2 += 4) {
             int f;
-            const long long col = column(i2, f);
-            if (col >= 0 && row < N) __stcg(L.A[f] + col * N + row, (double) tile[rr][i2]);
+            const long long col = L.sh.column(t, MX_COLS, c_r, i2, mlast, f);
+            if (col >= 0 && f < L.nf && row < N) __stcg(L.A[f] + col * N + row, (double) tile[rr][i2]);
         }
     }
 }
@@ -907,8 +957,8 @@ cudaError_t launch_blocked_transpose(void * plan, bool to_T, double * const * A,
     L.nf = nf;
     L.N = N;
     L.M = M;
-    L.nbeta = B->nbeta;
-    L.Lq = ((N + 1) / 2 + 3) / 4;
+    L.sh = B->sh;
+    L.Lq = quads(B, N);
     L.T = T;
     L.tasks = reinterpret_cast<const BlkTask *>(tl.d_tasks);
     const dim3 grid(tl.ntasks, (4 * L.Lq + 31) / 32);

@@ -176,7 +176,7 @@ HarmonicPlan * as_plan(const ft_harmonic_plan * P);
 // device task list already built for (RP, M), without building one (api.cu)
 bool find_tasks(ft_rotation_plan * RP, int M, const RotTask ** d_tasks, int * ntasks);
 
-// Blocked sweeps for fields sharing one sph plan (blocked.cu).
+// Blocked sweeps for fields sharing one plan (blocked.cu).
 struct BlkTaskList { void * d_tasks = nullptr; int ntasks = 0; };
 void * blocked_plan_build(HarmonicPlan * H);
 void blocked_plan_free(void * p);
@@ -189,7 +189,7 @@ bool blocked_mixed_prepare(void * plan, int ns);
 bool blocked_tasks_mixed(void * plan, int nf, int N, int M, BlkTaskList * out);
 cudaError_t launch_blocked_mixed(void * plan, int ns, bool hi2lo, float * T, int N, int M, const BlkTaskList & tl,
                                  int * counter, cudaStream_t st);
-size_t blocked_mixed_T_elems(void * plan, int nf, int N);
+size_t blocked_mixed_T_elems(void * plan, int ntasks, int N);   // ntasks of blocked_tasks_mixed
 cudaError_t launch_blocked_transpose(void * plan, bool to_T, double * const * A, int nf, int N, int M, float * T,
                                      const BlkTaskList & tl, cudaStream_t st);
 int blocked_device_error(void * plan);

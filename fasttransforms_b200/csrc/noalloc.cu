@@ -112,6 +112,10 @@ int run(HarmonicPlan * H, bool forward, char TRANS, double * A, int N, int M, cu
     if (TRANS != 'N' && TRANS != 'T') { set_error(FT_B200_EINVAL, "TRANS must be 'N' or 'T'"); return FT_B200_EINVAL; }
     if (!A) { set_error(FT_B200_EINVAL, "NULL matrix"); return FT_B200_EINVAL; }
     if (N != H->n || M < 1 || (H->kind == TRI && M != N)) { set_error(FT_B200_EINVAL, "N, M do not match the plan"); return FT_B200_EINVAL; }
+    if (H->kind != TRI && M >= 4 && M % 2 == 0) {   // order M/2 would reach column M
+        set_error(FT_B200_EINVAL, "sph and disk matrices need an odd number of columns M");
+        return FT_B200_EINVAL;
+    }
     if ((size_t) N * (size_t) M > (size_t) FT_B200_NOALLOC_MAX_ELEMS) {
         set_error(FT_B200_EINVAL, "N*M = " + std::to_string((long long) N * M) + " exceeds the allocation-free limit of " +
                                   std::to_string((long long) FT_B200_NOALLOC_MAX_ELEMS) + " elements");

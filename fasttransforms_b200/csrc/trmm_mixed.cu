@@ -1,4 +1,4 @@
-// The sph connection multiply (src/drivers.c:833-865: four column classes j = 0,1,2,3 mod 4,
+// The sph and disk connection multiply (src/drivers.c:833-865, 989-1021: four column classes j = 0,1,2,3 mod 4,
 // class j multiplied by U[0] for j = 0, 3 and U[1] for j = 1, 2, U upper triangular)
 // on the tcgen05 tensor cores, from fixed-point BF16 slices.
 //
@@ -392,7 +392,7 @@ int mixed_trmm_device_error(void * p) {
     return v;
 }
 
-// Out = op(U) In for the four column classes of every field (sph), U = P or Pinv of the
+// Out = op(U) In for the four column classes of every field (sph, disk), U = P or Pinv of the
 // plan, with nu slices of U (3 or 4) and 3 of the input.  Builds the plan's slice
 // images of op(U) on first use (into *plan_slot) and the batch's work buffers (*work_slot).
 cudaError_t launch_trmm_mixed(HarmonicPlan * H, void ** plan_slot, void ** work_slot, int nu, bool inverse, bool trans,

@@ -179,22 +179,24 @@ int ft_b200_execute_noalloc_dev(const ft_harmonic_plan * P, int forward, char TR
 
 /* Fields sharing one plan (same n, same M, same family), in one call.
  * precision FT_B200_FP64: the direct sweeps, as ft_b200_execute_batched_dev.
- * precision FT_B200_FP64_BLOCKED (sph only): blocks of 32 consecutive sweeps
+ * precision FT_B200_FP64_BLOCKED: blocks of 32 consecutive sweeps
  * are cut into tiles whose rotations are pre-multiplied (in FP64, once per
  * plan) into dense orthogonal 64 x 64 matrices, applied to every field's
  * columns as FP64 tensor-core (DMMA) products; a column's sweeps above its
  * last whole block stay direct.  Not bit-identical to the direct sweeps (the
  * products round differently); the relative 2-norm difference is of the order
  * of 1e-14.  The first call on a plan builds its tile matrices (device memory,
- * about 550 MB at n = 4096); make it before any stream capture.
- * precision FT_B200_MIXED_BF16 (sph only): the same blocks, each tile product
+ * about 550 MB for sph at n = 4096; disk and tri keep one chain of tiles per
+ * block, twice as long); make it before any stream capture.
+ * precision FT_B200_MIXED_BF16: the same blocks, each tile product
  * computed on the tcgen05 tensor cores from three 9-bit fixed-point BF16
  * slices per operand (eight slice products, exact FP32 accumulation per order
  * level); a value is carried between tiles at FP32 accuracy, in global memory
- * the matrices stay FP64.  The connection multiply runs on the tensor cores
- * too (four 8-bit slices of the matrix, three of the input, exact chunks of
- * 256 rows, FP32 running sums).  Relative 2-norm error against the FP64
- * transform about 5e-7 at n = 4096.
+ * the matrices stay FP64.  The connection multiply of sph and disk runs on
+ * the tensor cores too (four 8-bit slices of the matrix, three of the input,
+ * exact chunks of 256 rows, FP32 running sums); tri keeps its FP64 left and
+ * right multiplies and normalisation.  Relative 2-norm error against the FP64
+ * transform about 5e-7 at n = 4096 (sph).
  * precision FT_B200_MIXED_BF16X4: four slices in the blocks (ten products),
  * about 3.5e-7 at n = 4096.  The first call of either builds its slice images
  * of the tiles and of the connection matrices (about 1 GB at n = 4096). */

@@ -76,10 +76,10 @@ def test_mixed_large_and_round_trip(env, prec):
     P.close()
 
 
-def test_mixed_rejects_other_families(env):
+def test_shared_rejects_unknown_precision(env):
     ft, torch, O = env
     P = ft.plan_tri2cheb(16, 0.0, 0.0, 0.0)
     t = torch.zeros(16 * 16, dtype=torch.float64, device="cuda")
     with pytest.raises(ft.FTB200Error):
-        ft.execute_shared_dev(P, True, "N", [t.data_ptr()], ft.MIXED_BF16X4)
+        ft.execute_shared_dev(P, True, "N", [t.data_ptr()], 7)
     P.close()

@@ -61,12 +61,3 @@ def test_blocked_round_trip_large(env):
     for A, t in zip(As, ts):
         assert rel2(t.cpu().numpy().reshape(A.shape, order="F"), A) < 4 * np.sqrt(n) * EPS * 10
     P.close()
-
-
-def test_shared_rejects_blocked_for_other_families(env):
-    ft, torch, O = env
-    P = ft.plan_tri2cheb(64, 0.0, 0.0, 0.0)
-    t = torch.zeros(64 * 64, dtype=torch.float64, device="cuda")
-    with pytest.raises(ft.FTB200Error):
-        ft.execute_shared_dev(P, True, "N", [t.data_ptr()], ft.FP64_BLOCKED)
-    P.close()
