@@ -211,6 +211,22 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
+def profiled_traffic(workload, kernel):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of `kernel` on
+    `workload`, from the table of ncu figures kept in profiles/traffic.txt (None if absent)."""
+    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        f = line.split()
+        if len(f) >= 3 and not line.startswith("#") and f[0] == workload and f[1] == kernel:
+            try:
+                return float(f[2])
+            except ValueError:
+                return None
+    return None
+
+
 def max_over_ranks(x: float, dist, device: str) -> float:
     """The largest of every rank's x (each rank times its own replica; the job's time is the
     slowest rank's).  dist None: single process."""
@@ -400,13 +416,7 @@ def run_ours(args, rank, world, local_rank, dist):
     # the algorithmic rate at which the tensor pipe is saturated: BF16 peak over the eight
     # slice products and the 4/3 of a 64 x 64 tile product over its 32 x 32 rotations
     alg_peak = bf16 / (products * 4.0 / 3.0)
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        try:
-            traffic = json.load(open(tpath)).get(f"shared{nf}_n{n}", {}).get("blocked_mixed_kernel")
-        except Exception:
-            traffic = None
+    traffic = profiled_traffic(f"shared{nf}_n{n}", "blocked_mixed_kernel")
     roofline = {
         "bound": "tensor", "kernel": "blocked_mixed_kernel (tcgen05 split-BF16 tile products, 3 slices)",
         "achieved": achieved, "peak": alg_peak, "unit": "TFLOP/s", "frac": achieved / alg_peak, "traffic": traffic,
@@ -513,13 +523,7 @@ def plain_single(args, torch, ft):
     per_launch = (rot_ms / max(rot_n, 1)) if famname == "rotations" else (trmm_ms / max(trmm_n, 1))
     flops = rot_flops if famname == "rotations" else tr_flops
     achieved = flops / (per_launch * 1e-3) / 1e12
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        try:
-            traffic = json.load(open(tpath)).get(f"sph_n{n}", {}).get(famname)
-        except Exception:
-            traffic = None
+    traffic = profiled_traffic(f"sph_n{n}", famname)
     total = 2 * (rot_flops + tr_flops)
     return {
         "coeffs_per_s": n * n * steps / (ms * 1e-3), "ms_per_step": ms / steps,
@@ -641,7 +645,9 @@ def extra_workloads(args, torch, ft):
     out["shared_16_n4096"] = res
     del fields
     Pn.close()
-    # sibling families at degree 2047, 8 fields per transform
+    # sibling families at degree 2047, 8 fields per transform: the plain FP64 form (batched
+    # path) and the shared-plan forms, with the forward errors of the mixed forms against
+    # the FP64 transform of field 0
     for name, kind, params in (("tri_000", "tri", (0.0, 0.0, 0.0)), ("tri_hhh", "tri", (-0.5, -0.5, -0.5)),
                                ("disk_00", "disk", (0.0, 0.0))):
         n = 2048
@@ -650,6 +656,8 @@ def extra_workloads(args, torch, ft):
         M = p.M
         fields = [torch.from_numpy(ft.rand_layout(kind, n, SEED + f).ravel(order="F").copy()).cuda() for f in range(8)]
         fptr = [f.data_ptr() for f in fields]
+        field0 = fields[0].clone()
+        per_field = n * (n + 1) // 2 if kind == "tri" else 2 * n * n - n
 
         def step():
             ft.execute_batched_dev([p] * 8, True, "N", fptr, [n] * 8, [M] * 8, sp)
@@ -657,10 +665,31 @@ def extra_workloads(args, torch, ft):
         for _ in range(max(1, args.warmup)):
             step()
         ms = timed(step, max(3, args.steps // 4))
-        per_field = n * (n + 1) // 2 if kind == "tri" else 2 * n * n - n
-        out[name] = {"coeffs_per_s": 8 * per_field / (ms * 1e-3), "ms_per_step": ms,
-                     "workload": f"{kind}{params}, degree {n - 1}, 8 fields, fwd+bwd 'N'"}
-        del fields
+        res = {"coeffs_per_s": 8 * per_field / (ms * 1e-3), "ms_per_step": ms,
+               "workload": f"{kind}{params}, degree {n - 1}, 8 fields, fwd+bwd 'N'"}
+        ref_out = None
+        for pname, prec in (("fp64_shared", ft.FP64), ("fp64_blocked", ft.FP64_BLOCKED),
+                            ("mixed_bf16_3slices", ft.MIXED_BF16), ("mixed_bf16_4slices", ft.MIXED_BF16X4)):
+            x0 = field0.clone()
+            ft.execute_shared_dev(p, True, "N", [x0.data_ptr()], prec, sp)   # builds tables outside timing
+            torch.cuda.synchronize()
+            if ref_out is None:
+                ref_out = x0
+                e2 = einf = 0.0
+            else:
+                e2 = float(torch.linalg.norm(x0 - ref_out) / torch.linalg.norm(ref_out))
+                einf = float((x0 - ref_out).abs().max() / ref_out.abs().max())
+
+            def sstep(prec=prec):
+                ft.execute_shared_dev(p, True, "N", fptr, prec, sp)
+                ft.execute_shared_dev(p, False, "N", fptr, prec, sp)
+            sstep()
+            ms = timed(sstep, max(3, args.steps // 4))
+            res[pname] = {"coeffs_per_s": 8 * per_field / (ms * 1e-3), "ms_per_step": ms,
+                          "eps2_fwd_vs_fp64": e2, "epsinf_fwd_vs_fp64": einf}
+        res["mixed_bf16_over_fp64"] = res["mixed_bf16_3slices"]["coeffs_per_s"] / res["coeffs_per_s"]
+        out[name] = res
+        del fields, field0, ref_out
         p.close()
     return out
 
