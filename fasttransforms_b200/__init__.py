@@ -273,10 +273,12 @@ def execute_shared_dev(P: HarmonicPlan, forward: bool, trans: str, ptrs: Sequenc
     precision FP64: the direct sweeps; FP64_BLOCKED: whole blocks of 32 sweeps
     applied as pre-multiplied 64 x 64 tile matrices on the FP64 tensor pipe
     (rounds differently from the direct sweeps, ~1e-14 relative); MIXED_BF16:
-    the tile products on the BF16 tensor cores from fixed-point BF16 slices
-    (three per operand, ~5e-7 relative at n = 4096), and the connection
-    multiply of sph and disk likewise (tri keeps its FP64 multiplies);
-    MIXED_BF16X4: four slices in the blocks (~3.5e-7).  All three families.
+    the tile products and the connection multiply on the BF16 tensor cores
+    from fixed-point BF16 slices (three per operand in the blocks, ~5e-7
+    relative for sph at n = 4096); MIXED_BF16X4: four slices in the blocks and
+    of the multiply's input (~1.4e-7 for sph at n = 2048).  All three
+    families; the errors of tri and of generic disk parameters are larger (the
+    connection multiplies amplify the sweeps' error).
     """
     nf = len(ptrs)
     aa = (C.c_void_p * nf)(*ptrs)

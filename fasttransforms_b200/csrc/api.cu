@@ -640,14 +640,29 @@ int execute_batch_chunk(HarmonicPlan * const * H, bool forward, char TRANS, doub
         return cuda_ok(e, "rotation kernel");
     };
     auto trmm = [&](const TrmmSet & T, int mode, bool inverse, bool from_A) -> bool {
-        if (mixed && kind != TRI) {   // the left multiplies of sph and disk, mode 0 (U In) or 1 (U^T In)
+        if (mixed) {
             std::vector<double *> in(nf), out(nf);
             for (int f = 0; f < nf; f++) { in[f] = from_A ? A[f] : S[f]; out[f] = from_A ? S[f] : A[f]; }
-            prof_begin(FAM_TRMM, st);
             // four slices of the connection matrix for both block precisions: its K runs over all
-            // n rows, where three slices would cost about 2e-6 at n = 4096
-            const cudaError_t e = launch_trmm_mixed(H[0], &H[0]->mixed_trmm, &B->mx_trmm, 4, inverse, mode == 1,
-                                                    in.data(), out.data(), nf, M[0], st);
+            // n rows, where three slices would cost about 2e-6 at n = 4096.  Four slices of the
+            // input for MIXED_BF16X4 and for tri, whose multiplies cancel more: three leave
+            // about 3e-6 there (2e-7 for sph, 1e-6 for disk with generic parameters)
+            const int nx = (ns == 4 || kind == TRI) ? 4 : 3;
+            cudaError_t e;
+            prof_begin(FAM_TRMM, st);
+            if (kind != TRI) {          // the four column classes of sph and disk: mode 0 (U In) or 1 (U^T In)
+                e = launch_trmm_mixed(H[0], &H[0]->mixed_trmm, &B->mx_trmm, 4, nx, inverse, mode == 1, in.data(),
+                                      out.data(), nf, M[0], st);
+            } else if (mode < 2) {      // tri, left: U[0] In or U[0]^T In over all columns
+                e = launch_trmm_mixed(H[0], &H[0]->mixed_trmm, &B->mx_trmm, 4, nx, inverse, mode == 1, in.data(),
+                                      out.data(), nf, M[0], st, 1, 0);
+            } else {                    // tri, right: In op(U[1]) = (op(U[1])^T In^T)^T through two transposes
+                e = launch_transpose_square(in.data(), out.data(), nf, N[0], st);
+                if (e == cudaSuccess)
+                    e = launch_trmm_mixed(H[0], &H[0]->mixed_trmm, &B->mx_trmm, 4, nx, inverse, mode == 2, out.data(),
+                                          in.data(), nf, M[0], st, 1, 1);
+                if (e == cudaSuccess) e = launch_transpose_square(in.data(), out.data(), nf, N[0], st);
+            }
             prof_end(st);
             return cuda_ok(e, "tensor-core trmm");
         }

@@ -193,9 +193,14 @@ size_t blocked_mixed_T_elems(void * plan, int ntasks, int N);   // ntasks of blo
 cudaError_t launch_blocked_transpose(void * plan, bool to_T, double * const * A, int nf, int N, int M, float * T,
                                      const BlkTaskList & tl, cudaStream_t st);
 int blocked_device_error(void * plan);
-// connection multiply of the sph family on the tensor cores from BF16 slices (trmm_mixed.cu)
-cudaError_t launch_trmm_mixed(HarmonicPlan * H, void ** plan_slot, void ** work_slot, int nu, bool inverse, bool trans,
-                              double * const * in, double * const * out, int nf, int M, cudaStream_t st);
+// connection multiply on the tensor cores from BF16 slices (trmm_mixed.cu), with nu = 4
+// slices of U and nx = 3 (128-column tiles) or 4 (96-column tiles) of the input:
+// ncls = 4, the column classes of sph and disk; ncls = 1, every column with U[which] (tri)
+cudaError_t launch_trmm_mixed(HarmonicPlan * H, void ** plan_slot, void ** work_slot, int nu, int nx, bool inverse,
+                              bool trans, double * const * in, double * const * out, int nf, int M, cudaStream_t st,
+                              int ncls = 4, int which = 0);
+// out = in^T for square n x n matrices of nf fields
+cudaError_t launch_transpose_square(double * const * in, double * const * out, int nf, int n, cudaStream_t st);
 void mixed_trmm_plan_free(void * p);
 void mixed_trmm_work_free(void * p);
 int mixed_trmm_device_error(void * p);

@@ -15,13 +15,18 @@
 // 1 / sU_i and writes FP64.  Configurations: NU = 3 slices of U (levels <= 2,
 // six products) and NU = 4 (levels <= 3, nine products), both with NX = 3.
 //
-// Work: output tiles of 128 rows x 128 columns of one class of one field,
+// Work: output tiles of 128 rows x TBN columns of one class of one field,
 // longest K first, strided over persistent CTAs.  The operands come as
 // pre-sliced images in the tensor cores' K-major 128-byte swizzled layout:
 // U's once per plan, the input's by a slicing pass before each multiply.
 // Warp 8 issues the MMAs (one thread) and owns the TMEM allocation, warp 9
 // streams the K-tiles into a two-stage buffer with bulk copies, warps 0-7
-// fold the chunks (two warps per TMEM lane quarter, 64 columns each).
+// fold the chunks (two warps per TMEM lane quarter, TBN / 2 columns each).
+// Configurations (NU, NX, TBN): (4, 3, 128), nine products, and (4, 4, 96), ten
+// products, whose fourth input slice takes the input's slicing residual from
+// 2^-24 to 2^-32 of a chunk's largest entry (the residual is what the
+// cancellation in the multiply amplifies; four input slices at 128 columns
+// would not fit two stages into shared memory).
 #include <algorithm>
 #include <cstdio>
 #include <vector>
@@ -34,18 +39,21 @@
 namespace ftb {
 namespace {
 
-constexpr int TB = 128;                     // output tile rows and columns
+constexpr int TB = 128;                     // output tile rows (rows of op(U))
 constexpr int KT = 64;                      // K per tile of the images
 constexpr int CHUNK_KT = 4;                 // K-tiles per exact chunk (256 rows)
-constexpr int PIECE = TB * KT * 2;          // bytes of one slice of one K-tile (16 KB)
+constexpr int PIECE = TB * KT * 2;          // bytes of one slice of one K-tile of op(U) (16 KB)
 constexpr int THREADS = 320;
-constexpr uint32_t IDESC = tc::idesc_bf16(TB, TB);
 
-template <int NU, int NX> struct Cfg {
+// NU slices of op(U), NX of the input, TBN input columns per output tile
+template <int NU, int NX, int TBN> struct Cfg {
     static constexpr int NL = NU;                           // levels kept: 0 .. NU - 1
-    static constexpr int STAGE = (NU + NX) * PIECE;
+    static constexpr int XPIECE = TBN * KT * 2;             // bytes of one input slice of one K-tile
+    static constexpr int STAGE = NU * PIECE + NX * XPIECE;
     static constexpr size_t SMEM = 2 * (size_t) STAGE + 1024;
-    static_assert(NL * TB <= 512, "accumulators exceed tensor memory");
+    static constexpr uint32_t IDESC = tc::idesc_bf16(TB, TBN);
+    static_assert(TBN % 16 == 0 && TBN <= 128, "tile width");
+    static_assert(NL * TBN <= 512, "accumulators exceed tensor memory");
     static_assert(SMEM <= 227 * 1024, "shared memory");
 };
 
@@ -60,11 +68,14 @@ struct MixLaunch {
     const MixTile * tiles;
     int ntiles;
     int n, M, nkt, njt;                 // njt: column tiles per class (max over classes)
+    int ncls;                           // column classes: 4 (stride 4, sph and disk) or 1 (all columns)
     int * err;
 };
 
-__host__ __device__ __forceinline__ int class_cols(int M, int r) { return (M - r + 3) / 4; }
-__host__ __device__ __forceinline__ int class_matrix(int r) { return (r == 0 || r == 3) ? 0 : 1; }
+// Column classes: with four, class r holds the columns r + 4 j and takes U[0] for r = 0, 3 and
+// U[1] for r = 1, 2; with one, every column, and the single matrix the caller picked.
+__host__ __device__ __forceinline__ int class_cols(int M, int r, int ncls) { return (M - r + ncls - 1) / ncls; }
+__host__ __device__ __forceinline__ int class_matrix(int r, int ncls) { return (ncls == 4 && (r == 1 || r == 2)) ? 1 : 0; }
 
 // ---------------------------------------------------------------------------
 // slicing passes
@@ -142,30 +153,31 @@ __global__ void slice_matrix_kernel(const double * __restrict__ U, int n, bool t
 
 struct SliceXLaunch {
     const double * in[kMaxFields];
-    int n, M, nkt, njt;
+    int n, M, nkt, njt, ncls;
     unsigned char * img;
     float * inv;
 };
 
-// One CTA per (field, class, column tile, chunk), one warp per column at a time:
-// the chunk's 256 rows are read coalesced into shared memory, then each lane
-// slices 8 consecutive rows.
-template <int NS>
+// One CTA per (field, class, column tile of TBN, chunk), one warp per column at a
+// time: the chunk's 256 rows are read coalesced into shared memory, then each
+// lane slices 8 consecutive rows.
+template <int NS, int TBN>
 __global__ void __launch_bounds__(256) slice_input_kernel(const __grid_constant__ SliceXLaunch L) {
+    constexpr int XPIECE = TBN * KT * 2;
     __shared__ float buf[8][256];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nch = (L.nkt + CHUNK_KT - 1) / CHUNK_KT;
     int b = blockIdx.x;
     const int q = b % nch; b /= nch;
     const int jt = b % L.njt; b /= L.njt;
-    const int r = b % 4;
-    const int f = b / 4;
-    const int ncols = class_cols(L.M, r);
-    const long long tile_base = ((long long) (f * 4 + r) * L.njt + jt);
-    for (int ci = warp; ci < TB; ci += 8) {
-        const int j = jt * TB + ci;
+    const int r = b % L.ncls;
+    const int f = b / L.ncls;
+    const int ncols = class_cols(L.M, r, L.ncls);
+    const long long tile_base = ((long long) (f * L.ncls + r) * L.njt + jt);
+    for (int ci = warp; ci < TBN; ci += 8) {
+        const int j = jt * TBN + ci;
         const bool cok = j < ncols;
-        const double * col = L.in[f] + (long long) (r + 4LL * j) * L.n;
+        const double * col = L.in[f] + (long long) (r + (long long) L.ncls * j) * L.n;
         float amax = 0.0f;
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
@@ -186,22 +198,24 @@ __global__ void __launch_bounds__(256) slice_input_kernel(const __grid_constant_
         if (kt < L.nkt) {
             uint4 ch[NS];
             slice8<NS>(t, ch);
-            unsigned char * base = L.img + (tile_base * L.nkt + kt) * NS * PIECE;
+            unsigned char * base = L.img + (tile_base * L.nkt + kt) * NS * XPIECE;
             const uint32_t off = tc::sw128_offset(ci, 8 * (lane % 8));
 #pragma unroll
-            for (int a = 0; a < NS; ++a) *reinterpret_cast<uint4 *>(base + a * PIECE + off) = ch[a];
+            for (int a = 0; a < NS; ++a) *reinterpret_cast<uint4 *>(base + a * XPIECE + off) = ch[a];
         }
-        if (lane == 0) L.inv[(tile_base * nch + q) * TB + ci] = 1.0f / s;
+        if (lane == 0) L.inv[(tile_base * nch + q) * TBN + ci] = 1.0f / s;
     }
 }
 
 // ---------------------------------------------------------------------------
 // the multiply
 // ---------------------------------------------------------------------------
-template <int NU, int NX>
+template <int NU, int NX, int TBN>
 __global__ void __launch_bounds__(THREADS, 1) trmm_mixed_kernel(const __grid_constant__ MixLaunch L) {
-    using C = Cfg<NU, NX>;
+    using C = Cfg<NU, NX, TBN>;
     constexpr int NL = C::NL;
+    constexpr int XPIECE = C::XPIECE;
+    constexpr int HALF = TBN / 2;                     // columns per epilogue thread
     extern __shared__ unsigned char smem_raw[];
     unsigned char * const sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t) 1023);
     __shared__ __align__(8) uint64_t bar_full[2], bar_empty[2], bar_accf, bar_acce, bar_done;
@@ -232,14 +246,14 @@ __global__ void __launch_bounds__(THREADS, 1) trmm_mixed_kernel(const __grid_con
             unsigned q = 0;
             for (int t = blockIdx.x; t < L.ntiles && !s_abort; t += gridDim.x) {
                 const MixTile T = L.tiles[t];
-                const unsigned char * ua = L.Uimg[class_matrix(T.cls)] + (long long) T.it * L.nkt * NU * PIECE;
-                const unsigned char * xb = L.Ximg + (((long long) (T.field * 4 + T.cls) * L.njt + T.jt) * L.nkt) * NX * PIECE;
+                const unsigned char * ua = L.Uimg[class_matrix(T.cls, L.ncls)] + (long long) T.it * L.nkt * NU * PIECE;
+                const unsigned char * xb = L.Ximg + (((long long) (T.field * L.ncls + T.cls) * L.njt + T.jt) * L.nkt) * NX * XPIECE;
                 for (int kt = T.k0; kt <= T.k1; ++kt, ++q) {
                     const int st = q & 1, u = q >> 1;
                     if (!tc::mbar_wait(&bar_empty[st], (u & 1) ^ 1, &s_abort)) { fail(); break; }
                     tc::mbar_arrive_expect_tx(&bar_full[st], C::STAGE);
                     tc::bulk_g2s(sm + st * C::STAGE, ua + (long long) kt * NU * PIECE, NU * PIECE, &bar_full[st]);
-                    tc::bulk_g2s(sm + st * C::STAGE + NU * PIECE, xb + (long long) kt * NX * PIECE, NX * PIECE, &bar_full[st]);
+                    tc::bulk_g2s(sm + st * C::STAGE + NU * PIECE, xb + (long long) kt * NX * XPIECE, NX * XPIECE, &bar_full[st]);
                 }
             }
         }
@@ -271,8 +285,8 @@ __global__ void __launch_bounds__(THREADS, 1) trmm_mixed_kernel(const __grid_con
                                 const int a = lv - b;
                                 // level lv starts afresh with its first product of the chunk
                                 const bool fresh = cs && kk == 0 && b == bmin;
-                                tc::mma_bf16(tmem + lv * TB, tc::desc_sw128(ua + b * PIECE + kk * 32),
-                                             tc::desc_sw128(xb + a * PIECE + kk * 32), IDESC, !fresh);
+                                tc::mma_bf16(tmem + lv * TBN, tc::desc_sw128(ua + b * PIECE + kk * 32),
+                                             tc::desc_sw128(xb + a * XPIECE + kk * 32), C::IDESC, !fresh);
                             }
                         }
                     tc::commit(&bar_empty[st]);
@@ -282,29 +296,29 @@ __global__ void __launch_bounds__(THREADS, 1) trmm_mixed_kernel(const __grid_con
         }
         __syncwarp();
     } else {
-        // ---- epilogue: lane quarter q4, columns 64 h .. 64 h + 63 of the tile ----
+        // ---- epilogue: lane quarter q4, columns HALF h .. HALF h + HALF - 1 of the tile ----
         const int q4 = warp & 3, h = warp >> 2;
         const int row_in = 32 * q4 + lane;
-        const uint32_t tbase = tmem + ((uint32_t) (32 * q4) << 16) + 64 * h;
+        const uint32_t tbase = tmem + ((uint32_t) (32 * q4) << 16) + HALF * h;
         unsigned nacc = 0;
         for (int t = blockIdx.x; t < L.ntiles && !s_abort; t += gridDim.x) {
             const MixTile T = L.tiles[t];
-            float acc[64];
+            float acc[HALF];
 #pragma unroll
-            for (int j = 0; j < 64; ++j) acc[j] = 0.0f;
-            const float * xinv = L.Xinv + ((long long) (T.field * 4 + T.cls) * L.njt + T.jt) * nch * TB + 64 * h;
+            for (int j = 0; j < HALF; ++j) acc[j] = 0.0f;
+            const float * xinv = L.Xinv + ((long long) (T.field * L.ncls + T.cls) * L.njt + T.jt) * nch * TBN + HALF * h;
             for (int kt = T.k0; kt <= T.k1; ++kt) {
                 if (!chunk_end(kt, T.k1)) continue;
                 if (!tc::mbar_wait(&bar_accf, nacc & 1, &s_abort)) { fail(); break; }
                 nacc++;
                 __syncwarp();
                 tc::fence_after_sync();
-                const float * xi = xinv + (long long) (kt / CHUNK_KT) * TB;
+                const float * xi = xinv + (long long) (kt / CHUNK_KT) * TBN;
 #pragma unroll
-                for (int g = 0; g < 8; ++g) {
+                for (int g = 0; g < HALF / 8; ++g) {
                     uint32_t a[NL][8];
 #pragma unroll
-                    for (int lv = 0; lv < NL; ++lv) tc::tmem_ld8_async(tbase + lv * TB + 8 * g, a[lv]);
+                    for (int lv = 0; lv < NL; ++lv) tc::tmem_ld8_async(tbase + lv * TBN + 8 * g, a[lv]);
                     tc::tmem_wait_ld();
 #pragma unroll
                     for (int e = 0; e < 8; ++e) {
@@ -321,13 +335,13 @@ __global__ void __launch_bounds__(THREADS, 1) trmm_mixed_kernel(const __grid_con
             // out = acc 2^-14 / sU_i
             const int row = T.it * TB + row_in;
             if (row < L.n) {
-                const double sc = (double) __ldg(L.Uinv[class_matrix(T.cls)] + row);
+                const double sc = (double) __ldg(L.Uinv[class_matrix(T.cls, L.ncls)] + row);
                 double * const o = L.out[T.field];
-                const int ncols = class_cols(L.M, T.cls);
+                const int ncols = class_cols(L.M, T.cls, L.ncls);
 #pragma unroll
-                for (int j = 0; j < 64; ++j) {
-                    const int jj = T.jt * TB + 64 * h + j;
-                    if (jj < ncols) __stcg(o + (long long) (T.cls + 4LL * jj) * L.n + row, (double) acc[j] * sc);
+                for (int j = 0; j < HALF; ++j) {
+                    const int jj = T.jt * TBN + HALF * h + j;
+                    if (jj < ncols) __stcg(o + (long long) (T.cls + (long long) L.ncls * jj) * L.n + row, (double) acc[j] * sc);
                 }
             }
         }
@@ -357,14 +371,58 @@ struct MixedTrmmPlan {
     int * d_err = nullptr;
 };
 
+// Work buffers of one batch, per input configuration (0: three input slices, 128
+// columns per tile; 1: four slices, 96 columns), built on first use.
 struct MixedTrmmWork {
-    int nf = 0, n = 0, M = 0, nkt = 0, njt = 0, nch = 0;
-    unsigned char * ximg = nullptr;      // sliced input (NX = 4 size, either slice count fits)
-    float * xinv = nullptr;
-    MixTile * tiles[2] = {nullptr, nullptr};   // [trans], longest K first
-    int ntiles = 0;
+    int nf = 0, n = 0, M = 0, nkt = 0, nch = 0, ncls = 0;
+    struct Sub {
+        int njt = 0;
+        unsigned char * ximg = nullptr;          // sliced input
+        float * xinv = nullptr;
+        MixTile * tiles[2] = {nullptr, nullptr}; // [trans], longest K first
+        int ntiles = 0;
+    } sub[2];
 };
 
+// B = A^T for square n x n FP64 matrices of every field (32 x 32 tiles through shared memory).
+struct TransposeLaunch {
+    const double * in[kMaxFields];
+    double * out[kMaxFields];
+    int n;
+};
+
+__global__ void __launch_bounds__(256) transpose_square_kernel(const __grid_constant__ TransposeLaunch L) {
+    __shared__ double tile[32][33];
+    const int f = blockIdx.z;
+    const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;   // rows, columns of the input tile
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
+    const double * A = L.in[f];
+    double * B = L.out[f];
+    for (int y = ty; y < 32; y += 8) {
+        const int i = i0 + tx, j = j0 + y;                   // tile[y][tx] = A(i0 + tx, j0 + y)
+        tile[y][tx] = (i < L.n && j < L.n) ? __ldcg(A + (long long) j * L.n + i) : 0.0;
+    }
+    __syncthreads();
+    for (int y = ty; y < 32; y += 8) {
+        const int i = j0 + tx, j = i0 + y;                   // B(i, j) = A(j, i) = tile[tx][y]
+        if (i < L.n && j < L.n) __stcg(B + (long long) j * L.n + i, tile[tx][y]);
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_transpose_square(double * const * in, double * const * out, int nf, int n, cudaStream_t st) {
+    if (nf <= 0 || n <= 0) return cudaSuccess;
+    static thread_local TransposeLaunch L;
+    for (int f = 0; f < nf; ++f) { L.in[f] = in[f]; L.out[f] = out[f]; }
+    L.n = n;
+    const dim3 grid((n + 31) / 32, (n + 31) / 32, nf);
+    transpose_square_kernel<<<grid, 256, 0, st>>>(L);
+    count_launch();
+    return cudaGetLastError();
+}
+
+namespace {
 }  // namespace
 
 void mixed_trmm_plan_free(void * p) {
@@ -379,7 +437,7 @@ void mixed_trmm_plan_free(void * p) {
 void mixed_trmm_work_free(void * p) {
     MixedTrmmWork * W = static_cast<MixedTrmmWork *>(p);
     if (!W) return;
-    cudaFree(W->ximg); cudaFree(W->xinv); cudaFree(W->tiles[0]); cudaFree(W->tiles[1]);
+    for (auto & x : W->sub) { cudaFree(x.ximg); cudaFree(x.xinv); cudaFree(x.tiles[0]); cudaFree(x.tiles[1]); }
     delete W;
 }
 
@@ -392,13 +450,21 @@ int mixed_trmm_device_error(void * p) {
     return v;
 }
 
-// Out = op(U) In for the four column classes of every field (sph, disk), U = P or Pinv of the
-// plan, with nu slices of U (3 or 4) and 3 of the input.  Builds the plan's slice
-// images of op(U) on first use (into *plan_slot) and the batch's work buffers (*work_slot).
-cudaError_t launch_trmm_mixed(HarmonicPlan * H, void ** plan_slot, void ** work_slot, int nu, bool inverse, bool trans,
-                              double * const * in, double * const * out, int nf, int M, cudaStream_t st) {
+// Out = op(U) In for the column classes of every field, U = P or Pinv of the plan, with nu
+// slices of U (4) and nx (3 or 4) of the input.  ncls = 4: the four stride-4 classes of
+// sph and disk, U[0] on classes 0 and 3 and U[1] on 1 and 2; ncls = 1: every column,
+// U[which].  In and Out may be the same matrices: the input is sliced into the work
+// buffers before the multiply writes.  Builds the plan's slice images of op(U) on first
+// use (into *plan_slot) and the batch's work buffers (*work_slot).
+cudaError_t launch_trmm_mixed(HarmonicPlan * H, void ** plan_slot, void ** work_slot, int nu, int nx, bool inverse,
+                              bool trans, double * const * in, double * const * out, int nf, int M, cudaStream_t st,
+                              int ncls, int which) {
     const int n = H->n;
     const int nkt = (n + KT - 1) / KT, nit = (n + TB - 1) / TB;
+    if (ncls != 4 && ncls != 1) return cudaErrorInvalidValue;
+    if (nu != 4 || (nx != 3 && nx != 4)) return cudaErrorInvalidValue;   // the configurations built
+    const int cfg = nx == 4 ? 1 : 0;
+    const int tbn = cfg ? 96 : 128;
     if (!*plan_slot) *plan_slot = new MixedTrmmPlan();
     MixedTrmmPlan * T = static_cast<MixedTrmmPlan *>(*plan_slot);
     if (!T->d_err) {
@@ -408,15 +474,14 @@ cudaError_t launch_trmm_mixed(HarmonicPlan * H, void ** plan_slot, void ** work_
     }
     const int ui = nu - 3, ii = inverse ? 1 : 0, ti = trans ? 1 : 0;
     for (int u = 0; u < 2; ++u) {
-        if (T->img[ui][ii][ti][u]) continue;
+        if (T->img[ui][ii][ti][u] || (ncls == 1 && u != which)) continue;
         const size_t bytes = (size_t) nit * nkt * nu * PIECE;
         cudaError_t e = cudaMalloc(&T->img[ui][ii][ti][u], bytes);
         if (e == cudaSuccess) e = cudaMalloc(&T->inv[ui][ii][ti][u], sizeof(float) * (size_t) nit * TB);
         if (e != cudaSuccess) return e;
         const double * U = inverse ? H->dPinv[u] : H->dP[u];
         const int rows = nit * TB;
-        if (nu == 3) slice_matrix_kernel<3><<<(rows + 7) / 8, 256, 0, st>>>(U, n, trans, nkt, T->img[ui][ii][ti][u], T->inv[ui][ii][ti][u]);
-        else         slice_matrix_kernel<4><<<(rows + 7) / 8, 256, 0, st>>>(U, n, trans, nkt, T->img[ui][ii][ti][u], T->inv[ui][ii][ti][u]);
+        slice_matrix_kernel<4><<<(rows + 7) / 8, 256, 0, st>>>(U, n, trans, nkt, T->img[ui][ii][ti][u], T->inv[ui][ii][ti][u]);
         count_launch();
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
@@ -425,63 +490,71 @@ cudaError_t launch_trmm_mixed(HarmonicPlan * H, void ** plan_slot, void ** work_
     if (!W) {
         W = new MixedTrmmWork();
         *work_slot = W;
-        W->nf = nf; W->n = n; W->M = M; W->nkt = nkt;
-        W->njt = (class_cols(M, 0) + TB - 1) / TB;
+        W->nf = nf; W->n = n; W->M = M; W->nkt = nkt; W->ncls = ncls;
         W->nch = (nkt + CHUNK_KT - 1) / CHUNK_KT;
-        const size_t xbytes = (size_t) nf * 4 * W->njt * nkt * 4 * PIECE;
-        cudaError_t e = cudaMalloc(&W->ximg, xbytes);
-        if (e == cudaSuccess) e = cudaMalloc(&W->xinv, sizeof(float) * (size_t) nf * 4 * W->njt * W->nch * TB);
+    }
+    if (W->nf != nf || W->n != n || W->M != M || W->ncls != ncls) return cudaErrorInvalidValue;
+    MixedTrmmWork::Sub & X = W->sub[cfg];
+    if (!X.ximg) {
+        X.njt = (class_cols(M, 0, ncls) + tbn - 1) / tbn;
+        const size_t xbytes = (size_t) nf * ncls * X.njt * nkt * nx * tbn * KT * 2;
+        cudaError_t e = cudaMalloc(&X.ximg, xbytes);
+        if (e == cudaSuccess) e = cudaMalloc(&X.xinv, sizeof(float) * (size_t) nf * ncls * X.njt * W->nch * tbn);
         if (e != cudaSuccess) return e;
         for (int tr = 0; tr < 2; ++tr) {
             std::vector<std::pair<int, MixTile>> v;
             for (int f = 0; f < nf; ++f)
-                for (int r = 0; r < 4; ++r)
+                for (int r = 0; r < ncls; ++r)
                     for (int it = 0; it < nit; ++it)
-                        for (int jt = 0; jt * TB < class_cols(M, r); ++jt) {
+                        for (int jt = 0; jt * tbn < class_cols(M, r, ncls); ++jt) {
                             const int k0 = tr ? 0 : 2 * it, k1 = tr ? std::min(nkt - 1, 2 * it + 1) : nkt - 1;
                             v.push_back({k1 - k0 + 1, MixTile{f, r, it, jt, k0, k1}});
                         }
             std::stable_sort(v.begin(), v.end(), [](const auto & a, const auto & b) { return a.first > b.first; });
             std::vector<MixTile> tl;
             for (auto & x : v) tl.push_back(x.second);
-            W->ntiles = (int) tl.size();
-            e = cudaMalloc(&W->tiles[tr], sizeof(MixTile) * std::max<size_t>(1, tl.size()));
-            if (e == cudaSuccess && !tl.empty()) e = cudaMemcpy(W->tiles[tr], tl.data(), sizeof(MixTile) * tl.size(), cudaMemcpyHostToDevice);
+            X.ntiles = (int) tl.size();
+            e = cudaMalloc(&X.tiles[tr], sizeof(MixTile) * std::max<size_t>(1, tl.size()));
+            if (e == cudaSuccess && !tl.empty()) e = cudaMemcpy(X.tiles[tr], tl.data(), sizeof(MixTile) * tl.size(), cudaMemcpyHostToDevice);
             if (e != cudaSuccess) return e;
         }
     }
-    if (W->nf != nf || W->n != n || W->M != M) return cudaErrorInvalidValue;
     // slice the input
     static thread_local SliceXLaunch SX;
     for (int f = 0; f < nf; ++f) SX.in[f] = in[f];
-    SX.n = n; SX.M = M; SX.nkt = nkt; SX.njt = W->njt;
-    SX.img = W->ximg; SX.inv = W->xinv;
-    const int sgrid = nf * 4 * W->njt * W->nch;
-    slice_input_kernel<3><<<sgrid, 256, 0, st>>>(SX);
+    SX.n = n; SX.M = M; SX.nkt = nkt; SX.njt = X.njt; SX.ncls = ncls;
+    SX.img = X.ximg; SX.inv = X.xinv;
+    const int sgrid = nf * ncls * X.njt * W->nch;
+    if (cfg) slice_input_kernel<4, 96><<<sgrid, 256, 0, st>>>(SX);
+    else     slice_input_kernel<3, 128><<<sgrid, 256, 0, st>>>(SX);
     count_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     // multiply
     static thread_local MixLaunch L;
     for (int f = 0; f < nf; ++f) L.out[f] = out[f];
-    for (int u = 0; u < 2; ++u) { L.Uimg[u] = T->img[ui][ii][ti][u]; L.Uinv[u] = T->inv[ui][ii][ti][u]; }
-    L.Ximg = W->ximg; L.Xinv = W->xinv;
-    L.tiles = W->tiles[ti]; L.ntiles = W->ntiles;
-    L.n = n; L.M = M; L.nkt = nkt; L.njt = W->njt;
+    for (int u = 0; u < 2; ++u) {
+        const int us = ncls == 1 ? which : u;   // one class: the chosen matrix in slot 0
+        L.Uimg[u] = T->img[ui][ii][ti][us];
+        L.Uinv[u] = T->inv[ui][ii][ti][us];
+    }
+    L.Ximg = X.ximg; L.Xinv = X.xinv;
+    L.tiles = X.tiles[ti]; L.ntiles = X.ntiles;
+    L.n = n; L.M = M; L.nkt = nkt; L.njt = X.njt; L.ncls = ncls;
     L.err = T->d_err;
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int ctas = std::min(sms, W->ntiles);
+    const int ctas = std::min(sms, X.ntiles);
     if (ctas <= 0) return cudaSuccess;
-    if (nu == 3) {
-        auto kern = trmm_mixed_kernel<3, 3>;
-        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) Cfg<3, 3>::SMEM);
-        if (e == cudaSuccess) { kern<<<ctas, THREADS, Cfg<3, 3>::SMEM, st>>>(L); e = cudaGetLastError(); }
+    if (cfg) {
+        auto kern = trmm_mixed_kernel<4, 4, 96>;
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) Cfg<4, 4, 96>::SMEM);
+        if (e == cudaSuccess) { kern<<<ctas, THREADS, Cfg<4, 4, 96>::SMEM, st>>>(L); e = cudaGetLastError(); }
     } else {
-        auto kern = trmm_mixed_kernel<4, 3>;
-        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) Cfg<4, 3>::SMEM);
-        if (e == cudaSuccess) { kern<<<ctas, THREADS, Cfg<4, 3>::SMEM, st>>>(L); e = cudaGetLastError(); }
+        auto kern = trmm_mixed_kernel<4, 3, 128>;
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) Cfg<4, 3, 128>::SMEM);
+        if (e == cudaSuccess) { kern<<<ctas, THREADS, Cfg<4, 3, 128>::SMEM, st>>>(L); e = cudaGetLastError(); }
     }
     count_launch();
     return e;

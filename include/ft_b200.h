@@ -192,13 +192,17 @@ int ft_b200_execute_noalloc_dev(const ft_harmonic_plan * P, int forward, char TR
  * computed on the tcgen05 tensor cores from three 9-bit fixed-point BF16
  * slices per operand (eight slice products, exact FP32 accumulation per order
  * level); a value is carried between tiles at FP32 accuracy, in global memory
- * the matrices stay FP64.  The connection multiply of sph and disk runs on
- * the tensor cores too (four 8-bit slices of the matrix, three of the input,
- * exact chunks of 256 rows, FP32 running sums); tri keeps its FP64 left and
- * right multiplies and normalisation.  Relative 2-norm error against the FP64
- * transform about 5e-7 at n = 4096 (sph).
- * precision FT_B200_MIXED_BF16X4: four slices in the blocks (ten products),
- * about 3.5e-7 at n = 4096.  The first call of either builds its slice images
+ * the matrices stay FP64.  The connection multiply runs on the tensor cores
+ * too (four 8-bit slices of the matrix, three of the input, four for tri;
+ * exact chunks of 256 rows, FP32 running sums; tri's right multiply through
+ * two transposes, its normalisation in FP64).  Relative 2-norm error against
+ * the FP64 transform about 5e-7 for sph at n = 4096; the connection
+ * multiplies amplify the sweeps' error by a factor that depends on the family
+ * and its parameters (up to about 3e-5 for tri with generic parameters at
+ * n = 2048).
+ * precision FT_B200_MIXED_BF16X4: four slices in the blocks (ten products)
+ * and four of the input in the connection multiply: about 1.4e-7 for sph at
+ * n = 2048 (up to about 9e-6 for tri with generic parameters).  The first call of either builds its slice images
  * of the tiles and of the connection matrices (about 1 GB at n = 4096). */
 #define FT_B200_FP64 0
 #define FT_B200_FP64_BLOCKED 1
