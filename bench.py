@@ -606,8 +606,9 @@ def extra_workloads(args, torch, ft):
     ms = timed(g.replay, max(3, args.steps // 2))
     coeffs = sum(n * n for n in degs)
     # same fields one plan call after another, eager, for comparison
-    ms_loop = timed(lambda: [ft.execute_dev(p, fw, "N", d.data_ptr(), p.n, p.M, sp)
-                             for fw in (True, False) for p, d in zip(P, data)], max(3, args.steps // 4))
+    loop = lambda: [ft.execute_dev(p, fw, "N", d.data_ptr(), p.n, p.M, sp) for fw in (True, False) for p, d in zip(P, data)]
+    loop()   # first calls per degree build task lists and tune launch shapes
+    ms_loop = timed(loop, max(3, args.steps // 4))
     out["batched_uneven_64"] = {"coeffs_per_s": coeffs / (ms * 1e-3), "ms_per_step": ms,
                                 "per_field_loop_coeffs_per_s": coeffs / (ms_loop * 1e-3),
                                 "degrees": "64 fields, U{127,255,511,1023,2047} seed 20261203",

@@ -29,7 +29,7 @@ __all__ = [
     "plan_rotsphere", "plan_rottriangle", "plan_rotdisk",
     "execute_sph_hi2lo", "execute_sph_lo2hi", "execute_tri_hi2lo", "execute_tri_lo2hi",
     "execute_disk_hi2lo", "execute_disk_lo2hi",
-    "execute_dev", "execute_shared_dev", "FP64", "FP64_BLOCKED", "MIXED_BF16", "MIXED_BF16X4", "device_status", "execute_noalloc_dev", "NOALLOC_MAX_ELEMS", "execute_batched_dev", "rotations_dev", "kernel_launches", "profile", "profile_read",
+    "execute_dev", "execute_shared_dev", "FP64", "FP64_BLOCKED", "MIXED_BF16", "MIXED_BF16X4", "device_status", "execute_noalloc_dev", "NOALLOC_MAX_ELEMS", "execute_batched_dev", "rotations_dev", "kernel_launches", "profile", "profile_read", "set_rotation_config",
     "layout_cols", "rand_layout", "sphrand", "trirand", "diskrand",
     "SPH", "TRI", "DISK",
 ]
@@ -70,6 +70,7 @@ def _load() -> C.CDLL:
         "ft_b200_execute_shared_dev": (i, [vp, i, ch, C.POINTER(vp), i, i, vp]),
         "ft_b200_device_status": (i, [vp]),
         "ft_b200_profile": (i, [i]), "ft_b200_profile_read": (i, [i, C.POINTER(C.c_double), C.POINTER(i)]),
+        "ft_b200_set_rotation_config": (None, [i]),
     }
     for name in ("sph2fourier", "fourier2sph", "tri2cheb", "cheb2tri", "disk2cxf", "cxf2disk", "sphv2fourier", "fourier2sphv"):
         sig["ft_execute_" + name] = (None, [ch, vp, dp, i, i])
@@ -90,6 +91,11 @@ def _check():
     st = lib.ft_b200_last_status()
     if st != 0:
         raise FTB200Error(st, lib.ft_b200_last_error().decode())
+
+
+def set_rotation_config(cfg: int) -> None:
+    """Force the rotation kernel's launch shape (0 .. 3) or let the autotuner choose (-1)."""
+    lib.ft_b200_set_rotation_config(int(cfg))
 
 
 def profile(enable: bool) -> None:

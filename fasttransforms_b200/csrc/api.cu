@@ -173,8 +173,10 @@ bool rotations(ft_rotation_plan * RP, bool hi2lo, const double * in, double * ou
     L.tasks = d_tasks;
     L.ntasks = ntasks;
     L.counter = RP->d_counter;
+    // out of place, the destination holds nothing live yet: the autotuner may time there
+    double * const dead[1] = {out};
     prof_begin(FAM_ROT, st);
-    const cudaError_t e = launch_rotations(RP->kind, hi2lo, L, 0, st);
+    const cudaError_t e = launch_rotations(RP->kind, hi2lo, L, 0, st, in != out ? dead : nullptr);
     prof_end(st);
     return cuda_ok(e, "rotation kernel");
 }
@@ -634,8 +636,11 @@ int execute_batch_chunk(HarmonicPlan * const * H, bool forward, char TRANS, doub
         L.tasks = B->d_tasks;
         L.ntasks = B->ntasks;
         L.counter = B->d_counter;
+        // out of place, the destinations hold nothing live yet: the autotuner may time there
+        std::vector<double *> dead(nf);
+        for (int f = 0; f < nf; f++) dead[f] = to_A ? A[f] : S[f];
         prof_begin(FAM_ROT, st);
-        const cudaError_t e = launch_rotations(kind, hi2lo, L, 0, st);
+        const cudaError_t e = launch_rotations(kind, hi2lo, L, 0, st, from_A != to_A ? dead.data() : nullptr);
         prof_end(st);
         return cuda_ok(e, "rotation kernel");
     };
@@ -765,6 +770,8 @@ extern "C" {
 int ft_b200_last_status(void) { return t_status; }
 const char * ft_b200_last_error(void) { return t_message.c_str(); }
 unsigned long long ft_b200_kernel_launches(void) { return g_launches.load(); }
+
+void ft_b200_set_rotation_config(int cfg) { set_rotation_config(cfg); }
 
 int ft_b200_profile(int enable) {
     std::lock_guard<std::mutex> lk(g_prof_mu);

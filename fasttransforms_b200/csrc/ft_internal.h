@@ -95,7 +95,12 @@ struct RotLaunch {
     int ntasks;
     int * counter;             // device work counter (reset by the launcher)
 };
-cudaError_t launch_rotations(int kind, bool hi2lo, const RotLaunch & L, int max_ctas, cudaStream_t st);
+// dead: per field, memory the caller has no live data in (N x M at the field's leading
+// dimension), or null.  With it, the first launch of a shape times every configuration
+// there and keeps the fastest for the shape (the autotuner; FT_B200_AUTOTUNE=0 turns it off).
+cudaError_t launch_rotations(int kind, bool hi2lo, const RotLaunch & L, int max_ctas, cudaStream_t st,
+                             double * const * dead = nullptr);
+void set_rotation_config(int cfg);   // 0 .. 3 forces a configuration, -1 chooses per shape
 int rotation_ctas_per_sm(int kind);
 
 // Triangular multiplies (trmm.cu).  Out = op(U) * In on column classes.

@@ -36,6 +36,10 @@
 #include <cstdlib>
 #include <type_traits>
 
+#include <map>
+#include <mutex>
+#include <string>
+
 #include "ft_internal.h"
 
 namespace ftb {
@@ -410,7 +414,8 @@ cudaError_t launch_kind(int cfg, const RotLaunch & L, int max_ctas, cudaStream_t
 
 int g_rot_cfg = -2;
 
-// FT_B200_ROT_CFG = 0..3 forces a configuration; otherwise -1 (choose per launch)
+// FT_B200_ROT_CFG = 0..3 forces a configuration (as does ft_b200_set_rotation_config);
+// otherwise -1 (chosen per launch shape)
 int rotation_config() {
     if (g_rot_cfg == -2) {
         const char * e = std::getenv("FT_B200_ROT_CFG");
@@ -419,18 +424,107 @@ int rotation_config() {
     return g_rot_cfg;
 }
 
-cudaError_t launch_rotations(int kind, bool hi2lo, const RotLaunch & L, int max_ctas, cudaStream_t st) {
-    if (L.ntasks <= 0) return cudaSuccess;
-    // Launches that run only the heads above whole blocks (blk > 0: fewer than blk sweeps
-    // per column, 2 blk - 2 per task at most) keep more stages busy with 4 sweeps per warp.
-    int cfg = rotation_config();
-    if (cfg < 0) cfg = (L.nfields > 0 && L.fields[0].blk > 0) ? 3 : 0;
+void set_rotation_config(int cfg) { g_rot_cfg = (cfg >= 0 && cfg <= 3) ? cfg : -1; }
+
+namespace {
+
+cudaError_t launch_with(int kind, bool hi2lo, int cfg, const RotLaunch & L, int max_ctas, cudaStream_t st) {
     switch (kind) {
         case SPH:  return hi2lo ? launch_kind<SPH, true>(cfg, L, max_ctas, st) : launch_kind<SPH, false>(cfg, L, max_ctas, st);
         case TRI:  return hi2lo ? launch_kind<TRI, true>(cfg, L, max_ctas, st) : launch_kind<TRI, false>(cfg, L, max_ctas, st);
         case DISK: return hi2lo ? launch_kind<DISK, true>(cfg, L, max_ctas, st) : launch_kind<DISK, false>(cfg, L, max_ctas, st);
     }
     return cudaErrorInvalidValue;
+}
+
+// Configuration without measurements: launches that run only the heads above whole
+// blocks (blk > 0: fewer than blk sweeps per column, 2 blk - 2 per task at most) keep more
+// stages busy with 4 sweeps per warp; full sweeps use 8 per warp.
+int default_config(const RotLaunch & L) { return (L.nfields > 0 && L.fields[0].blk > 0) ? 3 : 0; }
+
+// The autotuner's choices, by launch shape: family, direction, heads only or all sweeps,
+// fields, tasks, and the first field's N and M (the tasks of a shape are the same).
+std::mutex g_tune_mu;
+std::map<std::string, int> g_tuned;
+
+std::string shape_key(int kind, bool hi2lo, const RotLaunch & L) {
+    char k[160];
+    std::snprintf(k, sizeof k, "%d/%d/%d/%d/%d/%d/%d", kind, hi2lo ? 1 : 0, L.fields[0].blk > 0 ? 1 : 0, L.nfields,
+                  L.ntasks, L.fields[0].N, L.fields[0].M);
+    return k;
+}
+
+bool autotune_enabled() {
+    static const bool on = [] {
+        const char * e = std::getenv("FT_B200_AUTOTUNE");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+// Times every configuration once (after one untimed launch) with CUDA events on the
+// launch stream, on a copy of L whose fields read and write only dead[f] (memory whose
+// contents the caller no longer needs, at least the field's N x M at its leading
+// dimension); returns the fastest, or -1 if a launch or an event failed.  The rotation
+// kernel's cost does not depend on the values, and every configuration computes the same
+// results bit for bit (each element meets its rotations in the same order).
+int tune(int kind, bool hi2lo, const RotLaunch & L, double * const * dead, int max_ctas, cudaStream_t st) {
+    static thread_local RotLaunch S;
+    S = L;
+    for (int f = 0; f < L.nfields; ++f) { S.fields[f].in = dead[f]; S.fields[f].out = dead[f]; }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        if (e0) cudaEventDestroy(e0);
+        return -1;
+    }
+    int best = -1;
+    float best_ms = 0.0f;
+    const int ncfg = 4;
+    for (int cfg = 0; cfg < ncfg; ++cfg) {
+        if (kind == TRI && cfg == 1) continue;   // not built for tri (falls back to 0)
+        if (launch_with(kind, hi2lo, cfg, S, max_ctas, st) != cudaSuccess) { best = -1; break; }
+        if (cudaEventRecord(e0, st) != cudaSuccess) { best = -1; break; }
+        if (launch_with(kind, hi2lo, cfg, S, max_ctas, st) != cudaSuccess) { best = -1; break; }
+        float ms = 0.0f;
+        if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+            cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) { best = -1; break; }
+        if (best < 0 || ms < best_ms) { best = cfg; best_ms = ms; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return best;
+}
+
+}  // namespace
+
+cudaError_t launch_rotations(int kind, bool hi2lo, const RotLaunch & L, int max_ctas, cudaStream_t st,
+                             double * const * dead) {
+    if (L.ntasks <= 0) return cudaSuccess;
+    int cfg = rotation_config();
+    if (cfg < 0) {
+        cfg = default_config(L);
+        if (autotune_enabled() && L.nfields > 0) {
+            const std::string key = shape_key(kind, hi2lo, L);
+            int known = -1;
+            {
+                std::lock_guard<std::mutex> lk(g_tune_mu);
+                auto it = g_tuned.find(key);
+                if (it != g_tuned.end()) known = it->second;
+            }
+            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+            if (known >= 0) {
+                cfg = known;
+            } else if (dead && cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) {
+                const int t = tune(kind, hi2lo, L, dead, max_ctas, st);
+                if (t >= 0) {
+                    std::lock_guard<std::mutex> lk(g_tune_mu);
+                    g_tuned[key] = t;
+                    cfg = t;
+                }
+            }
+        }
+    }
+    return launch_with(kind, hi2lo, cfg, L, max_ctas, st);
 }
 
 int rotation_ctas_per_sm(int) { return 1; }
