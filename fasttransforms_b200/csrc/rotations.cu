@@ -86,7 +86,7 @@ __device__ __forceinline__ void rot_lo2hi(double & x, double & y, double s, doub
 // tri: column m).  The NCOL columns of a lane share every (sin, cos) pair, so
 // one shared-memory load feeds NCOL rotations.
 template <int KIND, bool HI2LO, int W, int B, int E>
-__global__ void __launch_bounds__(W * 32, 1)
+__global__ void __launch_bounds__(W * 32, W <= 4 ? 2 : 1)
 rot_kernel(const __grid_constant__ RotLaunch L) {
     using T = KT<KIND>;
     constexpr int CH = T::CH, STEP = T::STEP, NCOL = T::NCOL, ORD = T::ORD, COLS = T::COLS, CPAD = T::CPAD;
@@ -377,7 +377,9 @@ cudaError_t launch_cfg(const RotLaunch & L, int max_ctas, cudaStream_t st) {
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int ctas = sms;
+    int per_sm = 1;   // resident CTAs per SM (two for the four-warp shapes)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, W * 32, shm) != cudaSuccess || per_sm < 1) per_sm = 1;
+    int ctas = sms * per_sm;
     if (max_ctas > 0 && ctas > max_ctas) ctas = max_ctas;
     if (ctas > L.ntasks) ctas = L.ntasks;
     if (ctas <= 0) return cudaSuccess;
@@ -402,6 +404,8 @@ cudaError_t launch_cfg(const RotLaunch & L, int max_ctas, cudaStream_t st) {
 //   1: W = 16, B = 4, E = 8  (128 registers, four warps per sub-partition)
 //   2: W = 8,  B = 4, E = 8  (fewer sweeps per warp: lighter register pressure)
 //   3: W = 8,  B = 4, E = 16
+//   4: W = 4,  B = 4, E = 16 (two CTAs per SM)
+//   5: W = 4,  B = 8, E = 16 (two CTAs per SM where shared memory allows: tri, disk)
 template <int KIND, bool HI2LO>
 cudaError_t launch_kind(int cfg, const RotLaunch & L, int max_ctas, cudaStream_t st) {
     if constexpr (KIND != TRI) {
@@ -409,22 +413,24 @@ cudaError_t launch_kind(int cfg, const RotLaunch & L, int max_ctas, cudaStream_t
     }
     if (cfg == 2) return launch_cfg<KIND, HI2LO, 8, 4, 8>(L, max_ctas, st);
     if (cfg == 3) return launch_cfg<KIND, HI2LO, 8, 4, 16>(L, max_ctas, st);
+    if (cfg == 4) return launch_cfg<KIND, HI2LO, 4, 4, 16>(L, max_ctas, st);
+    if (cfg == 5) return launch_cfg<KIND, HI2LO, 4, 8, 16>(L, max_ctas, st);
     return launch_cfg<KIND, HI2LO, 8, 8, 16>(L, max_ctas, st);
 }
 
 int g_rot_cfg = -2;
 
-// FT_B200_ROT_CFG = 0..3 forces a configuration (as does ft_b200_set_rotation_config);
+// FT_B200_ROT_CFG = 0..5 forces a configuration (as does ft_b200_set_rotation_config);
 // otherwise -1 (chosen per launch shape)
 int rotation_config() {
     if (g_rot_cfg == -2) {
         const char * e = std::getenv("FT_B200_ROT_CFG");
-        g_rot_cfg = (e && e[0] >= '0' && e[0] <= '3') ? e[0] - '0' : -1;
+        g_rot_cfg = (e && e[0] >= '0' && e[0] <= '5') ? e[0] - '0' : -1;
     }
     return g_rot_cfg;
 }
 
-void set_rotation_config(int cfg) { g_rot_cfg = (cfg >= 0 && cfg <= 3) ? cfg : -1; }
+void set_rotation_config(int cfg) { g_rot_cfg = (cfg >= 0 && cfg <= 5) ? cfg : -1; }
 
 namespace {
 
@@ -479,7 +485,7 @@ int tune(int kind, bool hi2lo, const RotLaunch & L, double * const * dead, int m
     }
     int best = -1;
     float best_ms = 0.0f;
-    const int ncfg = 4;
+    const int ncfg = 6;
     for (int cfg = 0; cfg < ncfg; ++cfg) {
         if (kind == TRI && cfg == 1) continue;   // not built for tri (falls back to 0)
         if (launch_with(kind, hi2lo, cfg, S, max_ctas, st) != cudaSuccess) { best = -1; break; }

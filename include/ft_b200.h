@@ -234,9 +234,10 @@ int ft_b200_profile(int enable);
 int ft_b200_profile_read(int family, double * ms, int * launches);
 
 /* Launch shape of the rotation kernel (no counterpart in the reference, whose
- * kernels have no launch shape).  cfg = 0 .. 3 forces one of the built shapes
- * (warps x sweeps per warp x chunk: 8 x 8 x 16, 16 x 4 x 8, 8 x 4 x 8, 8 x 4 x 16;
- * tri has no 16 x 4 x 8 and runs 8 x 8 x 16 for it); cfg = -1 (the default, or
+ * kernels have no launch shape).  cfg = 0 .. 5 forces one of the built shapes
+ * (warps x sweeps per warp x chunk: 8 x 8 x 16, 16 x 4 x 8, 8 x 4 x 8, 8 x 4 x 16,
+ * 4 x 4 x 16 and 4 x 8 x 16, the last two with as many CTAs per SM as fit; tri has
+ * no 16 x 4 x 8 and runs 8 x 8 x 16 for it); cfg = -1 (the default, or
  * FT_B200_ROT_CFG unset) lets the autotuner choose: the first out-of-place
  * launch of each shape (family, direction, all sweeps or heads only, fields,
  * tasks, N, M) times every configuration once on its destination, whose

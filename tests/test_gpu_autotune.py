@@ -42,7 +42,7 @@ def test_every_shape_bit_identical(env, kind, n, params):
     try:
         ft.set_rotation_config(-1)
         ref = {(fwd, tr): transform(ft, torch, P, A, fwd, tr) for fwd in (True, False) for tr in "NT"}
-        for cfg in range(4):
+        for cfg in range(6):
             ft.set_rotation_config(cfg)
             for (fwd, tr), r in ref.items():
                 assert np.array_equal(transform(ft, torch, P, A, fwd, tr), r), (kind, cfg, fwd, tr)
@@ -65,6 +65,6 @@ def test_first_launch_of_a_shape_is_tuned(env):
     second = transform(ft, torch, P, A, True, "N")
     c2 = ft.kernel_launches()
     assert np.array_equal(first, second)
-    # four shapes for sph, one untimed and one timed launch each
-    assert (c1 - c0) - (c2 - c1) == 8, (c1 - c0, c2 - c1)
+    # six shapes for sph, one untimed and one timed launch each
+    assert (c1 - c0) - (c2 - c1) == 12, (c1 - c0, c2 - c1)
     P.close()
