@@ -568,6 +568,11 @@ def extra_workloads(args, torch, ft):
     """Secondary workloads (reported beside the headline, same device timing rules)."""
     import numpy as np
     out = {"plain_fp64_n%d" % args.n: plain_single(args, torch, ft)}
+    if args.n != 1024:   # the plain path's other degree, 1023 (its 16.8 MB matrix stays in L2)
+        a2 = argparse.Namespace(**vars(args))
+        a2.n = 1024
+        out["plain_fp64_n1024"] = plain_single(a2, torch, ft)
+        out["plain_fp64_n1024"]["note"] = "matrix (16.8 MB) resident in L2 between steps"
     st = torch.cuda.current_stream()
     sp = st.cuda_stream
 

@@ -94,7 +94,8 @@ def _check():
 
 
 def set_rotation_config(cfg: int) -> None:
-    """Force the rotation kernel's launch shape (0 .. 5) or let the autotuner choose (-1)."""
+    """Force the rotation kernel's launch shape (0 .. 5; + 8 through the pass pipeline) or
+    let the autotuner choose (-1)."""
     lib.ft_b200_set_rotation_config(int(cfg))
 
 

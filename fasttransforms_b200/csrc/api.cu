@@ -121,6 +121,7 @@ ft_rotation_plan * make_rotation_plan(int kind, int n, double alpha, double beta
     RP->c = static_cast<double *>(std::calloc(len, sizeof(double)));
     RP->mu = new std::mutex();
     RP->tasks = new std::map<int, std::pair<RotTask *, int>>();
+    RP->sched = new std::map<int, RotSchedule *>();
     if (!RP->s || !RP->c) { set_error(FT_B200_ENOMEM, "host allocation"); ft_destroy_rotation_plan(RP); return nullptr; }
     rotation_tables(kind, n, alpha, beta, gamma, RP->s, RP->c);
     std::vector<double2> sc(len);
@@ -149,6 +150,7 @@ bool get_tasks(ft_rotation_plan * RP, int M, RotTask ** d_tasks, int * ntasks) {
         if (!cuda_ok(cudaMemcpy(d, t.data(), sizeof(RotTask) * t.size(), cudaMemcpyHostToDevice), "cudaMemcpy(tasks)")) return false;
     }
     (*RP->tasks)[M] = {d, (int) t.size()};
+    (*RP->sched)[M] = rot_schedule_new(t);
     *d_tasks = d; *ntasks = (int) t.size();
     return true;
 }
@@ -176,7 +178,13 @@ bool rotations(ft_rotation_plan * RP, bool hi2lo, const double * in, double * ou
     // out of place, the destination holds nothing live yet: the autotuner may time there
     double * const dead[1] = {out};
     prof_begin(FAM_ROT, st);
-    const cudaError_t e = launch_rotations(RP->kind, hi2lo, L, 0, st, in != out ? dead : nullptr);
+    RotSchedule * sched = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(*RP->mu);
+        auto it = RP->sched->find(M);
+        if (it != RP->sched->end()) sched = it->second;
+    }
+    const cudaError_t e = launch_rotations(RP->kind, hi2lo, L, 0, st, in != out ? dead : nullptr, sched);
     prof_end(st);
     return cuda_ok(e, "rotation kernel");
 }
@@ -484,6 +492,7 @@ struct BatchCtx {
     bool mx_ready = false;
     float * d_T = nullptr;                         // their task-major copy of the columns
     void * mx_trmm = nullptr;                      // sliced inputs and tile lists of the tensor-core multiply
+    RotSchedule * sched = nullptr;                 // pass pipeline of the rotation tasks
 };
 std::mutex g_batch_mu;
 std::map<std::string, BatchCtx *> g_batches;
@@ -543,6 +552,7 @@ void release_batches(HarmonicPlan * H) {
         BatchCtx * B = it->second;
         for (void * p : B->allocs) cudaFree(p);
         mixed_trmm_work_free(B->mx_trmm);
+        rot_schedule_free(B->sched);
         delete B;
         it = g_batches.erase(it);
     }
@@ -589,6 +599,7 @@ BatchCtx * get_batch(HarmonicPlan * const * H, const int * N, const int * M, int
         return nullptr;
     }
     B->ntasks = (int) tasks.size();
+    B->sched = rot_schedule_new(tasks);
     g_batches[key] = B;
     return B;
 }
@@ -640,7 +651,7 @@ int execute_batch_chunk(HarmonicPlan * const * H, bool forward, char TRANS, doub
         std::vector<double *> dead(nf);
         for (int f = 0; f < nf; f++) dead[f] = to_A ? A[f] : S[f];
         prof_begin(FAM_ROT, st);
-        const cudaError_t e = launch_rotations(kind, hi2lo, L, 0, st, from_A != to_A ? dead.data() : nullptr);
+        const cudaError_t e = launch_rotations(kind, hi2lo, L, 0, st, from_A != to_A ? dead.data() : nullptr, B->sched);
         prof_end(st);
         return cuda_ok(e, "rotation kernel");
     };
@@ -850,6 +861,10 @@ void ft_destroy_rotation_plan(ft_rotation_plan * RP) {
         for (auto & kv : *RP->tasks) if (kv.second.first) cudaFree(kv.second.first);
         delete RP->tasks;
     }
+    if (RP->sched) {
+        for (auto & kv : *RP->sched) rot_schedule_free(kv.second);
+        delete RP->sched;
+    }
     delete RP->mu;
     if (RP->d_sc) cudaFree(RP->d_sc);
     if (RP->d_counter) cudaFree(RP->d_counter);
@@ -927,7 +942,8 @@ int ft_b200_device_status(const ft_harmonic_plan * P) {
     if (!H) { set_error(FT_B200_EINVAL, "not a plan created by this library"); return -1; }
     const int a = H->blocked ? blocked_device_error(H->blocked) : 0;
     const int b = H->mixed_trmm ? mixed_trmm_device_error(H->mixed_trmm) : 0;
-    return a ? a : b;
+    const int c = rotation_device_error();   // the rotation kernel's pass-pipeline waits (library-wide)
+    return a ? a : (b ? b : c);
 }
 
 int ft_b200_plan_kind(const ft_harmonic_plan * P) {

@@ -63,6 +63,30 @@ struct Geo {
     // orders per rotation task: one lane per (order, chain) of a 32-lane warp
     __host__ __device__ static inline int task_orders(int kind) { return kind == SPH ? 16 : 32; }
     __host__ __device__ static inline int last_order(int kind, int M) { return kind == TRI ? M - 1 : M / 2; }
+    // Sweeps of the rotation task of lowest order mbase: every sweep j = jlo, jlo + step, ..,
+    // jhi applies to at least one of its columns (order m runs j = jpar .. m - step; with
+    // blk > 0 only its sweeps above its last whole block of blk sweeps).  Returns their number
+    // (0: nothing to do).  The kernel and the host's pass schedule both use this.
+    __host__ __device__ static inline int task_sweeps(int kind, int M, int mbase, int blk, int * jlo_out, int * jhi_out) {
+        const int st = step(kind), ord = task_orders(kind), mlast = last_order(kind, M);
+        int omax = mbase + st * (ord - 1);
+        if (omax > mlast) omax = mbase + st * ((mlast - mbase) / st);
+        const int jpar = kind == TRI ? 0 : (mbase & 1);
+        int jlo = jpar;
+        if (blk > 0) {
+            jlo = mbase - st * (((mbase - jpar) / st) % blk);
+            for (int o = 1; o < ord; ++o) {
+                const int m = mbase + st * o;
+                if (m > mlast) break;
+                const int c = m - st * (((m - jpar) / st) % blk);
+                if (c < jlo) jlo = c;
+            }
+        }
+        const int jhi = omax - st;
+        *jlo_out = jlo;
+        *jhi_out = jhi;
+        return jhi < jlo ? 0 : (jhi - jlo) / st + 1;
+    }
 };
 
 // A unit of work of the rotation kernel: the columns of task_orders(kind)
@@ -94,12 +118,27 @@ struct RotLaunch {
     const RotTask * tasks;     // device, longest first
     int ntasks;
     int * counter;             // device work counter (reset by the launcher)
+    // Pass pipeline (null units: each CTA runs every pass of a task itself).  Unit u is pass
+    // units[u].pass of task units[u].task; it streams down the columns behind its
+    // predecessor unit units[u].prev (pass - 1 of the same task, pulled earlier from the
+    // queue), whose progress word it waits on; prog[u] is its own (cleared by the launcher).
+    const struct RotUnit * units;
+    int nunits;
+    int * prog;
 };
+struct RotUnit { int task, pass, prev; };
+// Host side of the pass pipeline of one task list: the host copy of the device list (same
+// order) and the unit lists built from it per pass length and head mode (rotations.cu).
+struct RotSchedule;
+RotSchedule * rot_schedule_new(const std::vector<RotTask> & tasks);
+void rot_schedule_free(RotSchedule * s);
+int rotation_device_error();   // reads and clears the rotation kernel's status word (-1: read failed)
 // dead: per field, memory the caller has no live data in (N x M at the field's leading
 // dimension), or null.  With it, the first launch of a shape times every configuration
 // there and keeps the fastest for the shape (the autotuner; FT_B200_AUTOTUNE=0 turns it off).
+// sched: the task list's schedule (null: no pass pipeline).
 cudaError_t launch_rotations(int kind, bool hi2lo, const RotLaunch & L, int max_ctas, cudaStream_t st,
-                             double * const * dead = nullptr);
+                             double * const * dead = nullptr, RotSchedule * sched = nullptr);
 void set_rotation_config(int cfg);   // 0 .. 3 forces a configuration, -1 chooses per shape
 int rotation_ctas_per_sm(int kind);
 
@@ -235,4 +274,5 @@ struct ft_rotation_plan_s {
     int * d_counter;           // work counter for the persistent kernel
     std::mutex * mu;
     std::map<int, std::pair<ftb::RotTask *, int>> * tasks;   // M -> device task list (longest first)
+    std::map<int, ftb::RotSchedule *> * sched;               // M -> pass schedule of that list
 };

@@ -81,6 +81,32 @@ __device__ __forceinline__ void rot_lo2hi(double & x, double & y, double s, doub
     x = xn; y = yn;
 }
 
+// Status word of the rotation kernel: nonzero once a wait of the pass pipeline ran out
+// (its output is then not valid).  Read and cleared by rotation_device_error().
+__device__ int g_rot_status;
+
+// Progress word of a pipeline unit: hi2lo, -X where every position >= X of its columns is
+// final for the pass; lo2hi, X where every position <= X is final.  The launcher clears the
+// words to a value below any position; a finished unit publishes INT_MAX.
+__device__ __forceinline__ void publish_progress(int * p, int v) {
+    __threadfence();
+    asm volatile("st.release.gpu.global.s32 [%0], %1;\n" :: "l"(p), "r"(v) : "memory");
+}
+// Waits until *p >= need; gives up after about 2^32 SM cycles, setting the status word, and
+// at once when the word is already set (so one failed wait costs a launch about that long,
+// not that long per unit).
+__device__ __forceinline__ void wait_progress(const int * p, int need) {
+    const long long t0 = clock64();
+    for (;;) {
+        int v;
+        asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+        if (v >= need) return;
+        if (*(volatile int *) &g_rot_status != 0) return;
+        if (clock64() - t0 > (1LL << 32)) { atomicExch(&g_rot_status, 3); return; }
+        __nanosleep(128);
+    }
+}
+
 // Lane layout: lane = o * CH + c owns chain c of the NCOL columns of order
 // mbase + STEP * o (sph: cos and sin columns 2m-1, 2m; disk: the same pair;
 // tri: column m).  The NCOL columns of a lane share every (sin, cos) pair, so
@@ -109,38 +135,36 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
     const int q = warp;                       // stage index
     const int o_lane = lane / CH, c_lane = lane % CH;
 
+    const bool pipe = L.units != nullptr;
     for (;;) {
         if (threadIdx.x == 0) s_task = atomicAdd(L.counter, 1);
         __syncthreads();
         const int tid = s_task;
         __syncthreads();
-        if (tid >= L.ntasks) break;
-        const RotTask task = L.tasks[tid];
+        if (tid >= (pipe ? L.nunits : L.ntasks)) break;
+        // one pass of a task (pipeline) or all of its passes
+        const RotUnit unit = pipe ? L.units[tid] : RotUnit{tid, -1, -1};
+        const RotTask task = L.tasks[unit.task];
         const RotField & F = L.fields[task.field];
         const int N = F.N;
         const long long lda = F.lda;
         const int mlast = Geo::last_order(KIND, F.M);
         const int mbase = task.mbase;
-        int omax = mbase + STEP * (ORD - 1);
-        if (omax > mlast) omax = mbase + STEP * ((mlast - mbase) / STEP);
         const int jpar = KIND == TRI ? 0 : (mbase & 1);   // lowest sweep of every column
         // With F.blk > 0 a column of order m runs only its sweeps j >= jcut(m): the
         // (m - jpar)/STEP mod blk sweeps above its last whole block of blk sweeps.
         auto jcut = [&](int m) -> int {
             return F.blk > 0 ? m - STEP * (((m - jpar) / STEP) % F.blk) : jpar;
         };
-        int jlo = jpar;
-        if (F.blk > 0) {
-            jlo = jcut(mbase);
-            for (int o = 1; o < ORD; ++o) {
-                const int m = mbase + STEP * o;
-                if (m <= mlast) jlo = min(jlo, jcut(m));
-            }
-        }
-        const int jhi = omax - STEP;
-        if (jhi < jlo) continue;   // nothing to do for this task (uniform)
-        const int nsw = (jhi - jlo) / STEP + 1;
+        int jlo, jhi;
+        const int nsw = Geo::task_sweeps(KIND, F.M, mbase, F.blk, &jlo, &jhi);
+        if (nsw == 0) continue;   // nothing to do for this task (uniform)
         const int npass = (nsw + WB - 1) / WB;
+        const int rbeg = pipe ? unit.pass : 0, rend = pipe ? unit.pass + 1 : npass;
+        if (rend > npass) {       // a schedule that does not match this launch shape
+            if (threadIdx.x == 0) atomicExch(&g_rot_status, 4);
+            continue;
+        }
         const int m_lane = mbase + STEP * o_lane;
         const int jcut_lane = jcut(m_lane);
         int jlo_all_max = jpar;   // highest first sweep over the task's columns
@@ -151,7 +175,7 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
             }
         const int L0 = Geo::chain_len(KIND, N, 0);
 
-        for (int r = 0; r < npass; ++r) {
+        for (int r = rbeg; r < rend; ++r) {
             const double * src = r == 0 ? F.in : F.out;
             double * dst = F.out;
             const bool copy_all = r == 0 && F.in != F.out;
@@ -174,6 +198,9 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
             const int tstart = HI2LO ? ref - emax : -1;
             const int tend = HI2LO ? ref + 2 * WAB : emax + 2 * WAB - 1;
             const int K = (tend - tstart + 1 + E - 1) / E;
+            // pass pipeline: the predecessor's progress word and this unit's own
+            const int * const prev_prog = (pipe && unit.prev >= 0) ? L.prog + unit.prev : nullptr;
+            int * const my_prog = pipe ? L.prog + tid : nullptr;
 
             // ---- stage state: per column a window of 2B chain positions ----
             double win[NCOL][2 * B];
@@ -280,6 +307,13 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
                 const int row = CH * pmin + rro[v];
                 return colok[v] && p >= 0 && p <= emax && row < N;
             };
+            // (thread 0) wait until the predecessor has finished the positions chunk k loads
+            auto wait_chunk = [&](int k) {
+                if (!prev_prog || k >= K) return;
+                const int pmin = pmin_of(k, false), pmax = pmin + E - 1;
+                if (pmax < 0 || pmin > emax) return;                 // nothing of the chunk is loaded
+                wait_progress(prev_prog, HI2LO ? -max(pmin, 0) : min(pmax, emax));
+            };
             auto load_chunk = [&](int k) {
                 const int pmin = pmin_of(k, false);
 #pragma unroll
@@ -297,7 +331,18 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
 #pragma unroll
                 for (int v = 0; v < PER_W; ++v)
                     if (row_ok(pmin, v)) __stcg(gdst[v] + (long long) CH * pmin, bw[soff[v]]);
+                if (pipe) __threadfence();   // before the barrier after which they are published
             };
+            if (pipe) {
+                if (threadIdx.x == 0) {
+                    wait_chunk(0);
+                    wait_chunk(1);
+                    // hi2lo: positions above this pass's range are final once the predecessor
+                    // has finished the first chunk's (they belong to earlier passes only)
+                    publish_progress(my_prog, HI2LO ? -(emax + 1) : -1);
+                }
+                __syncthreads();
+            }
             load_chunk(0);
             stash_chunk(0);
             if (q == 0) prefetch_sc(0);
@@ -361,8 +406,15 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
                 }
                 if (it + 1 < K) stash_chunk(it + 1);
                 cp_async_wait_all();
+                if (pipe && threadIdx.x == 0) wait_chunk(it + 2);   // loaded next iteration
                 __syncthreads();
+                // the chunk stored this iteration is final: publish it
+                if (pipe && threadIdx.x == 0 && it - WA >= 0 && it - WA < K) {
+                    const int pmin = pmin_of(it - WA, true);
+                    publish_progress(my_prog, HI2LO ? -pmin : pmin + E - 1);
+                }
             }
+            if (pipe && threadIdx.x == 0) publish_progress(my_prog, 0x7fffffff);
         }
     }
 }
@@ -381,7 +433,8 @@ cudaError_t launch_cfg(const RotLaunch & L, int max_ctas, cudaStream_t st) {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, W * 32, shm) != cudaSuccess || per_sm < 1) per_sm = 1;
     int ctas = sms * per_sm;
     if (max_ctas > 0 && ctas > max_ctas) ctas = max_ctas;
-    if (ctas > L.ntasks) ctas = L.ntasks;
+    const int work = L.units ? L.nunits : L.ntasks;   // queue entries: pass units or tasks
+    if (ctas > work) ctas = work;
     if (ctas <= 0) return cudaSuccess;
     e = cudaMemsetAsync(L.counter, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
@@ -420,19 +473,106 @@ cudaError_t launch_kind(int cfg, const RotLaunch & L, int max_ctas, cudaStream_t
 
 int g_rot_cfg = -2;
 
-// FT_B200_ROT_CFG = 0..5 forces a configuration (as does ft_b200_set_rotation_config);
-// otherwise -1 (chosen per launch shape)
+// A configuration is a launch shape 0 .. 5, plus 8 to run through the pass pipeline.
+// FT_B200_ROT_CFG forces one (as does ft_b200_set_rotation_config); otherwise -1 (chosen
+// per launch shape).
+bool valid_config(int cfg) { return cfg >= 0 && (cfg & 7) <= 5 && cfg < 16; }
+
 int rotation_config() {
     if (g_rot_cfg == -2) {
         const char * e = std::getenv("FT_B200_ROT_CFG");
-        g_rot_cfg = (e && e[0] >= '0' && e[0] <= '5') ? e[0] - '0' : -1;
+        const int v = e ? std::atoi(e) : -1;
+        g_rot_cfg = (e && e[0] >= '0' && e[0] <= '9' && valid_config(v)) ? v : -1;
     }
     return g_rot_cfg;
 }
 
-void set_rotation_config(int cfg) { g_rot_cfg = (cfg >= 0 && cfg <= 5) ? cfg : -1; }
+void set_rotation_config(int cfg) { g_rot_cfg = valid_config(cfg) ? cfg : -1; }
+
+struct RotSchedule {
+    std::vector<RotTask> tasks;                          // host copy of the device list (same order)
+    struct Units { RotUnit * d_units = nullptr; int * d_prog = nullptr; int n = 0; };
+    std::map<std::pair<int, int>, Units> lists;          // (sweeps per pass, heads only) -> units
+    std::mutex mu;
+};
+
+RotSchedule * rot_schedule_new(const std::vector<RotTask> & tasks) {
+    RotSchedule * s = new RotSchedule();
+    s->tasks = tasks;
+    return s;
+}
+
+void rot_schedule_free(RotSchedule * s) {
+    if (!s) return;
+    for (auto & kv : s->lists) { cudaFree(kv.second.d_units); cudaFree(kv.second.d_prog); }
+    delete s;
+}
+
+int rotation_device_error() {
+    int v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_rot_status, sizeof(int)) != cudaSuccess) return -1;
+    if (v) {
+        const int z = 0;
+        if (cudaMemcpyToSymbol(g_rot_status, &z, sizeof(int)) != cudaSuccess) return -1;
+    }
+    return v;
+}
 
 namespace {
+
+// Sweeps per pass (W x B) of each launch shape.
+int shape_pass(int cfg) {
+    static const int wb[6] = {64, 64, 32, 32, 16, 32};
+    return (cfg >= 0 && cfg < 6) ? wb[cfg] : 64;
+}
+
+// The units of L's tasks for passes of wb sweeps, in queue order (a unit's predecessor is
+// always pulled first).  Built on first use; null when the stream is capturing then (the
+// upload synchronises) or on an allocation failure.
+const RotSchedule::Units * schedule_units(RotSchedule * S, int kind, const RotLaunch & L, int wb, cudaStream_t st) {
+    const int blk = L.fields[0].blk;
+    std::lock_guard<std::mutex> lk(S->mu);
+    const auto key = std::make_pair(wb, blk > 0 ? blk : 0);
+    auto it = S->lists.find(key);
+    if (it != S->lists.end()) return it->second.d_units ? &it->second : nullptr;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return nullptr;
+    const int nt = (int) S->tasks.size();
+    std::vector<int> npass(nt, 0);
+    int maxp = 0;
+    for (int t = 0; t < nt; ++t) {
+        const RotTask & T = S->tasks[t];
+        const RotField & F = L.fields[T.field];
+        int jlo, jhi;
+        const int nsw = Geo::task_sweeps(kind, F.M, T.mbase, F.blk, &jlo, &jhi);
+        npass[t] = (nsw + wb - 1) / wb;
+        maxp = std::max(maxp, npass[t]);
+    }
+    // pass-major (every task's pass r before any task's pass r + 1, so a unit's predecessor
+    // is always pulled first), tasks in list order (longest first) within a pass.  (Ordering
+    // by passes left in the task, which keeps a task's passes closer together, measured the
+    // same or slightly slower.)
+    std::vector<RotUnit> u;
+    std::vector<int> last(nt, -1);   // unit index of each task's latest pass so far
+    for (int r = 0; r < maxp; ++r)
+        for (int t = 0; t < nt; ++t)
+            if (r < npass[t]) {
+                u.push_back(RotUnit{t, r, last[t]});
+                last[t] = (int) u.size() - 1;
+            }
+    RotSchedule::Units U;
+    U.n = (int) u.size();
+    if (U.n > 0) {
+        if (cudaMalloc(&U.d_units, sizeof(RotUnit) * u.size()) != cudaSuccess ||
+            cudaMalloc(&U.d_prog, sizeof(int) * u.size()) != cudaSuccess ||
+            cudaMemcpy(U.d_units, u.data(), sizeof(RotUnit) * u.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+            cudaFree(U.d_units); cudaFree(U.d_prog);
+            U = RotSchedule::Units{};
+        }
+    }
+    S->lists[key] = U;
+    return U.d_units ? &S->lists[key] : nullptr;
+}
 
 cudaError_t launch_with(int kind, bool hi2lo, int cfg, const RotLaunch & L, int max_ctas, cudaStream_t st) {
     switch (kind) {
@@ -441,6 +581,23 @@ cudaError_t launch_with(int kind, bool hi2lo, int cfg, const RotLaunch & L, int 
         case DISK: return hi2lo ? launch_kind<DISK, true>(cfg, L, max_ctas, st) : launch_kind<DISK, false>(cfg, L, max_ctas, st);
     }
     return cudaErrorInvalidValue;
+}
+
+// One launch in configuration cfg: shape cfg & 7, through the pass pipeline when cfg & 8
+// and the task list has a schedule (else each CTA runs every pass of its tasks).
+cudaError_t launch_shape(int kind, bool hi2lo, int cfg, const RotLaunch & L, int max_ctas, cudaStream_t st,
+                         RotSchedule * sched) {
+    const int shape = cfg & 7;
+    const RotSchedule::Units * U = ((cfg & 8) && sched) ? schedule_units(sched, kind, L, shape_pass(shape), st) : nullptr;
+    if (!U) return launch_with(kind, hi2lo, shape, L, max_ctas, st);
+    static thread_local RotLaunch P;
+    P = L;
+    P.units = U->d_units;
+    P.nunits = U->n;
+    P.prog = U->d_prog;
+    const cudaError_t e = cudaMemsetAsync(U->d_prog, 0x80, sizeof(int) * U->n, st);   // below any position
+    if (e != cudaSuccess) return e;
+    return launch_with(kind, hi2lo, shape, P, max_ctas, st);
 }
 
 // Configuration without measurements: launches that run only the heads above whole
@@ -474,7 +631,8 @@ bool autotune_enabled() {
 // dimension); returns the fastest, or -1 if a launch or an event failed.  The rotation
 // kernel's cost does not depend on the values, and every configuration computes the same
 // results bit for bit (each element meets its rotations in the same order).
-int tune(int kind, bool hi2lo, const RotLaunch & L, double * const * dead, int max_ctas, cudaStream_t st) {
+int tune(int kind, bool hi2lo, const RotLaunch & L, double * const * dead, int max_ctas, cudaStream_t st,
+         RotSchedule * sched) {
     static thread_local RotLaunch S;
     S = L;
     for (int f = 0; f < L.nfields; ++f) { S.fields[f].in = dead[f]; S.fields[f].out = dead[f]; }
@@ -485,12 +643,15 @@ int tune(int kind, bool hi2lo, const RotLaunch & L, double * const * dead, int m
     }
     int best = -1;
     float best_ms = 0.0f;
-    const int ncfg = 6;
-    for (int cfg = 0; cfg < ncfg; ++cfg) {
-        if (kind == TRI && cfg == 1) continue;   // not built for tri (falls back to 0)
-        if (launch_with(kind, hi2lo, cfg, S, max_ctas, st) != cudaSuccess) { best = -1; break; }
+    // every shape, each also through the pass pipeline when the list has a schedule (it
+    // spreads a task's passes over SMs: worth it when there are few tasks, not when the
+    // columns would leave L2 between passes)
+    for (int cfg = 0; cfg < 14; ++cfg) {
+        if ((cfg & 7) > 5 || (kind == TRI && (cfg & 7) == 1)) continue;   // tri: shape 1 not built
+        if ((cfg & 8) && !sched) continue;
+        if (launch_shape(kind, hi2lo, cfg, S, max_ctas, st, sched) != cudaSuccess) { best = -1; break; }
         if (cudaEventRecord(e0, st) != cudaSuccess) { best = -1; break; }
-        if (launch_with(kind, hi2lo, cfg, S, max_ctas, st) != cudaSuccess) { best = -1; break; }
+        if (launch_shape(kind, hi2lo, cfg, S, max_ctas, st, sched) != cudaSuccess) { best = -1; break; }
         float ms = 0.0f;
         if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
             cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) { best = -1; break; }
@@ -504,7 +665,7 @@ int tune(int kind, bool hi2lo, const RotLaunch & L, double * const * dead, int m
 }  // namespace
 
 cudaError_t launch_rotations(int kind, bool hi2lo, const RotLaunch & L, int max_ctas, cudaStream_t st,
-                             double * const * dead) {
+                             double * const * dead, RotSchedule * sched) {
     if (L.ntasks <= 0) return cudaSuccess;
     int cfg = rotation_config();
     if (cfg < 0) {
@@ -521,7 +682,7 @@ cudaError_t launch_rotations(int kind, bool hi2lo, const RotLaunch & L, int max_
             if (known >= 0) {
                 cfg = known;
             } else if (dead && cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) {
-                const int t = tune(kind, hi2lo, L, dead, max_ctas, st);
+                const int t = tune(kind, hi2lo, L, dead, max_ctas, st, sched);
                 if (t >= 0) {
                     std::lock_guard<std::mutex> lk(g_tune_mu);
                     g_tuned[key] = t;
@@ -530,7 +691,7 @@ cudaError_t launch_rotations(int kind, bool hi2lo, const RotLaunch & L, int max_
             }
         }
     }
-    return launch_with(kind, hi2lo, cfg, L, max_ctas, st);
+    return launch_shape(kind, hi2lo, cfg, L, max_ctas, st, sched);
 }
 
 int rotation_ctas_per_sm(int) { return 1; }

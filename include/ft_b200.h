@@ -233,19 +233,23 @@ unsigned long long ft_b200_kernel_launches(void);
 int ft_b200_profile(int enable);
 int ft_b200_profile_read(int family, double * ms, int * launches);
 
-/* Launch shape of the rotation kernel (no counterpart in the reference, whose
- * kernels have no launch shape).  cfg = 0 .. 5 forces one of the built shapes
+/* Launch configuration of the rotation kernel (no counterpart in the reference,
+ * whose kernels have no launch shape).  cfg = s or s + 8 forces shape s = 0 .. 5
  * (warps x sweeps per warp x chunk: 8 x 8 x 16, 16 x 4 x 8, 8 x 4 x 8, 8 x 4 x 16,
  * 4 x 4 x 16 and 4 x 8 x 16, the last two with as many CTAs per SM as fit; tri has
- * no 16 x 4 x 8 and runs 8 x 8 x 16 for it); cfg = -1 (the default, or
- * FT_B200_ROT_CFG unset) lets the autotuner choose: the first out-of-place
- * launch of each shape (family, direction, all sweeps or heads only, fields,
- * tasks, N, M) times every configuration once on its destination, whose
- * contents are not needed yet, and keeps the fastest for that shape.  That first
- * launch synchronises with the stream, so make it before any stream capture; a
- * capturing stream or an in-place launch uses the untimed default (8 x 8 x 16,
- * 8 x 4 x 16 for heads).  FT_B200_AUTOTUNE=0 turns the timing off.  Results are
- * bit-identical for every configuration.  Process-wide. */
+ * no 16 x 4 x 8 and runs 8 x 8 x 16 for it); + 8 runs the pass pipeline, where
+ * each pass of 16 .. 64 sweeps of a task is its own work unit and streams down the
+ * columns on another SM right behind the previous pass (for inputs with fewer
+ * tasks than SMs; it loses where the columns would leave L2 between passes).
+ * cfg = -1 (the default, or FT_B200_ROT_CFG unset) lets the autotuner choose:
+ * the first out-of-place launch of each shape (family, direction, all sweeps or
+ * heads only, fields, tasks, N, M) times every configuration once on its
+ * destination, whose contents are not needed yet, and keeps the fastest for that
+ * shape.  That first launch synchronises with the stream, so make it before any
+ * stream capture; a capturing stream or an in-place launch uses the untimed
+ * default (8 x 8 x 16, 8 x 4 x 16 for heads, no pipeline).  FT_B200_AUTOTUNE=0
+ * turns the timing off.  Results are bit-identical for every configuration.
+ * Process-wide. */
 void ft_b200_set_rotation_config(int cfg);
 
 #ifdef __cplusplus
