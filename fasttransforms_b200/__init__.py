@@ -31,6 +31,9 @@ __all__ = [
     "execute_disk_hi2lo", "execute_disk_lo2hi",
     "execute_dev", "execute_shared_dev", "FP64", "FP64_BLOCKED", "MIXED_BF16", "MIXED_BF16X4", "device_status", "execute_noalloc_dev", "NOALLOC_MAX_ELEMS", "execute_batched_dev", "rotations_dev", "kernel_launches", "profile", "profile_read", "set_rotation_config",
     "layout_cols", "rand_layout", "sphrand", "trirand", "diskrand",
+    "SphereGridPlan", "plan_sph_synthesis", "plan_sph_analysis", "plan_sphv_synthesis", "plan_sphv_analysis",
+    "execute_sph_synthesis", "execute_sph_analysis", "execute_sphv_synthesis", "execute_sphv_analysis",
+    "execute_sph_grid_dev", "GRID_OPS",
     "SPH", "TRI", "DISK",
 ]
 
@@ -71,7 +74,13 @@ def _load() -> C.CDLL:
         "ft_b200_device_status": (i, [vp]),
         "ft_b200_profile": (i, [i]), "ft_b200_profile_read": (i, [i, C.POINTER(C.c_double), C.POINTER(i)]),
         "ft_b200_set_rotation_config": (None, [i]),
+        "ft_plan_sph_synthesis": (vp, [i, i, C.c_uint]), "ft_plan_sph_analysis": (vp, [i, i, C.c_uint]),
+        "ft_plan_sphv_synthesis": (vp, [i, i, C.c_uint]), "ft_plan_sphv_analysis": (vp, [i, i, C.c_uint]),
+        "ft_destroy_sphere_fftw_plan": (None, [vp]),
+        "ft_b200_execute_sph_grid_dev": (i, [vp, i, ch, vp, i, i, vp]),
     }
+    for name in ("sph_synthesis", "sph_analysis", "sphv_synthesis", "sphv_analysis"):
+        sig["ft_execute_" + name] = (None, [ch, vp, dp, i, i])
     for name in ("sph2fourier", "fourier2sph", "tri2cheb", "cheb2tri", "disk2cxf", "cxf2disk", "sphv2fourier", "fourier2sphv"):
         sig["ft_execute_" + name] = (None, [ch, vp, dp, i, i])
     for fam in ("sph", "tri", "disk"):
@@ -177,6 +186,49 @@ def plan_disk2cxf(n: int, alpha: float, beta: float) -> HarmonicPlan:
     return _plan("disk", n, lib.ft_plan_disk2cxf(n, alpha, beta), (alpha, beta))
 
 
+class SphereGridPlan(HarmonicPlan):
+    """Owns an ``ft_sphere_fftw_plan *``: synthesis / analysis on the sphere's N x M grid
+    (reference: src/fftw.c:63-277; cuFFT and this library's kernels in place of FFTW)."""
+
+    def __init__(self, ptr: int, kind: str, n: int, m: int):
+        super().__init__(ptr, kind, n)
+        self.m = m
+
+    @property
+    def M(self) -> int:
+        return self.m
+
+    def close(self):
+        if self.ptr:
+            lib.ft_destroy_sphere_fftw_plan(self.ptr)
+            self.ptr = None
+
+
+def _grid_plan(kind, n, m):
+    m = 2 * n - 1 if m is None else m
+    ptr = getattr(lib, "ft_plan_" + kind)(n, m, 0)
+    if not ptr:
+        _check()
+        raise FTB200Error(-1, "plan creation failed")
+    return SphereGridPlan(ptr, kind, n, m)
+
+
+def plan_sph_synthesis(n: int, m: int = None) -> SphereGridPlan: return _grid_plan("sph_synthesis", n, m)
+def plan_sph_analysis(n: int, m: int = None) -> SphereGridPlan: return _grid_plan("sph_analysis", n, m)
+def plan_sphv_synthesis(n: int, m: int = None) -> SphereGridPlan: return _grid_plan("sphv_synthesis", n, m)
+def plan_sphv_analysis(n: int, m: int = None) -> SphereGridPlan: return _grid_plan("sphv_analysis", n, m)
+
+
+GRID_OPS = {"sph_synthesis": 0, "sph_analysis": 1, "sphv_synthesis": 2, "sphv_analysis": 3}
+
+
+def execute_sph_grid_dev(P: SphereGridPlan, op: str, trans: str, ptr: int, N: int, M: int, stream: int = 0) -> None:
+    """Grid synthesis / analysis (op: a key of GRID_OPS) on a device matrix, asynchronous."""
+    st = lib.ft_b200_execute_sph_grid_dev(P.ptr, GRID_OPS[op], trans.encode(), C.c_void_p(ptr), N, M, C.c_void_p(stream))
+    if st != 0:
+        _check()
+
+
 def _host_matrix(A: np.ndarray) -> np.ndarray:
     if not (isinstance(A, np.ndarray) and A.dtype == np.float64 and A.ndim == 2 and A.flags.f_contiguous and A.flags.writeable):
         raise TypeError("A must be a writeable 2-D float64 numpy array in Fortran order")
@@ -194,6 +246,10 @@ def _exec_host(fname: str, trans: str, P: HarmonicPlan, A: np.ndarray, N=None, M
 
 
 def execute_sph2fourier(trans, P, A, N=None, M=None): _exec_host("ft_execute_sph2fourier", trans, P, A, N, M)
+def execute_sph_synthesis(trans, P, A, N=None, M=None): _exec_host("ft_execute_sph_synthesis", trans, P, A, N, M)
+def execute_sph_analysis(trans, P, A, N=None, M=None): _exec_host("ft_execute_sph_analysis", trans, P, A, N, M)
+def execute_sphv_synthesis(trans, P, A, N=None, M=None): _exec_host("ft_execute_sphv_synthesis", trans, P, A, N, M)
+def execute_sphv_analysis(trans, P, A, N=None, M=None): _exec_host("ft_execute_sphv_analysis", trans, P, A, N, M)
 def execute_fourier2sph(trans, P, A, N=None, M=None): _exec_host("ft_execute_fourier2sph", trans, P, A, N, M)
 def execute_tri2cheb(trans, P, A, N=None, M=None): _exec_host("ft_execute_tri2cheb", trans, P, A, N, M)
 def execute_cheb2tri(trans, P, A, N=None, M=None): _exec_host("ft_execute_cheb2tri", trans, P, A, N, M)

@@ -19,7 +19,8 @@ OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libft_b200.so")
 BUILD_DIR = os.path.join(HERE, "_build")
 
-SOURCES = ["rotations.cu", "trmm.cu", "blocked.cu", "trmm_mixed.cu", "api.cu", "noalloc.cu", "plan.cpp"]
+SOURCES = ["rotations.cu", "trmm.cu", "blocked.cu", "trmm_mixed.cu", "grid.cu", "api.cu", "noalloc.cu", "plan.cpp"]
+CUDA_LIB = "/usr/local/cuda/lib64"   # cuFFT (grid synthesis / analysis), same path on every box of this image
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "-ccbin", "/usr/bin/g++"]
@@ -48,7 +49,7 @@ def build(verbose: bool = False) -> str:
         objs.append(obj)
     link = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-cudart", "static",
             "-Xlinker", "--version-script=" + os.path.join(CSRC, "exports.map"), "-Xlinker", "-Bsymbolic",
-            "-lpthread"]
+            "-L" + CUDA_LIB, "-lcufft", "-Xlinker", "-rpath=" + CUDA_LIB, "-lpthread"]
     _run(link)
     return LIB
 

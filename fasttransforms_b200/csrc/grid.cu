@@ -1,0 +1,387 @@
+// Synthesis and analysis on the sphere's tensor-product grid (the reference's
+// ft_plan_sph_synthesis / ft_execute_sph_synthesis and friends, src/fftw.c:63-277):
+// the Fourier coefficients that sph2fourier produces become values at the N x M
+// points theta_i = (i + 1/2) pi / N, phi_k = 2 pi k / M, and back.
+//
+// Two one-dimensional stages:
+//   theta (down each column, length N): the four stride-4 column classes take the
+//     plan's two kinds (classes 0 and 3 the first, 1 and 2 the second), each a
+//     cosine or sine transform of type II (analysis) or III (synthesis) in FFTW's
+//     unnormalised definitions (REDFT10 / RODFT10 / REDFT01 / RODFT01);
+//   phi (along each row, length M): a real DFT, complex-to-real for synthesis and
+//     real-to-complex for analysis, unnormalised, on the half spectrum laid out as
+//     the reference's: column 2j is the real part of frequency j, column 2j - 1 the
+//     negated imaginary part.
+// with the reference's scalings and end-entry factors in between.
+//
+// The cosine transforms go through complex FFTs of length N (Makhoul's reordering):
+//   DCT-II:  v = (x_0, x_2, x_4, .., x_5, x_3, x_1), V = DFT(v),
+//            y_k = 2 Re(exp(-i pi k / 2N) V_k);
+//   DCT-III: V_k = (y_k - i y_{N-k}) exp(i pi k / 2N) (y_N = 0), a Hermitian
+//            spectrum, v = unnormalised inverse DFT(V), x = v un-permuted;
+// and the sine transforms through them: DST-II(x)_k = DCT-II((-1)^n x_n)_{N-1-k},
+// DST-III(x)_k = (-1)^k DCT-III(x reversed)_k.  The DFTs are cuFFT's (library
+// FFTs, batched over all M columns at once); the reorderings, twiddles, scalings and
+// the half-spectrum packing are this file's kernels.
+#include <cmath>
+#include <cstring>
+#include <mutex>
+
+#include <cufft.h>
+
+#include "ft_internal.h"
+
+namespace ftb {
+namespace {
+
+// FFTW r2r kinds used by the plans (the values of fftw3.h's enum)
+enum { K_REDFT01 = 4, K_REDFT10 = 5, K_RODFT01 = 8, K_RODFT10 = 9 };
+enum Op { SPH_SYN = 0, SPH_ANA = 1, SPHV_SYN = 2, SPHV_ANA = 3 };
+
+constexpr int kGridMagic = 0x46544753;   // "FTGS"
+
+// The reference's constants (src/ftinternal.h:48-56)
+constexpr double C_1_4_SQRT_PI = 0.141047395886939072;   // 1 / (4 sqrt(pi))
+constexpr double C_1_2_SQRT_PI = 0.282094791773878143;   // 1 / (2 sqrt(pi))
+constexpr double C_4_SQRT_PI = 7.089815403622064109;     // 4 sqrt(pi)
+constexpr double C_2_SQRT_PI = 3.544907701811032055;     // 2 sqrt(pi)
+constexpr double C_SQRT2 = 1.41421356237309504880;
+constexpr double C_SQRT1_2 = 0.70710678118654752440;
+
+bool is_dst(int kind) { return kind == K_RODFT01 || kind == K_RODFT10; }
+bool is_type3(int kind) { return kind == K_REDFT01 || kind == K_RODFT01; }
+
+}  // namespace
+
+struct SphereGridPlan {
+    int magic = kGridMagic;
+    int N = 0, M = 0;
+    int kind[2] = {0, 0};        // theta kinds of column classes {0, 3} and {1, 2}
+    int device = 0;
+    cufftHandle t_r2c = 0;       // length N, batch M (cosine type II)
+    cufftHandle t_c2r = 0;       // length N, batch M (cosine type III)
+    cufftHandle p_r2c = 0;       // length M along rows, batch N
+    cufftHandle p_c2r = 0;
+    bool have_t_r2c = false, have_t_c2r = false, have_p_r2c = false, have_p_c2r = false;
+    double * d_work = nullptr;   // N x M real
+    double2 * d_cwork = nullptr; // (N/2 + 1) x M complex
+    double2 * d_Y = nullptr;     // N x (M/2 + 1) complex, element (i, j) at i + j N
+    double * d_stage = nullptr;  // N x M, host-pointer calls
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+};
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// theta stage kernels: one thread per (entry, column); column j uses the kind of
+// its class, cls(j) = j mod 4 in {0, 3} -> kind[0], {1, 2} -> kind[1]
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool col_dst(int j, int k0dst, int k1dst) {
+    const int r = j & 3;
+    return (r == 0 || r == 3) ? k0dst : k1dst;
+}
+
+// type II, before the FFT: v = permute(sign-flipped x) into work
+__global__ void t2_pre(const double * __restrict__ X, double * __restrict__ V, int N, int M, int k0dst, int k1dst) {
+    const long long idx = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long) N * M) return;
+    const int j = (int) (idx / N), n = (int) (idx % N);
+    const bool dst = col_dst(j, k0dst, k1dst);
+    // v[n] = x'[2n] for n < ceil(N/2), v[N-1-n'] = x'[2n'+1]
+    const int h = (N + 1) / 2;
+    const int src = n < h ? 2 * n : 2 * (N - 1 - n) + 1;
+    double x = X[(long long) j * N + src];
+    if (dst && (src & 1)) x = -x;            // (-1)^n x_n
+    V[(long long) j * N + n] = x;
+}
+
+// type II, after the FFT: y_k = 2 Re(exp(-i pi k / 2N) V_k), reversed for sine columns
+__global__ void t2_post(const double2 * __restrict__ C, double * __restrict__ X, int N, int M, int k0dst, int k1dst) {
+    const long long idx = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long) N * M) return;
+    const int j = (int) (idx / N), k = (int) (idx % N);
+    const bool dst = col_dst(j, k0dst, k1dst);
+    const int H = N / 2 + 1;
+    double2 v = k < H ? C[(long long) j * H + k] : C[(long long) j * H + (N - k)];
+    if (k >= H) v.y = -v.y;                  // V_k = conj(V_{N-k})
+    double s, c;
+    sincospi((double) k / (2.0 * N), &s, &c);
+    const double y = 2.0 * (c * v.x + s * v.y);   // Re((c - i s)(v.x + i v.y))
+    X[(long long) j * N + (dst ? N - 1 - k : k)] = y;
+}
+
+// type III, before the inverse FFT: V_k = (y_k - i y_{N-k}) exp(i pi k / 2N), k <= N/2,
+// with y reversed for sine columns
+__global__ void t3_pre(const double * __restrict__ X, double2 * __restrict__ C, int N, int M, int k0dst, int k1dst) {
+    const int H = N / 2 + 1;
+    const long long idx = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long) H * M) return;
+    const int j = (int) (idx / H), k = (int) (idx % H);
+    const bool dst = col_dst(j, k0dst, k1dst);
+    const double * y = X + (long long) j * N;
+    auto yy = [&](int t) -> double { return t >= N ? 0.0 : (dst ? y[N - 1 - t] : y[t]); };
+    const double a = yy(k), b = k == 0 ? 0.0 : yy(N - k);
+    double s, c;
+    sincospi((double) k / (2.0 * N), &s, &c);
+    double2 v = make_double2(a * c + b * s, a * s - b * c);   // (a - i b)(c + i s)
+    if ((N & 1) == 0 && k == N / 2) v.y = 0.0;                // the Nyquist term is real
+    C[(long long) j * H + k] = v;
+}
+
+// type III, after the inverse FFT: x un-permuted, (-1)^k for sine columns
+__global__ void t3_post(const double * __restrict__ V, double * __restrict__ X, int N, int M, int k0dst, int k1dst) {
+    const long long idx = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long) N * M) return;
+    const int j = (int) (idx / N), k = (int) (idx % N);
+    const bool dst = col_dst(j, k0dst, k1dst);
+    const int h = (N + 1) / 2;
+    const int n = (k & 1) ? N - 1 - (k >> 1) : (k >> 1);     // x[2n] = v[n], x[2n+1] = v[N-1-n]
+    double x = V[(long long) j * N + n];
+    if (dst && (k & 1)) x = -x;
+    (void) h;
+    X[(long long) j * N + k] = x;
+}
+
+// ---------------------------------------------------------------------------
+// phi stage packing and the scalings
+// ---------------------------------------------------------------------------
+// Y(i, 0) = (s X(i, 0)) f0; Y(i, j) = s (X(i, 2j) - i X(i, 2j - 1)), j = 1 .. M/2
+__global__ void pack_r2c(const double * __restrict__ X, double2 * __restrict__ Y, int N, int M, double s, double f0) {
+    const int H = M / 2 + 1;
+    const long long idx = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long) N * H) return;
+    const int j = (int) (idx / N), i = (int) (idx % N);
+    double2 v;
+    if (j == 0) v = make_double2((s * X[i]) * f0, 0.0);
+    else        v = make_double2(s * X[i + (long long) (2 * j) * N], -s * X[i + (long long) (2 * j - 1) * N]);
+    Y[idx] = v;
+}
+
+// X(i, 0) = (s Re Y(i, 0)) f0; X(i, 2j) = s Re Y(i, j); X(i, 2j - 1) = s (-Im Y(i, j))
+__global__ void unpack_c2r(const double2 * __restrict__ Y, double * __restrict__ X, int N, int M, double s, double f0) {
+    const int H = M / 2 + 1;
+    const long long idx = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long) N * H) return;
+    const int j = (int) (idx / N), i = (int) (idx % N);
+    const double2 v = Y[idx];
+    if (j == 0) { X[i] = (s * v.x) * f0; return; }
+    X[i + (long long) (2 * j) * N] = s * v.x;
+    X[i + (long long) (2 * j - 1) * N] = -s * v.y;
+}
+
+// Multiplies the first (last = 0) or last (last = 1) entry of the columns
+// {c0} (c0 >= 0) and {start + 4t, start + 1 + 4t, t >= 0} by f.
+__global__ void scale_ends(double * X, int N, int M, bool last, int c0, int start, double f) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int row = last ? N - 1 : 0;
+    if (t == 0 && c0 >= 0 && c0 < M) X[(long long) c0 * N + row] *= f;
+    const int j0 = start + 4 * t;
+    if (j0 < M) X[(long long) j0 * N + row] *= f;
+    if (j0 + 1 < M) X[(long long) (j0 + 1) * N + row] *= f;
+}
+
+bool ok(cudaError_t e, const char * what) {
+    if (e == cudaSuccess) return true;
+    set_error(e == cudaErrorMemoryAllocation ? FT_B200_ENOMEM : FT_B200_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return false;
+}
+bool fok(cufftResult r, const char * what) {
+    if (r == CUFFT_SUCCESS) return true;
+    set_error(r == CUFFT_ALLOC_FAILED ? FT_B200_ENOMEM : FT_B200_ECUDA, std::string(what) + ": cuFFT error " + std::to_string((int) r));
+    return false;
+}
+
+unsigned blocks(long long n) { return (unsigned) ((n + 255) / 256); }
+
+SphereGridPlan * make_plan(int N, int M, int k0, int k1) {
+    clear_error();
+    if (N < 1 || M < 1) { set_error(FT_B200_EINVAL, "N and M must be positive"); return nullptr; }
+    if (M % 2 == 0) { set_error(FT_B200_EINVAL, "M must be odd (the half spectrum holds columns 2j - 1, 2j)"); return nullptr; }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { set_error(FT_B200_ENODEV, "no CUDA device"); return nullptr; }
+    SphereGridPlan * P = new SphereGridPlan();
+    P->N = N; P->M = M; P->kind[0] = k0; P->kind[1] = k1;
+    cudaGetDevice(&P->device);
+    const size_t nm = (size_t) N * M;
+    bool good = ok(cudaMalloc(&P->d_work, sizeof(double) * nm), "cudaMalloc(grid work)") &&
+                ok(cudaMalloc(&P->d_cwork, sizeof(double2) * (size_t) (N / 2 + 1) * M), "cudaMalloc(grid work)") &&
+                ok(cudaMalloc(&P->d_Y, sizeof(double2) * (size_t) N * (M / 2 + 1)), "cudaMalloc(grid spectrum)") &&
+                ok(cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (good) {
+        int n[1] = {N};
+        if (is_type3(k0)) {
+            good = fok(cufftPlanMany(&P->t_c2r, 1, n, nullptr, 1, N / 2 + 1, nullptr, 1, N, CUFFT_Z2D, M), "cufftPlanMany");
+            P->have_t_c2r = good;
+        } else {
+            good = fok(cufftPlanMany(&P->t_r2c, 1, n, nullptr, 1, N, nullptr, 1, N / 2 + 1, CUFFT_D2Z, M), "cufftPlanMany");
+            P->have_t_r2c = good;
+        }
+    }
+    if (good) {
+        // phi: along rows, element stride N, rows one apart
+        int m[1] = {M}, hm[1] = {M / 2 + 1};
+        good = fok(cufftPlanMany(&P->p_c2r, 1, m, hm, N, 1, m, N, 1, CUFFT_Z2D, N), "cufftPlanMany");
+        P->have_p_c2r = good;
+        if (good) {
+            good = fok(cufftPlanMany(&P->p_r2c, 1, m, m, N, 1, hm, N, 1, CUFFT_D2Z, N), "cufftPlanMany");
+            P->have_p_r2c = good;
+        }
+    }
+    if (!good) {
+        ft_destroy_sphere_fftw_plan(reinterpret_cast<ft_sphere_fftw_plan *>(P));
+        return nullptr;
+    }
+    return P;
+}
+
+// theta transforms of all M columns in place (the plan's kinds by column class)
+bool theta(SphereGridPlan * P, double * X, cudaStream_t st) {
+    const int N = P->N, M = P->M;
+    const int d0 = is_dst(P->kind[0]), d1 = is_dst(P->kind[1]);
+    if (is_type3(P->kind[0])) {
+        if (!fok(cufftSetStream(P->t_c2r, st), "cufftSetStream")) return false;
+        t3_pre<<<blocks((long long) (N / 2 + 1) * M), 256, 0, st>>>(X, P->d_cwork, N, M, d0, d1);
+        count_launch();
+        if (!ok(cudaGetLastError(), "t3_pre")) return false;
+        if (!fok(cufftExecZ2D(P->t_c2r, reinterpret_cast<cufftDoubleComplex *>(P->d_cwork), P->d_work), "cufftExecZ2D")) return false;
+        t3_post<<<blocks((long long) N * M), 256, 0, st>>>(P->d_work, X, N, M, d0, d1);
+        count_launch();
+        return ok(cudaGetLastError(), "t3_post");
+    }
+    if (!fok(cufftSetStream(P->t_r2c, st), "cufftSetStream")) return false;
+    t2_pre<<<blocks((long long) N * M), 256, 0, st>>>(X, P->d_work, N, M, d0, d1);
+    count_launch();
+    if (!ok(cudaGetLastError(), "t2_pre")) return false;
+    if (!fok(cufftExecD2Z(P->t_r2c, P->d_work, reinterpret_cast<cufftDoubleComplex *>(P->d_cwork)), "cufftExecD2Z")) return false;
+    t2_post<<<blocks((long long) N * M), 256, 0, st>>>(P->d_cwork, X, N, M, d0, d1);
+    count_launch();
+    return ok(cudaGetLastError(), "t2_post");
+}
+
+bool phi_c2r(SphereGridPlan * P, const double * X, double s, double f0, cudaStream_t st) {
+    const int N = P->N, M = P->M;
+    pack_r2c<<<blocks((long long) N * (M / 2 + 1)), 256, 0, st>>>(X, P->d_Y, N, M, s, f0);
+    count_launch();
+    if (!ok(cudaGetLastError(), "pack_r2c")) return false;
+    return fok(cufftSetStream(P->p_c2r, st), "cufftSetStream") &&
+           fok(cufftExecZ2D(P->p_c2r, reinterpret_cast<cufftDoubleComplex *>(P->d_Y), const_cast<double *>(X)), "cufftExecZ2D");
+}
+
+bool phi_r2c(SphereGridPlan * P, double * X, double s, double f0, cudaStream_t st) {
+    const int N = P->N, M = P->M;
+    if (!fok(cufftSetStream(P->p_r2c, st), "cufftSetStream") ||
+        !fok(cufftExecD2Z(P->p_r2c, X, reinterpret_cast<cufftDoubleComplex *>(P->d_Y)), "cufftExecD2Z")) return false;
+    unpack_c2r<<<blocks((long long) N * (M / 2 + 1)), 256, 0, st>>>(P->d_Y, X, N, M, s, f0);
+    count_launch();
+    return ok(cudaGetLastError(), "unpack_c2r");
+}
+
+bool ends(SphereGridPlan * P, double * X, bool last, int c0, int start, double f, cudaStream_t st) {
+    const int t = (P->M - start + 3) / 4 + 1;
+    scale_ends<<<blocks(t > 0 ? t : 1), 256, 0, st>>>(X, P->N, P->M, last, c0, start, f);
+    count_launch();
+    return ok(cudaGetLastError(), "scale_ends");
+}
+
+// The reference's execute sequences (src/fftw.c:131-277).  End-entry factors: first
+// entries of {0, 3, 4, 7, 8, ..} (sph) or {1, 2, 5, 6, ..} (sphv); last entries of
+// {1, 2, 5, 6, ..} (sph) or {0, 3, 4, 7, 8, ..} (sphv).
+bool run(SphereGridPlan * P, int op, char T, double * X, cudaStream_t st) {
+    const int N = P->N, M = P->M;
+    const double nm2 = 2.0 * N * M;
+    const bool sph = op == SPH_SYN || op == SPH_ANA;
+    auto first = [&](double f) { return sph ? ends(P, X, false, 0, 3, f, st) : ends(P, X, false, -1, 1, f, st); };
+    auto last = [&](double f) { return sph ? ends(P, X, true, -1, 1, f, st) : ends(P, X, true, 0, 3, f, st); };
+    if (op == SPH_SYN || op == SPHV_SYN) {
+        if (T == 'N') return first(2.0) && theta(P, X, st) && phi_c2r(P, X, C_1_4_SQRT_PI, C_SQRT2, st);
+        return phi_r2c(P, X, C_1_2_SQRT_PI, C_SQRT1_2, st) && theta(P, X, st) && last(0.5);
+    }
+    if (T == 'N') return phi_r2c(P, X, C_4_SQRT_PI / nm2, C_SQRT1_2, st) && theta(P, X, st) && first(0.5);
+    return last(2.0) && theta(P, X, st) && phi_c2r(P, X, C_2_SQRT_PI / nm2, C_SQRT2, st);
+}
+
+SphereGridPlan * as_grid(const ft_sphere_fftw_plan * P) {
+    SphereGridPlan * G = reinterpret_cast<SphereGridPlan *>(const_cast<ft_sphere_fftw_plan *>(P));
+    return (G && G->magic == kGridMagic) ? G : nullptr;
+}
+
+int check_call(SphereGridPlan * G, char T, const double * X, int N, int M) {
+    if (!G) { set_error(FT_B200_EINVAL, "not a sphere grid plan of this library"); return FT_B200_EINVAL; }
+    if (T != 'N' && T != 'T') { set_error(FT_B200_EINVAL, "TRANS must be 'N' or 'T'"); return FT_B200_EINVAL; }
+    if (!X) { set_error(FT_B200_EINVAL, "NULL matrix"); return FT_B200_EINVAL; }
+    if (N != G->N || M != G->M) { set_error(FT_B200_EINVAL, "N, M do not match the plan"); return FT_B200_EINVAL; }
+    return FT_B200_OK;
+}
+
+void execute_host(int op, char T, const ft_sphere_fftw_plan * P, double * X, int N, int M) {
+    clear_error();
+    SphereGridPlan * G = as_grid(P);
+    if (check_call(G, T, X, N, M) != FT_B200_OK) return;
+    std::lock_guard<std::mutex> lk(G->mu);
+    cudaSetDevice(G->device);
+    const size_t bytes = sizeof(double) * (size_t) N * M;
+    if (!G->d_stage && !ok(cudaMalloc(&G->d_stage, bytes), "cudaMalloc(grid stage)")) return;
+    if (!ok(cudaMemcpyAsync(G->d_stage, X, bytes, cudaMemcpyHostToDevice, G->stream), "cudaMemcpyAsync(H2D)")) return;
+    if (!run(G, op, T, G->d_stage, G->stream)) return;
+    if (!ok(cudaMemcpyAsync(X, G->d_stage, bytes, cudaMemcpyDeviceToHost, G->stream), "cudaMemcpyAsync(D2H)")) return;
+    ok(cudaStreamSynchronize(G->stream), "cudaStreamSynchronize");
+}
+
+}  // namespace
+}  // namespace ftb
+
+using namespace ftb;
+
+extern "C" {
+
+ft_sphere_fftw_plan * ft_plan_sph_synthesis(const int N, const int M, const unsigned) {
+    return reinterpret_cast<ft_sphere_fftw_plan *>(make_plan(N, M, K_REDFT01, K_RODFT01));
+}
+ft_sphere_fftw_plan * ft_plan_sph_analysis(const int N, const int M, const unsigned) {
+    return reinterpret_cast<ft_sphere_fftw_plan *>(make_plan(N, M, K_REDFT10, K_RODFT10));
+}
+ft_sphere_fftw_plan * ft_plan_sphv_synthesis(const int N, const int M, const unsigned) {
+    return reinterpret_cast<ft_sphere_fftw_plan *>(make_plan(N, M, K_RODFT01, K_REDFT01));
+}
+ft_sphere_fftw_plan * ft_plan_sphv_analysis(const int N, const int M, const unsigned) {
+    return reinterpret_cast<ft_sphere_fftw_plan *>(make_plan(N, M, K_RODFT10, K_REDFT10));
+}
+
+void ft_destroy_sphere_fftw_plan(ft_sphere_fftw_plan * Pp) {
+    SphereGridPlan * P = as_grid(Pp);
+    if (!P) return;
+    if (P->have_t_r2c) cufftDestroy(P->t_r2c);
+    if (P->have_t_c2r) cufftDestroy(P->t_c2r);
+    if (P->have_p_r2c) cufftDestroy(P->p_r2c);
+    if (P->have_p_c2r) cufftDestroy(P->p_c2r);
+    cudaFree(P->d_work); cudaFree(P->d_cwork); cudaFree(P->d_Y); cudaFree(P->d_stage);
+    if (P->stream) cudaStreamDestroy(P->stream);
+    P->magic = 0;
+    delete P;
+}
+
+void ft_execute_sph_synthesis(const char TRANS, const ft_sphere_fftw_plan * P, double * X, const int N, const int M) {
+    execute_host(SPH_SYN, TRANS, P, X, N, M);
+}
+void ft_execute_sph_analysis(const char TRANS, const ft_sphere_fftw_plan * P, double * X, const int N, const int M) {
+    execute_host(SPH_ANA, TRANS, P, X, N, M);
+}
+void ft_execute_sphv_synthesis(const char TRANS, const ft_sphere_fftw_plan * P, double * X, const int N, const int M) {
+    execute_host(SPHV_SYN, TRANS, P, X, N, M);
+}
+void ft_execute_sphv_analysis(const char TRANS, const ft_sphere_fftw_plan * P, double * X, const int N, const int M) {
+    execute_host(SPHV_ANA, TRANS, P, X, N, M);
+}
+
+int ft_b200_execute_sph_grid_dev(const ft_sphere_fftw_plan * P, int op, char TRANS, double * dX, int N, int M, void * stream) {
+    clear_error();
+    SphereGridPlan * G = as_grid(P);
+    const int c = check_call(G, TRANS, dX, N, M);
+    if (c != FT_B200_OK) return c;
+    if (op < SPH_SYN || op > SPHV_ANA) { set_error(FT_B200_EINVAL, "op must be 0 .. 3"); return FT_B200_EINVAL; }
+    std::lock_guard<std::mutex> lk(G->mu);
+    return run(G, op, TRANS, dX, static_cast<cudaStream_t>(stream)) ? FT_B200_OK : ft_b200_last_status();
+}
+
+}  // extern "C"

@@ -109,6 +109,29 @@ void ft_execute_cxf2disk(const char TRANS, const ft_harmonic_plan * P, double * 
 /* replaces ft_destroy_harmonic_plan, src/drivers.c:793-814 */
 void ft_destroy_harmonic_plan(ft_harmonic_plan * P);
 
+/* Synthesis and analysis on the sphere's grid (theta_i = (i + 1/2) pi / N,
+ * phi_k = 2 pi k / M), src/fftw.c.  The plan type is this library's own (the
+ * reference's holds FFTW plans); the flags argument is accepted and not used.
+ * M must be odd.  Host-pointer calls stage X on the device and synchronise;
+ * ft_b200_execute_sph_grid_dev is the device-pointer form. */
+typedef struct ft_sphere_fftw_plan_s ft_sphere_fftw_plan;
+/* replace ft_plan_sph_synthesis / ft_plan_sph_analysis, src/fftw.c:104-112 */
+ft_sphere_fftw_plan * ft_plan_sph_synthesis(const int N, const int M, const unsigned flags);
+ft_sphere_fftw_plan * ft_plan_sph_analysis(const int N, const int M, const unsigned flags);
+/* replace ft_plan_sphv_synthesis / ft_plan_sphv_analysis, src/fftw.c:114-122 */
+ft_sphere_fftw_plan * ft_plan_sphv_synthesis(const int N, const int M, const unsigned flags);
+ft_sphere_fftw_plan * ft_plan_sphv_analysis(const int N, const int M, const unsigned flags);
+/* replaces ft_destroy_sphere_fftw_plan, src/fftw.c:66-74 */
+void ft_destroy_sphere_fftw_plan(ft_sphere_fftw_plan * P);
+/* replace ft_execute_sph_synthesis / ft_execute_sph_analysis, src/fftw.c:124-200 */
+void ft_execute_sph_synthesis(const char TRANS, const ft_sphere_fftw_plan * P, double * X, const int N, const int M);
+void ft_execute_sph_analysis(const char TRANS, const ft_sphere_fftw_plan * P, double * X, const int N, const int M);
+/* replace ft_execute_sphv_synthesis / ft_execute_sphv_analysis, src/fftw.c:202-277 */
+void ft_execute_sphv_synthesis(const char TRANS, const ft_sphere_fftw_plan * P, double * X, const int N, const int M);
+void ft_execute_sphv_analysis(const char TRANS, const ft_sphere_fftw_plan * P, double * X, const int N, const int M);
+/* the reference's flags for these planners (src/ftutilities.h:24); not used here */
+#define FT_FFTW_FLAGS 0u
+
 /* Rotation level. */
 /* replaces ft_plan_rotsphere, src/rotations.c:116-133 */
 ft_rotation_plan * ft_plan_rotsphere(const int n);
@@ -138,6 +161,12 @@ enum { FT_B200_SPH = 0, FT_B200_TRI = 1, FT_B200_DISK = 2 };
 /* Full transform.  forward = 1: sph2fourier / tri2cheb / disk2cxf;
  * forward = 0: fourier2sph / cheb2tri / cxf2disk. */
 int ft_b200_execute_dev(const ft_harmonic_plan * P, int forward, char TRANS, double * dA, int N, int M, void * stream);
+/* Grid synthesis / analysis on device memory: op 0 sph synthesis, 1 sph analysis,
+ * 2 sphv synthesis, 3 sphv analysis (the sequences of the ft_execute_* above, with
+ * the plan's transform kinds), asynchronous on stream.  No counterpart in the
+ * reference (its calls take host memory). */
+int ft_b200_execute_sph_grid_dev(const ft_sphere_fftw_plan * P, int op, char TRANS, double * dX, int N, int M, void * stream);
+
 /* The sph vector-field transforms on device memory (forward = 1: sphv2fourier). */
 int ft_b200_execute_sphv_dev(const ft_harmonic_plan * P, int forward, char TRANS, double * dA, int N, int M, void * stream);
 /* Rotation stage alone (hi2lo = 1: ft_execute_*_hi2lo; 0: *_lo2hi). */

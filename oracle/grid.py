@@ -1,0 +1,148 @@
+"""Oracle (test infrastructure, not the product): a CPU restatement of the
+sphere grid synthesis and analysis of the reference (src/fftw.c:63-277:
+ft_plan_sph_with_kind, ft_execute_sph_synthesis / _analysis and the sphv
+variants) in numpy / scipy.
+
+FFTW, which the reference calls for these transforms, is not available here, so
+its one-dimensional transforms are restated from their published definitions
+(FFTW manual, "What FFTW Really Computes"), all unnormalised:
+  REDFT10 (DCT-II)  y_k = 2 sum_j x_j cos(pi (j + 1/2) k / N)
+  REDFT01 (DCT-III) y_k = x_0 + 2 sum_{j>=1} x_j cos(pi j (k + 1/2) / N)
+  RODFT10 (DST-II)  y_k = 2 sum_j x_j sin(pi (j + 1/2) (k + 1) / N)
+  RODFT01 (DST-III) y_k = (-1)^k x_{N-1} + 2 sum_{j<N-1} x_j sin(pi (j + 1) (k + 1/2) / N)
+  c2r of length M   x_k = sum over the Hermitian-completed spectrum of Y_j e^{2 pi i jk / M}
+  r2c of length M   Y_j = sum_k x_k e^{-2 pi i jk / M}
+which scipy.fft's dct / dst of types 2 and 3 (norm=None) and numpy's rfft /
+irfft (times M) compute.  tests/test_oracle_grid.py checks those identities
+against the explicit sums, and pins the sequences and scalings through the
+reference's own test (src/fftw.c round trip with the compiled reference's
+sph2fourier / fourier2sph, test/test_fftw.c:43-73) and known harmonics.
+"""
+import numpy as np
+import scipy.fft as sf
+
+REDFT01, REDFT10, RODFT01, RODFT10 = "REDFT01", "REDFT10", "RODFT01", "RODFT10"
+
+# plan kinds (classes {0, 3}, classes {1, 2}): src/fftw.c:104-122
+PLANS = {
+    "sph_synthesis": (REDFT01, RODFT01),
+    "sph_analysis": (REDFT10, RODFT10),
+    "sphv_synthesis": (RODFT01, REDFT01),
+    "sphv_analysis": (RODFT10, REDFT10),
+}
+
+# src/ftinternal.h:48-56
+M_1_4_SQRT_PI = 0.141047395886939072
+M_1_2_SQRT_PI = 0.282094791773878143
+M_4_SQRT_PI = 7.089815403622064109
+M_2_SQRT_PI = 3.544907701811032055
+M_SQRT2 = 1.41421356237309504880
+M_SQRT1_2 = 0.70710678118654752440
+
+
+def r2r(x, kind):
+    """FFTW's 1-d real transform `kind` down the columns of x (axis 0)."""
+    if kind == REDFT10:
+        return sf.dct(x, type=2, axis=0)
+    if kind == REDFT01:
+        return sf.dct(x, type=3, axis=0)
+    if kind == RODFT10:
+        return sf.dst(x, type=2, axis=0)
+    if kind == RODFT01:
+        return sf.dst(x, type=3, axis=0)
+    raise ValueError(kind)
+
+
+def theta(X, kinds):
+    """plantheta1 .. 4 (src/fftw.c:85-95): column classes j mod 4 = 0, 3 take
+    kinds[0], classes 1, 2 take kinds[1]."""
+    Y = X.copy()
+    for r, k in ((0, kinds[0]), (1, kinds[1]), (2, kinds[1]), (3, kinds[0])):
+        if Y[:, r::4].shape[1]:
+            Y[:, r::4] = r2r(X[:, r::4], k)
+    return Y
+
+
+def data_r2c(X):
+    """src/fftw.c:40-49: column 0 -> frequency 0, (2j, 2j - 1) -> Re, -Im of frequency j."""
+    N, M = X.shape
+    Y = np.zeros((N, M // 2 + 1), dtype=complex)
+    Y[:, 0] = X[:, 0]
+    for j in range(1, M // 2 + 1):
+        Y[:, j] = X[:, 2 * j] - 1j * X[:, 2 * j - 1]
+    return Y
+
+
+def data_c2r(Y, M):
+    """src/fftw.c:51-60."""
+    N = Y.shape[0]
+    X = np.zeros((N, M))
+    X[:, 0] = Y[:, 0].real
+    for j in range(1, M // 2 + 1):
+        X[:, 2 * j] = Y[:, j].real
+        X[:, 2 * j - 1] = -Y[:, j].imag
+    return X
+
+
+def c2r(Y, M):
+    return np.fft.irfft(Y, n=M, axis=1) * M
+
+
+def r2c(X):
+    return np.fft.rfft(X, axis=1)
+
+
+def _ends(X, first, sph, f):
+    """The end-entry factors of the sequences: first entries of columns
+    {0, 3, 4, 7, 8, ..} (sph) or {1, 2, 5, 6, ..} (sphv); last entries of
+    {1, 2, 5, 6, ..} (sph) or {0, 3, 4, 7, 8, ..} (sphv)."""
+    N, M = X.shape
+    row = 0 if first else N - 1
+    if first == sph:
+        cols = [0] + [c for j in range(3, M, 4) for c in (j, j + 1) if c < M]
+    else:
+        cols = [c for j in range(1, M, 4) for c in (j, j + 1) if c < M]
+    for c in cols:
+        X[row, c] *= f
+
+
+def execute(op, trans, plan, X):
+    """ft_execute_{sph,sphv}_{synthesis,analysis}(trans, P, X) with P a plan of
+    kind `plan` (a key of PLANS).  op: "sph_synthesis", "sph_analysis",
+    "sphv_synthesis", "sphv_analysis".  Returns the new X (N x M, column-major
+    meaning: X[i, j] is row i, column j)."""
+    X = np.array(X, dtype=float, copy=True)
+    N, M = X.shape
+    kinds = PLANS[plan]
+    sph = op.startswith("sph_")
+    nm2 = 2.0 * N * M
+    if op.endswith("synthesis"):
+        if trans == "N":                                # src/fftw.c:124-146, 202-219
+            _ends(X, True, sph, 2.0)
+            X = theta(X, kinds)
+            X *= M_1_4_SQRT_PI
+            X[:, 0] *= M_SQRT2
+            return c2r(data_r2c(X), M)
+        X = data_c2r(r2c(X), M)                         # :147-164, 220-237
+        X *= M_1_2_SQRT_PI
+        X[:, 0] *= M_SQRT1_2
+        X = theta(X, kinds)
+        _ends(X, False, sph, 0.5)
+        return X
+    if trans == "N":                                    # :166-183, 239-256
+        X = data_c2r(r2c(X), M)
+        X *= M_4_SQRT_PI / nm2
+        X[:, 0] *= M_SQRT1_2
+        X = theta(X, kinds)
+        _ends(X, True, sph, 0.5)
+        return X
+    _ends(X, False, sph, 2.0)                           # :184-199, 257-276
+    X = theta(X, kinds)
+    X *= M_2_SQRT_PI / nm2
+    X[:, 0] *= M_SQRT2
+    return c2r(data_r2c(X), M)
+
+
+def grid(N, M):
+    """The points: theta_i = (i + 1/2) pi / N, phi_k = 2 pi k / M."""
+    return (np.arange(N) + 0.5) * np.pi / N, 2 * np.pi * np.arange(M) / M

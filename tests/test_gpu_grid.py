@@ -1,0 +1,123 @@
+"""Sphere grid synthesis and analysis on the GPU (ft_plan_sph_synthesis ..
+ft_execute_sphv_analysis, src/fftw.c:63-277), through the C ABI.
+
+Against the oracle (oracle/grid.py, pinned in tests/test_oracle_grid.py): every
+operation, both TRANS values and the plans the reference's test crosses, within
+1e-14 relative 2-norm.  The reference's own accuracy test (test/test_fftw.c:43-73)
+on the GPU path: sph2fourier, synthesis, analysis, fourier2sph in 'N' then 'T'
+return the input within 4 sqrt(N) eps and 2N eps.  Known harmonics on the grid."""
+import numpy as np
+import pytest
+
+from conftest import EPS, rel2
+
+pytestmark = pytest.mark.gpu
+
+OPS = ["sph_synthesis", "sph_analysis", "sphv_synthesis", "sphv_analysis"]
+
+
+@pytest.fixture(scope="module")
+def env():
+    import torch
+    import fasttransforms_b200 as ft
+    torch.cuda.set_device(0)
+    return ft, torch
+
+
+def run_dev(ft, torch, P, op, tr, X):
+    n, m = X.shape
+    t = torch.from_numpy(np.asfortranarray(X).ravel(order="F").copy()).cuda()
+    ft.execute_sph_grid_dev(P, op, tr, t.data_ptr(), n, m, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    return t.cpu().numpy().reshape((n, m), order="F")
+
+
+@pytest.mark.parametrize("N,M", [(1, 1), (2, 3), (3, 5), (8, 15), (17, 33), (64, 127), (33, 21), (256, 511)])
+def test_grid_vs_oracle(env, N, M):
+    ft, torch = env
+    from oracle import grid as G
+    X = np.random.default_rng(N * 1000 + M).uniform(-1, 1, (N, M))
+    plans = {k: getattr(ft, "plan_" + k)(N, M) for k in OPS}
+    try:
+        for op in OPS:
+            for tr in "NT":
+                for plan in OPS:   # every plan with every sequence (the reference's test crosses them)
+                    got = run_dev(ft, torch, plans[plan], op, tr, X)
+                    want = G.execute(op, tr, plan, X)
+                    assert rel2(got, want) <= 1e-14, (N, M, op, tr, plan, rel2(got, want))
+    finally:
+        for P in plans.values():
+            P.close()
+
+
+@pytest.mark.parametrize("N", [64, 128, 256, 1024])
+def test_reference_round_trip_on_gpu(env, N):
+    """test/test_fftw.c:43-73 on this library: every stage on the GPU."""
+    ft, torch = env
+    M = 2 * N - 1
+    A = ft.sphrand(N, 9)
+    P = ft.plan_sph2fourier(N)
+    PS, PA = ft.plan_sph_synthesis(N), ft.plan_sph_analysis(N)
+    st = torch.cuda.current_stream().cuda_stream
+    t = torch.from_numpy(A.ravel(order="F").copy()).cuda()
+    p = t.data_ptr()
+    ft.execute_dev(P, True, "N", p, N, M, st)
+    ft.execute_sph_grid_dev(PS, "sph_synthesis", "N", p, N, M, st)
+    ft.execute_sph_grid_dev(PA, "sph_analysis", "N", p, N, M, st)
+    ft.execute_dev(P, False, "N", p, N, M, st)
+    ft.execute_dev(P, True, "T", p, N, M, st)
+    ft.execute_sph_grid_dev(PA, "sph_synthesis", "T", p, N, M, st)
+    ft.execute_sph_grid_dev(PS, "sph_analysis", "T", p, N, M, st)
+    ft.execute_dev(P, False, "T", p, N, M, st)
+    torch.cuda.synchronize()
+    B = t.cpu().numpy().reshape((N, M), order="F")
+    assert rel2(B, A) <= 4 * np.sqrt(N) * EPS
+    assert np.abs(B - A).max() / np.abs(A).max() <= 2 * N * EPS
+    for Q in (P, PS, PA):
+        Q.close()
+
+
+def test_known_harmonics_on_gpu(env):
+    """sph2fourier + synthesis of a unit coefficient: the real orthonormal harmonic
+    at theta_i = (i + 1/2) pi / N, phi_k = 2 pi k / M."""
+    ft, torch = env
+    from oracle import grid as G
+    N, M = 48, 95
+    P = ft.plan_sph2fourier(N)
+    PS = ft.plan_sph_synthesis(N)
+    th, ph = G.grid(N, M)
+    c1 = np.sqrt(3 / (4 * np.pi))
+    st = torch.cuda.current_stream().cuda_stream
+    for row, col, want in [(0, 0, np.full((N, M), 0.5 / np.sqrt(np.pi))),
+                           (1, 0, np.outer(c1 * np.cos(th), np.ones(M))),
+                           (0, 1, np.outer(c1 * np.sin(th), np.sin(ph))),
+                           (0, 2, np.outer(c1 * np.sin(th), np.cos(ph)))]:
+        A = np.zeros((N, M))
+        A[row, col] = 1.0
+        t = torch.from_numpy(A.ravel(order="F").copy()).cuda()
+        ft.execute_dev(P, True, "N", t.data_ptr(), N, M, st)
+        ft.execute_sph_grid_dev(PS, "sph_synthesis", "N", t.data_ptr(), N, M, st)
+        torch.cuda.synchronize()
+        got = t.cpu().numpy().reshape((N, M), order="F")
+        assert np.abs(got - want).max() < 1e-14, (row, col)
+    P.close()
+    PS.close()
+
+
+def test_host_entry_points(env):
+    ft, torch = env
+    N, M = 20, 39
+    X = np.random.default_rng(4).uniform(-1, 1, (N, M))
+    for op in OPS:
+        P = getattr(ft, "plan_" + op)(N, M)
+        for tr in "NT":
+            H = np.asfortranarray(X.copy())
+            getattr(ft, "execute_" + op)(tr, P, H)
+            assert np.array_equal(H, run_dev(ft, torch, P, op, tr, X)), (op, tr)
+        P.close()
+
+
+def test_even_m_rejected(env):
+    ft, torch = env
+    with pytest.raises(ft.FTB200Error):
+        ft.plan_sph_synthesis(8, 16)

@@ -1,0 +1,96 @@
+"""Pins the sphere grid oracle (oracle/grid.py, a restatement of src/fftw.c:63-277;
+FFTW is not available here).  CPU only.
+
+1. The one-dimensional transforms equal FFTW's published definitions (explicit
+   sums) for every kind the plans use.
+2. The reference's own accuracy test (test/test_fftw.c:43-73): the compiled
+   reference's sph2fourier, the oracle's synthesis and analysis, the compiled
+   reference's fourier2sph, in 'N' then 'T' (with the plans crossed, as there),
+   return the input within 4 sqrt(N) eps (2-norm) and 2N eps (max norm).
+3. Known harmonics: the reference's sph2fourier of a unit coefficient followed
+   by the oracle's synthesis gives the real orthonormal spherical harmonic on the
+   grid (Y_0^0, Y_1^0, and order 1 in columns 1 (sin phi) and 2 (cos phi))."""
+import numpy as np
+import pytest
+
+from conftest import EPS
+from oracle import grid as G
+
+
+def explicit(x, kind):
+    N = x.shape[0]
+    k = np.arange(N)[:, None]
+    j = np.arange(N)[None, :]
+    if kind == G.REDFT10:
+        A = 2 * np.cos(np.pi * (j + 0.5) * k / N)
+    elif kind == G.REDFT01:
+        A = 2 * np.cos(np.pi * j * (k + 0.5) / N)
+        A[:, 0] = 1.0
+    elif kind == G.RODFT10:
+        A = 2 * np.sin(np.pi * (j + 0.5) * (k + 1) / N)
+    else:
+        A = 2 * np.sin(np.pi * (j + 1) * (k + 0.5) / N)
+        A[:, N - 1] = (-1.0) ** np.arange(N)
+    return A @ x
+
+
+@pytest.mark.parametrize("N", [1, 2, 5, 8, 13])
+@pytest.mark.parametrize("kind", [G.REDFT10, G.REDFT01, G.RODFT10, G.RODFT01])
+def test_kinds_are_fftws_definitions(N, kind):
+    x = np.random.default_rng(N).standard_normal((N, 3))
+    assert np.allclose(G.r2r(x, kind), explicit(x, kind), rtol=1e-13, atol=1e-13)
+
+
+def test_phi_transforms_are_unnormalised_dfts():
+    M = 9
+    x = np.random.default_rng(3).standard_normal((2, M))
+    Y = G.r2c(x)
+    k = np.arange(M)
+    for j in range(M // 2 + 1):
+        assert np.allclose(Y[:, j], x @ np.exp(-2j * np.pi * j * k / M))
+    back = G.c2r(Y, M)
+    assert np.allclose(back, M * x)
+
+
+@pytest.fixture(scope="module")
+def ref():
+    from oracle.bind import Reference
+    return Reference()
+
+
+@pytest.mark.parametrize("N", [64, 128])
+def test_reference_round_trip(ref, N):
+    from fasttransforms_b200.utilities import rand_layout
+    A = rand_layout("sph", N, 5)
+    P = ref.plan("sph", N)
+    X = A.copy(order="F")
+    ref.execute("sph", P, True, "N", X)
+    X = G.execute("sph_synthesis", "N", "sph_synthesis", X)
+    X = np.asfortranarray(G.execute("sph_analysis", "N", "sph_analysis", X))
+    ref.execute("sph", P, False, "N", X)
+    ref.execute("sph", P, True, "T", X)
+    X = G.execute("sph_synthesis", "T", "sph_analysis", X)
+    X = np.asfortranarray(G.execute("sph_analysis", "T", "sph_synthesis", X))
+    ref.execute("sph", P, False, "T", X)
+    ref.destroy(P)
+    assert np.linalg.norm(X - A) / np.linalg.norm(A) <= 4 * np.sqrt(N) * EPS
+    assert np.abs(X - A).max() / np.abs(A).max() <= 2 * N * EPS
+
+
+def test_known_harmonics(ref):
+    N = 32
+    M = 2 * N - 1
+    P = ref.plan("sph", N)
+    th, ph = G.grid(N, M)
+    c1 = np.sqrt(3 / (4 * np.pi))
+    cases = [(0, 0, np.full((N, M), 0.5 / np.sqrt(np.pi))),
+             (1, 0, np.outer(c1 * np.cos(th), np.ones(M))),
+             (0, 1, np.outer(c1 * np.sin(th), np.sin(ph))),
+             (0, 2, np.outer(c1 * np.sin(th), np.cos(ph)))]
+    for row, col, want in cases:
+        A = np.zeros((N, M), order="F")
+        A[row, col] = 1.0
+        ref.execute("sph", P, True, "N", A)
+        got = G.execute("sph_synthesis", "N", "sph_synthesis", A)
+        assert np.abs(got - want).max() < 1e-14, (row, col)
+    ref.destroy(P)
