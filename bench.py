@@ -586,6 +586,38 @@ def extra_workloads(args, torch, ft):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / steps
 
+    # the full spherical-harmonic transform on the device: sph2fourier + grid synthesis, then
+    # grid analysis + fourier2sph (plain FP64), one field of degree n - 1
+    n = args.n
+    M = 2 * n - 1
+    Pn, PS, PA = ft.plan_sph2fourier(n), ft.plan_sph_synthesis(n), ft.plan_sph_analysis(n)
+    A = ft.sphrand(n, SEED)
+    d = torch.from_numpy(A.ravel(order="F").copy()).cuda()
+    dp = d.data_ptr()
+
+    def sht():
+        ft.execute_dev(Pn, True, "N", dp, n, M, sp)
+        ft.execute_sph_grid_dev(PS, "sph_synthesis", "N", dp, n, M, sp)
+        ft.execute_sph_grid_dev(PA, "sph_analysis", "N", dp, n, M, sp)
+        ft.execute_dev(Pn, False, "N", dp, n, M, sp)
+
+    def grid_only():
+        ft.execute_sph_grid_dev(PS, "sph_synthesis", "N", dp, n, M, sp)
+        ft.execute_sph_grid_dev(PA, "sph_analysis", "N", dp, n, M, sp)
+    sht()
+    back = d.cpu().numpy().reshape((n, M), order="F")
+    rt = float(np.linalg.norm(back - A) / np.linalg.norm(A))
+    for _ in range(max(1, args.warmup)):
+        sht()
+    ms = timed(sht, max(3, args.steps // 4))
+    ms_grid = timed(grid_only, max(3, args.steps // 4))
+    out["sht_full_n%d" % n] = {"coeffs_per_s": n * n / (ms * 1e-3), "ms_per_step": ms,
+                              "grid_synthesis_plus_analysis_ms": ms_grid, "roundtrip_eps2": rt,
+                              "workload": f"sph2fourier + synthesis, analysis + fourier2sph, degree {n - 1}, 1 field, "
+                                          f"{n} x {M} grid (plain FP64, cuFFT DFTs inside the grid stage)"}
+    del d
+    for q in (Pn, PS, PA):
+        q.close()
     # 64 FP64 sph fields, degrees drawn from {127, 255, 511, 1023, 2047}, one launch per stage,
     # fwd+bwd captured in one CUDA graph
     rng = np.random.default_rng(SEED)
