@@ -47,3 +47,28 @@ def trirand(n: int, seed: int) -> np.ndarray:
 
 def diskrand(n: int, seed: int) -> np.ndarray:
     return rand_layout("disk", n, seed)
+
+
+def _u_pm1(seed: int, idx: np.ndarray) -> np.ndarray:
+    """2u - 1, u from splitmix64 at counter idx (see the module docstring)."""
+    idx = idx.astype(np.uint64)
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed) + (idx + np.uint64(1)) * np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return 2.0 * ((z >> np.uint64(11)).astype(np.float64) * 2.0 ** -53) - 1.0
+
+
+def spinsphrand(n: int, s: int, seed: int, m: int = None) -> np.ndarray:
+    """n x M complex128 matrix, Fortran order, in the spin layout of the reference's
+    spinsphrand (src/ftutilities.c:159-167): rows i < n - |s|, columns j < M - 2i, real and
+    imaginary parts U(-1, 1) from the counter at the interleaved double index."""
+    M = 2 * n - 1 if m is None else m
+    i = np.arange(n, dtype=np.int64)[:, None]
+    j = np.arange(M, dtype=np.int64)[None, :]
+    on = (i < n - abs(s)) & (j < M - 2 * i)
+    e = i + j * n
+    re = np.where(on, _u_pm1(seed, 2 * e), 0.0)
+    im = np.where(on, _u_pm1(seed, 2 * e + 1), 0.0)
+    return np.asfortranarray(re + 1j * im)

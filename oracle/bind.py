@@ -52,8 +52,21 @@ def fill(kind: str, n: int, seed: int) -> np.ndarray:
     return np.asfortranarray(A)
 
 
+def fill_spin(n: int, M: int, s: int, seed: int) -> np.ndarray:
+    """Seeded complex fill in spinsphrand's layout (src/ftutilities.c:159-167); identical to
+    ``oracle_fill_spin`` in ft_oracle.c and ``fasttransforms_b200.utilities.spinsphrand``."""
+    from fasttransforms_b200.utilities import spinsphrand
+    return spinsphrand(n, s, seed, M)
+
+
 def _ptr(a: np.ndarray):
     assert a.dtype == np.float64 and a.flags.f_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _cptr(a: np.ndarray):
+    """complex128 Fortran-order array as interleaved doubles (the ft_complex layout)."""
+    assert a.dtype == np.complex128 and a.flags.f_contiguous
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
@@ -101,8 +114,40 @@ class Oracle:
         self._libc = C.CDLL(None)
         self._libc.free.argtypes = [C.c_void_p]
 
+        sp = C.c_void_p
+        L.oracle_plan_spinsph2fourier.restype = sp
+        L.oracle_plan_spinsph2fourier.argtypes = [C.c_int, C.c_int, C.c_int]
+        L.oracle_destroy_spin_plan.argtypes = [sp]
+        L.oracle_execute_spin.argtypes = [sp, C.c_int, C.c_char, dp, C.c_int, C.c_int]
+        for f in ("oracle_execute_spinsph_hi2lo", "oracle_execute_spinsph_lo2hi"):
+            getattr(L, f).argtypes = [sp, dp, C.c_int]
+        L.oracle_fill_spin.argtypes = [C.c_int, C.c_int, C.c_int, C.c_ulonglong, dp]
+
     def set_fused(self, fused: bool):
         self.lib.oracle_set_fused(1 if fused else 0)
+
+    # spin-weighted spherical harmonics: complex128 N x M arrays in Fortran order (the
+    # interleaved (re, im) layout of ft_complex)
+    def spin_plan(self, n: int, s: int, connections: bool = True):
+        return self.lib.oracle_plan_spinsph2fourier(n, s, 1 if connections else 0)
+
+    def spin_destroy(self, P):
+        self.lib.oracle_destroy_spin_plan(P)
+
+    def spin_execute(self, P, forward: bool, trans: str, A: np.ndarray):
+        N, M = A.shape
+        self.lib.oracle_execute_spin(P, 1 if forward else 0, trans.encode(), _cptr(A), N, M)
+
+    def spin_hi2lo(self, P, A: np.ndarray):
+        self.lib.oracle_execute_spinsph_hi2lo(P, _cptr(A), A.shape[1])
+
+    def spin_lo2hi(self, P, A: np.ndarray):
+        self.lib.oracle_execute_spinsph_lo2hi(P, _cptr(A), A.shape[1])
+
+    def spin_fill(self, n: int, M: int, s: int, seed: int) -> np.ndarray:
+        A = np.zeros((n, M), dtype=complex, order="F")
+        self.lib.oracle_fill_spin(n, M, s, seed, _cptr(A))
+        return A
 
     def plan(self, kind: str, n: int, alpha=0.0, beta=0.0, gamma=0.0, rotations_only=False):
         L = self.lib
@@ -195,6 +240,37 @@ class Reference:
         for f in list(self._FWD.values()) + list(self._BWD.values()):
             getattr(L, f).argtypes = [C.c_char, HP, C.POINTER(C.c_double), C.c_int, C.c_int]
         L.ft_set_num_threads.argtypes = [C.c_int]
+        sp, dp = C.c_void_p, C.POINTER(C.c_double)
+        L.ft_plan_spinsph2fourier.restype = sp
+        L.ft_plan_spinsph2fourier.argtypes = [C.c_int, C.c_int]
+        L.ft_destroy_spin_harmonic_plan.argtypes = [sp]
+        for f in ("ft_execute_spinsph2fourier", "ft_execute_fourier2spinsph"):
+            getattr(L, f).argtypes = [C.c_char, sp, dp, C.c_int, C.c_int]
+        L.ft_plan_rotspinsphere.restype = sp
+        L.ft_plan_rotspinsphere.argtypes = [C.c_int, C.c_int]
+        L.ft_destroy_spin_rotation_plan.argtypes = [sp]
+        for f in ("ft_execute_spinsph_hi2lo", "ft_execute_spinsph_lo2hi"):
+            getattr(L, f).argtypes = [sp, dp, dp, C.c_int]
+
+    # spin-weighted spherical harmonics (complex128 Fortran arrays)
+    def spin_plan(self, n: int, s: int):
+        return self.lib.ft_plan_spinsph2fourier(n, s)
+
+    def spin_destroy(self, P):
+        self.lib.ft_destroy_spin_harmonic_plan(P)
+
+    def spin_execute(self, P, forward: bool, trans: str, A: np.ndarray):
+        N, M = A.shape
+        f = self.lib.ft_execute_spinsph2fourier if forward else self.lib.ft_execute_fourier2spinsph
+        f(trans.encode(), P, _cptr(A), N, M)
+
+    def spin_rotations(self, n: int, s: int, hi2lo: bool, A: np.ndarray):
+        """The rotation stage alone (ft_execute_spinsph_hi2lo / lo2hi, with a scratch array)."""
+        SRP = self.lib.ft_plan_rotspinsphere(n, s)
+        B = np.zeros_like(A)
+        f = self.lib.ft_execute_spinsph_hi2lo if hi2lo else self.lib.ft_execute_spinsph_lo2hi
+        f(SRP, _cptr(A), _cptr(B), A.shape[1])
+        self.lib.ft_destroy_spin_rotation_plan(SRP)
 
     def set_num_threads(self, t: int):
         self.lib.ft_set_num_threads(t)

@@ -739,3 +739,137 @@ void oracle_fill(int kind, int N, int M, unsigned long long seed, double * A) {
             A[idx] = on ? u_pm1(seed, idx) : 0.0;
         }
 }
+
+/* ---------------------------------------------------------------------------
+ * Spin-weighted spherical harmonics.  Complex matrices are interleaved (re, im)
+ * doubles, column-major N x M (ft_complex, src/fasttransforms.h:11).
+ * ------------------------------------------------------------------------- */
+
+/* src/rotations.c:445-478 (ft_plan_rotspinsphere): s1, c1 are the sph table (same
+ * expression); s2, c2 indexed (l, j, m) at l + j n + m |s| n. */
+oracle_spin_plan * oracle_plan_spinsph2fourier(int n, int s, int connections) {
+    oracle_spin_plan * P = calloc(1, sizeof(oracle_spin_plan));
+    P->n = n;
+    P->s = s;
+    P->sph = connections ? oracle_plan_sph2fourier(n) : oracle_plan_rotations(ORACLE_SPH, n, 0, 0, 0);
+    int as = abs(s);
+    P->s2 = calloc((size_t) as * n * n + 1, sizeof(double));
+    P->c2 = calloc((size_t) as * n * n + 1, sizeof(double));
+    for (int m = 0; m < n; m++)
+        for (int j = 0; j < as; j++)
+            for (int l = 0; l < n - m - j; l++) {
+                double nums = (l + 1) * (l + m + 1);
+                double numc = (2 * j + m + 1) * (2 * l + 2 * j + 2 * m + 3);
+                double den = (l + 2 * j + m + 2) * (l + 2 * j + 2 * m + 2);
+                size_t idx = (size_t) l + (size_t) j * n + (size_t) m * as * n;
+                P->s2[idx] = sqrt(nums / den);
+                P->c2[idx] = sqrt(numc / den);
+            }
+    return P;
+}
+
+void oracle_destroy_spin_plan(oracle_spin_plan * P) {
+    if (!P) return;
+    oracle_destroy_plan(P->sph);
+    free(P->s2);
+    free(P->c2);
+    free(P);
+}
+
+/* src/rotations/rotations_default.c:17-29: the real rotation on both parts */
+static inline void cgivens(double S, double C, double * X, double * Y) { givens(S, C, X, Y); givens(S, C, X + 1, Y + 1); }
+static inline void cgivens_t(double S, double C, double * X, double * Y) { givens_t(S, C, X, Y); givens_t(S, C, X + 1, Y + 1); }
+
+#define SPIN_S2(P, l, j, m) (P)->s2[(size_t) (l) + (size_t) (j) * (P)->n + (size_t) (m) * abs((P)->s) * (P)->n]
+#define SPIN_C2(P, l, j, m) (P)->c2[(size_t) (l) + (size_t) (j) * (P)->n + (size_t) (m) * abs((P)->s) * (P)->n]
+
+/* src/rotations/rotations_default.c:87-101 (kernel_spinsph_hi2lo_default); A: one complex column */
+void oracle_kernel_spinsph_hi2lo(const oracle_spin_plan * P, int m, double * A) {
+    int n = P->n, s = P->s, as = abs(s), am = abs(m), d = abs(am - as);
+    const double * s1 = P->sph->s, * c1 = P->sph->c;
+    for (int j = MIN(am, as) - 1; j >= 0; j--)
+        for (int k = n - 2 - d - j; k >= 0; k--) {
+            if (m * s >= 0) cgivens(SPIN_S2(P, k, j, d), SPIN_C2(P, k, j, d), A + 2 * k, A + 2 * (k + 1));
+            else            cgivens_t(SPIN_S2(P, k, j, d), SPIN_C2(P, k, j, d), A + 2 * k, A + 2 * (k + 1));
+        }
+    for (int j = d - 2; j >= (am + as) % 2; j -= 2)
+        for (int k = n - 3 - j; k >= 0; k--)
+            cgivens(s1[tri_idx(n, k, j)], c1[tri_idx(n, k, j)], A + 2 * k, A + 2 * (k + 2));
+}
+
+/* src/rotations/rotations_default.c:103-117 (kernel_spinsph_lo2hi_default) */
+void oracle_kernel_spinsph_lo2hi(const oracle_spin_plan * P, int m, double * A) {
+    int n = P->n, s = P->s, as = abs(s), am = abs(m), d = abs(am - as);
+    const double * s1 = P->sph->s, * c1 = P->sph->c;
+    for (int j = (am + as) % 2; j <= d - 2; j += 2)
+        for (int k = 0; k <= n - 3 - j; k++)
+            cgivens_t(s1[tri_idx(n, k, j)], c1[tri_idx(n, k, j)], A + 2 * k, A + 2 * (k + 2));
+    for (int j = 0; j < MIN(am, as); j++)
+        for (int k = 0; k <= n - 2 - d - j; k++) {
+            if (m * s >= 0) cgivens_t(SPIN_S2(P, k, j, d), SPIN_C2(P, k, j, d), A + 2 * k, A + 2 * (k + 1));
+            else            cgivens(SPIN_S2(P, k, j, d), SPIN_C2(P, k, j, d), A + 2 * k, A + 2 * (k + 1));
+        }
+}
+
+/* src/drivers.c:677-695: column 0 is order 0, columns 2m - 1 and 2m orders -m and m */
+static void execute_spin_rot(const oracle_spin_plan * P, double * A, int M, int hi2lo) {
+    int N = P->n;
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (int c = 0; c < M; c++) {
+        int m = c == 0 ? 0 : (c % 2 ? -(c + 1) / 2 : c / 2);
+        double * col = A + (size_t) 2 * N * c;
+        if (hi2lo) oracle_kernel_spinsph_hi2lo(P, m, col);
+        else       oracle_kernel_spinsph_lo2hi(P, m, col);
+    }
+}
+
+void oracle_execute_spinsph_hi2lo(const oracle_spin_plan * P, double * A, int M) { execute_spin_rot(P, A, M, 1); }
+void oracle_execute_spinsph_lo2hi(const oracle_spin_plan * P, double * A, int M) { execute_spin_rot(P, A, M, 0); }
+
+/* cblas_ztrmm with a real matrix stored as complex (src/drivers.c:1295-1361): the real
+ * triangular multiply on the real and the imaginary parts */
+static void ztrmm4(char trans, int N, int M, const double * U0, const double * U1, double * A) {
+    size_t nm = (size_t) N * M;
+    double * re = malloc(sizeof(double) * nm), * im = malloc(sizeof(double) * nm);
+    for (size_t i = 0; i < nm; i++) { re[i] = A[2 * i]; im[i] = A[2 * i + 1]; }
+    trmm4(trans, N, M, U0, U1, re);
+    trmm4(trans, N, M, U0, U1, im);
+    for (size_t i = 0; i < nm; i++) { A[2 * i] = re[i]; A[2 * i + 1] = im[i]; }
+    free(re);
+    free(im);
+}
+
+/* src/drivers.c:1295-1361 (ft_execute_spinsph2fourier / ft_execute_fourier2spinsph):
+ * classes 0, 3 take P1 and 1, 2 take P2 for even s, the other way round for odd s */
+void oracle_execute_spin(const oracle_spin_plan * P, int forward, char TRANS, double * A, int N, int M) {
+    if (TRANS != 'N' && TRANS != 'T') return;
+    int even = P->s % 2 == 0;
+    const double * U0 = even ? P->sph->P[0] : P->sph->P[1], * U1 = even ? P->sph->P[1] : P->sph->P[0];
+    const double * V0 = even ? P->sph->Pinv[0] : P->sph->Pinv[1], * V1 = even ? P->sph->Pinv[1] : P->sph->Pinv[0];
+    int tN = TRANS == 'N';
+    if (forward && tN) {
+        oracle_execute_spinsph_hi2lo(P, A, M);
+        ztrmm4('N', N, M, U0, U1, A);
+    } else if (forward) {
+        ztrmm4('T', N, M, U0, U1, A);
+        oracle_execute_spinsph_lo2hi(P, A, M);
+    } else if (tN) {
+        ztrmm4('N', N, M, V0, V1, A);
+        oracle_execute_spinsph_lo2hi(P, A, M);
+    } else {
+        oracle_execute_spinsph_hi2lo(P, A, M);
+        ztrmm4('T', N, M, V0, V1, A);
+    }
+}
+
+/* spinsphrand's layout (src/ftutilities.c:159-167): rows i < N - |s|, columns j < M - 2i,
+ * both parts U(-1,1) from the counter at the double index */
+void oracle_fill_spin(int N, int M, int s, unsigned long long seed, double * A) {
+    for (int j = 0; j < M; j++)
+        for (int i = 0; i < N; i++) {
+            size_t e = (size_t) i + (size_t) j * N;
+            int on = i < N - abs(s) && j < M - 2 * i;
+            A[2 * e] = on ? u_pm1(seed, 2 * e) : 0.0;
+            A[2 * e + 1] = on ? u_pm1(seed, 2 * e + 1) : 0.0;
+        }
+}

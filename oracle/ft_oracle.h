@@ -68,6 +68,24 @@ double * oracle_plan_chebyshev_to_legendre(int normcheb, int normleg, int n);
 double * oracle_plan_ultraspherical_to_ultraspherical(int norm1, int norm2, int n, double lambda, double mu);
 double * oracle_plan_jacobi_to_jacobi(int norm1, int norm2, int n, double alpha, double beta, double gamma, double delta);
 
+/* Spin-weighted spherical harmonics (src/rotations.c:445-485, src/drivers.c:645-791,
+ * 1259-1361).  Complex matrices: interleaved (re, im) doubles, column-major N x M. */
+typedef struct {
+    int n, s;
+    double * s2, * c2;   /* the spin sweeps' table, (l, j, m) at l + j n + m |s| n */
+    oracle_plan * sph;   /* the sph table (the spin plan's s1, c1) and connection matrices */
+} oracle_spin_plan;
+/* connections = 0: rotation tables only */
+oracle_spin_plan * oracle_plan_spinsph2fourier(int n, int s, int connections);
+void oracle_destroy_spin_plan(oracle_spin_plan * P);
+void oracle_kernel_spinsph_hi2lo(const oracle_spin_plan * P, int m, double * A);
+void oracle_kernel_spinsph_lo2hi(const oracle_spin_plan * P, int m, double * A);
+void oracle_execute_spinsph_hi2lo(const oracle_spin_plan * P, double * A, int M);
+void oracle_execute_spinsph_lo2hi(const oracle_spin_plan * P, double * A, int M);
+/* forward = 1: spinsph2fourier; 0: fourier2spinsph */
+void oracle_execute_spin(const oracle_spin_plan * P, int forward, char TRANS, double * A, int N, int M);
+void oracle_fill_spin(int N, int M, int s, unsigned long long seed, double * A);
+
 /* Seeded fills in the reference layouts (src/ftutilities.c:75-113), U(-1,1) from splitmix64. */
 void oracle_fill(int kind, int N, int M, unsigned long long seed, double * A);
 

@@ -9,9 +9,12 @@ seeded inputs and stores inputs and outputs as compressed .npz files:
     odd n, several Jacobi parameters); for sph also the vector-field transforms
     (ft_execute_sphv2fourier / ft_execute_fourier2sphv, keys "v_fwd_N" ...);
   * rotation stages alone (ft_execute_*_hi2lo / _lo2hi);
-  * the four dense connection matrices of each plan.
+  * the four dense connection matrices of each plan;
+  * spin-weighted transforms (ft_execute_spinsph2fourier / ft_execute_fourier2spinsph and
+    the rotation stages ft_execute_spinsph_hi2lo / _lo2hi) on complex inputs in
+    spinsphrand's layout, files spin_n<n>_s<s>.npz.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [sph tri disk spin]   (default: all)
 """
 from __future__ import annotations
 
@@ -23,13 +26,14 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
-from oracle.bind import Reference, _ptr, fill  # noqa: E402
+from oracle.bind import Reference, _ptr, fill, fill_spin  # noqa: E402
 
 CASES = [
     ("sph", 8, ()), ("sph", 17, ()), ("sph", 33, ()),
     ("tri", 16, (0.0, 0.0, 0.0)), ("tri", 17, (-0.5, -0.5, -0.5)), ("tri", 16, (0.5, 1.0, -0.25)),
     ("disk", 9, (0.0, 0.0)), ("disk", 16, (0.0, 0.0)), ("disk", 12, (0.5, -0.25)),
 ]
+SPIN_CASES = [(8, -2), (17, 0), (17, 1), (16, 3), (33, -1), (12, 4)]
 SEED = 20261203
 
 
@@ -51,7 +55,10 @@ def main():
         for d in ("hi2lo", "lo2hi"):
             getattr(L, f"ft_execute_{fam}_{d}").argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int]
     L.ft_destroy_rotation_plan.argtypes = [C.c_void_p]
+    families = set(sys.argv[1:]) or {"sph", "tri", "disk", "spin"}
     for kind, n, params in CASES:
+        if kind not in families:
+            continue
         A = fill(kind, n, SEED)
         P = R.plan(kind, n, *params)
         out = {"A": A, "params": np.array(params, dtype=np.float64)}
@@ -78,6 +85,25 @@ def main():
         path = os.path.join(HERE, case_name(kind, n, params) + ".npz")
         np.savez_compressed(path, **out)
         print("wrote", os.path.relpath(path), A.shape)
+    if "spin" in families:
+        for n, sw in SPIN_CASES:
+            M = 2 * n - 1
+            A = fill_spin(n, M, sw, SEED)
+            P = R.spin_plan(n, sw)
+            out = {"A": A, "s": np.array(sw)}
+            for fwd in (True, False):
+                for tr in "NT":
+                    B = A.copy(order="F")
+                    R.spin_execute(P, fwd, tr, B)
+                    out[("fwd" if fwd else "bwd") + "_" + tr] = B
+            R.spin_destroy(P)
+            for d in ("hi2lo", "lo2hi"):
+                B = A.copy(order="F")
+                R.spin_rotations(n, sw, d == "hi2lo", B)
+                out["rot_" + d] = B
+            path = os.path.join(HERE, f"spin_n{n}_s{sw}.npz".replace("-", "m"))
+            np.savez_compressed(path, **out)
+            print("wrote", os.path.relpath(path), A.shape)
 
 
 if __name__ == "__main__":
