@@ -19,7 +19,7 @@ from typing import Sequence
 
 import numpy as np
 
-from .utilities import diskrand, layout_cols, rand_layout, sphrand, trirand
+from .utilities import diskrand, layout_cols, rand_layout, sphrand, spinsphrand, trirand
 
 __all__ = [
     "FTB200Error", "HarmonicPlan", "RotationPlan", "library_path", "lib",
@@ -34,6 +34,9 @@ __all__ = [
     "SphereGridPlan", "plan_sph_synthesis", "plan_sph_analysis", "plan_sphv_synthesis", "plan_sphv_analysis",
     "execute_sph_synthesis", "execute_sph_analysis", "execute_sphv_synthesis", "execute_sphv_analysis",
     "execute_sph_grid_dev", "GRID_OPS",
+    "SpinHarmonicPlan", "SpinRotationPlan", "plan_spinsph2fourier", "plan_rotspinsphere",
+    "execute_spinsph2fourier", "execute_fourier2spinsph", "execute_spinsph_hi2lo", "execute_spinsph_lo2hi",
+    "execute_spin_dev", "spin_rotations_dev", "spinsphrand",
     "SPH", "TRI", "DISK",
 ]
 
@@ -78,6 +81,12 @@ def _load() -> C.CDLL:
         "ft_plan_sphv_synthesis": (vp, [i, i, C.c_uint]), "ft_plan_sphv_analysis": (vp, [i, i, C.c_uint]),
         "ft_destroy_sphere_fftw_plan": (None, [vp]),
         "ft_b200_execute_sph_grid_dev": (i, [vp, i, ch, vp, i, i, vp]),
+        "ft_plan_rotspinsphere": (vp, [i, i]), "ft_destroy_spin_rotation_plan": (None, [vp]),
+        "ft_execute_spinsph_hi2lo": (None, [vp, dp, dp, i]), "ft_execute_spinsph_lo2hi": (None, [vp, dp, dp, i]),
+        "ft_plan_spinsph2fourier": (vp, [i, i]), "ft_destroy_spin_harmonic_plan": (None, [vp]),
+        "ft_execute_spinsph2fourier": (None, [ch, vp, dp, i, i]), "ft_execute_fourier2spinsph": (None, [ch, vp, dp, i, i]),
+        "ft_b200_execute_spin_dev": (i, [vp, i, ch, vp, i, i, vp]),
+        "ft_b200_spin_rotations_dev": (i, [vp, i, vp, i, vp]),
     }
     for name in ("sph_synthesis", "sph_analysis", "sphv_synthesis", "sphv_analysis"):
         sig["ft_execute_" + name] = (None, [ch, vp, dp, i, i])
@@ -225,6 +234,91 @@ GRID_OPS = {"sph_synthesis": 0, "sph_analysis": 1, "sphv_synthesis": 2, "sphv_an
 def execute_sph_grid_dev(P: SphereGridPlan, op: str, trans: str, ptr: int, N: int, M: int, stream: int = 0) -> None:
     """Grid synthesis / analysis (op: a key of GRID_OPS) on a device matrix, asynchronous."""
     st = lib.ft_b200_execute_sph_grid_dev(P.ptr, GRID_OPS[op], trans.encode(), C.c_void_p(ptr), N, M, C.c_void_p(stream))
+    if st != 0:
+        _check()
+
+
+class SpinRotationPlan(HarmonicPlan):
+    """Owns an ``ft_spin_rotation_plan *`` (reference: src/rotations.c:431-478)."""
+
+    def __init__(self, ptr: int, n: int, s: int):
+        super().__init__(ptr, "spin", n)
+        self.s = s
+
+    def close(self):
+        if self.ptr:
+            lib.ft_destroy_spin_rotation_plan(self.ptr)
+            self.ptr = None
+
+
+class SpinHarmonicPlan(SpinRotationPlan):
+    """Owns an ``ft_spin_harmonic_plan *`` (reference: src/drivers.c:1259-1361)."""
+
+    def close(self):
+        if self.ptr:
+            lib.ft_destroy_spin_harmonic_plan(self.ptr)
+            self.ptr = None
+
+
+def plan_rotspinsphere(n: int, s: int) -> SpinRotationPlan:
+    p = lib.ft_plan_rotspinsphere(n, s)
+    if not p:
+        _check()
+        raise FTB200Error(-1, "plan creation failed")
+    return SpinRotationPlan(p, n, s)
+
+
+def plan_spinsph2fourier(n: int, s: int) -> SpinHarmonicPlan:
+    p = lib.ft_plan_spinsph2fourier(n, s)
+    if not p:
+        _check()
+        raise FTB200Error(-1, "plan creation failed")
+    return SpinHarmonicPlan(p, n, s)
+
+
+def _complex_matrix(A: np.ndarray) -> np.ndarray:
+    if not (isinstance(A, np.ndarray) and A.dtype == np.complex128 and A.ndim == 2 and A.flags.f_contiguous and A.flags.writeable):
+        raise TypeError("A must be a writeable 2-D complex128 numpy array in Fortran order")
+    return A
+
+
+def _exec_spin(fname: str, trans: str, P: SpinHarmonicPlan, A: np.ndarray, N=None, M=None):
+    A = _complex_matrix(A)
+    N = A.shape[0] if N is None else N
+    M = A.shape[1] if M is None else M
+    if N * M > A.size:
+        raise ValueError("N x M exceeds the array")
+    getattr(lib, fname)(trans.encode(), P.ptr, A.ctypes.data_as(C.POINTER(C.c_double)), N, M)
+    _check()
+
+
+def execute_spinsph2fourier(trans, P, A, N=None, M=None): _exec_spin("ft_execute_spinsph2fourier", trans, P, A, N, M)
+def execute_fourier2spinsph(trans, P, A, N=None, M=None): _exec_spin("ft_execute_fourier2spinsph", trans, P, A, N, M)
+
+
+def _exec_spin_rot(fname, SRP, A, M=None):
+    A = _complex_matrix(A)
+    M = A.shape[1] if M is None else M
+    if A.shape[0] != SRP.n or M > A.shape[1]:
+        raise ValueError("A must have the plan's n rows and at least M columns")
+    getattr(lib, fname)(SRP.ptr, A.ctypes.data_as(C.POINTER(C.c_double)), None, M)
+    _check()
+
+
+def execute_spinsph_hi2lo(SRP, A, M=None): _exec_spin_rot("ft_execute_spinsph_hi2lo", SRP, A, M)
+def execute_spinsph_lo2hi(SRP, A, M=None): _exec_spin_rot("ft_execute_spinsph_lo2hi", SRP, A, M)
+
+
+def execute_spin_dev(P: SpinHarmonicPlan, forward: bool, trans: str, ptr: int, N: int, M: int, stream: int = 0) -> None:
+    """Spin-weighted transform on a device matrix of N x M interleaved complex doubles."""
+    st = lib.ft_b200_execute_spin_dev(P.ptr, 1 if forward else 0, trans.encode(), C.c_void_p(ptr), N, M, C.c_void_p(stream))
+    if st != 0:
+        _check()
+
+
+def spin_rotations_dev(SRP: SpinRotationPlan, hi2lo: bool, ptr: int, M: int, stream: int = 0) -> None:
+    """The spin rotation stage alone on a device matrix (interleaved complex)."""
+    st = lib.ft_b200_spin_rotations_dev(SRP.ptr, 1 if hi2lo else 0, C.c_void_p(ptr), M, C.c_void_p(stream))
     if st != 0:
         _check()
 

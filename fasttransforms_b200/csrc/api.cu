@@ -772,6 +772,14 @@ bool same_tri_flags(HarmonicPlan * const * H, int nf) {
 }
 
 }  // namespace
+
+// The four stride-4 column classes of sph and disk, exported for the spin-weighted
+// transforms (spin.cu), which apply them to the real and the imaginary parts.
+bool connection_multiply(HarmonicPlan * H, bool inverse, bool trans, const double * in, double * out, int M,
+                         cudaStream_t st, bool swap) {
+    return trmm4(H, inverse, trans, in, out, M, st, swap);
+}
+
 }  // namespace ftb
 
 using namespace ftb;

@@ -15,7 +15,9 @@
 
 namespace ftb {
 
-enum Kind { SPH = 0, TRI = 1, DISK = 2 };
+// SPIN: stage two of the spin-weighted sweeps (sph sweeps of order |m - |s|| on interleaved
+// complex columns, both columns of an order in one lane; spin.cu).
+enum Kind { SPH = 0, TRI = 1, DISK = 2, SPIN = 3 };
 
 // ---------------------------------------------------------------------------
 // Rotation geometry.
@@ -38,16 +40,17 @@ enum Kind { SPH = 0, TRI = 1, DISK = 2 };
 // ---------------------------------------------------------------------------
 struct Geo {
     __host__ __device__ static inline int floordiv2(int x) { return x >= 0 ? x / 2 : -((1 - x) / 2); }
-    __host__ __device__ static inline int chains(int kind) { return kind == SPH ? 2 : 1; }
+    __host__ __device__ static inline bool sphlike(int kind) { return kind == SPH || kind == SPIN; }
+    __host__ __device__ static inline int chains(int kind) { return sphlike(kind) ? 2 : 1; }
     __host__ __device__ static inline int step(int kind) { return kind == TRI ? 1 : 2; }
     __host__ __device__ static inline int top(int kind, int N, int j, int c) {
-        if (kind == SPH) return floordiv2(N - 3 - j - c);
+        if (sphlike(kind)) return floordiv2(N - 3 - j - c);
         if (kind == TRI) return N - 2 - j;
         return N - 2 - (j + 1) / 2;
     }
     // number of positions of chain c in a column of N rows
     __host__ __device__ static inline int chain_len(int kind, int N, int c) {
-        return kind == SPH ? (N - c + 1) / 2 : N;
+        return sphlike(kind) ? (N - c + 1) / 2 : N;
     }
     // packed table offset of column j (entry l of sweep j is at offset + l)
     __host__ __device__ static inline long long table_base(int kind, int N, int j) {
@@ -59,18 +62,28 @@ struct Geo {
     }
     // number of order columns the rotation stage visits for an N x M matrix
     // sph / disk: pairs (2m-1, 2m), m = 2 .. M/2; tri: column m, m = 1 .. M-1
-    __host__ __device__ static inline int first_order(int kind) { return kind == TRI ? 1 : 2; }
+    __host__ __device__ static inline int first_order(int kind) { return kind == TRI ? 1 : (kind == SPIN ? 0 : 2); }
     // orders per rotation task: one lane per (order, chain) of a 32-lane warp
-    __host__ __device__ static inline int task_orders(int kind) { return kind == SPH ? 16 : 32; }
+    __host__ __device__ static inline int task_orders(int kind) { return sphlike(kind) ? 16 : 32; }
     __host__ __device__ static inline int last_order(int kind, int M) { return kind == TRI ? M - 1 : M / 2; }
     // Sweeps of the rotation task of lowest order mbase: every sweep j = jlo, jlo + step, ..,
     // jhi applies to at least one of its columns (order m runs j = jpar .. m - step; with
     // blk > 0 only its sweeps above its last whole block of blk sweeps).  Returns their number
     // (0: nothing to do).  The kernel and the host's pass schedule both use this.
-    __host__ __device__ static inline int task_sweeps(int kind, int M, int mbase, int blk, int * jlo_out, int * jhi_out) {
+    // SPIN: order m runs the sph sweeps of order |m - spin|, j = (m + spin) mod 2 .. |m - spin| - 2.
+    __host__ __device__ static inline int task_sweeps(int kind, int M, int mbase, int blk, int * jlo_out, int * jhi_out,
+                                                      int spin = 0) {
         const int st = step(kind), ord = task_orders(kind), mlast = last_order(kind, M);
         int omax = mbase + st * (ord - 1);
         if (omax > mlast) omax = mbase + st * ((mlast - mbase) / st);
+        if (kind == SPIN) {
+            int emax = 0;   // largest effective order of the task
+            for (int m = mbase; m <= omax; m += st) emax = (m - spin > emax) ? m - spin : (spin - m > emax ? spin - m : emax);
+            const int jlo = (mbase + spin) & 1, jhi = emax - st;
+            *jlo_out = jlo;
+            *jhi_out = jhi;
+            return jhi < jlo ? 0 : (jhi - jlo) / st + 1;
+        }
         const int jpar = kind == TRI ? 0 : (mbase & 1);
         int jlo = jpar;
         if (blk > 0) {
@@ -107,6 +120,7 @@ struct RotField {
     long long lda;
     int blk;                // 0: all sweeps; > 0: only each column's sweeps above the last
                             // whole block of blk sweeps (the rest run as blocked products)
+    int spin;               // SPIN: |s|
 };
 
 // Kernel launchers (rotations.cu).  The field table travels by value in the
@@ -215,6 +229,10 @@ struct HarmonicPlan {
     void * blocked;             // tile matrices of the blocked sweeps (built on first use)
     void * mixed_trmm;          // sliced images of the connection matrices (built on first use)
 };
+// Out = op(U) In over the four stride-4 column classes (U[0] on 0 and 3, U[1] on 1 and 2; swapped
+// with swap), U = the plan's P or Pinv (api.cu)
+bool connection_multiply(HarmonicPlan * H, bool inverse, bool trans, const double * in, double * out, int M,
+                         cudaStream_t st, bool swap);
 // NULL unless P is a live plan of this library (api.cu)
 HarmonicPlan * as_plan(const ft_harmonic_plan * P);
 // device task list already built for (RP, M), without building one (api.cu)

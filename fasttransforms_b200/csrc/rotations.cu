@@ -47,9 +47,12 @@ namespace {
 
 template <int KIND>
 struct KT {
-    static constexpr int CH = KIND == SPH ? 2 : 1;        // chains per column
+    static constexpr int CH = (KIND == SPH || KIND == SPIN) ? 2 : 1;   // chains per column
     static constexpr int STEP = KIND == TRI ? 1 : 2;      // order step between sweeps
-    static constexpr int NCOL = KIND == TRI ? 1 : 2;      // columns per order (cos, sin)
+    // sequences per order sharing the rotations: cos, sin columns (sph, disk), the column
+    // (tri), or the real and imaginary parts of the columns of -m and m (spin)
+    static constexpr int NCOL = KIND == TRI ? 1 : (KIND == SPIN ? 4 : 2);
+    static constexpr int ES = KIND == SPIN ? 2 : 1;       // doubles per element (interleaved complex)
     static constexpr int ORD = 32 / CH;                   // orders per task (one lane per order and chain)
     static constexpr int COLS = ORD * NCOL;               // columns per task
     static constexpr int CPAD = COLS + 1;                 // padded column dimension of the stage buffers
@@ -109,13 +112,15 @@ __device__ __forceinline__ void wait_progress(const int * p, int need) {
 
 // Lane layout: lane = o * CH + c owns chain c of the NCOL columns of order
 // mbase + STEP * o (sph: cos and sin columns 2m-1, 2m; disk: the same pair;
-// tri: column m).  The NCOL columns of a lane share every (sin, cos) pair, so
-// one shared-memory load feeds NCOL rotations.
+// tri: column m; spin: the real and imaginary parts of the complex columns of
+// orders -m and m, which share the sph sweeps of order |m - s|).  The NCOL columns
+// of a lane share every (sin, cos) pair, so one shared-memory load feeds NCOL
+// rotations.
 template <int KIND, bool HI2LO, int W, int B, int E>
 __global__ void __launch_bounds__(W * 32, W <= 4 ? 2 : 1)
 rot_kernel(const __grid_constant__ RotLaunch L) {
     using T = KT<KIND>;
-    constexpr int CH = T::CH, STEP = T::STEP, NCOL = T::NCOL, ORD = T::ORD, COLS = T::COLS, CPAD = T::CPAD;
+    constexpr int CH = T::CH, STEP = T::STEP, NCOL = T::NCOL, ORD = T::ORD, COLS = T::COLS, CPAD = T::CPAD, ES = T::ES;
     constexpr int WB = W * B;
     static_assert(E % (2 * B) == 0, "chunk must be a multiple of the window");
     static_assert((B * E * CH) % 32 == 0, "a chunk's (sin, cos) entries must split evenly over the lanes");
@@ -150,14 +155,15 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
         const long long lda = F.lda;
         const int mlast = Geo::last_order(KIND, F.M);
         const int mbase = task.mbase;
-        const int jpar = KIND == TRI ? 0 : (mbase & 1);   // lowest sweep of every column
+        // lowest sweep of every column (spin: the parity of the effective orders |m - s|)
+        const int jpar = KIND == TRI ? 0 : (KIND == SPIN ? ((mbase + F.spin) & 1) : (mbase & 1));
         // With F.blk > 0 a column of order m runs only its sweeps j >= jcut(m): the
         // (m - jpar)/STEP mod blk sweeps above its last whole block of blk sweeps.
         auto jcut = [&](int m) -> int {
             return F.blk > 0 ? m - STEP * (((m - jpar) / STEP) % F.blk) : jpar;
         };
         int jlo, jhi;
-        const int nsw = Geo::task_sweeps(KIND, F.M, mbase, F.blk, &jlo, &jhi);
+        const int nsw = Geo::task_sweeps(KIND, F.M, mbase, F.blk, &jlo, &jhi, F.spin);
         if (nsw == 0) continue;   // nothing to do for this task (uniform)
         const int npass = (nsw + WB - 1) / WB;
         const int rbeg = pipe ? unit.pass : 0, rend = pipe ? unit.pass + 1 : npass;
@@ -167,6 +173,17 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
         }
         const int m_lane = mbase + STEP * o_lane;
         const int jcut_lane = jcut(m_lane);
+        // the order whose sweeps a lane runs: its own, or |m - s| for spin; emin: the least
+        // over the task's orders (every sweep below emin - STEP applies to all lanes)
+        const int me_lane = KIND == SPIN ? abs(m_lane - F.spin) : m_lane;
+        int emin = mbase;
+        if (KIND == SPIN) {
+            emin = abs(mbase - F.spin);
+            for (int o = 1; o < ORD; ++o) {
+                const int m = mbase + STEP * o;
+                if (m <= mlast) emin = min(emin, abs(m - F.spin));
+            }
+        }
         int jlo_all_max = jpar;   // highest first sweep over the task's columns
         if (F.blk > 0)
             for (int o = 0; o < ORD; ++o) {
@@ -229,13 +246,13 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
             const int jmax = HI2LO ? jfirst - STEP * (q * B) : jfirst + STEP * (q * B + B - 1);
             const int jmin = HI2LO ? jfirst - STEP * (q * B + B - 1) : jfirst + STEP * (q * B);
             // every sweep of this stage applies to every order of the task
-            const bool full_lanes = jmax <= mbase - STEP && (F.blk == 0 || jmin >= jlo_all_max);
+            const bool full_lanes = jmax <= emin - STEP && (F.blk == 0 || jmin >= jlo_all_max);
             unsigned lane_mask = 0;                          // sweeps that apply to this lane's order
 #pragma unroll
             for (int b = 0; b < B; ++b) {
                 const int sg = q * B + b;
                 const int j = HI2LO ? jfirst - STEP * sg : jfirst + STEP * sg;
-                if (j <= m_lane - STEP && j >= jcut_lane) lane_mask |= 1u << b;
+                if (j <= me_lane - STEP && j >= jcut_lane) lane_mask |= 1u << b;
             }
 
             // Stage the (sin, cos) pairs of a chunk: entry (b, jj) is the pair sweep b
@@ -286,9 +303,18 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
                 const int cl = f / RPC, rr = f % RPC;
                 const int o = cl / NCOL, h = cl % NCOL;
                 const int mcl = mbase + STEP * o;
-                const long long colc = KIND == TRI ? mcl : 2 * mcl - 1 + h;
-                colok[v] = mcl <= mlast;
-                const long long coff = colok[v] ? colc * lda + rr : 0;
+                long long coff;
+                if constexpr (KIND == SPIN) {
+                    // h: real / imaginary part (h & 1) of the column of -m (h < 2: 2m - 1, or 0
+                    // for m = 0) or of m (2m)
+                    const long long colc = h < 2 ? (mcl == 0 ? 0 : 2 * mcl - 1) : 2 * mcl;
+                    colok[v] = mcl <= mlast && !(mcl == 0 && h >= 2) && colc < F.M;
+                    coff = colok[v] ? ES * (colc * lda + rr) + (h & 1) : 0;
+                } else {
+                    const long long colc = KIND == TRI ? mcl : 2 * mcl - 1 + h;
+                    colok[v] = mcl <= mlast;
+                    coff = colok[v] ? colc * lda + rr : 0;
+                }
                 gsrc[v] = src + coff;
                 gdst[v] = dst + coff;
                 ioff[v] = CH == 2 ? (rr >> 1) : rr;
@@ -318,7 +344,7 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
                 const int pmin = pmin_of(k, false);
 #pragma unroll
                 for (int v = 0; v < PER_W; ++v)
-                    pre[v] = (k < K && row_ok(pmin, v)) ? __ldcg(gsrc[v] + (long long) CH * pmin) : 0.0;
+                    pre[v] = (k < K && row_ok(pmin, v)) ? __ldcg(gsrc[v] + (long long) ES * CH * pmin) : 0.0;
             };
             auto stash_chunk = [&](int k) {
                 double * const b0 = buf(0, k & 1, 0, 0);
@@ -330,7 +356,7 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
                 const double * const bw = buf(WA, k & 1, 0, 0);
 #pragma unroll
                 for (int v = 0; v < PER_W; ++v)
-                    if (row_ok(pmin, v)) __stcg(gdst[v] + (long long) CH * pmin, bw[soff[v]]);
+                    if (row_ok(pmin, v)) __stcg(gdst[v] + (long long) ES * CH * pmin, bw[soff[v]]);
                 if (pipe) __threadfence();   // before the barrier after which they are published
             };
             if (pipe) {
@@ -461,14 +487,19 @@ cudaError_t launch_cfg(const RotLaunch & L, int max_ctas, cudaStream_t st) {
 //   5: W = 4,  B = 8, E = 16 (two CTAs per SM where shared memory allows: tri, disk)
 template <int KIND, bool HI2LO>
 cudaError_t launch_kind(int cfg, const RotLaunch & L, int max_ctas, cudaStream_t st) {
-    if constexpr (KIND != TRI) {
-        if (cfg == 1) return launch_cfg<KIND, HI2LO, 16, 4, 8>(L, max_ctas, st);
+    if constexpr (KIND == SPIN) {
+        (void) cfg;   // four sequences per lane: only 8 x 4 x 8 fits the stage buffers
+        return launch_cfg<KIND, HI2LO, 8, 4, 8>(L, max_ctas, st);
+    } else {
+        if constexpr (KIND != TRI) {
+            if (cfg == 1) return launch_cfg<KIND, HI2LO, 16, 4, 8>(L, max_ctas, st);
+        }
+        if (cfg == 2) return launch_cfg<KIND, HI2LO, 8, 4, 8>(L, max_ctas, st);
+        if (cfg == 3) return launch_cfg<KIND, HI2LO, 8, 4, 16>(L, max_ctas, st);
+        if (cfg == 4) return launch_cfg<KIND, HI2LO, 4, 4, 16>(L, max_ctas, st);
+        if (cfg == 5) return launch_cfg<KIND, HI2LO, 4, 8, 16>(L, max_ctas, st);
+        return launch_cfg<KIND, HI2LO, 8, 8, 16>(L, max_ctas, st);
     }
-    if (cfg == 2) return launch_cfg<KIND, HI2LO, 8, 4, 8>(L, max_ctas, st);
-    if (cfg == 3) return launch_cfg<KIND, HI2LO, 8, 4, 16>(L, max_ctas, st);
-    if (cfg == 4) return launch_cfg<KIND, HI2LO, 4, 4, 16>(L, max_ctas, st);
-    if (cfg == 5) return launch_cfg<KIND, HI2LO, 4, 8, 16>(L, max_ctas, st);
-    return launch_cfg<KIND, HI2LO, 8, 8, 16>(L, max_ctas, st);
 }
 
 int g_rot_cfg = -2;
@@ -579,6 +610,7 @@ cudaError_t launch_with(int kind, bool hi2lo, int cfg, const RotLaunch & L, int 
         case SPH:  return hi2lo ? launch_kind<SPH, true>(cfg, L, max_ctas, st) : launch_kind<SPH, false>(cfg, L, max_ctas, st);
         case TRI:  return hi2lo ? launch_kind<TRI, true>(cfg, L, max_ctas, st) : launch_kind<TRI, false>(cfg, L, max_ctas, st);
         case DISK: return hi2lo ? launch_kind<DISK, true>(cfg, L, max_ctas, st) : launch_kind<DISK, false>(cfg, L, max_ctas, st);
+        case SPIN: return hi2lo ? launch_kind<SPIN, true>(cfg, L, max_ctas, st) : launch_kind<SPIN, false>(cfg, L, max_ctas, st);
     }
     return cudaErrorInvalidValue;
 }

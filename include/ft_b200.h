@@ -132,6 +132,40 @@ void ft_execute_sphv_analysis(const char TRANS, const ft_sphere_fftw_plan * P, d
 /* the reference's flags for these planners (src/ftutilities.h:24); not used here */
 #define FT_FFTW_FLAGS 0u
 
+/* Spin-weighted spherical harmonics.  Complex matrices are interleaved (re, im)
+ * doubles, N x M column-major: column 0 holds order 0, columns 2m - 1 and 2m the
+ * orders -m and m (src/drivers.c:645-695).  M must be odd. */
+typedef double ft_complex[2];   /* src/fasttransforms.h:11 */
+/* Opaque, as in the reference's public header (src/fasttransforms.h:336). */
+typedef struct ft_spin_rotation_plan_s ft_spin_rotation_plan;
+/* replaces ft_plan_rotspinsphere, src/rotations.c:445-478 */
+ft_spin_rotation_plan * ft_plan_rotspinsphere(const int n, const int s);
+/* replaces ft_destroy_spin_rotation_plan, src/rotations.c:431-437 */
+void ft_destroy_spin_rotation_plan(ft_spin_rotation_plan * SRP);
+/* replace ft_execute_spinsph_hi2lo / lo2hi, src/drivers.c:645-675; B (the reference's
+ * scratch) is accepted and not used */
+void ft_execute_spinsph_hi2lo(const ft_spin_rotation_plan * SRP, ft_complex * A, ft_complex * B, const int M);
+void ft_execute_spinsph_lo2hi(const ft_spin_rotation_plan * SRP, ft_complex * A, ft_complex * B, const int M);
+/* Same members as the reference's (src/fasttransforms.h:441-450).  P1 .. P2inv are
+ * host copies of the connection matrices (the real sph matrices stored as complex);
+ * B is NULL. */
+typedef struct {
+    ft_spin_rotation_plan * SRP;
+    ft_complex * B;
+    ft_complex * P1;
+    ft_complex * P2;
+    ft_complex * P1inv;
+    ft_complex * P2inv;
+    int s;
+} ft_spin_harmonic_plan;
+/* replaces ft_plan_spinsph2fourier, src/drivers.c:1269-1293 */
+ft_spin_harmonic_plan * ft_plan_spinsph2fourier(const int n, const int s);
+/* replaces ft_destroy_spin_harmonic_plan, src/drivers.c:1259-1267 */
+void ft_destroy_spin_harmonic_plan(ft_spin_harmonic_plan * P);
+/* replace ft_execute_spinsph2fourier / ft_execute_fourier2spinsph, src/drivers.c:1295-1361 */
+void ft_execute_spinsph2fourier(const char TRANS, const ft_spin_harmonic_plan * P, ft_complex * A, const int N, const int M);
+void ft_execute_fourier2spinsph(const char TRANS, const ft_spin_harmonic_plan * P, ft_complex * A, const int N, const int M);
+
 /* Rotation level. */
 /* replaces ft_plan_rotsphere, src/rotations.c:116-133 */
 ft_rotation_plan * ft_plan_rotsphere(const int n);
@@ -171,6 +205,11 @@ int ft_b200_execute_sph_grid_dev(const ft_sphere_fftw_plan * P, int op, char TRA
 int ft_b200_execute_sphv_dev(const ft_harmonic_plan * P, int forward, char TRANS, double * dA, int N, int M, void * stream);
 /* Rotation stage alone (hi2lo = 1: ft_execute_*_hi2lo; 0: *_lo2hi). */
 int ft_b200_rotations_dev(const ft_rotation_plan * RP, int hi2lo, double * dA, int M, void * stream);
+/* Spin-weighted transforms on device memory: dA holds 2 N M doubles (interleaved
+ * complex); forward = 1: spinsph2fourier, 0: fourier2spinsph. */
+int ft_b200_execute_spin_dev(const ft_spin_harmonic_plan * P, int forward, char TRANS, double * dA, int N, int M, void * stream);
+/* The spin rotation stage alone (hi2lo = 1: ft_execute_spinsph_hi2lo; 0: _lo2hi). */
+int ft_b200_spin_rotations_dev(const ft_spin_rotation_plan * SRP, int hi2lo, double * dA, int M, void * stream);
 
 /* Batched drop-in: nfields fields, each with its own plan (plans may repeat,
  * degrees may differ), all in one persistent launch per stage.  dA[f] is the
