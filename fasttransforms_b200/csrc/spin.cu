@@ -45,7 +45,8 @@ struct ft_spin_rotation_plan_s {
     double * d_stage = nullptr;     // host-pointer calls
     size_t stage_elems = 0;
     cudaStream_t stream = nullptr;
-    std::mutex mu;
+    std::mutex mu;                  // host-pointer calls (staging buffer and stream)
+    std::mutex task_mu;             // the task lists (taken inside calls that hold mu)
 };
 
 namespace ftb {
@@ -213,7 +214,7 @@ SpinRotPlan * make_srp(int n, int s) {
 
 // stage-2 tasks for M columns: 16 orders of one parity each, longest first
 bool spin_tasks(SpinRotPlan * P, int M, RotTask ** d, int * nt) {
-    std::lock_guard<std::mutex> lk(P->mu);
+    std::lock_guard<std::mutex> lk(P->task_mu);
     auto it = P->tasks.find(M);
     if (it != P->tasks.end()) { *d = it->second.first; *nt = it->second.second; return true; }
     const int mlast = Geo::last_order(SPIN, M), as = std::abs(P->s);
