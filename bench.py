@@ -20,8 +20,10 @@ Arms:
              stream, end-to-end timing with the fields copied from and to pinned
              host memory inside the timed region (e2e), and the reference's CPU
              build timed on a sample of the same workload; the secondary
-             workloads (plain FP64 single field, uneven batch, every precision of
-             the shared-plan call, tri / disk) follow under "workloads".
+             workloads (plain FP64 single field, the full spherical-harmonic
+             transform with the grid stage, the spin-weighted transform, uneven
+             batch, every precision of the shared-plan call, tri / disk) follow
+             under "workloads".
   reference  the reference FastTransforms library compiled from its own sources
              (oracle/_ref/libft_ref.so, OpenMP + its AVX kernels + OpenBLAS), run
              on the host cores, one field of the workload per step.
@@ -161,9 +163,27 @@ def cpu_sample(n: int, reps: int) -> dict:
         ts.append(time.perf_counter() - t0)
     R.destroy(P)
     t = statistics.median(ts)
-    return {"value": n * n / t, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"sph n={n} (degree {n - 1}), 1 field, fwd+bwd 'N', median of {reps} after 1 warm-up, "
-                      f"OMP threads = BLAS threads = {threads}", "sec_per_step": t}
+    res = {"value": n * n / t, "unit": UNIT, "cores": threads, "kind": kind,
+           "sample": f"sph n={n} (degree {n - 1}), 1 field, fwd+bwd 'N', median of {reps} after 1 warm-up, "
+                     f"OMP threads = BLAS threads = {threads}", "sec_per_step": t}
+    if kind == "reference":
+        # the spin-weighted transform (s = 2) beside the GPU's spin workload: one timed
+        # fwd+bwd 'N' after one warm-up
+        from oracle.bind import fill_spin
+        s = 2
+        Z = fill_spin(n, 2 * n - 1, s, SEED)
+        SP = R.spin_plan(n, s)
+        R.spin_execute(SP, True, "N", Z)
+        R.spin_execute(SP, False, "N", Z)
+        t0 = time.perf_counter()
+        R.spin_execute(SP, True, "N", Z)
+        R.spin_execute(SP, False, "N", Z)
+        ts = time.perf_counter() - t0
+        R.spin_destroy(SP)
+        res["spin_s2"] = {"value": n * n / ts, "sec_per_step": ts, "cores": threads,
+                          "sample": f"spinsph2fourier + fourier2spinsph 'N', s = {s}, n={n}, 1 complex field, "
+                                    f"1 timed after 1 warm-up"}
+    return res
 
 
 def run_reference(args, rank, world):
@@ -444,6 +464,11 @@ def run_ours(args, rank, world, local_rank, dist):
             cpu = json.loads(out.stdout.strip().splitlines()[-1])
         except Exception as exc:  # the line still carries the GPU numbers
             cpu = {"value": None, "error": repr(exc)[:200]}
+        spin_cpu = cpu.pop("spin_s2", None) if isinstance(cpu, dict) else None
+        spin_key = "spin_s2_n%d" % args.n
+        if spin_cpu and isinstance(extra, dict) and spin_key in extra:
+            extra[spin_key]["reference_cpu"] = spin_cpu
+            extra[spin_key]["gpu_over_reference_cpu"] = extra[spin_key]["coeffs_per_s"] / spin_cpu["value"]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -618,6 +643,35 @@ def extra_workloads(args, torch, ft):
     del d
     for q in (Pn, PS, PA):
         q.close()
+    # spin-weighted transform (s = 2): spinsph2fourier + fourier2spinsph 'N' on one complex
+    # field of degree n - 1 (plain FP64), and its rotation stage alone (hi2lo + lo2hi)
+    s = 2
+    SP, SRP = ft.plan_spinsph2fourier(n, s), ft.plan_rotspinsphere(n, s)
+    Z = ft.spinsphrand(n, s, SEED)
+    dz = torch.from_numpy(Z.ravel(order="F").view(np.float64).copy()).cuda()
+    zp = dz.data_ptr()
+
+    def spin():
+        ft.execute_spin_dev(SP, True, "N", zp, n, M, sp)
+        ft.execute_spin_dev(SP, False, "N", zp, n, M, sp)
+
+    def spin_rot():
+        ft.spin_rotations_dev(SRP, True, zp, M, sp)
+        ft.spin_rotations_dev(SRP, False, zp, M, sp)
+    spin()
+    back = dz.cpu().numpy().view(np.complex128).reshape((n, M), order="F")
+    rt = float(np.linalg.norm(back - Z) / np.linalg.norm(Z))
+    for _ in range(max(1, args.warmup)):
+        spin()
+    ms = timed(spin, max(3, args.steps // 4))
+    ms_rot = timed(spin_rot, max(3, args.steps // 4))
+    out["spin_s2_n%d" % n] = {"coeffs_per_s": n * n / (ms * 1e-3), "ms_per_step": ms,
+                             "rotations_hi2lo_plus_lo2hi_ms": ms_rot, "roundtrip_eps2": rt,
+                             "workload": f"spinsph2fourier + fourier2spinsph 'N', s = {s}, degree {n - 1}, "
+                                         f"1 complex field {n} x {M} (plain FP64)"}
+    del dz
+    SP.close()
+    SRP.close()
     # 64 FP64 sph fields, degrees drawn from {127, 255, 511, 1023, 2047}, one launch per stage,
     # fwd+bwd captured in one CUDA graph
     rng = np.random.default_rng(SEED)
