@@ -1,7 +1,7 @@
 """Seeded fills in the reference's coefficient layouts.
 
 The reference's test utilities fill the triangular layouts with unseeded
-``rand()`` (src/ftutilities.c:75-113).  These fills use a counter-based
+``rand()`` (src/ftutilities.c:75-129).  These fills use a counter-based
 splitmix64 generator instead, so the same (kind, n, seed) gives the same
 matrix on every machine: the value at column-major linear index idx is
 2u - 1 with u the top 53 bits of mix(seed + (idx + 1) * 0x9E3779B97F4A7C15)
@@ -11,14 +11,14 @@ from __future__ import annotations
 
 import numpy as np
 
-__all__ = ["layout_cols", "sphrand", "trirand", "diskrand", "rand_layout"]
+__all__ = ["layout_cols", "sphrand", "trirand", "diskrand", "rectdiskrand", "rand_layout"]
 
-_STEP = {"sph": 2, "tri": 1, "disk": 4}
+_STEP = {"sph": 2, "tri": 1, "disk": 4, "rect": 1}
 
 
 def layout_cols(kind: str, n: int) -> int:
-    """Columns M of the layout for n rows: 2n-1 (sph), n (tri), 4n-3 (disk)."""
-    return {"sph": 2 * n - 1, "tri": n, "disk": 4 * n - 3}[kind]
+    """Columns M of the layout for n rows: 2n-1 (sph), n (tri, rect), 4n-3 (disk)."""
+    return {"sph": 2 * n - 1, "tri": n, "disk": 4 * n - 3, "rect": n}[kind]
 
 
 def rand_layout(kind: str, n: int, seed: int) -> np.ndarray:
@@ -47,6 +47,11 @@ def trirand(n: int, seed: int) -> np.ndarray:
 
 def diskrand(n: int, seed: int) -> np.ndarray:
     return rand_layout("disk", n, seed)
+
+
+def rectdiskrand(n: int, seed: int) -> np.ndarray:
+    """The Dunkl-Xu layout of src/ftutilities.c:123-129: rows i, columns j < M - i (M = n)."""
+    return rand_layout("rect", n, seed)
 
 
 def _u_pm1(seed: int, idx: np.ndarray) -> np.ndarray:

@@ -21,13 +21,13 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libft_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libft_ref.so")
 
-SPH, TRI, DISK = 0, 1, 2
-KIND = {"sph": SPH, "tri": TRI, "disk": DISK}
+SPH, TRI, DISK, RECT = 0, 1, 2, 3
+KIND = {"sph": SPH, "tri": TRI, "disk": DISK, "rect": RECT}
 
 
 def layout_cols(kind: str, n: int) -> int:
     """Number of columns M of the reference layout for degree n-1."""
-    return {"sph": 2 * n - 1, "tri": n, "disk": 4 * n - 3}[kind]
+    return {"sph": 2 * n - 1, "tri": n, "disk": 4 * n - 3, "rect": n}[kind]
 
 
 def fill(kind: str, n: int, seed: int) -> np.ndarray:
@@ -39,7 +39,7 @@ def fill(kind: str, n: int, seed: int) -> np.ndarray:
     M = layout_cols(kind, n)
     i = np.arange(n, dtype=np.int64)[:, None]
     j = np.arange(M, dtype=np.int64)[None, :]
-    step = {"sph": 2, "tri": 1, "disk": 4}[kind]
+    step = {"sph": 2, "tri": 1, "disk": 4, "rect": 1}[kind]
     on = j < M - step * i
     idx = (i + j * n).astype(np.uint64)
     with np.errstate(over="ignore"):
@@ -72,8 +72,8 @@ def _cptr(a: np.ndarray):
 
 class _OraclePlan(C.Structure):
     _fields_ = [("kind", C.c_int), ("n", C.c_int), ("s", C.POINTER(C.c_double)),
-                ("c", C.POINTER(C.c_double)), ("P", C.POINTER(C.c_double) * 2),
-                ("Pinv", C.POINTER(C.c_double) * 2), ("alpha", C.c_double),
+                ("c", C.POINTER(C.c_double)), ("P", C.POINTER(C.c_double) * 3),
+                ("Pinv", C.POINTER(C.c_double) * 3), ("alpha", C.c_double),
                 ("beta", C.c_double), ("gamma", C.c_double)]
 
 
@@ -91,6 +91,8 @@ class Oracle:
         L.oracle_plan_tri2cheb.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double]
         L.oracle_plan_disk2cxf.restype = PP
         L.oracle_plan_disk2cxf.argtypes = [C.c_int, C.c_double, C.c_double]
+        L.oracle_plan_rectdisk2cheb.restype = PP
+        L.oracle_plan_rectdisk2cheb.argtypes = [C.c_int, C.c_double]
         L.oracle_plan_rotations.restype = PP
         L.oracle_plan_rotations.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
         L.oracle_destroy_plan.argtypes = [PP]
@@ -157,6 +159,8 @@ class Oracle:
             return L.oracle_plan_sph2fourier(n)
         if kind == "tri":
             return L.oracle_plan_tri2cheb(n, alpha, beta, gamma)
+        if kind == "rect":
+            return L.oracle_plan_rectdisk2cheb(n, beta)
         return L.oracle_plan_disk2cxf(n, alpha, beta)
 
     def destroy(self, P):
@@ -195,7 +199,8 @@ class Oracle:
         p = P.contents
         n = p.n
         get = lambda q: np.ctypeslib.as_array(q, shape=(n * n,)).reshape(n, n, order="F").copy()
-        return [get(p.P[0]), get(p.P[1])], [get(p.Pinv[0]), get(p.Pinv[1])]
+        k = 3 if p.kind == RECT else 2
+        return [get(p.P[i]) for i in range(k)], [get(p.Pinv[i]) for i in range(k)]
 
     def fill(self, kind: str, n: int, seed: int) -> np.ndarray:
         M = layout_cols(kind, n)
@@ -217,9 +222,9 @@ class Reference:
     """The reference library compiled from its own sources (oracle/_ref)."""
 
     _FWD = {"sph": "ft_execute_sph2fourier", "tri": "ft_execute_tri2cheb", "disk": "ft_execute_disk2cxf",
-            "sphv": "ft_execute_sphv2fourier"}
+            "sphv": "ft_execute_sphv2fourier", "rect": "ft_execute_rectdisk2cheb"}
     _BWD = {"sph": "ft_execute_fourier2sph", "tri": "ft_execute_cheb2tri", "disk": "ft_execute_cxf2disk",
-            "sphv": "ft_execute_fourier2sphv"}
+            "sphv": "ft_execute_fourier2sphv", "rect": "ft_execute_cheb2rectdisk"}
 
     @staticmethod
     def available(path: str = REF_SO) -> bool:
@@ -236,7 +241,14 @@ class Reference:
         L.ft_plan_tri2cheb.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double]
         L.ft_plan_disk2cxf.restype = HP
         L.ft_plan_disk2cxf.argtypes = [C.c_int, C.c_double, C.c_double]
+        L.ft_plan_rectdisk2cheb.restype = HP
+        L.ft_plan_rectdisk2cheb.argtypes = [C.c_int, C.c_double]
         L.ft_destroy_harmonic_plan.argtypes = [HP]
+        L.ft_plan_rotrectdisk.restype = C.c_void_p
+        L.ft_plan_rotrectdisk.argtypes = [C.c_int, C.c_double]
+        L.ft_destroy_rotation_plan.argtypes = [C.c_void_p]
+        for f in ("ft_execute_rectdisk_hi2lo", "ft_execute_rectdisk_lo2hi"):
+            getattr(L, f).argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int]
         for f in list(self._FWD.values()) + list(self._BWD.values()):
             getattr(L, f).argtypes = [C.c_char, HP, C.POINTER(C.c_double), C.c_int, C.c_int]
         L.ft_set_num_threads.argtypes = [C.c_int]
@@ -272,6 +284,14 @@ class Reference:
         f(SRP, _cptr(A), _cptr(B), A.shape[1])
         self.lib.ft_destroy_spin_rotation_plan(SRP)
 
+    def rect_rotations(self, n: int, beta: float, hi2lo: bool, A: np.ndarray):
+        """The Dunkl-Xu rotation stage alone (ft_execute_rectdisk_hi2lo / lo2hi)."""
+        RP = self.lib.ft_plan_rotrectdisk(n, beta)
+        B = np.zeros_like(A)
+        f = self.lib.ft_execute_rectdisk_hi2lo if hi2lo else self.lib.ft_execute_rectdisk_lo2hi
+        f(RP, _ptr(A), _ptr(B), A.shape[1])
+        self.lib.ft_destroy_rotation_plan(RP)
+
     def set_num_threads(self, t: int):
         self.lib.ft_set_num_threads(t)
 
@@ -281,6 +301,8 @@ class Reference:
             return L.ft_plan_sph2fourier(n)
         if kind == "tri":
             return L.ft_plan_tri2cheb(n, alpha, beta, gamma)
+        if kind == "rect":
+            return L.ft_plan_rectdisk2cheb(n, beta)
         return L.ft_plan_disk2cxf(n, alpha, beta)
 
     def destroy(self, P):
@@ -294,4 +316,4 @@ class Reference:
     def connection(self, P, n: int):
         p = P.contents
         get = lambda q: np.ctypeslib.as_array(q, shape=(n * n,)).reshape(n, n, order="F").copy()
-        return [get(p.P[0]), get(p.P[1])], [get(p.Pinv[0]), get(p.Pinv[1])]
+        return [get(p.P[i]) for i in range(p.NP)], [get(p.Pinv[i]) for i in range(p.NP)]

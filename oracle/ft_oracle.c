@@ -66,6 +66,18 @@ static void plan_rotdisk(int n, double alpha, double beta, double * s, double * 
         }
 }
 
+/* src/rotations.c:270-287 (ft_plan_rotrectdisk): the sph packing, beta-dependent entries */
+static void plan_rotrectdisk(int n, double beta, double * s, double * c) {
+    for (int m = 0; m < n; m++)
+        for (int l = 0; l < n - m; l++) {
+            double nums = (l + 1) * (l + 2);
+            double numc = (2 * m + 2 * beta + 3) * (2 * l + 2 * m + 2 * beta + 6);
+            double den = (l + 2 * m + 2 * beta + 4) * (l + 2 * m + 2 * beta + 5);
+            s[tri_idx(n, l, m)] = sqrt(nums / den);
+            c[tri_idx(n, l, m)] = sqrt(numc / den);
+        }
+}
+
 /* ---------------------------------------------------------------------------
  * Givens rotations: src/rotations/rotations_default.c:3-15 (scalar form) and
  * src/rotations/rotations_AVX512F.c:4-15 (fused form).
@@ -97,11 +109,11 @@ static inline void givens_t(double S, double C, double * X, double * Y) {
     }
 }
 
-/* src/rotations/rotations_default.c:31-36 (sph), :45-50 (tri), :59-64 (disk) */
+/* src/rotations/rotations_default.c:31-36 (sph), :45-50 (tri), :59-64 (disk), :73-78 (rect) */
 void oracle_kernel_hi2lo(const oracle_plan * P, int m1, int m2, double * A, int S) {
     int n = P->n;
     const double * s = P->s, * c = P->c;
-    if (P->kind == ORACLE_SPH) {
+    if (P->kind == ORACLE_SPH || P->kind == ORACLE_RECT) {
         for (int j = m2 - 2; j >= m1; j -= 2)
             for (int k = n - 3 - j; k >= 0; k--)
                 givens(s[tri_idx(n, k, j)], c[tri_idx(n, k, j)], A + k * S, A + (k + 2) * S);
@@ -116,11 +128,11 @@ void oracle_kernel_hi2lo(const oracle_plan * P, int m1, int m2, double * A, int 
     }
 }
 
-/* src/rotations/rotations_default.c:38-43 (sph), :52-57 (tri), :66-71 (disk) */
+/* src/rotations/rotations_default.c:38-43 (sph), :52-57 (tri), :66-71 (disk), :80-85 (rect) */
 void oracle_kernel_lo2hi(const oracle_plan * P, int m1, int m2, double * A, int S) {
     int n = P->n;
     const double * s = P->s, * c = P->c;
-    if (P->kind == ORACLE_SPH) {
+    if (P->kind == ORACLE_SPH || P->kind == ORACLE_RECT) {
         for (int j = m1; j < m2; j += 2)
             for (int k = 0; k <= n - 3 - j; k++)
                 givens_t(s[tri_idx(n, k, j)], c[tri_idx(n, k, j)], A + k * S, A + (k + 2) * S);
@@ -139,6 +151,14 @@ void oracle_kernel_lo2hi(const oracle_plan * P, int m1, int m2, double * A, int 
  * Column pair (2m-1, 2m) carries order m for sph and disk; column m carries order m for tri. */
 static void execute_rot(const oracle_plan * P, double * A, int M, int hi2lo) {
     int N = P->n;
+    if (P->kind == ORACLE_RECT) {   /* src/drivers.c:496-508: order m on column m, m = 2 .. M-1 */
+        #pragma omp parallel for schedule(dynamic, 1)
+        for (int m = 2; m < M; m++) {
+            if (hi2lo) oracle_kernel_hi2lo(P, m % 2, m, A + (size_t) N * m, 1);
+            else       oracle_kernel_lo2hi(P, m % 2, m, A + (size_t) N * m, 1);
+        }
+        return;
+    }
     if (P->kind == ORACLE_TRI) {
         #pragma omp parallel for schedule(dynamic, 1)
         for (int m = 1; m < M; m++) {
@@ -553,6 +573,7 @@ oracle_plan * oracle_plan_rotations(int kind, int n, double alpha, double beta, 
     P->c = calloc(len ? len : 1, sizeof(double));
     if (kind == ORACLE_SPH) plan_rotsphere(n, P->s, P->c);
     else if (kind == ORACLE_TRI) plan_rottriangle(n, alpha, beta, gamma, P->s, P->c);
+    else if (kind == ORACLE_RECT) plan_rotrectdisk(n, beta, P->s, P->c);
     else plan_rotdisk(n, alpha, beta, P->s, P->c);
     return P;
 }
@@ -611,10 +632,45 @@ oracle_plan * oracle_plan_disk2cxf(int n, double alpha, double beta) {
     return P;
 }
 
+/* plan_ultraspherical_to_chebyshev(1, 0, n, lambda) (src/transforms.c:185-197): the normalised
+ * Jacobi connection (lambda - 1/2, lambda - 1/2) -> (-1/2, -1/2), entries i = j, j - 2, .. of
+ * row i scaled to the unnormalised Chebyshev basis */
+static double * ultraspherical_to_chebyshev(int n, double lambda) {
+    double * V = oracle_plan_jacobi_to_jacobi(1, 1, n, lambda - 0.5, lambda - 0.5, -0.5, -0.5);
+    for (int j = 0; j < n; j++)
+        for (int i = j; i >= 0; i -= 2) {
+            double r = i ? sqrtl(M_2_PIl) : sqrtl(M_1_PIl);
+            V[i + (size_t) j * n] *= r;
+        }
+    return V;
+}
+
+/* plan_chebyshev_to_ultraspherical(0, 1, n, lambda) (src/transforms.c:199-211) */
+static double * chebyshev_to_ultraspherical(int n, double lambda) {
+    double * V = oracle_plan_jacobi_to_jacobi(1, 1, n, -0.5, -0.5, lambda - 0.5, lambda - 0.5);
+    for (int j = 0; j < n; j++) {
+        double r = j ? sqrtl(M_PI_2l) : sqrtl(M_PIl);
+        for (int i = j; i >= 0; i -= 2) V[i + (size_t) j * n] *= r;
+    }
+    return V;
+}
+
+/* src/drivers.c:1123-1141 */
+oracle_plan * oracle_plan_rectdisk2cheb(int n, double beta) {
+    oracle_plan * P = oracle_plan_rotations(ORACLE_RECT, n, 0, beta, 0);
+    P->P[0] = ultraspherical_to_chebyshev(n, beta + 1.0);
+    P->P[1] = oracle_plan_ultraspherical_to_ultraspherical(1, 0, n, beta + 2.0, 1.0);
+    P->P[2] = ultraspherical_to_chebyshev(n, beta + 0.5);
+    P->Pinv[0] = chebyshev_to_ultraspherical(n, beta + 1.0);
+    P->Pinv[1] = oracle_plan_ultraspherical_to_ultraspherical(0, 1, n, 1.0, beta + 2.0);
+    P->Pinv[2] = chebyshev_to_ultraspherical(n, beta + 0.5);
+    return P;
+}
+
 void oracle_destroy_plan(oracle_plan * P) {
     if (!P) return;
     free(P->s); free(P->c);
-    for (int i = 0; i < 2; i++) { free(P->P[i]); free(P->Pinv[i]); }
+    for (int i = 0; i < 3; i++) { free(P->P[i]); free(P->Pinv[i]); }
     free(P);
 }
 
@@ -642,6 +698,23 @@ static void trmm4(char trans, int N, int M, const double * U0, const double * U1
 void oracle_execute(const oracle_plan * P, int forward, char TRANS, double * A, int N, int M) {
     if (TRANS != 'N' && TRANS != 'T') return;
     int tN = TRANS == 'N';
+    if (P->kind == ORACLE_RECT) {   /* src/drivers.c:1143-1171; M == N (the right multiply is n x n) */
+        double * const * U = forward ? P->P : P->Pinv;
+        if ((forward && tN) || (!forward && !tN)) {
+            char t = forward ? 'N' : 'T';
+            oracle_execute_hi2lo(P, A, M);
+            oracle_trmm('L', t, N, U[0], (M + 1) / 2, A, 2 * N);
+            oracle_trmm('L', t, N, U[1], M / 2, A + N, 2 * N);
+            oracle_trmm('R', forward ? 'T' : 'N', N, U[2], N, A, N);
+        } else {
+            char t = forward ? 'T' : 'N';
+            oracle_trmm('R', forward ? 'N' : 'T', N, U[2], N, A, N);
+            oracle_trmm('L', t, N, U[0], (M + 1) / 2, A, 2 * N);
+            oracle_trmm('L', t, N, U[1], M / 2, A + N, 2 * N);
+            oracle_execute_lo2hi(P, A, M);
+        }
+        return;
+    }
     if (P->kind == ORACLE_TRI) {
         double a = P->alpha, b = P->beta, g = P->gamma;
         int left = (b + g != -1.5) || (a != -0.5);
@@ -734,7 +807,7 @@ static inline double u_pm1(unsigned long long seed, unsigned long long idx) {
 void oracle_fill(int kind, int N, int M, unsigned long long seed, double * A) {
     for (int j = 0; j < M; j++)
         for (int i = 0; i < N; i++) {
-            int on = kind == ORACLE_SPH ? (j < M - 2 * i) : kind == ORACLE_TRI ? (j < M - i) : (j < M - 4 * i);
+            int on = kind == ORACLE_SPH ? (j < M - 2 * i) : (kind == ORACLE_TRI || kind == ORACLE_RECT) ? (j < M - i) : (j < M - 4 * i);
             size_t idx = (size_t) i + (size_t) j * N;
             A[idx] = on ? u_pm1(seed, idx) : 0.0;
         }

@@ -18,15 +18,15 @@
 extern "C" {
 #endif
 
-enum { ORACLE_SPH = 0, ORACLE_TRI = 1, ORACLE_DISK = 2 };
+enum { ORACLE_SPH = 0, ORACLE_TRI = 1, ORACLE_DISK = 2, ORACLE_RECT = 3 };
 
 typedef struct {
-    int kind;          /* ORACLE_SPH / ORACLE_TRI / ORACLE_DISK */
+    int kind;          /* ORACLE_SPH / ORACLE_TRI / ORACLE_DISK / ORACLE_RECT (Dunkl-Xu rectangularised disk) */
     int n;             /* degree + 1 (rows of the coefficient matrix) */
     double * s;        /* rotation sines, packed triangle (sph, tri) or disk packing */
     double * c;        /* rotation cosines, same packing */
-    double * P[2];     /* dense n x n upper-triangular connection matrices, column-major */
-    double * Pinv[2];  /* their inverses */
+    double * P[3];     /* dense n x n upper-triangular connection matrices, column-major (rect: 3) */
+    double * Pinv[3];  /* their inverses */
     double alpha, beta, gamma;
 } oracle_plan;
 
@@ -39,6 +39,8 @@ void oracle_set_fused(int fused);
 oracle_plan * oracle_plan_sph2fourier(int n);
 oracle_plan * oracle_plan_tri2cheb(int n, double alpha, double beta, double gamma);
 oracle_plan * oracle_plan_disk2cxf(int n, double alpha, double beta);
+/* src/drivers.c:1123-1141 (ft_plan_rectdisk2cheb) */
+oracle_plan * oracle_plan_rectdisk2cheb(int n, double beta);
 /* Rotation tables only (no connection matrices): cheap, for rotation-stage checks. */
 oracle_plan * oracle_plan_rotations(int kind, int n, double alpha, double beta, double gamma);
 void oracle_destroy_plan(oracle_plan * P);
@@ -86,7 +88,8 @@ void oracle_execute_spinsph_lo2hi(const oracle_spin_plan * P, double * A, int M)
 void oracle_execute_spin(const oracle_spin_plan * P, int forward, char TRANS, double * A, int N, int M);
 void oracle_fill_spin(int N, int M, int s, unsigned long long seed, double * A);
 
-/* Seeded fills in the reference layouts (src/ftutilities.c:75-113), U(-1,1) from splitmix64. */
+/* Seeded fills in the reference layouts (src/ftutilities.c:75-129), U(-1,1) from splitmix64
+ * (rect: rows i, columns j < M - i, like tri). */
 void oracle_fill(int kind, int N, int M, unsigned long long seed, double * A);
 
 #ifdef __cplusplus

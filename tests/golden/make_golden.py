@@ -12,9 +12,12 @@ seeded inputs and stores inputs and outputs as compressed .npz files:
   * the four dense connection matrices of each plan;
   * spin-weighted transforms (ft_execute_spinsph2fourier / ft_execute_fourier2spinsph and
     the rotation stages ft_execute_spinsph_hi2lo / _lo2hi) on complex inputs in
-    spinsphrand's layout, files spin_n<n>_s<s>.npz.
+    spinsphrand's layout, files spin_n<n>_s<s>.npz;
+  * Dunkl-Xu (rectangularised disk) transforms (ft_execute_rectdisk2cheb /
+    ft_execute_cheb2rectdisk, M = N), their rotation stages (ft_execute_rectdisk_hi2lo /
+    _lo2hi) and the six connection matrices, files rect_n<n>_b<beta>.npz.
 
-    python tests/golden/make_golden.py [sph tri disk spin]   (default: all)
+    python tests/golden/make_golden.py [sph tri disk spin rect]   (default: all)
 """
 from __future__ import annotations
 
@@ -34,6 +37,7 @@ CASES = [
     ("disk", 9, (0.0, 0.0)), ("disk", 16, (0.0, 0.0)), ("disk", 12, (0.5, -0.25)),
 ]
 SPIN_CASES = [(8, -2), (17, 0), (17, 1), (16, 3), (33, -1), (12, 4)]
+RECT_CASES = [(8, 0.0), (17, 0.5), (16, -0.25), (33, 1.5)]
 SEED = 20261203
 
 
@@ -55,7 +59,7 @@ def main():
         for d in ("hi2lo", "lo2hi"):
             getattr(L, f"ft_execute_{fam}_{d}").argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int]
     L.ft_destroy_rotation_plan.argtypes = [C.c_void_p]
-    families = set(sys.argv[1:]) or {"sph", "tri", "disk", "spin"}
+    families = set(sys.argv[1:]) or {"sph", "tri", "disk", "spin", "rect"}
     for kind, n, params in CASES:
         if kind not in families:
             continue
@@ -102,6 +106,27 @@ def main():
                 R.spin_rotations(n, sw, d == "hi2lo", B)
                 out["rot_" + d] = B
             path = os.path.join(HERE, f"spin_n{n}_s{sw}.npz".replace("-", "m"))
+            np.savez_compressed(path, **out)
+            print("wrote", os.path.relpath(path), A.shape)
+    if "rect" in families:
+        for n, beta in RECT_CASES:
+            A = fill("rect", n, SEED)
+            P = R.plan("rect", n, beta=beta)
+            out = {"A": A, "beta": np.array(beta)}
+            for fwd in (True, False):
+                for tr in "NT":
+                    B = A.copy(order="F")
+                    R.execute("rect", P, fwd, tr, B)
+                    out[("fwd" if fwd else "bwd") + "_" + tr] = B
+            Ps, Pinvs = R.connection(P, n)
+            for i in range(3):
+                out[f"P{i}"], out[f"Pinv{i}"] = Ps[i], Pinvs[i]
+            R.destroy(P)
+            for d in ("hi2lo", "lo2hi"):
+                B = A.copy(order="F")
+                R.rect_rotations(n, beta, d == "hi2lo", B)
+                out["rot_" + d] = B
+            path = os.path.join(HERE, case_name("rect", n, (beta,)) + ".npz")
             np.savez_compressed(path, **out)
             print("wrote", os.path.relpath(path), A.shape)
 

@@ -19,9 +19,9 @@ from conftest import EPS, rel2, relinf
 
 pytestmark = pytest.mark.gpu
 
-# the harmonic-plan fixtures (the spin fixtures have their own tests)
+# the sph / tri / disk fixtures (the spin and Dunkl-Xu fixtures have their own tests)
 GOLDEN = sorted(p for p in glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz"))
-                if not os.path.basename(p).startswith("spin_"))
+                if os.path.basename(p).split("_")[0] in ("sph", "tri", "disk"))
 TOL = {"sph": (4, 2), "tri": (32, 8), "disk": (8, 4)}
 FAMILIES = [("sph", ()), ("tri", (0.0, 0.0, 0.0)), ("tri", (-0.5, -0.5, -0.5)), ("tri", (0.5, 1.0, -0.25)),
             ("disk", (0.0, 0.0)), ("disk", (0.5, -0.25))]

@@ -13,9 +13,9 @@ import pytest
 from conftest import EPS, rel2, relinf
 from oracle.bind import Oracle, Reference, fill
 
-# the harmonic-plan fixtures (the spin fixtures have their own tests)
+# the sph / tri / disk fixtures (the spin and Dunkl-Xu fixtures have their own tests)
 GOLDEN = sorted(p for p in glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz"))
-                if not os.path.basename(p).startswith("spin_"))
+                if os.path.basename(p).split("_")[0] in ("sph", "tri", "disk"))
 
 
 @pytest.fixture(scope="module")
