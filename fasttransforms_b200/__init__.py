@@ -19,7 +19,7 @@ from typing import Sequence
 
 import numpy as np
 
-from .utilities import diskrand, layout_cols, rand_layout, sphrand, spinsphrand, trirand
+from .utilities import diskrand, layout_cols, rand_layout, rectdiskrand, sphrand, spinsphrand, trirand
 
 __all__ = [
     "FTB200Error", "HarmonicPlan", "RotationPlan", "library_path", "lib",
@@ -37,6 +37,8 @@ __all__ = [
     "SpinHarmonicPlan", "SpinRotationPlan", "plan_spinsph2fourier", "plan_rotspinsphere",
     "execute_spinsph2fourier", "execute_fourier2spinsph", "execute_spinsph_hi2lo", "execute_spinsph_lo2hi",
     "execute_spin_dev", "spin_rotations_dev", "spinsphrand",
+    "plan_rectdisk2cheb", "execute_rectdisk2cheb", "execute_cheb2rectdisk", "plan_rotrectdisk",
+    "execute_rectdisk_hi2lo", "execute_rectdisk_lo2hi", "rectdiskrand",
     "SPH", "TRI", "DISK",
 ]
 
@@ -87,12 +89,14 @@ def _load() -> C.CDLL:
         "ft_execute_spinsph2fourier": (None, [ch, vp, dp, i, i]), "ft_execute_fourier2spinsph": (None, [ch, vp, dp, i, i]),
         "ft_b200_execute_spin_dev": (i, [vp, i, ch, vp, i, i, vp]),
         "ft_b200_spin_rotations_dev": (i, [vp, i, vp, i, vp]),
+        "ft_plan_rectdisk2cheb": (vp, [i, d]), "ft_plan_rotrectdisk": (vp, [i, d]),
     }
     for name in ("sph_synthesis", "sph_analysis", "sphv_synthesis", "sphv_analysis"):
         sig["ft_execute_" + name] = (None, [ch, vp, dp, i, i])
-    for name in ("sph2fourier", "fourier2sph", "tri2cheb", "cheb2tri", "disk2cxf", "cxf2disk", "sphv2fourier", "fourier2sphv"):
+    for name in ("sph2fourier", "fourier2sph", "tri2cheb", "cheb2tri", "disk2cxf", "cxf2disk", "sphv2fourier", "fourier2sphv",
+                 "rectdisk2cheb", "cheb2rectdisk"):
         sig["ft_execute_" + name] = (None, [ch, vp, dp, i, i])
-    for fam in ("sph", "tri", "disk"):
+    for fam in ("sph", "tri", "disk", "rectdisk"):
         for d_ in ("hi2lo", "lo2hi"):
             sig[f"ft_execute_{fam}_{d_}"] = (None, [vp, dp, dp, i])
     for name, (res, args) in sig.items():
@@ -193,6 +197,11 @@ def plan_tri2cheb(n: int, alpha: float, beta: float, gamma: float) -> HarmonicPl
 
 def plan_disk2cxf(n: int, alpha: float, beta: float) -> HarmonicPlan:
     return _plan("disk", n, lib.ft_plan_disk2cxf(n, alpha, beta), (alpha, beta))
+
+
+def plan_rectdisk2cheb(n: int, beta: float) -> HarmonicPlan:
+    """Dunkl-Xu (rectangularised disk) plan (reference: src/drivers.c:1123-1141); M = n."""
+    return _plan("rect", n, lib.ft_plan_rectdisk2cheb(n, beta), (beta,))
 
 
 class SphereGridPlan(HarmonicPlan):
@@ -351,6 +360,8 @@ def execute_disk2cxf(trans, P, A, N=None, M=None): _exec_host("ft_execute_disk2c
 def execute_cxf2disk(trans, P, A, N=None, M=None): _exec_host("ft_execute_cxf2disk", trans, P, A, N, M)
 def execute_sphv2fourier(trans, P, A, N=None, M=None): _exec_host("ft_execute_sphv2fourier", trans, P, A, N, M)
 def execute_fourier2sphv(trans, P, A, N=None, M=None): _exec_host("ft_execute_fourier2sphv", trans, P, A, N, M)
+def execute_rectdisk2cheb(trans, P, A, N=None, M=None): _exec_host("ft_execute_rectdisk2cheb", trans, P, A, N, M)
+def execute_cheb2rectdisk(trans, P, A, N=None, M=None): _exec_host("ft_execute_cheb2rectdisk", trans, P, A, N, M)
 
 
 def plan_rotsphere(n: int) -> RotationPlan:
@@ -374,6 +385,13 @@ def plan_rotdisk(n: int, alpha: float, beta: float) -> RotationPlan:
     return RotationPlan(p, "disk", n, (alpha, beta))
 
 
+def plan_rotrectdisk(n: int, beta: float) -> RotationPlan:
+    p = lib.ft_plan_rotrectdisk(n, beta)
+    if not p:
+        _check()
+    return RotationPlan(p, "rect", n, (beta,))
+
+
 def _exec_rot(fname, RP, A, M=None):
     A = _host_matrix(A)
     M = A.shape[1] if M is None else M
@@ -387,6 +405,8 @@ def execute_tri_hi2lo(RP, A, M=None): _exec_rot("ft_execute_tri_hi2lo", RP, A, M
 def execute_tri_lo2hi(RP, A, M=None): _exec_rot("ft_execute_tri_lo2hi", RP, A, M)
 def execute_disk_hi2lo(RP, A, M=None): _exec_rot("ft_execute_disk_hi2lo", RP, A, M)
 def execute_disk_lo2hi(RP, A, M=None): _exec_rot("ft_execute_disk_lo2hi", RP, A, M)
+def execute_rectdisk_hi2lo(RP, A, M=None): _exec_rot("ft_execute_rectdisk_hi2lo", RP, A, M)
+def execute_rectdisk_lo2hi(RP, A, M=None): _exec_rot("ft_execute_rectdisk_lo2hi", RP, A, M)
 
 
 def execute_dev(P: HarmonicPlan, forward: bool, trans: str, ptr: int, N: int, M: int, stream: int = 0) -> None:

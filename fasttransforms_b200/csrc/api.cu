@@ -157,7 +157,7 @@ bool get_tasks(ft_rotation_plan * RP, int M, RotTask ** d_tasks, int * ntasks) {
 
 // Columns the rotation stage leaves alone (orders 0 and 1): copied when the
 // stage runs out of place.
-int untouched_cols(int kind, int M) { return std::min(M, kind == TRI ? 1 : 3); }
+int untouched_cols(int kind, int M) { return std::min(M, kind == TRI ? 1 : (kind == RECT ? 2 : 3)); }
 
 bool rotations(ft_rotation_plan * RP, bool hi2lo, const double * in, double * out, int M, long long lda, cudaStream_t st) {
     RotTask * d_tasks = nullptr;
@@ -205,7 +205,7 @@ bool rotations_sphv(ft_rotation_plan * RP, bool hi2lo, const double * in, double
 // (src/drivers.c:94-110, 414-430), so an even M >= 4 would put the last order's
 // second column at index M, past the matrix; such M are rejected.
 bool valid_pairs(int kind, int M) {
-    if (kind != TRI && M >= 4 && M % 2 == 0) {
+    if (kind != TRI && kind != RECT && M >= 4 && M % 2 == 0) {
         set_error(FT_B200_EINVAL, "sph and disk matrices need an odd number of columns M");
         return false;
     }
@@ -780,6 +780,15 @@ bool connection_multiply(HarmonicPlan * H, bool inverse, bool trans, const doubl
     return trmm4(H, inverse, trans, in, out, M, st, swap);
 }
 
+// Rotation plans and sweeps for the plans of other files (the Dunkl-Xu plans, rectdisk.cu).
+ft_rotation_plan * rotation_plan_new(int kind, int n, double alpha, double beta, double gamma) {
+    return make_rotation_plan(kind, n, alpha, beta, gamma);
+}
+bool rotation_sweeps(ft_rotation_plan * RP, bool hi2lo, const double * in, double * out, int M, long long lda,
+                     cudaStream_t st) {
+    return rotations(RP, hi2lo, in, out, M, lda, st);
+}
+
 }  // namespace ftb
 
 using namespace ftb;
@@ -833,7 +842,10 @@ ft_harmonic_plan * ft_plan_disk2cxf(const int n, const double alpha, const doubl
 
 void ft_destroy_harmonic_plan(ft_harmonic_plan * P) {
     HarmonicPlan * H = as_plan(P);
-    if (!H) return;
+    if (!H) {
+        rect_plan_destroy(P);   // a Dunkl-Xu plan (rectdisk.cu), or nothing of this library
+        return;
+    }
     if (H->stream) { cudaStreamSynchronize(H->stream); cudaStreamDestroy(H->stream); }
     if (H->rp_arr[0]) ft_destroy_rotation_plan(H->rp_arr[0]);
     for (int i = 0; i < 2; i++) {
@@ -862,6 +874,7 @@ void ft_execute_cxf2disk(const char TRANS, const ft_harmonic_plan * P, double * 
 ft_rotation_plan * ft_plan_rotsphere(const int n) { return make_rotation_plan(SPH, n, 0, 0, 0); }
 ft_rotation_plan * ft_plan_rottriangle(const int n, const double alpha, const double beta, const double gamma) { return make_rotation_plan(TRI, n, alpha, beta, gamma); }
 ft_rotation_plan * ft_plan_rotdisk(const int n, const double alpha, const double beta) { return make_rotation_plan(DISK, n, alpha, beta, 0); }
+ft_rotation_plan * ft_plan_rotrectdisk(const int n, const double beta) { return make_rotation_plan(RECT, n, 0, beta, 0); }
 
 void ft_destroy_rotation_plan(ft_rotation_plan * RP) {
     if (!RP) return;
@@ -887,11 +900,18 @@ void ft_execute_tri_hi2lo(const ft_rotation_plan * RP, double * A, double *, con
 void ft_execute_tri_lo2hi(const ft_rotation_plan * RP, double * A, double *, const int M) { rotations_host(RP, false, A, M, TRI); }
 void ft_execute_disk_hi2lo(const ft_rotation_plan * RP, double * A, double *, const int M) { rotations_host(RP, true, A, M, DISK); }
 void ft_execute_disk_lo2hi(const ft_rotation_plan * RP, double * A, double *, const int M) { rotations_host(RP, false, A, M, DISK); }
+void ft_execute_rectdisk_hi2lo(const ft_rotation_plan * RP, double * A, double *, const int M) { rotations_host(RP, true, A, M, RECT); }
+void ft_execute_rectdisk_lo2hi(const ft_rotation_plan * RP, double * A, double *, const int M) { rotations_host(RP, false, A, M, RECT); }
 
 int ft_b200_execute_dev(const ft_harmonic_plan * P, int forward, char TRANS, double * dA, int N, int M, void * stream) {
     clear_error();
     HarmonicPlan * H = as_plan(P);
-    if (!H) { set_error(FT_B200_EINVAL, "not a plan created by this library"); return t_status; }
+    if (!H) {
+        const int r = rect_execute_dev(P, forward != 0, TRANS, dA, N, M, static_cast<cudaStream_t>(stream));
+        if (r >= 0) return r;   // a Dunkl-Xu plan (rectdisk.cu)
+        set_error(FT_B200_EINVAL, "not a plan created by this library");
+        return t_status;
+    }
     return execute_dev_impl(H, forward != 0, TRANS, dA, N, M, static_cast<cudaStream_t>(stream));
 }
 

@@ -17,7 +17,9 @@ namespace ftb {
 
 // SPIN: stage two of the spin-weighted sweeps (sph sweeps of order |m - |s|| on interleaved
 // complex columns, both columns of an order in one lane; spin.cu).
-enum Kind { SPH = 0, TRI = 1, DISK = 2, SPIN = 3 };
+// RECT: the Dunkl-Xu (rectangularised disk) sweeps: the sph sweep shape (rotations (k, k + 2),
+// j = m - 2 .. m mod 2) on one column per order, column m for m = 2 .. M - 1.
+enum Kind { SPH = 0, TRI = 1, DISK = 2, SPIN = 3, RECT = 4 };
 
 // ---------------------------------------------------------------------------
 // Rotation geometry.
@@ -40,7 +42,7 @@ enum Kind { SPH = 0, TRI = 1, DISK = 2, SPIN = 3 };
 // ---------------------------------------------------------------------------
 struct Geo {
     __host__ __device__ static inline int floordiv2(int x) { return x >= 0 ? x / 2 : -((1 - x) / 2); }
-    __host__ __device__ static inline bool sphlike(int kind) { return kind == SPH || kind == SPIN; }
+    __host__ __device__ static inline bool sphlike(int kind) { return kind == SPH || kind == SPIN || kind == RECT; }
     __host__ __device__ static inline int chains(int kind) { return sphlike(kind) ? 2 : 1; }
     __host__ __device__ static inline int step(int kind) { return kind == TRI ? 1 : 2; }
     __host__ __device__ static inline int top(int kind, int N, int j, int c) {
@@ -65,7 +67,7 @@ struct Geo {
     __host__ __device__ static inline int first_order(int kind) { return kind == TRI ? 1 : (kind == SPIN ? 0 : 2); }
     // orders per rotation task: one lane per (order, chain) of a 32-lane warp
     __host__ __device__ static inline int task_orders(int kind) { return sphlike(kind) ? 16 : 32; }
-    __host__ __device__ static inline int last_order(int kind, int M) { return kind == TRI ? M - 1 : M / 2; }
+    __host__ __device__ static inline int last_order(int kind, int M) { return (kind == TRI || kind == RECT) ? M - 1 : M / 2; }
     // Sweeps of the rotation task of lowest order mbase: every sweep j = jlo, jlo + step, ..,
     // jhi applies to at least one of its columns (order m runs j = jpar .. m - step; with
     // blk > 0 only its sweeps above its last whole block of blk sweeps).  Returns their number
@@ -235,6 +237,13 @@ bool connection_multiply(HarmonicPlan * H, bool inverse, bool trans, const doubl
                          cudaStream_t st, bool swap);
 // NULL unless P is a live plan of this library (api.cu)
 HarmonicPlan * as_plan(const ft_harmonic_plan * P);
+// A rotation plan of any kind, and its sweeps on device memory (in == out allowed) (api.cu)
+ft_rotation_plan * rotation_plan_new(int kind, int n, double alpha, double beta, double gamma);
+bool rotation_sweeps(ft_rotation_plan * RP, bool hi2lo, const double * in, double * out, int M, long long lda,
+                     cudaStream_t st);
+// Dunkl-Xu plans (rectdisk.cu): false / -1 when P is not one
+bool rect_plan_destroy(ft_harmonic_plan * P);
+int rect_execute_dev(const ft_harmonic_plan * P, bool forward, char TRANS, double * dA, int N, int M, cudaStream_t st);
 // device task list already built for (RP, M), without building one (api.cu)
 bool find_tasks(ft_rotation_plan * RP, int M, const RotTask ** d_tasks, int * ntasks);
 

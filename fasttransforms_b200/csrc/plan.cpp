@@ -22,7 +22,8 @@ namespace ftb {
 
 // ---------------------------------------------------------------------------
 // Rotation tables (FP64 square roots of rationals).
-// sph: src/rotations.c:116-133, tri: :143-160, disk: :173-190 (negated sine).
+// sph: src/rotations.c:116-133, tri: :143-160, disk: :173-190 (negated sine),
+// rect: :270-287 (the sph packing, entries depending on beta).
 // ---------------------------------------------------------------------------
 void rotation_tables(int kind, int n, double alpha, double beta, double gamma, double * s, double * c) {
     if (kind == SPH) {
@@ -42,6 +43,16 @@ void rotation_tables(int kind, int n, double alpha, double beta, double gamma, d
                 const double numc = (2 * m + beta + gamma + 2) * (2 * l + 2 * m + alpha + beta + gamma + 4);
                 const double den = (l + 2 * m + beta + gamma + 3) * (l + 2 * m + alpha + beta + gamma + 3);
                 const long long o = Geo::table_base(TRI, n, m) + l;
+                s[o] = std::sqrt(nums / den);
+                c[o] = std::sqrt(numc / den);
+            }
+    } else if (kind == RECT) {
+        for (int m = 0; m < n; m++)
+            for (int l = 0; l < n - m; l++) {
+                const double nums = (l + 1) * (l + 2);
+                const double numc = (2 * m + 2 * beta + 3) * (2 * l + 2 * m + 2 * beta + 6);
+                const double den = (l + 2 * m + 2 * beta + 4) * (l + 2 * m + 2 * beta + 5);
+                const long long o = Geo::table_base(RECT, n, m) + l;
                 s[o] = std::sqrt(nums / den);
                 c[o] = std::sqrt(numc / den);
             }

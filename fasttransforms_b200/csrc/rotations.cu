@@ -47,11 +47,11 @@ namespace {
 
 template <int KIND>
 struct KT {
-    static constexpr int CH = (KIND == SPH || KIND == SPIN) ? 2 : 1;   // chains per column
+    static constexpr int CH = (KIND == SPH || KIND == SPIN || KIND == RECT) ? 2 : 1;   // chains per column
     static constexpr int STEP = KIND == TRI ? 1 : 2;      // order step between sweeps
     // sequences per order sharing the rotations: cos, sin columns (sph, disk), the column
-    // (tri), or the real and imaginary parts of the columns of -m and m (spin)
-    static constexpr int NCOL = KIND == TRI ? 1 : (KIND == SPIN ? 4 : 2);
+    // (tri, rect), or the real and imaginary parts of the columns of -m and m (spin)
+    static constexpr int NCOL = (KIND == TRI || KIND == RECT) ? 1 : (KIND == SPIN ? 4 : 2);
     static constexpr int ES = KIND == SPIN ? 2 : 1;       // doubles per element (interleaved complex)
     static constexpr int ORD = 32 / CH;                   // orders per task (one lane per order and chain)
     static constexpr int COLS = ORD * NCOL;               // columns per task
@@ -311,7 +311,7 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
                     colok[v] = mcl <= mlast && !(mcl == 0 && h >= 2) && colc < F.M;
                     coff = colok[v] ? ES * (colc * lda + rr) + (h & 1) : 0;
                 } else {
-                    const long long colc = KIND == TRI ? mcl : 2 * mcl - 1 + h;
+                    const long long colc = (KIND == TRI || KIND == RECT) ? mcl : 2 * mcl - 1 + h;
                     colok[v] = mcl <= mlast;
                     coff = colok[v] ? colc * lda + rr : 0;
                 }
@@ -491,7 +491,7 @@ cudaError_t launch_kind(int cfg, const RotLaunch & L, int max_ctas, cudaStream_t
         (void) cfg;   // four sequences per lane: only 8 x 4 x 8 fits the stage buffers
         return launch_cfg<KIND, HI2LO, 8, 4, 8>(L, max_ctas, st);
     } else {
-        if constexpr (KIND != TRI) {
+        if constexpr (KIND != TRI && KIND != RECT) {   // one sequence per lane: too few rows per warp
             if (cfg == 1) return launch_cfg<KIND, HI2LO, 16, 4, 8>(L, max_ctas, st);
         }
         if (cfg == 2) return launch_cfg<KIND, HI2LO, 8, 4, 8>(L, max_ctas, st);
@@ -611,6 +611,7 @@ cudaError_t launch_with(int kind, bool hi2lo, int cfg, const RotLaunch & L, int 
         case TRI:  return hi2lo ? launch_kind<TRI, true>(cfg, L, max_ctas, st) : launch_kind<TRI, false>(cfg, L, max_ctas, st);
         case DISK: return hi2lo ? launch_kind<DISK, true>(cfg, L, max_ctas, st) : launch_kind<DISK, false>(cfg, L, max_ctas, st);
         case SPIN: return hi2lo ? launch_kind<SPIN, true>(cfg, L, max_ctas, st) : launch_kind<SPIN, false>(cfg, L, max_ctas, st);
+        case RECT: return hi2lo ? launch_kind<RECT, true>(cfg, L, max_ctas, st) : launch_kind<RECT, false>(cfg, L, max_ctas, st);
     }
     return cudaErrorInvalidValue;
 }
@@ -679,7 +680,7 @@ int tune(int kind, bool hi2lo, const RotLaunch & L, double * const * dead, int m
     // spreads a task's passes over SMs: worth it when there are few tasks, not when the
     // columns would leave L2 between passes)
     for (int cfg = 0; cfg < 14; ++cfg) {
-        if ((cfg & 7) > 5 || (kind == TRI && (cfg & 7) == 1)) continue;   // tri: shape 1 not built
+        if ((cfg & 7) > 5 || ((kind == TRI || kind == RECT) && (cfg & 7) == 1)) continue;   // tri, rect: shape 1 not built
         if ((cfg & 8) && !sched) continue;
         if (launch_shape(kind, hi2lo, cfg, S, max_ctas, st, sched) != cudaSuccess) { best = -1; break; }
         if (cudaEventRecord(e0, st) != cudaSuccess) { best = -1; break; }

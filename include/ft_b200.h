@@ -106,7 +106,15 @@ void ft_execute_disk2cxf(const char TRANS, const ft_harmonic_plan * P, double * 
 /* replaces ft_execute_cxf2disk, src/drivers.c:1006-1021 */
 void ft_execute_cxf2disk(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M);
 
-/* replaces ft_destroy_harmonic_plan, src/drivers.c:793-814 */
+/* replaces ft_plan_rectdisk2cheb, src/drivers.c:1123-1141: Dunkl-Xu (rectangularised disk)
+ * transforms; the plan has NP = 3 connection pairs in P / Pinv (host copies) */
+ft_harmonic_plan * ft_plan_rectdisk2cheb(const int n, const double beta);
+/* replace ft_execute_rectdisk2cheb / ft_execute_cheb2rectdisk, src/drivers.c:1143-1171;
+ * M must equal N (the right multiply is n x n), as in the reference's tests */
+void ft_execute_rectdisk2cheb(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M);
+void ft_execute_cheb2rectdisk(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M);
+
+/* replaces ft_destroy_harmonic_plan, src/drivers.c:793-814 (every plan kind above) */
 void ft_destroy_harmonic_plan(ft_harmonic_plan * P);
 
 /* Synthesis and analysis on the sphere's grid (theta_i = (i + 1/2) pi / N,
@@ -173,6 +181,8 @@ ft_rotation_plan * ft_plan_rotsphere(const int n);
 ft_rotation_plan * ft_plan_rottriangle(const int n, const double alpha, const double beta, const double gamma);
 /* replaces ft_plan_rotdisk, src/rotations.c:173-190 */
 ft_rotation_plan * ft_plan_rotdisk(const int n, const double alpha, const double beta);
+/* replaces ft_plan_rotrectdisk, src/rotations.c:270-287 */
+ft_rotation_plan * ft_plan_rotrectdisk(const int n, const double beta);
 /* replaces ft_destroy_rotation_plan, src/rotations.c:6-10 */
 void ft_destroy_rotation_plan(ft_rotation_plan * RP);
 /* replace ft_execute_{sph,tri,disk}_{hi2lo,lo2hi}, src/drivers.c:58-92, 278-312, 378-412.
@@ -183,6 +193,9 @@ void ft_execute_tri_hi2lo(const ft_rotation_plan * RP, double * A, double * B, c
 void ft_execute_tri_lo2hi(const ft_rotation_plan * RP, double * A, double * B, const int M);
 void ft_execute_disk_hi2lo(const ft_rotation_plan * RP, double * A, double * B, const int M);
 void ft_execute_disk_lo2hi(const ft_rotation_plan * RP, double * A, double * B, const int M);
+/* replace ft_execute_rectdisk_hi2lo / lo2hi, src/drivers.c:488-508 (order m on column m) */
+void ft_execute_rectdisk_hi2lo(const ft_rotation_plan * RP, double * A, double * B, const int M);
+void ft_execute_rectdisk_lo2hi(const ft_rotation_plan * RP, double * A, double * B, const int M);
 
 /* ------------------------------------------------------------------------ */
 /* Device-pointer entry points (no host copies).  A is a device pointer     */
@@ -192,8 +205,8 @@ void ft_execute_disk_lo2hi(const ft_rotation_plan * RP, double * A, double * B, 
 /* ------------------------------------------------------------------------ */
 enum { FT_B200_SPH = 0, FT_B200_TRI = 1, FT_B200_DISK = 2 };
 
-/* Full transform.  forward = 1: sph2fourier / tri2cheb / disk2cxf;
- * forward = 0: fourier2sph / cheb2tri / cxf2disk. */
+/* Full transform.  forward = 1: sph2fourier / tri2cheb / disk2cxf / rectdisk2cheb;
+ * forward = 0: fourier2sph / cheb2tri / cxf2disk / cheb2rectdisk. */
 int ft_b200_execute_dev(const ft_harmonic_plan * P, int forward, char TRANS, double * dA, int N, int M, void * stream);
 /* Grid synthesis / analysis on device memory: op 0 sph synthesis, 1 sph analysis,
  * 2 sphv synthesis, 3 sphv analysis (the sequences of the ft_execute_* above, with
