@@ -19,7 +19,7 @@ from typing import Sequence
 
 import numpy as np
 
-from .utilities import diskrand, layout_cols, rand_layout, rectdiskrand, sphrand, spinsphrand, trirand
+from .utilities import diskrand, layout_cols, rand_layout, rectdiskrand, sphrand, spinsphrand, tetrand, trirand
 
 __all__ = [
     "FTB200Error", "HarmonicPlan", "RotationPlan", "library_path", "lib",
@@ -39,6 +39,8 @@ __all__ = [
     "execute_spin_dev", "spin_rotations_dev", "spinsphrand",
     "plan_rectdisk2cheb", "execute_rectdisk2cheb", "execute_cheb2rectdisk", "plan_rotrectdisk",
     "execute_rectdisk_hi2lo", "execute_rectdisk_lo2hi", "rectdiskrand",
+    "TetPlan", "plan_tet2cheb", "execute_tet2cheb", "execute_cheb2tet", "execute_tet_hi2lo", "execute_tet_lo2hi",
+    "execute_tet_dev", "tet_rotations_dev", "tetrand",
     "SPH", "TRI", "DISK",
 ]
 
@@ -90,6 +92,11 @@ def _load() -> C.CDLL:
         "ft_b200_execute_spin_dev": (i, [vp, i, ch, vp, i, i, vp]),
         "ft_b200_spin_rotations_dev": (i, [vp, i, vp, i, vp]),
         "ft_plan_rectdisk2cheb": (vp, [i, d]), "ft_plan_rotrectdisk": (vp, [i, d]),
+        "ft_plan_tet2cheb": (vp, [i, d, d, d, d]),
+        "ft_execute_tet2cheb": (None, [ch, vp, dp, i, i, i]), "ft_execute_cheb2tet": (None, [ch, vp, dp, i, i, i]),
+        "ft_execute_tet_hi2lo": (None, [vp, vp, dp, i, i]), "ft_execute_tet_lo2hi": (None, [vp, vp, dp, i, i]),
+        "ft_b200_execute_tet_dev": (i, [vp, i, ch, vp, i, i, i, vp]),
+        "ft_b200_tet_rotations_dev": (i, [vp, i, vp, i, i, vp]),
     }
     for name in ("sph_synthesis", "sph_analysis", "sphv_synthesis", "sphv_analysis"):
         sig["ft_execute_" + name] = (None, [ch, vp, dp, i, i])
@@ -328,6 +335,70 @@ def execute_spin_dev(P: SpinHarmonicPlan, forward: bool, trans: str, ptr: int, N
 def spin_rotations_dev(SRP: SpinRotationPlan, hi2lo: bool, ptr: int, M: int, stream: int = 0) -> None:
     """The spin rotation stage alone on a device matrix (interleaved complex)."""
     st = lib.ft_b200_spin_rotations_dev(SRP.ptr, 1 if hi2lo else 0, C.c_void_p(ptr), M, C.c_void_p(stream))
+    if st != 0:
+        _check()
+
+
+class TetPlan(HarmonicPlan):
+    """Owns a tetrahedral ``ft_harmonic_plan *`` (reference: src/drivers.c:1173-1257); tensors are
+    n x n x n float64 in Fortran order."""
+
+    def __init__(self, ptr: int, n: int, params):
+        super().__init__(ptr, "tet", n, params)
+        self.RP = C.cast(C.c_void_p(ptr), C.POINTER(C.c_void_p))[0]   # the plan's RP member: its two rotation plans
+
+    @property
+    def M(self) -> int:
+        return self.n
+
+
+def plan_tet2cheb(n: int, alpha: float, beta: float, gamma: float, delta: float) -> TetPlan:
+    p = lib.ft_plan_tet2cheb(n, alpha, beta, gamma, delta)
+    if not p:
+        _check()
+        raise FTB200Error(-1, "plan creation failed")
+    return TetPlan(p, n, (alpha, beta, gamma, delta))
+
+
+def _tensor(A: np.ndarray) -> np.ndarray:
+    if not (isinstance(A, np.ndarray) and A.dtype == np.float64 and A.ndim == 3 and A.flags.f_contiguous and A.flags.writeable):
+        raise TypeError("A must be a writeable 3-D float64 numpy array in Fortran order")
+    return A
+
+
+def _exec_tet(fname: str, trans: str, P: TetPlan, A: np.ndarray):
+    A = _tensor(A)
+    N, L, M = A.shape
+    getattr(lib, fname)(trans.encode(), P.ptr, A.ctypes.data_as(C.POINTER(C.c_double)), N, L, M)
+    _check()
+
+
+def execute_tet2cheb(trans, P, A): _exec_tet("ft_execute_tet2cheb", trans, P, A)
+def execute_cheb2tet(trans, P, A): _exec_tet("ft_execute_cheb2tet", trans, P, A)
+
+
+def _exec_tet_rot(fname, P: TetPlan, A: np.ndarray):
+    """ft_execute_tet_hi2lo / lo2hi with the plan's two rotation plans."""
+    A = _tensor(A)
+    rp = C.cast(C.c_void_p(P.RP), C.POINTER(C.c_void_p))
+    getattr(lib, fname)(rp[0], rp[1], A.ctypes.data_as(C.POINTER(C.c_double)), A.shape[1], A.shape[2])
+    _check()
+
+
+def execute_tet_hi2lo(P, A): _exec_tet_rot("ft_execute_tet_hi2lo", P, A)
+def execute_tet_lo2hi(P, A): _exec_tet_rot("ft_execute_tet_lo2hi", P, A)
+
+
+def execute_tet_dev(P: TetPlan, forward: bool, trans: str, ptr: int, N: int, L: int, M: int, stream: int = 0) -> None:
+    """Tetrahedral transform on a device tensor (N x L x M, column-major), asynchronous."""
+    st = lib.ft_b200_execute_tet_dev(P.ptr, 1 if forward else 0, trans.encode(), C.c_void_p(ptr), N, L, M, C.c_void_p(stream))
+    if st != 0:
+        _check()
+
+
+def tet_rotations_dev(P: TetPlan, hi2lo: bool, ptr: int, L: int, M: int, stream: int = 0) -> None:
+    """The plan's tetrahedral rotation stage alone on a device tensor."""
+    st = lib.ft_b200_tet_rotations_dev(P.ptr, 1 if hi2lo else 0, C.c_void_p(ptr), L, M, C.c_void_p(stream))
     if st != 0:
         _check()
 

@@ -843,7 +843,8 @@ ft_harmonic_plan * ft_plan_disk2cxf(const int n, const double alpha, const doubl
 void ft_destroy_harmonic_plan(ft_harmonic_plan * P) {
     HarmonicPlan * H = as_plan(P);
     if (!H) {
-        rect_plan_destroy(P);   // a Dunkl-Xu plan (rectdisk.cu), or nothing of this library
+        // a Dunkl-Xu plan (rectdisk.cu), a tetrahedral plan (tet.cu), or nothing of this library
+        if (!rect_plan_destroy(P)) tet_plan_destroy(P);
         return;
     }
     if (H->stream) { cudaStreamSynchronize(H->stream); cudaStreamDestroy(H->stream); }

@@ -11,7 +11,7 @@ from __future__ import annotations
 
 import numpy as np
 
-__all__ = ["layout_cols", "sphrand", "trirand", "diskrand", "rectdiskrand", "rand_layout"]
+__all__ = ["layout_cols", "sphrand", "trirand", "diskrand", "rectdiskrand", "tetrand", "rand_layout"]
 
 _STEP = {"sph": 2, "tri": 1, "disk": 4, "rect": 1}
 
@@ -52,6 +52,20 @@ def diskrand(n: int, seed: int) -> np.ndarray:
 def rectdiskrand(n: int, seed: int) -> np.ndarray:
     """The Dunkl-Xu layout of src/ftutilities.c:123-129: rows i, columns j < M - i (M = n)."""
     return rand_layout("rect", n, seed)
+
+
+def tetrand(n: int, seed: int, L: int = None, M: int = None) -> np.ndarray:
+    """n x L x M float64 tensor, Fortran order, in tetrand's layout (src/ftutilities.c:140-147):
+    entry (i, l, m) with l < L - m and i < n - l - m is U(-1, 1) from the counter at its
+    column-major index i + n l + n L m, the rest zero (L = M = n by default)."""
+    L = n if L is None else L
+    M = n if M is None else M
+    i = np.arange(n, dtype=np.int64)[:, None, None]
+    l = np.arange(L, dtype=np.int64)[None, :, None]
+    m = np.arange(M, dtype=np.int64)[None, None, :]
+    on = (l < L - m) & (i < n - l - m)
+    e = i + n * l + n * L * m
+    return np.asfortranarray(np.where(on, _u_pm1(seed, e), 0.0))
 
 
 def _u_pm1(seed: int, idx: np.ndarray) -> np.ndarray:

@@ -114,6 +114,15 @@ ft_harmonic_plan * ft_plan_rectdisk2cheb(const int n, const double beta);
 void ft_execute_rectdisk2cheb(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M);
 void ft_execute_cheb2rectdisk(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M);
 
+/* replaces ft_plan_tet2cheb, src/drivers.c:1173-1195: tetrahedral harmonics; NRP = 2 rotation
+ * plans (triangle tables), NP = 3 connection pairs (host copies) */
+ft_harmonic_plan * ft_plan_tet2cheb(const int n, const double alpha, const double beta, const double gamma, const double delta);
+/* replace ft_execute_tet2cheb / ft_execute_cheb2tet, src/drivers.c:1197-1257: A is N x L x M
+ * column-major (entry (i, l, m) at i + N l + N L m); L and M must equal N, as in the
+ * reference's tests (its multiplies along l and m are n x n) */
+void ft_execute_tet2cheb(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int L, const int M);
+void ft_execute_cheb2tet(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int L, const int M);
+
 /* replaces ft_destroy_harmonic_plan, src/drivers.c:793-814 (every plan kind above) */
 void ft_destroy_harmonic_plan(ft_harmonic_plan * P);
 
@@ -193,6 +202,11 @@ void ft_execute_tri_hi2lo(const ft_rotation_plan * RP, double * A, double * B, c
 void ft_execute_tri_lo2hi(const ft_rotation_plan * RP, double * A, double * B, const int M);
 void ft_execute_disk_hi2lo(const ft_rotation_plan * RP, double * A, double * B, const int M);
 void ft_execute_disk_lo2hi(const ft_rotation_plan * RP, double * A, double * B, const int M);
+/* replace ft_execute_tet_hi2lo / lo2hi, src/drivers.c:510-528: RP1, RP2 triangle plans of one n
+ * (ft_plan_rottriangle(n, alpha, beta, gamma + delta + 1) and (n, beta, gamma, delta) for the
+ * tetrahedral transform); A is n x L x M with L <= n */
+void ft_execute_tet_hi2lo(const ft_rotation_plan * RP1, const ft_rotation_plan * RP2, double * A, const int L, const int M);
+void ft_execute_tet_lo2hi(const ft_rotation_plan * RP1, const ft_rotation_plan * RP2, double * A, const int L, const int M);
 /* replace ft_execute_rectdisk_hi2lo / lo2hi, src/drivers.c:488-508 (order m on column m) */
 void ft_execute_rectdisk_hi2lo(const ft_rotation_plan * RP, double * A, double * B, const int M);
 void ft_execute_rectdisk_lo2hi(const ft_rotation_plan * RP, double * A, double * B, const int M);
@@ -221,6 +235,10 @@ int ft_b200_rotations_dev(const ft_rotation_plan * RP, int hi2lo, double * dA, i
 /* Spin-weighted transforms on device memory: dA holds 2 N M doubles (interleaved
  * complex); forward = 1: spinsph2fourier, 0: fourier2spinsph. */
 int ft_b200_execute_spin_dev(const ft_spin_harmonic_plan * P, int forward, char TRANS, double * dA, int N, int M, void * stream);
+/* Tetrahedral transforms on device memory (forward = 1: tet2cheb, 0: cheb2tet), and the
+ * plan's rotation stage alone (hi2lo = 1: ft_execute_tet_hi2lo with the plan's two tables). */
+int ft_b200_execute_tet_dev(const ft_harmonic_plan * P, int forward, char TRANS, double * dA, int N, int L, int M, void * stream);
+int ft_b200_tet_rotations_dev(const ft_harmonic_plan * P, int hi2lo, double * dA, int L, int M, void * stream);
 /* The spin rotation stage alone (hi2lo = 1: ft_execute_spinsph_hi2lo; 0: _lo2hi). */
 int ft_b200_spin_rotations_dev(const ft_spin_rotation_plan * SRP, int hi2lo, double * dA, int M, void * stream);
 

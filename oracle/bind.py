@@ -64,6 +64,12 @@ def _ptr(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
+def _ptr3(a: np.ndarray):
+    """float64 Fortran-order array of any rank as a double pointer."""
+    assert a.dtype == np.float64 and a.flags.f_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
 def _cptr(a: np.ndarray):
     """complex128 Fortran-order array as interleaved doubles (the ft_complex layout)."""
     assert a.dtype == np.complex128 and a.flags.f_contiguous
@@ -75,6 +81,12 @@ class _OraclePlan(C.Structure):
                 ("c", C.POINTER(C.c_double)), ("P", C.POINTER(C.c_double) * 3),
                 ("Pinv", C.POINTER(C.c_double) * 3), ("alpha", C.c_double),
                 ("beta", C.c_double), ("gamma", C.c_double)]
+
+
+class _OracleTetPlan(C.Structure):
+    _fields_ = [("n", C.c_int), ("rp1", C.c_void_p), ("rp2", C.c_void_p),
+                ("P", C.POINTER(C.c_double) * 3), ("Pinv", C.POINTER(C.c_double) * 3),
+                ("alpha", C.c_double), ("beta", C.c_double), ("gamma", C.c_double), ("delta", C.c_double)]
 
 
 class Oracle:
@@ -124,9 +136,44 @@ class Oracle:
         for f in ("oracle_execute_spinsph_hi2lo", "oracle_execute_spinsph_lo2hi"):
             getattr(L, f).argtypes = [sp, dp, C.c_int]
         L.oracle_fill_spin.argtypes = [C.c_int, C.c_int, C.c_int, C.c_ulonglong, dp]
+        L.oracle_plan_tet2cheb.restype = sp
+        L.oracle_plan_tet2cheb.argtypes = [C.c_int] + [C.c_double] * 4 + [C.c_int]
+        L.oracle_destroy_tet_plan.argtypes = [sp]
+        for f in ("oracle_execute_tet_hi2lo", "oracle_execute_tet_lo2hi"):
+            getattr(L, f).argtypes = [sp, dp, C.c_int, C.c_int]
+        L.oracle_execute_tet.argtypes = [sp, C.c_int, C.c_char, dp, C.c_int, C.c_int, C.c_int]
+        L.oracle_fill_tet.argtypes = [C.c_int, C.c_int, C.c_int, C.c_ulonglong, dp]
 
     def set_fused(self, fused: bool):
         self.lib.oracle_set_fused(1 if fused else 0)
+
+    # tetrahedral harmonics: float64 N x L x M arrays in Fortran order
+    def tet_plan(self, n: int, alpha=0.0, beta=0.0, gamma=0.0, delta=0.0, connections: bool = True):
+        return self.lib.oracle_plan_tet2cheb(n, alpha, beta, gamma, delta, 1 if connections else 0)
+
+    def tet_destroy(self, P):
+        self.lib.oracle_destroy_tet_plan(P)
+
+    def tet_connection(self, P):
+        p = C.cast(C.c_void_p(P), C.POINTER(_OracleTetPlan)).contents
+        n = p.n
+        get = lambda q: np.ctypeslib.as_array(q, shape=(n * n,)).reshape(n, n, order="F").copy()
+        return [get(p.P[i]) for i in range(3)], [get(p.Pinv[i]) for i in range(3)]
+
+    def tet_execute(self, P, forward: bool, trans: str, A: np.ndarray):
+        N, L, M = A.shape
+        self.lib.oracle_execute_tet(P, 1 if forward else 0, trans.encode(), _ptr3(A), N, L, M)
+
+    def tet_hi2lo(self, P, A: np.ndarray):
+        self.lib.oracle_execute_tet_hi2lo(P, _ptr3(A), A.shape[1], A.shape[2])
+
+    def tet_lo2hi(self, P, A: np.ndarray):
+        self.lib.oracle_execute_tet_lo2hi(P, _ptr3(A), A.shape[1], A.shape[2])
+
+    def tet_fill(self, N: int, L: int, M: int, seed: int) -> np.ndarray:
+        A = np.zeros((N, L, M), order="F")
+        self.lib.oracle_fill_tet(N, L, M, seed, _ptr3(A))
+        return A
 
     # spin-weighted spherical harmonics: complex128 N x M arrays in Fortran order (the
     # interleaved (re, im) layout of ft_complex)
@@ -244,6 +291,14 @@ class Reference:
         L.ft_plan_rectdisk2cheb.restype = HP
         L.ft_plan_rectdisk2cheb.argtypes = [C.c_int, C.c_double]
         L.ft_destroy_harmonic_plan.argtypes = [HP]
+        L.ft_plan_tet2cheb.restype = HP
+        L.ft_plan_tet2cheb.argtypes = [C.c_int] + [C.c_double] * 4
+        for f in ("ft_execute_tet2cheb", "ft_execute_cheb2tet"):
+            getattr(L, f).argtypes = [C.c_char, HP, C.POINTER(C.c_double), C.c_int, C.c_int, C.c_int]
+        L.ft_plan_rottriangle.restype = C.c_void_p
+        L.ft_plan_rottriangle.argtypes = [C.c_int] + [C.c_double] * 3
+        for f in ("ft_execute_tet_hi2lo", "ft_execute_tet_lo2hi"):
+            getattr(L, f).argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_int, C.c_int]
         L.ft_plan_rotrectdisk.restype = C.c_void_p
         L.ft_plan_rotrectdisk.argtypes = [C.c_int, C.c_double]
         L.ft_destroy_rotation_plan.argtypes = [C.c_void_p]
@@ -291,6 +346,25 @@ class Reference:
         f = self.lib.ft_execute_rectdisk_hi2lo if hi2lo else self.lib.ft_execute_rectdisk_lo2hi
         f(RP, _ptr(A), _ptr(B), A.shape[1])
         self.lib.ft_destroy_rotation_plan(RP)
+
+    def tet_plan(self, n: int, alpha=0.0, beta=0.0, gamma=0.0, delta=0.0):
+        return self.lib.ft_plan_tet2cheb(n, alpha, beta, gamma, delta)
+
+    def tet_execute(self, P, forward: bool, trans: str, A: np.ndarray):
+        N, L, M = A.shape
+        f = self.lib.ft_execute_tet2cheb if forward else self.lib.ft_execute_cheb2tet
+        f(trans.encode(), P, _ptr3(A), N, L, M)
+
+    def tet_rotations(self, n: int, params, hi2lo: bool, A: np.ndarray):
+        """The tetrahedral rotation stage alone (ft_execute_tet_hi2lo / lo2hi) with the plan's two
+        triangle tables (src/drivers.c:1176-1177)."""
+        a, b, g, d = params
+        RP1 = self.lib.ft_plan_rottriangle(n, a, b, g + d + 1.0)
+        RP2 = self.lib.ft_plan_rottriangle(n, b, g, d)
+        f = self.lib.ft_execute_tet_hi2lo if hi2lo else self.lib.ft_execute_tet_lo2hi
+        f(RP1, RP2, _ptr3(A), A.shape[1], A.shape[2])
+        self.lib.ft_destroy_rotation_plan(RP1)
+        self.lib.ft_destroy_rotation_plan(RP2)
 
     def set_num_threads(self, t: int):
         self.lib.ft_set_num_threads(t)

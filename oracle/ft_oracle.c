@@ -946,3 +946,143 @@ void oracle_fill_spin(int N, int M, int s, unsigned long long seed, double * A) 
             A[2 * e + 1] = on ? u_pm1(seed, 2 * e + 1) : 0.0;
         }
 }
+
+/* ---------------------------------------------------------------------------
+ * Tetrahedral harmonics.
+ * ------------------------------------------------------------------------- */
+
+/* src/drivers.c:1173-1195 */
+oracle_tet_plan * oracle_plan_tet2cheb(int n, double alpha, double beta, double gamma, double delta, int connections) {
+    oracle_tet_plan * P = calloc(1, sizeof(oracle_tet_plan));
+    P->n = n;
+    P->alpha = alpha; P->beta = beta; P->gamma = gamma; P->delta = delta;
+    P->rp1 = oracle_plan_rotations(ORACLE_TRI, n, alpha, beta, gamma + delta + 1.0);
+    P->rp2 = oracle_plan_rotations(ORACLE_TRI, n, beta, gamma, delta);
+    if (connections) {
+        P->P[0] = oracle_plan_jacobi_to_jacobi(1, 1, n, beta + gamma + delta + 2.0, alpha, -0.5, -0.5);
+        P->P[1] = oracle_plan_jacobi_to_jacobi(1, 1, n, gamma + delta + 1.0, beta, -0.5, -0.5);
+        P->P[2] = oracle_plan_jacobi_to_jacobi(1, 1, n, delta, gamma, -0.5, -0.5);
+        P->Pinv[0] = oracle_plan_jacobi_to_jacobi(1, 1, n, -0.5, -0.5, beta + gamma + delta + 2.0, alpha);
+        P->Pinv[1] = oracle_plan_jacobi_to_jacobi(1, 1, n, -0.5, -0.5, gamma + delta + 1.0, beta);
+        P->Pinv[2] = oracle_plan_jacobi_to_jacobi(1, 1, n, -0.5, -0.5, delta, gamma);
+    }
+    return P;
+}
+
+void oracle_destroy_tet_plan(oracle_tet_plan * P) {
+    if (!P) return;
+    oracle_destroy_plan(P->rp1);
+    oracle_destroy_plan(P->rp2);
+    for (int i = 0; i < 3; i++) { free(P->P[i]); free(P->Pinv[i]); }
+    free(P);
+}
+
+/* src/rotations.c:297-321 (ft_kernel_tet_hi2lo / lo2hi): sweeps across the columns of the
+ * N x L slab of order m, every row rotated alike */
+static void kernel_tet(const oracle_plan * RP, int L, int m, double * A, int hi2lo) {
+    int n = RP->n;
+    const double * s = RP->s, * c = RP->c;
+    if (hi2lo) {
+        for (int j = m - 1; j >= 0; j--)
+            for (int l = L - 2 - j; l >= 0; l--) {
+                double S = s[tri_idx(n, l, j)], C = c[tri_idx(n, l, j)];
+                for (int k = 0; k < n; k++) givens(S, C, A + k + (size_t) n * l, A + k + (size_t) n * (l + 1));
+            }
+    } else {
+        for (int j = 0; j < m; j++)
+            for (int l = 0; l <= L - 2 - j; l++) {
+                double S = s[tri_idx(n, l, j)], C = c[tri_idx(n, l, j)];
+                for (int k = 0; k < n; k++) givens_t(S, C, A + k + (size_t) n * l, A + k + (size_t) n * (l + 1));
+            }
+    }
+}
+
+/* src/drivers.c:510-528: slab m: the tri sweeps of order l + m down column l (l < L - m),
+ * then the sweeps across the slab (lo2hi: the reverse) */
+static void execute_tet_rot(const oracle_tet_plan * P, double * A, int L, int M, int hi2lo) {
+    int N = P->n;
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (int m = 0; m < M; m++) {
+        double * slab = A + (size_t) N * L * m;
+        if (hi2lo) {
+            for (int l = 0; l < L - m; l++) oracle_kernel_hi2lo(P->rp1, 0, l + m, slab + (size_t) N * l, 1);
+            kernel_tet(P->rp2, L, m, slab, 1);
+        } else {
+            kernel_tet(P->rp2, L, m, slab, 0);
+            for (int l = 0; l < L - m; l++) oracle_kernel_lo2hi(P->rp1, 0, l + m, slab + (size_t) N * l, 1);
+        }
+    }
+}
+
+void oracle_execute_tet_hi2lo(const oracle_tet_plan * P, double * A, int L, int M) { execute_tet_rot(P, A, L, M, 1); }
+void oracle_execute_tet_lo2hi(const oracle_tet_plan * P, double * A, int L, int M) { execute_tet_rot(P, A, L, M, 0); }
+
+/* src/drivers.c:26-54: entry (i, l, m) times r if m == 0, r if l == 0, r if i == 0, then g,
+ * in that order */
+static void cheb_normalize_3d(double * A, int N, int L, int M, int transposed) {
+    const double r = transposed ? M_SQRT2 : M_SQRT1_2;
+    const double g = transposed ? 1.968701243215302468 : 0.507949087473927758;   /* (pi/2)^1.5, (2/pi)^1.5: src/ftinternal.h:59-60 */
+    for (int l = 0; l < L; l++)
+        for (int i = 0; i < N; i++) A[i + (size_t) l * N] *= r;
+    for (int m = 0; m < M; m++) {
+        for (int i = 0; i < N; i++) A[i + (size_t) m * L * N] *= r;
+        for (int l = 0; l < L; l++) {
+            A[(l + (size_t) m * L) * N] *= r;
+            for (int i = 0; i < N; i++) A[i + (l + (size_t) m * L) * N] *= g;
+        }
+    }
+}
+
+/* x <- op(U) x along the m axis of every (i, l) fibre (stride N L): cblas_dtrmv on the fibres */
+static void trmv_fibres(char trans, int N, int L, int M, const double * U, double * A) {
+    #pragma omp parallel
+    {
+        double * x = malloc(sizeof(double) * M), * y = malloc(sizeof(double) * M);
+        #pragma omp for schedule(static)
+        for (int f = 0; f < N * L; f++) {
+            for (int m = 0; m < M; m++) x[m] = A[f + (size_t) N * L * m];
+            for (int i = 0; i < M; i++) {
+                double acc = 0.0;
+                if (trans == 'N') for (int k = i; k < M; k++) acc += U[i + (size_t) k * N] * x[k];
+                else              for (int k = 0; k <= i; k++) acc += U[k + (size_t) i * N] * x[k];
+                y[i] = acc;
+            }
+            for (int m = 0; m < M; m++) A[f + (size_t) N * L * m] = y[m];
+        }
+        free(x); free(y);
+    }
+}
+
+/* src/drivers.c:1197-1257 (N = L = M, as in the reference's tests); each multiply is skipped
+ * where the reference skips it (its parameters make it the identity) */
+void oracle_execute_tet(const oracle_tet_plan * P, int forward, char TRANS, double * A, int N, int L, int M) {
+    if (TRANS != 'N' && TRANS != 'T') return;
+    const double a = P->alpha, b = P->beta, g = P->gamma, d = P->delta;
+    const int u0 = (b + g + d != -2.5) || (a != -0.5);
+    const int u1 = (g + d != -1.5) || (b != -0.5);
+    const int u2 = (d != -0.5) || (g != -0.5);
+    double * const * U = forward ? P->P : P->Pinv;
+    if ((forward && TRANS == 'N') || (!forward && TRANS == 'T')) {
+        char t = forward ? 'N' : 'T';
+        oracle_execute_tet_hi2lo(P, A, L, M);
+        if (u0) oracle_trmm('L', t, N, U[0], L * M, A, N);
+        if (u1) for (int m = 0; m < M; m++) oracle_trmm('R', forward ? 'T' : 'N', L, U[1], N, A + (size_t) N * L * m, N);
+        if (u2) trmv_fibres(forward ? 'T' : 'N', N, L, M, U[2], A);
+        cheb_normalize_3d(A, N, L, M, !forward);
+    } else {
+        cheb_normalize_3d(A, N, L, M, !forward);
+        if (u2) trmv_fibres(forward ? 'N' : 'T', N, L, M, U[2], A);
+        if (u1) for (int m = 0; m < M; m++) oracle_trmm('R', forward ? 'N' : 'T', L, U[1], N, A + (size_t) N * L * m, N);
+        if (u0) oracle_trmm('L', forward ? 'T' : 'N', N, U[0], L * M, A, N);
+        oracle_execute_tet_lo2hi(P, A, L, M);
+    }
+}
+
+void oracle_fill_tet(int N, int L, int M, unsigned long long seed, double * A) {
+    for (int m = 0; m < M; m++)
+        for (int l = 0; l < L; l++)
+            for (int i = 0; i < N; i++) {
+                size_t e = (size_t) i + (size_t) N * l + (size_t) N * L * m;
+                A[e] = (l < L - m && i < N - l - m) ? u_pm1(seed, e) : 0.0;
+            }
+}

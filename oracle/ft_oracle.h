@@ -88,6 +88,25 @@ void oracle_execute_spinsph_lo2hi(const oracle_spin_plan * P, double * A, int M)
 void oracle_execute_spin(const oracle_spin_plan * P, int forward, char TRANS, double * A, int N, int M);
 void oracle_fill_spin(int N, int M, int s, unsigned long long seed, double * A);
 
+/* Tetrahedral harmonics (src/rotations.c:297-321, src/drivers.c:510-528, 1173-1257).  Tensors
+ * are N x L x M column-major (entry (i, l, m) at i + N l + N L m). */
+typedef struct {
+    int n;
+    oracle_plan * rp1;   /* tri table (alpha, beta, gamma + delta + 1): the sweeps down each (l, m) column */
+    oracle_plan * rp2;   /* tri table (beta, gamma, delta): the sweeps across the columns of a slab */
+    double * P[3], * Pinv[3];
+    double alpha, beta, gamma, delta;
+} oracle_tet_plan;
+/* connections = 0: rotation tables only */
+oracle_tet_plan * oracle_plan_tet2cheb(int n, double alpha, double beta, double gamma, double delta, int connections);
+void oracle_destroy_tet_plan(oracle_tet_plan * P);
+void oracle_execute_tet_hi2lo(const oracle_tet_plan * P, double * A, int L, int M);
+void oracle_execute_tet_lo2hi(const oracle_tet_plan * P, double * A, int L, int M);
+/* forward = 1: tet2cheb; 0: cheb2tet */
+void oracle_execute_tet(const oracle_tet_plan * P, int forward, char TRANS, double * A, int N, int L, int M);
+/* tetrand's layout (src/ftutilities.c:140-147): (i, l, m) with l < L - m, i < N - l - m */
+void oracle_fill_tet(int N, int L, int M, unsigned long long seed, double * A);
+
 /* Seeded fills in the reference layouts (src/ftutilities.c:75-129), U(-1,1) from splitmix64
  * (rect: rows i, columns j < M - i, like tri). */
 void oracle_fill(int kind, int N, int M, unsigned long long seed, double * A);

@@ -15,9 +15,12 @@ seeded inputs and stores inputs and outputs as compressed .npz files:
     spinsphrand's layout, files spin_n<n>_s<s>.npz;
   * Dunkl-Xu (rectangularised disk) transforms (ft_execute_rectdisk2cheb /
     ft_execute_cheb2rectdisk, M = N), their rotation stages (ft_execute_rectdisk_hi2lo /
-    _lo2hi) and the six connection matrices, files rect_n<n>_b<beta>.npz.
+    _lo2hi) and the six connection matrices, files rect_n<n>_b<beta>.npz;
+  * tetrahedral transforms (ft_execute_tet2cheb / ft_execute_cheb2tet, N = L = M), their
+    rotation stages (ft_execute_tet_hi2lo / _lo2hi) and the six connection matrices, files
+    tet_n<n>_<params>.npz.
 
-    python tests/golden/make_golden.py [sph tri disk spin rect]   (default: all)
+    python tests/golden/make_golden.py [sph tri disk spin rect tet]   (default: all)
 """
 from __future__ import annotations
 
@@ -38,6 +41,7 @@ CASES = [
 ]
 SPIN_CASES = [(8, -2), (17, 0), (17, 1), (16, 3), (33, -1), (12, 4)]
 RECT_CASES = [(8, 0.0), (17, 0.5), (16, -0.25), (33, 1.5)]
+TET_CASES = [(8, (0.0, 0.0, 0.0, 0.0)), (9, (-0.5, -0.5, -0.5, -0.5)), (12, (0.5, -0.25, 0.25, 1.0))]
 SEED = 20261203
 
 
@@ -59,7 +63,7 @@ def main():
         for d in ("hi2lo", "lo2hi"):
             getattr(L, f"ft_execute_{fam}_{d}").argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int]
     L.ft_destroy_rotation_plan.argtypes = [C.c_void_p]
-    families = set(sys.argv[1:]) or {"sph", "tri", "disk", "spin", "rect"}
+    families = set(sys.argv[1:]) or {"sph", "tri", "disk", "spin", "rect", "tet"}
     for kind, n, params in CASES:
         if kind not in families:
             continue
@@ -127,6 +131,28 @@ def main():
                 R.rect_rotations(n, beta, d == "hi2lo", B)
                 out["rot_" + d] = B
             path = os.path.join(HERE, case_name("rect", n, (beta,)) + ".npz")
+            np.savez_compressed(path, **out)
+            print("wrote", os.path.relpath(path), A.shape)
+    if "tet" in families:
+        from fasttransforms_b200.utilities import tetrand
+        for n, params in TET_CASES:
+            A = tetrand(n, SEED)
+            P = R.tet_plan(n, *params)
+            out = {"A": A, "params": np.array(params, dtype=np.float64)}
+            for fwd in (True, False):
+                for tr in "NT":
+                    B = A.copy(order="F")
+                    R.tet_execute(P, fwd, tr, B)
+                    out[("fwd" if fwd else "bwd") + "_" + tr] = B
+            Ps, Pinvs = R.connection(P, n)
+            for i in range(3):
+                out[f"P{i}"], out[f"Pinv{i}"] = Ps[i], Pinvs[i]
+            R.destroy(P)
+            for d in ("hi2lo", "lo2hi"):
+                B = A.copy(order="F")
+                R.tet_rotations(n, params, d == "hi2lo", B)
+                out["rot_" + d] = B
+            path = os.path.join(HERE, case_name("tet", n, params) + ".npz")
             np.savez_compressed(path, **out)
             print("wrote", os.path.relpath(path), A.shape)
 
