@@ -41,6 +41,7 @@ __all__ = [
     "execute_rectdisk_hi2lo", "execute_rectdisk_lo2hi", "rectdiskrand",
     "TetPlan", "plan_tet2cheb", "execute_tet2cheb", "execute_cheb2tet", "execute_tet_hi2lo", "execute_tet_lo2hi",
     "execute_tet_dev", "tet_rotations_dev", "tetrand",
+    "plan_ann2cxf", "execute_ann2cxf", "execute_cxf2ann", "plan_rotannulus",
     "SPH", "TRI", "DISK",
 ]
 
@@ -93,6 +94,7 @@ def _load() -> C.CDLL:
         "ft_b200_spin_rotations_dev": (i, [vp, i, vp, i, vp]),
         "ft_plan_rectdisk2cheb": (vp, [i, d]), "ft_plan_rotrectdisk": (vp, [i, d]),
         "ft_plan_tet2cheb": (vp, [i, d, d, d, d]),
+        "ft_plan_ann2cxf": (vp, [i, d, d, d, d]), "ft_plan_rotannulus": (vp, [i, d, d, d, d]),
         "ft_execute_tet2cheb": (None, [ch, vp, dp, i, i, i]), "ft_execute_cheb2tet": (None, [ch, vp, dp, i, i, i]),
         "ft_execute_tet_hi2lo": (None, [vp, vp, dp, i, i]), "ft_execute_tet_lo2hi": (None, [vp, vp, dp, i, i]),
         "ft_b200_execute_tet_dev": (i, [vp, i, ch, vp, i, i, i, vp]),
@@ -101,7 +103,7 @@ def _load() -> C.CDLL:
     for name in ("sph_synthesis", "sph_analysis", "sphv_synthesis", "sphv_analysis"):
         sig["ft_execute_" + name] = (None, [ch, vp, dp, i, i])
     for name in ("sph2fourier", "fourier2sph", "tri2cheb", "cheb2tri", "disk2cxf", "cxf2disk", "sphv2fourier", "fourier2sphv",
-                 "rectdisk2cheb", "cheb2rectdisk"):
+                 "rectdisk2cheb", "cheb2rectdisk", "ann2cxf", "cxf2ann"):
         sig["ft_execute_" + name] = (None, [ch, vp, dp, i, i])
     for fam in ("sph", "tri", "disk", "rectdisk"):
         for d_ in ("hi2lo", "lo2hi"):
@@ -204,6 +206,11 @@ def plan_tri2cheb(n: int, alpha: float, beta: float, gamma: float) -> HarmonicPl
 
 def plan_disk2cxf(n: int, alpha: float, beta: float) -> HarmonicPlan:
     return _plan("disk", n, lib.ft_plan_disk2cxf(n, alpha, beta), (alpha, beta))
+
+
+def plan_ann2cxf(n: int, alpha: float, beta: float, gamma: float, rho: float) -> HarmonicPlan:
+    """Annulus plan (reference: src/drivers.c:1023-1071; gamma must be 0); the disk layout, M = 4n - 3."""
+    return _plan("disk", n, lib.ft_plan_ann2cxf(n, alpha, beta, gamma, rho), (alpha, beta, gamma, rho))
 
 
 def plan_rectdisk2cheb(n: int, beta: float) -> HarmonicPlan:
@@ -432,6 +439,8 @@ def execute_cxf2disk(trans, P, A, N=None, M=None): _exec_host("ft_execute_cxf2di
 def execute_sphv2fourier(trans, P, A, N=None, M=None): _exec_host("ft_execute_sphv2fourier", trans, P, A, N, M)
 def execute_fourier2sphv(trans, P, A, N=None, M=None): _exec_host("ft_execute_fourier2sphv", trans, P, A, N, M)
 def execute_rectdisk2cheb(trans, P, A, N=None, M=None): _exec_host("ft_execute_rectdisk2cheb", trans, P, A, N, M)
+def execute_ann2cxf(trans, P, A, N=None, M=None): _exec_host("ft_execute_ann2cxf", trans, P, A, N, M)
+def execute_cxf2ann(trans, P, A, N=None, M=None): _exec_host("ft_execute_cxf2ann", trans, P, A, N, M)
 def execute_cheb2rectdisk(trans, P, A, N=None, M=None): _exec_host("ft_execute_cheb2rectdisk", trans, P, A, N, M)
 
 
@@ -454,6 +463,15 @@ def plan_rotdisk(n: int, alpha: float, beta: float) -> RotationPlan:
     if not p:
         _check()
     return RotationPlan(p, "disk", n, (alpha, beta))
+
+
+def plan_rotannulus(n: int, alpha: float, beta: float, gamma: float, rho: float) -> RotationPlan:
+    """A disk-kind rotation plan with the annulus table (use execute_disk_hi2lo / lo2hi)."""
+    p = lib.ft_plan_rotannulus(n, alpha, beta, gamma, rho)
+    if not p:
+        _check()
+        raise FTB200Error(-1, "plan creation failed")
+    return RotationPlan(p, "disk", n, (alpha, beta, gamma, rho))
 
 
 def plan_rotrectdisk(n: int, beta: float) -> RotationPlan:

@@ -844,7 +844,7 @@ void ft_destroy_harmonic_plan(ft_harmonic_plan * P) {
     HarmonicPlan * H = as_plan(P);
     if (!H) {
         // a Dunkl-Xu plan (rectdisk.cu), a tetrahedral plan (tet.cu), or nothing of this library
-        if (!rect_plan_destroy(P)) tet_plan_destroy(P);
+        if (!rect_plan_destroy(P) && !tet_plan_destroy(P)) ann_plan_destroy(P);
         return;
     }
     if (H->stream) { cudaStreamSynchronize(H->stream); cudaStreamDestroy(H->stream); }
@@ -908,8 +908,10 @@ int ft_b200_execute_dev(const ft_harmonic_plan * P, int forward, char TRANS, dou
     clear_error();
     HarmonicPlan * H = as_plan(P);
     if (!H) {
-        const int r = rect_execute_dev(P, forward != 0, TRANS, dA, N, M, static_cast<cudaStream_t>(stream));
+        int r = rect_execute_dev(P, forward != 0, TRANS, dA, N, M, static_cast<cudaStream_t>(stream));
         if (r >= 0) return r;   // a Dunkl-Xu plan (rectdisk.cu)
+        r = ann_execute_dev(P, forward != 0, TRANS, dA, N, M, static_cast<cudaStream_t>(stream));
+        if (r >= 0) return r;   // an annulus plan (ann.cu)
         set_error(FT_B200_EINVAL, "not a plan created by this library");
         return t_status;
     }

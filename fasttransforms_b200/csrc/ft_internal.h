@@ -245,6 +245,9 @@ bool rotation_sweeps(ft_rotation_plan * RP, bool hi2lo, const double * in, doubl
 bool rect_plan_destroy(ft_harmonic_plan * P);
 // Tetrahedral plans (tet.cu): false when P is not one
 bool tet_plan_destroy(ft_harmonic_plan * P);
+// Annulus plans (ann.cu): false / -1 when P is not one
+bool ann_plan_destroy(ft_harmonic_plan * P);
+int ann_execute_dev(const ft_harmonic_plan * P, bool forward, char TRANS, double * dA, int N, int M, cudaStream_t st);
 int rect_execute_dev(const ft_harmonic_plan * P, bool forward, char TRANS, double * dA, int N, int M, cudaStream_t st);
 // device task list already built for (RP, M), without building one (api.cu)
 bool find_tasks(ft_rotation_plan * RP, int M, const RotTask ** d_tasks, int * ntasks);

@@ -114,6 +114,15 @@ ft_harmonic_plan * ft_plan_rectdisk2cheb(const int n, const double beta);
 void ft_execute_rectdisk2cheb(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M);
 void ft_execute_cheb2rectdisk(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M);
 
+/* replaces ft_plan_ann2cxf, src/drivers.c:1023-1071: annulus harmonics (the disk layout,
+ * M = 4N - 3); gamma must be 0 (the reference implements no other: it warns), else NULL with
+ * FT_B200_EUNSUPPORTED.  NRP = 1, NP = 1; the two modified plans (identity and the Cholesky
+ * factor of t I + X) are held on the device: NMP = 2, MP = NULL. */
+ft_harmonic_plan * ft_plan_ann2cxf(const int n, const double alpha, const double beta, const double gamma, const double rho);
+/* replace ft_execute_ann2cxf / ft_execute_cxf2ann, src/drivers.c:1073-1121 */
+void ft_execute_ann2cxf(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M);
+void ft_execute_cxf2ann(const char TRANS, const ft_harmonic_plan * P, double * A, const int N, const int M);
+
 /* replaces ft_plan_tet2cheb, src/drivers.c:1173-1195: tetrahedral harmonics; NRP = 2 rotation
  * plans (triangle tables), NP = 3 connection pairs (host copies) */
 ft_harmonic_plan * ft_plan_tet2cheb(const int n, const double alpha, const double beta, const double gamma, const double delta);
@@ -190,6 +199,9 @@ ft_rotation_plan * ft_plan_rotsphere(const int n);
 ft_rotation_plan * ft_plan_rottriangle(const int n, const double alpha, const double beta, const double gamma);
 /* replaces ft_plan_rotdisk, src/rotations.c:173-190 */
 ft_rotation_plan * ft_plan_rotdisk(const int n, const double alpha, const double beta);
+/* replaces ft_plan_rotannulus, src/rotations.c:192-268 (gamma = 0): a disk-kind plan (use it with
+ * ft_execute_disk_hi2lo / lo2hi, as the reference's ann2cxf does) */
+ft_rotation_plan * ft_plan_rotannulus(const int n, const double alpha, const double beta, const double gamma, const double rho);
 /* replaces ft_plan_rotrectdisk, src/rotations.c:270-287 */
 ft_rotation_plan * ft_plan_rotrectdisk(const int n, const double beta);
 /* replaces ft_destroy_rotation_plan, src/rotations.c:6-10 */
@@ -219,8 +231,8 @@ void ft_execute_rectdisk_lo2hi(const ft_rotation_plan * RP, double * A, double *
 /* ------------------------------------------------------------------------ */
 enum { FT_B200_SPH = 0, FT_B200_TRI = 1, FT_B200_DISK = 2 };
 
-/* Full transform.  forward = 1: sph2fourier / tri2cheb / disk2cxf / rectdisk2cheb;
- * forward = 0: fourier2sph / cheb2tri / cxf2disk / cheb2rectdisk. */
+/* Full transform.  forward = 1: sph2fourier / tri2cheb / disk2cxf / rectdisk2cheb / ann2cxf;
+ * forward = 0: fourier2sph / cheb2tri / cxf2disk / cheb2rectdisk / cxf2ann. */
 int ft_b200_execute_dev(const ft_harmonic_plan * P, int forward, char TRANS, double * dA, int N, int M, void * stream);
 /* Grid synthesis / analysis on device memory: op 0 sph synthesis, 1 sph analysis,
  * 2 sphv synthesis, 3 sphv analysis (the sequences of the ft_execute_* above, with

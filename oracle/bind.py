@@ -83,6 +83,11 @@ class _OraclePlan(C.Structure):
                 ("beta", C.c_double), ("gamma", C.c_double)]
 
 
+class _OracleAnnPlan(C.Structure):
+    _fields_ = [("disk", C.POINTER(_OraclePlan)), ("rd", C.POINTER(C.c_double)), ("ru", C.POINTER(C.c_double)),
+                ("rho", C.c_double)]
+
+
 class _OracleTetPlan(C.Structure):
     _fields_ = [("n", C.c_int), ("rp1", C.c_void_p), ("rp2", C.c_void_p),
                 ("P", C.POINTER(C.c_double) * 3), ("Pinv", C.POINTER(C.c_double) * 3),
@@ -136,6 +141,11 @@ class Oracle:
         for f in ("oracle_execute_spinsph_hi2lo", "oracle_execute_spinsph_lo2hi"):
             getattr(L, f).argtypes = [sp, dp, C.c_int]
         L.oracle_fill_spin.argtypes = [C.c_int, C.c_int, C.c_int, C.c_ulonglong, dp]
+        AP = C.POINTER(_OracleAnnPlan)
+        L.oracle_plan_ann2cxf.restype = AP
+        L.oracle_plan_ann2cxf.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_int]
+        L.oracle_destroy_ann_plan.argtypes = [AP]
+        L.oracle_execute_ann.argtypes = [AP, C.c_int, C.c_char, dp, C.c_int, C.c_int]
         L.oracle_plan_tet2cheb.restype = sp
         L.oracle_plan_tet2cheb.argtypes = [C.c_int] + [C.c_double] * 4 + [C.c_int]
         L.oracle_destroy_tet_plan.argtypes = [sp]
@@ -146,6 +156,37 @@ class Oracle:
 
     def set_fused(self, fused: bool):
         self.lib.oracle_set_fused(1 if fused else 0)
+
+    # annulus harmonics (gamma = 0): float64 N x (4N - 3) arrays in Fortran order
+    def ann_plan(self, n: int, alpha=0.0, beta=0.0, rho=0.5, connections: bool = True):
+        return self.lib.oracle_plan_ann2cxf(n, alpha, beta, rho, 1 if connections else 0)
+
+    def ann_destroy(self, P):
+        self.lib.oracle_destroy_ann_plan(P)
+
+    def ann_execute(self, P, forward: bool, trans: str, A: np.ndarray):
+        N, M = A.shape
+        self.lib.oracle_execute_ann(P, 1 if forward else 0, trans.encode(), _ptr(A), N, M)
+
+    def ann_hi2lo(self, P, A: np.ndarray):
+        self.lib.oracle_execute_hi2lo(P.contents.disk, _ptr(A), A.shape[1])
+
+    def ann_lo2hi(self, P, A: np.ndarray):
+        self.lib.oracle_execute_lo2hi(P.contents.disk, _ptr(A), A.shape[1])
+
+    def ann_table(self, P):
+        return self.tables(P.contents.disk)
+
+    def ann_connection(self, P):
+        p = P.contents.disk.contents
+        n = p.n
+        get = lambda q: np.ctypeslib.as_array(q, shape=(n * n,)).reshape(n, n, order="F").copy()
+        return get(p.P[0]), get(p.Pinv[0])
+
+    def ann_cholesky(self, P):
+        p = P.contents
+        n = p.disk.contents.n
+        return np.ctypeslib.as_array(p.rd, shape=(n,)).copy(), np.ctypeslib.as_array(p.ru, shape=(max(n - 1, 1),))[: n - 1].copy()
 
     # tetrahedral harmonics: float64 N x L x M arrays in Fortran order
     def tet_plan(self, n: int, alpha=0.0, beta=0.0, gamma=0.0, delta=0.0, connections: bool = True):
@@ -291,6 +332,14 @@ class Reference:
         L.ft_plan_rectdisk2cheb.restype = HP
         L.ft_plan_rectdisk2cheb.argtypes = [C.c_int, C.c_double]
         L.ft_destroy_harmonic_plan.argtypes = [HP]
+        L.ft_plan_ann2cxf.restype = HP
+        L.ft_plan_ann2cxf.argtypes = [C.c_int] + [C.c_double] * 4
+        for f in ("ft_execute_ann2cxf", "ft_execute_cxf2ann"):
+            getattr(L, f).argtypes = [C.c_char, HP, C.POINTER(C.c_double), C.c_int, C.c_int]
+        L.ft_plan_rotannulus.restype = C.POINTER(C.POINTER(C.c_double))
+        L.ft_plan_rotannulus.argtypes = [C.c_int] + [C.c_double] * 4
+        for f in ("ft_execute_disk_hi2lo", "ft_execute_disk_lo2hi"):
+            getattr(L, f).argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int]
         L.ft_plan_tet2cheb.restype = HP
         L.ft_plan_tet2cheb.argtypes = [C.c_int] + [C.c_double] * 4
         for f in ("ft_execute_tet2cheb", "ft_execute_cheb2tet"):
@@ -346,6 +395,31 @@ class Reference:
         f = self.lib.ft_execute_rectdisk_hi2lo if hi2lo else self.lib.ft_execute_rectdisk_lo2hi
         f(RP, _ptr(A), _ptr(B), A.shape[1])
         self.lib.ft_destroy_rotation_plan(RP)
+
+    def ann_plan(self, n: int, alpha=0.0, beta=0.0, rho=0.5):
+        return self.lib.ft_plan_ann2cxf(n, alpha, beta, 0.0, rho)
+
+    def ann_execute(self, P, forward: bool, trans: str, A: np.ndarray):
+        N, M = A.shape
+        f = self.lib.ft_execute_ann2cxf if forward else self.lib.ft_execute_cxf2ann
+        f(trans.encode(), P, _ptr(A), N, M)
+
+    def ann_rotations(self, n: int, alpha: float, beta: float, rho: float, hi2lo: bool, A: np.ndarray):
+        """The annulus rotation stage alone: ft_plan_rotannulus's table through the disk sweeps
+        (ft_execute_disk_hi2lo / lo2hi), as ft_execute_ann2cxf runs it."""
+        RP = self.lib.ft_plan_rotannulus(n, alpha, beta, 0.0, rho)
+        B = np.zeros_like(A)
+        f = self.lib.ft_execute_disk_hi2lo if hi2lo else self.lib.ft_execute_disk_lo2hi
+        f(C.cast(RP, C.c_void_p), _ptr(A), _ptr(B), A.shape[1])
+        self.lib.ft_destroy_rotation_plan(C.cast(RP, C.c_void_p))
+
+    def ann_table(self, n: int, alpha: float, beta: float, rho: float):
+        """ft_plan_rotannulus's sine and cosine tables (the disk packing, n^2 entries)."""
+        RP = self.lib.ft_plan_rotannulus(n, alpha, beta, 0.0, rho)
+        s = np.ctypeslib.as_array(RP[0], shape=(n * n,)).copy()
+        c = np.ctypeslib.as_array(RP[1], shape=(n * n,)).copy()
+        self.lib.ft_destroy_rotation_plan(C.cast(RP, C.c_void_p))
+        return s, c
 
     def tet_plan(self, n: int, alpha=0.0, beta=0.0, gamma=0.0, delta=0.0):
         return self.lib.ft_plan_tet2cheb(n, alpha, beta, gamma, delta)

@@ -10,6 +10,7 @@
  * Build: make -C oracle  ->  oracle/_build/libft_oracle.so
  */
 #define _GNU_SOURCE
+#include <float.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -1085,4 +1086,200 @@ void oracle_fill_tet(int N, int L, int M, unsigned long long seed, double * A) {
                 size_t e = (size_t) i + (size_t) N * l + (size_t) N * L * m;
                 A[e] = (l < L - m && i < N - l - m) ? u_pm1(seed, e) : 0.0;
             }
+}
+
+/* ---------------------------------------------------------------------------
+ * Annulus harmonics (gamma = 0).
+ * ------------------------------------------------------------------------- */
+
+/* src/banded_source.c:1797-1830 (create_jacobi_multiplication, norm = 1) as the three diagonals
+ * of an m x m matrix: d[j] = X(j, j), lo[j] = X(j + 1, j), up[j] = X(j, j + 1); each entry with the
+ * reference's own expression (the lower and upper entries are computed separately) */
+static void jacobi_tridiagonal(int m, double a, double b, double * d, double * lo, double * up) {
+    for (int j = 0; j < m; j++) {
+        double v;
+        if (j == 1) v = 2 * sqrt(((a + 1) * (b + 1)) / ((a + b + 2) * (a + b + 2) * (a + b + 3)));
+        else v = 2 * sqrt((j * (j + a) * (j + b) * (j + a + b)) / ((2 * j + a + b - 1) * (2 * j + a + b) * (2 * j + a + b) * (2 * j + a + b + 1)));
+        if (j >= 1) up[j - 1] = v;
+        if (j == 0) {
+            d[0] = (b - a) / (a + b + 2);
+            if (m > 1) lo[0] = 2 * sqrt(((a + 1) * (b + 1)) / ((a + b + 2) * (a + b + 2) * (a + b + 3)));
+        } else {
+            d[j] = ((b - a) * (a + b)) / ((2 * j + a + b) * (2 * j + a + b + 2));
+            if (j + 1 < m)
+                lo[j] = 2 * sqrt(((j + 1) * (j + a + 1) * (j + b + 1) * (j + a + b + 1)) / ((2 * j + a + b + 1) * (2 * j + a + b + 2) * (2 * j + a + b + 2) * (2 * j + a + b + 3)));
+        }
+    }
+}
+
+/* src/banded_source.c:1415-1425 */
+static void compute_givens(double x, double y, double * c, double * s, double * r) {
+    *r = hypot(x, y);
+    if (*r <= DBL_MIN / DBL_EPSILON) { *c = 1; *s = 0; }
+    else { *c = x / *r; *s = y / *r; }
+}
+
+/* src/banded_source.c:1429-1458: Givens QR of the symmetric tridiagonal (a, b) of size k; R's
+ * diagonals r0, r1, r2 */
+static void tridiagonal_qr(int k, const double * a, const double * b, double * s, double * c, double * r0, double * r1, double * r2) {
+    double r, aip1 = a[0], bip1r = b[0];
+    for (int i = 0; i < k - 2; i++) {
+        compute_givens(aip1, -b[i], c + i, s + i, &r);
+        r0[i] = r;
+        r1[i] = c[i] * bip1r - s[i] * a[i + 1];
+        r2[i] = -s[i] * b[i + 1];
+        aip1 = c[i] * a[i + 1] + s[i] * bip1r;
+        bip1r = c[i] * b[i + 1];
+    }
+    compute_givens(aip1, -b[k - 2], c + k - 2, s + k - 2, &r);
+    r0[k - 2] = r;
+    r1[k - 2] = c[k - 2] * bip1r - s[k - 2] * a[k - 1];
+    r0[k - 1] = c[k - 2] * a[k - 1] + s[k - 2] * bip1r;
+}
+
+/* src/banded_source.c:1609-1619 (R-based branch): (aq, bq) of size k - 1 from (ap, bp) of size k */
+static void jacobi_similarity(int k, const double * r0, const double * r1, const double * ap, const double * bp, double * aq, double * bq) {
+    for (int i = 0; i < k - 2; i++) bq[i] = r0[i + 1] / r0[i] * bp[i];
+    aq[0] = ap[0] + r1[0] / r0[0] * bp[0];
+    for (int i = 1; i < k - 1; i++) aq[i] = (r0[i] * ap[i] + r1[i] * bp[i] - r1[i - 1] * bq[i - 1]) / r0[i];
+}
+
+/* src/banded_source.c:471-498 on the tridiagonal (d, lo, up) of size k: R's diagonal rd and
+ * superdiagonal ru (upper Cholesky factor, R^T R = the matrix) */
+static void tridiagonal_cholesky(int k, double * d, const double * lo, const double * up, double * rd, double * ru) {
+    for (int j = 0; j < k; j++) {
+        double v0 = d[j];
+        double v1 = j + 1 < k ? lo[j] / v0 : 0.0;
+        rd[j] = sqrt(v0);
+        if (j + 1 < k) {
+            d[j + 1] -= v1 * up[j];
+            ru[j] = up[j] / rd[j];
+        }
+    }
+}
+
+/* src/rotations.c:192-262 (ft_plan_rotannulus, gamma = 0): the even orders' sines and cosines
+ * from the QR factorisations of the shifted Jacobi matrix and its successive similarity
+ * transforms; the odd orders' the same after one Cholesky-based similarity */
+static void plan_rotannulus(int n, double alpha, double beta, double rho, double * s, double * c) {
+    const double t = 1.0 + 2.0 * rho * rho / (1.0 - rho * rho);
+    int k = n + 1;
+    double * d = malloc(sizeof(double) * (k + 1)), * lo = malloc(sizeof(double) * (k + 1)), * up = malloc(sizeof(double) * (k + 1));
+    double * a = malloc(sizeof(double) * (k + 1)), * b = malloc(sizeof(double) * (k + 1));
+    double * a2 = malloc(sizeof(double) * (k + 1)), * b2 = malloc(sizeof(double) * (k + 1));
+    double * qs = malloc(sizeof(double) * (k + 1)), * qc = malloc(sizeof(double) * (k + 1));
+    double * r0 = malloc(sizeof(double) * (k + 1)), * r1 = malloc(sizeof(double) * (k + 1)), * r2 = malloc(sizeof(double) * (k + 1));
+    for (int parity = 0; parity < 2; parity++) {
+        jacobi_tridiagonal(n + 1, beta, alpha, d, lo, up);
+        for (int i = 0; i < n + 1; i++) a[i] = d[i] + t;
+        for (int i = 0; i < n; i++) b[i] = up[i];
+        k = n + 1;
+        if (parity == 1) {
+            /* one similarity by the Cholesky factor of (X + t I) */
+            for (int i = 0; i < n + 1; i++) d[i] = t + d[i];
+            tridiagonal_cholesky(n + 1, d, lo, up, r0, r1);
+            jacobi_similarity(k, r0, r1, a, b, a2, b2);
+            k--;
+            memcpy(a, a2, sizeof(double) * k);
+            if (k > 1) memcpy(b, b2, sizeof(double) * (k - 1));
+        }
+        for (int m = parity; m < 2 * n - 1; m += 2) {
+            tridiagonal_qr(k, a, b, qs, qc, r0, r1, r2);
+            for (int l = 0; l < n - (m + 1) / 2; l++) {
+                s[disk_idx(n, l, m)] = qs[l];
+                c[disk_idx(n, l, m)] = qc[l];
+            }
+            jacobi_similarity(k, r0, r1, a, b, a2, b2);
+            k--;
+            memcpy(a, a2, sizeof(double) * k);
+            if (k > 1) memcpy(b, b2, sizeof(double) * (k - 1));
+        }
+    }
+    free(d); free(lo); free(up); free(a); free(b); free(a2); free(b2); free(qs); free(qc); free(r0); free(r1); free(r2);
+}
+
+/* src/drivers.c:1023-1071 (gamma = 0) */
+oracle_ann_plan * oracle_plan_ann2cxf(int n, double alpha, double beta, double rho, int connections) {
+    oracle_ann_plan * P = calloc(1, sizeof(oracle_ann_plan));
+    P->rho = rho;
+    oracle_plan * D = P->disk = calloc(1, sizeof(oracle_plan));
+    D->kind = ORACLE_DISK; D->n = n; D->alpha = alpha; D->beta = beta;
+    D->s = calloc((size_t) n * n + 1, sizeof(double));
+    D->c = calloc((size_t) n * n + 1, sizeof(double));
+    plan_rotannulus(n, alpha, beta, rho, D->s, D->c);
+    /* MP[1]: the Cholesky factor of (t I + X) of size n (src/drivers.c:1036-1046) */
+    const double t = 1.0 + 2.0 * rho * rho / (1.0 - rho * rho);
+    double * d = malloc(sizeof(double) * (n + 1)), * lo = malloc(sizeof(double) * (n + 1)), * up = malloc(sizeof(double) * (n + 1));
+    jacobi_tridiagonal(n, beta, alpha, d, lo, up);
+    for (int i = 0; i < n; i++) d[i] = t + d[i];
+    P->rd = calloc(n + 1, sizeof(double));
+    P->ru = calloc(n + 1, sizeof(double));
+    tridiagonal_cholesky(n, d, lo, up, P->rd, P->ru);
+    free(d); free(lo); free(up);
+    if (connections) {
+        D->P[0] = oracle_plan_jacobi_to_jacobi(1, 1, n, beta, alpha, -0.5, -0.5);
+        D->Pinv[0] = oracle_plan_jacobi_to_jacobi(1, 1, n, -0.5, -0.5, beta, alpha);
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i <= j; i++) {
+                double r = i ? sqrtl(M_2_PIl) : sqrtl(M_1_PIl), q = j ? sqrtl(M_PI_2l) : sqrtl(M_PIl);
+                D->P[0][i + (size_t) j * n] *= r;
+                D->Pinv[0][i + (size_t) j * n] *= q;
+            }
+        double cst = sqrt(2.0) * pow(2.0 / (1.0 - rho * rho), 0.5 * (alpha + beta + 1.0));
+        double cstinv = 1.0 / cst;
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i <= j; i++) {
+                D->P[0][i + (size_t) j * n] *= cst;
+                D->Pinv[0][i + (size_t) j * n] *= cstinv;
+            }
+    }
+    return P;
+}
+
+void oracle_destroy_ann_plan(oracle_ann_plan * P) {
+    if (!P) return;
+    oracle_destroy_plan(P->disk);
+    free(P->rd); free(P->ru);
+    free(P);
+}
+
+/* src/banded_source.c:381-422 with b = 1: x <- R^{-1} x, R^{-T} x (solve) or R x, R^T x */
+static void bidiagonal(const double * rd, const double * ru, int n, char trans, int solve, double * x) {
+    if (solve) {
+        if (trans == 'N') for (int i = n - 1; i >= 0; i--) { double t = 0; if (i + 1 < n) t += ru[i] * x[i + 1]; x[i] = (x[i] - t) / rd[i]; }
+        else for (int i = 0; i < n; i++) { double t = 0; if (i > 0) t += ru[i - 1] * x[i - 1]; x[i] = (x[i] - t) / rd[i]; }
+    } else {
+        if (trans == 'N') for (int i = 0; i < n; i++) { double t = 0; t += rd[i] * x[i]; if (i + 1 < n) t += ru[i] * x[i + 1]; x[i] = t; }
+        else for (int i = n - 1; i >= 0; i--) { double t = 0; if (i > 0) t += ru[i - 1] * x[i - 1]; t += rd[i] * x[i]; x[i] = t; }
+    }
+}
+
+/* classes 1 and 2 of the columns (j mod 4 = 1, 2): src/drivers.c:1073-1121 (mpmm: solve; mpsm: multiply;
+ * classes 0 and 3 take the identity) */
+static void ann_modified(const oracle_ann_plan * P, int N, int M, char trans, int solve, double * A) {
+    #pragma omp parallel for schedule(static)
+    for (int j = 0; j < M; j++)
+        if (j % 4 == 1 || j % 4 == 2) bidiagonal(P->rd, P->ru, N, trans, solve, A + (size_t) j * N);
+}
+
+void oracle_execute_ann(const oracle_ann_plan * P, int forward, char TRANS, double * A, int N, int M) {
+    if (TRANS != 'N' && TRANS != 'T') return;
+    const oracle_plan * D = P->disk;
+    if (forward && TRANS == 'N') {
+        oracle_execute_hi2lo(D, A, M);
+        ann_modified(P, N, M, 'N', 1, A);
+        oracle_trmm('L', 'N', N, D->P[0], M, A, N);
+    } else if (forward) {
+        oracle_trmm('L', 'T', N, D->P[0], M, A, N);
+        ann_modified(P, N, M, 'T', 1, A);
+        oracle_execute_lo2hi(D, A, M);
+    } else if (TRANS == 'N') {
+        oracle_trmm('L', 'N', N, D->Pinv[0], M, A, N);
+        ann_modified(P, N, M, 'N', 0, A);
+        oracle_execute_lo2hi(D, A, M);
+    } else {
+        oracle_execute_hi2lo(D, A, M);
+        ann_modified(P, N, M, 'T', 0, A);
+        oracle_trmm('L', 'T', N, D->Pinv[0], M, A, N);
+    }
 }

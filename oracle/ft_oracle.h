@@ -88,6 +88,21 @@ void oracle_execute_spinsph_lo2hi(const oracle_spin_plan * P, double * A, int M)
 void oracle_execute_spin(const oracle_spin_plan * P, int forward, char TRANS, double * A, int N, int M);
 void oracle_fill_spin(int N, int M, int s, unsigned long long seed, double * A);
 
+/* Annulus harmonics, gamma = 0 (src/rotations.c:192-268, src/drivers.c:1023-1121,
+ * src/banded_source.c): a disk-shaped plan whose sweep table comes from the QR factorisations
+ * of shifted Jacobi matrices; classes 1 and 2 of the columns also go through the bidiagonal
+ * Cholesky factor R of (t I + X), t = 1 + 2 rho^2 / (1 - rho^2). */
+typedef struct {
+    oracle_plan * disk;  /* kind ORACLE_DISK: the annulus table in the disk packing; P[0], Pinv[0] */
+    double * rd, * ru;   /* R: diagonal (n) and superdiagonal (n - 1) */
+    double rho;
+} oracle_ann_plan;
+/* connections = 0: rotation table only */
+oracle_ann_plan * oracle_plan_ann2cxf(int n, double alpha, double beta, double rho, int connections);
+void oracle_destroy_ann_plan(oracle_ann_plan * P);
+/* forward = 1: ann2cxf; 0: cxf2ann */
+void oracle_execute_ann(const oracle_ann_plan * P, int forward, char TRANS, double * A, int N, int M);
+
 /* Tetrahedral harmonics (src/rotations.c:297-321, src/drivers.c:510-528, 1173-1257).  Tensors
  * are N x L x M column-major (entry (i, l, m) at i + N l + N L m). */
 typedef struct {

@@ -18,9 +18,12 @@ seeded inputs and stores inputs and outputs as compressed .npz files:
     _lo2hi) and the six connection matrices, files rect_n<n>_b<beta>.npz;
   * tetrahedral transforms (ft_execute_tet2cheb / ft_execute_cheb2tet, N = L = M), their
     rotation stages (ft_execute_tet_hi2lo / _lo2hi) and the six connection matrices, files
-    tet_n<n>_<params>.npz.
+    tet_n<n>_<params>.npz;
+  * annulus transforms (ft_execute_ann2cxf / ft_execute_cxf2ann, gamma = 0, M = 4N - 3), the
+    annulus rotation table (ft_plan_rotannulus) and its sweeps through ft_execute_disk_hi2lo /
+    _lo2hi, files ann_n<n>_<params>.npz.
 
-    python tests/golden/make_golden.py [sph tri disk spin rect tet]   (default: all)
+    python tests/golden/make_golden.py [sph tri disk spin rect tet ann]   (default: all)
 """
 from __future__ import annotations
 
@@ -41,6 +44,7 @@ CASES = [
 ]
 SPIN_CASES = [(8, -2), (17, 0), (17, 1), (16, 3), (33, -1), (12, 4)]
 RECT_CASES = [(8, 0.0), (17, 0.5), (16, -0.25), (33, 1.5)]
+ANN_CASES = [(8, (0.0, 0.0, 0.5773502691896257)), (13, (0.5, -0.25, 0.4)), (16, (0.0, 0.0, 0.0))]
 TET_CASES = [(8, (0.0, 0.0, 0.0, 0.0)), (9, (-0.5, -0.5, -0.5, -0.5)), (12, (0.5, -0.25, 0.25, 1.0))]
 SEED = 20261203
 
@@ -63,7 +67,7 @@ def main():
         for d in ("hi2lo", "lo2hi"):
             getattr(L, f"ft_execute_{fam}_{d}").argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int]
     L.ft_destroy_rotation_plan.argtypes = [C.c_void_p]
-    families = set(sys.argv[1:]) or {"sph", "tri", "disk", "spin", "rect", "tet"}
+    families = set(sys.argv[1:]) or {"sph", "tri", "disk", "spin", "rect", "tet", "ann"}
     for kind, n, params in CASES:
         if kind not in families:
             continue
@@ -131,6 +135,25 @@ def main():
                 R.rect_rotations(n, beta, d == "hi2lo", B)
                 out["rot_" + d] = B
             path = os.path.join(HERE, case_name("rect", n, (beta,)) + ".npz")
+            np.savez_compressed(path, **out)
+            print("wrote", os.path.relpath(path), A.shape)
+    if "ann" in families:
+        for n, (a, b, rho) in ANN_CASES:
+            A = fill("disk", n, SEED)
+            P = R.ann_plan(n, a, b, rho)
+            out = {"A": A, "params": np.array((a, b, rho), dtype=np.float64)}
+            for fwd in (True, False):
+                for tr in "NT":
+                    B = A.copy(order="F")
+                    R.ann_execute(P, fwd, tr, B)
+                    out[("fwd" if fwd else "bwd") + "_" + tr] = B
+            R.destroy(P)
+            out["s"], out["c"] = R.ann_table(n, a, b, rho)
+            for d in ("hi2lo", "lo2hi"):
+                B = A.copy(order="F")
+                R.ann_rotations(n, a, b, rho, d == "hi2lo", B)
+                out["rot_" + d] = B
+            path = os.path.join(HERE, case_name("ann", n, (a, b, rho)) + ".npz")
             np.savez_compressed(path, **out)
             print("wrote", os.path.relpath(path), A.shape)
     if "tet" in families:
