@@ -42,6 +42,8 @@ __all__ = [
     "TetPlan", "plan_tet2cheb", "execute_tet2cheb", "execute_cheb2tet", "execute_tet_hi2lo", "execute_tet_lo2hi",
     "execute_tet_dev", "tet_rotations_dev", "tetrand",
     "plan_ann2cxf", "execute_ann2cxf", "execute_cxf2ann", "plan_rotannulus",
+    "plan_disk_synthesis", "plan_disk_analysis", "execute_disk_synthesis", "execute_disk_analysis", "execute_disk_grid_dev",
+    "plan_tri_synthesis", "plan_tri_analysis", "execute_tri_synthesis", "execute_tri_analysis", "execute_tri_grid_dev",
     "SPH", "TRI", "DISK",
 ]
 
@@ -95,12 +97,19 @@ def _load() -> C.CDLL:
         "ft_plan_rectdisk2cheb": (vp, [i, d]), "ft_plan_rotrectdisk": (vp, [i, d]),
         "ft_plan_tet2cheb": (vp, [i, d, d, d, d]),
         "ft_plan_ann2cxf": (vp, [i, d, d, d, d]), "ft_plan_rotannulus": (vp, [i, d, d, d, d]),
+        "ft_plan_disk_synthesis": (vp, [i, i, C.c_uint]), "ft_plan_disk_analysis": (vp, [i, i, C.c_uint]),
+        "ft_destroy_disk_fftw_plan": (None, [vp]),
+        "ft_plan_tri_synthesis": (vp, [i, i, C.c_uint]), "ft_plan_tri_analysis": (vp, [i, i, C.c_uint]),
+        "ft_destroy_triangle_fftw_plan": (None, [vp]),
+        "ft_b200_execute_disk_grid_dev": (i, [vp, i, ch, vp, i, i, vp]),
+        "ft_b200_execute_tri_grid_dev": (i, [vp, i, ch, vp, i, i, vp]),
         "ft_execute_tet2cheb": (None, [ch, vp, dp, i, i, i]), "ft_execute_cheb2tet": (None, [ch, vp, dp, i, i, i]),
         "ft_execute_tet_hi2lo": (None, [vp, vp, dp, i, i]), "ft_execute_tet_lo2hi": (None, [vp, vp, dp, i, i]),
         "ft_b200_execute_tet_dev": (i, [vp, i, ch, vp, i, i, i, vp]),
         "ft_b200_tet_rotations_dev": (i, [vp, i, vp, i, i, vp]),
     }
-    for name in ("sph_synthesis", "sph_analysis", "sphv_synthesis", "sphv_analysis"):
+    for name in ("sph_synthesis", "sph_analysis", "sphv_synthesis", "sphv_analysis", "disk_synthesis", "disk_analysis",
+                 "tri_synthesis", "tri_analysis"):
         sig["ft_execute_" + name] = (None, [ch, vp, dp, i, i])
     for name in ("sph2fourier", "fourier2sph", "tri2cheb", "cheb2tri", "disk2cxf", "cxf2disk", "sphv2fourier", "fourier2sphv",
                  "rectdisk2cheb", "cheb2rectdisk", "ann2cxf", "cxf2ann"):
@@ -252,6 +261,53 @@ def plan_sphv_analysis(n: int, m: int = None) -> SphereGridPlan: return _grid_pl
 
 
 GRID_OPS = {"sph_synthesis": 0, "sph_analysis": 1, "sphv_synthesis": 2, "sphv_analysis": 3}
+
+
+class _FamilyGridPlan(SphereGridPlan):
+    """A disk or triangle grid plan (reference: src/fftw.c:279-330, 404-532)."""
+
+    _destroy = None
+
+    def close(self):
+        if self.ptr:
+            getattr(lib, self._destroy)(self.ptr)
+            self.ptr = None
+
+
+class DiskGridPlan(_FamilyGridPlan):
+    _destroy = "ft_destroy_disk_fftw_plan"
+
+
+class TriGridPlan(_FamilyGridPlan):
+    _destroy = "ft_destroy_triangle_fftw_plan"
+
+
+def _family_plan(cls, fname, n, m):
+    ptr = getattr(lib, fname)(n, m, 0)
+    if not ptr:
+        _check()
+        raise FTB200Error(-1, "plan creation failed")
+    return cls(ptr, fname[8:], n, m)
+
+
+def plan_disk_synthesis(n: int, m: int = None) -> DiskGridPlan: return _family_plan(DiskGridPlan, "ft_plan_disk_synthesis", n, 4 * n - 3 if m is None else m)
+def plan_disk_analysis(n: int, m: int = None) -> DiskGridPlan: return _family_plan(DiskGridPlan, "ft_plan_disk_analysis", n, 4 * n - 3 if m is None else m)
+def plan_tri_synthesis(n: int, m: int = None) -> TriGridPlan: return _family_plan(TriGridPlan, "ft_plan_tri_synthesis", n, n if m is None else m)
+def plan_tri_analysis(n: int, m: int = None) -> TriGridPlan: return _family_plan(TriGridPlan, "ft_plan_tri_analysis", n, n if m is None else m)
+
+
+def execute_disk_grid_dev(P: DiskGridPlan, analysis: bool, trans: str, ptr: int, N: int, M: int, stream: int = 0) -> None:
+    """The disk grid's synthesis (analysis = False) or analysis sequence with P's kinds on a device matrix."""
+    st = lib.ft_b200_execute_disk_grid_dev(P.ptr, 1 if analysis else 0, trans.encode(), C.c_void_p(ptr), N, M, C.c_void_p(stream))
+    if st != 0:
+        _check()
+
+
+def execute_tri_grid_dev(P: TriGridPlan, analysis: bool, trans: str, ptr: int, N: int, M: int, stream: int = 0) -> None:
+    """The triangle grid's synthesis (analysis = False) or analysis sequence with P's kinds on a device matrix."""
+    st = lib.ft_b200_execute_tri_grid_dev(P.ptr, 1 if analysis else 0, trans.encode(), C.c_void_p(ptr), N, M, C.c_void_p(stream))
+    if st != 0:
+        _check()
 
 
 def execute_sph_grid_dev(P: SphereGridPlan, op: str, trans: str, ptr: int, N: int, M: int, stream: int = 0) -> None:
@@ -431,6 +487,10 @@ def execute_sph_synthesis(trans, P, A, N=None, M=None): _exec_host("ft_execute_s
 def execute_sph_analysis(trans, P, A, N=None, M=None): _exec_host("ft_execute_sph_analysis", trans, P, A, N, M)
 def execute_sphv_synthesis(trans, P, A, N=None, M=None): _exec_host("ft_execute_sphv_synthesis", trans, P, A, N, M)
 def execute_sphv_analysis(trans, P, A, N=None, M=None): _exec_host("ft_execute_sphv_analysis", trans, P, A, N, M)
+def execute_disk_synthesis(trans, P, A, N=None, M=None): _exec_host("ft_execute_disk_synthesis", trans, P, A, N, M)
+def execute_disk_analysis(trans, P, A, N=None, M=None): _exec_host("ft_execute_disk_analysis", trans, P, A, N, M)
+def execute_tri_synthesis(trans, P, A, N=None, M=None): _exec_host("ft_execute_tri_synthesis", trans, P, A, N, M)
+def execute_tri_analysis(trans, P, A, N=None, M=None): _exec_host("ft_execute_tri_analysis", trans, P, A, N, M)
 def execute_fourier2sph(trans, P, A, N=None, M=None): _exec_host("ft_execute_fourier2sph", trans, P, A, N, M)
 def execute_tri2cheb(trans, P, A, N=None, M=None): _exec_host("ft_execute_tri2cheb", trans, P, A, N, M)
 def execute_cheb2tri(trans, P, A, N=None, M=None): _exec_host("ft_execute_cheb2tri", trans, P, A, N, M)

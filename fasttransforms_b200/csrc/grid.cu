@@ -35,8 +35,10 @@ namespace ftb {
 namespace {
 
 // FFTW r2r kinds used by the plans (the values of fftw3.h's enum)
-enum { K_REDFT01 = 4, K_REDFT10 = 5, K_RODFT01 = 8, K_RODFT10 = 9 };
-enum Op { SPH_SYN = 0, SPH_ANA = 1, SPHV_SYN = 2, SPHV_ANA = 3 };
+enum { K_REDFT01 = 4, K_REDFT10 = 5, K_REDFT11 = 6, K_RODFT01 = 8, K_RODFT10 = 9 };
+enum Op { SPH_SYN = 0, SPH_ANA = 1, SPHV_SYN = 2, SPHV_ANA = 3, DISK_SYN = 4, DISK_ANA = 5, TRI_SYN = 6, TRI_ANA = 7 };
+// plan families: the sphere's (sph, sphv), the disk's, the triangle's
+enum Family { F_SPHERE = 0, F_DISK = 1, F_TRI = 2 };
 
 constexpr int kGridMagic = 0x46544753;   // "FTGS"
 
@@ -55,8 +57,9 @@ bool is_type3(int kind) { return kind == K_REDFT01 || kind == K_RODFT01; }
 
 struct SphereGridPlan {
     int magic = kGridMagic;
+    int family = F_SPHERE;
     int N = 0, M = 0;
-    int kind[2] = {0, 0};        // theta kinds of column classes {0, 3} and {1, 2}
+    int kind[2] = {0, 0};        // theta kinds of column classes {0, 3} and {1, 2} (tri: both dimensions)
     int device = 0;
     cufftHandle t_r2c = 0;       // length N, batch M (cosine type II)
     cufftHandle t_c2r = 0;       // length N, batch M (cosine type III)
@@ -67,6 +70,13 @@ struct SphereGridPlan {
     double2 * d_cwork = nullptr; // (N/2 + 1) x M complex
     double2 * d_Y = nullptr;     // N x (M/2 + 1) complex, element (i, j) at i + j N
     double * d_stage = nullptr;  // N x M, host-pointer calls
+    // disk: the DCT-IV of the columns of classes 1 and 2 (nq of them) as a zero-padded complex
+    // DFT of length 2N
+    cufftHandle t4 = 0;
+    bool have_t4 = false;
+    int nq = 0;
+    double2 * d_u = nullptr;     // 2N x nq
+    double * d_work2 = nullptr;  // tri: N x N, the transposed matrix
     cudaStream_t stream = nullptr;
     std::mutex mu;
 };
@@ -144,6 +154,50 @@ __global__ void t3_post(const double * __restrict__ V, double * __restrict__ X, 
 }
 
 // ---------------------------------------------------------------------------
+// DCT-IV (REDFT11) of the columns of classes 1 and 2 (column 4 (q / 2) + 1 + q % 2 for q < nq):
+//   y_k = 2 sum_j x_j cos(pi (j + 1/2)(k + 1/2) / N)
+//       = 2 Re(exp(-i pi (2k + 1) / 4N) DFT_2N(x_j exp(-i pi j / 2N), zero-padded)_k)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int class12_col(int q) { return 4 * (q / 2) + 1 + (q & 1); }
+
+__global__ void dct4_pre(const double * __restrict__ X, double2 * __restrict__ U, int N, int nq) {
+    const long long idx = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= 2LL * N * nq) return;
+    const int q = (int) (idx / (2 * N)), j = (int) (idx % (2 * N));
+    double2 u = make_double2(0.0, 0.0);
+    if (j < N) {
+        const double x = X[(long long) class12_col(q) * N + j];
+        double s, c;
+        sincospi((double) j / (2.0 * N), &s, &c);
+        u = make_double2(x * c, -x * s);
+    }
+    U[idx] = u;
+}
+
+__global__ void dct4_post(const double2 * __restrict__ U, double * __restrict__ X, int N, int nq) {
+    const long long idx = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long) N * nq) return;
+    const int q = (int) (idx / N), k = (int) (idx % N);
+    const double2 v = U[(long long) q * 2 * N + k];
+    double s, c;
+    sincospi((double) (2 * k + 1) / (4.0 * N), &s, &c);
+    X[(long long) class12_col(q) * N + k] = 2.0 * (c * v.x + s * v.y);   // 2 Re((c - i s) v)
+}
+
+// triangle scalings (src/fftw.c:292-330), entry (i, j) of the N x M matrix: times ef when
+// j == 0, times ef when i == 0, then times s (mul) or divided by d (d > 0)
+__global__ void tri_scale(double * X, int N, int M, double ef, double s, double d) {
+    const long long total = (long long) N * M;
+    for (long long e = blockIdx.x * (long long) blockDim.x + threadIdx.x; e < total; e += (long long) gridDim.x * blockDim.x) {
+        const int i = (int) (e % N), j = (int) (e / N);
+        double v = X[e];
+        if (j == 0) v *= ef;
+        if (i == 0) v *= ef;
+        X[e] = d > 0.0 ? v / d : v * s;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // phi stage packing and the scalings
 // ---------------------------------------------------------------------------
 // Y(i, 0) = (s X(i, 0)) f0; Y(i, j) = s (X(i, 2j) - i X(i, 2j - 1)), j = 1 .. M/2
@@ -194,20 +248,38 @@ bool fok(cufftResult r, const char * what) {
 
 unsigned blocks(long long n) { return (unsigned) ((n + 255) / 256); }
 
-SphereGridPlan * make_plan(int N, int M, int k0, int k1) {
+SphereGridPlan * make_plan(int N, int M, int k0, int k1, int family = F_SPHERE) {
     clear_error();
     if (N < 1 || M < 1) { set_error(FT_B200_EINVAL, "N and M must be positive"); return nullptr; }
-    if (M % 2 == 0) { set_error(FT_B200_EINVAL, "M must be odd (the half spectrum holds columns 2j - 1, 2j)"); return nullptr; }
+    if (family != F_TRI && M % 2 == 0) {
+        set_error(FT_B200_EINVAL, "M must be odd (the half spectrum holds columns 2j - 1, 2j)");
+        return nullptr;
+    }
+    if (family == F_TRI && M != N) {
+        set_error(FT_B200_EINVAL, "triangle grids need M == N (the reference's 2-D plan reads the matrix both ways)");
+        return nullptr;
+    }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { set_error(FT_B200_ENODEV, "no CUDA device"); return nullptr; }
     SphereGridPlan * P = new SphereGridPlan();
+    P->family = family;
     P->N = N; P->M = M; P->kind[0] = k0; P->kind[1] = k1;
     cudaGetDevice(&P->device);
     const size_t nm = (size_t) N * M;
     bool good = ok(cudaMalloc(&P->d_work, sizeof(double) * nm), "cudaMalloc(grid work)") &&
                 ok(cudaMalloc(&P->d_cwork, sizeof(double2) * (size_t) (N / 2 + 1) * M), "cudaMalloc(grid work)") &&
-                ok(cudaMalloc(&P->d_Y, sizeof(double2) * (size_t) N * (M / 2 + 1)), "cudaMalloc(grid spectrum)") &&
+                (family == F_TRI || ok(cudaMalloc(&P->d_Y, sizeof(double2) * (size_t) N * (M / 2 + 1)), "cudaMalloc(grid spectrum)")) &&
+                (family != F_TRI || ok(cudaMalloc(&P->d_work2, sizeof(double) * nm), "cudaMalloc(grid work)")) &&
                 ok(cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (good && family == F_DISK) {
+        P->nq = (M + 2) / 4 + (M + 1) / 4;
+        if (P->nq > 0) {
+            int n2[1] = {2 * N};
+            good = ok(cudaMalloc(&P->d_u, sizeof(double2) * 2 * (size_t) N * P->nq), "cudaMalloc(grid work)") &&
+                   fok(cufftPlanMany(&P->t4, 1, n2, nullptr, 1, 2 * N, nullptr, 1, 2 * N, CUFFT_Z2Z, P->nq), "cufftPlanMany");
+            P->have_t4 = good;
+        }
+    }
     if (good) {
         int n[1] = {N};
         if (is_type3(k0)) {
@@ -218,7 +290,7 @@ SphereGridPlan * make_plan(int N, int M, int k0, int k1) {
             P->have_t_r2c = good;
         }
     }
-    if (good) {
+    if (good && family != F_TRI) {
         // phi: along rows, element stride N, rows one apart
         int m[1] = {M}, hm[1] = {M / 2 + 1};
         good = fok(cufftPlanMany(&P->p_c2r, 1, m, hm, N, 1, m, N, 1, CUFFT_Z2D, N), "cufftPlanMany");
@@ -235,10 +307,11 @@ SphereGridPlan * make_plan(int N, int M, int k0, int k1) {
     return P;
 }
 
-// theta transforms of all M columns in place (the plan's kinds by column class)
+// theta transforms of all M columns in place (the plan's kinds by column class; disk: kind[0]
+// on every column here, the DCT-IV of classes 1 and 2 in theta_disk)
 bool theta(SphereGridPlan * P, double * X, cudaStream_t st) {
     const int N = P->N, M = P->M;
-    const int d0 = is_dst(P->kind[0]), d1 = is_dst(P->kind[1]);
+    const int d0 = is_dst(P->kind[0]), d1 = P->family == F_SPHERE ? is_dst(P->kind[1]) : d0;
     if (is_type3(P->kind[0])) {
         if (!fok(cufftSetStream(P->t_c2r, st), "cufftSetStream")) return false;
         t3_pre<<<blocks((long long) (N / 2 + 1) * M), 256, 0, st>>>(X, P->d_cwork, N, M, d0, d1);
@@ -257,6 +330,42 @@ bool theta(SphereGridPlan * P, double * X, cudaStream_t st) {
     t2_post<<<blocks((long long) N * M), 256, 0, st>>>(P->d_cwork, X, N, M, d0, d1);
     count_launch();
     return ok(cudaGetLastError(), "t2_post");
+}
+
+// disk: classes 1 and 2 by the DCT-IV (their inputs read before theta overwrites them)
+bool theta_disk(SphereGridPlan * P, double * X, cudaStream_t st) {
+    const int N = P->N, nq = P->nq;
+    if (nq > 0) {
+        dct4_pre<<<blocks(2LL * N * nq), 256, 0, st>>>(X, P->d_u, N, nq);
+        count_launch();
+        if (!ok(cudaGetLastError(), "dct4_pre") || !fok(cufftSetStream(P->t4, st), "cufftSetStream") ||
+            !fok(cufftExecZ2Z(P->t4, reinterpret_cast<cufftDoubleComplex *>(P->d_u), reinterpret_cast<cufftDoubleComplex *>(P->d_u),
+                              CUFFT_FORWARD), "cufftExecZ2Z"))
+            return false;
+    }
+    if (!theta(P, X, st)) return false;
+    if (nq > 0) {
+        dct4_post<<<blocks((long long) N * nq), 256, 0, st>>>(P->d_u, X, N, nq);
+        count_launch();
+        return ok(cudaGetLastError(), "dct4_post");
+    }
+    return true;
+}
+
+// triangle: the plan's kind along both dimensions of the square matrix
+bool theta_tri(SphereGridPlan * P, double * X, cudaStream_t st) {
+    double * a[1] = {X}, * b[1] = {P->d_work2};
+    return theta(P, X, st) && ok(launch_transpose_square(a, b, 1, P->N, st), "transpose") && theta(P, P->d_work2, st) &&
+           ok(launch_transpose_square(b, a, 1, P->N, st), "transpose");
+}
+
+bool tri_scaling(SphereGridPlan * P, double * X, double ef, double s, double d, cudaStream_t st) {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    tri_scale<<<sms * 4, 256, 0, st>>>(X, P->N, P->M, ef, s, d);
+    count_launch();
+    return ok(cudaGetLastError(), "tri_scale");
 }
 
 bool phi_c2r(SphereGridPlan * P, const double * X, double s, double f0, cudaStream_t st) {
@@ -290,6 +399,22 @@ bool ends(SphereGridPlan * P, double * X, bool last, int c0, int start, double f
 bool run(SphereGridPlan * P, int op, char T, double * X, cudaStream_t st) {
     const int N = P->N, M = P->M;
     const double nm2 = 2.0 * N * M;
+    if (op == DISK_SYN || op == DISK_ANA) {   // src/fftw.c:460-532: first entries of {0, 3, 4, 7, 8, ..} only
+        auto first = [&](double f) { return ends(P, X, false, 0, 3, f, st); };
+        if (op == DISK_SYN) {
+            if (T == 'N') return first(2.0) && theta_disk(P, X, st) && phi_c2r(P, X, C_1_4_SQRT_PI, C_SQRT2, st);
+            return phi_r2c(P, X, C_1_2_SQRT_PI, C_SQRT1_2, st) && theta_disk(P, X, st);
+        }
+        if (T == 'N') return phi_r2c(P, X, C_4_SQRT_PI / nm2, C_SQRT1_2, st) && theta_disk(P, X, st) && first(0.5);
+        return theta_disk(P, X, st) && phi_c2r(P, X, C_2_SQRT_PI / nm2, C_SQRT2, st);
+    }
+    if (op == TRI_SYN || op == TRI_ANA) {     // src/fftw.c:292-330
+        if (N <= 1 || M <= 1) return true;
+        const double nm = (double) (N * M);
+        if (op == TRI_SYN) return tri_scaling(P, X, T == 'N' ? 2.0 : 1.0, 0.25, 0.0, st) && theta_tri(P, X, st);
+        if (T == 'N') return theta_tri(P, X, st) && tri_scaling(P, X, 0.5, 1.0, nm, st);
+        return tri_scaling(P, X, 1.0, 1.0, nm, st) && theta_tri(P, X, st);
+    }
     const bool sph = op == SPH_SYN || op == SPH_ANA;
     auto first = [&](double f) { return sph ? ends(P, X, false, 0, 3, f, st) : ends(P, X, false, -1, 1, f, st); };
     auto last = [&](double f) { return sph ? ends(P, X, true, -1, 1, f, st) : ends(P, X, true, 0, 3, f, st); };
@@ -306,18 +431,20 @@ SphereGridPlan * as_grid(const ft_sphere_fftw_plan * P) {
     return (G && G->magic == kGridMagic) ? G : nullptr;
 }
 
-int check_call(SphereGridPlan * G, char T, const double * X, int N, int M) {
-    if (!G) { set_error(FT_B200_EINVAL, "not a sphere grid plan of this library"); return FT_B200_EINVAL; }
+int family_of(int op) { return op <= SPHV_ANA ? F_SPHERE : (op <= DISK_ANA ? F_DISK : F_TRI); }
+
+int check_call(SphereGridPlan * G, char T, const double * X, int N, int M, int family = F_SPHERE) {
+    if (!G || G->family != family) { set_error(FT_B200_EINVAL, "not a grid plan of this family of this library"); return FT_B200_EINVAL; }
     if (T != 'N' && T != 'T') { set_error(FT_B200_EINVAL, "TRANS must be 'N' or 'T'"); return FT_B200_EINVAL; }
     if (!X) { set_error(FT_B200_EINVAL, "NULL matrix"); return FT_B200_EINVAL; }
     if (N != G->N || M != G->M) { set_error(FT_B200_EINVAL, "N, M do not match the plan"); return FT_B200_EINVAL; }
     return FT_B200_OK;
 }
 
-void execute_host(int op, char T, const ft_sphere_fftw_plan * P, double * X, int N, int M) {
+void execute_host(int op, char T, const void * P, double * X, int N, int M) {
     clear_error();
-    SphereGridPlan * G = as_grid(P);
-    if (check_call(G, T, X, N, M) != FT_B200_OK) return;
+    SphereGridPlan * G = as_grid(static_cast<const ft_sphere_fftw_plan *>(P));
+    if (check_call(G, T, X, N, M, family_of(op)) != FT_B200_OK) return;
     std::lock_guard<std::mutex> lk(G->mu);
     cudaSetDevice(G->device);
     const size_t bytes = sizeof(double) * (size_t) N * M;
@@ -355,7 +482,8 @@ void ft_destroy_sphere_fftw_plan(ft_sphere_fftw_plan * Pp) {
     if (P->have_t_c2r) cufftDestroy(P->t_c2r);
     if (P->have_p_r2c) cufftDestroy(P->p_r2c);
     if (P->have_p_c2r) cufftDestroy(P->p_c2r);
-    cudaFree(P->d_work); cudaFree(P->d_cwork); cudaFree(P->d_Y); cudaFree(P->d_stage);
+    if (P->have_t4) cufftDestroy(P->t4);
+    cudaFree(P->d_work); cudaFree(P->d_cwork); cudaFree(P->d_Y); cudaFree(P->d_stage); cudaFree(P->d_u); cudaFree(P->d_work2);
     if (P->stream) cudaStreamDestroy(P->stream);
     P->magic = 0;
     delete P;
@@ -372,6 +500,58 @@ void ft_execute_sphv_synthesis(const char TRANS, const ft_sphere_fftw_plan * P, 
 }
 void ft_execute_sphv_analysis(const char TRANS, const ft_sphere_fftw_plan * P, double * X, const int N, const int M) {
     execute_host(SPHV_ANA, TRANS, P, X, N, M);
+}
+
+ft_disk_fftw_plan * ft_plan_disk_synthesis(const int N, const int M, const unsigned) {
+    return reinterpret_cast<ft_disk_fftw_plan *>(make_plan(N, M, K_REDFT01, K_REDFT11, F_DISK));
+}
+ft_disk_fftw_plan * ft_plan_disk_analysis(const int N, const int M, const unsigned) {
+    return reinterpret_cast<ft_disk_fftw_plan *>(make_plan(N, M, K_REDFT10, K_REDFT11, F_DISK));
+}
+void ft_destroy_disk_fftw_plan(ft_disk_fftw_plan * P) {
+    SphereGridPlan * G = as_grid(reinterpret_cast<ft_sphere_fftw_plan *>(P));
+    if (G && G->family == F_DISK) ft_destroy_sphere_fftw_plan(reinterpret_cast<ft_sphere_fftw_plan *>(P));
+}
+void ft_execute_disk_synthesis(const char TRANS, const ft_disk_fftw_plan * P, double * X, const int N, const int M) {
+    execute_host(DISK_SYN, TRANS, P, X, N, M);
+}
+void ft_execute_disk_analysis(const char TRANS, const ft_disk_fftw_plan * P, double * X, const int N, const int M) {
+    execute_host(DISK_ANA, TRANS, P, X, N, M);
+}
+
+ft_triangle_fftw_plan * ft_plan_tri_synthesis(const int N, const int M, const unsigned) {
+    return reinterpret_cast<ft_triangle_fftw_plan *>(make_plan(N, M, K_REDFT01, K_REDFT01, F_TRI));
+}
+ft_triangle_fftw_plan * ft_plan_tri_analysis(const int N, const int M, const unsigned) {
+    return reinterpret_cast<ft_triangle_fftw_plan *>(make_plan(N, M, K_REDFT10, K_REDFT10, F_TRI));
+}
+void ft_destroy_triangle_fftw_plan(ft_triangle_fftw_plan * P) {
+    SphereGridPlan * G = as_grid(reinterpret_cast<ft_sphere_fftw_plan *>(P));
+    if (G && G->family == F_TRI) ft_destroy_sphere_fftw_plan(reinterpret_cast<ft_sphere_fftw_plan *>(P));
+}
+void ft_execute_tri_synthesis(const char TRANS, const ft_triangle_fftw_plan * P, double * X, const int N, const int M) {
+    execute_host(TRI_SYN, TRANS, P, X, N, M);
+}
+void ft_execute_tri_analysis(const char TRANS, const ft_triangle_fftw_plan * P, double * X, const int N, const int M) {
+    execute_host(TRI_ANA, TRANS, P, X, N, M);
+}
+
+int ft_b200_execute_disk_grid_dev(const ft_disk_fftw_plan * P, int analysis, char TRANS, double * dX, int N, int M, void * stream) {
+    clear_error();
+    SphereGridPlan * G = as_grid(reinterpret_cast<const ft_sphere_fftw_plan *>(P));
+    const int c = check_call(G, TRANS, dX, N, M, F_DISK);
+    if (c != FT_B200_OK) return c;
+    std::lock_guard<std::mutex> lk(G->mu);
+    return run(G, analysis ? DISK_ANA : DISK_SYN, TRANS, dX, static_cast<cudaStream_t>(stream)) ? FT_B200_OK : ft_b200_last_status();
+}
+
+int ft_b200_execute_tri_grid_dev(const ft_triangle_fftw_plan * P, int analysis, char TRANS, double * dX, int N, int M, void * stream) {
+    clear_error();
+    SphereGridPlan * G = as_grid(reinterpret_cast<const ft_sphere_fftw_plan *>(P));
+    const int c = check_call(G, TRANS, dX, N, M, F_TRI);
+    if (c != FT_B200_OK) return c;
+    std::lock_guard<std::mutex> lk(G->mu);
+    return run(G, analysis ? TRI_ANA : TRI_SYN, TRANS, dX, static_cast<cudaStream_t>(stream)) ? FT_B200_OK : ft_b200_last_status();
 }
 
 int ft_b200_execute_sph_grid_dev(const ft_sphere_fftw_plan * P, int op, char TRANS, double * dX, int N, int M, void * stream) {

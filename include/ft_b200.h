@@ -158,6 +158,29 @@ void ft_execute_sphv_analysis(const char TRANS, const ft_sphere_fftw_plan * P, d
 /* the reference's flags for these planners (src/ftutilities.h:24); not used here */
 #define FT_FFTW_FLAGS 0u
 
+/* Synthesis and analysis on the disk's grid (src/fftw.c:404-532) and the triangle's
+ * (src/fftw.c:279-330); this library's own plan types, flags not used.  Disk: M odd (the
+ * reference's M = 4N - 3).  Triangle: M must equal N (the reference's 2-D plan reads the
+ * column-major matrix as row-major, which agrees only when M == N). */
+typedef struct ft_disk_fftw_plan_s ft_disk_fftw_plan;
+/* replace ft_plan_disk_synthesis / ft_plan_disk_analysis, src/fftw.c:450-458 */
+ft_disk_fftw_plan * ft_plan_disk_synthesis(const int N, const int M, const unsigned flags);
+ft_disk_fftw_plan * ft_plan_disk_analysis(const int N, const int M, const unsigned flags);
+/* replaces ft_destroy_disk_fftw_plan, src/fftw.c:404-412 */
+void ft_destroy_disk_fftw_plan(ft_disk_fftw_plan * P);
+/* replace ft_execute_disk_synthesis / ft_execute_disk_analysis, src/fftw.c:460-532 */
+void ft_execute_disk_synthesis(const char TRANS, const ft_disk_fftw_plan * P, double * X, const int N, const int M);
+void ft_execute_disk_analysis(const char TRANS, const ft_disk_fftw_plan * P, double * X, const int N, const int M);
+typedef struct ft_triangle_fftw_plan_s ft_triangle_fftw_plan;
+/* replace ft_plan_tri_synthesis / ft_plan_tri_analysis, src/fftw.c:289-290 */
+ft_triangle_fftw_plan * ft_plan_tri_synthesis(const int N, const int M, const unsigned flags);
+ft_triangle_fftw_plan * ft_plan_tri_analysis(const int N, const int M, const unsigned flags);
+/* replaces ft_destroy_triangle_fftw_plan, src/fftw.c:276-279 */
+void ft_destroy_triangle_fftw_plan(ft_triangle_fftw_plan * P);
+/* replace ft_execute_tri_synthesis / ft_execute_tri_analysis, src/fftw.c:292-330 */
+void ft_execute_tri_synthesis(const char TRANS, const ft_triangle_fftw_plan * P, double * X, const int N, const int M);
+void ft_execute_tri_analysis(const char TRANS, const ft_triangle_fftw_plan * P, double * X, const int N, const int M);
+
 /* Spin-weighted spherical harmonics.  Complex matrices are interleaved (re, im)
  * doubles, N x M column-major: column 0 holds order 0, columns 2m - 1 and 2m the
  * orders -m and m (src/drivers.c:645-695).  M must be odd. */
@@ -239,6 +262,11 @@ int ft_b200_execute_dev(const ft_harmonic_plan * P, int forward, char TRANS, dou
  * the plan's transform kinds), asynchronous on stream.  No counterpart in the
  * reference (its calls take host memory). */
 int ft_b200_execute_sph_grid_dev(const ft_sphere_fftw_plan * P, int op, char TRANS, double * dX, int N, int M, void * stream);
+/* Disk and triangle grids on device memory: analysis = 0 runs the plan through the synthesis
+ * sequence, 1 through the analysis sequence (the plan's kinds either way, as the reference's
+ * tests cross them), asynchronous on stream.  No counterpart in the reference. */
+int ft_b200_execute_disk_grid_dev(const ft_disk_fftw_plan * P, int analysis, char TRANS, double * dX, int N, int M, void * stream);
+int ft_b200_execute_tri_grid_dev(const ft_triangle_fftw_plan * P, int analysis, char TRANS, double * dX, int N, int M, void * stream);
 
 /* The sph vector-field transforms on device memory (forward = 1: sphv2fourier). */
 int ft_b200_execute_sphv_dev(const ft_harmonic_plan * P, int forward, char TRANS, double * dA, int N, int M, void * stream);

@@ -1,7 +1,8 @@
 """Oracle (test infrastructure, not the product): a CPU restatement of the
-sphere grid synthesis and analysis of the reference (src/fftw.c:63-277:
-ft_plan_sph_with_kind, ft_execute_sph_synthesis / _analysis and the sphv
-variants) in numpy / scipy.
+sphere, disk and triangle grid synthesis and analysis of the reference
+(src/fftw.c:63-330, 404-532: ft_plan_sph_with_kind, ft_execute_sph_synthesis /
+_analysis and the sphv variants, ft_execute_disk_* and ft_execute_tri_*) in numpy /
+scipy.
 
 FFTW, which the reference calls for these transforms, is not available here, so
 its one-dimensional transforms are restated from their published definitions
@@ -10,6 +11,7 @@ its one-dimensional transforms are restated from their published definitions
   REDFT01 (DCT-III) y_k = x_0 + 2 sum_{j>=1} x_j cos(pi j (k + 1/2) / N)
   RODFT10 (DST-II)  y_k = 2 sum_j x_j sin(pi (j + 1/2) (k + 1) / N)
   RODFT01 (DST-III) y_k = (-1)^k x_{N-1} + 2 sum_{j<N-1} x_j sin(pi (j + 1) (k + 1/2) / N)
+  REDFT11 (DCT-IV)  y_k = 2 sum_j x_j cos(pi (j + 1/2) (k + 1/2) / N)
   c2r of length M   x_k = sum over the Hermitian-completed spectrum of Y_j e^{2 pi i jk / M}
   r2c of length M   Y_j = sum_k x_k e^{-2 pi i jk / M}
 which scipy.fft's dct / dst of types 2 and 3 (norm=None) and numpy's rfft /
@@ -21,7 +23,7 @@ sph2fourier / fourier2sph, test/test_fftw.c:43-73) and known harmonics.
 import numpy as np
 import scipy.fft as sf
 
-REDFT01, REDFT10, RODFT01, RODFT10 = "REDFT01", "REDFT10", "RODFT01", "RODFT10"
+REDFT01, REDFT10, RODFT01, RODFT10, REDFT11 = "REDFT01", "REDFT10", "RODFT01", "RODFT10", "REDFT11"
 
 # plan kinds (classes {0, 3}, classes {1, 2}): src/fftw.c:104-122
 PLANS = {
@@ -30,6 +32,10 @@ PLANS = {
     "sphv_synthesis": (RODFT01, REDFT01),
     "sphv_analysis": (RODFT10, REDFT10),
 }
+# disk plan kinds (classes {0, 3}, classes {1, 2}): src/fftw.c:450-458
+DISK_PLANS = {"disk_synthesis": (REDFT01, REDFT11), "disk_analysis": (REDFT10, REDFT11)}
+# triangle plan kinds (both dimensions): src/fftw.c:289-290
+TRI_PLANS = {"tri_synthesis": REDFT01, "tri_analysis": REDFT10}
 
 # src/ftinternal.h:48-56
 M_1_4_SQRT_PI = 0.141047395886939072
@@ -50,6 +56,8 @@ def r2r(x, kind):
         return sf.dst(x, type=2, axis=0)
     if kind == RODFT01:
         return sf.dst(x, type=3, axis=0)
+    if kind == REDFT11:
+        return sf.dct(x, type=4, axis=0)
     raise ValueError(kind)
 
 
@@ -146,3 +154,62 @@ def execute(op, trans, plan, X):
 def grid(N, M):
     """The points: theta_i = (i + 1/2) pi / N, phi_k = 2 pi k / M."""
     return (np.arange(N) + 0.5) * np.pi / N, 2 * np.pi * np.arange(M) / M
+
+
+def execute_disk(op, trans, plan, X):
+    """ft_execute_disk_{synthesis,analysis}(trans, P, X) with P a plan of kind `plan` (a key of
+    DISK_PLANS), src/fftw.c:460-532: the sph sequences with the disk's kinds (classes 1, 2 a
+    DCT-IV) and only the first-entry factors of columns {0, 3, 4, 7, 8, ..}."""
+    X = np.array(X, dtype=float, copy=True)
+    N, M = X.shape
+    kinds = DISK_PLANS[plan]
+    nm2 = 2.0 * N * M
+    if op == "disk_synthesis":
+        if trans == "N":
+            _ends(X, True, True, 2.0)
+            X = theta(X, kinds)
+            X *= M_1_4_SQRT_PI
+            X[:, 0] *= M_SQRT2
+            return c2r(data_r2c(X), M)
+        X = data_c2r(r2c(X), M)
+        X *= M_1_2_SQRT_PI
+        X[:, 0] *= M_SQRT1_2
+        return theta(X, kinds)
+    if trans == "N":
+        X = data_c2r(r2c(X), M)
+        X *= M_4_SQRT_PI / nm2
+        X[:, 0] *= M_SQRT1_2
+        X = theta(X, kinds)
+        _ends(X, True, True, 0.5)
+        return X
+    X = theta(X, kinds)
+    X *= M_2_SQRT_PI / nm2
+    X[:, 0] *= M_SQRT2
+    return c2r(data_r2c(X), M)
+
+
+def _r2r_2d(X, kind):
+    return r2r(r2r(X, kind).T, kind).T
+
+
+def execute_tri(op, trans, plan, X):
+    """ft_execute_tri_{synthesis,analysis}(trans, P, X), src/fftw.c:292-330: a 2-D transform of
+    the plan's kind along both dimensions (N = M; nothing happens unless N, M > 1), with the
+    first row and column factors and the 1/4 or 1/(N M) scalings."""
+    X = np.array(X, dtype=float, copy=True)
+    N, M = X.shape
+    if N <= 1 or M <= 1:
+        return X
+    kind = TRI_PLANS[plan]
+    if op == "tri_synthesis":
+        if trans == "N":
+            X[:, 0] *= 2.0
+            X[0, :] *= 2.0
+        X *= 0.25
+        return _r2r_2d(X, kind)
+    if trans == "N":
+        X = _r2r_2d(X, kind)
+        X[:, 0] *= 0.5
+        X[0, :] *= 0.5
+        return X / (N * M)
+    return _r2r_2d(X / (N * M), kind)

@@ -121,3 +121,104 @@ def test_even_m_rejected(env):
     ft, torch = env
     with pytest.raises(ft.FTB200Error):
         ft.plan_sph_synthesis(8, 16)
+
+
+# ---------------------------------------------------------------------------
+# Disk and triangle grids (src/fftw.c:279-330, 404-532)
+# ---------------------------------------------------------------------------
+def run_family_dev(ft, torch, fn, P, analysis, tr, X):
+    n, m = X.shape
+    t = torch.from_numpy(np.asfortranarray(X).ravel(order="F").copy()).cuda()
+    fn(P, analysis, tr, t.data_ptr(), n, m, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    return t.cpu().numpy().reshape((n, m), order="F")
+
+
+@pytest.mark.parametrize("N,M", [(1, 1), (2, 5), (3, 9), (8, 29), (17, 65), (64, 253), (33, 21), (256, 1021)])
+def test_disk_grid_vs_oracle(env, N, M):
+    ft, torch = env
+    from oracle import grid as G
+    X = np.random.default_rng(N * 7 + M).uniform(-1, 1, (N, M))
+    plans = {"disk_synthesis": ft.plan_disk_synthesis(N, M), "disk_analysis": ft.plan_disk_analysis(N, M)}
+    try:
+        for op in plans:
+            for tr in "NT":
+                for plan in plans:
+                    got = run_family_dev(ft, torch, ft.execute_disk_grid_dev, plans[plan], op == "disk_analysis", tr, X)
+                    want = G.execute_disk(op, tr, plan, X)
+                    assert rel2(got, want) <= 1e-14, (N, M, op, tr, plan, rel2(got, want))
+    finally:
+        for P in plans.values():
+            P.close()
+
+
+@pytest.mark.parametrize("N", [1, 2, 3, 8, 17, 64, 255, 512])
+def test_tri_grid_vs_oracle(env, N):
+    ft, torch = env
+    from oracle import grid as G
+    X = np.random.default_rng(N).uniform(-1, 1, (N, N))
+    plans = {"tri_synthesis": ft.plan_tri_synthesis(N), "tri_analysis": ft.plan_tri_analysis(N)}
+    try:
+        for op in plans:
+            for tr in "NT":
+                for plan in plans:
+                    got = run_family_dev(ft, torch, ft.execute_tri_grid_dev, plans[plan], op == "tri_analysis", tr, X)
+                    want = G.execute_tri(op, tr, plan, X)
+                    assert rel2(got, want) <= 1e-14, (N, op, tr, plan, rel2(got, want))
+    finally:
+        for P in plans.values():
+            P.close()
+
+
+@pytest.mark.parametrize("N", [64, 256, 1024])
+def test_disk_and_tri_reference_round_trips_on_gpu(env, N):
+    """test/test_fftw.c:164-195 and 226-255 on this library: every stage on the GPU."""
+    ft, torch = env
+    st = torch.cuda.current_stream().cuda_stream
+    for kind, plan, syn, ana, grid_dev, e2, einf in (
+            ("disk", ft.plan_disk2cxf(N, 0.0, 0.0), ft.plan_disk_synthesis, ft.plan_disk_analysis, ft.execute_disk_grid_dev, 8 * np.sqrt(N), 4 * N),
+            ("tri", ft.plan_tri2cheb(N, 0.0, 0.0, 0.0), ft.plan_tri_synthesis, ft.plan_tri_analysis, ft.execute_tri_grid_dev, 32 * np.sqrt(N), 8 * N)):
+        A = ft.rand_layout(kind, N, 9)
+        M = A.shape[1]
+        PS, PA = syn(N), ana(N)
+        t = torch.from_numpy(A.ravel(order="F").copy()).cuda()
+        p = t.data_ptr()
+        ft.execute_dev(plan, True, "N", p, N, M, st)
+        grid_dev(PS, False, "N", p, N, M, st)
+        grid_dev(PA, True, "N", p, N, M, st)
+        ft.execute_dev(plan, False, "N", p, N, M, st)
+        ft.execute_dev(plan, True, "T", p, N, M, st)
+        grid_dev(PA, False, "T", p, N, M, st)
+        grid_dev(PS, True, "T", p, N, M, st)
+        ft.execute_dev(plan, False, "T", p, N, M, st)
+        torch.cuda.synchronize()
+        B = t.cpu().numpy().reshape((N, M), order="F")
+        assert rel2(B, A) <= e2 * EPS, kind
+        assert np.abs(B - A).max() / np.abs(A).max() <= einf * EPS, kind
+        for Q in (plan, PS, PA):
+            Q.close()
+
+
+def test_family_host_entry_points(env):
+    ft, torch = env
+    N = 20
+    for fn_plan, host, dev, M in ((ft.plan_disk_synthesis, ft.execute_disk_synthesis, ft.execute_disk_grid_dev, 77),
+                                  (ft.plan_disk_analysis, ft.execute_disk_analysis, ft.execute_disk_grid_dev, 77),
+                                  (ft.plan_tri_synthesis, ft.execute_tri_synthesis, ft.execute_tri_grid_dev, N),
+                                  (ft.plan_tri_analysis, ft.execute_tri_analysis, ft.execute_tri_grid_dev, N)):
+        X = np.random.default_rng(M).uniform(-1, 1, (N, M))
+        P = fn_plan(N, M)
+        analysis = "analysis" in host.__name__
+        for tr in "NT":
+            H = np.asfortranarray(X.copy())
+            host(tr, P, H)
+            assert np.array_equal(H, run_family_dev(ft, torch, dev, P, analysis, tr, X)), (host.__name__, tr)
+        P.close()
+
+
+def test_family_bad_arguments(env):
+    ft, torch = env
+    with pytest.raises(ft.FTB200Error):
+        ft.plan_disk_synthesis(8, 30)     # even M
+    with pytest.raises(ft.FTB200Error):
+        ft.plan_tri_synthesis(8, 9)       # M != N

@@ -1,5 +1,5 @@
-"""Pins the sphere grid oracle (oracle/grid.py, a restatement of src/fftw.c:63-277;
-FFTW is not available here).  CPU only.
+"""Pins the grid oracle (oracle/grid.py, a restatement of src/fftw.c:63-330, 404-532: the
+sphere's, the disk's and the triangle's grids; FFTW is not available here).  CPU only.
 
 1. The one-dimensional transforms equal FFTW's published definitions (explicit
    sums) for every kind the plans use.
@@ -28,6 +28,8 @@ def explicit(x, kind):
         A[:, 0] = 1.0
     elif kind == G.RODFT10:
         A = 2 * np.sin(np.pi * (j + 0.5) * (k + 1) / N)
+    elif kind == G.REDFT11:
+        A = 2 * np.cos(np.pi * (j + 0.5) * (k + 0.5) / N)
     else:
         A = 2 * np.sin(np.pi * (j + 1) * (k + 0.5) / N)
         A[:, N - 1] = (-1.0) ** np.arange(N)
@@ -35,7 +37,7 @@ def explicit(x, kind):
 
 
 @pytest.mark.parametrize("N", [1, 2, 5, 8, 13])
-@pytest.mark.parametrize("kind", [G.REDFT10, G.REDFT01, G.RODFT10, G.RODFT01])
+@pytest.mark.parametrize("kind", [G.REDFT10, G.REDFT01, G.RODFT10, G.RODFT01, G.REDFT11])
 def test_kinds_are_fftws_definitions(N, kind):
     x = np.random.default_rng(N).standard_normal((N, 3))
     assert np.allclose(G.r2r(x, kind), explicit(x, kind), rtol=1e-13, atol=1e-13)
@@ -94,3 +96,58 @@ def test_known_harmonics(ref):
         got = G.execute("sph_synthesis", "N", "sph_synthesis", A)
         assert np.abs(got - want).max() < 1e-14, (row, col)
     ref.destroy(P)
+
+
+@pytest.mark.parametrize("N", [64, 128])
+def test_disk_reference_round_trip(ref, N):
+    """test/test_fftw.c:226-255: the compiled reference's disk2cxf / cxf2disk around the oracle's
+    disk synthesis and analysis, 'N' then 'T' with the plans crossed: 8 sqrt(N) eps, 4N eps."""
+    from fasttransforms_b200.utilities import rand_layout
+    A = rand_layout("disk", N, 5)
+    P = ref.plan("disk", N, 0.0, 0.0)
+    X = A.copy(order="F")
+    ref.execute("disk", P, True, "N", X)
+    X = G.execute_disk("disk_synthesis", "N", "disk_synthesis", X)
+    X = np.asfortranarray(G.execute_disk("disk_analysis", "N", "disk_analysis", X))
+    ref.execute("disk", P, False, "N", X)
+    ref.execute("disk", P, True, "T", X)
+    X = G.execute_disk("disk_synthesis", "T", "disk_analysis", X)
+    X = np.asfortranarray(G.execute_disk("disk_analysis", "T", "disk_synthesis", X))
+    ref.execute("disk", P, False, "T", X)
+    ref.destroy(P)
+    assert np.linalg.norm(X - A) / np.linalg.norm(A) <= 8 * np.sqrt(N) * EPS
+    assert np.abs(X - A).max() / np.abs(A).max() <= 4 * N * EPS
+
+
+@pytest.mark.parametrize("N", [64, 128])
+def test_tri_reference_round_trip(ref, N):
+    """test/test_fftw.c:164-195 (M = N): 32 sqrt(N) eps, 8N eps."""
+    from fasttransforms_b200.utilities import rand_layout
+    A = rand_layout("tri", N, 5)
+    P = ref.plan("tri", N, 0.0, 0.0, 0.0)
+    X = A.copy(order="F")
+    ref.execute("tri", P, True, "N", X)
+    X = G.execute_tri("tri_synthesis", "N", "tri_synthesis", X)
+    X = np.asfortranarray(G.execute_tri("tri_analysis", "N", "tri_analysis", X))
+    ref.execute("tri", P, False, "N", X)
+    ref.execute("tri", P, True, "T", X)
+    X = G.execute_tri("tri_synthesis", "T", "tri_analysis", X)
+    X = np.asfortranarray(G.execute_tri("tri_analysis", "T", "tri_synthesis", X))
+    ref.execute("tri", P, False, "T", X)
+    ref.destroy(P)
+    assert np.linalg.norm(X - A) / np.linalg.norm(A) <= 32 * np.sqrt(N) * EPS
+    assert np.abs(X - A).max() / np.abs(A).max() <= 8 * N * EPS
+
+
+def test_tri_grid_is_a_2d_cosine_series():
+    """Known answer: the triangle synthesis of a unit coefficient (i, j) (i, j > 0) is
+    T_i(x) T_j(y) on the Chebyshev points x_k = cos((k + 1/2) pi / N) (FFTW's REDFT01 with the
+    reference's 1/4 scaling)."""
+    N = 9
+    th = (np.arange(N) + 0.5) * np.pi / N
+    for i, j in [(1, 2), (3, 1), (4, 4)]:
+        A = np.zeros((N, N))
+        A[i, j] = 1.0
+        got = G.execute_tri("tri_synthesis", "N", "tri_synthesis", A)
+        want = np.outer(np.cos(i * th), np.cos(j * th))
+        assert np.abs(got - want).max() < 1e-14, (i, j)
