@@ -170,9 +170,35 @@ def test_tri_grid_vs_oracle(env, N):
             P.close()
 
 
+def reference_round_trip_error(kind, N, A):
+    """The same round trip with the compiled reference's transforms and the oracle's grids (2-norm
+    and max relative errors), or None where the reference is not built."""
+    from oracle import grid as G
+    from oracle.bind import Reference
+    if not Reference.available():
+        return None
+    R = Reference()
+    P = R.plan(kind, N, 0.0, 0.0, 0.0) if kind == "tri" else R.plan(kind, N, 0.0, 0.0)
+    ex = G.execute_tri if kind == "tri" else G.execute_disk
+    syn, ana = kind + "_synthesis", kind + "_analysis"
+    X = A.copy(order="F")
+    R.execute(kind, P, True, "N", X)
+    X = np.asfortranarray(ex(ana, "N", ana, ex(syn, "N", syn, X)))
+    R.execute(kind, P, False, "N", X)
+    R.execute(kind, P, True, "T", X)
+    X = np.asfortranarray(ex(ana, "T", syn, ex(syn, "T", ana, X)))
+    R.execute(kind, P, False, "T", X)
+    R.destroy(P)
+    return rel2(X, A), np.abs(X - A).max() / np.abs(A).max()
+
+
 @pytest.mark.parametrize("N", [64, 256, 1024])
 def test_disk_and_tri_reference_round_trips_on_gpu(env, N):
-    """test/test_fftw.c:164-195 and 226-255 on this library: every stage on the GPU."""
+    """test/test_fftw.c:164-195 and 226-255 on this library, every stage on the GPU: within that
+    test's bounds (32 sqrt(N) eps, 8N eps for tri; 8 sqrt(N) eps, 4N eps for disk), or within twice
+    the reference algorithm's own error of the same sequence where that is larger (the reference's
+    tri2cheb / cheb2tri round trip alone exceeds 32 sqrt(N) eps from N = 256: 1.25x at 256, 1.62x
+    at 512; the reference's test runs N = 64)."""
     ft, torch = env
     st = torch.cuda.current_stream().cuda_stream
     for kind, plan, syn, ana, grid_dev, e2, einf in (
@@ -193,8 +219,12 @@ def test_disk_and_tri_reference_round_trips_on_gpu(env, N):
         ft.execute_dev(plan, False, "T", p, N, M, st)
         torch.cuda.synchronize()
         B = t.cpu().numpy().reshape((N, M), order="F")
-        assert rel2(B, A) <= e2 * EPS, kind
-        assert np.abs(B - A).max() / np.abs(A).max() <= einf * EPS, kind
+        b2, binf = e2 * EPS, einf * EPS
+        own = reference_round_trip_error(kind, N, A) if N > 64 else None
+        if own:
+            b2, binf = max(b2, 2 * own[0]), max(binf, 2 * own[1])
+        assert rel2(B, A) <= b2, (kind, rel2(B, A), b2)
+        assert np.abs(B - A).max() / np.abs(A).max() <= binf, kind
         for Q in (plan, PS, PA):
             Q.close()
 
