@@ -131,6 +131,7 @@ class ClockSampler:
 
 def cpu_sample(n: int, reps: int) -> dict:
     """Reference CPU build on this host's cores: one plan, `reps` timed fwd+bwd after one warm-up."""
+    import numpy as np
     threads = os.cpu_count() or 1
     from oracle.bind import Reference, Oracle, fill
     A = fill("sph", n, SEED)
@@ -183,6 +184,36 @@ def cpu_sample(n: int, reps: int) -> dict:
         res["spin_s2"] = {"value": n * n / ts, "sec_per_step": ts, "cores": threads,
                           "sample": f"spinsph2fourier + fourier2spinsph 'N', s = {s}, n={n}, 1 complex field, "
                                     f"1 timed after 1 warm-up"}
+        # the other families beside the GPU's family workloads: one timed fwd+bwd 'N' after one warm-up
+        from oracle.bind import fill as fill2
+        from fasttransforms_b200.utilities import tetrand, rectdiskrand
+
+        def once(run):
+            run()
+            t0 = time.perf_counter()
+            run()
+            return time.perf_counter() - t0
+        fam = {}
+        try:
+            P = R.plan("rect", 4096, beta=0.0)
+            Z = rectdiskrand(4096, SEED)
+            t = once(lambda: (R.execute("rect", P, True, "N", Z), R.execute("rect", P, False, "N", Z)))
+            R.destroy(P)
+            fam["rectdisk_n4096"] = {"value": 4096 * 4097 // 2 / t, "sec_per_step": t}
+            rho = float(np.sqrt(1 / 3))
+            P = R.ann_plan(2048, 0.0, 0.0, rho)
+            Z = fill2("disk", 2048, SEED)
+            t = once(lambda: (R.ann_execute(P, True, "N", Z), R.ann_execute(P, False, "N", Z)))
+            R.destroy(P)
+            fam["ann_n2048"] = {"value": (2 * 2048 * 2048 - 2048) / t, "sec_per_step": t}
+            P = R.tet_plan(256, 0.0, 0.0, 0.0, 0.0)
+            Z = tetrand(256, SEED)
+            t = once(lambda: (R.tet_execute(P, True, "N", Z), R.tet_execute(P, False, "N", Z)))
+            R.destroy(P)
+            fam["tet_n256"] = {"value": 256 * 257 * 258 // 6 / t, "sec_per_step": t}
+        except Exception as exc:
+            fam["error"] = repr(exc)[:200]
+        res["families"] = fam
     return res
 
 
@@ -469,6 +500,13 @@ def run_ours(args, rank, world, local_rank, dist):
         if spin_cpu and isinstance(extra, dict) and spin_key in extra:
             extra[spin_key]["reference_cpu"] = spin_cpu
             extra[spin_key]["gpu_over_reference_cpu"] = extra[spin_key]["coeffs_per_s"] / spin_cpu["value"]
+        fam_cpu = cpu.pop("families", None) if isinstance(cpu, dict) else None
+        for key, v in (fam_cpu or {}).items():
+            if isinstance(extra, dict) and isinstance(v, dict) and key in extra and "coeffs_per_s" in extra[key]:
+                v["cores"] = cpu.get("cores")
+                v["sample"] = "the compiled reference, one timed fwd+bwd 'N' after one warm-up, same size"
+                extra[key]["reference_cpu"] = v
+                extra[key]["gpu_over_reference_cpu"] = extra[key]["coeffs_per_s"] / v["value"]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -589,6 +627,117 @@ def profile_case(n: int, precision: str, fields: int) -> None:
                       "max_abs": max(float(t.abs().max()) for t in d)}))
 
 
+def _family_timing(torch, fwd, bwd, reps=5):
+    """Mean device time (ms) of fwd(); bwd() after one untimed pair, CUDA events on the stream."""
+    st = torch.cuda.current_stream()
+    fwd(); bwd()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(reps):
+        fwd(); bwd()
+    e1.record(st)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def family_rectdisk(n):
+    import numpy as np
+    import torch
+    import fasttransforms_b200 as ft
+    sp = torch.cuda.current_stream().cuda_stream
+    P = ft.plan_rectdisk2cheb(n, 0.0)
+    A = ft.rectdiskrand(n, SEED)
+    d = torch.from_numpy(A.ravel(order="F").copy()).cuda()
+    f = lambda: ft.execute_dev(P, True, "N", d.data_ptr(), n, n, sp)
+    b = lambda: ft.execute_dev(P, False, "N", d.data_ptr(), n, n, sp)
+    d.copy_(torch.from_numpy(A.ravel(order="F").copy()))
+    f(); b()
+    torch.cuda.synchronize()
+    rt = float(np.linalg.norm(d.cpu().numpy() - A.ravel(order="F")) / np.linalg.norm(A))
+    ms = _family_timing(torch, f, b)
+    P.close()
+    coeffs = n * (n + 1) // 2
+    return {"coeffs_per_s": coeffs / (ms * 1e-3), "ms_per_step": ms, "roundtrip_eps2": rt,
+            "workload": f"rectdisk2cheb + cheb2rectdisk 'N', beta = 0, degree {n - 1}, 1 field {n} x {n} (plain FP64; "
+                        f"{coeffs} coefficients)"}
+
+
+def family_ann(n):
+    import numpy as np
+    import torch
+    import fasttransforms_b200 as ft
+    sp = torch.cuda.current_stream().cuda_stream
+    rho = float(np.sqrt(1 / 3))
+    P = ft.plan_ann2cxf(n, 0.0, 0.0, 0.0, rho)
+    A = ft.diskrand(n, SEED)
+    M = A.shape[1]
+    d = torch.from_numpy(A.ravel(order="F").copy()).cuda()
+    f = lambda: ft.execute_dev(P, True, "N", d.data_ptr(), n, M, sp)
+    b = lambda: ft.execute_dev(P, False, "N", d.data_ptr(), n, M, sp)
+    f(); b()
+    torch.cuda.synchronize()
+    rt = float(np.linalg.norm(d.cpu().numpy() - A.ravel(order="F")) / np.linalg.norm(A))
+    ms = _family_timing(torch, f, b)
+    P.close()
+    coeffs = 2 * n * n - n
+    return {"coeffs_per_s": coeffs / (ms * 1e-3), "ms_per_step": ms, "roundtrip_eps2": rt,
+            "workload": f"ann2cxf + cxf2ann 'N', alpha = beta = 0, rho = sqrt(1/3), degree {n - 1}, 1 field {n} x {M} "
+                        f"(plain FP64)"}
+
+
+def family_tet(n):
+    import numpy as np
+    import torch
+    import fasttransforms_b200 as ft
+    sp = torch.cuda.current_stream().cuda_stream
+    P = ft.plan_tet2cheb(n, 0.0, 0.0, 0.0, 0.0)
+    A = ft.tetrand(n, SEED)
+    d = torch.from_numpy(A.ravel(order="F").copy()).cuda()
+    f = lambda: ft.execute_tet_dev(P, True, "N", d.data_ptr(), n, n, n, sp)
+    b = lambda: ft.execute_tet_dev(P, False, "N", d.data_ptr(), n, n, n, sp)
+    f(); b()
+    torch.cuda.synchronize()
+    rt = float(np.linalg.norm(d.cpu().numpy() - A.ravel(order="F")) / np.linalg.norm(A))
+    ms = _family_timing(torch, f, b)
+    P.close()
+    coeffs = n * (n + 1) * (n + 2) // 6
+    return {"coeffs_per_s": coeffs / (ms * 1e-3), "ms_per_step": ms, "roundtrip_eps2": rt,
+            "workload": f"tet2cheb + cheb2tet 'N', parameters 0, degree {n - 1}, 1 field {n} x {n} x {n} (plain FP64; "
+                        f"{coeffs} coefficients)"}
+
+
+def family_grid(kind, n):
+    """The family's full transform on the device: to Chebyshev / Fourier, synthesis, analysis, back."""
+    import numpy as np
+    import torch
+    import fasttransforms_b200 as ft
+    sp = torch.cuda.current_stream().cuda_stream
+    if kind == "disk":
+        P, PS, PA, grid = ft.plan_disk2cxf(n, 0.0, 0.0), ft.plan_disk_synthesis(n), ft.plan_disk_analysis(n), ft.execute_disk_grid_dev
+        coeffs = 2 * n * n - n
+    else:
+        P, PS, PA, grid = ft.plan_tri2cheb(n, 0.0, 0.0, 0.0), ft.plan_tri_synthesis(n), ft.plan_tri_analysis(n), ft.execute_tri_grid_dev
+        coeffs = n * (n + 1) // 2
+    A = ft.rand_layout(kind, n, SEED)
+    M = A.shape[1]
+    d = torch.from_numpy(A.ravel(order="F").copy()).cuda()
+    p = d.data_ptr()
+    f = lambda: (ft.execute_dev(P, True, "N", p, n, M, sp), grid(PS, False, "N", p, n, M, sp))
+    b = lambda: (grid(PA, True, "N", p, n, M, sp), ft.execute_dev(P, False, "N", p, n, M, sp))
+    f(); b()
+    torch.cuda.synchronize()
+    rt = float(np.linalg.norm(d.cpu().numpy() - A.ravel(order="F")) / np.linalg.norm(A))
+    ms = _family_timing(torch, f, b)
+    ms_grid = _family_timing(torch, lambda: grid(PS, False, "N", p, n, M, sp), lambda: grid(PA, True, "N", p, n, M, sp))
+    for q in (P, PS, PA):
+        q.close()
+    return {"coeffs_per_s": coeffs / (ms * 1e-3), "ms_per_step": ms, "grid_synthesis_plus_analysis_ms": ms_grid,
+            "roundtrip_eps2": rt,
+            "workload": f"{kind}: to the Chebyshev / Fourier series, synthesis on the grid, analysis, back ('N'), "
+                        f"degree {n - 1}, 1 field {n} x {M} (plain FP64, cuFFT DFTs inside the grid stage)"}
+
+
 def extra_workloads(args, torch, ft):
     """Secondary workloads (reported beside the headline, same device timing rules)."""
     import numpy as np
@@ -672,6 +821,15 @@ def extra_workloads(args, torch, ft):
     del dz
     SP.close()
     SRP.close()
+    # the other families' drop-in transforms and the disk / triangle grids, one field each, fwd+bwd
+    # 'N' on the device (plain FP64); each in its own guard so that one failure leaves the rest
+    for name, fn in (("rectdisk_n4096", lambda: family_rectdisk(4096)), ("ann_n2048", lambda: family_ann(2048)),
+                     ("tet_n256", lambda: family_tet(256)), ("disk_full_grid_n2048", lambda: family_grid("disk", 2048)),
+                     ("tri_full_grid_n2048", lambda: family_grid("tri", 2048))):
+        try:
+            out[name] = fn()
+        except Exception as exc:
+            out[name] = {"error": repr(exc)[:200]}
     # 64 FP64 sph fields, degrees drawn from {127, 255, 511, 1023, 2047}, one launch per stage,
     # fwd+bwd captured in one CUDA graph
     rng = np.random.default_rng(SEED)
