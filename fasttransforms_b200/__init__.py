@@ -1,8 +1,10 @@
 """B200-native (sm_100a) harmonic-conversion path of FastTransforms.
 
 Python mirror of the reference's C API for sph2fourier / fourier2sph,
-tri2cheb / cheb2tri and disk2cxf / cxf2disk (src/fasttransforms.h:370-415),
-over the C ABI in include/ft_b200.h.  The compute runs in hand-written CUDA
+tri2cheb / cheb2tri and disk2cxf / cxf2disk (src/fasttransforms.h:370-415), the
+sphere's vector-field and spin-weighted transforms, the Dunkl-Xu, annulus and
+tetrahedral transforms and the sphere, disk and triangle grids, over the C ABI
+in include/ft_b200.h.  The compute runs in hand-written CUDA
 kernels in ``_lib/libft_b200.so``; there is no CPU fallback: importing this
 package fails if the library is missing, and planning fails without an sm_100
 device.

@@ -3,13 +3,16 @@
  *
  * Drop-in for FastTransforms' harmonic-conversion path: the Givens-rotation
  * sweeps behind sph2fourier / fourier2sph and the same kernel family used by
- * tri2cheb / cheb2tri and disk2cxf / cxf2disk.  Link with -lft_b200 instead of
+ * tri2cheb / cheb2tri and disk2cxf / cxf2disk, with the sphere's vector-field and
+ * spin-weighted transforms, the Dunkl-Xu, annulus and tetrahedral transforms and
+ * the sphere, disk and triangle grids.  Link with -lft_b200 instead of
  * -lfasttransforms; existing callers of the functions below need no change.
  *
  * Conventions (identical to the reference):
  *   - A is column-major with leading dimension N (host memory for the drop-in
  *     entry points, device memory for the *_dev entry points);
- *     M = 2N-1 (sph), N (tri), 4N-3 (disk).
+ *     M = 2N-1 (sph, spin), N (tri, rectdisk), 4N-3 (disk, annulus);
+ *     N x L x M tensors for the tetrahedron.
  *   - Column pair (2m-1, 2m) carries order m for sph and disk; column m for tri.
  *   - TRANS 'N' applies the operator, 'T' its transpose; any other character
  *     is a no-op (the reference silently ignores it; here the status is

@@ -2,9 +2,10 @@
  * ft_oracle.h -- TEST INFRASTRUCTURE ONLY.
  *
  * A plain-C, single-source restatement of FastTransforms' harmonic-conversion
- * path (sph2fourier / fourier2sph, tri2cheb / cheb2tri, disk2cxf / cxf2disk):
- * rotation tables, scalar Givens sweeps, the execute loops over orders, the
- * dense connection matrices and the triangular multiplies.  It is the checker
+ * path (sph2fourier / fourier2sph, tri2cheb / cheb2tri, disk2cxf / cxf2disk, and
+ * the spin-weighted, Dunkl-Xu, annulus and tetrahedral transforms): rotation
+ * tables, scalar Givens sweeps, the execute loops over orders, the dense
+ * connection matrices and the triangular multiplies.  It is the checker
  * for the CUDA library: only tests, the smoke check and bench.py's CPU
  * baseline may load it.  The product never calls into it.
  *

@@ -50,3 +50,25 @@ def test_no_device_fails_cleanly():
     assert ft.lib.ft_b200_last_status() in (2, 4)
     with pytest.raises(ft.FTB200Error):
         ft.plan_sph2fourier(16)
+
+
+def test_c_caller_compiles_links_and_runs(tmp_path):
+    """A C program written against the reference's API (tests/c/dropin.c) compiles against
+    include/ft_b200.h, links with -lft_b200 and runs: without a usable device it reports
+    FT_B200_ENODEV cleanly; with one, its sph2fourier / fourier2sph round trip is below 1e-13."""
+    import shutil
+    import subprocess
+    import fasttransforms_b200 as ft
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    libdir = os.path.dirname(ft.library_path)
+    exe = str(tmp_path / "dropin")
+    subprocess.run([cc, "-O2", "-std=c11", "-I", os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "c", "dropin.c"),
+                    "-L", libdir, "-lft_b200", "-Wl,-rpath," + libdir, "-lm", "-o", exe], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    if has_gpu():
+        assert float(r.stdout.strip()) < 1e-13
+    else:
+        assert r.stdout.strip() == "ENODEV"
