@@ -1,8 +1,8 @@
 """Oracle (test infrastructure, not the product): a CPU restatement of the
 sphere, disk and triangle grid synthesis and analysis of the reference
-(src/fftw.c:63-330, 404-532: ft_plan_sph_with_kind, ft_execute_sph_synthesis /
-_analysis and the sphv variants, ft_execute_disk_* and ft_execute_tri_*) in numpy /
-scipy.
+(src/fftw.c:63-330, 404-753: ft_plan_sph_with_kind, ft_execute_sph_synthesis /
+_analysis and the sphv variants, ft_execute_disk_*, ft_execute_tri_*, ft_execute_annulus_*
+and ft_execute_rectdisk_*) in numpy / scipy.
 
 FFTW, which the reference calls for these transforms, is not available here, so
 its one-dimensional transforms are restated from their published definitions
@@ -213,3 +213,107 @@ def execute_tri(op, trans, plan, X):
         X[0, :] *= 0.5
         return X / (N * M)
     return _r2r_2d(X / (N * M), kind)
+
+
+# annulus plan kinds (all columns): src/fftw.c:573-581
+ANN_PLANS = {"annulus_synthesis": REDFT01, "annulus_analysis": REDFT10}
+# rectdisk plan kinds (even columns, odd columns, rows): src/fftw.c:687-695
+RECT_PLANS = {"rectdisk_synthesis": (REDFT01, RODFT01, REDFT01), "rectdisk_analysis": (REDFT10, RODFT10, REDFT10)}
+
+
+def annulus_weights(N, rho):
+    """src/fftw.c:545-551: w_n = sqrt(2 (sin^2 t + rho^2 cos^2 t) / (1 - rho^2)), t = (N - n - 1/2) pi / 2N."""
+    w = np.empty(N)
+    for n in range(N):
+        t = (N - n - 0.5) * np.pi / (2.0 * N)
+        ct, st = np.sin(t), np.cos(t)
+        w[n] = np.sqrt(2.0 * (ct * ct + rho * rho * st * st) / (1.0 - rho * rho))
+    return w
+
+
+def _ann_cols(M):
+    return [c for j in range(1, M, 4) for c in (j, j + 1) if c < M]
+
+
+def execute_annulus(op, trans, plan, X, rho):
+    """ft_execute_annulus_{synthesis,analysis}(trans, P, X) with P a plan of kind `plan` (a key of
+    ANN_PLANS) and radius ratio rho, src/fftw.c:583-658: the plan's cosine transform on every
+    column, the columns of classes 1 and 2 weighted by w (divided in analysis), the sph phi stage
+    and scalings, and the first-row factors."""
+    X = np.array(X, dtype=float, copy=True)
+    N, M = X.shape
+    kind = ANN_PLANS[plan]
+    w = annulus_weights(N, rho)[:, None]
+    cols = _ann_cols(M)
+    nm2 = 2.0 * N * M
+    if op == "annulus_synthesis":
+        if trans == "N":
+            X[0, :] *= 2.0
+            X = r2r(X, kind)
+            X[:, cols] *= w
+            X *= M_1_4_SQRT_PI
+            X[:, 0] *= M_SQRT2
+            return c2r(data_r2c(X), M)
+        X = data_c2r(r2c(X), M)
+        X *= M_1_2_SQRT_PI
+        X[:, 0] *= M_SQRT1_2
+        X[:, cols] *= w
+        return r2r(X, kind)
+    if trans == "N":
+        X = data_c2r(r2c(X), M)
+        X *= M_4_SQRT_PI / nm2
+        X[:, 0] *= M_SQRT1_2
+        X[:, cols] /= w
+        X = r2r(X, kind)
+        X[0, :] *= 0.5
+        return X
+    X = r2r(X, kind)
+    X[:, cols] /= w
+    X *= M_2_SQRT_PI / nm2
+    X[:, 0] *= M_SQRT2
+    return c2r(data_r2c(X), M)
+
+
+def _rect_x(X, kinds):
+    Y = X.copy()
+    if Y[:, 0::2].shape[1]:
+        Y[:, 0::2] = r2r(X[:, 0::2], kinds[0])
+    if Y[:, 1::2].shape[1]:
+        Y[:, 1::2] = r2r(X[:, 1::2], kinds[1])
+    return Y
+
+
+def _rect_y(X, kind):
+    return r2r(X.T, kind).T
+
+
+def execute_rectdisk(op, trans, plan, X):
+    """ft_execute_rectdisk_{synthesis,analysis}(trans, P, X), src/fftw.c:697-753: the plan's first
+    kind down the even columns and its second down the odd ones, its third along the rows, with
+    the reference's end-entry factors and scalings."""
+    X = np.array(X, dtype=float, copy=True)
+    N, M = X.shape
+    kinds = RECT_PLANS[plan]
+    if op == "rectdisk_synthesis":
+        if trans == "N":
+            X[0, 0::2] *= 2.0
+            X = _rect_x(X, kinds)
+            X[:, 0] *= 2.0
+            X *= 0.25
+            return _rect_y(X, kinds[2])
+        X = _rect_y(X, kinds[2])
+        X *= 0.25
+        X = _rect_x(X, kinds)
+        X[N - 1, 1::2] *= 0.5
+        return X
+    if trans == "N":
+        X = _rect_y(X, kinds[2])
+        X /= N * M
+        X[:, 0] *= 0.5
+        X = _rect_x(X, kinds)
+        X[0, 0::2] *= 0.5
+        return X
+    X[N - 1, 1::2] *= 2.0
+    X = _rect_x(X, kinds)
+    X = _rect_y(X, kinds[2])
+    return X / (N * M)

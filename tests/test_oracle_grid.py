@@ -151,3 +151,59 @@ def test_tri_grid_is_a_2d_cosine_series():
         got = G.execute_tri("tri_synthesis", "N", "tri_synthesis", A)
         want = np.outer(np.cos(i * th), np.cos(j * th))
         assert np.abs(got - want).max() < 1e-14, (i, j)
+
+
+@pytest.mark.parametrize("N", [64, 128])
+def test_annulus_reference_round_trip(ref, N):
+    """test/test_fftw.c:288-320 (rho = sqrt(1/3), plans crossed in 'T'): the compiled reference's
+    ann2cxf / cxf2ann around the oracle's annulus synthesis and analysis: 8 sqrt(N) eps, 4N eps."""
+    from fasttransforms_b200.utilities import rand_layout
+    rho = np.sqrt(1 / 3)
+    A = rand_layout("disk", N, 5)
+    P = ref.ann_plan(N, 0.0, 0.0, rho)
+    X = A.copy(order="F")
+    ref.ann_execute(P, True, "N", X)
+    X = G.execute_annulus("annulus_synthesis", "N", "annulus_synthesis", X, rho)
+    X = np.asfortranarray(G.execute_annulus("annulus_analysis", "N", "annulus_analysis", X, rho))
+    ref.ann_execute(P, False, "N", X)
+    ref.ann_execute(P, True, "T", X)
+    X = G.execute_annulus("annulus_synthesis", "T", "annulus_analysis", X, rho)
+    X = np.asfortranarray(G.execute_annulus("annulus_analysis", "T", "annulus_synthesis", X, rho))
+    ref.ann_execute(P, False, "T", X)
+    ref.destroy(P)
+    assert np.linalg.norm(X - A) / np.linalg.norm(A) <= 8 * np.sqrt(N) * EPS
+    assert np.abs(X - A).max() / np.abs(A).max() <= 4 * N * EPS
+
+
+@pytest.mark.parametrize("N", [64, 128])
+def test_rectdisk_reference_round_trip(ref, N):
+    """test/test_fftw.c:350-380 (M = N, beta = 0, plans crossed in 'T'): 8 sqrt(N) eps, 4N eps."""
+    from fasttransforms_b200.utilities import rand_layout
+    A = rand_layout("rect", N, 5)
+    P = ref.plan("rect", N, beta=0.0)
+    X = A.copy(order="F")
+    ref.execute("rect", P, True, "N", X)
+    X = G.execute_rectdisk("rectdisk_synthesis", "N", "rectdisk_synthesis", X)
+    X = np.asfortranarray(G.execute_rectdisk("rectdisk_analysis", "N", "rectdisk_analysis", X))
+    ref.execute("rect", P, False, "N", X)
+    ref.execute("rect", P, True, "T", X)
+    X = G.execute_rectdisk("rectdisk_synthesis", "T", "rectdisk_analysis", X)
+    X = np.asfortranarray(G.execute_rectdisk("rectdisk_analysis", "T", "rectdisk_synthesis", X))
+    ref.execute("rect", P, False, "T", X)
+    ref.destroy(P)
+    assert np.linalg.norm(X - A) / np.linalg.norm(A) <= 8 * np.sqrt(N) * EPS
+    assert np.abs(X - A).max() / np.abs(A).max() <= 4 * N * EPS
+
+
+def test_rectdisk_grid_is_a_chebyshev_product():
+    """Known answer: the rectdisk synthesis of a unit coefficient in an even column j = 2q is
+    T_i(x) T_j(y) (the plan's DCT-III down the even columns and along the rows, with the
+    reference's factors) on the Chebyshev points."""
+    N = 9
+    th = (np.arange(N) + 0.5) * np.pi / N
+    for i, j in [(1, 2), (3, 4), (2, 6)]:
+        A = np.zeros((N, N))
+        A[i, j] = 1.0
+        got = G.execute_rectdisk("rectdisk_synthesis", "N", "rectdisk_synthesis", A)
+        want = np.outer(np.cos(i * th), np.cos(j * th))
+        assert np.abs(got - want).max() < 1e-14, (i, j)
