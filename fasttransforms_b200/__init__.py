@@ -46,6 +46,9 @@ __all__ = [
     "plan_ann2cxf", "execute_ann2cxf", "execute_cxf2ann", "plan_rotannulus",
     "plan_disk_synthesis", "plan_disk_analysis", "execute_disk_synthesis", "execute_disk_analysis", "execute_disk_grid_dev",
     "plan_tri_synthesis", "plan_tri_analysis", "execute_tri_synthesis", "execute_tri_analysis", "execute_tri_grid_dev",
+    "plan_annulus_synthesis", "plan_annulus_analysis", "execute_annulus_synthesis", "execute_annulus_analysis",
+    "execute_annulus_grid_dev", "plan_rectdisk_synthesis", "plan_rectdisk_analysis", "execute_rectdisk_synthesis",
+    "execute_rectdisk_analysis", "execute_rectdisk_grid_dev",
     "SPH", "TRI", "DISK",
 ]
 
@@ -105,13 +108,20 @@ def _load() -> C.CDLL:
         "ft_destroy_triangle_fftw_plan": (None, [vp]),
         "ft_b200_execute_disk_grid_dev": (i, [vp, i, ch, vp, i, i, vp]),
         "ft_b200_execute_tri_grid_dev": (i, [vp, i, ch, vp, i, i, vp]),
+        "ft_plan_annulus_synthesis": (vp, [i, i, d, C.c_uint]), "ft_plan_annulus_analysis": (vp, [i, i, d, C.c_uint]),
+        "ft_destroy_annulus_fftw_plan": (None, [vp]), "ft_get_rho_annulus_fftw_plan": (d, [vp]),
+        "ft_plan_rectdisk_synthesis": (vp, [i, i, C.c_uint]), "ft_plan_rectdisk_analysis": (vp, [i, i, C.c_uint]),
+        "ft_destroy_rectdisk_fftw_plan": (None, [vp]),
+        "ft_b200_execute_annulus_grid_dev": (i, [vp, i, ch, vp, i, i, vp]),
+        "ft_b200_execute_rectdisk_grid_dev": (i, [vp, i, ch, vp, i, i, vp]),
         "ft_execute_tet2cheb": (None, [ch, vp, dp, i, i, i]), "ft_execute_cheb2tet": (None, [ch, vp, dp, i, i, i]),
         "ft_execute_tet_hi2lo": (None, [vp, vp, dp, i, i]), "ft_execute_tet_lo2hi": (None, [vp, vp, dp, i, i]),
         "ft_b200_execute_tet_dev": (i, [vp, i, ch, vp, i, i, i, vp]),
         "ft_b200_tet_rotations_dev": (i, [vp, i, vp, i, i, vp]),
     }
     for name in ("sph_synthesis", "sph_analysis", "sphv_synthesis", "sphv_analysis", "disk_synthesis", "disk_analysis",
-                 "tri_synthesis", "tri_analysis"):
+                 "tri_synthesis", "tri_analysis", "annulus_synthesis", "annulus_analysis", "rectdisk_synthesis",
+                 "rectdisk_analysis"):
         sig["ft_execute_" + name] = (None, [ch, vp, dp, i, i])
     for name in ("sph2fourier", "fourier2sph", "tri2cheb", "cheb2tri", "disk2cxf", "cxf2disk", "sphv2fourier", "fourier2sphv",
                  "rectdisk2cheb", "cheb2rectdisk", "ann2cxf", "cxf2ann"):
@@ -282,6 +292,54 @@ class DiskGridPlan(_FamilyGridPlan):
 
 class TriGridPlan(_FamilyGridPlan):
     _destroy = "ft_destroy_triangle_fftw_plan"
+
+
+class AnnulusGridPlan(_FamilyGridPlan):
+    _destroy = "ft_destroy_annulus_fftw_plan"
+
+    @property
+    def rho(self) -> float:
+        return lib.ft_get_rho_annulus_fftw_plan(self.ptr)
+
+
+class RectdiskGridPlan(_FamilyGridPlan):
+    _destroy = "ft_destroy_rectdisk_fftw_plan"
+
+
+def plan_annulus_synthesis(n: int, rho: float, m: int = None) -> AnnulusGridPlan:
+    m = 4 * n - 3 if m is None else m
+    ptr = lib.ft_plan_annulus_synthesis(n, m, rho, 0)
+    if not ptr:
+        _check()
+        raise FTB200Error(-1, "plan creation failed")
+    return AnnulusGridPlan(ptr, "annulus_synthesis", n, m)
+
+
+def plan_annulus_analysis(n: int, rho: float, m: int = None) -> AnnulusGridPlan:
+    m = 4 * n - 3 if m is None else m
+    ptr = lib.ft_plan_annulus_analysis(n, m, rho, 0)
+    if not ptr:
+        _check()
+        raise FTB200Error(-1, "plan creation failed")
+    return AnnulusGridPlan(ptr, "annulus_analysis", n, m)
+
+
+def plan_rectdisk_synthesis(n: int, m: int = None) -> RectdiskGridPlan: return _family_plan(RectdiskGridPlan, "ft_plan_rectdisk_synthesis", n, n if m is None else m)
+def plan_rectdisk_analysis(n: int, m: int = None) -> RectdiskGridPlan: return _family_plan(RectdiskGridPlan, "ft_plan_rectdisk_analysis", n, n if m is None else m)
+
+
+def execute_annulus_grid_dev(P: AnnulusGridPlan, analysis: bool, trans: str, ptr: int, N: int, M: int, stream: int = 0) -> None:
+    """The annulus grid's synthesis (analysis = False) or analysis sequence with P's kind and rho."""
+    st = lib.ft_b200_execute_annulus_grid_dev(P.ptr, 1 if analysis else 0, trans.encode(), C.c_void_p(ptr), N, M, C.c_void_p(stream))
+    if st != 0:
+        _check()
+
+
+def execute_rectdisk_grid_dev(P: RectdiskGridPlan, analysis: bool, trans: str, ptr: int, N: int, M: int, stream: int = 0) -> None:
+    """The rectangularised disk grid's synthesis (analysis = False) or analysis sequence with P's kinds."""
+    st = lib.ft_b200_execute_rectdisk_grid_dev(P.ptr, 1 if analysis else 0, trans.encode(), C.c_void_p(ptr), N, M, C.c_void_p(stream))
+    if st != 0:
+        _check()
 
 
 def _family_plan(cls, fname, n, m):
@@ -493,6 +551,10 @@ def execute_disk_synthesis(trans, P, A, N=None, M=None): _exec_host("ft_execute_
 def execute_disk_analysis(trans, P, A, N=None, M=None): _exec_host("ft_execute_disk_analysis", trans, P, A, N, M)
 def execute_tri_synthesis(trans, P, A, N=None, M=None): _exec_host("ft_execute_tri_synthesis", trans, P, A, N, M)
 def execute_tri_analysis(trans, P, A, N=None, M=None): _exec_host("ft_execute_tri_analysis", trans, P, A, N, M)
+def execute_annulus_synthesis(trans, P, A, N=None, M=None): _exec_host("ft_execute_annulus_synthesis", trans, P, A, N, M)
+def execute_annulus_analysis(trans, P, A, N=None, M=None): _exec_host("ft_execute_annulus_analysis", trans, P, A, N, M)
+def execute_rectdisk_synthesis(trans, P, A, N=None, M=None): _exec_host("ft_execute_rectdisk_synthesis", trans, P, A, N, M)
+def execute_rectdisk_analysis(trans, P, A, N=None, M=None): _exec_host("ft_execute_rectdisk_analysis", trans, P, A, N, M)
 def execute_fourier2sph(trans, P, A, N=None, M=None): _exec_host("ft_execute_fourier2sph", trans, P, A, N, M)
 def execute_tri2cheb(trans, P, A, N=None, M=None): _exec_host("ft_execute_tri2cheb", trans, P, A, N, M)
 def execute_cheb2tri(trans, P, A, N=None, M=None): _exec_host("ft_execute_cheb2tri", trans, P, A, N, M)

@@ -26,6 +26,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <vector>
 
 #include <cufft.h>
 
@@ -36,9 +37,11 @@ namespace {
 
 // FFTW r2r kinds used by the plans (the values of fftw3.h's enum)
 enum { K_REDFT01 = 4, K_REDFT10 = 5, K_REDFT11 = 6, K_RODFT01 = 8, K_RODFT10 = 9 };
-enum Op { SPH_SYN = 0, SPH_ANA = 1, SPHV_SYN = 2, SPHV_ANA = 3, DISK_SYN = 4, DISK_ANA = 5, TRI_SYN = 6, TRI_ANA = 7 };
-// plan families: the sphere's (sph, sphv), the disk's, the triangle's
-enum Family { F_SPHERE = 0, F_DISK = 1, F_TRI = 2 };
+enum Op { SPH_SYN = 0, SPH_ANA = 1, SPHV_SYN = 2, SPHV_ANA = 3, DISK_SYN = 4, DISK_ANA = 5, TRI_SYN = 6, TRI_ANA = 7,
+          ANN_SYN = 8, ANN_ANA = 9, RECT_SYN = 10, RECT_ANA = 11 };
+// plan families: the sphere's (sph, sphv), the disk's, the triangle's, the annulus's, the
+// rectangularised disk's
+enum Family { F_SPHERE = 0, F_DISK = 1, F_TRI = 2, F_ANN = 3, F_RECT = 4 };
 
 constexpr int kGridMagic = 0x46544753;   // "FTGS"
 
@@ -59,7 +62,11 @@ struct SphereGridPlan {
     int magic = kGridMagic;
     int family = F_SPHERE;
     int N = 0, M = 0;
-    int kind[2] = {0, 0};        // theta kinds of column classes {0, 3} and {1, 2} (tri: both dimensions)
+    int kind[2] = {0, 0};        // theta kinds of column classes {0, 3} and {1, 2} (tri: both dimensions;
+                                 // rect: even and odd columns)
+    int kind_rows = 0;           // rect: the kind along the rows
+    double rho = 0.0;            // annulus: the radius ratio
+    double * d_w = nullptr;      // annulus: the N radial weights
     int device = 0;
     cufftHandle t_r2c = 0;       // length N, batch M (cosine type II)
     cufftHandle t_c2r = 0;       // length N, batch M (cosine type III)
@@ -87,7 +94,9 @@ namespace {
 // theta stage kernels: one thread per (entry, column); column j uses the kind of
 // its class, cls(j) = j mod 4 in {0, 3} -> kind[0], {1, 2} -> kind[1]
 // ---------------------------------------------------------------------------
+// k1dst bit 1 set: the classes are the even and odd columns instead (the rectangularised disk's)
 __device__ __forceinline__ bool col_dst(int j, int k0dst, int k1dst) {
+    if (k1dst & 2) return (j & 1) ? (k1dst & 1) : k0dst;
     const int r = j & 3;
     return (r == 0 || r == 3) ? k0dst : k1dst;
 }
@@ -184,6 +193,37 @@ __global__ void dct4_post(const double2 * __restrict__ U, double * __restrict__ 
     X[(long long) class12_col(q) * N + k] = 2.0 * (c * v.x + s * v.y);   // 2 Re((c - i s) v)
 }
 
+// entries (row, start + step t) times f
+__global__ void scale_row(double * X, int N, int M, int row, int start, int step, double f) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const long long j = start + (long long) step * t;
+    if (j < M) X[j * N + row] *= f;
+}
+
+// annulus: the columns of classes 1 and 2 (j mod 4 = 1, 2) times w_i (divide: divided by w_i)
+__global__ void ann_weights(double * X, const double * __restrict__ w, int N, int M, bool divide) {
+    const long long idx = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long) N * M) return;
+    const int j = (int) (idx / N), i = (int) (idx % N);
+    const int r = j & 3;
+    if (r != 1 && r != 2) return;
+    X[idx] = divide ? X[idx] / w[i] : X[idx] * w[i];
+}
+
+// rect: column 0 times f0 and every entry times s or divided by d (d > 0), in the reference's order
+// (f0 first when f0_first, else last)
+__global__ void col0_scale(double * X, int N, int M, double f0, double s, double d, bool f0_first) {
+    const long long total = (long long) N * M;
+    for (long long e = blockIdx.x * (long long) blockDim.x + threadIdx.x; e < total; e += (long long) gridDim.x * blockDim.x) {
+        const bool c0 = e < N;
+        double v = X[e];
+        if (f0_first && c0) v *= f0;
+        v = d > 0.0 ? v / d : v * s;
+        if (!f0_first && c0) v *= f0;
+        X[e] = v;
+    }
+}
+
 // triangle scalings (src/fftw.c:292-330), entry (i, j) of the N x M matrix: times ef when
 // j == 0, times ef when i == 0, then times s (mul) or divided by d (d > 0)
 __global__ void tri_scale(double * X, int N, int M, double ef, double s, double d) {
@@ -248,28 +288,30 @@ bool fok(cufftResult r, const char * what) {
 
 unsigned blocks(long long n) { return (unsigned) ((n + 255) / 256); }
 
-SphereGridPlan * make_plan(int N, int M, int k0, int k1, int family = F_SPHERE) {
+SphereGridPlan * make_plan(int N, int M, int k0, int k1, int family = F_SPHERE, int krows = 0, double rho = 0.0) {
     clear_error();
+    const bool square = family == F_TRI || family == F_RECT;   // row transforms through a square transpose
     if (N < 1 || M < 1) { set_error(FT_B200_EINVAL, "N and M must be positive"); return nullptr; }
-    if (family != F_TRI && M % 2 == 0) {
+    if (!square && M % 2 == 0) {
         set_error(FT_B200_EINVAL, "M must be odd (the half spectrum holds columns 2j - 1, 2j)");
         return nullptr;
     }
-    if (family == F_TRI && M != N) {
-        set_error(FT_B200_EINVAL, "triangle grids need M == N (the reference's 2-D plan reads the matrix both ways)");
+    if (square && M != N) {
+        set_error(FT_B200_EINVAL, family == F_TRI ? "triangle grids need M == N (the reference's 2-D plan reads the matrix both ways)"
+                                                  : "rectangularised-disk grids need M == N here (the rows go through a square transpose)");
         return nullptr;
     }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { set_error(FT_B200_ENODEV, "no CUDA device"); return nullptr; }
     SphereGridPlan * P = new SphereGridPlan();
     P->family = family;
-    P->N = N; P->M = M; P->kind[0] = k0; P->kind[1] = k1;
+    P->N = N; P->M = M; P->kind[0] = k0; P->kind[1] = k1; P->kind_rows = krows; P->rho = rho;
     cudaGetDevice(&P->device);
     const size_t nm = (size_t) N * M;
     bool good = ok(cudaMalloc(&P->d_work, sizeof(double) * nm), "cudaMalloc(grid work)") &&
                 ok(cudaMalloc(&P->d_cwork, sizeof(double2) * (size_t) (N / 2 + 1) * M), "cudaMalloc(grid work)") &&
-                (family == F_TRI || ok(cudaMalloc(&P->d_Y, sizeof(double2) * (size_t) N * (M / 2 + 1)), "cudaMalloc(grid spectrum)")) &&
-                (family != F_TRI || ok(cudaMalloc(&P->d_work2, sizeof(double) * nm), "cudaMalloc(grid work)")) &&
+                (square || ok(cudaMalloc(&P->d_Y, sizeof(double2) * (size_t) N * (M / 2 + 1)), "cudaMalloc(grid spectrum)")) &&
+                (!square || ok(cudaMalloc(&P->d_work2, sizeof(double) * nm), "cudaMalloc(grid work)")) &&
                 ok(cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     if (good && family == F_DISK) {
         P->nq = (M + 2) / 4 + (M + 1) / 4;
@@ -290,7 +332,17 @@ SphereGridPlan * make_plan(int N, int M, int k0, int k1, int family = F_SPHERE) 
             P->have_t_r2c = good;
         }
     }
-    if (good && family != F_TRI) {
+    if (good && family == F_ANN) {   // src/fftw.c:545-551
+        std::vector<double> w(N);
+        for (int n = 0; n < N; n++) {
+            const double t = (N - n - 0.5) * M_PI / (2.0 * N);
+            const double ct = std::sin(t), st = std::cos(t);
+            w[n] = std::sqrt(2.0 * (ct * ct + rho * rho * st * st) / (1.0 - rho * rho));
+        }
+        good = ok(cudaMalloc(&P->d_w, sizeof(double) * N), "cudaMalloc(weights)") &&
+               ok(cudaMemcpy(P->d_w, w.data(), sizeof(double) * N, cudaMemcpyHostToDevice), "cudaMemcpy(weights)");
+    }
+    if (good && !square) {
         // phi: along rows, element stride N, rows one apart
         int m[1] = {M}, hm[1] = {M / 2 + 1};
         good = fok(cufftPlanMany(&P->p_c2r, 1, m, hm, N, 1, m, N, 1, CUFFT_Z2D, N), "cufftPlanMany");
@@ -309,9 +361,13 @@ SphereGridPlan * make_plan(int N, int M, int k0, int k1, int family = F_SPHERE) 
 
 // theta transforms of all M columns in place (the plan's kinds by column class; disk: kind[0]
 // on every column here, the DCT-IV of classes 1 and 2 in theta_disk)
-bool theta(SphereGridPlan * P, double * X, cudaStream_t st) {
+bool theta(SphereGridPlan * P, double * X, cudaStream_t st, bool rows = false) {
     const int N = P->N, M = P->M;
-    const int d0 = is_dst(P->kind[0]), d1 = P->family == F_SPHERE ? is_dst(P->kind[1]) : d0;
+    int d0 = is_dst(P->kind[0]), d1 = P->family == F_SPHERE ? is_dst(P->kind[1]) : d0;
+    if (P->family == F_RECT) {
+        if (rows) { d0 = is_dst(P->kind_rows); d1 = d0; }   // every column of the transposed matrix
+        else d1 = is_dst(P->kind[1]) | 2;                    // even and odd columns
+    }
     if (is_type3(P->kind[0])) {
         if (!fok(cufftSetStream(P->t_c2r, st), "cufftSetStream")) return false;
         t3_pre<<<blocks((long long) (N / 2 + 1) * M), 256, 0, st>>>(X, P->d_cwork, N, M, d0, d1);
@@ -357,6 +413,36 @@ bool theta_tri(SphereGridPlan * P, double * X, cudaStream_t st) {
     double * a[1] = {X}, * b[1] = {P->d_work2};
     return theta(P, X, st) && ok(launch_transpose_square(a, b, 1, P->N, st), "transpose") && theta(P, P->d_work2, st) &&
            ok(launch_transpose_square(b, a, 1, P->N, st), "transpose");
+}
+
+// rect: the plan's row kind along the rows of the square matrix (transpose, columns, transpose back)
+bool theta_rows(SphereGridPlan * P, double * X, cudaStream_t st) {
+    double * a[1] = {X}, * b[1] = {P->d_work2};
+    return ok(launch_transpose_square(a, b, 1, P->N, st), "transpose") && theta(P, P->d_work2, st, true) &&
+           ok(launch_transpose_square(b, a, 1, P->N, st), "transpose");
+}
+
+bool row_factor(SphereGridPlan * P, double * X, int row, int start, int step, double f, cudaStream_t st) {
+    const int t = (P->M - start + step - 1) / step;
+    if (t <= 0) return true;
+    scale_row<<<blocks(t), 256, 0, st>>>(X, P->N, P->M, row, start, step, f);
+    count_launch();
+    return ok(cudaGetLastError(), "scale_row");
+}
+
+bool weights(SphereGridPlan * P, double * X, bool divide, cudaStream_t st) {
+    ann_weights<<<blocks((long long) P->N * P->M), 256, 0, st>>>(X, P->d_w, P->N, P->M, divide);
+    count_launch();
+    return ok(cudaGetLastError(), "ann_weights");
+}
+
+bool col0_scaling(SphereGridPlan * P, double * X, double f0, double s, double d, bool f0_first, cudaStream_t st) {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    col0_scale<<<sms * 4, 256, 0, st>>>(X, P->N, P->M, f0, s, d, f0_first);
+    count_launch();
+    return ok(cudaGetLastError(), "col0_scale");
 }
 
 bool tri_scaling(SphereGridPlan * P, double * X, double ef, double s, double d, cudaStream_t st) {
@@ -408,6 +494,29 @@ bool run(SphereGridPlan * P, int op, char T, double * X, cudaStream_t st) {
         if (T == 'N') return phi_r2c(P, X, C_4_SQRT_PI / nm2, C_SQRT1_2, st) && theta_disk(P, X, st) && first(0.5);
         return theta_disk(P, X, st) && phi_c2r(P, X, C_2_SQRT_PI / nm2, C_SQRT2, st);
     }
+    if (op == ANN_SYN || op == ANN_ANA) {     // src/fftw.c:583-658: every column the plan's kind, classes 1, 2 weighted
+        if (op == ANN_SYN) {
+            if (T == 'N') return row_factor(P, X, 0, 0, 1, 2.0, st) && theta(P, X, st) && weights(P, X, false, st) &&
+                                 phi_c2r(P, X, C_1_4_SQRT_PI, C_SQRT2, st);
+            return phi_r2c(P, X, C_1_2_SQRT_PI, C_SQRT1_2, st) && weights(P, X, false, st) && theta(P, X, st);
+        }
+        if (T == 'N') return phi_r2c(P, X, C_4_SQRT_PI / nm2, C_SQRT1_2, st) && weights(P, X, true, st) && theta(P, X, st) &&
+                             row_factor(P, X, 0, 0, 1, 0.5, st);
+        return theta(P, X, st) && weights(P, X, true, st) && phi_c2r(P, X, C_2_SQRT_PI / nm2, C_SQRT2, st);
+    }
+    if (op == RECT_SYN || op == RECT_ANA) {   // src/fftw.c:697-753
+        const double nm = (double) (N * M);
+        if (op == RECT_SYN) {
+            if (T == 'N') return row_factor(P, X, 0, 0, 2, 2.0, st) && theta(P, X, st) && col0_scaling(P, X, 2.0, 0.25, 0.0, true, st) &&
+                                 theta_rows(P, X, st);
+            return theta_rows(P, X, st) && col0_scaling(P, X, 1.0, 0.25, 0.0, true, st) && theta(P, X, st) &&
+                   row_factor(P, X, N - 1, 1, 2, 0.5, st);
+        }
+        if (T == 'N') return theta_rows(P, X, st) && col0_scaling(P, X, 0.5, 1.0, nm, false, st) && theta(P, X, st) &&
+                             row_factor(P, X, 0, 0, 2, 0.5, st);
+        return row_factor(P, X, N - 1, 1, 2, 2.0, st) && theta(P, X, st) && theta_rows(P, X, st) &&
+               col0_scaling(P, X, 1.0, 1.0, nm, false, st);
+    }
     if (op == TRI_SYN || op == TRI_ANA) {     // src/fftw.c:292-330
         if (N <= 1 || M <= 1) return true;
         const double nm = (double) (N * M);
@@ -431,7 +540,12 @@ SphereGridPlan * as_grid(const ft_sphere_fftw_plan * P) {
     return (G && G->magic == kGridMagic) ? G : nullptr;
 }
 
-int family_of(int op) { return op <= SPHV_ANA ? F_SPHERE : (op <= DISK_ANA ? F_DISK : F_TRI); }
+int family_of(int op) {
+    if (op <= SPHV_ANA) return F_SPHERE;
+    if (op <= DISK_ANA) return F_DISK;
+    if (op <= TRI_ANA) return F_TRI;
+    return op <= ANN_ANA ? F_ANN : F_RECT;
+}
 
 int check_call(SphereGridPlan * G, char T, const double * X, int N, int M, int family = F_SPHERE) {
     if (!G || G->family != family) { set_error(FT_B200_EINVAL, "not a grid plan of this family of this library"); return FT_B200_EINVAL; }
@@ -484,6 +598,7 @@ void ft_destroy_sphere_fftw_plan(ft_sphere_fftw_plan * Pp) {
     if (P->have_p_c2r) cufftDestroy(P->p_c2r);
     if (P->have_t4) cufftDestroy(P->t4);
     cudaFree(P->d_work); cudaFree(P->d_cwork); cudaFree(P->d_Y); cudaFree(P->d_stage); cudaFree(P->d_u); cudaFree(P->d_work2);
+    cudaFree(P->d_w);
     if (P->stream) cudaStreamDestroy(P->stream);
     P->magic = 0;
     delete P;
@@ -534,6 +649,62 @@ void ft_execute_tri_synthesis(const char TRANS, const ft_triangle_fftw_plan * P,
 }
 void ft_execute_tri_analysis(const char TRANS, const ft_triangle_fftw_plan * P, double * X, const int N, const int M) {
     execute_host(TRI_ANA, TRANS, P, X, N, M);
+}
+
+ft_annulus_fftw_plan * ft_plan_annulus_synthesis(const int N, const int M, const double rho, const unsigned) {
+    return reinterpret_cast<ft_annulus_fftw_plan *>(make_plan(N, M, K_REDFT01, K_REDFT01, F_ANN, 0, rho));
+}
+ft_annulus_fftw_plan * ft_plan_annulus_analysis(const int N, const int M, const double rho, const unsigned) {
+    return reinterpret_cast<ft_annulus_fftw_plan *>(make_plan(N, M, K_REDFT10, K_REDFT10, F_ANN, 0, rho));
+}
+void ft_destroy_annulus_fftw_plan(ft_annulus_fftw_plan * P) {
+    SphereGridPlan * G = as_grid(reinterpret_cast<ft_sphere_fftw_plan *>(P));
+    if (G && G->family == F_ANN) ft_destroy_sphere_fftw_plan(reinterpret_cast<ft_sphere_fftw_plan *>(P));
+}
+double ft_get_rho_annulus_fftw_plan(ft_annulus_fftw_plan * P) {
+    SphereGridPlan * G = as_grid(reinterpret_cast<ft_sphere_fftw_plan *>(P));
+    return (G && G->family == F_ANN) ? G->rho : 0.0;
+}
+void ft_execute_annulus_synthesis(const char TRANS, const ft_annulus_fftw_plan * P, double * X, const int N, const int M) {
+    execute_host(ANN_SYN, TRANS, P, X, N, M);
+}
+void ft_execute_annulus_analysis(const char TRANS, const ft_annulus_fftw_plan * P, double * X, const int N, const int M) {
+    execute_host(ANN_ANA, TRANS, P, X, N, M);
+}
+
+ft_rectdisk_fftw_plan * ft_plan_rectdisk_synthesis(const int N, const int M, const unsigned) {
+    return reinterpret_cast<ft_rectdisk_fftw_plan *>(make_plan(N, M, K_REDFT01, K_RODFT01, F_RECT, K_REDFT01));
+}
+ft_rectdisk_fftw_plan * ft_plan_rectdisk_analysis(const int N, const int M, const unsigned) {
+    return reinterpret_cast<ft_rectdisk_fftw_plan *>(make_plan(N, M, K_REDFT10, K_RODFT10, F_RECT, K_REDFT10));
+}
+void ft_destroy_rectdisk_fftw_plan(ft_rectdisk_fftw_plan * P) {
+    SphereGridPlan * G = as_grid(reinterpret_cast<ft_sphere_fftw_plan *>(P));
+    if (G && G->family == F_RECT) ft_destroy_sphere_fftw_plan(reinterpret_cast<ft_sphere_fftw_plan *>(P));
+}
+void ft_execute_rectdisk_synthesis(const char TRANS, const ft_rectdisk_fftw_plan * P, double * X, const int N, const int M) {
+    execute_host(RECT_SYN, TRANS, P, X, N, M);
+}
+void ft_execute_rectdisk_analysis(const char TRANS, const ft_rectdisk_fftw_plan * P, double * X, const int N, const int M) {
+    execute_host(RECT_ANA, TRANS, P, X, N, M);
+}
+
+int ft_b200_execute_annulus_grid_dev(const ft_annulus_fftw_plan * P, int analysis, char TRANS, double * dX, int N, int M, void * stream) {
+    clear_error();
+    SphereGridPlan * G = as_grid(reinterpret_cast<const ft_sphere_fftw_plan *>(P));
+    const int c = check_call(G, TRANS, dX, N, M, F_ANN);
+    if (c != FT_B200_OK) return c;
+    std::lock_guard<std::mutex> lk(G->mu);
+    return run(G, analysis ? ANN_ANA : ANN_SYN, TRANS, dX, static_cast<cudaStream_t>(stream)) ? FT_B200_OK : ft_b200_last_status();
+}
+
+int ft_b200_execute_rectdisk_grid_dev(const ft_rectdisk_fftw_plan * P, int analysis, char TRANS, double * dX, int N, int M, void * stream) {
+    clear_error();
+    SphereGridPlan * G = as_grid(reinterpret_cast<const ft_sphere_fftw_plan *>(P));
+    const int c = check_call(G, TRANS, dX, N, M, F_RECT);
+    if (c != FT_B200_OK) return c;
+    std::lock_guard<std::mutex> lk(G->mu);
+    return run(G, analysis ? RECT_ANA : RECT_SYN, TRANS, dX, static_cast<cudaStream_t>(stream)) ? FT_B200_OK : ft_b200_last_status();
 }
 
 int ft_b200_execute_disk_grid_dev(const ft_disk_fftw_plan * P, int analysis, char TRANS, double * dX, int N, int M, void * stream) {

@@ -184,6 +184,31 @@ void ft_destroy_triangle_fftw_plan(ft_triangle_fftw_plan * P);
 void ft_execute_tri_synthesis(const char TRANS, const ft_triangle_fftw_plan * P, double * X, const int N, const int M);
 void ft_execute_tri_analysis(const char TRANS, const ft_triangle_fftw_plan * P, double * X, const int N, const int M);
 
+/* Annulus grids (src/fftw.c:534-658): M odd (the reference's M = 4N - 3), rho the radius ratio. */
+typedef struct ft_annulus_fftw_plan_s ft_annulus_fftw_plan;
+/* replace ft_plan_annulus_synthesis / ft_plan_annulus_analysis, src/fftw.c:573-581 */
+ft_annulus_fftw_plan * ft_plan_annulus_synthesis(const int N, const int M, const double rho, const unsigned flags);
+ft_annulus_fftw_plan * ft_plan_annulus_analysis(const int N, const int M, const double rho, const unsigned flags);
+/* replaces ft_destroy_annulus_fftw_plan, src/fftw.c:524-530 */
+void ft_destroy_annulus_fftw_plan(ft_annulus_fftw_plan * P);
+/* replaces ft_get_rho_annulus_fftw_plan, src/fftw.c:532 */
+double ft_get_rho_annulus_fftw_plan(ft_annulus_fftw_plan * P);
+/* replace ft_execute_annulus_synthesis / ft_execute_annulus_analysis, src/fftw.c:583-658 */
+void ft_execute_annulus_synthesis(const char TRANS, const ft_annulus_fftw_plan * P, double * X, const int N, const int M);
+void ft_execute_annulus_analysis(const char TRANS, const ft_annulus_fftw_plan * P, double * X, const int N, const int M);
+
+/* Dunkl-Xu (rectangularised disk) grids (src/fftw.c:653-753): M must equal N here (the rows go
+ * through a square transpose; the reference's tests use M = N). */
+typedef struct ft_rectdisk_fftw_plan_s ft_rectdisk_fftw_plan;
+/* replace ft_plan_rectdisk_synthesis / ft_plan_rectdisk_analysis, src/fftw.c:687-695 */
+ft_rectdisk_fftw_plan * ft_plan_rectdisk_synthesis(const int N, const int M, const unsigned flags);
+ft_rectdisk_fftw_plan * ft_plan_rectdisk_analysis(const int N, const int M, const unsigned flags);
+/* replaces ft_destroy_rectdisk_fftw_plan, src/fftw.c:653-658 */
+void ft_destroy_rectdisk_fftw_plan(ft_rectdisk_fftw_plan * P);
+/* replace ft_execute_rectdisk_synthesis / ft_execute_rectdisk_analysis, src/fftw.c:697-753 */
+void ft_execute_rectdisk_synthesis(const char TRANS, const ft_rectdisk_fftw_plan * P, double * X, const int N, const int M);
+void ft_execute_rectdisk_analysis(const char TRANS, const ft_rectdisk_fftw_plan * P, double * X, const int N, const int M);
+
 /* Spin-weighted spherical harmonics.  Complex matrices are interleaved (re, im)
  * doubles, N x M column-major: column 0 holds order 0, columns 2m - 1 and 2m the
  * orders -m and m (src/drivers.c:645-695).  M must be odd. */
@@ -270,6 +295,8 @@ int ft_b200_execute_sph_grid_dev(const ft_sphere_fftw_plan * P, int op, char TRA
  * tests cross them), asynchronous on stream.  No counterpart in the reference. */
 int ft_b200_execute_disk_grid_dev(const ft_disk_fftw_plan * P, int analysis, char TRANS, double * dX, int N, int M, void * stream);
 int ft_b200_execute_tri_grid_dev(const ft_triangle_fftw_plan * P, int analysis, char TRANS, double * dX, int N, int M, void * stream);
+int ft_b200_execute_annulus_grid_dev(const ft_annulus_fftw_plan * P, int analysis, char TRANS, double * dX, int N, int M, void * stream);
+int ft_b200_execute_rectdisk_grid_dev(const ft_rectdisk_fftw_plan * P, int analysis, char TRANS, double * dX, int N, int M, void * stream);
 
 /* The sph vector-field transforms on device memory (forward = 1: sphv2fourier). */
 int ft_b200_execute_sphv_dev(const ft_harmonic_plan * P, int forward, char TRANS, double * dA, int N, int M, void * stream);

@@ -254,3 +254,97 @@ def test_family_bad_arguments(env):
         ft.plan_disk_synthesis(8, 30)     # even M
     with pytest.raises(ft.FTB200Error):
         ft.plan_tri_synthesis(8, 9)       # M != N
+
+
+# ---------------------------------------------------------------------------
+# Annulus and Dunkl-Xu grids (src/fftw.c:534-753)
+# ---------------------------------------------------------------------------
+RHO = float(np.sqrt(1 / 3))
+
+
+@pytest.mark.parametrize("N,M", [(1, 1), (2, 5), (3, 9), (8, 29), (17, 65), (64, 253), (33, 21), (256, 1021)])
+def test_annulus_grid_vs_oracle(env, N, M):
+    ft, torch = env
+    from oracle import grid as G
+    X = np.random.default_rng(N * 11 + M).uniform(-1, 1, (N, M))
+    plans = {"annulus_synthesis": ft.plan_annulus_synthesis(N, RHO, M), "annulus_analysis": ft.plan_annulus_analysis(N, RHO, M)}
+    try:
+        assert plans["annulus_synthesis"].rho == RHO
+        for op in plans:
+            for tr in "NT":
+                for plan in plans:
+                    got = run_family_dev(ft, torch, ft.execute_annulus_grid_dev, plans[plan], op == "annulus_analysis", tr, X)
+                    want = G.execute_annulus(op, tr, plan, X, RHO)
+                    assert rel2(got, want) <= 1e-14, (N, M, op, tr, plan, rel2(got, want))
+    finally:
+        for P in plans.values():
+            P.close()
+
+
+@pytest.mark.parametrize("N", [1, 2, 3, 8, 17, 64, 255, 512])
+def test_rectdisk_grid_vs_oracle(env, N):
+    ft, torch = env
+    from oracle import grid as G
+    X = np.random.default_rng(N + 5).uniform(-1, 1, (N, N))
+    plans = {"rectdisk_synthesis": ft.plan_rectdisk_synthesis(N), "rectdisk_analysis": ft.plan_rectdisk_analysis(N)}
+    try:
+        for op in plans:
+            for tr in "NT":
+                for plan in plans:
+                    got = run_family_dev(ft, torch, ft.execute_rectdisk_grid_dev, plans[plan], op == "rectdisk_analysis", tr, X)
+                    want = G.execute_rectdisk(op, tr, plan, X)
+                    assert rel2(got, want) <= 1e-14, (N, op, tr, plan, rel2(got, want))
+    finally:
+        for P in plans.values():
+            P.close()
+
+
+def test_annulus_and_rectdisk_reference_round_trips_on_gpu(env):
+    """test/test_fftw.c:288-320 and 350-380 on this library at their N = 64: 8 sqrt(N) eps, 4N eps."""
+    ft, torch = env
+    N = 64
+    st = torch.cuda.current_stream().cuda_stream
+    cases = (("disk", ft.plan_ann2cxf(N, 0.0, 0.0, 0.0, RHO), ft.plan_annulus_synthesis(N, RHO), ft.plan_annulus_analysis(N, RHO),
+              ft.execute_annulus_grid_dev),
+             ("rect", ft.plan_rectdisk2cheb(N, 0.0), ft.plan_rectdisk_synthesis(N), ft.plan_rectdisk_analysis(N),
+              ft.execute_rectdisk_grid_dev))
+    for kind, plan, PS, PA, grid_dev in cases:
+        A = ft.rand_layout(kind, N, 9)
+        M = A.shape[1]
+        t = torch.from_numpy(A.ravel(order="F").copy()).cuda()
+        p = t.data_ptr()
+        ft.execute_dev(plan, True, "N", p, N, M, st)
+        grid_dev(PS, False, "N", p, N, M, st)
+        grid_dev(PA, True, "N", p, N, M, st)
+        ft.execute_dev(plan, False, "N", p, N, M, st)
+        ft.execute_dev(plan, True, "T", p, N, M, st)
+        grid_dev(PA, False, "T", p, N, M, st)
+        grid_dev(PS, True, "T", p, N, M, st)
+        ft.execute_dev(plan, False, "T", p, N, M, st)
+        torch.cuda.synchronize()
+        B = t.cpu().numpy().reshape((N, M), order="F")
+        assert rel2(B, A) <= 8 * np.sqrt(N) * EPS, kind
+        assert np.abs(B - A).max() / np.abs(A).max() <= 4 * N * EPS, kind
+        for Q in (plan, PS, PA):
+            Q.close()
+
+
+def test_annulus_rectdisk_host_entry_points_and_errors(env):
+    ft, torch = env
+    N = 20
+    for fn_plan, host, dev, M in ((lambda n, m: ft.plan_annulus_synthesis(n, RHO, m), ft.execute_annulus_synthesis, ft.execute_annulus_grid_dev, 77),
+                                  (lambda n, m: ft.plan_annulus_analysis(n, RHO, m), ft.execute_annulus_analysis, ft.execute_annulus_grid_dev, 77),
+                                  (ft.plan_rectdisk_synthesis, ft.execute_rectdisk_synthesis, ft.execute_rectdisk_grid_dev, N),
+                                  (ft.plan_rectdisk_analysis, ft.execute_rectdisk_analysis, ft.execute_rectdisk_grid_dev, N)):
+        X = np.random.default_rng(M + 1).uniform(-1, 1, (N, M))
+        P = fn_plan(N, M)
+        analysis = "analysis" in host.__name__
+        for tr in "NT":
+            H = np.asfortranarray(X.copy())
+            host(tr, P, H)
+            assert np.array_equal(H, run_family_dev(ft, torch, dev, P, analysis, tr, X)), (host.__name__, tr)
+        P.close()
+    with pytest.raises(ft.FTB200Error):
+        ft.plan_annulus_synthesis(8, RHO, 30)    # even M
+    with pytest.raises(ft.FTB200Error):
+        ft.plan_rectdisk_synthesis(8, 9)         # M != N
