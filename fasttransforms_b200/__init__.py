@@ -49,6 +49,7 @@ __all__ = [
     "plan_annulus_synthesis", "plan_annulus_analysis", "execute_annulus_synthesis", "execute_annulus_analysis",
     "execute_annulus_grid_dev", "plan_rectdisk_synthesis", "plan_rectdisk_analysis", "execute_rectdisk_synthesis",
     "execute_rectdisk_analysis", "execute_rectdisk_grid_dev",
+    "plan_tet_synthesis", "plan_tet_analysis", "execute_tet_synthesis", "execute_tet_analysis", "execute_tet_grid_dev",
     "SPH", "TRI", "DISK",
 ]
 
@@ -112,6 +113,10 @@ def _load() -> C.CDLL:
         "ft_destroy_annulus_fftw_plan": (None, [vp]), "ft_get_rho_annulus_fftw_plan": (d, [vp]),
         "ft_plan_rectdisk_synthesis": (vp, [i, i, C.c_uint]), "ft_plan_rectdisk_analysis": (vp, [i, i, C.c_uint]),
         "ft_destroy_rectdisk_fftw_plan": (None, [vp]),
+        "ft_plan_tet_synthesis": (vp, [i, i, i, C.c_uint]), "ft_plan_tet_analysis": (vp, [i, i, i, C.c_uint]),
+        "ft_destroy_tetrahedron_fftw_plan": (None, [vp]),
+        "ft_execute_tet_synthesis": (None, [ch, vp, dp, i, i, i]), "ft_execute_tet_analysis": (None, [ch, vp, dp, i, i, i]),
+        "ft_b200_execute_tet_grid_dev": (i, [vp, i, ch, vp, i, i, i, vp]),
         "ft_b200_execute_annulus_grid_dev": (i, [vp, i, ch, vp, i, i, vp]),
         "ft_b200_execute_rectdisk_grid_dev": (i, [vp, i, ch, vp, i, i, vp]),
         "ft_execute_tet2cheb": (None, [ch, vp, dp, i, i, i]), "ft_execute_cheb2tet": (None, [ch, vp, dp, i, i, i]),
@@ -304,6 +309,37 @@ class AnnulusGridPlan(_FamilyGridPlan):
 
 class RectdiskGridPlan(_FamilyGridPlan):
     _destroy = "ft_destroy_rectdisk_fftw_plan"
+
+
+class TetGridPlan(_FamilyGridPlan):
+    _destroy = "ft_destroy_tetrahedron_fftw_plan"
+
+
+def plan_tet_synthesis(n: int) -> TetGridPlan:
+    ptr = lib.ft_plan_tet_synthesis(n, n, n, 0)
+    if not ptr:
+        _check()
+        raise FTB200Error(-1, "plan creation failed")
+    return TetGridPlan(ptr, "tet_synthesis", n, n)
+
+
+def plan_tet_analysis(n: int) -> TetGridPlan:
+    ptr = lib.ft_plan_tet_analysis(n, n, n, 0)
+    if not ptr:
+        _check()
+        raise FTB200Error(-1, "plan creation failed")
+    return TetGridPlan(ptr, "tet_analysis", n, n)
+
+
+def execute_tet_synthesis(trans, P, A): _exec_tet("ft_execute_tet_synthesis", trans, P, A)
+def execute_tet_analysis(trans, P, A): _exec_tet("ft_execute_tet_analysis", trans, P, A)
+
+
+def execute_tet_grid_dev(P: TetGridPlan, analysis: bool, trans: str, ptr: int, N: int, L: int, M: int, stream: int = 0) -> None:
+    """The tetrahedron grid's synthesis (analysis = False) or analysis sequence with P's kind on a device tensor."""
+    st = lib.ft_b200_execute_tet_grid_dev(P.ptr, 1 if analysis else 0, trans.encode(), C.c_void_p(ptr), N, L, M, C.c_void_p(stream))
+    if st != 0:
+        _check()
 
 
 def plan_annulus_synthesis(n: int, rho: float, m: int = None) -> AnnulusGridPlan:

@@ -38,10 +38,11 @@ namespace {
 // FFTW r2r kinds used by the plans (the values of fftw3.h's enum)
 enum { K_REDFT01 = 4, K_REDFT10 = 5, K_REDFT11 = 6, K_RODFT01 = 8, K_RODFT10 = 9 };
 enum Op { SPH_SYN = 0, SPH_ANA = 1, SPHV_SYN = 2, SPHV_ANA = 3, DISK_SYN = 4, DISK_ANA = 5, TRI_SYN = 6, TRI_ANA = 7,
-          ANN_SYN = 8, ANN_ANA = 9, RECT_SYN = 10, RECT_ANA = 11 };
+          ANN_SYN = 8, ANN_ANA = 9, RECT_SYN = 10, RECT_ANA = 11, TET_SYN = 12, TET_ANA = 13 };
 // plan families: the sphere's (sph, sphv), the disk's, the triangle's, the annulus's, the
-// rectangularised disk's
-enum Family { F_SPHERE = 0, F_DISK = 1, F_TRI = 2, F_ANN = 3, F_RECT = 4 };
+// rectangularised disk's, the tetrahedron's (an n x n x n tensor held as the n x n^2 matrix of its
+// columns)
+enum Family { F_SPHERE = 0, F_DISK = 1, F_TRI = 2, F_ANN = 3, F_RECT = 4, F_TET = 5 };
 
 constexpr int kGridMagic = 0x46544753;   // "FTGS"
 
@@ -224,6 +225,30 @@ __global__ void col0_scale(double * X, int N, int M, double f0, double s, double
     }
 }
 
+// tetrahedron: out = in with axes 0 and 1 (swap01) or 0 and 2 swapped, an n x n x n tensor
+__global__ void permute3(const double * __restrict__ in, double * __restrict__ out, int n, bool swap01) {
+    const long long total = (long long) n * n * n;
+    for (long long e = blockIdx.x * (long long) blockDim.x + threadIdx.x; e < total; e += (long long) gridDim.x * blockDim.x) {
+        const long long i = e % n, l = (e / n) % n, m = e / ((long long) n * n);
+        const long long o = swap01 ? l + n * i + (long long) n * n * m : m + n * l + (long long) n * n * i;
+        out[o] = in[e];
+    }
+}
+
+// tetrahedron scalings (src/fftw.c:351-402): entry (i, l, m) times ef when m == 0, when i == 0, when
+// l == 0 (in the reference's order), then times s or divided by d (d > 0)
+__global__ void tet_scale(double * X, int n, double ef, double s, double d) {
+    const long long total = (long long) n * n * n;
+    for (long long e = blockIdx.x * (long long) blockDim.x + threadIdx.x; e < total; e += (long long) gridDim.x * blockDim.x) {
+        const long long i = e % n, l = (e / n) % n, m = e / ((long long) n * n);
+        double v = X[e];
+        if (m == 0) v *= ef;
+        if (i == 0) v *= ef;
+        if (l == 0) v *= ef;
+        X[e] = d > 0.0 ? v / d : v * s;
+    }
+}
+
 // triangle scalings (src/fftw.c:292-330), entry (i, j) of the N x M matrix: times ef when
 // j == 0, times ef when i == 0, then times s (mul) or divided by d (d > 0)
 __global__ void tri_scale(double * X, int N, int M, double ef, double s, double d) {
@@ -291,8 +316,9 @@ unsigned blocks(long long n) { return (unsigned) ((n + 255) / 256); }
 SphereGridPlan * make_plan(int N, int M, int k0, int k1, int family = F_SPHERE, int krows = 0, double rho = 0.0) {
     clear_error();
     const bool square = family == F_TRI || family == F_RECT;   // row transforms through a square transpose
+    const bool nophi = square || family == F_TET;
     if (N < 1 || M < 1) { set_error(FT_B200_EINVAL, "N and M must be positive"); return nullptr; }
-    if (!square && M % 2 == 0) {
+    if (!nophi && M % 2 == 0) {
         set_error(FT_B200_EINVAL, "M must be odd (the half spectrum holds columns 2j - 1, 2j)");
         return nullptr;
     }
@@ -310,8 +336,8 @@ SphereGridPlan * make_plan(int N, int M, int k0, int k1, int family = F_SPHERE, 
     const size_t nm = (size_t) N * M;
     bool good = ok(cudaMalloc(&P->d_work, sizeof(double) * nm), "cudaMalloc(grid work)") &&
                 ok(cudaMalloc(&P->d_cwork, sizeof(double2) * (size_t) (N / 2 + 1) * M), "cudaMalloc(grid work)") &&
-                (square || ok(cudaMalloc(&P->d_Y, sizeof(double2) * (size_t) N * (M / 2 + 1)), "cudaMalloc(grid spectrum)")) &&
-                (!square || ok(cudaMalloc(&P->d_work2, sizeof(double) * nm), "cudaMalloc(grid work)")) &&
+                (nophi || ok(cudaMalloc(&P->d_Y, sizeof(double2) * (size_t) N * (M / 2 + 1)), "cudaMalloc(grid spectrum)")) &&
+                (!nophi || ok(cudaMalloc(&P->d_work2, sizeof(double) * nm), "cudaMalloc(grid work)")) &&
                 ok(cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     if (good && family == F_DISK) {
         P->nq = (M + 2) / 4 + (M + 1) / 4;
@@ -342,7 +368,7 @@ SphereGridPlan * make_plan(int N, int M, int k0, int k1, int family = F_SPHERE, 
         good = ok(cudaMalloc(&P->d_w, sizeof(double) * N), "cudaMalloc(weights)") &&
                ok(cudaMemcpy(P->d_w, w.data(), sizeof(double) * N, cudaMemcpyHostToDevice), "cudaMemcpy(weights)");
     }
-    if (good && !square) {
+    if (good && !nophi) {
         // phi: along rows, element stride N, rows one apart
         int m[1] = {M}, hm[1] = {M / 2 + 1};
         good = fok(cufftPlanMany(&P->p_c2r, 1, m, hm, N, 1, m, N, 1, CUFFT_Z2D, N), "cufftPlanMany");
@@ -420,6 +446,31 @@ bool theta_rows(SphereGridPlan * P, double * X, cudaStream_t st) {
     double * a[1] = {X}, * b[1] = {P->d_work2};
     return ok(launch_transpose_square(a, b, 1, P->N, st), "transpose") && theta(P, P->d_work2, st, true) &&
            ok(launch_transpose_square(b, a, 1, P->N, st), "transpose");
+}
+
+// tetrahedron: the plan's kind along all three axes (axis 0 as the columns of the n x n^2 matrix,
+// the other two after swapping them with axis 0)
+bool theta_tet(SphereGridPlan * P, double * X, cudaStream_t st) {
+    const int n = P->N;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    auto perm = [&](const double * a, double * b, bool swap01) {
+        permute3<<<sms * 4, 256, 0, st>>>(a, b, n, swap01);
+        count_launch();
+        return ok(cudaGetLastError(), "permute3");
+    };
+    return theta(P, X, st) && perm(X, P->d_work2, true) && theta(P, P->d_work2, st) && perm(P->d_work2, X, true) &&
+           perm(X, P->d_work2, false) && theta(P, P->d_work2, st) && perm(P->d_work2, X, false);
+}
+
+bool tet_scaling(SphereGridPlan * P, double * X, double ef, double s, double d, cudaStream_t st) {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    tet_scale<<<sms * 4, 256, 0, st>>>(X, P->N, ef, s, d);
+    count_launch();
+    return ok(cudaGetLastError(), "tet_scale");
 }
 
 bool row_factor(SphereGridPlan * P, double * X, int row, int start, int step, double f, cudaStream_t st) {
@@ -517,6 +568,17 @@ bool run(SphereGridPlan * P, int op, char T, double * X, cudaStream_t st) {
         return row_factor(P, X, N - 1, 1, 2, 2.0, st) && theta(P, X, st) && theta_rows(P, X, st) &&
                col0_scaling(P, X, 1.0, 1.0, nm, false, st);
     }
+    if (op == TET_SYN || op == TET_ANA) {     // src/fftw.c:351-402 (n x n x n)
+        const int n = N;
+        if (n <= 1) return true;
+        const double nlm = (double) (n * n * n);
+        if (op == TET_SYN) {
+            if (T == 'N') return tet_scaling(P, X, 2.0, 0.125, 0.0, st) && theta_tet(P, X, st);
+            return theta_tet(P, X, st) && tet_scaling(P, X, 1.0, 0.125, 0.0, st);
+        }
+        if (T == 'N') return theta_tet(P, X, st) && tet_scaling(P, X, 0.5, 1.0, nlm, st);
+        return tet_scaling(P, X, 1.0, 1.0, nlm, st) && theta_tet(P, X, st);
+    }
     if (op == TRI_SYN || op == TRI_ANA) {     // src/fftw.c:292-330
         if (N <= 1 || M <= 1) return true;
         const double nm = (double) (N * M);
@@ -544,7 +606,8 @@ int family_of(int op) {
     if (op <= SPHV_ANA) return F_SPHERE;
     if (op <= DISK_ANA) return F_DISK;
     if (op <= TRI_ANA) return F_TRI;
-    return op <= ANN_ANA ? F_ANN : F_RECT;
+    if (op <= ANN_ANA) return F_ANN;
+    return op <= RECT_ANA ? F_RECT : F_TET;
 }
 
 int check_call(SphereGridPlan * G, char T, const double * X, int N, int M, int family = F_SPHERE) {
@@ -687,6 +750,56 @@ void ft_execute_rectdisk_synthesis(const char TRANS, const ft_rectdisk_fftw_plan
 }
 void ft_execute_rectdisk_analysis(const char TRANS, const ft_rectdisk_fftw_plan * P, double * X, const int N, const int M) {
     execute_host(RECT_ANA, TRANS, P, X, N, M);
+}
+
+// the tetrahedron's grids: N = L = M = n, the tensor as the n x n^2 matrix of its columns
+static ft_tetrahedron_fftw_plan * tet_grid_plan(int N, int L, int M, int kind) {
+    clear_error();
+    if (N < 1 || L != N || M != N) {
+        set_error(FT_B200_EINVAL, "tetrahedral grids need N = L = M (the reference's 3-D plan reads the tensor in reverse)");
+        return nullptr;
+    }
+    return reinterpret_cast<ft_tetrahedron_fftw_plan *>(make_plan(N, N * N, kind, kind, F_TET));
+}
+ft_tetrahedron_fftw_plan * ft_plan_tet_synthesis(const int N, const int L, const int M, const unsigned) {
+    return tet_grid_plan(N, L, M, K_REDFT01);
+}
+ft_tetrahedron_fftw_plan * ft_plan_tet_analysis(const int N, const int L, const int M, const unsigned) {
+    return tet_grid_plan(N, L, M, K_REDFT10);
+}
+void ft_destroy_tetrahedron_fftw_plan(ft_tetrahedron_fftw_plan * P) {
+    SphereGridPlan * G = as_grid(reinterpret_cast<ft_sphere_fftw_plan *>(P));
+    if (G && G->family == F_TET) ft_destroy_sphere_fftw_plan(reinterpret_cast<ft_sphere_fftw_plan *>(P));
+}
+static int tet_dims(const void * P, int N, int L, int M, int * cols) {
+    const SphereGridPlan * G = as_grid(static_cast<const ft_sphere_fftw_plan *>(P));
+    if (!G || G->family != F_TET || L != N || M != N || N != G->N) {
+        set_error(FT_B200_EINVAL, "not a tetrahedral grid plan of this size");
+        return FT_B200_EINVAL;
+    }
+    *cols = L * M;
+    return FT_B200_OK;
+}
+void ft_execute_tet_synthesis(const char TRANS, const ft_tetrahedron_fftw_plan * P, double * X, const int N, const int L, const int M) {
+    clear_error();
+    int cols = 0;
+    if (tet_dims(P, N, L, M, &cols) == FT_B200_OK) execute_host(TET_SYN, TRANS, P, X, N, cols);
+}
+void ft_execute_tet_analysis(const char TRANS, const ft_tetrahedron_fftw_plan * P, double * X, const int N, const int L, const int M) {
+    clear_error();
+    int cols = 0;
+    if (tet_dims(P, N, L, M, &cols) == FT_B200_OK) execute_host(TET_ANA, TRANS, P, X, N, cols);
+}
+int ft_b200_execute_tet_grid_dev(const ft_tetrahedron_fftw_plan * P, int analysis, char TRANS, double * dX, int N, int L, int M,
+                                 void * stream) {
+    clear_error();
+    int cols = 0;
+    if (tet_dims(P, N, L, M, &cols) != FT_B200_OK) return FT_B200_EINVAL;
+    SphereGridPlan * G = as_grid(reinterpret_cast<const ft_sphere_fftw_plan *>(P));
+    const int c = check_call(G, TRANS, dX, N, cols, F_TET);
+    if (c != FT_B200_OK) return c;
+    std::lock_guard<std::mutex> lk(G->mu);
+    return run(G, analysis ? TET_ANA : TET_SYN, TRANS, dX, static_cast<cudaStream_t>(stream)) ? FT_B200_OK : ft_b200_last_status();
 }
 
 int ft_b200_execute_annulus_grid_dev(const ft_annulus_fftw_plan * P, int analysis, char TRANS, double * dX, int N, int M, void * stream) {

@@ -197,6 +197,18 @@ double ft_get_rho_annulus_fftw_plan(ft_annulus_fftw_plan * P);
 void ft_execute_annulus_synthesis(const char TRANS, const ft_annulus_fftw_plan * P, double * X, const int N, const int M);
 void ft_execute_annulus_analysis(const char TRANS, const ft_annulus_fftw_plan * P, double * X, const int N, const int M);
 
+/* Tetrahedral grids (src/fftw.c:332-402): N = L = M (the reference's 3-D plan reads the
+ * column-major tensor in reverse order, which agrees only for a cube). */
+typedef struct ft_tetrahedron_fftw_plan_s ft_tetrahedron_fftw_plan;
+/* replace ft_plan_tet_synthesis / ft_plan_tet_analysis, src/fftw.c:348-349 */
+ft_tetrahedron_fftw_plan * ft_plan_tet_synthesis(const int N, const int L, const int M, const unsigned flags);
+ft_tetrahedron_fftw_plan * ft_plan_tet_analysis(const int N, const int L, const int M, const unsigned flags);
+/* replaces ft_destroy_tetrahedron_fftw_plan, src/fftw.c:335-338 */
+void ft_destroy_tetrahedron_fftw_plan(ft_tetrahedron_fftw_plan * P);
+/* replace ft_execute_tet_synthesis / ft_execute_tet_analysis, src/fftw.c:351-402 */
+void ft_execute_tet_synthesis(const char TRANS, const ft_tetrahedron_fftw_plan * P, double * X, const int N, const int L, const int M);
+void ft_execute_tet_analysis(const char TRANS, const ft_tetrahedron_fftw_plan * P, double * X, const int N, const int L, const int M);
+
 /* Dunkl-Xu (rectangularised disk) grids (src/fftw.c:653-753): M must equal N here (the rows go
  * through a square transpose; the reference's tests use M = N). */
 typedef struct ft_rectdisk_fftw_plan_s ft_rectdisk_fftw_plan;
@@ -297,6 +309,7 @@ int ft_b200_execute_disk_grid_dev(const ft_disk_fftw_plan * P, int analysis, cha
 int ft_b200_execute_tri_grid_dev(const ft_triangle_fftw_plan * P, int analysis, char TRANS, double * dX, int N, int M, void * stream);
 int ft_b200_execute_annulus_grid_dev(const ft_annulus_fftw_plan * P, int analysis, char TRANS, double * dX, int N, int M, void * stream);
 int ft_b200_execute_rectdisk_grid_dev(const ft_rectdisk_fftw_plan * P, int analysis, char TRANS, double * dX, int N, int M, void * stream);
+int ft_b200_execute_tet_grid_dev(const ft_tetrahedron_fftw_plan * P, int analysis, char TRANS, double * dX, int N, int L, int M, void * stream);
 
 /* The sph vector-field transforms on device memory (forward = 1: sphv2fourier). */
 int ft_b200_execute_sphv_dev(const ft_harmonic_plan * P, int forward, char TRANS, double * dA, int N, int M, void * stream);

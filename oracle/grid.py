@@ -1,7 +1,7 @@
 """Oracle (test infrastructure, not the product): a CPU restatement of the
 sphere, disk and triangle grid synthesis and analysis of the reference
-(src/fftw.c:63-330, 404-753: ft_plan_sph_with_kind, ft_execute_sph_synthesis /
-_analysis and the sphv variants, ft_execute_disk_*, ft_execute_tri_*, ft_execute_annulus_*
+(src/fftw.c:63-753: ft_plan_sph_with_kind, ft_execute_sph_synthesis / _analysis and the
+sphv variants, ft_execute_disk_*, ft_execute_tri_*, ft_execute_tet_*, ft_execute_annulus_*
 and ft_execute_rectdisk_*) in numpy / scipy.
 
 FFTW, which the reference calls for these transforms, is not available here, so
@@ -317,3 +317,39 @@ def execute_rectdisk(op, trans, plan, X):
     X = _rect_x(X, kinds)
     X = _rect_y(X, kinds[2])
     return X / (N * M)
+
+
+# tetrahedron plan kinds (all three dimensions): src/fftw.c:348-349
+TET_PLANS = {"tet_synthesis": REDFT01, "tet_analysis": REDFT10}
+
+
+def _r2r_3d(X, kind):
+    Y = r2r(X, kind)                                   # axis 0
+    Y = np.moveaxis(r2r(np.moveaxis(Y, 1, 0), kind), 0, 1)
+    return np.moveaxis(r2r(np.moveaxis(Y, 2, 0), kind), 0, 2)
+
+
+def execute_tet(op, trans, plan, X):
+    """ft_execute_tet_{synthesis,analysis}(trans, P, X), src/fftw.c:351-402: the plan's kind along
+    all three dimensions of the N x L x M tensor (N = L = M; nothing happens unless all exceed 1),
+    with the factors of the faces m = 0, i = 0, l = 0 and the 1/8 or 1/(N L M) scalings."""
+    X = np.array(X, dtype=float, copy=True)
+    N, L, M = X.shape
+    if N <= 1 or L <= 1 or M <= 1:
+        return X
+    kind = TET_PLANS[plan]
+    if op == "tet_synthesis":
+        if trans == "N":
+            X[:, :, 0] *= 2.0
+            X[0, :, :] *= 2.0
+            X[:, 0, :] *= 2.0
+            X *= 0.125
+            return _r2r_3d(X, kind)
+        return _r2r_3d(X, kind) * 0.125
+    if trans == "N":
+        X = _r2r_3d(X, kind)
+        X[:, :, 0] *= 0.5
+        X[0, :, :] *= 0.5
+        X[:, 0, :] *= 0.5
+        return X / (N * L * M)
+    return _r2r_3d(X / (N * L * M), kind)

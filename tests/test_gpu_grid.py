@@ -348,3 +348,77 @@ def test_annulus_rectdisk_host_entry_points_and_errors(env):
         ft.plan_annulus_synthesis(8, RHO, 30)    # even M
     with pytest.raises(ft.FTB200Error):
         ft.plan_rectdisk_synthesis(8, 9)         # M != N
+
+
+# ---------------------------------------------------------------------------
+# Tetrahedral grids (src/fftw.c:332-402)
+# ---------------------------------------------------------------------------
+def run_tet_dev(ft, torch, P, analysis, tr, X):
+    t = torch.from_numpy(np.asfortranarray(X).ravel(order="F").copy()).cuda()
+    n = X.shape[0]
+    ft.execute_tet_grid_dev(P, analysis, tr, t.data_ptr(), n, n, n, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    return t.cpu().numpy().reshape(X.shape, order="F")
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 8, 17, 64])
+def test_tet_grid_vs_oracle(env, n):
+    ft, torch = env
+    from oracle import grid as G
+    X = np.random.default_rng(n + 9).uniform(-1, 1, (n, n, n))
+    plans = {"tet_synthesis": ft.plan_tet_synthesis(n), "tet_analysis": ft.plan_tet_analysis(n)}
+    try:
+        for op in plans:
+            for tr in "NT":
+                for plan in plans:
+                    got = run_tet_dev(ft, torch, plans[plan], op == "tet_analysis", tr, X)
+                    want = G.execute_tet(op, tr, plan, X)
+                    assert rel2(got, want) <= 1e-14, (n, op, tr, plan, rel2(got, want))
+    finally:
+        for P in plans.values():
+            P.close()
+
+
+@pytest.mark.parametrize("n", [16, 32])
+def test_tet_reference_round_trip_on_gpu(env, n):
+    """test/test_fftw.c:412-447 on this library, every stage on the GPU, with that test's bounds."""
+    ft, torch = env
+    st = torch.cuda.current_stream().cuda_stream
+    A = ft.tetrand(n, 5)
+    P = ft.plan_tet2cheb(n, 0.0, 0.0, 0.0, 0.0)
+    TS, TA = ft.plan_tet_synthesis(n), ft.plan_tet_analysis(n)
+    t = torch.from_numpy(A.ravel(order="F").copy()).cuda()
+    p = t.data_ptr()
+    einf = lambda B: np.abs(B - A).max() / np.abs(A).max()
+    ft.execute_tet_dev(P, True, "N", p, n, n, n, st)
+    ft.execute_tet_grid_dev(TS, False, "N", p, n, n, n, st)
+    ft.execute_tet_grid_dev(TA, True, "N", p, n, n, n, st)
+    ft.execute_tet_dev(P, False, "N", p, n, n, n, st)
+    torch.cuda.synchronize()
+    B = t.cpu().numpy().reshape(A.shape, order="F")
+    assert rel2(B, A) <= 8 * n * EPS and einf(B) <= 4 * n * n * EPS
+    ft.execute_tet_dev(P, True, "T", p, n, n, n, st)
+    ft.execute_tet_grid_dev(TA, False, "T", p, n, n, n, st)
+    ft.execute_tet_grid_dev(TS, True, "T", p, n, n, n, st)
+    ft.execute_tet_dev(P, False, "T", p, n, n, n, st)
+    torch.cuda.synchronize()
+    B = t.cpu().numpy().reshape(A.shape, order="F")
+    assert rel2(B, A) <= 64 * n * n * EPS and einf(B) <= 32 * n ** 3 * EPS
+    for Q in (P, TS, TA):
+        Q.close()
+
+
+def test_tet_grid_host_entry_points_and_errors(env):
+    ft, torch = env
+    n = 12
+    X = np.random.default_rng(3).uniform(-1, 1, (n, n, n))
+    for fn_plan, host, analysis in ((ft.plan_tet_synthesis, ft.execute_tet_synthesis, False),
+                                    (ft.plan_tet_analysis, ft.execute_tet_analysis, True)):
+        P = fn_plan(n)
+        for tr in "NT":
+            H = np.asfortranarray(X.copy())
+            host(tr, P, H)
+            assert np.array_equal(H, run_tet_dev(ft, torch, P, analysis, tr, X)), (host.__name__, tr)
+        P.close()
+    assert not ft.lib.ft_plan_tet_synthesis(8, 8, 9, 0)      # L = M = N required
+    assert ft.lib.ft_b200_last_status() == 1                  # FT_B200_EINVAL

@@ -207,3 +207,38 @@ def test_rectdisk_grid_is_a_chebyshev_product():
         got = G.execute_rectdisk("rectdisk_synthesis", "N", "rectdisk_synthesis", A)
         want = np.outer(np.cos(i * th), np.cos(j * th))
         assert np.abs(got - want).max() < 1e-14, (i, j)
+
+
+@pytest.mark.parametrize("N", [16, 32])
+def test_tet_reference_round_trip(ref, N):
+    """test/test_fftw.c:412-447 (L = M = N, parameters 0, plans crossed in 'T'): after the 'N' pair
+    8 (NLM)^(1/3) eps, 4 (NLM)^(2/3) eps; after the 'T' pair 64 (NLM)^(2/3) eps, 32 NLM eps."""
+    from fasttransforms_b200.utilities import tetrand
+    A = tetrand(N, 5)
+    P = ref.tet_plan(N, 0.0, 0.0, 0.0, 0.0)
+    X = A.copy(order="F")
+    ref.tet_execute(P, True, "N", X)
+    X = G.execute_tet("tet_synthesis", "N", "tet_synthesis", X)
+    X = np.asfortranarray(G.execute_tet("tet_analysis", "N", "tet_analysis", X))
+    ref.tet_execute(P, False, "N", X)
+    einf = lambda B: np.abs(B - A).max() / np.abs(A).max()
+    assert np.linalg.norm(X - A) / np.linalg.norm(A) <= 8 * N * EPS and einf(X) <= 4 * N * N * EPS
+    ref.tet_execute(P, True, "T", X)
+    X = G.execute_tet("tet_synthesis", "T", "tet_analysis", X)
+    X = np.asfortranarray(G.execute_tet("tet_analysis", "T", "tet_synthesis", X))
+    ref.tet_execute(P, False, "T", X)
+    ref.destroy(P)
+    assert np.linalg.norm(X - A) / np.linalg.norm(A) <= 64 * N * N * EPS and einf(X) <= 32 * N ** 3 * EPS
+
+
+def test_tet_grid_is_a_chebyshev_product():
+    """Known answer: the tet synthesis of a unit coefficient (i, l, m) (all > 0) is
+    T_i(x) T_l(y) T_m(z) on the Chebyshev points."""
+    N = 7
+    th = (np.arange(N) + 0.5) * np.pi / N
+    for i, l, m in [(1, 2, 3), (4, 1, 2)]:
+        A = np.zeros((N, N, N))
+        A[i, l, m] = 1.0
+        got = G.execute_tet("tet_synthesis", "N", "tet_synthesis", A)
+        want = np.einsum("a,b,c->abc", np.cos(i * th), np.cos(l * th), np.cos(m * th))
+        assert np.abs(got - want).max() < 1e-14, (i, l, m)
