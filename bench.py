@@ -716,10 +716,19 @@ def family_grid(kind, n):
     if kind == "disk":
         P, PS, PA, grid = ft.plan_disk2cxf(n, 0.0, 0.0), ft.plan_disk_synthesis(n), ft.plan_disk_analysis(n), ft.execute_disk_grid_dev
         coeffs = 2 * n * n - n
+    elif kind == "annulus":
+        rho = float(np.sqrt(1 / 3))
+        P, PS, PA = ft.plan_ann2cxf(n, 0.0, 0.0, 0.0, rho), ft.plan_annulus_synthesis(n, rho), ft.plan_annulus_analysis(n, rho)
+        grid = ft.execute_annulus_grid_dev
+        coeffs = 2 * n * n - n
+    elif kind == "rectdisk":
+        P, PS, PA = ft.plan_rectdisk2cheb(n, 0.0), ft.plan_rectdisk_synthesis(n), ft.plan_rectdisk_analysis(n)
+        grid = ft.execute_rectdisk_grid_dev
+        coeffs = n * (n + 1) // 2
     else:
         P, PS, PA, grid = ft.plan_tri2cheb(n, 0.0, 0.0, 0.0), ft.plan_tri_synthesis(n), ft.plan_tri_analysis(n), ft.execute_tri_grid_dev
         coeffs = n * (n + 1) // 2
-    A = ft.rand_layout(kind, n, SEED)
+    A = ft.rand_layout({"annulus": "disk", "rectdisk": "rect"}.get(kind, kind), n, SEED)
     M = A.shape[1]
     d = torch.from_numpy(A.ravel(order="F").copy()).cuda()
     p = d.data_ptr()
@@ -736,6 +745,33 @@ def family_grid(kind, n):
             "roundtrip_eps2": rt,
             "workload": f"{kind}: to the Chebyshev / Fourier series, synthesis on the grid, analysis, back ('N'), "
                         f"degree {n - 1}, 1 field {n} x {M} (plain FP64, cuFFT DFTs inside the grid stage)"}
+
+
+def family_tet_grid(n):
+    """tet2cheb + synthesis on the n^3 grid, analysis + cheb2tet ('N'), on the device."""
+    import numpy as np
+    import torch
+    import fasttransforms_b200 as ft
+    sp = torch.cuda.current_stream().cuda_stream
+    P, TS, TA = ft.plan_tet2cheb(n, 0.0, 0.0, 0.0, 0.0), ft.plan_tet_synthesis(n), ft.plan_tet_analysis(n)
+    A = ft.tetrand(n, SEED)
+    d = torch.from_numpy(A.ravel(order="F").copy()).cuda()
+    p = d.data_ptr()
+    f = lambda: (ft.execute_tet_dev(P, True, "N", p, n, n, n, sp), ft.execute_tet_grid_dev(TS, False, "N", p, n, n, n, sp))
+    b = lambda: (ft.execute_tet_grid_dev(TA, True, "N", p, n, n, n, sp), ft.execute_tet_dev(P, False, "N", p, n, n, n, sp))
+    f(); b()
+    torch.cuda.synchronize()
+    rt = float(np.linalg.norm(d.cpu().numpy() - A.ravel(order="F")) / np.linalg.norm(A))
+    ms = _family_timing(torch, f, b)
+    ms_grid = _family_timing(torch, lambda: ft.execute_tet_grid_dev(TS, False, "N", p, n, n, n, sp),
+                             lambda: ft.execute_tet_grid_dev(TA, True, "N", p, n, n, n, sp))
+    for q in (P, TS, TA):
+        q.close()
+    coeffs = n * (n + 1) * (n + 2) // 6
+    return {"coeffs_per_s": coeffs / (ms * 1e-3), "ms_per_step": ms, "grid_synthesis_plus_analysis_ms": ms_grid,
+            "roundtrip_eps2": rt,
+            "workload": f"tet: tet2cheb, synthesis on the {n}^3 grid, analysis, cheb2tet ('N'), degree {n - 1}, 1 field "
+                        f"(plain FP64, cuFFT DFTs inside the grid stage)"}
 
 
 def extra_workloads(args, torch, ft):
@@ -825,7 +861,10 @@ def extra_workloads(args, torch, ft):
     # 'N' on the device (plain FP64); each in its own guard so that one failure leaves the rest
     for name, fn in (("rectdisk_n4096", lambda: family_rectdisk(4096)), ("ann_n2048", lambda: family_ann(2048)),
                      ("tet_n256", lambda: family_tet(256)), ("disk_full_grid_n2048", lambda: family_grid("disk", 2048)),
-                     ("tri_full_grid_n2048", lambda: family_grid("tri", 2048))):
+                     ("tri_full_grid_n2048", lambda: family_grid("tri", 2048)),
+                     ("annulus_full_grid_n2048", lambda: family_grid("annulus", 2048)),
+                     ("rectdisk_full_grid_n2048", lambda: family_grid("rectdisk", 2048)),
+                     ("tet_full_grid_n128", lambda: family_tet_grid(128))):
         try:
             out[name] = fn()
         except Exception as exc:
