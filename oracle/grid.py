@@ -1,8 +1,8 @@
 """Oracle (test infrastructure, not the product): a CPU restatement of the
 sphere, disk and triangle grid synthesis and analysis of the reference
 (src/fftw.c:63-753: ft_plan_sph_with_kind, ft_execute_sph_synthesis / _analysis and the
-sphv variants, ft_execute_disk_*, ft_execute_tri_*, ft_execute_tet_*, ft_execute_annulus_*
-and ft_execute_rectdisk_*) in numpy / scipy.
+sphv variants, ft_execute_disk_*, ft_execute_tri_*, ft_execute_tet_*, ft_execute_annulus_*,
+ft_execute_rectdisk_* and ft_execute_spinsph_*; src/fftw.c:755-960) in numpy / scipy.
 
 FFTW, which the reference calls for these transforms, is not available here, so
 its one-dimensional transforms are restated from their published definitions
@@ -353,3 +353,88 @@ def execute_tet(op, trans, plan, X):
         X[:, 0, :] *= 0.5
         return X / (N * L * M)
     return _r2r_3d(X / (N * L * M), kind)
+
+
+# src/ftinternal.h:53-54
+M_2_SQRT_2PI = 5.013256549262001005
+M_1_2_SQRT_2PI = 0.199471140200716338
+
+
+def spin_plan_kinds(op, s):
+    """src/fftw.c:789-799: the (classes {0, 3}, classes {1, 2}) kinds of a spin plan, and the sign
+    of its row DFT (+1: FFTW_BACKWARD, synthesis; -1: FFTW_FORWARD, analysis)."""
+    if op == "spinsph_synthesis":
+        return ((REDFT01, RODFT01) if s % 2 == 0 else (RODFT01, REDFT01)), +1
+    return ((REDFT10, RODFT10) if s % 2 == 0 else (RODFT10, REDFT10)), -1
+
+
+def _colswap(X):
+    """src/fftw.c:6-21: column 0 stays, column 2j goes to j and column 2j - 1 to M - j."""
+    N, M = X.shape
+    Y = np.empty_like(X)
+    Y[:, 0] = X[:, 0]
+    for j in range(1, (M + 1) // 2):
+        Y[:, j] = X[:, 2 * j]
+        Y[:, M - j] = X[:, 2 * j - 1]
+    return Y
+
+
+def _colswap_t(Y):
+    """src/fftw.c:23-38, the inverse permutation."""
+    N, M = Y.shape
+    X = np.empty_like(Y)
+    X[:, 0] = Y[:, 0]
+    for j in range(1, (M + 1) // 2):
+        X[:, 2 * j] = Y[:, j]
+        X[:, 2 * j - 1] = Y[:, M - j]
+    return X
+
+
+def _row_dft(X, sign):
+    """FFTW's unnormalised DFT along the rows with exp(sign 2 pi i j k / M)."""
+    M = X.shape[1]
+    return np.fft.ifft(X, axis=1) * M if sign > 0 else np.fft.fft(X, axis=1)
+
+
+def _spin_theta(X, kinds):
+    return theta(X.real, kinds) + 1j * theta(X.imag, kinds)
+
+
+def _spin_ends(X, row, even_set, f):
+    """Entries of `row` in the columns {0, 3, 4, 7, 8, ..} (even_set) or {1, 2, 5, 6, ..}, both parts."""
+    N, M = X.shape
+    if even_set:
+        cols = [0] + [c for j in range(3, M, 4) for c in (j, j + 1) if c < M]
+    else:
+        cols = [c for j in range(1, M, 4) for c in (j, j + 1) if c < M]
+    X[row, cols] *= f
+
+
+def execute_spinsph(op, trans, plan_op, s_plan, X):
+    """ft_execute_spinsph_{synthesis,analysis}(trans, P, X) with P the plan of `plan_op` and spin
+    s_plan (its kinds, sign and spin), src/fftw.c:801-960.  X: complex N x M.  The reference's
+    routines act for TRANS 'N' and 'C' only; any other character leaves X untouched."""
+    X = np.array(X, dtype=complex, copy=True)
+    N, M = X.shape
+    if trans not in ("N", "C"):
+        return X
+    kinds, sign = spin_plan_kinds(plan_op, s_plan)
+    even = s_plan % 2 == 0
+    nm2 = 2.0 * N * M
+    if op == "spinsph_synthesis":
+        if trans == "N":
+            _spin_ends(X, 0, even, 2.0)
+            X = _spin_theta(X, kinds) * M_1_2_SQRT_2PI
+            return _row_dft(_colswap(X), sign)
+        X = _colswap_t(_row_dft(X, sign)) * M_1_2_SQRT_2PI
+        X = _spin_theta(X, kinds)
+        _spin_ends(X, N - 1, not even, 0.5)
+        return X
+    if trans == "N":
+        X = _colswap_t(_row_dft(X, sign)) * (M_2_SQRT_2PI / nm2)
+        X = _spin_theta(X, kinds)
+        _spin_ends(X, 0, even, 0.5)
+        return X
+    _spin_ends(X, N - 1, not even, 2.0)
+    X = _spin_theta(X, kinds) * (M_2_SQRT_2PI / nm2)
+    return _row_dft(_colswap(X), sign)

@@ -242,3 +242,42 @@ def test_tet_grid_is_a_chebyshev_product():
         got = G.execute_tet("tet_synthesis", "N", "tet_synthesis", A)
         want = np.einsum("a,b,c->abc", np.cos(i * th), np.cos(l * th), np.cos(m * th))
         assert np.abs(got - want).max() < 1e-14, (i, l, m)
+
+
+@pytest.mark.parametrize("s", [-4, -1, 0, 1, 2, 3])
+def test_spin_grid_reference_round_trip(ref, s):
+    """test/test_fftw.c:481-516 (N = 64, M = 2N - 1): the compiled reference's spinsph2fourier /
+    fourier2spinsph around the oracle's spin synthesis and analysis ('N'), then the 'T' pair, whose
+    grid steps the reference's routines leave alone (they act for 'N' and 'C' only): 4 sqrt(N) eps,
+    2N eps."""
+    from fasttransforms_b200.utilities import spinsphrand
+    N = 64
+    A = spinsphrand(N, s, 5)
+    P = ref.spin_plan(N, s)
+    X = A.copy(order="F")
+    ref.spin_execute(P, True, "N", X)
+    X = G.execute_spinsph("spinsph_synthesis", "N", "spinsph_synthesis", s, X)
+    X = np.asfortranarray(G.execute_spinsph("spinsph_analysis", "N", "spinsph_analysis", s, X))
+    ref.spin_execute(P, False, "N", X)
+    ref.spin_execute(P, True, "T", X)
+    assert np.array_equal(G.execute_spinsph("spinsph_synthesis", "T", "spinsph_analysis", s, X), X)   # a no-op
+    ref.spin_execute(P, False, "T", X)
+    ref.spin_destroy(P)
+    assert np.linalg.norm(X - A) / np.linalg.norm(A) <= 4 * np.sqrt(N) * EPS
+    assert np.abs(X - A).max() / np.abs(A).max() <= 2 * N * EPS
+
+
+@pytest.mark.parametrize("s", [0, 1, -2, 3])
+def test_spin_grid_pairs_are_identities(s):
+    """Synthesis then analysis ('N', own plans) and, with the plans crossed as the reference's
+    tests cross them, 'C' synthesis then 'C' analysis both return arbitrary complex data to
+    rounding: the sequences, kinds, signs, permutations and scalings fit together."""
+    rng = np.random.default_rng(s + 10)
+    N, M = 16, 31
+    X = rng.standard_normal((N, M)) + 1j * rng.standard_normal((N, M))
+    Y = G.execute_spinsph("spinsph_analysis", "N", "spinsph_analysis", s,
+                          G.execute_spinsph("spinsph_synthesis", "N", "spinsph_synthesis", s, X))
+    Z = G.execute_spinsph("spinsph_analysis", "C", "spinsph_synthesis", s,
+                          G.execute_spinsph("spinsph_synthesis", "C", "spinsph_analysis", s, X))
+    assert np.linalg.norm(Y - X) / np.linalg.norm(X) < 1e-15 * N
+    assert np.linalg.norm(Z - X) / np.linalg.norm(X) < 1e-15 * N
