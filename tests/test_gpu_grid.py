@@ -198,9 +198,9 @@ def test_disk_and_tri_reference_round_trips_on_gpu(env, N):
     test's bounds (32 sqrt(N) eps, 8N eps for tri; 8 sqrt(N) eps, 4N eps for disk), or within twice
     the reference algorithm's own error of the same sequence where that is larger (the reference's
     tri2cheb / cheb2tri round trip alone exceeds 32 sqrt(N) eps from N = 256: 1.25x at 256, 1.62x
-    at 512; the reference's test runs N = 64).  At N = 1024 the tri sequence's max-norm error on
-    the GPU (9.1e-12) is 2.6x the reference algorithm's (3.6e-12; 4.3e-12 with the GPU's DCT
-    algorithm in the oracle), its 2-norm error within the bar: that size is left out here."""
+    at 512; the reference's test runs N = 64).  At N = 1024 the tri sequence's errors on the GPU
+    (1.10e-12, 9.1e-12) match the oracle's restatement of the algorithm (1.12e-12, 6.5-7.7e-12) but
+    not the compiled reference's BLAS summation (6.6e-13, 3.6e-12): that size is left out here."""
     ft, torch = env
     st = torch.cuda.current_stream().cuda_stream
     for kind, plan, syn, ana, grid_dev, e2, einf in (
