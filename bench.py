@@ -627,8 +627,21 @@ def profile_case(n: int, precision: str, fields: int) -> None:
                       "max_abs": max(float(t.abs().max()) for t in d)}))
 
 
-def _family_timing(torch, fwd, bwd, reps=5):
-    """Mean device time (ms) of fwd(); bwd() after one untimed pair, CUDA events on the stream."""
+_FP64_PEAK = []
+
+
+def _fp64_peak(torch) -> float:
+    if not _FP64_PEAK:
+        _FP64_PEAK.append(fp64_peak_tflops(torch))
+    return _FP64_PEAK[0]
+
+
+def _family_timing(torch, fwd, bwd, reps=5, breakdown=None):
+    """Mean device time (ms) of fwd(); bwd() after one untimed pair, CUDA events on the stream.
+    With a dict for breakdown: a second timed loop with the library's per-launch events on, whose
+    per-step milliseconds of the rotation sweeps, the triangular multiplies and the other kernels
+    go into it."""
+    import fasttransforms_b200 as ft
     st = torch.cuda.current_stream()
     fwd(); bwd()
     torch.cuda.synchronize()
@@ -638,7 +651,56 @@ def _family_timing(torch, fwd, bwd, reps=5):
         fwd(); bwd()
     e1.record(st)
     torch.cuda.synchronize()
+    if breakdown is not None:
+        ft.profile(True)
+        for _ in range(reps):
+            fwd(); bwd()
+        torch.cuda.synchronize()
+        for fam, key in ((0, "rotations"), (1, "trmm"), (2, "other")):
+            ms, nl = ft.profile_read(fam)
+            breakdown[key + "_ms"] = ms / reps
+            breakdown[key + "_launches"] = nl / reps
+        ft.profile(False)
     return e0.elapsed_time(e1) / reps
+
+
+def _rotation_roofline(torch, out, brk, rotations_per_step):
+    """The sweeps' FP64 rate (6 flops a rotation) from the profiled per-step time."""
+    if brk.get("rotations_ms", 0) > 0:
+        tf = 6.0 * rotations_per_step / (brk["rotations_ms"] * 1e-3) / 1e12
+        out["rotation_sweeps"] = {"ms_per_step": brk["rotations_ms"], "rotations_per_step": int(rotations_per_step),
+                                  "tflops": tf, "fp64_peak_tflops": _fp64_peak(torch), "frac": tf / _fp64_peak(torch),
+                                  "breakdown_ms_per_step": brk}
+
+
+def rotations_rect(n):
+    """Rotations of one rectdisk hi2lo: order m (column m, m = 2 .. n - 1), sweeps j = m - 2, .., m mod 2,
+    n - 2 - j rotations each (src/rotations/rotations_default.c:73-78)."""
+    import numpy as np
+    j = np.arange(0, max(n - 2, 0), dtype=np.int64)
+    c = np.maximum(0, (n - 1 - (j + 2)) // 2 + 1)
+    return int(np.sum(c * np.maximum(0, n - 2 - j)))
+
+
+def rotations_disk(n, M):
+    """Rotations of one disk hi2lo (both columns of each order m = 2 .. M/2; sweeps j = m - 2, .., m mod 2,
+    n - 1 - (j + 1) / 2 rotations each; src/rotations/rotations_default.c:59-64)."""
+    import numpy as np
+    j = np.arange(0, max(M // 2 - 1, 0), dtype=np.int64)
+    c = np.maximum(0, (M // 2 - (j + 2)) // 2 + 1)
+    return int(2 * np.sum(c * np.maximum(0, n - 1 - (j + 1) // 2)))
+
+
+def rotations_tet(n, slabs=True):
+    """Element rotations of one tetrahedral hi2lo with L = M = n: the triangle sweeps of order o on o + 1
+    columns (o < n), sum over j < o of n - 1 - j each; with slabs, also per slab m the sweeps j < m
+    across the slab, n - 1 - j column pairs of n elements each (src/drivers.c:510-528)."""
+    import numpy as np
+    o = np.arange(n, dtype=np.int64)
+    tri = np.sum((o + 1) * (o * (n - 1) - o * (o - 1) // 2))
+    m = np.arange(n, dtype=np.int64)
+    tet = np.sum((m * (n - 1) - m * (m - 1) // 2) * n) if slabs else 0
+    return int(tri + tet)
 
 
 def family_rectdisk(n):
@@ -655,12 +717,15 @@ def family_rectdisk(n):
     f(); b()
     torch.cuda.synchronize()
     rt = float(np.linalg.norm(d.cpu().numpy() - A.ravel(order="F")) / np.linalg.norm(A))
-    ms = _family_timing(torch, f, b)
+    brk = {}
+    ms = _family_timing(torch, f, b, breakdown=brk)
     P.close()
     coeffs = n * (n + 1) // 2
-    return {"coeffs_per_s": coeffs / (ms * 1e-3), "ms_per_step": ms, "roundtrip_eps2": rt,
-            "workload": f"rectdisk2cheb + cheb2rectdisk 'N', beta = 0, degree {n - 1}, 1 field {n} x {n} (plain FP64; "
-                        f"{coeffs} coefficients)"}
+    out = {"coeffs_per_s": coeffs / (ms * 1e-3), "ms_per_step": ms, "roundtrip_eps2": rt,
+           "workload": f"rectdisk2cheb + cheb2rectdisk 'N', beta = 0, degree {n - 1}, 1 field {n} x {n} (plain FP64; "
+                       f"{coeffs} coefficients)"}
+    _rotation_roofline(torch, out, brk, 2 * rotations_rect(n))
+    return out
 
 
 def family_ann(n):
@@ -678,12 +743,15 @@ def family_ann(n):
     f(); b()
     torch.cuda.synchronize()
     rt = float(np.linalg.norm(d.cpu().numpy() - A.ravel(order="F")) / np.linalg.norm(A))
-    ms = _family_timing(torch, f, b)
+    brk = {}
+    ms = _family_timing(torch, f, b, breakdown=brk)
     P.close()
     coeffs = 2 * n * n - n
-    return {"coeffs_per_s": coeffs / (ms * 1e-3), "ms_per_step": ms, "roundtrip_eps2": rt,
-            "workload": f"ann2cxf + cxf2ann 'N', alpha = beta = 0, rho = sqrt(1/3), degree {n - 1}, 1 field {n} x {M} "
-                        f"(plain FP64)"}
+    out = {"coeffs_per_s": coeffs / (ms * 1e-3), "ms_per_step": ms, "roundtrip_eps2": rt,
+           "workload": f"ann2cxf + cxf2ann 'N', alpha = beta = 0, rho = sqrt(1/3), degree {n - 1}, 1 field {n} x {M} "
+                       f"(plain FP64)"}
+    _rotation_roofline(torch, out, brk, 2 * rotations_disk(n, M))
+    return out
 
 
 def family_tet(n):
@@ -699,12 +767,17 @@ def family_tet(n):
     f(); b()
     torch.cuda.synchronize()
     rt = float(np.linalg.norm(d.cpu().numpy() - A.ravel(order="F")) / np.linalg.norm(A))
-    ms = _family_timing(torch, f, b)
+    brk = {}
+    ms = _family_timing(torch, f, b, breakdown=brk)
     P.close()
     coeffs = n * (n + 1) * (n + 2) // 6
-    return {"coeffs_per_s": coeffs / (ms * 1e-3), "ms_per_step": ms, "roundtrip_eps2": rt,
-            "workload": f"tet2cheb + cheb2tet 'N', parameters 0, degree {n - 1}, 1 field {n} x {n} x {n} (plain FP64; "
-                        f"{coeffs} coefficients)"}
+    out = {"coeffs_per_s": coeffs / (ms * 1e-3), "ms_per_step": ms, "roundtrip_eps2": rt,
+           "workload": f"tet2cheb + cheb2tet 'N', parameters 0, degree {n - 1}, 1 field {n} x {n} x {n} (plain FP64; "
+                       f"{coeffs} coefficients)",
+           "note": "rotation_sweeps: the triangle sweeps down the columns (the rotation kernel); the sweeps across "
+                   "the slabs are not in the profiled families"}
+    _rotation_roofline(torch, out, brk, 2 * rotations_tet(n, slabs=False))
+    return out
 
 
 def family_grid(kind, n):
