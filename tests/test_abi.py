@@ -75,3 +75,51 @@ def test_c_caller_compiles_links_and_runs(tmp_path, src):
         assert out == "ok" or float(out) < 1e-13, out
     else:
         assert r.stdout.strip() == "ENODEV"
+
+
+def _prototypes():
+    """name -> (return type, [parameter declarations]) for every function the header declares."""
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    text = "\n".join(line for line in text.splitlines() if not line.lstrip().startswith("#"))
+    text = re.sub(r"\s+", " ", text)
+    protos = {}
+    for m in re.finditer(r"(?:^|(?<=[;{}]))\s*([A-Za-z_][\w \*]*?)\b(ft_\w+)\s*\(([^()]*)\)\s*;", text):
+        ret, name, params = m.group(1).strip(), m.group(2), m.group(3).strip()
+        protos[name] = (ret, [] if params in ("", "void") else [q.strip() for q in params.split(",")])
+    return protos
+
+
+def _kind(decl, named=True):
+    """'int' / 'double' / 'char' / 'uint' / 'void' / 'ptr' of a return type or a parameter."""
+    if "*" in decl or "[" in decl:
+        return "ptr"
+    toks = [t for t in decl.split() if t != "const"]
+    if named and len(toks) > 1:
+        toks = toks[:-1]
+    for t, k in (("long", "ull"), ("int", "int"), ("double", "double"), ("char", "char"), ("unsigned", "uint"),
+                 ("void", "void")):
+        if t in toks:
+            return k
+    return "ptr"
+
+
+def test_python_bindings_match_the_header():
+    """Every function fasttransforms_b200 binds has the header's arity and scalar types."""
+    import ctypes
+    import fasttransforms_b200 as ft
+    kinds = {ctypes.c_int: "int", ctypes.c_double: "double", ctypes.c_char: "char", ctypes.c_uint: "uint",
+             ctypes.c_ulonglong: "ull"}
+    protos = _prototypes()
+    checked = 0
+    for name, (ret, params) in protos.items():
+        f = getattr(ft.lib, name, None)
+        if f is None or f.argtypes is None:
+            continue
+        got = [kinds.get(a, "ptr") for a in f.argtypes]
+        want = [_kind(q) for q in params]
+        assert got == want, (name, got, want)
+        r = f.restype
+        rk = "void" if r is None else kinds.get(r, "ptr")
+        assert rk == _kind(ret, named=False), (name, rk, ret)
+        checked += 1
+    assert checked > 60
