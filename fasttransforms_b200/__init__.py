@@ -39,6 +39,8 @@ __all__ = [
     "SpinHarmonicPlan", "SpinRotationPlan", "plan_spinsph2fourier", "plan_rotspinsphere",
     "execute_spinsph2fourier", "execute_fourier2spinsph", "execute_spinsph_hi2lo", "execute_spinsph_lo2hi",
     "execute_spin_dev", "spin_rotations_dev", "spinsphrand",
+    "SpinGridPlan", "plan_spinsph_synthesis", "plan_spinsph_analysis", "execute_spinsph_synthesis",
+    "execute_spinsph_analysis", "execute_spinsph_grid_dev",
     "plan_rectdisk2cheb", "execute_rectdisk2cheb", "execute_cheb2rectdisk", "plan_rotrectdisk",
     "execute_rectdisk_hi2lo", "execute_rectdisk_lo2hi", "rectdiskrand",
     "TetPlan", "plan_tet2cheb", "execute_tet2cheb", "execute_cheb2tet", "execute_tet_hi2lo", "execute_tet_lo2hi",
@@ -123,6 +125,10 @@ def _load() -> C.CDLL:
         "ft_execute_tet_hi2lo": (None, [vp, vp, dp, i, i]), "ft_execute_tet_lo2hi": (None, [vp, vp, dp, i, i]),
         "ft_b200_execute_tet_dev": (i, [vp, i, ch, vp, i, i, i, vp]),
         "ft_b200_tet_rotations_dev": (i, [vp, i, vp, i, i, vp]),
+        "ft_plan_spinsph_synthesis": (vp, [i, i, i, C.c_uint]), "ft_plan_spinsph_analysis": (vp, [i, i, i, C.c_uint]),
+        "ft_destroy_spinsphere_fftw_plan": (None, [vp]), "ft_get_spin_spinsphere_fftw_plan": (i, [vp]),
+        "ft_execute_spinsph_synthesis": (None, [ch, vp, dp, i, i]), "ft_execute_spinsph_analysis": (None, [ch, vp, dp, i, i]),
+        "ft_b200_execute_spinsph_grid_dev": (i, [vp, i, ch, vp, i, i, vp]),
     }
     for name in ("sph_synthesis", "sph_analysis", "sphv_synthesis", "sphv_analysis", "disk_synthesis", "disk_analysis",
                  "tri_synthesis", "tri_analysis", "annulus_synthesis", "annulus_analysis", "rectdisk_synthesis",
@@ -482,6 +488,45 @@ def _exec_spin_rot(fname, SRP, A, M=None):
 
 def execute_spinsph_hi2lo(SRP, A, M=None): _exec_spin_rot("ft_execute_spinsph_hi2lo", SRP, A, M)
 def execute_spinsph_lo2hi(SRP, A, M=None): _exec_spin_rot("ft_execute_spinsph_lo2hi", SRP, A, M)
+
+
+class SpinGridPlan(_FamilyGridPlan):
+    """Owns an ``ft_spinsphere_fftw_plan *`` (reference: src/fftw.c:743-960)."""
+
+    _destroy = "ft_destroy_spinsphere_fftw_plan"
+
+    @property
+    def s(self) -> int:
+        return lib.ft_get_spin_spinsphere_fftw_plan(self.ptr)
+
+
+def _spin_grid_plan(fname, n, s, m):
+    m = 2 * n - 1 if m is None else m
+    ptr = getattr(lib, fname)(n, m, s, 0)
+    if not ptr:
+        _check()
+        raise FTB200Error(-1, "plan creation failed")
+    return SpinGridPlan(ptr, fname[8:], n, m)
+
+
+def plan_spinsph_synthesis(n: int, s: int, m: int = None) -> SpinGridPlan:
+    return _spin_grid_plan("ft_plan_spinsph_synthesis", n, s, m)
+
+
+def plan_spinsph_analysis(n: int, s: int, m: int = None) -> SpinGridPlan:
+    return _spin_grid_plan("ft_plan_spinsph_analysis", n, s, m)
+
+
+def execute_spinsph_synthesis(trans, P, A, N=None, M=None): _exec_spin("ft_execute_spinsph_synthesis", trans, P, A, N, M)
+def execute_spinsph_analysis(trans, P, A, N=None, M=None): _exec_spin("ft_execute_spinsph_analysis", trans, P, A, N, M)
+
+
+def execute_spinsph_grid_dev(P: SpinGridPlan, analysis: bool, trans: str, ptr: int, N: int, M: int, stream: int = 0) -> None:
+    """The spin grid's synthesis (analysis = False) or analysis sequence with P's kinds on a device
+    matrix of N x M interleaved complex doubles, asynchronous."""
+    st = lib.ft_b200_execute_spinsph_grid_dev(P.ptr, 1 if analysis else 0, trans.encode(), C.c_void_p(ptr), N, M, C.c_void_p(stream))
+    if st != 0:
+        _check()
 
 
 def execute_spin_dev(P: SpinHarmonicPlan, forward: bool, trans: str, ptr: int, N: int, M: int, stream: int = 0) -> None:

@@ -23,6 +23,10 @@
 // DST-III(x)_k = (-1)^k DCT-III(x reversed)_k.  The DFTs are cuFFT's (library
 // FFTs, batched over all M columns at once); the reorderings, twiddles, scalings and
 // the half-spectrum packing are this file's kernels.
+//
+// The spin-weighted sphere's grid (a complex N x M matrix, src/fftw.c:755-960) runs the same
+// theta stage on the 2M real columns of its split parts, and a complex DFT along the rows around
+// the reference's column permutation (columns 2j and 2j - 1 to j and M - j).
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -38,11 +42,11 @@ namespace {
 // FFTW r2r kinds used by the plans (the values of fftw3.h's enum)
 enum { K_REDFT01 = 4, K_REDFT10 = 5, K_REDFT11 = 6, K_RODFT01 = 8, K_RODFT10 = 9 };
 enum Op { SPH_SYN = 0, SPH_ANA = 1, SPHV_SYN = 2, SPHV_ANA = 3, DISK_SYN = 4, DISK_ANA = 5, TRI_SYN = 6, TRI_ANA = 7,
-          ANN_SYN = 8, ANN_ANA = 9, RECT_SYN = 10, RECT_ANA = 11, TET_SYN = 12, TET_ANA = 13 };
+          ANN_SYN = 8, ANN_ANA = 9, RECT_SYN = 10, RECT_ANA = 11, TET_SYN = 12, TET_ANA = 13, SPIN_SYN = 14, SPIN_ANA = 15 };
 // plan families: the sphere's (sph, sphv), the disk's, the triangle's, the annulus's, the
 // rectangularised disk's, the tetrahedron's (an n x n x n tensor held as the n x n^2 matrix of its
-// columns)
-enum Family { F_SPHERE = 0, F_DISK = 1, F_TRI = 2, F_ANN = 3, F_RECT = 4, F_TET = 5 };
+// columns), the spin-weighted sphere's (a complex N x M matrix)
+enum Family { F_SPHERE = 0, F_DISK = 1, F_TRI = 2, F_ANN = 3, F_RECT = 4, F_TET = 5, F_SPIN = 6 };
 
 constexpr int kGridMagic = 0x46544753;   // "FTGS"
 
@@ -51,6 +55,8 @@ constexpr double C_1_4_SQRT_PI = 0.141047395886939072;   // 1 / (4 sqrt(pi))
 constexpr double C_1_2_SQRT_PI = 0.282094791773878143;   // 1 / (2 sqrt(pi))
 constexpr double C_4_SQRT_PI = 7.089815403622064109;     // 4 sqrt(pi)
 constexpr double C_2_SQRT_PI = 3.544907701811032055;     // 2 sqrt(pi)
+constexpr double C_1_2_SQRT_2PI = 0.199471140200716338;  // 1 / (2 sqrt(2 pi))
+constexpr double C_2_SQRT_2PI = 5.013256549262001005;    // 2 sqrt(2 pi)
 constexpr double C_SQRT2 = 1.41421356237309504880;
 constexpr double C_SQRT1_2 = 0.70710678118654752440;
 
@@ -67,16 +73,19 @@ struct SphereGridPlan {
                                  // rect: even and odd columns)
     int kind_rows = 0;           // rect: the kind along the rows
     double rho = 0.0;            // annulus: the radius ratio
+    int spin = 0;                // spin: the plan's spin S (its parity picks the kinds and the end entries)
     double * d_w = nullptr;      // annulus: the N radial weights
     int device = 0;
     cufftHandle t_r2c = 0;       // length N, batch M (cosine type II)
     cufftHandle t_c2r = 0;       // length N, batch M (cosine type III)
     cufftHandle p_r2c = 0;       // length M along rows, batch N
     cufftHandle p_c2r = 0;
-    bool have_t_r2c = false, have_t_c2r = false, have_p_r2c = false, have_p_c2r = false;
+    cufftHandle p_z2z = 0;       // spin: complex DFT of length M along rows, batch N
+    bool have_t_r2c = false, have_t_c2r = false, have_p_r2c = false, have_p_c2r = false, have_p_z2z = false;
+    // (spin: the theta stage runs on 2M real columns, so the work buffers below hold 2M columns)
     double * d_work = nullptr;   // N x M real
     double2 * d_cwork = nullptr; // (N/2 + 1) x M complex
-    double2 * d_Y = nullptr;     // N x (M/2 + 1) complex, element (i, j) at i + j N
+    double2 * d_Y = nullptr;     // N x (M/2 + 1) complex, element (i, j) at i + j N (spin: N x M)
     double * d_stage = nullptr;  // N x M, host-pointer calls
     // disk: the DCT-IV of the columns of classes 1 and 2 (nq of them) as a zero-padded complex
     // DFT of length 2N
@@ -84,7 +93,7 @@ struct SphereGridPlan {
     bool have_t4 = false;
     int nq = 0;
     double2 * d_u = nullptr;     // 2N x nq
-    double * d_work2 = nullptr;  // tri: N x N, the transposed matrix
+    double * d_work2 = nullptr;  // tri: N x N, the transposed matrix; spin: N x 2M, the parts split
     cudaStream_t stream = nullptr;
     std::mutex mu;
 };
@@ -95,8 +104,10 @@ namespace {
 // theta stage kernels: one thread per (entry, column); column j uses the kind of
 // its class, cls(j) = j mod 4 in {0, 3} -> kind[0], {1, 2} -> kind[1]
 // ---------------------------------------------------------------------------
-// k1dst bit 1 set: the classes are the even and odd columns instead (the rectangularised disk's)
+// k1dst bit 1 set: the classes are the even and odd columns instead (the rectangularised disk's);
+// bit 2 set: column j is part j & 1 of complex column j >> 1, whose class decides (the spin grid's)
 __device__ __forceinline__ bool col_dst(int j, int k0dst, int k1dst) {
+    if (k1dst & 4) { j >>= 1; k1dst &= 1; }
     if (k1dst & 2) return (j & 1) ? (k1dst & 1) : k0dst;
     const int r = j & 3;
     return (r == 0 || r == 3) ? k0dst : k1dst;
@@ -300,6 +311,52 @@ __global__ void scale_ends(double * X, int N, int M, bool last, int c0, int star
     if (j0 + 1 < M) X[(long long) (j0 + 1) * N + row] *= f;
 }
 
+// ---------------------------------------------------------------------------
+// spin grids (src/fftw.c:6-38, 801-960): the complex N x M matrix X (interleaved parts) and W, the
+// real N x 2M matrix whose column 2c + p is part p of column c, on which the theta stage runs.
+// Column c of the destination comes from column src(c) of the source:
+//   perm 0: src(c) = c;
+//   perm 1 (colswap_t): src(0) = 0, src(2j) = j, src(2j - 1) = M - j;
+//   perm 2 (colswap):   src(0) = 0, src(k) = 2k for k <= (M - 1) / 2, 2 (M - k) - 1 above (M odd);
+// then every entry times s, and the entries of `row` in the column classes {0, 3} (set 0) or
+// {1, 2} (set 1) times f as well (row -1: none).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int spin_src(int c, int M, int perm) {
+    if (perm == 0 || c == 0) return c;
+    if (perm == 1) return (c & 1) ? M - (c + 1) / 2 : c / 2;
+    return c <= (M - 1) / 2 ? 2 * c : 2 * (M - c) - 1;
+}
+__device__ __forceinline__ bool spin_end(int i, int c, int row, int set) {
+    const int r = c & 3;
+    return i == row && ((r == 1 || r == 2) ? 1 : 0) == set;
+}
+
+// X (2 N M doubles) -> W (N x 2M)
+__global__ void spin_split(const double * __restrict__ X, double * __restrict__ W, int N, int M, int perm, double s,
+                           int row, int set, double f) {
+    const long long idx = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long) N * M) return;
+    const int c = (int) (idx / N), i = (int) (idx % N);
+    const long long from = 2 * ((long long) spin_src(c, M, perm) * N + i);
+    double re = X[from] * s, im = X[from + 1] * s;
+    if (spin_end(i, c, row, set)) { re *= f; im *= f; }
+    W[(long long) (2 * c) * N + i] = re;
+    W[(long long) (2 * c + 1) * N + i] = im;
+}
+
+// W (N x 2M) -> X (2 N M doubles)
+__global__ void spin_merge(const double * __restrict__ W, double * __restrict__ X, int N, int M, int perm, double s,
+                           int row, int set, double f) {
+    const long long idx = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long) N * M) return;
+    const int c = (int) (idx / N), i = (int) (idx % N);
+    const int q = spin_src(c, M, perm);
+    double re = W[(long long) (2 * q) * N + i] * s, im = W[(long long) (2 * q + 1) * N + i] * s;
+    if (spin_end(i, c, row, set)) { re *= f; im *= f; }
+    X[2 * idx] = re;
+    X[2 * idx + 1] = im;
+}
+
 bool ok(cudaError_t e, const char * what) {
     if (e == cudaSuccess) return true;
     set_error(e == cudaErrorMemoryAllocation ? FT_B200_ENOMEM : FT_B200_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
@@ -319,7 +376,8 @@ SphereGridPlan * make_plan(int N, int M, int k0, int k1, int family = F_SPHERE, 
     const bool nophi = square || family == F_TET;
     if (N < 1 || M < 1) { set_error(FT_B200_EINVAL, "N and M must be positive"); return nullptr; }
     if (!nophi && M % 2 == 0) {
-        set_error(FT_B200_EINVAL, "M must be odd (the half spectrum holds columns 2j - 1, 2j)");
+        set_error(FT_B200_EINVAL, family == F_SPIN ? "M must be odd (the column permutation pairs columns 2j - 1, 2j)"
+                                                   : "M must be odd (the half spectrum holds columns 2j - 1, 2j)");
         return nullptr;
     }
     if (square && M != N) {
@@ -333,11 +391,13 @@ SphereGridPlan * make_plan(int N, int M, int k0, int k1, int family = F_SPHERE, 
     P->family = family;
     P->N = N; P->M = M; P->kind[0] = k0; P->kind[1] = k1; P->kind_rows = krows; P->rho = rho;
     cudaGetDevice(&P->device);
-    const size_t nm = (size_t) N * M;
+    const bool spin = family == F_SPIN;
+    const int TM = spin ? 2 * M : M;   // real columns of the theta stage
+    const size_t nm = (size_t) N * TM;
     bool good = ok(cudaMalloc(&P->d_work, sizeof(double) * nm), "cudaMalloc(grid work)") &&
-                ok(cudaMalloc(&P->d_cwork, sizeof(double2) * (size_t) (N / 2 + 1) * M), "cudaMalloc(grid work)") &&
-                (nophi || ok(cudaMalloc(&P->d_Y, sizeof(double2) * (size_t) N * (M / 2 + 1)), "cudaMalloc(grid spectrum)")) &&
-                (!nophi || ok(cudaMalloc(&P->d_work2, sizeof(double) * nm), "cudaMalloc(grid work)")) &&
+                ok(cudaMalloc(&P->d_cwork, sizeof(double2) * (size_t) (N / 2 + 1) * TM), "cudaMalloc(grid work)") &&
+                (nophi || ok(cudaMalloc(&P->d_Y, sizeof(double2) * (size_t) N * (spin ? M : M / 2 + 1)), "cudaMalloc(grid spectrum)")) &&
+                (!(nophi || spin) || ok(cudaMalloc(&P->d_work2, sizeof(double) * nm), "cudaMalloc(grid work)")) &&
                 ok(cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     if (good && family == F_DISK) {
         P->nq = (M + 2) / 4 + (M + 1) / 4;
@@ -351,10 +411,10 @@ SphereGridPlan * make_plan(int N, int M, int k0, int k1, int family = F_SPHERE, 
     if (good) {
         int n[1] = {N};
         if (is_type3(k0)) {
-            good = fok(cufftPlanMany(&P->t_c2r, 1, n, nullptr, 1, N / 2 + 1, nullptr, 1, N, CUFFT_Z2D, M), "cufftPlanMany");
+            good = fok(cufftPlanMany(&P->t_c2r, 1, n, nullptr, 1, N / 2 + 1, nullptr, 1, N, CUFFT_Z2D, TM), "cufftPlanMany");
             P->have_t_c2r = good;
         } else {
-            good = fok(cufftPlanMany(&P->t_r2c, 1, n, nullptr, 1, N, nullptr, 1, N / 2 + 1, CUFFT_D2Z, M), "cufftPlanMany");
+            good = fok(cufftPlanMany(&P->t_r2c, 1, n, nullptr, 1, N, nullptr, 1, N / 2 + 1, CUFFT_D2Z, TM), "cufftPlanMany");
             P->have_t_r2c = good;
         }
     }
@@ -368,7 +428,12 @@ SphereGridPlan * make_plan(int N, int M, int k0, int k1, int family = F_SPHERE, 
         good = ok(cudaMalloc(&P->d_w, sizeof(double) * N), "cudaMalloc(weights)") &&
                ok(cudaMemcpy(P->d_w, w.data(), sizeof(double) * N, cudaMemcpyHostToDevice), "cudaMemcpy(weights)");
     }
-    if (good && !nophi) {
+    if (good && spin) {
+        // phi: complex, along rows, element stride N, rows one apart
+        int m[1] = {M};
+        good = fok(cufftPlanMany(&P->p_z2z, 1, m, m, N, 1, m, N, 1, CUFFT_Z2Z, N), "cufftPlanMany");
+        P->have_p_z2z = good;
+    } else if (good && !nophi) {
         // phi: along rows, element stride N, rows one apart
         int m[1] = {M}, hm[1] = {M / 2 + 1};
         good = fok(cufftPlanMany(&P->p_c2r, 1, m, hm, N, 1, m, N, 1, CUFFT_Z2D, N), "cufftPlanMany");
@@ -388,8 +453,9 @@ SphereGridPlan * make_plan(int N, int M, int k0, int k1, int family = F_SPHERE, 
 // theta transforms of all M columns in place (the plan's kinds by column class; disk: kind[0]
 // on every column here, the DCT-IV of classes 1 and 2 in theta_disk)
 bool theta(SphereGridPlan * P, double * X, cudaStream_t st, bool rows = false) {
-    const int N = P->N, M = P->M;
+    const int N = P->N, M = P->family == F_SPIN ? 2 * P->M : P->M;
     int d0 = is_dst(P->kind[0]), d1 = P->family == F_SPHERE ? is_dst(P->kind[1]) : d0;
+    if (P->family == F_SPIN) d1 = is_dst(P->kind[1]) | 4;   // W's columns by their complex column's class
     if (P->family == F_RECT) {
         if (rows) { d0 = is_dst(P->kind_rows); d1 = d0; }   // every column of the transposed matrix
         else d1 = is_dst(P->kind[1]) | 2;                    // even and odd columns
@@ -533,9 +599,50 @@ bool ends(SphereGridPlan * P, double * X, bool last, int c0, int start, double f
 // The reference's execute sequences (src/fftw.c:131-277).  End-entry factors: first
 // entries of {0, 3, 4, 7, 8, ..} (sph) or {1, 2, 5, 6, ..} (sphv); last entries of
 // {1, 2, 5, 6, ..} (sph) or {0, 3, 4, 7, 8, ..} (sphv).
+// spin: X <-> the split matrix in d_work2 (see spin_split / spin_merge)
+bool split(SphereGridPlan * P, const double * X, int perm, double s, int row, int set, double f, cudaStream_t st) {
+    spin_split<<<blocks((long long) P->N * P->M), 256, 0, st>>>(X, P->d_work2, P->N, P->M, perm, s, row, set, f);
+    count_launch();
+    return ok(cudaGetLastError(), "spin_split");
+}
+bool merge(SphereGridPlan * P, double * X, int perm, double s, int row, int set, double f, cudaStream_t st) {
+    spin_merge<<<blocks((long long) P->N * P->M), 256, 0, st>>>(P->d_work2, X, P->N, P->M, perm, s, row, set, f);
+    count_launch();
+    return ok(cudaGetLastError(), "spin_merge");
+}
+// spin: the unnormalised complex DFT along the rows, from `in` to `out` (FFTW_BACKWARD, exp(+i..),
+// for the synthesis plans; FFTW_FORWARD for the analysis plans)
+bool phi_z2z(SphereGridPlan * P, const double * in, double * out, cudaStream_t st) {
+    const int dir = is_type3(P->kind[0]) ? CUFFT_INVERSE : CUFFT_FORWARD;
+    return fok(cufftSetStream(P->p_z2z, st), "cufftSetStream") &&
+           fok(cufftExecZ2Z(P->p_z2z, reinterpret_cast<cufftDoubleComplex *>(const_cast<double *>(in)),
+                            reinterpret_cast<cufftDoubleComplex *>(out), dir), "cufftExecZ2Z");
+}
+
+// src/fftw.c:801-960.  The end entries: row 0 of the classes {0, 3} for even S ({1, 2} for odd S)
+// before the synthesis / after the analysis; row N - 1 of the other classes in the 'C' forms.
+bool run_spin(SphereGridPlan * P, int op, char T, double * X, cudaStream_t st) {
+    if (T != 'N' && T != 'C') return true;
+    const int N = P->N, M = P->M;
+    const int first = P->spin % 2 == 0 ? 0 : 1, last = 1 - first;
+    double * Y = reinterpret_cast<double *>(P->d_Y);
+    const double sa = C_2_SQRT_2PI / (2.0 * N * M);
+    if (op == SPIN_SYN) {
+        if (T == 'N') return split(P, X, 0, 1.0, 0, first, 2.0, st) && theta(P, P->d_work2, st) &&
+                             merge(P, Y, 2, C_1_2_SQRT_2PI, -1, 0, 1.0, st) && phi_z2z(P, Y, X, st);
+        return phi_z2z(P, X, Y, st) && split(P, Y, 1, C_1_2_SQRT_2PI, -1, 0, 1.0, st) && theta(P, P->d_work2, st) &&
+               merge(P, X, 0, 1.0, N - 1, last, 0.5, st);
+    }
+    if (T == 'N') return phi_z2z(P, X, Y, st) && split(P, Y, 1, sa, -1, 0, 1.0, st) && theta(P, P->d_work2, st) &&
+                         merge(P, X, 0, 1.0, 0, first, 0.5, st);
+    return split(P, X, 0, 1.0, N - 1, last, 2.0, st) && theta(P, P->d_work2, st) && merge(P, Y, 2, sa, -1, 0, 1.0, st) &&
+           phi_z2z(P, Y, X, st);
+}
+
 bool run(SphereGridPlan * P, int op, char T, double * X, cudaStream_t st) {
     const int N = P->N, M = P->M;
     const double nm2 = 2.0 * N * M;
+    if (op == SPIN_SYN || op == SPIN_ANA) return run_spin(P, op, T, X, st);
     if (op == DISK_SYN || op == DISK_ANA) {   // src/fftw.c:460-532: first entries of {0, 3, 4, 7, 8, ..} only
         auto first = [&](double f) { return ends(P, X, false, 0, 3, f, st); };
         if (op == DISK_SYN) {
@@ -607,12 +714,15 @@ int family_of(int op) {
     if (op <= DISK_ANA) return F_DISK;
     if (op <= TRI_ANA) return F_TRI;
     if (op <= ANN_ANA) return F_ANN;
-    return op <= RECT_ANA ? F_RECT : F_TET;
+    if (op <= RECT_ANA) return F_RECT;
+    return op <= TET_ANA ? F_TET : F_SPIN;
 }
 
 int check_call(SphereGridPlan * G, char T, const double * X, int N, int M, int family = F_SPHERE) {
     if (!G || G->family != family) { set_error(FT_B200_EINVAL, "not a grid plan of this family of this library"); return FT_B200_EINVAL; }
-    if (T != 'N' && T != 'T') { set_error(FT_B200_EINVAL, "TRANS must be 'N' or 'T'"); return FT_B200_EINVAL; }
+    // spin: 'N' and 'C' run, any other TRANS leaves X untouched, as the reference's (its own
+    // round-trip test, test/test_fftw.c:504-505, passes 'T')
+    if (family != F_SPIN && T != 'N' && T != 'T') { set_error(FT_B200_EINVAL, "TRANS must be 'N' or 'T'"); return FT_B200_EINVAL; }
     if (!X) { set_error(FT_B200_EINVAL, "NULL matrix"); return FT_B200_EINVAL; }
     if (N != G->N || M != G->M) { set_error(FT_B200_EINVAL, "N, M do not match the plan"); return FT_B200_EINVAL; }
     return FT_B200_OK;
@@ -622,9 +732,10 @@ void execute_host(int op, char T, const void * P, double * X, int N, int M) {
     clear_error();
     SphereGridPlan * G = as_grid(static_cast<const ft_sphere_fftw_plan *>(P));
     if (check_call(G, T, X, N, M, family_of(op)) != FT_B200_OK) return;
+    if (G->family == F_SPIN && T != 'N' && T != 'C') return;
     std::lock_guard<std::mutex> lk(G->mu);
     cudaSetDevice(G->device);
-    const size_t bytes = sizeof(double) * (size_t) N * M;
+    const size_t bytes = sizeof(double) * (size_t) N * M * (G->family == F_SPIN ? 2 : 1);   // spin: complex
     if (!G->d_stage && !ok(cudaMalloc(&G->d_stage, bytes), "cudaMalloc(grid stage)")) return;
     if (!ok(cudaMemcpyAsync(G->d_stage, X, bytes, cudaMemcpyHostToDevice, G->stream), "cudaMemcpyAsync(H2D)")) return;
     if (!run(G, op, T, G->d_stage, G->stream)) return;
@@ -660,6 +771,7 @@ void ft_destroy_sphere_fftw_plan(ft_sphere_fftw_plan * Pp) {
     if (P->have_p_r2c) cufftDestroy(P->p_r2c);
     if (P->have_p_c2r) cufftDestroy(P->p_c2r);
     if (P->have_t4) cufftDestroy(P->t4);
+    if (P->have_p_z2z) cufftDestroy(P->p_z2z);
     cudaFree(P->d_work); cudaFree(P->d_cwork); cudaFree(P->d_Y); cudaFree(P->d_stage); cudaFree(P->d_u); cudaFree(P->d_work2);
     cudaFree(P->d_w);
     if (P->stream) cudaStreamDestroy(P->stream);
@@ -836,6 +948,49 @@ int ft_b200_execute_tri_grid_dev(const ft_triangle_fftw_plan * P, int analysis, 
     if (c != FT_B200_OK) return c;
     std::lock_guard<std::mutex> lk(G->mu);
     return run(G, analysis ? TRI_ANA : TRI_SYN, TRANS, dX, static_cast<cudaStream_t>(stream)) ? FT_B200_OK : ft_b200_last_status();
+}
+
+// the spin-weighted sphere's grids (src/fftw.c:743-960): kinds by the parity of S
+static ft_spinsphere_fftw_plan * spin_grid_plan(int N, int M, int S, bool analysis) {
+    const bool even = S % 2 == 0;
+    const int k0 = analysis ? (even ? K_REDFT10 : K_RODFT10) : (even ? K_REDFT01 : K_RODFT01);
+    const int k1 = analysis ? (even ? K_RODFT10 : K_REDFT10) : (even ? K_RODFT01 : K_REDFT01);
+    SphereGridPlan * P = make_plan(N, M, k0, k1, F_SPIN);
+    if (P) P->spin = S;
+    return reinterpret_cast<ft_spinsphere_fftw_plan *>(P);
+}
+ft_spinsphere_fftw_plan * ft_plan_spinsph_synthesis(const int N, const int M, const int S, const unsigned) {
+    return spin_grid_plan(N, M, S, false);
+}
+ft_spinsphere_fftw_plan * ft_plan_spinsph_analysis(const int N, const int M, const int S, const unsigned) {
+    return spin_grid_plan(N, M, S, true);
+}
+void ft_destroy_spinsphere_fftw_plan(ft_spinsphere_fftw_plan * P) {
+    SphereGridPlan * G = as_grid(reinterpret_cast<ft_sphere_fftw_plan *>(P));
+    if (G && G->family == F_SPIN) ft_destroy_sphere_fftw_plan(reinterpret_cast<ft_sphere_fftw_plan *>(P));
+}
+int ft_get_spin_spinsphere_fftw_plan(const ft_spinsphere_fftw_plan * P) {
+    const SphereGridPlan * G = as_grid(reinterpret_cast<const ft_sphere_fftw_plan *>(P));
+    return (G && G->family == F_SPIN) ? G->spin : 0;
+}
+void ft_execute_spinsph_synthesis(const char TRANS, const ft_spinsphere_fftw_plan * P, ft_complex * X, const int N, const int M) {
+    execute_host(SPIN_SYN, TRANS, P, reinterpret_cast<double *>(X), N, M);
+}
+void ft_execute_spinsph_analysis(const char TRANS, const ft_spinsphere_fftw_plan * P, ft_complex * X, const int N, const int M) {
+    execute_host(SPIN_ANA, TRANS, P, reinterpret_cast<double *>(X), N, M);
+}
+int ft_b200_execute_spinsph_grid_dev(const ft_spinsphere_fftw_plan * P, int analysis, char TRANS, double * dX, int N, int M,
+                                     void * stream) {
+    clear_error();
+    SphereGridPlan * G = as_grid(reinterpret_cast<const ft_sphere_fftw_plan *>(P));
+    const int c = check_call(G, TRANS, dX, N, M, F_SPIN);
+    if (c != FT_B200_OK) return c;
+    if (reinterpret_cast<uintptr_t>(dX) % 16 != 0) {   // cuFFT's complex operands
+        set_error(FT_B200_EINVAL, "dX must be 16-byte aligned (complex doubles)");
+        return FT_B200_EINVAL;
+    }
+    std::lock_guard<std::mutex> lk(G->mu);
+    return run(G, analysis ? SPIN_ANA : SPIN_SYN, TRANS, dX, static_cast<cudaStream_t>(stream)) ? FT_B200_OK : ft_b200_last_status();
 }
 
 int ft_b200_execute_sph_grid_dev(const ft_sphere_fftw_plan * P, int op, char TRANS, double * dX, int N, int M, void * stream) {

@@ -255,6 +255,21 @@ void ft_destroy_spin_harmonic_plan(ft_spin_harmonic_plan * P);
 void ft_execute_spinsph2fourier(const char TRANS, const ft_spin_harmonic_plan * P, ft_complex * A, const int N, const int M);
 void ft_execute_fourier2spinsph(const char TRANS, const ft_spin_harmonic_plan * P, ft_complex * A, const int N, const int M);
 
+/* Synthesis and analysis on the spin-weighted sphere's grid (N x M complex, M odd).  Opaque
+ * (the reference's struct holds FFTW plans).  TRANS 'N' or 'C'; any other character leaves X
+ * untouched, as in the reference. */
+typedef struct ft_spinsphere_fftw_plan_s ft_spinsphere_fftw_plan;
+/* replace ft_plan_spinsph_synthesis / ft_plan_spinsph_analysis, src/fftw.c:789-799 */
+ft_spinsphere_fftw_plan * ft_plan_spinsph_synthesis(const int N, const int M, const int S, const unsigned flags);
+ft_spinsphere_fftw_plan * ft_plan_spinsph_analysis(const int N, const int M, const int S, const unsigned flags);
+/* replaces ft_destroy_spinsphere_fftw_plan, src/fftw.c:743-751 */
+void ft_destroy_spinsphere_fftw_plan(ft_spinsphere_fftw_plan * P);
+/* replaces ft_get_spin_spinsphere_fftw_plan, src/fftw.c:753 */
+int ft_get_spin_spinsphere_fftw_plan(const ft_spinsphere_fftw_plan * P);
+/* replace ft_execute_spinsph_synthesis / ft_execute_spinsph_analysis, src/fftw.c:801-960 */
+void ft_execute_spinsph_synthesis(const char TRANS, const ft_spinsphere_fftw_plan * P, ft_complex * X, const int N, const int M);
+void ft_execute_spinsph_analysis(const char TRANS, const ft_spinsphere_fftw_plan * P, ft_complex * X, const int N, const int M);
+
 /* Rotation level. */
 /* replaces ft_plan_rotsphere, src/rotations.c:116-133 */
 ft_rotation_plan * ft_plan_rotsphere(const int n);
@@ -324,6 +339,11 @@ int ft_b200_execute_tet_dev(const ft_harmonic_plan * P, int forward, char TRANS,
 int ft_b200_tet_rotations_dev(const ft_harmonic_plan * P, int hi2lo, double * dA, int L, int M, void * stream);
 /* The spin rotation stage alone (hi2lo = 1: ft_execute_spinsph_hi2lo; 0: _lo2hi). */
 int ft_b200_spin_rotations_dev(const ft_spin_rotation_plan * SRP, int hi2lo, double * dA, int M, void * stream);
+/* The spin grid's synthesis (analysis = 0) or analysis sequence with the plan's kinds on device
+ * memory: dX holds 2 N M doubles (interleaved complex, 16-byte aligned), asynchronous on stream.
+ * No counterpart in the reference. */
+int ft_b200_execute_spinsph_grid_dev(const ft_spinsphere_fftw_plan * P, int analysis, char TRANS, double * dX, int N, int M,
+                                     void * stream);
 
 /* Batched drop-in: nfields fields, each with its own plan (plans may repeat,
  * degrees may differ), all in one persistent launch per stage.  dA[f] is the

@@ -1,5 +1,5 @@
 /* Every family's entry points as a C caller of the reference's API would use them (spin-weighted
- * with ft_complex data, Dunkl-Xu, annulus, tetrahedral, and the grids), built against
+ * with ft_complex data and its grid, Dunkl-Xu, annulus, tetrahedral, and the grids), built against
  * include/ft_b200.h with -lft_b200.  Without a usable device the first plan reports
  * FT_B200_ENODEV and the program prints "ENODEV"; with one, each family's forward then backward
  * transform must return its input to 1e-10, and the program prints "ok". */
@@ -37,9 +37,15 @@ int main(void) {
     for (int j = 0; j < M; j++)
         for (int i = 0; i < N - 2; i++)
             if (j < M - 2 * i) { Z[i + j * N][0] = Z0[i + j * N][0] = 0.5 / (1 + i + j); Z[i + j * N][1] = Z0[i + j * N][1] = -0.25 / (1 + i); }
+    ft_spinsphere_fftw_plan * ZS = ft_plan_spinsph_synthesis(N, M, 2, FT_FFTW_FLAGS), * ZA = ft_plan_spinsph_analysis(N, M, 2, FT_FFTW_FLAGS);
+    bad |= ft_get_spin_spinsphere_fftw_plan(ZA) != 2;
     ft_execute_spinsph2fourier('N', SP, Z, N, M);
+    ft_execute_spinsph_synthesis('N', ZS, Z, N, M);
+    ft_execute_spinsph_analysis('N', ZA, Z, N, M);
     ft_execute_fourier2spinsph('N', SP, Z, N, M);
     bad |= rt((double *) Z, (double *) Z0, 2 * (size_t) N * M) > 1e-10;
+    ft_destroy_spinsphere_fftw_plan(ZS);
+    ft_destroy_spinsphere_fftw_plan(ZA);
     ft_destroy_spin_harmonic_plan(SP);
     /* Dunkl-Xu, annulus, with their grids */
     double * A = malloc(sizeof(double) * (size_t) N * MD), * B = malloc(sizeof(double) * (size_t) N * MD);
