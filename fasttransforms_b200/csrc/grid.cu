@@ -663,7 +663,7 @@ bool run(SphereGridPlan * P, int op, char T, double * X, cudaStream_t st) {
         return theta(P, X, st) && weights(P, X, true, st) && phi_c2r(P, X, C_2_SQRT_PI / nm2, C_SQRT2, st);
     }
     if (op == RECT_SYN || op == RECT_ANA) {   // src/fftw.c:697-753
-        const double nm = (double) (N * M);
+        const double nm = (double) N * M;
         if (op == RECT_SYN) {
             if (T == 'N') return row_factor(P, X, 0, 0, 2, 2.0, st) && theta(P, X, st) && col0_scaling(P, X, 2.0, 0.25, 0.0, true, st) &&
                                  theta_rows(P, X, st);
@@ -678,7 +678,7 @@ bool run(SphereGridPlan * P, int op, char T, double * X, cudaStream_t st) {
     if (op == TET_SYN || op == TET_ANA) {     // src/fftw.c:351-402 (n x n x n)
         const int n = N;
         if (n <= 1) return true;
-        const double nlm = (double) (n * n * n);
+        const double nlm = (double) n * n * n;
         if (op == TET_SYN) {
             if (T == 'N') return tet_scaling(P, X, 2.0, 0.125, 0.0, st) && theta_tet(P, X, st);
             return theta_tet(P, X, st) && tet_scaling(P, X, 1.0, 0.125, 0.0, st);
@@ -688,7 +688,7 @@ bool run(SphereGridPlan * P, int op, char T, double * X, cudaStream_t st) {
     }
     if (op == TRI_SYN || op == TRI_ANA) {     // src/fftw.c:292-330
         if (N <= 1 || M <= 1) return true;
-        const double nm = (double) (N * M);
+        const double nm = (double) N * M;
         if (op == TRI_SYN) return tri_scaling(P, X, T == 'N' ? 2.0 : 1.0, 0.25, 0.0, st) && theta_tri(P, X, st);
         if (T == 'N') return theta_tri(P, X, st) && tri_scaling(P, X, 0.5, 1.0, nm, st);
         return tri_scaling(P, X, 1.0, 1.0, nm, st) && theta_tri(P, X, st);

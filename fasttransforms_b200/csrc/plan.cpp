@@ -29,9 +29,9 @@ void rotation_tables(int kind, int n, double alpha, double beta, double gamma, d
     if (kind == SPH) {
         for (int m = 0; m < n; m++)
             for (int l = 0; l < n - m; l++) {
-                const double nums = (l + 1) * (l + 2);
-                const double numc = (2 * m + 2) * (2 * l + 2 * m + 5);
-                const double den = (l + 2 * m + 3) * (l + 2 * m + 4);
+                const double nums = (double) ((long long) (l + 1) * (l + 2));   // exact integers (no int overflow)
+                const double numc = (double) ((long long) (2 * m + 2) * (2 * l + 2 * m + 5));
+                const double den = (double) ((long long) (l + 2 * m + 3) * (l + 2 * m + 4));
                 const long long o = Geo::table_base(SPH, n, m) + l;
                 s[o] = std::sqrt(nums / den);
                 c[o] = std::sqrt(numc / den);

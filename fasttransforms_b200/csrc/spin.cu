@@ -197,9 +197,9 @@ SpinRotPlan * make_srp(int n, int s) {
     for (int m = 0; m < n; m++)
         for (int j = 0; j < as; j++)
             for (int l = 0; l < n - m - j; l++) {
-                const double nums = (l + 1) * (l + m + 1);
-                const double numc = (2 * j + m + 1) * (2 * l + 2 * j + 2 * m + 3);
-                const double den = (l + 2 * j + m + 2) * (l + 2 * j + 2 * m + 2);
+                const double nums = (double) ((long long) (l + 1) * (l + m + 1));   // exact integers (no int overflow)
+                const double numc = (double) ((long long) (2 * j + m + 1) * (2 * l + 2 * j + 2 * m + 3));
+                const double den = (double) ((long long) (l + 2 * j + m + 2) * (l + 2 * j + 2 * m + 2));
                 sc[(size_t) l + (size_t) j * n + (size_t) m * as * n] = make_double2(std::sqrt(nums / den), std::sqrt(numc / den));
             }
     if (!ok(cudaMalloc(&P->d_sc2, sizeof(double2) * sc.size()), "cudaMalloc(spin table)") ||
