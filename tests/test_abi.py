@@ -5,6 +5,7 @@ import ctypes as C
 import os
 import re
 
+import numpy as np
 import pytest
 
 from conftest import ROOT, has_gpu
@@ -50,6 +51,28 @@ def test_no_device_fails_cleanly():
     assert ft.lib.ft_b200_last_status() in (2, 4)
     with pytest.raises(ft.FTB200Error):
         ft.plan_sph2fourier(16)
+
+
+def test_grid_plan_host_checks():
+    """Argument checks that run before any device work: the grid plans' odd-M rule (here before
+    the device probe, so it holds on any host), NULL plans in the getters, destroyers and execute
+    calls (a status, no crash), and the spin grid's no-op TRANS values."""
+    import fasttransforms_b200 as ft
+    L = ft.lib
+    for plan in (lambda: L.ft_plan_spinsph_synthesis(8, 14, 0, 0), lambda: L.ft_plan_spinsph_analysis(8, 14, 1, 0),
+                 lambda: L.ft_plan_sph_synthesis(8, 14, 0), lambda: L.ft_plan_disk_analysis(8, 14, 0)):
+        assert not plan()
+        assert L.ft_b200_last_status() == 1
+    assert L.ft_plan_spinsph_synthesis(0, 15, 0, 0) is None and L.ft_b200_last_status() == 1
+    assert L.ft_get_spin_spinsphere_fftw_plan(None) == 0
+    L.ft_destroy_spinsphere_fftw_plan(None)
+    X = np.zeros(2 * 8 * 15)
+    ptr = X.ctypes.data_as(C.POINTER(C.c_double))
+    L.ft_execute_spinsph_synthesis(b"N", None, ptr, 8, 15)
+    assert L.ft_b200_last_status() == 1
+    L.ft_execute_sph_analysis(b"N", None, ptr, 8, 15)
+    assert L.ft_b200_last_status() == 1
+    assert L.ft_b200_execute_spinsph_grid_dev(None, 0, b"N", None, 8, 15, None) == 1
 
 
 @pytest.mark.parametrize("src", ["dropin.c", "families.c"])
