@@ -38,7 +38,7 @@ __all__ = [
     "execute_sph_grid_dev", "GRID_OPS",
     "SpinHarmonicPlan", "SpinRotationPlan", "plan_spinsph2fourier", "plan_rotspinsphere",
     "execute_spinsph2fourier", "execute_fourier2spinsph", "execute_spinsph_hi2lo", "execute_spinsph_lo2hi",
-    "execute_spin_dev", "spin_rotations_dev", "spinsphrand",
+    "execute_spin_dev", "spin_rotations_dev", "spinsphrand", "kernel_column",
     "SpinGridPlan", "plan_spinsph_synthesis", "plan_spinsph_analysis", "execute_spinsph_synthesis",
     "execute_spinsph_analysis", "execute_spinsph_grid_dev",
     "plan_rectdisk2cheb", "execute_rectdisk2cheb", "execute_cheb2rectdisk", "plan_rotrectdisk",
@@ -140,6 +140,7 @@ def _load() -> C.CDLL:
     for fam in ("sph", "tri", "disk", "rectdisk"):
         for d_ in ("hi2lo", "lo2hi"):
             sig[f"ft_execute_{fam}_{d_}"] = (None, [vp, dp, dp, i])
+            sig[f"ft_kernel_{fam}_{d_}"] = (None, [vp, i, i, dp, i])
     for name, (res, args) in sig.items():
         f = getattr(L, name)
         f.restype = res
@@ -701,6 +702,21 @@ def execute_disk_hi2lo(RP, A, M=None): _exec_rot("ft_execute_disk_hi2lo", RP, A,
 def execute_disk_lo2hi(RP, A, M=None): _exec_rot("ft_execute_disk_lo2hi", RP, A, M)
 def execute_rectdisk_hi2lo(RP, A, M=None): _exec_rot("ft_execute_rectdisk_hi2lo", RP, A, M)
 def execute_rectdisk_lo2hi(RP, A, M=None): _exec_rot("ft_execute_rectdisk_lo2hi", RP, A, M)
+
+
+_KERNEL_FAMILY = {"sph": "sph", "tri": "tri", "disk": "disk", "rect": "rectdisk"}
+
+
+def kernel_column(RP: "RotationPlan", hi2lo: bool, m1: int, m2: int, a: np.ndarray, S: int = 1) -> None:
+    """ft_kernel_<family>_{hi2lo,lo2hi}(RP, m1, m2, a, S) on a writeable float64 host array, in
+    place: the sweeps between orders m1 and m2 on the column a[0], a[S], a[2 S], .."""
+    if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.ndim == 1 and a.flags.c_contiguous and a.flags.writeable):
+        raise TypeError("a must be a writeable contiguous 1-D float64 array")
+    if S < 1 or (a.size - 1) // S + 1 < RP.n:
+        raise ValueError("a must hold the plan's n entries at stride S")
+    fam = _KERNEL_FAMILY[RP.kind]
+    getattr(lib, f"ft_kernel_{fam}_{'hi2lo' if hi2lo else 'lo2hi'}")(RP.ptr, m1, m2, a.ctypes.data_as(C.POINTER(C.c_double)), S)
+    _check()
 
 
 def execute_dev(P: HarmonicPlan, forward: bool, trans: str, ptr: int, N: int, M: int, stream: int = 0) -> None:

@@ -19,7 +19,7 @@ OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libft_b200.so")
 BUILD_DIR = os.path.join(HERE, "_build")
 
-SOURCES = ["rotations.cu", "trmm.cu", "blocked.cu", "trmm_mixed.cu", "grid.cu", "spin.cu", "rectdisk.cu", "tet.cu", "ann.cu", "api.cu", "noalloc.cu", "plan.cpp"]
+SOURCES = ["rotations.cu", "trmm.cu", "blocked.cu", "trmm_mixed.cu", "grid.cu", "spin.cu", "rectdisk.cu", "tet.cu", "ann.cu", "column.cu", "api.cu", "noalloc.cu", "plan.cpp"]
 CUDA_LIB = "/usr/local/cuda/lib64"   # cuFFT (grid synthesis / analysis), same path on every box of this image
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

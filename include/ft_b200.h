@@ -300,6 +300,18 @@ void ft_execute_tet_lo2hi(const ft_rotation_plan * RP1, const ft_rotation_plan *
 /* replace ft_execute_rectdisk_hi2lo / lo2hi, src/drivers.c:488-508 (order m on column m) */
 void ft_execute_rectdisk_hi2lo(const ft_rotation_plan * RP, double * A, double * B, const int M);
 void ft_execute_rectdisk_lo2hi(const ft_rotation_plan * RP, double * A, double * B, const int M);
+/* replace ft_kernel_{sph,tri,disk,rectdisk}_{hi2lo,lo2hi}, src/rotations.c:135-141, 162-168,
+ * 262-268, 289-295: one host column A with stride S >= 1 (its entries k S), the sweeps from order
+ * m2 down to order m1 (hi2lo) or from m1 up to m2 (lo2hi), m1 >= 0, with the plan's table.  Only
+ * the entries the sweeps touch are read and written. */
+void ft_kernel_sph_hi2lo(const ft_rotation_plan * RP, const int m1, const int m2, double * A, const int S);
+void ft_kernel_sph_lo2hi(const ft_rotation_plan * RP, const int m1, const int m2, double * A, const int S);
+void ft_kernel_tri_hi2lo(const ft_rotation_plan * RP, const int m1, const int m2, double * A, const int S);
+void ft_kernel_tri_lo2hi(const ft_rotation_plan * RP, const int m1, const int m2, double * A, const int S);
+void ft_kernel_disk_hi2lo(const ft_rotation_plan * RP, const int m1, const int m2, double * A, const int S);
+void ft_kernel_disk_lo2hi(const ft_rotation_plan * RP, const int m1, const int m2, double * A, const int S);
+void ft_kernel_rectdisk_hi2lo(const ft_rotation_plan * RP, const int m1, const int m2, double * A, const int S);
+void ft_kernel_rectdisk_lo2hi(const ft_rotation_plan * RP, const int m1, const int m2, double * A, const int S);
 
 /* ------------------------------------------------------------------------ */
 /* Device-pointer entry points (no host copies).  A is a device pointer     */

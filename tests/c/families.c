@@ -47,6 +47,15 @@ int main(void) {
     ft_destroy_spinsphere_fftw_plan(ZS);
     ft_destroy_spinsphere_fftw_plan(ZA);
     ft_destroy_spin_harmonic_plan(SP);
+    /* one column's sweeps (the low-level kernels), stride 2, there and back */
+    ft_rotation_plan * RS1 = ft_plan_rotsphere(N);
+    double col[2 * 12], col0[2 * 12];
+    fill(col, 2 * (size_t) N, 4);
+    for (int k = 0; k < 2 * N; k++) col0[k] = col[k];
+    ft_kernel_sph_hi2lo(RS1, 1, 9, col, 2);
+    ft_kernel_sph_lo2hi(RS1, 1, 9, col, 2);
+    bad |= rt(col, col0, 2 * (size_t) N) > 1e-13;
+    ft_destroy_rotation_plan(RS1);
     /* Dunkl-Xu, annulus, with their grids */
     double * A = malloc(sizeof(double) * (size_t) N * MD), * B = malloc(sizeof(double) * (size_t) N * MD);
     fill(A, (size_t) N * N, 1);
