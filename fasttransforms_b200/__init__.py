@@ -38,7 +38,7 @@ __all__ = [
     "execute_sph_grid_dev", "GRID_OPS",
     "SpinHarmonicPlan", "SpinRotationPlan", "plan_spinsph2fourier", "plan_rotspinsphere",
     "execute_spinsph2fourier", "execute_fourier2spinsph", "execute_spinsph_hi2lo", "execute_spinsph_lo2hi",
-    "execute_spin_dev", "spin_rotations_dev", "spinsphrand", "kernel_column",
+    "execute_spin_dev", "spin_rotations_dev", "spinsphrand", "kernel_column", "kernel_spin_column", "kernel_tet_slab",
     "SpinGridPlan", "plan_spinsph_synthesis", "plan_spinsph_analysis", "execute_spinsph_synthesis",
     "execute_spinsph_analysis", "execute_spinsph_grid_dev",
     "plan_rectdisk2cheb", "execute_rectdisk2cheb", "execute_cheb2rectdisk", "plan_rotrectdisk",
@@ -129,6 +129,8 @@ def _load() -> C.CDLL:
         "ft_destroy_spinsphere_fftw_plan": (None, [vp]), "ft_get_spin_spinsphere_fftw_plan": (i, [vp]),
         "ft_execute_spinsph_synthesis": (None, [ch, vp, dp, i, i]), "ft_execute_spinsph_analysis": (None, [ch, vp, dp, i, i]),
         "ft_b200_execute_spinsph_grid_dev": (i, [vp, i, ch, vp, i, i, vp]),
+        "ft_kernel_spinsph_hi2lo": (None, [vp, i, dp, i]), "ft_kernel_spinsph_lo2hi": (None, [vp, i, dp, i]),
+        "ft_kernel_tet_hi2lo": (None, [vp, i, i, dp]), "ft_kernel_tet_lo2hi": (None, [vp, i, i, dp]),
     }
     for name in ("sph_synthesis", "sph_analysis", "sphv_synthesis", "sphv_analysis", "disk_synthesis", "disk_analysis",
                  "tri_synthesis", "tri_analysis", "annulus_synthesis", "annulus_analysis", "rectdisk_synthesis",
@@ -716,6 +718,29 @@ def kernel_column(RP: "RotationPlan", hi2lo: bool, m1: int, m2: int, a: np.ndarr
         raise ValueError("a must hold the plan's n entries at stride S")
     fam = _KERNEL_FAMILY[RP.kind]
     getattr(lib, f"ft_kernel_{fam}_{'hi2lo' if hi2lo else 'lo2hi'}")(RP.ptr, m1, m2, a.ctypes.data_as(C.POINTER(C.c_double)), S)
+    _check()
+
+
+def kernel_spin_column(SRP: "SpinRotationPlan", hi2lo: bool, m: int, a: np.ndarray, S: int = 1) -> None:
+    """ft_kernel_spinsph_{hi2lo,lo2hi}(SRP, m, a, S) on a writeable complex128 host array, in place:
+    the column a[0], a[S], a[2 S], .. of order m."""
+    if not (isinstance(a, np.ndarray) and a.dtype == np.complex128 and a.ndim == 1 and a.flags.c_contiguous and a.flags.writeable):
+        raise TypeError("a must be a writeable contiguous 1-D complex128 array")
+    if S < 1 or (a.size - 1) // S + 1 < SRP.n:
+        raise ValueError("a must hold the plan's n entries at stride S")
+    f = lib.ft_kernel_spinsph_hi2lo if hi2lo else lib.ft_kernel_spinsph_lo2hi
+    f(SRP.ptr, m, a.ctypes.data_as(C.POINTER(C.c_double)), S)
+    _check()
+
+
+def kernel_tet_slab(RP: "RotationPlan", hi2lo: bool, L: int, m: int, a: np.ndarray) -> None:
+    """ft_kernel_tet_{hi2lo,lo2hi}(RP, L, m, a) on the n x L slab a (float64, Fortran order), in place."""
+    if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.ndim == 2 and a.flags.f_contiguous and a.flags.writeable):
+        raise TypeError("a must be a writeable 2-D float64 array in Fortran order")
+    if a.shape != (RP.n, L):
+        raise ValueError("a must be n x L")
+    f = lib.ft_kernel_tet_hi2lo if hi2lo else lib.ft_kernel_tet_lo2hi
+    f(RP.ptr, L, m, a.ctypes.data_as(C.POINTER(C.c_double)))
     _check()
 
 

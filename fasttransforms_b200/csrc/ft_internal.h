@@ -285,6 +285,11 @@ int mixed_trmm_device_error(void * p);
 void set_error(int status, const std::string & msg);
 void clear_error();
 void count_launch(unsigned long long n = 1);
+// column.cu: one column's sweeps (kinds SPH, TRI, DISK, RECT, and SPIN for a spin column's first
+// stage with its table at k + j n + d |s| n) on device memory of len entries (double2 if cplx)
+int column_touched(int kind, int n, bool hi2lo, int m1, int m2, int d);
+bool column_sweeps_dev(void * dcol, bool cplx, const double2 * tab, int kind, int n, int m1, int m2, bool hi2lo, bool fwd, int d,
+                       int as, int len);
 // measurement hook: bracket a launch with events on its stream when profiling is on
 enum { FAM_ROT = 0, FAM_TRMM = 1, FAM_OTHER = 2, FAM_BLOCK = 3 };
 void prof_begin(int family, cudaStream_t st);

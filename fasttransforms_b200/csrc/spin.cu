@@ -359,6 +359,39 @@ void spin_host(const ft_spin_harmonic_plan * Pp, bool forward, char T, ft_comple
             [&](double * d) { return transform(P, forward, T, d, M, R->stream); });
 }
 
+// One spin column (the reference's ft_kernel_spinsph_hi2lo / lo2hi, src/rotations.c:479-485, whose
+// bodies are src/rotations/rotations_default.c:87-117): the host column A (stride S complex
+// entries) of order m; hi2lo runs the first stage (min(|m|, |s|) adjacent sweeps of the spin table,
+// forward for m s >= 0, transposed otherwise) and then the sph sweeps of order d = ||m| - |s||;
+// lo2hi runs the sph sweeps transposed and then the first stage with the other form.  Both
+// stages are column.cu's wavefront on the complex column.
+void spin_column_host(const ft_spin_rotation_plan * Pp, bool hi2lo, int m, ft_complex * A, int S) {
+    clear_error();
+    SpinRotPlan * P = as_srp(Pp);
+    if (!P || !A) { set_error(FT_B200_EINVAL, "NULL or foreign argument"); return; }
+    if (S < 1) { set_error(FT_B200_EINVAL, "S must be >= 1"); return; }
+    const int n = P->n, as = std::abs(P->s), am = std::abs(m);
+    const int d = std::abs(am - as), mn = std::min(am, as), par = (am + as) % 2;
+    const bool fwd1 = hi2lo == ((long long) m * P->s >= 0);
+    const int len = std::max(column_touched(SPIN, n, hi2lo, 0, mn, d), column_touched(SPH, n, hi2lo, par, d, 0));
+    if (len == 0) return;   // no rotation
+    std::vector<double2> h(len);
+    for (int k = 0; k < len; k++) h[k] = make_double2(A[(long long) k * S][0], A[(long long) k * S][1]);
+    int prev = 0;
+    if (!ok(cudaGetDevice(&prev), "cudaGetDevice") || !ok(cudaSetDevice(P->device), "cudaSetDevice")) return;
+    double2 * dcol = nullptr;
+    const size_t bytes = sizeof(double2) * (size_t) len;
+    auto stage1 = [&] { return column_sweeps_dev(dcol, true, P->d_sc2, SPIN, n, 0, mn, hi2lo, fwd1, d, as, len); };
+    auto stage2 = [&] { return column_sweeps_dev(dcol, true, P->sph->d_sc, SPH, n, par, d, hi2lo, hi2lo, 0, 0, len); };
+    bool good = ok(cudaMalloc(&dcol, bytes), "cudaMalloc") && ok(cudaMemcpy(dcol, h.data(), bytes, cudaMemcpyHostToDevice), "cudaMemcpy(H2D)") &&
+                (hi2lo ? (stage1() && stage2()) : (stage2() && stage1())) &&
+                ok(cudaMemcpy(h.data(), dcol, bytes, cudaMemcpyDeviceToHost), "cudaMemcpy(D2H)");
+    cudaFree(dcol);
+    cudaSetDevice(prev);
+    if (good)
+        for (int k = 0; k < len; k++) { A[(long long) k * S][0] = h[k].x; A[(long long) k * S][1] = h[k].y; }
+}
+
 }  // namespace
 }  // namespace ftb
 
@@ -375,6 +408,12 @@ void ft_execute_spinsph_hi2lo(const ft_spin_rotation_plan * SRP, ft_complex * A,
 }
 void ft_execute_spinsph_lo2hi(const ft_spin_rotation_plan * SRP, ft_complex * A, ft_complex *, const int M) {
     spin_rot_host(SRP, false, A, M);
+}
+void ft_kernel_spinsph_hi2lo(const ft_spin_rotation_plan * SRP, const int m, ft_complex * A, const int S) {
+    spin_column_host(SRP, true, m, A, S);
+}
+void ft_kernel_spinsph_lo2hi(const ft_spin_rotation_plan * SRP, const int m, ft_complex * A, const int S) {
+    spin_column_host(SRP, false, m, A, S);
 }
 
 int ft_b200_spin_rotations_dev(const ft_spin_rotation_plan * SRP, int hi2lo, double * dA, int M, void * stream) {

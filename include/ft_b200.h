@@ -235,6 +235,10 @@ void ft_destroy_spin_rotation_plan(ft_spin_rotation_plan * SRP);
  * scratch) is accepted and not used */
 void ft_execute_spinsph_hi2lo(const ft_spin_rotation_plan * SRP, ft_complex * A, ft_complex * B, const int M);
 void ft_execute_spinsph_lo2hi(const ft_spin_rotation_plan * SRP, ft_complex * A, ft_complex * B, const int M);
+/* replace ft_kernel_spinsph_hi2lo / lo2hi, src/rotations.c:479-485: one host column A of order m
+ * (stride S >= 1 complex entries); only the entries the sweeps touch are read and written. */
+void ft_kernel_spinsph_hi2lo(const ft_spin_rotation_plan * SRP, const int m, ft_complex * A, const int S);
+void ft_kernel_spinsph_lo2hi(const ft_spin_rotation_plan * SRP, const int m, ft_complex * A, const int S);
 /* Same members as the reference's (src/fasttransforms.h:441-450).  P1 .. P2inv are
  * host copies of the connection matrices (the real sph matrices stored as complex);
  * B is NULL. */
@@ -312,6 +316,11 @@ void ft_kernel_disk_hi2lo(const ft_rotation_plan * RP, const int m1, const int m
 void ft_kernel_disk_lo2hi(const ft_rotation_plan * RP, const int m1, const int m2, double * A, const int S);
 void ft_kernel_rectdisk_hi2lo(const ft_rotation_plan * RP, const int m1, const int m2, double * A, const int S);
 void ft_kernel_rectdisk_lo2hi(const ft_rotation_plan * RP, const int m1, const int m2, double * A, const int S);
+/* replace ft_kernel_tet_hi2lo / lo2hi, src/rotations.c:297-321: the contiguous n x L slab A (n the
+ * triangle plan's), sweeps j = m - 1 .. 0 of rotations of its column pairs (l, l + 1);
+ * 0 <= L <= n, 0 <= m <= n. */
+void ft_kernel_tet_hi2lo(const ft_rotation_plan * RP, const int L, const int m, double * A);
+void ft_kernel_tet_lo2hi(const ft_rotation_plan * RP, const int L, const int m, double * A);
 
 /* ------------------------------------------------------------------------ */
 /* Device-pointer entry points (no host copies).  A is a device pointer     */

@@ -140,6 +140,9 @@ class Oracle:
         L.oracle_execute_spin.argtypes = [sp, C.c_int, C.c_char, dp, C.c_int, C.c_int]
         for f in ("oracle_execute_spinsph_hi2lo", "oracle_execute_spinsph_lo2hi"):
             getattr(L, f).argtypes = [sp, dp, C.c_int]
+        for f in ("oracle_kernel_spinsph_hi2lo", "oracle_kernel_spinsph_lo2hi"):
+            getattr(L, f).argtypes = [sp, C.c_int, dp]
+        L.oracle_kernel_tet.argtypes = [PP, C.c_int, C.c_int, dp, C.c_int]
         L.oracle_fill_spin.argtypes = [C.c_int, C.c_int, C.c_int, C.c_ulonglong, dp]
         AP = C.POINTER(_OracleAnnPlan)
         L.oracle_plan_ann2cxf.restype = AP
@@ -233,6 +236,18 @@ class Oracle:
 
     def spin_lo2hi(self, P, A: np.ndarray):
         self.lib.oracle_execute_spinsph_lo2hi(P, _cptr(A), A.shape[1])
+
+    def spin_kernel(self, P, hi2lo: bool, m: int, col: np.ndarray) -> np.ndarray:
+        """One complex column of order m (src/rotations/rotations_default.c:87-117)."""
+        a = np.ascontiguousarray(col, dtype=complex).copy()
+        (self.lib.oracle_kernel_spinsph_hi2lo if hi2lo else self.lib.oracle_kernel_spinsph_lo2hi)(P, m, _cptr(a))
+        return a
+
+    def tet_kernel(self, RP, hi2lo: bool, L: int, m: int, A: np.ndarray) -> np.ndarray:
+        """The n x L slab of order m with a triangle rotation plan (src/rotations.c:297-321)."""
+        a = np.asfortranarray(A, dtype=np.float64).copy(order="F")
+        self.lib.oracle_kernel_tet(RP, L, m, _ptr(a), 1 if hi2lo else 0)
+        return a
 
     def spin_fill(self, n: int, M: int, s: int, seed: int) -> np.ndarray:
         A = np.zeros((n, M), dtype=complex, order="F")

@@ -997,6 +997,7 @@ static void kernel_tet(const oracle_plan * RP, int L, int m, double * A, int hi2
             }
     }
 }
+void oracle_kernel_tet(const oracle_plan * RP, int L, int m, double * A, int hi2lo) { kernel_tet(RP, L, m, A, hi2lo); }
 
 /* src/drivers.c:510-528: slab m: the tri sweeps of order l + m down column l (l < L - m),
  * then the sweeps across the slab (lo2hi: the reverse) */

@@ -83,6 +83,8 @@ oracle_spin_plan * oracle_plan_spinsph2fourier(int n, int s, int connections);
 void oracle_destroy_spin_plan(oracle_spin_plan * P);
 void oracle_kernel_spinsph_hi2lo(const oracle_spin_plan * P, int m, double * A);
 void oracle_kernel_spinsph_lo2hi(const oracle_spin_plan * P, int m, double * A);
+/* src/rotations.c:297-321: the n x L slab (n the triangle plan's) of order m */
+void oracle_kernel_tet(const oracle_plan * RP, int L, int m, double * A, int hi2lo);
 void oracle_execute_spinsph_hi2lo(const oracle_spin_plan * P, double * A, int M);
 void oracle_execute_spinsph_lo2hi(const oracle_spin_plan * P, double * A, int M);
 /* forward = 1: spinsph2fourier; 0: fourier2spinsph */

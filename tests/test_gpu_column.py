@@ -1,5 +1,6 @@
 """One column's sweeps on the GPU (ft_kernel_{sph,tri,disk,rectdisk}_{hi2lo,lo2hi}:
-src/rotations.c:135-141, 162-168, 262-268, 289-295), through the C ABI.
+src/rotations.c:135-141, 162-168, 262-268, 289-295; ft_kernel_spinsph_* and ft_kernel_tet_*:
+src/rotations.c:297-321, 479-485), through the C ABI.
 
 Against the oracle's sequential per-column loops (oracle/ft_oracle.c, oracle_kernel_hi2lo /
 lo2hi, pinned to the compiled reference in tests/test_oracle_pin.py) in its fused form, bit for
@@ -119,4 +120,43 @@ def test_bad_arguments(env):
     with pytest.raises(ValueError):
         ft.kernel_column(RP, True, 0, 4, np.zeros(7))
     ft.kernel_column(RP, True, 4, 4, a)          # no sweep: a no-op
+    RP.close()
+
+
+@pytest.mark.parametrize("n", [1, 3, 24, 200])
+@pytest.mark.parametrize("s", [-3, 0, 1, 4])
+def test_spin_column_vs_oracle_bit_exact(env, n, s):
+    """ft_kernel_spinsph_hi2lo / lo2hi (src/rotations.c:479-485) against the oracle's column
+    kernel: every order -(n + 1) .. n + 1, strides 1 and 2."""
+    ft, O = env
+    SRP = ft.plan_rotspinsphere(n, s)
+    P = O.spin_plan(n, s, connections=False)
+    rng = np.random.default_rng(n + 10 * s)
+    for m in range(-(n + 1), n + 2):
+        for S in (1, 2):
+            A = rng.uniform(-1, 1, n * S) + 1j * rng.uniform(-1, 1, n * S)
+            for hi2lo in (True, False):
+                want = O.spin_kernel(P, hi2lo, m, A[::S])
+                got = A.copy()
+                ft.kernel_spin_column(SRP, hi2lo, m, got, S)
+                assert np.array_equal(got[::S], want), (n, s, m, S, hi2lo)
+    O.spin_destroy(P)
+    SRP.close()
+
+
+@pytest.mark.parametrize("n,L", [(1, 1), (5, 5), (40, 40), (40, 17), (130, 130)])
+def test_tet_slab_vs_oracle_bit_exact(env, n, L):
+    """ft_kernel_tet_hi2lo / lo2hi (src/rotations.c:297-321) against the oracle's slab loops."""
+    ft, O = env
+    RP = ft.plan_rottriangle(n, 0.0, -0.5, 0.25)
+    Po = O.plan("tri", n, alpha=0.0, beta=-0.5, gamma=0.25, rotations_only=True)
+    rng = np.random.default_rng(n + L)
+    for m in sorted({0, 1, L // 2, L - 1, L, n}):
+        A = np.asfortranarray(rng.uniform(-1, 1, (n, L)))
+        for hi2lo in (True, False):
+            want = O.tet_kernel(Po, hi2lo, L, m, A)
+            got = A.copy(order="F")
+            ft.kernel_tet_slab(RP, hi2lo, L, m, got)
+            assert np.array_equal(got, want), (n, L, m, hi2lo)
+    O.destroy(Po)
     RP.close()

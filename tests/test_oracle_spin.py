@@ -89,3 +89,25 @@ def test_spin_rotation_round_trip(oracles):
             O.spin_destroy(Po)
             assert rel2(B, A) <= 4 * np.sqrt(n) * EPS
             assert np.abs(B - A).max() / np.abs(A).max() <= 2 * n * EPS
+
+
+@pytest.mark.parametrize("s", [-2, 0, 3])
+def test_oracle_spin_column_kernel_matches_matrix_form(s):
+    """The oracle's one-column kernel (the reference's ft_kernel_spinsph_hi2lo / lo2hi) on each
+    column of a matrix, order 0 in column 0 and orders -m, m in columns 2m - 1, 2m, equals its
+    matrix form: the checker of the device column kernels agrees with the pinned matrix sweeps."""
+    from oracle.bind import Oracle
+    O = Oracle()
+    n = 24
+    M = 2 * n - 1
+    P = O.spin_plan(n, s, connections=False)
+    A = O.spin_fill(n, M, s, 3)
+    for hi2lo in (True, False):
+        whole = A.copy(order="F")
+        (O.spin_hi2lo if hi2lo else O.spin_lo2hi)(P, whole)
+        cols = np.empty_like(A)
+        for c in range(M):
+            m = 0 if c == 0 else ((c + 1) // 2 if c % 2 == 0 else -((c + 1) // 2))
+            cols[:, c] = O.spin_kernel(P, hi2lo, m, A[:, c])
+        assert np.array_equal(cols, whole), hi2lo
+    O.spin_destroy(P)
