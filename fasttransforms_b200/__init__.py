@@ -39,6 +39,7 @@ __all__ = [
     "SpinHarmonicPlan", "SpinRotationPlan", "plan_spinsph2fourier", "plan_rotspinsphere",
     "execute_spinsph2fourier", "execute_fourier2spinsph", "execute_spinsph_hi2lo", "execute_spinsph_lo2hi",
     "execute_spin_dev", "spin_rotations_dev", "spinsphrand", "kernel_column", "kernel_spin_column", "kernel_tet_slab",
+    "execute_sphv_hi2lo", "execute_sphv_lo2hi",
     "SpinGridPlan", "plan_spinsph_synthesis", "plan_spinsph_analysis", "execute_spinsph_synthesis",
     "execute_spinsph_analysis", "execute_spinsph_grid_dev",
     "plan_rectdisk2cheb", "execute_rectdisk2cheb", "execute_cheb2rectdisk", "plan_rotrectdisk",
@@ -139,10 +140,11 @@ def _load() -> C.CDLL:
     for name in ("sph2fourier", "fourier2sph", "tri2cheb", "cheb2tri", "disk2cxf", "cxf2disk", "sphv2fourier", "fourier2sphv",
                  "rectdisk2cheb", "cheb2rectdisk", "ann2cxf", "cxf2ann"):
         sig["ft_execute_" + name] = (None, [ch, vp, dp, i, i])
-    for fam in ("sph", "tri", "disk", "rectdisk"):
+    for fam in ("sph", "tri", "disk", "rectdisk", "sphv"):
         for d_ in ("hi2lo", "lo2hi"):
             sig[f"ft_execute_{fam}_{d_}"] = (None, [vp, dp, dp, i])
-            sig[f"ft_kernel_{fam}_{d_}"] = (None, [vp, i, i, dp, i])
+            if fam != "sphv":
+                sig[f"ft_kernel_{fam}_{d_}"] = (None, [vp, i, i, dp, i])
     for name, (res, args) in sig.items():
         f = getattr(L, name)
         f.restype = res
@@ -704,6 +706,8 @@ def execute_disk_hi2lo(RP, A, M=None): _exec_rot("ft_execute_disk_hi2lo", RP, A,
 def execute_disk_lo2hi(RP, A, M=None): _exec_rot("ft_execute_disk_lo2hi", RP, A, M)
 def execute_rectdisk_hi2lo(RP, A, M=None): _exec_rot("ft_execute_rectdisk_hi2lo", RP, A, M)
 def execute_rectdisk_lo2hi(RP, A, M=None): _exec_rot("ft_execute_rectdisk_lo2hi", RP, A, M)
+def execute_sphv_hi2lo(RP, A, M=None): _exec_rot("ft_execute_sphv_hi2lo", RP, A, M)
+def execute_sphv_lo2hi(RP, A, M=None): _exec_rot("ft_execute_sphv_lo2hi", RP, A, M)
 
 
 _KERNEL_FAMILY = {"sph": "sph", "tri": "tri", "disk": "disk", "rect": "rectdisk"}

@@ -470,6 +470,25 @@ void rotations_host(const ft_rotation_plan * RPc, bool hi2lo, double * A, int M,
     cudaFree(d);
 }
 
+// sphv (src/drivers.c:168-276): order m on the column pair (2m + 1, 2m + 2), m = 2 .. M/2 - 1, the
+// sph sweeps on the matrix two columns in; orders exist for M >= 7
+void rotations_sphv_host(const ft_rotation_plan * RPc, bool hi2lo, double * A, int M) {
+    clear_error();
+    ft_rotation_plan * RP = const_cast<ft_rotation_plan *>(RPc);
+    if (!RP || !A) { set_error(FT_B200_EINVAL, "NULL argument"); return; }
+    if (RP->kind != SPH) { set_error(FT_B200_EINVAL, "sphv sweeps take a sph rotation plan"); return; }
+    if (M < 1) { set_error(FT_B200_EINVAL, "M must be positive"); return; }
+    if (!valid_pairs(SPH, M) || M < 7) return;
+    const size_t elems = (size_t) RP->n * M;
+    double * d = nullptr;
+    if (!cuda_ok(cudaMalloc(&d, elems * sizeof(double)), "cudaMalloc")) return;
+    if (cuda_ok(cudaMemcpy(d, A, elems * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy(H2D)") &&
+        rotations_sphv(RP, hi2lo, d, d, M, RP->n, 0) &&
+        cuda_ok(cudaDeviceSynchronize(), "cudaDeviceSynchronize"))
+        cuda_ok(cudaMemcpy(A, d, elems * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy(D2H)");
+    cudaFree(d);
+}
+
 // ---------------------------------------------------------------------------
 // batches: many fields in one launch per stage
 // ---------------------------------------------------------------------------
@@ -903,6 +922,8 @@ void ft_execute_disk_hi2lo(const ft_rotation_plan * RP, double * A, double *, co
 void ft_execute_disk_lo2hi(const ft_rotation_plan * RP, double * A, double *, const int M) { rotations_host(RP, false, A, M, DISK); }
 void ft_execute_rectdisk_hi2lo(const ft_rotation_plan * RP, double * A, double *, const int M) { rotations_host(RP, true, A, M, RECT); }
 void ft_execute_rectdisk_lo2hi(const ft_rotation_plan * RP, double * A, double *, const int M) { rotations_host(RP, false, A, M, RECT); }
+void ft_execute_sphv_hi2lo(const ft_rotation_plan * RP, double * A, double *, const int M) { rotations_sphv_host(RP, true, A, M); }
+void ft_execute_sphv_lo2hi(const ft_rotation_plan * RP, double * A, double *, const int M) { rotations_sphv_host(RP, false, A, M); }
 
 int ft_b200_execute_dev(const ft_harmonic_plan * P, int forward, char TRANS, double * dA, int N, int M, void * stream) {
     clear_error();

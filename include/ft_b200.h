@@ -296,6 +296,10 @@ void ft_execute_tri_hi2lo(const ft_rotation_plan * RP, double * A, double * B, c
 void ft_execute_tri_lo2hi(const ft_rotation_plan * RP, double * A, double * B, const int M);
 void ft_execute_disk_hi2lo(const ft_rotation_plan * RP, double * A, double * B, const int M);
 void ft_execute_disk_lo2hi(const ft_rotation_plan * RP, double * A, double * B, const int M);
+/* replace ft_execute_sphv_hi2lo / lo2hi, src/drivers.c:168-276: a sph rotation plan on the sphv
+ * layout (order m on columns 2m + 1, 2m + 2, m = 2 .. M/2 - 1; M odd); B is accepted and not used. */
+void ft_execute_sphv_hi2lo(const ft_rotation_plan * RP, double * A, double * B, const int M);
+void ft_execute_sphv_lo2hi(const ft_rotation_plan * RP, double * A, double * B, const int M);
 /* replace ft_execute_tet_hi2lo / lo2hi, src/drivers.c:510-528: RP1, RP2 triangle plans of one n
  * (ft_plan_rottriangle(n, alpha, beta, gamma + delta + 1) and (n, beta, gamma, delta) for the
  * tetrahedral transform); A is n x L x M with L <= n */

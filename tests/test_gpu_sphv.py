@@ -104,3 +104,25 @@ def test_sphv_rejects_other_families(env):
     with pytest.raises(ft.FTB200Error):
         ft.execute_sphv_dev(P, True, "N", t.data_ptr(), 8, P.M)
     P.close()
+
+
+@pytest.mark.skip(reason="host sphv rotation entry not yet run on a B200")
+@pytest.mark.parametrize("n", [1, 3, 4, 17, 65])
+def test_sphv_rotation_entry_points_bit_exact(env, n):
+    """ft_execute_sphv_hi2lo / lo2hi (src/drivers.c:168-276) against the oracle's column loops:
+    order m on the columns 2m + 1 and 2m + 2, m = 2 .. M/2 - 1, the other columns untouched."""
+    ft, torch, O = env
+    M = 2 * n - 1
+    RP = ft.plan_rotsphere(n)
+    Po = O.plan("sph", n, rotations_only=True)
+    A = np.asfortranarray(np.random.default_rng(n).uniform(-1, 1, (n, M)))
+    for hi2lo in (True, False):
+        want = A.copy(order="F")
+        for m in range(2, M // 2):
+            for c in (2 * m + 1, 2 * m + 2):
+                want[:, c] = O.kernel(Po, hi2lo, m % 2, m, A[:, c].copy())
+        got = A.copy(order="F")
+        (ft.execute_sphv_hi2lo if hi2lo else ft.execute_sphv_lo2hi)(RP, got)
+        assert np.array_equal(got, want), (n, hi2lo)
+    O.destroy(Po)
+    RP.close()
