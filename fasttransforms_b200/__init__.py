@@ -132,6 +132,7 @@ def _load() -> C.CDLL:
         "ft_b200_execute_spinsph_grid_dev": (i, [vp, i, ch, vp, i, i, vp]),
         "ft_kernel_spinsph_hi2lo": (None, [vp, i, dp, i]), "ft_kernel_spinsph_lo2hi": (None, [vp, i, dp, i]),
         "ft_kernel_tet_hi2lo": (None, [vp, i, i, dp]), "ft_kernel_tet_lo2hi": (None, [vp, i, i, dp]),
+        "ft_set_num_threads": (None, [i]), "ft_fftw_init_threads": (i, []), "ft_fftw_plan_with_nthreads": (None, [i]),
     }
     for name in ("sph_synthesis", "sph_analysis", "sphv_synthesis", "sphv_analysis", "disk_synthesis", "disk_analysis",
                  "tri_synthesis", "tri_analysis", "annulus_synthesis", "annulus_analysis", "rectdisk_synthesis",

@@ -58,6 +58,9 @@ void prof_end(cudaStream_t st) {
     t_prof_family = -1;
 }
 
+std::atomic<int> g_host_threads{0};
+int host_threads() { return g_host_threads.load(std::memory_order_relaxed); }
+
 void set_error(int status, const std::string & msg) { t_status = status; t_message = msg; }
 void clear_error() { t_status = FT_B200_OK; t_message.clear(); }
 void count_launch(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
@@ -922,6 +925,12 @@ void ft_execute_disk_hi2lo(const ft_rotation_plan * RP, double * A, double *, co
 void ft_execute_disk_lo2hi(const ft_rotation_plan * RP, double * A, double *, const int M) { rotations_host(RP, false, A, M, DISK); }
 void ft_execute_rectdisk_hi2lo(const ft_rotation_plan * RP, double * A, double *, const int M) { rotations_host(RP, true, A, M, RECT); }
 void ft_execute_rectdisk_lo2hi(const ft_rotation_plan * RP, double * A, double *, const int M) { rotations_host(RP, false, A, M, RECT); }
+// src/drivers.c:56: the reference's OpenMP thread count; here the threads that build plans (the
+// transforms run on the GPU).  n < 1 restores the default.
+void ft_set_num_threads(const int n) { g_host_threads.store(n > 0 ? std::min(n, 256) : 0, std::memory_order_relaxed); }
+// src/fftw.c:62-64: FFTW's threading set-up; the grids here use cuFFT, so these only succeed.
+int ft_fftw_init_threads(void) { return 1; }
+void ft_fftw_plan_with_nthreads(const int) {}
 void ft_execute_sphv_hi2lo(const ft_rotation_plan * RP, double * A, double *, const int M) { rotations_sphv_host(RP, true, A, M); }
 void ft_execute_sphv_lo2hi(const ft_rotation_plan * RP, double * A, double *, const int M) { rotations_sphv_host(RP, false, A, M); }
 

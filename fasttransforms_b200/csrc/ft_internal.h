@@ -285,6 +285,8 @@ int mixed_trmm_device_error(void * p);
 void set_error(int status, const std::string & msg);
 void clear_error();
 void count_launch(unsigned long long n = 1);
+// host threads for plan construction: the value of ft_set_num_threads, 0 when it was not called
+int host_threads();
 // column.cu: one column's sweeps (kinds SPH, TRI, DISK, RECT, and SPIN for a spin column's first
 // stage with its table at k + j n + d |s| n) on device memory of len entries (double2 if cplx)
 int column_touched(int kind, int n, bool hi2lo, int m1, int m2, int d);

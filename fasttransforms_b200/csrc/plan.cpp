@@ -151,7 +151,8 @@ double * eigenvectors(const Banded & A, const Banded & B, const std::vector<ld> 
         for (int i = 0; i <= j; i++) out[i] = (double) v[i];
     };
     if (n > 0) V[0] = (double) diag[0];
-    unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    const int set = host_threads();   // ft_set_num_threads, 0: unset
+    unsigned nt = set > 0 ? (unsigned) set : std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
     if (n < 256) nt = 1;
     std::vector<std::thread> pool;
     for (unsigned w = 0; w < nt; w++)

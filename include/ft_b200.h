@@ -286,6 +286,14 @@ ft_rotation_plan * ft_plan_rotdisk(const int n, const double alpha, const double
 ft_rotation_plan * ft_plan_rotannulus(const int n, const double alpha, const double beta, const double gamma, const double rho);
 /* replaces ft_plan_rotrectdisk, src/rotations.c:270-287 */
 ft_rotation_plan * ft_plan_rotrectdisk(const int n, const double beta);
+/* replaces ft_set_num_threads, src/drivers.c:56: the reference's OpenMP thread count; here the
+ * host threads that build plans (n < 1: the default, the hardware threads up to 32). */
+void ft_set_num_threads(const int n);
+/* replace ft_fftw_init_threads / ft_fftw_plan_with_nthreads, src/fftw.c:62-64: FFTW's threading
+ * set-up; the grid plans here run on cuFFT, so the first returns 1 (success) and the second does
+ * nothing. */
+int ft_fftw_init_threads(void);
+void ft_fftw_plan_with_nthreads(const int n);
 /* replaces ft_destroy_rotation_plan, src/rotations.c:6-10 */
 void ft_destroy_rotation_plan(ft_rotation_plan * RP);
 /* replace ft_execute_{sph,tri,disk}_{hi2lo,lo2hi}, src/drivers.c:58-92, 278-312, 378-412.

@@ -75,6 +75,16 @@ def test_grid_plan_host_checks():
     assert L.ft_b200_execute_spinsph_grid_dev(None, 0, b"N", None, 8, 15, None) == 1
 
 
+def test_thread_settings():
+    """ft_set_num_threads (plan-building threads) and the FFTW threading calls take any value."""
+    import fasttransforms_b200 as ft
+    for n in (4, 0, -1, 1000):
+        ft.lib.ft_set_num_threads(n)
+    assert ft.lib.ft_fftw_init_threads() == 1
+    ft.lib.ft_fftw_plan_with_nthreads(8)
+    ft.lib.ft_set_num_threads(0)
+
+
 @pytest.mark.parametrize("src", ["dropin.c", "families.c"])
 def test_c_caller_compiles_links_and_runs(tmp_path, src):
     """C programs written against the reference's API (tests/c/dropin.c: sph2fourier;
