@@ -133,6 +133,12 @@ def _load() -> C.CDLL:
         "ft_kernel_spinsph_hi2lo": (None, [vp, i, dp, i]), "ft_kernel_spinsph_lo2hi": (None, [vp, i, dp, i]),
         "ft_kernel_tet_hi2lo": (None, [vp, i, i, dp]), "ft_kernel_tet_lo2hi": (None, [vp, i, i, dp]),
         "ft_set_num_threads": (None, [i]), "ft_fftw_init_threads": (i, []), "ft_fftw_plan_with_nthreads": (None, [i]),
+        "ft_plan_sph_with_kind": (vp, [i, i, C.POINTER(i), C.c_uint]), "ft_plan_disk_with_kind": (vp, [i, i, C.POINTER(i), C.c_uint]),
+        "ft_plan_tri_with_kind": (vp, [i, i, i, i, C.c_uint]),
+        "ft_plan_annulus_with_kind": (vp, [i, i, d, C.POINTER(i), C.c_uint]),
+        "ft_plan_rectdisk_with_kind": (vp, [i, i, C.POINTER(i), C.c_uint]),
+        "ft_plan_tet_with_kind": (vp, [i, i, i, i, i, i, C.c_uint]),
+        "ft_plan_spinsph_with_kind": (vp, [i, i, i, C.POINTER(i), i, C.c_uint]),
     }
     for name in ("sph_synthesis", "sph_analysis", "sphv_synthesis", "sphv_analysis", "disk_synthesis", "disk_analysis",
                  "tri_synthesis", "tri_analysis", "annulus_synthesis", "annulus_analysis", "rectdisk_synthesis",

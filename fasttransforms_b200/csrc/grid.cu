@@ -74,6 +74,7 @@ struct SphereGridPlan {
     int kind_rows = 0;           // rect: the kind along the rows
     double rho = 0.0;            // annulus: the radius ratio
     int spin = 0;                // spin: the plan's spin S (its parity picks the kinds and the end entries)
+    int zsign = 0;               // spin: the row DFT's sign (+1 backward, -1 forward; 0: by the kinds)
     double * d_w = nullptr;      // annulus: the N radial weights
     int device = 0;
     cufftHandle t_r2c = 0;       // length N, batch M (cosine type II)
@@ -613,7 +614,7 @@ bool merge(SphereGridPlan * P, double * X, int perm, double s, int row, int set,
 // spin: the unnormalised complex DFT along the rows, from `in` to `out` (FFTW_BACKWARD, exp(+i..),
 // for the synthesis plans; FFTW_FORWARD for the analysis plans)
 bool phi_z2z(SphereGridPlan * P, const double * in, double * out, cudaStream_t st) {
-    const int dir = is_type3(P->kind[0]) ? CUFFT_INVERSE : CUFFT_FORWARD;
+    const int dir = P->zsign ? (P->zsign > 0 ? CUFFT_INVERSE : CUFFT_FORWARD) : (is_type3(P->kind[0]) ? CUFFT_INVERSE : CUFFT_FORWARD);
     return fok(cufftSetStream(P->p_z2z, st), "cufftSetStream") &&
            fok(cufftExecZ2Z(P->p_z2z, reinterpret_cast<cufftDoubleComplex *>(const_cast<double *>(in)),
                             reinterpret_cast<cufftDoubleComplex *>(out), dir), "cufftExecZ2Z");
@@ -948,6 +949,59 @@ int ft_b200_execute_tri_grid_dev(const ft_triangle_fftw_plan * P, int analysis, 
     if (c != FT_B200_OK) return c;
     std::lock_guard<std::mutex> lk(G->mu);
     return run(G, analysis ? TRI_ANA : TRI_SYN, TRANS, dX, static_cast<cudaStream_t>(stream)) ? FT_B200_OK : ft_b200_last_status();
+}
+
+// ---------------------------------------------------------------------------
+// plans with caller-chosen kinds (src/fftw.c:76-102, 281-288, 340-347, 414-449, 534-571, 660-686,
+// 755-787).  The kinds are FFTW's r2r constants.  Accepted: the combinations this file's
+// kernels compute -- cosine and sine kinds of type II (REDFT10, RODFT10) or III (REDFT01,
+// RODFT01), one type per plan, REDFT11 as the disk's second kind, the phi kind R2HC or HC2R (which
+// of the two is not used: every plan here holds both row transforms) -- and FT_B200_EUNSUPPORTED
+// otherwise.
+// ---------------------------------------------------------------------------
+static bool theta_kind(int k) { return k == K_REDFT01 || k == K_REDFT10 || k == K_RODFT01 || k == K_RODFT10; }
+static bool kinds_ok(bool good) {
+    clear_error();
+    if (!good) set_error(FT_B200_EUNSUPPORTED, "transform kinds not supported by these grid plans");
+    return good;
+}
+static bool phi_kind(int k) { return k == 0 || k == 1; }   // FFTW_R2HC, FFTW_HC2R
+
+ft_sphere_fftw_plan * ft_plan_sph_with_kind(const int N, const int M, const int kind[3][1], const unsigned) {
+    if (!kind || !kinds_ok(theta_kind(kind[0][0]) && theta_kind(kind[1][0]) && is_type3(kind[0][0]) == is_type3(kind[1][0]) &&
+                           phi_kind(kind[2][0]))) return nullptr;
+    return reinterpret_cast<ft_sphere_fftw_plan *>(make_plan(N, M, kind[0][0], kind[1][0]));
+}
+ft_disk_fftw_plan * ft_plan_disk_with_kind(const int N, const int M, const int kind[3][1], const unsigned) {
+    if (!kind || !kinds_ok(theta_kind(kind[0][0]) && kind[1][0] == K_REDFT11 && phi_kind(kind[2][0]))) return nullptr;
+    return reinterpret_cast<ft_disk_fftw_plan *>(make_plan(N, M, kind[0][0], K_REDFT11, F_DISK));
+}
+ft_triangle_fftw_plan * ft_plan_tri_with_kind(const int N, const int M, const int kind0, const int kind1, const unsigned) {
+    if (!kinds_ok(kind0 == kind1 && (kind0 == K_REDFT01 || kind0 == K_REDFT10))) return nullptr;
+    return reinterpret_cast<ft_triangle_fftw_plan *>(make_plan(N, M, kind0, kind0, F_TRI));
+}
+ft_annulus_fftw_plan * ft_plan_annulus_with_kind(const int N, const int M, const double rho, const int kind[2][1], const unsigned) {
+    if (!kind || !kinds_ok((kind[0][0] == K_REDFT01 || kind[0][0] == K_REDFT10) && phi_kind(kind[1][0]))) return nullptr;
+    return reinterpret_cast<ft_annulus_fftw_plan *>(make_plan(N, M, kind[0][0], kind[0][0], F_ANN, 0, rho));
+}
+ft_rectdisk_fftw_plan * ft_plan_rectdisk_with_kind(const int N, const int M, const int kind[3][1], const unsigned) {
+    if (!kind || !kinds_ok(theta_kind(kind[0][0]) && theta_kind(kind[1][0]) && theta_kind(kind[2][0]) &&
+                           is_type3(kind[0][0]) == is_type3(kind[1][0]) && is_type3(kind[0][0]) == is_type3(kind[2][0])))
+        return nullptr;
+    return reinterpret_cast<ft_rectdisk_fftw_plan *>(make_plan(N, M, kind[0][0], kind[1][0], F_RECT, kind[2][0]));
+}
+ft_tetrahedron_fftw_plan * ft_plan_tet_with_kind(const int N, const int L, const int M, const int kind0, const int kind1, const int kind2,
+                                                 const unsigned) {
+    if (!kinds_ok(kind0 == kind1 && kind1 == kind2 && (kind0 == K_REDFT01 || kind0 == K_REDFT10))) return nullptr;
+    return tet_grid_plan(N, L, M, kind0);
+}
+ft_spinsphere_fftw_plan * ft_plan_spinsph_with_kind(const int N, const int M, const int S, const int kind[2][1], const int sign,
+                                                    const unsigned) {
+    if (!kind || !kinds_ok(theta_kind(kind[0][0]) && theta_kind(kind[1][0]) && is_type3(kind[0][0]) == is_type3(kind[1][0]) &&
+                           (sign == 1 || sign == -1))) return nullptr;
+    SphereGridPlan * P = make_plan(N, M, kind[0][0], kind[1][0], F_SPIN);
+    if (P) { P->spin = S; P->zsign = sign; }
+    return reinterpret_cast<ft_spinsphere_fftw_plan *>(P);
 }
 
 // the spin-weighted sphere's grids (src/fftw.c:743-960): kinds by the parity of S

@@ -274,6 +274,24 @@ int ft_get_spin_spinsphere_fftw_plan(const ft_spinsphere_fftw_plan * P);
 void ft_execute_spinsph_synthesis(const char TRANS, const ft_spinsphere_fftw_plan * P, ft_complex * X, const int N, const int M);
 void ft_execute_spinsph_analysis(const char TRANS, const ft_spinsphere_fftw_plan * P, ft_complex * X, const int N, const int M);
 
+/* Grid plans with caller-chosen kinds (replace ft_plan_{sph,disk,tri,annulus,rectdisk,tet,spinsph}_
+ * with_kind, src/fftw.c:76-102, 414-449, 281-288, 534-571, 660-686, 340-347, 755-787).  The kinds
+ * are FFTW's r2r constants (fftw3.h: R2HC 0, HC2R 1, REDFT01 4, REDFT10 5, REDFT11 6, RODFT01 8,
+ * RODFT10 9), passed as int.  Accepted: cosine and sine kinds of one type per plan (II: REDFT10 /
+ * RODFT10, III: REDFT01 / RODFT01), REDFT11 as the disk's second kind, a cosine kind for the
+ * triangle, annulus and tetrahedron (one kind for all their dimensions), R2HC or HC2R for the sphere's,
+ * disk's and annulus's phi kind, sign +1 or -1 for the spin grid's row DFT.  Other combinations
+ * return NULL with FT_B200_EUNSUPPORTED. */
+ft_sphere_fftw_plan * ft_plan_sph_with_kind(const int N, const int M, const int kind[3][1], const unsigned flags);
+ft_disk_fftw_plan * ft_plan_disk_with_kind(const int N, const int M, const int kind[3][1], const unsigned flags);
+ft_triangle_fftw_plan * ft_plan_tri_with_kind(const int N, const int M, const int kind0, const int kind1, const unsigned flags);
+ft_annulus_fftw_plan * ft_plan_annulus_with_kind(const int N, const int M, const double rho, const int kind[2][1], const unsigned flags);
+ft_rectdisk_fftw_plan * ft_plan_rectdisk_with_kind(const int N, const int M, const int kind[3][1], const unsigned flags);
+ft_tetrahedron_fftw_plan * ft_plan_tet_with_kind(const int N, const int L, const int M, const int kind0, const int kind1, const int kind2,
+                                                 const unsigned flags);
+ft_spinsphere_fftw_plan * ft_plan_spinsph_with_kind(const int N, const int M, const int S, const int kind[2][1], const int sign,
+                                                    const unsigned flags);
+
 /* Rotation level. */
 /* replaces ft_plan_rotsphere, src/rotations.c:116-133 */
 ft_rotation_plan * ft_plan_rotsphere(const int n);

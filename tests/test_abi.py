@@ -75,6 +75,38 @@ def test_grid_plan_host_checks():
     assert L.ft_b200_execute_spinsph_grid_dev(None, 0, b"N", None, 8, 15, None) == 1
 
 
+def test_grid_plans_with_kind_check_their_kinds():
+    """ft_plan_*_with_kind accept the kind combinations the grid kernels compute and return NULL
+    with FT_B200_EUNSUPPORTED (status 6) for others, before any device work; an
+    accepted combination goes on to the device (ENODEV without one, or a plan)."""
+    import fasttransforms_b200 as ft
+    L = ft.lib
+    K = lambda *k: (C.c_int * len(k))(*k)
+    R2HC, HC2R, RE01, RE10, RE11, RO01, RO10, RE00 = 0, 1, 4, 5, 6, 8, 9, 3
+    bad = [lambda: L.ft_plan_sph_with_kind(8, 15, K(RE01, RO10, HC2R), 0),      # mixed types
+           lambda: L.ft_plan_sph_with_kind(8, 15, K(RE00, RO01, HC2R), 0),      # a kind not computed here
+           lambda: L.ft_plan_disk_with_kind(8, 29, K(RE01, RE01, HC2R), 0),     # the disk's second kind is REDFT11
+           lambda: L.ft_plan_tri_with_kind(8, 8, RE01, RE10, 0),
+           lambda: L.ft_plan_annulus_with_kind(8, 29, 0.5, K(RO01, HC2R), 0),
+           lambda: L.ft_plan_rectdisk_with_kind(8, 8, K(RE01, RO10, RE01), 0),
+           lambda: L.ft_plan_tet_with_kind(4, 4, 4, RE01, RE01, RE10, 0),
+           lambda: L.ft_plan_spinsph_with_kind(8, 15, 1, K(RO01, RE01), 2, 0)]   # sign must be +-1
+    for b in bad:
+        assert not b()
+        assert L.ft_b200_last_status() == 6
+    good = [(lambda: L.ft_plan_sph_with_kind(8, 15, K(RE01, RO01, HC2R), 0), L.ft_destroy_sphere_fftw_plan),
+            (lambda: L.ft_plan_disk_with_kind(8, 29, K(RE10, RE11, R2HC), 0), L.ft_destroy_disk_fftw_plan),
+            (lambda: L.ft_plan_tri_with_kind(8, 8, RE10, RE10, 0), L.ft_destroy_triangle_fftw_plan),
+            (lambda: L.ft_plan_spinsph_with_kind(8, 15, 1, K(RO01, RE01), 1, 0), L.ft_destroy_spinsphere_fftw_plan)]
+    for g, destroy in good:
+        p = g()
+        if has_gpu():
+            assert p
+            destroy(p)
+        else:
+            assert not p and L.ft_b200_last_status() in (2, 4)
+
+
 def test_thread_settings():
     """ft_set_num_threads (plan-building threads) and the FFTW threading calls take any value."""
     import fasttransforms_b200 as ft
