@@ -9,9 +9,9 @@ strided ones untouched), more than one chunk of 1024 sweeps, and a column past t
 size.  Consistency with the matrix form: the column kernel from order m down to m mod 2 on a
 matrix's columns equals ft_execute_*_hi2lo on that matrix.
 
-The device path has not yet run on a B200, so the module is skipped; a line-by-line port of its
-schedule and index arithmetic matched the oracle bit for bit on the CPU.  The skip is lifted once
-these tests pass on the GPU."""
+The device path has not yet run on a B200, so the module is skipped; its schedule and index
+arithmetic match the oracle bit for bit on the CPU in tests/test_device_schedules.py.  The skip
+is lifted once these tests pass on the GPU."""
 import numpy as np
 import pytest
 

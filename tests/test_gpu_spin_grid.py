@@ -8,8 +8,8 @@ test (test/test_fftw.c:481-516) with every stage on the GPU: spinsph2fourier, sy
 analysis, fourier2spinsph in 'N' then 'T' return the input within 4 sqrt(N) eps and 2N eps.
 
 The device path has not yet run on a B200, so the module is skipped; its host sequence and
-index maps were checked against the oracle on the CPU.  The skip is lifted once these tests
-pass on the GPU."""
+index maps are checked against the oracle on the CPU in tests/test_device_schedules.py.  The
+skip is lifted once these tests pass on the GPU."""
 import numpy as np
 import pytest
 
