@@ -49,9 +49,13 @@ __device__ __host__ inline ColumnGeo column_geo(int kind) {
     return g;
 }
 
-// first sweep's order and the number of sweeps
-__device__ __host__ inline int column_sweeps(int kind, bool hi2lo, int m1, int m2, int * j0) {
+// first sweep's order and the number of sweeps.  Sweeps of order j >= 2n + 2 have no rotation
+// in any kind, so m2 is first brought below 2n + 4 + st with its residue mod st kept (the sweeps
+// dropped are empty ones, the others keep their orders).
+__device__ __host__ inline int column_sweeps(int kind, bool hi2lo, int m1, int m2, int n, int * j0) {
     const ColumnGeo g = column_geo(kind);
+    const long long cap = 2LL * n + 4;
+    if (m2 > cap) m2 = (int) (m2 - (((long long) m2 - cap) / g.st) * g.st);
     if (hi2lo) {
         *j0 = m2 - g.st;
         return *j0 >= m1 ? (*j0 - m1) / g.st + 1 : 0;
@@ -89,7 +93,7 @@ __global__ void __launch_bounds__(1024) column_kernel(E * a, const double2 * __r
     const int D = HI2LO ? 1 : g.p + 1;
     const int sgn = HI2LO ? -1 : 1;   // direction of the sweep order
     int j0 = 0;
-    const int T = column_sweeps(kind, HI2LO, m1, m2, &j0);
+    const int T = column_sweeps(kind, HI2LO, m1, m2, n, &j0);
     const int B = blockDim.x, u = threadIdx.x;
     for (int t0 = 0; t0 < T; t0 += B) {
         const int nb = min(B, T - t0);
@@ -161,7 +165,7 @@ constexpr size_t kColumnSmemMax = 200 * 1024;
 int column_touched(int kind, int n, bool hi2lo, int m1, int m2, int d) {
     const ColumnGeo g = column_geo(kind);
     int j0 = 0;
-    const int T = column_sweeps(kind, hi2lo, m1, m2, &j0);
+    const int T = column_sweeps(kind, hi2lo, m1, m2, n, &j0);
     int len = 0;
     for (int t = 0; t < T; t += std::max(T - 1, 1)) {   // K(j) is monotone in j: its largest value is at an end
         const int j = hi2lo ? j0 - g.st * t : j0 + g.st * t;
@@ -176,7 +180,7 @@ int column_touched(int kind, int n, bool hi2lo, int m1, int m2, int d) {
 bool column_sweeps_dev(void * dcol, bool cplx, const double2 * tab, int kind, int n, int m1, int m2, bool hi2lo, bool fwd, int d,
                        int as, int len) {
     int j0 = 0;
-    const int T = column_sweeps(kind, hi2lo, m1, m2, &j0);
+    const int T = column_sweeps(kind, hi2lo, m1, m2, n, &j0);
     if (T == 0 || len == 0) return true;
     const int threads = std::min(1024, (T + 31) / 32 * 32);
     const size_t bytes = (cplx ? sizeof(double2) : sizeof(double)) * (size_t) len;

@@ -370,6 +370,7 @@ void spin_column_host(const ft_spin_rotation_plan * Pp, bool hi2lo, int m, ft_co
     SpinRotPlan * P = as_srp(Pp);
     if (!P || !A) { set_error(FT_B200_EINVAL, "NULL or foreign argument"); return; }
     if (S < 1) { set_error(FT_B200_EINVAL, "S must be >= 1"); return; }
+    if (m < -(1 << 30) || m > (1 << 30)) { set_error(FT_B200_EINVAL, "order m out of range"); return; }
     const int n = P->n, as = std::abs(P->s), am = std::abs(m);
     const int d = std::abs(am - as), mn = std::min(am, as), par = (am + as) % 2;
     const bool fwd1 = hi2lo == ((long long) m * P->s >= 0);

@@ -44,8 +44,11 @@ def _base(kind, n, j, d=0, a_s=0):
     return _cdiv(j * (2 * n + 1 - j), 2)
 
 
-def _sweeps(kind, hi, m1, m2):
+def _sweeps(kind, hi, m1, m2, n):
     st = _geo(kind)[1]
+    cap = 2 * n + 4   # orders j >= 2n + 2 have no rotation: m2 brought below cap + st, residue kept
+    if m2 > cap:
+        m2 -= ((m2 - cap) // st) * st
     if hi:
         j0 = m2 - st
         return j0, (_cdiv(j0 - m1, st) + 1 if j0 >= m1 else 0)
@@ -57,7 +60,7 @@ def wavefront(col, s_tab, c_tab, kind, n, m1, m2, hi, fwd, B, d=0, a_s=0):
     col = col.copy()
     p, st = _geo(kind)
     D, sgn = (1, -1) if hi else (p + 1, 1)
-    j0, T = _sweeps(kind, hi, m1, m2)
+    j0, T = _sweeps(kind, hi, m1, m2, n)
     for t0 in range(0, T, B):
         nb = min(B, T - t0)
         kmax = max(_top(kind, n, j0 + sgn * st * t0, d), _top(kind, n, j0 + sgn * st * (t0 + nb - 1), d))
@@ -96,14 +99,15 @@ def test_column_wavefront_is_the_sequential_order(O, name, kind, kw, n):
     s_tab, c_tab = O.tables(P)
     rng = np.random.default_rng(n + kind)
     mmax = 2 * n + 1 if kind == DISK else n + 2
-    for m2 in range(mmax + 1):
-        for m1 in range(m2 + 2):
-            col = rng.uniform(-1, 1, n)
-            for hi in (True, False):
-                want = O.kernel(P, hi, m1, m2, col.copy())
-                for B in (1, 3, 32):
-                    got = wavefront(col, s_tab, c_tab, kind, n, m1, m2, hi, hi, B)
-                    assert np.array_equal(got, want), (name, n, m1, m2, hi, B)
+    pairs = [(m1, m2) for m2 in range(mmax + 1) for m1 in range(m2 + 2)]
+    pairs += [(m1, m2) for m2 in (10 * n + 7, 10 * n + 8) for m1 in (0, 1, n // 2, 3 * n)]   # m2 past the clamp
+    for m1, m2 in pairs:
+        col = rng.uniform(-1, 1, n)
+        for hi in (True, False):
+            want = O.kernel(P, hi, m1, m2, col.copy())
+            for B in (1, 3, 32):
+                got = wavefront(col, s_tab, c_tab, kind, n, m1, m2, hi, hi, B)
+                assert np.array_equal(got, want), (name, n, m1, m2, hi, B)
     O.destroy(P)
 
 
