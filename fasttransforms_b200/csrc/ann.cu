@@ -79,26 +79,31 @@ void jacobi_tridiagonal(int m, double a, double b, double * d, double * lo, doub
     }
 }
 
-void compute_givens(double x, double y, double * c, double * s, double * r) {
+// the rotation taking (x, y) to (r, 0): r = hypot(x, y), (cos, sin) = (x, y) / r; the identity for r
+// at or below the smallest normal over the unit roundoff
+void givens_pair(double x, double y, double * cs, double * sn, double * r) {
     *r = std::hypot(x, y);
-    if (*r <= DBL_MIN / DBL_EPSILON) { *c = 1; *s = 0; }
-    else { *c = x / *r; *s = y / *r; }
+    if (*r <= DBL_MIN / DBL_EPSILON) { *cs = 1; *sn = 0; }
+    else { *cs = x / *r; *sn = y / *r; }
 }
 
-// Givens QR of the symmetric tridiagonal (a, b) of size k: rotations (c, s), R's diagonals r0, r1
-void tridiagonal_qr(int k, const double * a, const double * b, double * s, double * c, double * r0, double * r1) {
-    double r, aip1 = a[0], bip1r = b[0];
-    for (int i = 0; i < k - 2; i++) {
-        compute_givens(aip1, -b[i], c + i, s + i, &r);
-        r0[i] = r;
-        r1[i] = c[i] * bip1r - s[i] * a[i + 1];
-        aip1 = c[i] * a[i + 1] + s[i] * bip1r;
-        bip1r = c[i] * b[i + 1];
+// Givens QR of the symmetric tridiagonal T of size k (diagonal dg[0 .. k-1], off-diagonal
+// off[0 .. k-2]).  Step i rotates rows i and i + 1 so that the subdiagonal entry vanishes:
+// `pivot` is the running (i, i) entry of the partly reduced matrix and `above` its (i, i + 1)
+// entry; the step writes R's diagonal rd[i] and superdiagonal ru[i] and the rotation (cs, sn).
+// The expressions keep the reference's operation order (src/banded_source.c:1430-1455), so the
+// table built from them is bit-identical to the reference's.
+void tridiagonal_qr(int k, const double * dg, const double * off, double * sn, double * cs, double * rd, double * ru) {
+    double pivot = dg[0], above = off[0];
+    for (int i = 0; i + 1 < k; i++) {
+        double r;
+        givens_pair(pivot, -off[i], cs + i, sn + i, &r);
+        rd[i] = r;
+        ru[i] = cs[i] * above - sn[i] * dg[i + 1];
+        pivot = cs[i] * dg[i + 1] + sn[i] * above;
+        if (i + 2 < k) above = cs[i] * off[i + 1];
     }
-    compute_givens(aip1, -b[k - 2], c + k - 2, s + k - 2, &r);
-    r0[k - 2] = r;
-    r1[k - 2] = c[k - 2] * bip1r - s[k - 2] * a[k - 1];
-    r0[k - 1] = c[k - 2] * a[k - 1] + s[k - 2] * bip1r;
+    rd[k - 1] = pivot;
 }
 
 // R X R^{-1} restricted to size k - 1, from the upper-triangular R's first two diagonals

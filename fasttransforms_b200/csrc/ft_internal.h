@@ -156,7 +156,6 @@ int rotation_device_error();   // reads and clears the rotation kernel's status 
 cudaError_t launch_rotations(int kind, bool hi2lo, const RotLaunch & L, int max_ctas, cudaStream_t st,
                              double * const * dead = nullptr, RotSchedule * sched = nullptr);
 void set_rotation_config(int cfg);   // 0 .. 3 forces a configuration, -1 chooses per shape
-int rotation_ctas_per_sm(int kind);
 
 // Triangular multiplies (trmm.cu).  Out = op(U) * In on column classes.
 struct TrmmClass {

@@ -14,7 +14,9 @@
 // library holds it (kNoallocBytes + kNoallocHeader) until the process exits.
 // Host code cannot use the array's name as a device address: the address is
 // obtained once per device with cudaGetSymbolAddress, on the first call made
-// with that device current, and passed to the kernels.
+// with that device current, and passed to the kernels; it is kept for the life
+// of the process (a cudaDeviceReset, which invalidates every plan, would also
+// invalidate it).
 #include <mutex>
 
 #include "ft_internal.h"

@@ -29,8 +29,11 @@
 // With W = 8 warps every SM sub-partition holds two warps and the register
 // budget per thread is the full 255.
 //
-// No thread waits on another except through __syncthreads; there are no spin
-// loops.  Every global access is bounds-checked against the field's N, M.
+// Within a CTA no thread waits on another except through __syncthreads.  The
+// one spin loop is the pass pipeline's wait on another CTA's progress word
+// (pipelined configurations only), bounded, after which the launch records a
+// device status and every later wait gives up.  Every global access is
+// bounds-checked against the field's N, M.
 
 #include <cstdio>
 #include <cstdlib>
@@ -727,6 +730,5 @@ cudaError_t launch_rotations(int kind, bool hi2lo, const RotLaunch & L, int max_
     return launch_shape(kind, hi2lo, cfg, L, max_ctas, st, sched);
 }
 
-int rotation_ctas_per_sm(int) { return 1; }
 
 }  // namespace ftb

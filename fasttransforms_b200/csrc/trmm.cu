@@ -10,6 +10,15 @@
 // Tile: 128 x 64 outputs per CTA, 8 warps of 32 x 32, K slabs of 16 staged in
 // shared memory by a 3-deep cp.async pipeline.  Shared layouts are padded so
 // every fragment load is conflict-free.
+//
+// Summation: the accumulators sum one chunk of 256 consecutive k at a time;
+// at the end of each chunk a thread adds them into its outputs in C (which it
+// alone writes) and starts the next chunk from zero.  A single accumulation
+// over all n terms lets the rounding error grow with n; chunked sums, like a
+// BLAS's K panels, keep it near that of 256 terms plus n / 256 additions (the
+// reference's round trips, which amplify this error in the ill-conditioned
+// triangle transforms, then match its BLAS build).  C must not alias the
+// inputs (every caller multiplies out of place).
 
 #include "ft_internal.h"
 
@@ -17,6 +26,7 @@ namespace ftb {
 namespace {
 
 constexpr int BM = 128, BN = 64, BK = 16, NSTAGE = 3, NTHREADS = 256;
+constexpr int KCHUNK_SLABS = 16;   // slabs of BK summed before a partial sum is added into C
 
 __device__ __forceinline__ void cp_async16(void * smem, const void * gmem, bool valid) {
     unsigned sa = (unsigned) __cvta_generic_to_shared(smem);
@@ -52,6 +62,36 @@ struct GemmParams {
     int tiles_m, tiles_n;
     int mode;           // 0: left N (k >= i), 1: left T (k <= i), 2: right N (k <= j), 3: right T (k >= j)
 };
+
+// A thread's 32 accumulators (rows m0 + 8a, columns n0 + 8b + {0, 1}) into C:
+// C = acc (first chunk) or C + acc, then acc = 0 when more chunks follow.  All
+// loads are issued before any store, so they are in flight together.
+__device__ __forceinline__ void flush_partial(const GemmClass & C, const int m0, const int n0, double (&acc)[4][4][2],
+                                              const bool add, const bool restart) {
+    if (add) {
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const int m = m0 + a * 8;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int nn = n0 + b * 8;
+                if (m < C.mrows && nn < C.ncols) acc[a][b][0] += C.c[(long long) nn * C.c_ld + m];
+                if (m < C.mrows && nn + 1 < C.ncols) acc[a][b][1] += C.c[(long long) (nn + 1) * C.c_ld + m];
+            }
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int m = m0 + a * 8;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int nn = n0 + b * 8;
+            if (m < C.mrows && nn < C.ncols) C.c[(long long) nn * C.c_ld + m] = acc[a][b][0];
+            if (m < C.mrows && nn + 1 < C.ncols) C.c[(long long) (nn + 1) * C.c_ld + m] = acc[a][b][1];
+            if (restart) acc[a][b][0] = acc[a][b][1] = 0.0;
+        }
+    }
+}
 
 // One 128 x 64 output tile of class C: rows [tm*BM, ...), columns [tn*BN, ...).
 template <bool A_MC, bool B_KC, bool VEC16>
@@ -139,6 +179,7 @@ __device__ __forceinline__ void tri_tile(const GemmClass & C, const int n, const
     for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+    bool flushed = false;   // C holds the sum of the chunks before the current one
 
 #pragma unroll
     for (int s = 0; s < NSTAGE - 1; ++s) {
@@ -174,21 +215,15 @@ __device__ __forceinline__ void tri_tile(const GemmClass & C, const int n, const
 #pragma unroll
                 for (int b = 0; b < 4; ++b) dmma(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
         }
+        if ((slab + 1) % KCHUNK_SLABS == 0 && slab + 1 < nslab) {   // end of a chunk: into C, restart from zero
+            flush_partial(C, i0 + wm + fr, j0 + wn + fc * 2, acc, flushed, true);
+            flushed = true;
+        }
     }
     cp_wait<0>();
 
-    // epilogue: C(m, n) at c[n * c_ld + m]
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-        const int m = i0 + wm + a * 8 + fr;
-        if (m >= C.mrows) continue;
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            const int nn = j0 + wn + b * 8 + fc * 2;
-            if (nn < C.ncols) C.c[(long long) nn * C.c_ld + m] = acc[a][b][0];
-            if (nn + 1 < C.ncols) C.c[(long long) (nn + 1) * C.c_ld + m] = acc[a][b][1];
-        }
-    }
+    // epilogue: C(m, n) at c[n * c_ld + m] (plus the earlier chunks' sum)
+    flush_partial(C, i0 + wm + fr, j0 + wn + fc * 2, acc, flushed, false);
 }
 
 template <bool A_MC, bool B_KC, bool VEC16>

@@ -422,7 +422,9 @@ int ft_b200_execute_batched_dev(const ft_harmonic_plan * const * plans, int forw
  *     FT_B200_EUNSUPPORTED, since their task list would have to be allocated.
  *   - The first call on a device looks up the array's device address
  *     (cudaGetSymbolAddress) with that device current; make that first call
- *     before any stream capture.
+ *     before any stream capture.  The address is kept for the life of the
+ *     process, so do not use this entry point across a cudaDeviceReset (which
+ *     also invalidates every plan made before it).
  *   - All calls share the one array, which keeps the last call's contents; the
  *     work counter is cleared by every call.  Calls that overlap on the GPU
  *     (concurrent streams, or several host threads) race on the array and must

@@ -117,12 +117,9 @@ def test_thread_settings():
     ft.lib.ft_set_num_threads(0)
 
 
-@pytest.mark.parametrize("src", ["dropin.c", "families.c"])
-def test_c_caller_compiles_links_and_runs(tmp_path, src):
-    """C programs written against the reference's API (tests/c/dropin.c: sph2fourier;
-    tests/c/families.c: every other family and the grids) compile as C99 with -Wall -Werror
-    against include/ft_b200.h, link with -lft_b200 and run: without a usable device they report
-    FT_B200_ENODEV cleanly; with one, their round trips pass."""
+def _run_c_caller(tmp_path, src):
+    """Compile tests/c/<src> as C99 with -Wall -Werror against include/ft_b200.h, link it with
+    -lft_b200 and run it; returns the completed process."""
     import shutil
     import subprocess
     import fasttransforms_b200 as ft
@@ -133,13 +130,29 @@ def test_c_caller_compiles_links_and_runs(tmp_path, src):
     exe = str(tmp_path / src[:-2])
     subprocess.run([cc, "-O2", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "c", src),
                     "-L", libdir, "-lft_b200", "-Wl,-rpath," + libdir, "-lm", "-o", exe], check=True)
-    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    return subprocess.run([exe], capture_output=True, text=True, timeout=300)
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-device path; the device run is the gpu-marked twin")
+@pytest.mark.parametrize("src", ["dropin.c", "families.c"])
+def test_c_caller_compiles_links_and_runs(tmp_path, src):
+    """C programs written against the reference's API (tests/c/dropin.c: sph2fourier;
+    tests/c/families.c: every other family and the grids) compile, link and, without a usable
+    device, report FT_B200_ENODEV cleanly."""
+    r = _run_c_caller(tmp_path, src)
     assert r.returncode == 0, r.stderr
-    if has_gpu():
-        out = r.stdout.strip()
-        assert out == "ok" or float(out) < 1e-13, out
-    else:
-        assert r.stdout.strip() == "ENODEV"
+    assert r.stdout.strip() == "ENODEV"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("src", ["dropin.c", "families.c"])
+def test_c_caller_round_trips_on_device(tmp_path, src):
+    """The same C programs on an sm_100 device: every transform they call returns its input
+    (dropin.c prints the sph2fourier round-trip error, below 1e-13; families.c prints "ok")."""
+    r = _run_c_caller(tmp_path, src)
+    assert r.returncode == 0, r.stderr
+    out = r.stdout.strip()
+    assert out == "ok" or float(out) < 1e-13, out
 
 
 def _prototypes():

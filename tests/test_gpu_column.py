@@ -7,15 +7,12 @@ lo2hi, pinned to the compiled reference in tests/test_oracle_pin.py) in its fuse
 bit: every family, orders m1 <= m2 of both parities, strides 1 and 3 (the entries between the
 strided ones untouched), more than one chunk of 1024 sweeps, and a column past the shared-memory
 size.  Consistency with the matrix form: the column kernel from order m down to m mod 2 on a
-matrix's columns equals ft_execute_*_hi2lo on that matrix.
-
-The device path has not yet run on a B200, so the module is skipped; its schedule and index
-arithmetic match the oracle bit for bit on the CPU in tests/test_device_schedules.py.  The skip
-is lifted once these tests pass on the GPU."""
+matrix's columns equals ft_execute_*_hi2lo on that matrix.  The schedule and index arithmetic
+are also restated on the CPU in tests/test_device_schedules.py."""
 import numpy as np
 import pytest
 
-pytestmark = [pytest.mark.gpu, pytest.mark.skip(reason="column kernel not yet run on a B200")]
+pytestmark = pytest.mark.gpu
 
 FAMILIES = {"sph": (), "tri": (0.0, -0.5, 0.25), "disk": (0.5, -0.25), "rect": (0.5,)}
 
@@ -70,10 +67,18 @@ def test_column_vs_oracle_bit_exact(env, fam, n):
 @pytest.mark.parametrize("fam,n", [("sph", 2600), ("tri", 1500), ("disk", 1100), ("sph", 25700)])
 def test_long_columns_bit_exact(env, fam, n):
     """More than 1024 sweeps (several chunks), and (n = 25700, m1 = m2 mod 2) a column longer
-    than the shared-memory column of 25600 entries, kept in global memory."""
+    than the shared-memory column of 25600 entries, kept in global memory.
+
+    The reference's sph table multiplies in int (src/rotations.c:122-124, den = (l + 2m + 3)
+    (l + 2m + 4)), which overflows once l + 2m + 4 > 46340; the oracle restates that, while this
+    library multiplies in 64 bits.  The sweeps compared therefore stay below that: for the long
+    column the highest order is capped so that n + m2 + 1 <= 46340 (its column still spans
+    n - 1 entries)."""
     ft, O = env
     RP, Po = plans(ft, O, fam, n)
     m2 = 2 * n - 2 if fam == "disk" else n - 1
+    if fam == "sph":
+        m2 = min(m2, 46340 - n - 1)
     A = np.random.default_rng(1).uniform(-1, 1, n)
     for m1 in (m2 % 2, m2 - 40):
         for hi2lo in (True, False):
@@ -131,7 +136,7 @@ def test_spin_column_vs_oracle_bit_exact(env, n, s):
     ft, O = env
     SRP = ft.plan_rotspinsphere(n, s)
     P = O.spin_plan(n, s, connections=False)
-    rng = np.random.default_rng(n + 10 * s)
+    rng = np.random.default_rng(n + 10 * (s + 5))
     for m in range(-(n + 1), n + 2):
         for S in (1, 2):
             A = rng.uniform(-1, 1, n * S) + 1j * rng.uniform(-1, 1, n * S)

@@ -1,0 +1,114 @@
+"""FP64 parity at the benchmarked sizes: the GPU's transforms against the reference library
+compiled from its own sources (oracle/_ref/libft_ref.so), on the same seeded inputs, through
+the C ABI.
+
+* sph at degrees 255, 1023 and 4095 (n = 256, 1024, 4096; M = 2n - 1); tri with
+  (alpha, beta, gamma) = (0, 0, 0) and (-1/2, -1/2, -1/2) and disk with (alpha, beta) = (0, 0) at
+  n = 1024 and 2048: forward and backward, 'N' and 'T', each against the reference's output for
+  the same input; the bar is a relative 2-norm of 1e-14 (the rotation stage is bit-identical to
+  the oracle, the plans' connection matrices are the reference's bit for bit, and only the
+  triangular multiplies sum in another order).
+* The reference's own accuracy test (test/test_drivers.c:226-250 for sph, and the tri / disk
+  tests of the same file) at n = 64 * 2^i + J for the sizes above: sph2fourier and fourier2sph
+  'N' then 'T' return the input within its bounds (4 sqrt(N) eps / 2N eps sph, 32 sqrt(N) eps /
+  8N eps tri, 8 sqrt(N) eps / 4N eps disk), or within twice the reference's own round-trip error
+  for the same input where the reference itself exceeds them.
+"""
+import numpy as np
+import pytest
+
+from conftest import EPS, rel2, relinf
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"sph": (4, 2), "tri": (32, 8), "disk": (8, 4)}
+
+CASES = [("sph", (), 256), ("sph", (), 1024), ("sph", (), 4096),
+         ("tri", (0.0, 0.0, 0.0), 1024), ("tri", (-0.5, -0.5, -0.5), 1024), ("disk", (0.0, 0.0), 1024),
+         ("tri", (0.0, 0.0, 0.0), 2048), ("tri", (-0.5, -0.5, -0.5), 2048), ("disk", (0.0, 0.0), 2048)]
+
+
+def _id(c):
+    kind, params, n = c
+    return f"{kind}{''.join('%+.1f' % p for p in params)}-n{n}"
+
+
+@pytest.fixture(scope="module")
+def env():
+    import torch
+    import fasttransforms_b200 as ft
+    from oracle.bind import Reference
+    if not Reference.available():
+        pytest.fail("the compiled reference (oracle/_ref/libft_ref.so) is missing: run __graft_entry__.build()")
+    torch.cuda.set_device(0)
+    return ft, torch, Reference()
+
+
+def _gpu_plan(ft, kind, n, params):
+    return {"sph": ft.plan_sph2fourier, "tri": ft.plan_tri2cheb, "disk": ft.plan_disk2cxf}[kind](n, *params)
+
+
+def _dev(torch, A):
+    return torch.from_numpy(np.asfortranarray(A).ravel(order="F").copy()).cuda()
+
+
+def _host(t, n, M):
+    return t.cpu().numpy().reshape((n, M), order="F")
+
+
+@pytest.mark.parametrize("case", CASES, ids=[_id(c) for c in CASES])
+def test_transforms_vs_compiled_reference(env, case):
+    ft, torch, R = env
+    kind, params, n = case
+    A = ft.rand_layout(kind, n, 20261203)
+    M = A.shape[1]
+    P = _gpu_plan(ft, kind, n, params)
+    RP = R.plan(kind, n, *params)
+    stream = torch.cuda.current_stream().cuda_stream
+    errs = {}
+    try:
+        for fwd in (True, False):
+            for tr in "NT":
+                d = _dev(torch, A)
+                ft.execute_dev(P, fwd, tr, d.data_ptr(), n, M, stream)
+                got = _host(d, n, M)
+                ref = A.copy(order="F")
+                R.execute(kind, RP, fwd, tr, ref)
+                errs[("fwd" if fwd else "bwd") + tr] = (rel2(got, ref), relinf(got, ref))
+    finally:
+        R.destroy(RP)
+        P.close()
+    print(f"\n{_id(case)} vs reference (rel2, relinf): " + ", ".join(f"{k} {a:.2e} {b:.2e}" for k, (a, b) in errs.items()))
+    for k, (e2, _) in errs.items():
+        assert e2 <= 1e-14, (k, e2)
+
+
+RT_CASES = [("sph", (), 1024), ("sph", (), 2049), ("tri", (0.0, 0.0, 0.0), 1024), ("tri", (-0.5, -0.5, -0.5), 2048),
+            ("disk", (0.0, 0.0), 1025), ("disk", (0.0, 0.0), 2048)]
+
+
+@pytest.mark.parametrize("case", RT_CASES, ids=[_id(c) for c in RT_CASES])
+def test_reference_accuracy_test_at_scale(env, case):
+    """test/test_drivers.c's sequence: forward 'N', backward 'N', forward 'T', backward 'T'."""
+    ft, torch, R = env
+    kind, params, n = case
+    A = ft.rand_layout(kind, n, 7)
+    M = A.shape[1]
+    P = _gpu_plan(ft, kind, n, params)
+    stream = torch.cuda.current_stream().cuda_stream
+    seq = ((True, "N"), (False, "N"), (True, "T"), (False, "T"))
+    d = _dev(torch, A)
+    for fwd, tr in seq:
+        ft.execute_dev(P, fwd, tr, d.data_ptr(), n, M, stream)
+    got = _host(d, n, M)
+    P.close()
+    ref = A.copy(order="F")
+    RP = R.plan(kind, n, *params)
+    for fwd, tr in seq:
+        R.execute(kind, RP, fwd, tr, ref)
+    R.destroy(RP)
+    c2, ci = TOL[kind]
+    print(f"\n{_id(case)} round trip: GPU {rel2(got, A):.2e} / {relinf(got, A):.2e}, "
+          f"reference {rel2(ref, A):.2e} / {relinf(ref, A):.2e}, bounds {c2 * np.sqrt(n) * EPS:.2e} / {ci * n * EPS:.2e}")
+    assert rel2(got, A) < max(c2 * np.sqrt(n) * EPS, 2 * rel2(ref, A))
+    assert relinf(got, A) < max(ci * n * EPS, 2 * relinf(ref, A))

@@ -106,7 +106,6 @@ def test_sphv_rejects_other_families(env):
     P.close()
 
 
-@pytest.mark.skip(reason="host sphv rotation entry not yet run on a B200")
 @pytest.mark.parametrize("n", [1, 3, 4, 17, 65])
 def test_sphv_rotation_entry_points_bit_exact(env, n):
     """ft_execute_sphv_hi2lo / lo2hi (src/drivers.c:168-276) against the oracle's column loops:

@@ -5,17 +5,14 @@ Against the oracle (oracle/grid.py, pinned in tests/test_oracle_grid.py): both s
 and 'C', every plan with every sequence, spins of both parities, within 1e-14 relative 2-norm;
 other TRANS values leave the matrix untouched, as the reference's.  The reference's own accuracy
 test (test/test_fftw.c:481-516) with every stage on the GPU: spinsph2fourier, synthesis,
-analysis, fourier2spinsph in 'N' then 'T' return the input within 4 sqrt(N) eps and 2N eps.
-
-The device path has not yet run on a B200, so the module is skipped; its host sequence and
-index maps are checked against the oracle on the CPU in tests/test_device_schedules.py.  The
-skip is lifted once these tests pass on the GPU."""
+analysis, fourier2spinsph in 'N' then 'T' return the input within 4 sqrt(N) eps and 2N eps.  The host sequence and index maps are also
+restated on the CPU in tests/test_device_schedules.py."""
 import numpy as np
 import pytest
 
 from conftest import EPS, rel2
 
-pytestmark = [pytest.mark.gpu, pytest.mark.skip(reason="spin grid device path not yet run on a B200")]
+pytestmark = pytest.mark.gpu
 
 OPS = ["spinsph_synthesis", "spinsph_analysis"]
 

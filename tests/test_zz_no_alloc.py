@@ -7,12 +7,8 @@ device array inside the library instead of the plan's scratch.  This file is
 collected last, so a run that stops at the first failure has already run every
 other test; it also passes when run alone in a fresh process.
 """
-import ctypes as C
-
 import numpy as np
 import pytest
-
-from conftest import rel2
 
 pytestmark = pytest.mark.gpu
 
@@ -35,10 +31,32 @@ def test_noalloc_matches_execute_dev_twice(kind, params, n):
                 b = a.clone()
                 ft.execute_dev(plan, fwd, tr, a.data_ptr(), n, M, st)
                 ft.execute_noalloc_dev(plan, fwd, tr, b.data_ptr(), n, M, st)
-                ra = a.cpu().numpy()
-                rb = b.cpu().numpy()
-                assert rel2(rb, ra) <= 1e-14, (call, fwd, tr, rel2(rb, ra))
+                # the same kernels in the same order: bit-identical results
+                assert np.array_equal(b.cpu().numpy(), a.cpu().numpy()), (call, fwd, tr)
     plan.close()
+
+
+def test_noalloc_takes_no_device_memory():
+    """A warm call leaves the device's free memory unchanged (an allocation on this path, by the
+    library or by anything it calls, would lower it)."""
+    import torch
+    import fasttransforms_b200 as ft
+    torch.cuda.set_device(0)
+    n = 256
+    plan = ft.plan_sph2fourier(n)
+    M = plan.M
+    st = torch.cuda.current_stream().cuda_stream
+    a = torch.from_numpy(ft.rand_layout("sph", n, 5).ravel(order="F").copy()).cuda()
+    ft.execute_noalloc_dev(plan, True, "N", a.data_ptr(), n, M, st)   # first call: the per-device set-up
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for fwd in (True, False):
+        for tr in "NT":
+            ft.execute_noalloc_dev(plan, fwd, tr, a.data_ptr(), n, M, st)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    plan.close()
+    assert free1 == free0, (free0, free1)
 
 
 def test_noalloc_rejects_oversize_and_bad_arguments():
