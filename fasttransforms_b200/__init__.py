@@ -31,7 +31,7 @@ __all__ = [
     "plan_rotsphere", "plan_rottriangle", "plan_rotdisk",
     "execute_sph_hi2lo", "execute_sph_lo2hi", "execute_tri_hi2lo", "execute_tri_lo2hi",
     "execute_disk_hi2lo", "execute_disk_lo2hi",
-    "execute_dev", "execute_shared_dev", "FP64", "FP64_BLOCKED", "MIXED_BF16", "MIXED_BF16X4", "device_status", "execute_noalloc_dev", "NOALLOC_MAX_ELEMS", "execute_batched_dev", "rotations_dev", "kernel_launches", "profile", "profile_read", "set_rotation_config",
+    "execute_dev", "execute_shared_dev", "execute_shared_host", "FP64", "FP64_BLOCKED", "MIXED_BF16", "MIXED_BF16X4", "device_status", "execute_noalloc_dev", "NOALLOC_MAX_ELEMS", "execute_batched_dev", "rotations_dev", "kernel_launches", "profile", "profile_read", "set_rotation_config",
     "layout_cols", "rand_layout", "sphrand", "trirand", "diskrand",
     "SphereGridPlan", "plan_sph_synthesis", "plan_sph_analysis", "plan_sphv_synthesis", "plan_sphv_analysis",
     "execute_sph_synthesis", "execute_sph_analysis", "execute_sphv_synthesis", "execute_sphv_analysis",
@@ -90,6 +90,7 @@ def _load() -> C.CDLL:
         "ft_b200_plan_kind": (i, [vp]), "ft_b200_plan_device": (i, [vp]),
         "ft_b200_execute_noalloc_dev": (i, [vp, i, ch, vp, i, i, vp]),
         "ft_b200_execute_shared_dev": (i, [vp, i, ch, C.POINTER(vp), i, i, vp]),
+        "ft_b200_execute_shared_host": (i, [vp, i, C.POINTER(i), C.c_char_p, C.POINTER(vp), i, i]),
         "ft_b200_device_status": (i, [vp]),
         "ft_b200_profile": (i, [i]), "ft_b200_profile_read": (i, [i, C.POINTER(C.c_double), C.POINTER(i)]),
         "ft_b200_set_rotation_config": (None, [i]),
@@ -806,6 +807,34 @@ def execute_shared_dev(P: HarmonicPlan, forward: bool, trans: str, ptrs: Sequenc
     nf = len(ptrs)
     aa = (C.c_void_p * nf)(*ptrs)
     st = lib.ft_b200_execute_shared_dev(P.ptr, 1 if forward else 0, trans.encode(), aa, nf, precision, C.c_void_p(stream))
+    if st != 0:
+        _check()
+
+
+def execute_shared_host(P: HarmonicPlan, ops: Sequence[tuple], arrays: Sequence, precision: int = FP64) -> None:
+    """Host-pointer form of ``execute_shared_dev`` for a sequence of transforms.
+
+    ``ops``: (forward, trans) pairs applied in order to every field; ``arrays``:
+    N x M float64 host matrices in column-major order (numpy arrays in Fortran
+    order, or the flat buffers of page-locked tensors as integer addresses),
+    transformed in place.  Copies of one group of fields overlap the
+    transforms of the previous group (page-locked memory only); the call
+    returns when every result is back in host memory.
+    """
+    nops = len(ops)
+    fw = (C.c_int * max(nops, 1))(*[1 if f else 0 for f, _ in ops])
+    tr = "".join(t for _, t in ops).encode()
+    ptrs = []
+    for a in arrays:
+        if isinstance(a, int):
+            ptrs.append(a)
+        else:
+            if a.dtype != np.float64 or not a.flags.f_contiguous or a.shape != (P.n, P.M):
+                raise ValueError(f"each field must be a float64 Fortran-order {P.n} x {P.M} array")
+            ptrs.append(a.ctypes.data)
+    nf = len(ptrs)
+    aa = (C.c_void_p * max(nf, 1))(*ptrs)
+    st = lib.ft_b200_execute_shared_host(P.ptr, nops, fw, tr, aa, nf, precision)
     if st != 0:
         _check()
 

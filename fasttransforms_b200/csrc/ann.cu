@@ -167,7 +167,8 @@ ft_rotation_plan * annulus_rotation_plan(int n, double alpha, double beta, doubl
     annulus_table(n, alpha, beta, rho, RP->s, RP->c);
     std::vector<double2> sc(len);
     for (size_t i = 0; i < len; i++) sc[i] = make_double2(RP->s[i], RP->c[i]);
-    if (!ok(cudaMemcpy(RP->d_sc, sc.data(), sizeof(double2) * len, cudaMemcpyHostToDevice), "cudaMemcpy(table)")) {
+    if (!ok(cudaMemcpy(RP->d_sc, sc.data(), sizeof(double2) * len, cudaMemcpyHostToDevice), "cudaMemcpy(table)") ||
+        !rotation_plan_pad(RP)) {   // the padded copy the rotation kernel reads, from this table
         ft_destroy_rotation_plan(RP);
         return nullptr;
     }

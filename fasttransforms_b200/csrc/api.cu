@@ -131,7 +131,7 @@ ft_rotation_plan * make_rotation_plan(int kind, int n, double alpha, double beta
     for (long long i = 0; i < len; i++) sc[i] = make_double2(RP->s[i], RP->c[i]);
     if (!cuda_ok(cudaMalloc(&RP->d_sc, sizeof(double2) * len), "cudaMalloc(table)") ||
         !cuda_ok(cudaMemcpy(RP->d_sc, sc.data(), sizeof(double2) * len, cudaMemcpyHostToDevice), "cudaMemcpy(table)") ||
-        !cuda_ok(cudaMalloc(&RP->d_counter, sizeof(int)), "cudaMalloc(counter)")) {
+        !cuda_ok(cudaMalloc(&RP->d_counter, sizeof(int)), "cudaMalloc(counter)") || !rotation_plan_pad(RP)) {
         ft_destroy_rotation_plan(RP);
         return nullptr;
     }
@@ -174,7 +174,7 @@ bool rotations(ft_rotation_plan * RP, bool hi2lo, const double * in, double * ou
     if (ntasks == 0) return true;
     static thread_local RotLaunch L;   // large parameter block; kept off the stack
     L.nfields = 1;
-    L.fields[0] = RotField{in, out, RP->d_sc, RP->n, M, RP->kind, lda, 0};
+    L.fields[0] = RotField{in, out, RP->d_scp, RP->n, M, RP->kind, lda, 0};
     L.tasks = d_tasks;
     L.ntasks = ntasks;
     L.counter = RP->d_counter;
@@ -659,7 +659,7 @@ int execute_batch_chunk(HarmonicPlan * const * H, bool forward, char TRANS, doub
         for (int f = 0; f < nf; f++) {
             const double * in = from_A ? A[f] : S[f];
             double * out = to_A ? A[f] : S[f];
-            L.fields[f] = RotField{in, out, H[f]->rp_arr[0]->d_sc, N[f], M[f], H[f]->kind, (long long) N[f], blk};
+            L.fields[f] = RotField{in, out, H[f]->rp_arr[0]->d_scp, N[f], M[f], H[f]->kind, (long long) N[f], blk};
             if (in != out) {
                 const int nc = untouched_cols(H[f]->kind, M[f]);
                 if (!cuda_ok(cudaMemcpy2DAsync(out, N[f] * sizeof(double), in, N[f] * sizeof(double), N[f] * sizeof(double), nc,
@@ -811,6 +811,159 @@ bool rotation_sweeps(ft_rotation_plan * RP, bool hi2lo, const double * in, doubl
     return rotations(RP, hi2lo, in, out, M, lda, st);
 }
 
+// ---------------------------------------------------------------------------
+// host-pointer fields sharing a plan: the transfers of one group of fields
+// overlap the transforms of the previous group and the read-back of the one
+// before it (three device buffers in rotation, three streams, events between
+// them).  Groups: the first and the last hold half as many fields as the
+// others, so that the transfers not hidden behind compute (the first group's
+// copy in, the last group's copy out) are short.
+// ---------------------------------------------------------------------------
+struct HostPipe {
+    static constexpr int NBUF = 3;
+    cudaStream_t s_in = nullptr, s_comp = nullptr, s_out = nullptr;
+    cudaEvent_t ev_in[NBUF] = {}, ev_comp[NBUF] = {}, ev_out[NBUF] = {};
+    double * buf[NBUF] = {};   // cap matrices of elems doubles each
+    int cap = 0;
+    size_t elems = 0;
+    std::mutex mu;             // one call at a time per plan
+};
+std::mutex g_pipe_mu;
+std::map<HarmonicPlan *, HostPipe *> g_pipes;
+
+void host_pipe_free(HostPipe * Q) {
+    if (!Q) return;
+    for (cudaStream_t s : {Q->s_in, Q->s_comp, Q->s_out})
+        if (s) { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
+    for (int b = 0; b < HostPipe::NBUF; b++) {
+        if (Q->ev_in[b]) cudaEventDestroy(Q->ev_in[b]);
+        if (Q->ev_comp[b]) cudaEventDestroy(Q->ev_comp[b]);
+        if (Q->ev_out[b]) cudaEventDestroy(Q->ev_out[b]);
+        if (Q->buf[b]) cudaFree(Q->buf[b]);
+    }
+    delete Q;
+}
+
+void release_host_pipe(HarmonicPlan * H) {
+    std::lock_guard<std::mutex> lk(g_pipe_mu);
+    auto it = g_pipes.find(H);
+    if (it == g_pipes.end()) return;
+    host_pipe_free(it->second);
+    g_pipes.erase(it);
+}
+
+// The plan's pipeline with buffers for at least cap fields of elems doubles (grown on demand).
+HostPipe * host_pipe(HarmonicPlan * H, int cap, size_t elems) {
+    std::lock_guard<std::mutex> lk(g_pipe_mu);
+    HostPipe *& Q = g_pipes[H];
+    if (Q && (Q->cap < cap || Q->elems < elems)) { host_pipe_free(Q); Q = nullptr; }
+    if (Q) return Q;
+    Q = new HostPipe();
+    bool ok = cuda_ok(cudaStreamCreateWithFlags(&Q->s_in, cudaStreamNonBlocking), "cudaStreamCreate") &&
+              cuda_ok(cudaStreamCreateWithFlags(&Q->s_comp, cudaStreamNonBlocking), "cudaStreamCreate") &&
+              cuda_ok(cudaStreamCreateWithFlags(&Q->s_out, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (int b = 0; ok && b < HostPipe::NBUF; b++)
+        ok = cuda_ok(cudaEventCreateWithFlags(&Q->ev_in[b], cudaEventDisableTiming), "cudaEventCreate") &&
+             cuda_ok(cudaEventCreateWithFlags(&Q->ev_comp[b], cudaEventDisableTiming), "cudaEventCreate") &&
+             cuda_ok(cudaEventCreateWithFlags(&Q->ev_out[b], cudaEventDisableTiming), "cudaEventCreate") &&
+             cuda_ok(cudaMalloc(&Q->buf[b], sizeof(double) * elems * (size_t) cap), "cudaMalloc(host pipeline buffer)");
+    Q->cap = cap;
+    Q->elems = elems;
+    if (!ok) { host_pipe_free(Q); Q = nullptr; g_pipes.erase(H); }
+    return Q;
+}
+
+// Group sizes for nfields fields with groups of up to g: halves at both ends.
+std::vector<int> host_groups(int nfields, int g) {
+    std::vector<int> sizes;
+    const int half = std::max(1, g / 2);
+    const int first = std::min(nfields, half);
+    sizes.push_back(first);
+    int rem = nfields - first;
+    const int last = std::min(rem, half);
+    rem -= last;
+    while (rem > 0) { const int s = std::min(rem, g); sizes.push_back(s); rem -= s; }
+    if (last > 0) sizes.push_back(last);
+    return sizes;
+}
+
+int host_group_size() {
+    static const int g = [] {
+        const char * e = std::getenv("FT_B200_HOST_GROUP");
+        const int v = e ? std::atoi(e) : 0;
+        return (v >= 1 && v <= kMaxFields) ? v : 4;
+    }();
+    return g;
+}
+
+int shared_prepare(HarmonicPlan * H, int precision) {
+    if (precision != FT_B200_FP64 && precision != FT_B200_FP64_BLOCKED && precision != FT_B200_MIXED_BF16 &&
+        precision != FT_B200_MIXED_BF16X4) {
+        set_error(FT_B200_EINVAL, "unknown precision");
+        return FT_B200_EINVAL;
+    }
+    if (precision != FT_B200_FP64 && !H->blocked) {
+        H->blocked = blocked_plan_build(H);
+        if (!H->blocked) return t_status;
+    }
+    if ((precision == FT_B200_MIXED_BF16 || precision == FT_B200_MIXED_BF16X4) &&
+        !blocked_mixed_prepare(H->blocked, precision == FT_B200_MIXED_BF16X4 ? 4 : 3))
+        return t_status;
+    return FT_B200_OK;
+}
+
+int shared_run(HarmonicPlan * H, bool forward, char TRANS, double * const * dA, int nfields, int precision, cudaStream_t st) {
+    const int M = H->Mdef;
+    for (int f0 = 0; f0 < nfields; f0 += kMaxFields) {
+        const int nf = std::min(kMaxFields, nfields - f0);
+        std::vector<HarmonicPlan *> Hs(nf, H);
+        std::vector<int> Ns(nf, H->n), Ms(nf, M);
+        if (execute_batch_chunk(Hs.data(), forward, TRANS, dA + f0, Ns.data(), Ms.data(), nf, st, precision) != FT_B200_OK)
+            return t_status;
+    }
+    return FT_B200_OK;
+}
+
+int shared_host(HarmonicPlan * H, int nops, const int * forward, const char * TRANS, double * const * A, int nfields,
+                int precision) {
+    int dev = 0;
+    if (!cuda_ok(cudaGetDevice(&dev), "cudaGetDevice")) return t_status;
+    if (dev != H->device) { set_error(FT_B200_EINVAL, "the plan lives on another device (make it current)"); return t_status; }
+    if (shared_prepare(H, precision) != FT_B200_OK) return t_status;
+    const std::vector<int> groups = host_groups(nfields, host_group_size());
+    const int cap = *std::max_element(groups.begin(), groups.end());
+    const size_t elems = (size_t) H->n * H->Mdef, bytes = elems * sizeof(double);
+    HostPipe * Q = host_pipe(H, cap, elems);
+    if (!Q) return t_status;
+    std::lock_guard<std::mutex> lk(Q->mu);
+    bool ok = true;
+    int f0 = 0;
+    for (size_t g = 0; ok && g < groups.size(); g++) {
+        const int b = (int) (g % HostPipe::NBUF), nf = groups[g];
+        std::vector<double *> d(nf);
+        for (int i = 0; i < nf; i++) d[i] = Q->buf[b] + elems * (size_t) i;
+        // the buffer is free once the read-back of the group that used it before has finished
+        if (g >= (size_t) HostPipe::NBUF) ok = cuda_ok(cudaStreamWaitEvent(Q->s_in, Q->ev_out[b], 0), "cudaStreamWaitEvent");
+        for (int i = 0; ok && i < nf; i++)
+            ok = cuda_ok(cudaMemcpyAsync(d[i], A[f0 + i], bytes, cudaMemcpyHostToDevice, Q->s_in), "cudaMemcpyAsync(H2D)");
+        ok = ok && cuda_ok(cudaEventRecord(Q->ev_in[b], Q->s_in), "cudaEventRecord") &&
+             cuda_ok(cudaStreamWaitEvent(Q->s_comp, Q->ev_in[b], 0), "cudaStreamWaitEvent");
+        for (int o = 0; ok && o < nops; o++)
+            ok = shared_run(H, forward[o] != 0, TRANS[o], d.data(), nf, precision, Q->s_comp) == FT_B200_OK;
+        ok = ok && cuda_ok(cudaEventRecord(Q->ev_comp[b], Q->s_comp), "cudaEventRecord") &&
+             cuda_ok(cudaStreamWaitEvent(Q->s_out, Q->ev_comp[b], 0), "cudaStreamWaitEvent");
+        for (int i = 0; ok && i < nf; i++)
+            ok = cuda_ok(cudaMemcpyAsync(A[f0 + i], d[i], bytes, cudaMemcpyDeviceToHost, Q->s_out), "cudaMemcpyAsync(D2H)");
+        ok = ok && cuda_ok(cudaEventRecord(Q->ev_out[b], Q->s_out), "cudaEventRecord");
+        f0 += nf;
+    }
+    // the call returns with every result in host memory (or after everything enqueued has ended)
+    const bool done = cuda_ok(cudaStreamSynchronize(Q->s_in), "cudaStreamSynchronize") &
+                      cuda_ok(cudaStreamSynchronize(Q->s_comp), "cudaStreamSynchronize") &
+                      cuda_ok(cudaStreamSynchronize(Q->s_out), "cudaStreamSynchronize");
+    return (ok && done) ? FT_B200_OK : t_status;
+}
+
 }  // namespace ftb
 
 using namespace ftb;
@@ -881,6 +1034,7 @@ void ft_destroy_harmonic_plan(ft_harmonic_plan * P) {
     if (H->blocked) blocked_plan_free(H->blocked);
     if (H->mixed_trmm) mixed_trmm_plan_free(H->mixed_trmm);
     release_batches(H);
+    release_host_pipe(H);
     H->magic = 0;
     delete H;
 }
@@ -911,6 +1065,7 @@ void ft_destroy_rotation_plan(ft_rotation_plan * RP) {
     }
     delete RP->mu;
     if (RP->d_sc) cudaFree(RP->d_sc);
+    if (RP->d_scp) cudaFree(RP->d_scp);
     if (RP->d_counter) cudaFree(RP->d_counter);
     std::free(RP->s);
     std::free(RP->c);
@@ -978,23 +1133,25 @@ int ft_b200_execute_shared_dev(const ft_harmonic_plan * P, int forward, char TRA
     for (int f = 0; f < nfields; f++)
         if (!dA[f]) { set_error(FT_B200_EINVAL, "NULL matrix"); return t_status; }
     if (nfields == 0) return FT_B200_OK;
-    const cudaStream_t st = static_cast<cudaStream_t>(stream);
-    if (precision != FT_B200_FP64 && !H->blocked) {
-        H->blocked = blocked_plan_build(H);
-        if (!H->blocked) return t_status;
-    }
-    if ((precision == FT_B200_MIXED_BF16 || precision == FT_B200_MIXED_BF16X4) &&
-        !blocked_mixed_prepare(H->blocked, precision == FT_B200_MIXED_BF16X4 ? 4 : 3))
+    if (shared_prepare(H, precision) != FT_B200_OK) return t_status;
+    return shared_run(H, forward != 0, TRANS, dA, nfields, precision, static_cast<cudaStream_t>(stream));
+}
+
+int ft_b200_execute_shared_host(const ft_harmonic_plan * P, int nops, const int * forward, const char * TRANS,
+                                double * const * A, int nfields, int precision) {
+    clear_error();
+    HarmonicPlan * H = as_plan(P);
+    if (!H) { set_error(FT_B200_EINVAL, "not a plan created by this library"); return t_status; }
+    if (nops < 0 || nfields < 0 || (nops > 0 && (!forward || !TRANS)) || (nfields > 0 && !A)) {
+        set_error(FT_B200_EINVAL, "bad argument");
         return t_status;
-    const int M = H->Mdef;
-    for (int f0 = 0; f0 < nfields; f0 += kMaxFields) {
-        const int nf = std::min(kMaxFields, nfields - f0);
-        std::vector<HarmonicPlan *> Hs(nf, H);
-        std::vector<int> Ns(nf, H->n), Ms(nf, M);
-        if (execute_batch_chunk(Hs.data(), forward != 0, TRANS, dA + f0, Ns.data(), Ms.data(), nf, st, precision) != FT_B200_OK)
-            return t_status;
     }
-    return FT_B200_OK;
+    for (int o = 0; o < nops; o++)
+        if (TRANS[o] != 'N' && TRANS[o] != 'T') { set_error(FT_B200_EINVAL, "TRANS must be 'N' or 'T'"); return t_status; }
+    for (int f = 0; f < nfields; f++)
+        if (!A[f]) { set_error(FT_B200_EINVAL, "NULL matrix"); return t_status; }
+    if (nfields == 0 || nops == 0) return FT_B200_OK;
+    return shared_host(H, nops, forward, TRANS, A, nfields, precision);
 }
 
 int ft_b200_device_status(const ft_harmonic_plan * P) {

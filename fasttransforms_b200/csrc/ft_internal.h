@@ -62,6 +62,24 @@ struct Geo {
     __host__ __device__ static inline long long table_len(int kind, int N) {
         return kind == DISK ? (long long) N * N : (long long) N * (N + 1) / 2;
     }
+    // Padded copy of the table, read by the rotation kernel's bulk copies: an identity row of
+    // kIdLen pairs (sin 0, cos 1), then every column j of the packed table with kPadPos chain
+    // positions of identity pairs on each side, then another identity row.  Inside a column,
+    // entry l is the packed entry where the sweep has a rotation (0 <= l / CH <= top(j, l % CH)),
+    // the identity elsewhere, so a chunk of consecutive positions that overlaps the sweep's
+    // entries can be copied without a range check (kPadPos >= the chunk length E); a chunk
+    // entirely outside them is copied from an identity row.
+    static constexpr int kPadPos = 16;
+    static constexpr int kIdLen = 64;
+    __host__ __device__ static inline int table_cols(int kind, int N) { return kind == DISK ? 2 * N - 1 : N; }
+    __host__ __device__ static inline long long pad_side(int kind) { return (long long) kPadPos * chains(kind); }
+    // offset of entry l = 0 of column j in the padded table
+    __host__ __device__ static inline long long padded_col(int kind, int N, int j) {
+        return kIdLen + table_base(kind, N, j) + (2LL * j + 1) * pad_side(kind);
+    }
+    __host__ __device__ static inline long long padded_len(int kind, int N) {
+        return 2LL * kIdLen + table_len(kind, N) + 2LL * table_cols(kind, N) * pad_side(kind);
+    }
     // number of order columns the rotation stage visits for an N x M matrix
     // sph / disk: pairs (2m-1, 2m), m = 2 .. M/2; tri: column m, m = 1 .. M-1
     __host__ __device__ static inline int first_order(int kind) { return kind == TRI ? 1 : (kind == SPIN ? 0 : 2); }
@@ -117,7 +135,7 @@ struct RotTask {
 struct RotField {
     const double * in;      // first pass reads here
     double * out;           // every pass writes here (in == out allowed)
-    const double2 * sc;     // interleaved (sin, cos) table in the reference packing
+    const double2 * sc;     // the padded (sin, cos) table of the field's rotation plan (Geo::padded_col)
     int N, M, kind;
     long long lda;
     int blk;                // 0: all sweeps; > 0: only each column's sweeps above the last
@@ -134,15 +152,16 @@ struct RotLaunch {
     const RotTask * tasks;     // device, longest first
     int ntasks;
     int * counter;             // device work counter (reset by the launcher)
-    // Pass pipeline (null units: each CTA runs every pass of a task itself).  Unit u is pass
-    // units[u].pass of task units[u].task; it streams down the columns behind its
-    // predecessor unit units[u].prev (pass - 1 of the same task, pulled earlier from the
-    // queue), whose progress word it waits on; prog[u] is its own (cleared by the launcher).
-    const struct RotUnit * units;
-    int nunits;
+    // Pass pipeline (null chains: each CTA runs every pass of a task itself).  Queue entry c
+    // runs passes first, first + stride, ... of task chains[c].task; pass r streams down the
+    // columns behind pass r - 1 of the same task (run by another entry, or earlier by this
+    // one), waiting on that pass's progress word prog[prog0 + r - 1] and publishing its own,
+    // prog[prog0 + r] (cleared by the launcher).
+    const struct RotChain * chains;
+    int nchains;
     int * prog;
 };
-struct RotUnit { int task, pass, prev; };
+struct RotChain { int task, prog0, first, stride; };
 // Host side of the pass pipeline of one task list: the host copy of the device list (same
 // order) and the unit lists built from it per pass length and head mode (rotations.cu).
 struct RotSchedule;
@@ -156,6 +175,8 @@ int rotation_device_error();   // reads and clears the rotation kernel's status 
 cudaError_t launch_rotations(int kind, bool hi2lo, const RotLaunch & L, int max_ctas, cudaStream_t st,
                              double * const * dead = nullptr, RotSchedule * sched = nullptr);
 void set_rotation_config(int cfg);   // 0 .. 3 forces a configuration, -1 chooses per shape
+// (Re)builds RP->d_scp from RP->d_sc (call after every change of d_sc; synchronous)
+bool rotation_plan_pad(ft_rotation_plan * RP);
 
 // Triangular multiplies (trmm.cu).  Out = op(U) * In on column classes.
 struct TrmmClass {
@@ -309,6 +330,7 @@ struct ft_rotation_plan_s {
     double alpha, beta, gamma;
     int device;
     double2 * d_sc;            // interleaved table
+    double2 * d_scp;           // the same, padded for the rotation kernel's bulk copies (Geo::padded_col)
     int * d_counter;           // work counter for the persistent kernel
     std::mutex * mu;
     std::map<int, std::pair<ftb::RotTask *, int>> * tasks;   // M -> device task list (longest first)

@@ -75,7 +75,7 @@ bool rot(HarmonicPlan * H, bool hi2lo, const double * in, double * out, int M, i
     if (ntasks == 0) return true;
     static thread_local RotLaunch L;
     L.nfields = 1;
-    L.fields[0] = RotField{in, out, RP->d_sc, H->n, M, H->kind, lda, 0};
+    L.fields[0] = RotField{in, out, RP->d_scp, H->n, M, H->kind, lda, 0};
     L.tasks = tasks;
     L.ntasks = ntasks;
     L.counter = counter;   // reset to zero by the launcher before the kernel runs

@@ -40,10 +40,12 @@
 #include <type_traits>
 
 #include <map>
+#include <tuple>
 #include <mutex>
 #include <string>
 
 #include "ft_internal.h"
+#include "tc05.h"
 
 namespace ftb {
 namespace {
@@ -61,18 +63,27 @@ struct KT {
     static constexpr int CPAD = COLS + 1;                 // padded column dimension of the stage buffers
 };
 
-struct SweepInfo {
-    long long tbase;      // packed-table offset of the sweep's column
-    int j;                // order of the sweep
-    int tlo[2], thi[2];   // steps at which the sweep has a valid position, per chain
-};
-
-__device__ __forceinline__ void cp_async16(void * smem, const void * gmem) {
-    const unsigned sa = (unsigned) __cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" :: "r"(sa), "l"(gmem));
+// Builds the padded table (Geo::padded_col): block j fills column j's padded segment, blocks
+// >= cols the identity rows at both ends.
+__global__ void pad_table_kernel(const double2 * __restrict__ sc, double2 * __restrict__ out, int kind, int N) {
+    const int cols = Geo::table_cols(kind, N), ch = Geo::chains(kind);
+    const long long side = Geo::pad_side(kind);
+    const double2 id = make_double2(0.0, 1.0);
+    const int j = blockIdx.x;
+    if (j >= cols) {   // the identity row before column 0, and the one after the last column
+        double2 * row = j == cols ? out : out + Geo::padded_col(kind, N, cols - 1) + (Geo::table_base(kind, N, cols) -
+                                                                                     Geo::table_base(kind, N, cols - 1)) + side;
+        for (int e = threadIdx.x; e < Geo::kIdLen; e += blockDim.x) row[e] = id;
+        return;
+    }
+    const long long len = Geo::table_base(kind, N, j + 1) - Geo::table_base(kind, N, j);
+    const long long base = Geo::table_base(kind, N, j);
+    double2 * col = out + Geo::padded_col(kind, N, j);
+    for (long long l = -side + threadIdx.x; l < len + side; l += blockDim.x) {
+        const bool valid = l >= 0 && l < len && (int) (l / ch) <= Geo::top(kind, N, j, (int) (l % ch));
+        col[l] = valid ? sc[base + l] : id;
+    }
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 __device__ __forceinline__ void rot_hi2lo(double & x, double & y, double s, double c) {
     const double sy = __dmul_rn(s, y), sx = __dmul_rn(s, x);
@@ -136,23 +147,32 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
     // (sin, cos) pairs of the chunk a stage works on, staged one iteration ahead
     double2 * const sc_stage_base = reinterpret_cast<double2 *>(smem + (W + 1) * 2 * E * CH * CPAD);
     auto sc_stage = [&](int q, int slot) -> double2 * { return sc_stage_base + ((q * 2 + slot) * B) * (E * CH); };
+    static_assert(E <= Geo::kPadPos, "the padded table must cover a chunk's overhang");
+    static_assert(E * CH <= Geo::kIdLen, "the identity row must cover a chunk");
     __shared__ int s_task;
-    __shared__ SweepInfo sweep_info[W * B];
+    __shared__ __align__(8) uint64_t s_mbar[W * 2];   // per stage and slot: its (sin, cos) staged
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int q = warp;                       // stage index
     const int o_lane = lane / CH, c_lane = lane % CH;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < W * 2; ++i) tc::mbar_init(&s_mbar[i], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+    uint32_t sc_phase = 0u;                   // bit s: parity of the next phase of this stage's mbarrier s
+    uint32_t sc_live = 0u;                    // bit s: the chunk staged for slot s has a rotation (warp-uniform)
 
-    const bool pipe = L.units != nullptr;
+    const bool pipe = L.chains != nullptr;
     for (;;) {
         if (threadIdx.x == 0) s_task = atomicAdd(L.counter, 1);
         __syncthreads();
         const int tid = s_task;
         __syncthreads();
-        if (tid >= (pipe ? L.nunits : L.ntasks)) break;
-        // one pass of a task (pipeline) or all of its passes
-        const RotUnit unit = pipe ? L.units[tid] : RotUnit{tid, -1, -1};
-        const RotTask task = L.tasks[unit.task];
+        if (tid >= (pipe ? L.nchains : L.ntasks)) break;
+        // passes first, first + stride, .. of a task (pipeline), or all of its passes
+        const RotChain chain = pipe ? L.chains[tid] : RotChain{tid, 0, 0, 1};
+        const RotTask task = L.tasks[chain.task];
         const RotField & F = L.fields[task.field];
         const int N = F.N;
         const long long lda = F.lda;
@@ -169,8 +189,7 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
         const int nsw = Geo::task_sweeps(KIND, F.M, mbase, F.blk, &jlo, &jhi, F.spin);
         if (nsw == 0) continue;   // nothing to do for this task (uniform)
         const int npass = (nsw + WB - 1) / WB;
-        const int rbeg = pipe ? unit.pass : 0, rend = pipe ? unit.pass + 1 : npass;
-        if (rend > npass) {       // a schedule that does not match this launch shape
+        if (chain.first >= npass || chain.stride < 1) {   // a schedule that does not match this launch shape
             if (threadIdx.x == 0) atomicExch(&g_rot_status, 4);
             continue;
         }
@@ -195,7 +214,7 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
             }
         const int L0 = Geo::chain_len(KIND, N, 0);
 
-        for (int r = rbeg; r < rend; ++r) {
+        for (int r = chain.first; r < npass; r += chain.stride) {
             const double * src = r == 0 ? F.in : F.out;
             double * dst = F.out;
             const bool copy_all = r == 0 && F.in != F.out;
@@ -218,9 +237,9 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
             const int tstart = HI2LO ? ref - emax : -1;
             const int tend = HI2LO ? ref + 2 * WAB : emax + 2 * WAB - 1;
             const int K = (tend - tstart + 1 + E - 1) / E;
-            // pass pipeline: the predecessor's progress word and this unit's own
-            const int * const prev_prog = (pipe && unit.prev >= 0) ? L.prog + unit.prev : nullptr;
-            int * const my_prog = pipe ? L.prog + tid : nullptr;
+            // pass pipeline: the previous pass's progress word and this pass's own
+            const int * const prev_prog = (pipe && r > 0) ? L.prog + chain.prog0 + r - 1 : nullptr;
+            int * const my_prog = pipe ? L.prog + chain.prog0 + r : nullptr;
 
             // ---- stage state: per column a window of 2B chain positions ----
             double win[NCOL][2 * B];
@@ -228,24 +247,23 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
             for (int h = 0; h < NCOL; ++h)
 #pragma unroll
                 for (int x = 0; x < 2 * B; ++x) win[h][x] = 0.0;
-            // per sweep of this stage (lane b < B computes sweep q*B + b)
-            SweepInfo * const my = sweep_info + q * B;
+            // lane b < B: the padded-table column of sweep q*B + b and its last entry with a
+            // rotation, or -1 where the sweep has none (beyond the pass, or a column with no
+            // positions): the identity row
+            long long my_col = -1;
+            int my_lmax = -1;
             if (lane < B) {
                 const int s = q * B + lane;
-                SweepInfo si;
-                si.j = HI2LO ? jfirst - STEP * s : jfirst + STEP * s;
-                const bool sv = s < S;
-                si.tbase = sv ? Geo::table_base(KIND, N, si.j) : 0;
+                const int j = HI2LO ? jfirst - STEP * s : jfirst + STEP * s;
+                if (s < S && j >= 0 && j < Geo::table_cols(KIND, N)) {
 #pragma unroll
-                for (int c = 0; c < 2; ++c) {
-                    const int ts = HI2LO ? Geo::top(KIND, N, jfirst, c < CH ? c : 0) + s : Geo::top(KIND, N, jfirst, c < CH ? c : 0) - s;
-                    if (HI2LO) { si.tlo[c] = ref + 2 * s - ts; si.thi[c] = ref + 2 * s; }
-                    else       { si.tlo[c] = 2 * s;            si.thi[c] = 2 * s + ts; }
-                    if (!sv || ts < 0) { si.tlo[c] = 1; si.thi[c] = 0; }   // empty
+                    for (int c = 0; c < CH; ++c) {
+                        const int tc = Geo::top(KIND, N, j, c);
+                        if (tc >= 0) my_lmax = max(my_lmax, CH * tc + c);
+                    }
+                    if (my_lmax >= 0) my_col = Geo::padded_col(KIND, N, j);
                 }
-                my[lane] = si;
             }
-            __syncwarp();
             const int jmax = HI2LO ? jfirst - STEP * (q * B) : jfirst + STEP * (q * B + B - 1);
             const int jmin = HI2LO ? jfirst - STEP * (q * B + B - 1) : jfirst + STEP * (q * B);
             // every sweep of this stage applies to every order of the task
@@ -258,30 +276,46 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
                 if (j <= me_lane - STEP && j >= jcut_lane) lane_mask |= 1u << b;
             }
 
-            // Stage the (sin, cos) pairs of a chunk: entry (b, jj) is the pair sweep b
-            // uses at step u of the chunk on chain c; where the sweep has no valid
-            // position at that step the entry is the identity (sin 0, cos 1), so every
-            // chunk runs the same straight-line code and those rotations are exact no-ops.
+            // Stage the (sin, cos) pairs of a chunk: entry (b, jj) is the pair sweep b uses at step
+            // u of the chunk on chain c (jj = CH u + c, u reversed in hi2lo), i.e. the CH E
+            // consecutive entries of its padded column starting at chain position ibase, where the
+            // padding holds the identity (sin 0, cos 1) wherever the sweep has no rotation at that
+            // step: every chunk runs the same straight-line code and those rotations are exact
+            // no-ops.  One bulk copy per sweep (lanes 0 .. B-1) completes on the stage's mbarrier
+            // for the slot.  A chunk in which none of the stage's sweeps has a rotation is not
+            // staged at all: the stage passes its elements through unrotated (sc_live).
             auto prefetch_sc = [&](int kp) {
                 const int t0p = tstart + kp * E;
-                double2 * const d = sc_stage(q, kp & 1);
-#pragma unroll
-                for (int rr = 0; rr < (B * E * CH) / 32; ++rr) {
-                    const int f = rr * 32 + lane;
-                    const int b = f / (E * CH), jj = f % (E * CH);
-                    const int c = CH == 2 ? (jj & 1) : 0;
-                    const int u = HI2LO ? (E - 1 - (CH == 2 ? (jj >> 1) : jj)) : (CH == 2 ? (jj >> 1) : jj);
-                    const int t = t0p + u;
-                    const int s = q * B + b;
-                    const SweepInfo & si = my[b];
-                    if (t >= si.tlo[c] && t <= si.thi[c]) {
-                        const int i = HI2LO ? ref + 2 * s - t : t - 2 * s;
-                        cp_async16(d + f, F.sc + si.tbase + (CH == 2 ? 2 * i + c : i));
-                    } else {
-                        d[f] = make_double2(0.0, 1.0);
-                    }
+                const int slot = kp & 1;
+                double2 * const d = sc_stage(q, slot);
+                uint64_t * const bar = &s_mbar[q * 2 + slot];
+                int lo = 0;
+                bool overlaps = false;
+                if (lane < B) {
+                    const int sg = q * B + lane;
+                    lo = CH * (HI2LO ? ref + 2 * sg - t0p - E + 1 : t0p - 2 * sg);   // first entry
+                    // a chunk overlapping the sweep's entries reaches at most E positions past
+                    // them, into the padding; one outside them reads the identity row
+                    overlaps = my_col >= 0 && lo <= my_lmax && lo + CH * E > 0;
                 }
-                cp_async_commit();
+                const bool live = __ballot_sync(0xffffffffu, overlaps) != 0u;
+                sc_live = live ? (sc_live | (1u << slot)) : (sc_live & ~(1u << slot));
+                if (!live) return;
+                if (lane == 0) tc::mbar_arrive_expect_tx(bar, (uint32_t) (B * E * CH * sizeof(double2)));
+                __syncwarp();
+                if (lane < B) {
+                    const double2 * src = overlaps ? F.sc + my_col + lo : F.sc;
+                    tc::bulk_g2s(d + lane * (E * CH), src, (uint32_t) (E * CH * sizeof(double2)), bar);
+                }
+            };
+            // wait until the stage's (sin, cos) of chunk k have landed (bounded: a wait that runs out
+            // sets the status word, and every later wait of the launch gives up at once)
+            auto wait_sc = [&](int k) {
+                const int slot = k & 1;
+                if (!tc::mbar_wait(&s_mbar[q * 2 + slot], (sc_phase >> slot) & 1u, (volatile int *) &g_rot_status)) {
+                    if (lane == 0) atomicCAS(&g_rot_status, 0, 5);
+                }
+                sc_phase ^= 1u << slot;
             };
 
             // ---- global traffic, shared by all warps: warp w moves elements
@@ -375,7 +409,6 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
             load_chunk(0);
             stash_chunk(0);
             if (q == 0) prefetch_sc(0);
-            cp_async_wait_all();
             __syncthreads();
 
             for (int it = 0; it < K + WA; ++it) {
@@ -386,8 +419,25 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
                 // (sin, cos) of the chunk this stage works on next iteration
                 if (q < WA && it + 1 - q >= 0 && it + 1 - q < K) prefetch_sc(it + 1 - q);
                 const int k = it - q;
-                if (q < WA && k >= 0 && k < K) {
+                if (q < WA && k >= 0 && k < K && !((sc_live >> (k & 1)) & 1u)) {
+                    // no rotation of this stage in the chunk: the window only shifts, every element
+                    // leaves the stage as it entered (the sequential loops do not touch them either)
                     const int slot = k & 1;
+#pragma unroll
+                    for (int u = 0; u < E; ++u) {
+                        const int pn = u % (2 * B);
+                        const double * bin = buf(q, slot, u, c_lane) + o_lane * NCOL;
+                        double * bout = buf(q + 1, slot, u, c_lane) + o_lane * NCOL;
+#pragma unroll
+                        for (int h = 0; h < NCOL; ++h) {
+                            const double in = bin[h];
+                            bout[h] = win[h][pn];
+                            win[h][pn] = in;
+                        }
+                    }
+                } else if (q < WA && k >= 0 && k < K) {
+                    const int slot = k & 1;
+                    wait_sc(k);
                     const double2 * const scb = sc_stage(q, slot);
                     const bool masked = !full_lanes;
                     // two copies of the step loop: all sweeps apply to all lanes, or per-lane masks
@@ -434,7 +484,6 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
                     else        run(std::false_type{});
                 }
                 if (it + 1 < K) stash_chunk(it + 1);
-                cp_async_wait_all();
                 if (pipe && threadIdx.x == 0) wait_chunk(it + 2);   // loaded next iteration
                 __syncthreads();
                 // the chunk stored this iteration is final: publish it
@@ -462,7 +511,7 @@ cudaError_t launch_cfg(const RotLaunch & L, int max_ctas, cudaStream_t st) {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, W * 32, shm) != cudaSuccess || per_sm < 1) per_sm = 1;
     int ctas = sms * per_sm;
     if (max_ctas > 0 && ctas > max_ctas) ctas = max_ctas;
-    const int work = L.units ? L.nunits : L.ntasks;   // queue entries: pass units or tasks
+    const int work = L.chains ? L.nchains : L.ntasks;   // queue entries: pipeline entries or tasks
     if (ctas > work) ctas = work;
     if (ctas <= 0) return cudaSuccess;
     e = cudaMemsetAsync(L.counter, 0, sizeof(int), st);
@@ -507,10 +556,11 @@ cudaError_t launch_kind(int cfg, const RotLaunch & L, int max_ctas, cudaStream_t
 
 int g_rot_cfg = -2;
 
-// A configuration is a launch shape 0 .. 5, plus 8 to run through the pass pipeline.
-// FT_B200_ROT_CFG forces one (as does ft_b200_set_rotation_config); otherwise -1 (chosen
-// per launch shape).
-bool valid_config(int cfg) { return cfg >= 0 && (cfg & 7) <= 5 && cfg < 16; }
+// A configuration is a launch shape 0 .. 5 plus 8 x a pass-pipeline mode 0 .. 3
+// (schedule_chains).  FT_B200_ROT_CFG forces one (as does ft_b200_set_rotation_config);
+// otherwise -1 (chosen per launch shape).
+constexpr int kPipeModes = 4;
+bool valid_config(int cfg) { return cfg >= 0 && (cfg & 7) <= 5 && cfg < 8 * kPipeModes; }
 
 int rotation_config() {
     if (g_rot_cfg == -2) {
@@ -525,8 +575,8 @@ void set_rotation_config(int cfg) { g_rot_cfg = valid_config(cfg) ? cfg : -1; }
 
 struct RotSchedule {
     std::vector<RotTask> tasks;                          // host copy of the device list (same order)
-    struct Units { RotUnit * d_units = nullptr; int * d_prog = nullptr; int n = 0; };
-    std::map<std::pair<int, int>, Units> lists;          // (sweeps per pass, heads only) -> units
+    struct Units { RotChain * d_chains = nullptr; int * d_prog = nullptr; int n = 0, nprog = 0; };
+    std::map<std::tuple<int, int, int>, Units> lists;    // (sweeps per pass, heads only, pipeline mode) -> queue
     std::mutex mu;
 };
 
@@ -538,8 +588,28 @@ RotSchedule * rot_schedule_new(const std::vector<RotTask> & tasks) {
 
 void rot_schedule_free(RotSchedule * s) {
     if (!s) return;
-    for (auto & kv : s->lists) { cudaFree(kv.second.d_units); cudaFree(kv.second.d_prog); }
+    for (auto & kv : s->lists) { cudaFree(kv.second.d_chains); cudaFree(kv.second.d_prog); }
     delete s;
+}
+
+bool rotation_plan_pad(ft_rotation_plan * RP) {
+    if (RP->d_scp) { cudaFree(RP->d_scp); RP->d_scp = nullptr; }
+    const long long len = Geo::padded_len(RP->kind, RP->n);
+    cudaError_t e = cudaMalloc(&RP->d_scp, sizeof(double2) * len);
+    if (e != cudaSuccess) {
+        RP->d_scp = nullptr;
+        set_error(e == cudaErrorMemoryAllocation ? FT_B200_ENOMEM : FT_B200_ECUDA, std::string("cudaMalloc(padded table): ") + cudaGetErrorString(e));
+        return false;
+    }
+    pad_table_kernel<<<Geo::table_cols(RP->kind, RP->n) + 2, 256>>>(RP->d_sc, RP->d_scp, RP->kind, RP->n);
+    count_launch();
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        set_error(FT_B200_ECUDA, std::string("pad_table_kernel: ") + cudaGetErrorString(e));
+        return false;
+    }
+    return true;
 }
 
 int rotation_device_error() {
@@ -554,58 +624,94 @@ int rotation_device_error() {
 
 namespace {
 
-// Sweeps per pass (W x B) of each launch shape.
+// Sweeps per pass (W x B), stage warps W and sweeps per warp B of each launch shape.
 int shape_pass(int cfg) {
     static const int wb[6] = {64, 64, 32, 32, 16, 32};
     return (cfg >= 0 && cfg < 6) ? wb[cfg] : 64;
 }
+int shape_warps(int cfg) {
+    static const int w[6] = {8, 16, 8, 8, 4, 4};
+    return (cfg >= 0 && cfg < 6) ? w[cfg] : 8;
+}
+int shape_sweeps(int cfg) { return shape_pass(cfg) / shape_warps(cfg); }
 
-// The units of L's tasks for passes of wb sweeps, in queue order (a unit's predecessor is
-// always pulled first).  Built on first use; null when the stream is capturing then (the
-// upload synchronises) or on an allocation failure.
-const RotSchedule::Units * schedule_units(RotSchedule * S, int kind, const RotLaunch & L, int wb, cudaStream_t st) {
+// The queue of the pass pipeline for L's tasks with passes of wb sweeps (pipeline mode pm,
+// ctas resident CTAs), built on first use; null when the stream is capturing then (the upload
+// synchronises) or on an allocation failure.  Every entry's passes wait only on passes of the
+// same task, and a task's entries are adjacent in the queue, so at most one task is ever
+// partly pulled: every other running entry can finish, and the queue cannot deadlock while
+// that task's entries fit in the other CTAs (stride <= ctas / 2).
+//   pm 1: one entry per pass, pass-major (every task's pass r before any task's pass r + 1):
+//         a pass never waits long for its predecessor, but consecutive passes of a task run far
+//         apart in time, so its columns leave L2 between them when the matrix is large;
+//   pm 2, 3: task t in D_t entries (entry d runs passes d, d + D_t, ..), D_t from the task's
+//         cost (its passes' steps) against a target of 1/2 (pm 2) or 1/4 (pm 3) of the average
+//         load of a CTA; the entries of a task run side by side, a few chunks apart, so the
+//         columns stay in L2, and long tasks no longer leave SMs idle at the end of the queue.
+const RotSchedule::Units * schedule_chains(RotSchedule * S, int kind, const RotLaunch & L, int wb, int B, int pm, int ctas,
+                                           cudaStream_t st) {
     const int blk = L.fields[0].blk;
     std::lock_guard<std::mutex> lk(S->mu);
-    const auto key = std::make_pair(wb, blk > 0 ? blk : 0);
+    const auto key = std::make_tuple(wb, blk > 0 ? 1 : 0, pm);
     auto it = S->lists.find(key);
-    if (it != S->lists.end()) return it->second.d_units ? &it->second : nullptr;
+    if (it != S->lists.end()) return it->second.d_chains ? &it->second : nullptr;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return nullptr;
     const int nt = (int) S->tasks.size();
-    std::vector<int> npass(nt, 0);
-    int maxp = 0;
+    std::vector<int> npass(nt, 0), prog0(nt, 0);
+    std::vector<double> cost(nt, 0.0);
+    int nprog = 0, maxp = 0;
+    double total = 0.0;
     for (int t = 0; t < nt; ++t) {
         const RotTask & T = S->tasks[t];
         const RotField & F = L.fields[T.field];
         int jlo, jhi;
-        const int nsw = Geo::task_sweeps(kind, F.M, T.mbase, F.blk, &jlo, &jhi);
+        const int nsw = Geo::task_sweeps(kind, F.M, T.mbase, F.blk, &jlo, &jhi, F.spin);
         npass[t] = (nsw + wb - 1) / wb;
+        prog0[t] = nprog;
+        nprog += npass[t];
         maxp = std::max(maxp, npass[t]);
+        // steps of its passes: a pass covers the longest of its sweeps plus the wavefront's
+        // skew (2 steps per sweep); with chunk granularity this is the kernel's work to a few %
+        const int step = Geo::step(kind);
+        for (int r = 0; r < npass[t]; ++r) {
+            const int jlong = std::max(jlo, jhi - step * (std::min(nsw, (r + 1) * wb) - 1));   // lowest order of pass r
+            cost[t] += std::max(0, Geo::top(kind, F.N, jlong, 0) + 1) + 2.0 * std::min(wb, nsw - r * wb) + B;
+        }
+        total += cost[t];
     }
-    // pass-major (every task's pass r before any task's pass r + 1, so a unit's predecessor
-    // is always pulled first), tasks in list order (longest first) within a pass.  (Ordering
-    // by passes left in the task, which keeps a task's passes closer together, measured the
-    // same or slightly slower.)
-    std::vector<RotUnit> u;
-    std::vector<int> last(nt, -1);   // unit index of each task's latest pass so far
-    for (int r = 0; r < maxp; ++r)
-        for (int t = 0; t < nt; ++t)
-            if (r < npass[t]) {
-                u.push_back(RotUnit{t, r, last[t]});
-                last[t] = (int) u.size() - 1;
-            }
+    std::vector<RotChain> q;
+    if (pm == 1) {
+        for (int r = 0; r < maxp; ++r)
+            for (int t = 0; t < nt; ++t)
+                if (r < npass[t]) q.push_back(RotChain{t, prog0[t], r, npass[t]});
+    } else {
+        const double target = (pm == 2 ? 0.5 : 0.25) * total / std::max(1, ctas);
+        const int dmax = std::max(1, ctas / 2);
+        std::vector<std::pair<double, int>> order;   // (entry duration, task), longest first
+        std::vector<int> D(nt, 1);
+        for (int t = 0; t < nt; ++t) {
+            if (npass[t] == 0) continue;
+            D[t] = std::max(1, std::min({npass[t], dmax, (int) std::lround(cost[t] / std::max(target, 1.0))}));
+            order.push_back({cost[t] / D[t], t});
+        }
+        std::stable_sort(order.begin(), order.end(), [](const auto & a, const auto & b) { return a.first > b.first; });
+        for (auto & o : order)
+            for (int d = 0; d < D[o.second]; ++d) q.push_back(RotChain{o.second, prog0[o.second], d, D[o.second]});
+    }
     RotSchedule::Units U;
-    U.n = (int) u.size();
+    U.n = (int) q.size();
+    U.nprog = nprog;
     if (U.n > 0) {
-        if (cudaMalloc(&U.d_units, sizeof(RotUnit) * u.size()) != cudaSuccess ||
-            cudaMalloc(&U.d_prog, sizeof(int) * u.size()) != cudaSuccess ||
-            cudaMemcpy(U.d_units, u.data(), sizeof(RotUnit) * u.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
-            cudaFree(U.d_units); cudaFree(U.d_prog);
+        if (cudaMalloc(&U.d_chains, sizeof(RotChain) * q.size()) != cudaSuccess ||
+            cudaMalloc(&U.d_prog, sizeof(int) * std::max(nprog, 1)) != cudaSuccess ||
+            cudaMemcpy(U.d_chains, q.data(), sizeof(RotChain) * q.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+            cudaFree(U.d_chains); cudaFree(U.d_prog);
             U = RotSchedule::Units{};
         }
     }
     S->lists[key] = U;
-    return U.d_units ? &S->lists[key] : nullptr;
+    return U.d_chains ? &S->lists[key] : nullptr;
 }
 
 cudaError_t launch_with(int kind, bool hi2lo, int cfg, const RotLaunch & L, int max_ctas, cudaStream_t st) {
@@ -619,19 +725,27 @@ cudaError_t launch_with(int kind, bool hi2lo, int cfg, const RotLaunch & L, int 
     return cudaErrorInvalidValue;
 }
 
-// One launch in configuration cfg: shape cfg & 7, through the pass pipeline when cfg & 8
-// and the task list has a schedule (else each CTA runs every pass of its tasks).
+// One launch in configuration cfg: shape cfg & 7, through the pass pipeline in mode cfg >> 3
+// (schedule_chains; 0: none) when the task list has a schedule (else each CTA runs every pass
+// of its tasks).
 cudaError_t launch_shape(int kind, bool hi2lo, int cfg, const RotLaunch & L, int max_ctas, cudaStream_t st,
                          RotSchedule * sched) {
-    const int shape = cfg & 7;
-    const RotSchedule::Units * U = ((cfg & 8) && sched) ? schedule_units(sched, kind, L, shape_pass(shape), st) : nullptr;
+    const int shape = cfg & 7, pm = cfg >> 3;
+    const RotSchedule::Units * U = nullptr;
+    if (pm > 0 && sched) {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const int ctas = sms * (shape_warps(shape) <= 4 ? 2 : 1);
+        U = schedule_chains(sched, kind, L, shape_pass(shape), shape_sweeps(shape), pm, max_ctas > 0 ? std::min(ctas, max_ctas) : ctas, st);
+    }
     if (!U) return launch_with(kind, hi2lo, shape, L, max_ctas, st);
     static thread_local RotLaunch P;
     P = L;
-    P.units = U->d_units;
-    P.nunits = U->n;
+    P.chains = U->d_chains;
+    P.nchains = U->n;
     P.prog = U->d_prog;
-    const cudaError_t e = cudaMemsetAsync(U->d_prog, 0x80, sizeof(int) * U->n, st);   // below any position
+    const cudaError_t e = cudaMemsetAsync(U->d_prog, 0x80, sizeof(int) * U->nprog, st);   // below any position
     if (e != cudaSuccess) return e;
     return launch_with(kind, hi2lo, shape, P, max_ctas, st);
 }
@@ -682,9 +796,9 @@ int tune(int kind, bool hi2lo, const RotLaunch & L, double * const * dead, int m
     // every shape, each also through the pass pipeline when the list has a schedule (it
     // spreads a task's passes over SMs: worth it when there are few tasks, not when the
     // columns would leave L2 between passes)
-    for (int cfg = 0; cfg < 14; ++cfg) {
+    for (int cfg = 0; cfg < 8 * kPipeModes; ++cfg) {
         if ((cfg & 7) > 5 || ((kind == TRI || kind == RECT) && (cfg & 7) == 1)) continue;   // tri, rect: shape 1 not built
-        if ((cfg & 8) && !sched) continue;
+        if ((cfg >> 3) && !sched) continue;
         if (launch_shape(kind, hi2lo, cfg, S, max_ctas, st, sched) != cudaSuccess) { best = -1; break; }
         if (cudaEventRecord(e0, st) != cudaSuccess) { best = -1; break; }
         if (launch_shape(kind, hi2lo, cfg, S, max_ctas, st, sched) != cudaSuccess) { best = -1; break; }

@@ -252,12 +252,12 @@ bool stage2(SpinRotPlan * P, bool hi2lo, double * A, int M, cudaStream_t st) {
     if (nt == 0) return true;
     static thread_local RotLaunch L;   // large parameter block; kept off the stack
     L.nfields = 1;
-    L.fields[0] = RotField{A, A, P->sph->d_sc, P->n, M, SPIN, (long long) P->n, 0, std::abs(P->s)};
+    L.fields[0] = RotField{A, A, P->sph->d_scp, P->n, M, SPIN, (long long) P->n, 0, std::abs(P->s)};
     L.tasks = dt;
     L.ntasks = nt;
     L.counter = P->d_counter;
-    L.units = nullptr;   // no pass pipeline
-    L.nunits = 0;
+    L.chains = nullptr;   // no pass pipeline
+    L.nchains = 0;
     L.prog = nullptr;
     prof_begin(FAM_ROT, st);
     const cudaError_t e = launch_rotations(SPIN, hi2lo, L, 0, st);

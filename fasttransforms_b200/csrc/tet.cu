@@ -175,13 +175,13 @@ bool tri_sweeps(const ft_rotation_plan * RP1, const TriStage & T, bool hi2lo, do
             const int m = g.m0 + f;
             // column index = order: column l of slab m (order l + m) at base + (l + m) N
             double * base = A + (long long) N * L * m - (long long) N * m;
-            Lr.fields[f] = RotField{base, base, RP1->d_sc, N, L, TRI, (long long) N, 0, 0};
+            Lr.fields[f] = RotField{base, base, RP1->d_scp, N, L, TRI, (long long) N, 0, 0};
         }
         Lr.tasks = g.d_tasks;
         Lr.ntasks = g.ntasks;
         Lr.counter = RP1->d_counter;
-        Lr.units = nullptr;
-        Lr.nunits = 0;
+        Lr.chains = nullptr;
+        Lr.nchains = 0;
         Lr.prog = nullptr;
         prof_begin(FAM_ROT, st);
         const cudaError_t e = launch_rotations(TRI, hi2lo, Lr, 0, st);

@@ -466,6 +466,27 @@ int ft_b200_execute_noalloc_dev(const ft_harmonic_plan * P, int forward, char TR
 int ft_b200_execute_shared_dev(const ft_harmonic_plan * P, int forward, char TRANS, double * const * dA, int nfields,
                                int precision, void * stream);
 
+/* Host-pointer form of ft_b200_execute_shared_dev for a sequence of transforms:
+ * every field A[f] (a host N x M column-major matrix, the plan's N and default
+ * M) goes through transforms o = 0 .. nops-1 (forward[o] nonzero: the
+ * forward transform, else the backward one; TRANS[o] 'N' or 'T'), in place,
+ * at the given precision.  The reference's counterpart is one
+ * ft_execute_sph2fourier / ft_execute_fourier2sph call per field and
+ * transform (src/drivers.c:833-865, host pointers, in place).
+ * The fields move in groups through three device buffers owned by the plan:
+ * the copy of group g + 1 to the device and the copy of group g - 1 back to
+ * the host overlap the transforms of group g (streams of the plan's own,
+ * events between them); the first and the last group hold half as many
+ * fields as the others (FT_B200_HOST_GROUP, default 4), so that the copies
+ * that cannot overlap are short.  Returns when every result is back in host
+ * memory.  The copies overlap only from page-locked host memory
+ * (cudaHostAlloc / cudaHostRegister); pageable memory gives the same results
+ * with serial copies.  The first call allocates the buffers (3 groups of the
+ * largest group size, about 1 GB per field slot at n = 4096); they are freed
+ * with the plan.  Calls on one plan are serialised. */
+int ft_b200_execute_shared_host(const ft_harmonic_plan * P, int nops, const int * forward, const char * TRANS,
+                                double * const * A, int nfields, int precision);
+
 /* Reads and clears the plan's device status word: 0 normally; nonzero when a
  * wait inside one of its tensor-core kernels gave up (the kernel then stops
  * early and its output is not valid).  Synchronises with the device.  No
@@ -489,13 +510,18 @@ int ft_b200_profile(int enable);
 int ft_b200_profile_read(int family, double * ms, int * launches);
 
 /* Launch configuration of the rotation kernel (no counterpart in the reference,
- * whose kernels have no launch shape).  cfg = s or s + 8 forces shape s = 0 .. 5
+ * whose kernels have no launch shape).  cfg = s + 8 p forces shape s = 0 .. 5
  * (warps x sweeps per warp x chunk: 8 x 8 x 16, 16 x 4 x 8, 8 x 4 x 8, 8 x 4 x 16,
  * 4 x 4 x 16 and 4 x 8 x 16, the last two with as many CTAs per SM as fit; tri has
- * no 16 x 4 x 8 and runs 8 x 8 x 16 for it); + 8 runs the pass pipeline, where
- * each pass of 16 .. 64 sweeps of a task is its own work unit and streams down the
- * columns on another SM right behind the previous pass (for inputs with fewer
- * tasks than SMs; it loses where the columns would leave L2 between passes).
+ * no 16 x 4 x 8 and runs 8 x 8 x 16 for it) and pass-pipeline mode p = 0 .. 3.
+ * p = 0: each CTA runs all passes (of 16 .. 64 sweeps) of the tasks it takes.
+ * p > 0: a pass streams down the columns right behind the task's previous pass,
+ * run by another CTA; p = 1 queues every pass as its own entry, pass-major (for
+ * inputs with fewer tasks than SMs; it loses where the columns would leave L2
+ * between passes); p = 2, 3 split each task into a few entries that take every
+ * D-th pass and run side by side (D from the task's cost against 1/2 or 1/4 of
+ * the average load of an SM), which balances the queue while the columns stay
+ * in L2.
  * cfg = -1 (the default, or FT_B200_ROT_CFG unset) lets the autotuner choose:
  * the first out-of-place launch of each shape (family, direction, all sweeps or
  * heads only, fields, tasks, N, M) times every configuration once on its

@@ -1,5 +1,5 @@
-"""The rotation kernel's launch configurations (six shapes, each with or without
-the pass pipeline) and the autotuner that picks among them
+"""The rotation kernel's launch configurations (six shapes, each without the pass
+pipeline and with each of its three queue modes) and the autotuner that picks among them
 (ft_b200_set_rotation_config).  Every configuration computes the same rotations
 in the same order per element, so the transforms must agree bit for bit
 whichever runs; the first out-of-place launch of a new shape times the
@@ -9,7 +9,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-CASES = [("sph", 200, ()), ("tri", 150, (0.0, 0.0, 0.0)), ("disk", 150, (0.0, 0.0))]
+CASES = [("sph", 200, ()), ("tri", 150, (0.0, 0.0, 0.0)), ("disk", 150, (0.0, 0.0)), ("sph", 700, ())]
 
 
 @pytest.fixture(scope="module")
@@ -35,7 +35,7 @@ def transform(ft, torch, P, A, fwd, tr):
     return t.cpu().numpy()
 
 
-@pytest.mark.parametrize("kind,n,params", CASES, ids=[c[0] for c in CASES])
+@pytest.mark.parametrize("kind,n,params", CASES, ids=[f"{c[0]}{c[1]}" for c in CASES])
 def test_every_shape_bit_identical(env, kind, n, params):
     ft, torch = env
     P = make_plan(ft, kind, n, params)
@@ -43,7 +43,7 @@ def test_every_shape_bit_identical(env, kind, n, params):
     try:
         ft.set_rotation_config(-1)
         ref = {(fwd, tr): transform(ft, torch, P, A, fwd, tr) for fwd in (True, False) for tr in "NT"}
-        for cfg in list(range(6)) + list(range(8, 14)):
+        for cfg in [s + 8 * p for p in range(4) for s in range(6)]:
             ft.set_rotation_config(cfg)
             for (fwd, tr), r in ref.items():
                 assert np.array_equal(transform(ft, torch, P, A, fwd, tr), r), (kind, cfg, fwd, tr)
@@ -92,7 +92,7 @@ def test_pass_pipeline_rotation_stage_bitexact(env, kind, n, params):
         (O.hi2lo if hi2lo else O.lo2hi)(PO, r)
         refs[hi2lo] = r
     try:
-        for cfg in (8, 10, 12):
+        for cfg in (8, 10, 12, 16, 18, 24, 27):
             ft.set_rotation_config(cfg)
             for _ in range(3):
                 for hi2lo in (True, False):

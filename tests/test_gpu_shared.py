@@ -61,3 +61,33 @@ def test_blocked_round_trip_large(env):
     for A, t in zip(As, ts):
         assert rel2(t.cpu().numpy().reshape(A.shape, order="F"), A) < 4 * np.sqrt(n) * EPS * 10
     P.close()
+
+
+@pytest.mark.parametrize("kind,params,n,nf", [("sph", (), 64, 10), ("sph", (), 257, 5), ("disk", (0.0, 0.0), 96, 7),
+                                              ("tri", (0.0, 0.0, 0.0), 120, 3)])
+def test_shared_host_pipeline_matches_device_call(env, kind, params, n, nf):
+    """ft_b200_execute_shared_host (host fields in groups through three device buffers, copies
+    overlapped with the transforms) gives the device call's results bit for bit, for a sequence
+    of transforms, with uneven group sizes (10 fields: groups 2, 4, 2, 2), page-locked and
+    pageable host memory."""
+    ft, torch, O = env
+    st = torch.cuda.current_stream().cuda_stream
+    planner = {"sph": ft.plan_sph2fourier, "tri": ft.plan_tri2cheb, "disk": ft.plan_disk2cxf}[kind]
+    P = planner(n, *params)
+    As = [ft.rand_layout(kind, n, 300 + f) for f in range(nf)]
+    ops = [(True, "N"), (False, "T"), (True, "T")]
+    for prec in (ft.FP64, ft.MIXED_BF16):
+        ts = [torch.from_numpy(A.ravel(order="F").copy()).cuda() for A in As]
+        for fwd, tr in ops:
+            ft.execute_shared_dev(P, fwd, tr, [t.data_ptr() for t in ts], prec, st)
+        want = [t.cpu().numpy() for t in ts]
+        pageable = [A.copy(order="F") for A in As]
+        ft.execute_shared_host(P, ops, pageable, prec)
+        pinned = [torch.from_numpy(A.ravel(order="F").copy()).pin_memory() for A in As]
+        ft.execute_shared_host(P, ops, [h.data_ptr() for h in pinned], prec)
+        for f in range(nf):
+            assert np.array_equal(pageable[f].ravel(order="F"), want[f]), (prec, f)
+            assert np.array_equal(pinned[f].numpy(), want[f]), (prec, f)
+    with pytest.raises(ft.FTB200Error):
+        ft.execute_shared_host(P, [(True, "X")], [As[0].copy(order="F")], ft.FP64)
+    P.close()
