@@ -480,3 +480,52 @@ class Reference:
         p = P.contents
         get = lambda q: np.ctypeslib.as_array(q, shape=(n * n,)).reshape(n, n, order="F").copy()
         return [get(p.P[i]) for i in range(p.NP)], [get(p.Pinv[i]) for i in range(p.NP)]
+
+
+QUAD_SO = os.path.join(HERE, "_build", "libft_quad.so")
+
+
+class Quad:
+    """The __float128 restatement of the rotation tables, the default sweep kernels and (sph,
+    disk) the forward transform 'N' (oracle/ft_quad.c), on selected columns."""
+
+    KIND = {"sph": 0, "tri": 1, "disk": 2}
+
+    @staticmethod
+    def available(path: str = QUAD_SO) -> bool:
+        return os.path.exists(path)
+
+    def __init__(self, path: str = QUAD_SO):
+        L = self.lib = C.CDLL(path)
+        dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int)
+        L.quad_columns.restype = C.c_int
+        L.quad_columns.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, dp, C.c_longlong, ip, C.c_int,
+                                   C.c_int, dp, dp, dp, dp]
+        L.quad_table_column.restype = None
+        L.quad_table_column.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, dp, dp, dp, dp]
+
+    def columns(self, kind: str, A: np.ndarray, cols, params=(), hi2lo: bool = True, P=None):
+        """Columns `cols` of A (N x M, Fortran order) through the rotation stage (P None) or the
+        forward transform 'N' with connection matrices P = (P0, P1) (n x n, Fortran order).
+        Returns (hi, lo), N x len(cols) each: the quad result rounded to double, and the rest."""
+        n = A.shape[0]
+        a = tuple(params) + (0.0,) * (3 - len(params))
+        A = np.asfortranarray(A, dtype=np.float64)
+        cc = (C.c_int * max(len(cols), 1))(*[int(c) for c in cols])
+        hi = np.zeros((n, len(cols)), order="F")
+        lo = np.zeros((n, len(cols)), order="F")
+        p0 = p1 = None
+        if P is not None:
+            keep = (np.asfortranarray(P[0], dtype=np.float64), np.asfortranarray(P[1], dtype=np.float64))
+            p0, p1 = _ptr(keep[0]), _ptr(keep[1])
+        r = self.lib.quad_columns(self.KIND[kind], n, a[0], a[1], a[2], _ptr(A), n, cc, len(cols), 1 if hi2lo else 0,
+                                  p0, p1, _ptr(hi), _ptr(lo))
+        if r != 0:
+            raise RuntimeError(f"quad_columns failed ({r})")
+        return hi, lo
+
+    def table_column(self, kind: str, n: int, j: int, length: int, params=()):
+        a = tuple(params) + (0.0,) * (3 - len(params))
+        out = [np.zeros(length, order="F") for _ in range(4)]
+        self.lib.quad_table_column(self.KIND[kind], n, a[0], a[1], a[2], j, length, *[_ptr(o) for o in out])
+        return out

@@ -66,8 +66,9 @@ def test_first_launch_of_a_shape_is_tuned(env):
     second = transform(ft, torch, P, A, True, "N")
     c2 = ft.kernel_launches()
     assert np.array_equal(first, second)
-    # six shapes for sph, with and without the pipeline, one untimed and one timed launch each
-    assert (c1 - c0) - (c2 - c1) == 24, (c1 - c0, c2 - c1)
+    # six shapes for sph, each without the pipeline and in its three queue modes, one untimed
+    # and one timed launch each
+    assert (c1 - c0) - (c2 - c1) == 48, (c1 - c0, c2 - c1)
     P.close()
 
 

@@ -120,3 +120,61 @@ def test_reference_accuracy_test_at_scale(env, case):
           f"reference {rel2(ref, A):.2e} / {relinf(ref, A):.2e}, bounds {c2 * np.sqrt(n) * EPS:.2e} / {ci * n * EPS:.2e}")
     assert rel2(got, A) < max(c2 * np.sqrt(n) * EPS, 2 * rel2(ref, A))
     assert relinf(got, A) < max(ci * n * EPS, 2 * relinf(ref, A))
+
+
+QUAD_COLS = lambda M: sorted({0, 1, 2, 3, 4, 5, 6, M // 4 - 1, M // 4, M // 4 + 1, M // 4 + 2, M // 2 - 1, M // 2, M // 2 + 1,
+                              M // 2 + 2, 3 * M // 4, 3 * M // 4 + 1, M - 4, M - 3, M - 2, M - 1})
+
+
+def _host_connections(P, n):
+    """The plan's host connection matrices P[0], P[1] (the reference's, bit for bit)."""
+    import ctypes as C
+    from oracle.bind import _RefHarmonicPlan
+    hp = C.cast(C.c_void_p(P.ptr), C.POINTER(_RefHarmonicPlan)).contents
+    return [np.triu(np.ctypeslib.as_array(hp.P[i], shape=(n * n,)).reshape(n, n, order="F")) for i in range(2)]
+
+
+@pytest.mark.parametrize("kind,params,n", [("sph", (), 1024), ("sph", (), 4096), ("disk", (0.0, 0.0), 2048)])
+def test_forward_vs_quad_precision(env, kind, params, n):
+    """The plain FP64 forward transform 'N' against the __float128 oracle (oracle/ft_quad.c: the
+    reference's tables and sweeps in quad precision, with the plan's own connection matrices),
+    on columns of every class spread over all orders: within 1e-14 relative (the arithmetic
+    error of double precision; the compiled reference lies at the same distance)."""
+    ft, torch, R = env
+    from oracle.bind import Quad
+    A = ft.rand_layout(kind, n, 20261203)
+    M = A.shape[1]
+    P = _gpu_plan(ft, kind, n, params)
+    d = _dev(torch, A)
+    ft.execute_dev(P, True, "N", d.data_ptr(), n, M, torch.cuda.current_stream().cuda_stream)
+    got = _host(d, n, M)
+    cols = QUAD_COLS(M)
+    hi, _ = Quad().columns(kind, A, cols, params, True, _host_connections(P, n))
+    P.close()
+    e2, ei = rel2(got[:, cols], hi), relinf(got[:, cols], hi)
+    print(f"\n{_id((kind, params, n))} forward vs quad on {len(cols)} columns: {e2:.2e} / {ei:.2e}")
+    assert e2 <= 1e-14, e2
+
+
+@pytest.mark.parametrize("prec,bound", [("FP64", 1e-14), ("FP64_BLOCKED", 1e-13), ("MIXED_BF16", 1e-6), ("MIXED_BF16X4", 1e-6)])
+def test_shared_precisions_vs_quad_precision(env, prec, bound):
+    """Every precision of the shared-plan call (two fields of degree 2047) against the quad
+    oracle: FP64 and the blocked FP64 tile products at double-precision accuracy, the split-BF16
+    forms within the 1e-6 of the mixed-precision target."""
+    ft, torch, R = env
+    from oracle.bind import Quad
+    n = 2048
+    P = ft.plan_sph2fourier(n)
+    M = P.M
+    As = [ft.rand_layout("sph", n, 500 + f) for f in range(2)]
+    ts = [_dev(torch, A) for A in As]
+    ft.execute_shared_dev(P, True, "N", [t.data_ptr() for t in ts], getattr(ft, prec), torch.cuda.current_stream().cuda_stream)
+    cols = QUAD_COLS(M)
+    Q = Quad()
+    conn = _host_connections(P, n)
+    for A, t in zip(As, ts):
+        hi, _ = Q.columns("sph", A, cols, (), True, conn)
+        got = _host(t, n, M)[:, cols]
+        print(f"\n{prec} vs quad: {rel2(got, hi):.2e} / {relinf(got, hi):.2e}")
+        assert rel2(got, hi) <= bound, (prec, rel2(got, hi))
+    P.close()
