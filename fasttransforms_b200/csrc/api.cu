@@ -631,8 +631,12 @@ int execute_batch_chunk(HarmonicPlan * const * H, bool forward, char TRANS, doub
                         const int * M, int nf, cudaStream_t st, int precision = FT_B200_FP64) {
     BatchCtx * B = get_batch(H, N, M, nf);
     if (!B) return t_status;
-    const bool blocked = precision != FT_B200_FP64;
     const bool mixed = precision == FT_B200_MIXED_BF16 || precision == FT_B200_MIXED_BF16X4;
+    // tri's split-BF16 forms keep the sweeps in FP64 (the direct kernel) and put only its two
+    // connection multiplies on the tensor cores: the triangle's multiplies amplify a sweep
+    // error by a large factor (the sliced sweeps leave 3e-6 .. 9e-6 at degree 2047 with
+    // (0, 0, 0)), while sliced multiplies alone stay near 1e-7
+    const bool blocked = precision == FT_B200_FP64_BLOCKED || (mixed && H[0]->kind != TRI);
     const int ns = precision == FT_B200_MIXED_BF16X4 ? 4 : 3;
     const int blk = blocked ? blocked_block_size() : 0;
     if (blocked && !mixed && !B->blk_ready) {
@@ -640,7 +644,7 @@ int execute_batch_chunk(HarmonicPlan * const * H, bool forward, char TRANS, doub
         if (B->blk_tasks.d_tasks) B->allocs.push_back(B->blk_tasks.d_tasks);
         B->blk_ready = true;
     }
-    if (mixed && !B->mx_ready) {
+    if (mixed && blocked && !B->mx_ready) {
         if (!blocked_tasks_mixed(H[0]->blocked, nf, N[0], M[0], &B->mx_tasks)) return t_status;
         if (B->mx_tasks.d_tasks) B->allocs.push_back(B->mx_tasks.d_tasks);
         const size_t te = blocked_mixed_T_elems(H[0]->blocked, B->mx_tasks.ntasks, N[0]);
@@ -902,13 +906,13 @@ int shared_prepare(HarmonicPlan * H, int precision) {
         set_error(FT_B200_EINVAL, "unknown precision");
         return FT_B200_EINVAL;
     }
-    if (precision != FT_B200_FP64 && !H->blocked) {
+    const bool mixed = precision == FT_B200_MIXED_BF16 || precision == FT_B200_MIXED_BF16X4;
+    if (precision == FT_B200_FP64 || (mixed && H->kind == TRI)) return FT_B200_OK;   // no tile products
+    if (!H->blocked) {
         H->blocked = blocked_plan_build(H);
         if (!H->blocked) return t_status;
     }
-    if ((precision == FT_B200_MIXED_BF16 || precision == FT_B200_MIXED_BF16X4) &&
-        !blocked_mixed_prepare(H->blocked, precision == FT_B200_MIXED_BF16X4 ? 4 : 3))
-        return t_status;
+    if (mixed && !blocked_mixed_prepare(H->blocked, precision == FT_B200_MIXED_BF16X4 ? 4 : 3)) return t_status;
     return FT_B200_OK;
 }
 

@@ -153,10 +153,10 @@ struct RotLaunch {
     int ntasks;
     int * counter;             // device work counter (reset by the launcher)
     // Pass pipeline (null chains: each CTA runs every pass of a task itself).  Queue entry c
-    // runs passes first, first + stride, ... of task chains[c].task; pass r streams down the
-    // columns behind pass r - 1 of the same task (run by another entry, or earlier by this
-    // one), waiting on that pass's progress word prog[prog0 + r - 1] and publishing its own,
-    // prog[prog0 + r] (cleared by the launcher).
+    // runs passes first, first + stride, ... of task chains[c].task (the launcher queues one
+    // pass per entry); pass r streams down the columns behind pass r - 1 of the same task,
+    // pulled earlier from the queue, waiting on that pass's progress word prog[prog0 + r - 1]
+    // and publishing its own, prog[prog0 + r] (cleared by the launcher).
     const struct RotChain * chains;
     int nchains;
     int * prog;

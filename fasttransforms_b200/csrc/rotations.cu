@@ -40,7 +40,6 @@
 #include <type_traits>
 
 #include <map>
-#include <tuple>
 #include <mutex>
 #include <string>
 
@@ -556,11 +555,10 @@ cudaError_t launch_kind(int cfg, const RotLaunch & L, int max_ctas, cudaStream_t
 
 int g_rot_cfg = -2;
 
-// A configuration is a launch shape 0 .. 5 plus 8 x a pass-pipeline mode 0 .. 3
-// (schedule_chains).  FT_B200_ROT_CFG forces one (as does ft_b200_set_rotation_config);
-// otherwise -1 (chosen per launch shape).
-constexpr int kPipeModes = 4;
-bool valid_config(int cfg) { return cfg >= 0 && (cfg & 7) <= 5 && cfg < 8 * kPipeModes; }
+// A configuration is a launch shape 0 .. 5, plus 8 to run through the pass pipeline.
+// FT_B200_ROT_CFG forces one (as does ft_b200_set_rotation_config); otherwise -1 (chosen
+// per launch shape).
+bool valid_config(int cfg) { return cfg >= 0 && (cfg & 7) <= 5 && cfg < 16; }
 
 int rotation_config() {
     if (g_rot_cfg == -2) {
@@ -576,7 +574,7 @@ void set_rotation_config(int cfg) { g_rot_cfg = valid_config(cfg) ? cfg : -1; }
 struct RotSchedule {
     std::vector<RotTask> tasks;                          // host copy of the device list (same order)
     struct Units { RotChain * d_chains = nullptr; int * d_prog = nullptr; int n = 0, nprog = 0; };
-    std::map<std::tuple<int, int, int>, Units> lists;    // (sweeps per pass, heads only, pipeline mode) -> queue
+    std::map<std::pair<int, int>, Units> lists;          // (sweeps per pass, heads only) -> queue
     std::mutex mu;
 };
 
@@ -624,44 +622,32 @@ int rotation_device_error() {
 
 namespace {
 
-// Sweeps per pass (W x B), stage warps W and sweeps per warp B of each launch shape.
+// Sweeps per pass (W x B) of each launch shape.
 int shape_pass(int cfg) {
     static const int wb[6] = {64, 64, 32, 32, 16, 32};
     return (cfg >= 0 && cfg < 6) ? wb[cfg] : 64;
 }
-int shape_warps(int cfg) {
-    static const int w[6] = {8, 16, 8, 8, 4, 4};
-    return (cfg >= 0 && cfg < 6) ? w[cfg] : 8;
-}
-int shape_sweeps(int cfg) { return shape_pass(cfg) / shape_warps(cfg); }
 
-// The queue of the pass pipeline for L's tasks with passes of wb sweeps (pipeline mode pm,
-// ctas resident CTAs), built on first use; null when the stream is capturing then (the upload
-// synchronises) or on an allocation failure.  Every entry's passes wait only on passes of the
-// same task, and a task's entries are adjacent in the queue, so at most one task is ever
-// partly pulled: every other running entry can finish, and the queue cannot deadlock while
-// that task's entries fit in the other CTAs (stride <= ctas / 2).
-//   pm 1: one entry per pass, pass-major (every task's pass r before any task's pass r + 1):
-//         a pass never waits long for its predecessor, but consecutive passes of a task run far
-//         apart in time, so its columns leave L2 between them when the matrix is large;
-//   pm 2, 3: task t in D_t entries (entry d runs passes d, d + D_t, ..), D_t from the task's
-//         cost (its passes' steps) against a target of 1/2 (pm 2) or 1/4 (pm 3) of the average
-//         load of a CTA; the entries of a task run side by side, a few chunks apart, so the
-//         columns stay in L2, and long tasks no longer leave SMs idle at the end of the queue.
-const RotSchedule::Units * schedule_chains(RotSchedule * S, int kind, const RotLaunch & L, int wb, int B, int pm, int ctas,
-                                           cudaStream_t st) {
+// The queue of the pass pipeline for L's tasks with passes of wb sweeps, built on first use;
+// null when the stream is capturing then (the upload synchronises) or on an allocation
+// failure.  One entry per pass, pass-major (every task's pass r before any task's pass r + 1,
+// tasks in list order, longest first), so a pass's predecessor is always pulled first: a
+// pass rarely waits long for it, but consecutive passes of a task run far apart in time, so
+// its columns leave L2 between them when the matrix is large.  (Splitting each task into a
+// few entries that take every D-th pass side by side, which keeps the columns in L2, measured
+// slower at every size: a CTA whose entry waits for its task's previous pass cannot take
+// other work meanwhile.)
+const RotSchedule::Units * schedule_passes(RotSchedule * S, int kind, const RotLaunch & L, int wb, cudaStream_t st) {
     const int blk = L.fields[0].blk;
     std::lock_guard<std::mutex> lk(S->mu);
-    const auto key = std::make_tuple(wb, blk > 0 ? 1 : 0, pm);
+    const auto key = std::make_pair(wb, blk > 0 ? 1 : 0);
     auto it = S->lists.find(key);
     if (it != S->lists.end()) return it->second.d_chains ? &it->second : nullptr;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return nullptr;
     const int nt = (int) S->tasks.size();
     std::vector<int> npass(nt, 0), prog0(nt, 0);
-    std::vector<double> cost(nt, 0.0);
     int nprog = 0, maxp = 0;
-    double total = 0.0;
     for (int t = 0; t < nt; ++t) {
         const RotTask & T = S->tasks[t];
         const RotField & F = L.fields[T.field];
@@ -671,34 +657,11 @@ const RotSchedule::Units * schedule_chains(RotSchedule * S, int kind, const RotL
         prog0[t] = nprog;
         nprog += npass[t];
         maxp = std::max(maxp, npass[t]);
-        // steps of its passes: a pass covers the longest of its sweeps plus the wavefront's
-        // skew (2 steps per sweep); with chunk granularity this is the kernel's work to a few %
-        const int step = Geo::step(kind);
-        for (int r = 0; r < npass[t]; ++r) {
-            const int jlong = std::max(jlo, jhi - step * (std::min(nsw, (r + 1) * wb) - 1));   // lowest order of pass r
-            cost[t] += std::max(0, Geo::top(kind, F.N, jlong, 0) + 1) + 2.0 * std::min(wb, nsw - r * wb) + B;
-        }
-        total += cost[t];
     }
-    std::vector<RotChain> q;
-    if (pm == 1) {
-        for (int r = 0; r < maxp; ++r)
-            for (int t = 0; t < nt; ++t)
-                if (r < npass[t]) q.push_back(RotChain{t, prog0[t], r, npass[t]});
-    } else {
-        const double target = (pm == 2 ? 0.5 : 0.25) * total / std::max(1, ctas);
-        const int dmax = std::max(1, ctas / 2);
-        std::vector<std::pair<double, int>> order;   // (entry duration, task), longest first
-        std::vector<int> D(nt, 1);
-        for (int t = 0; t < nt; ++t) {
-            if (npass[t] == 0) continue;
-            D[t] = std::max(1, std::min({npass[t], dmax, (int) std::lround(cost[t] / std::max(target, 1.0))}));
-            order.push_back({cost[t] / D[t], t});
-        }
-        std::stable_sort(order.begin(), order.end(), [](const auto & a, const auto & b) { return a.first > b.first; });
-        for (auto & o : order)
-            for (int d = 0; d < D[o.second]; ++d) q.push_back(RotChain{o.second, prog0[o.second], d, D[o.second]});
-    }
+    std::vector<RotChain> q;   // entry: pass r of task t alone (stride npass)
+    for (int r = 0; r < maxp; ++r)
+        for (int t = 0; t < nt; ++t)
+            if (r < npass[t]) q.push_back(RotChain{t, prog0[t], r, npass[t]});
     RotSchedule::Units U;
     U.n = (int) q.size();
     U.nprog = nprog;
@@ -725,20 +688,12 @@ cudaError_t launch_with(int kind, bool hi2lo, int cfg, const RotLaunch & L, int 
     return cudaErrorInvalidValue;
 }
 
-// One launch in configuration cfg: shape cfg & 7, through the pass pipeline in mode cfg >> 3
-// (schedule_chains; 0: none) when the task list has a schedule (else each CTA runs every pass
-// of its tasks).
+// One launch in configuration cfg: shape cfg & 7, through the pass pipeline when cfg & 8
+// and the task list has a schedule (else each CTA runs every pass of its tasks).
 cudaError_t launch_shape(int kind, bool hi2lo, int cfg, const RotLaunch & L, int max_ctas, cudaStream_t st,
                          RotSchedule * sched) {
-    const int shape = cfg & 7, pm = cfg >> 3;
-    const RotSchedule::Units * U = nullptr;
-    if (pm > 0 && sched) {
-        int dev = 0, sms = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        const int ctas = sms * (shape_warps(shape) <= 4 ? 2 : 1);
-        U = schedule_chains(sched, kind, L, shape_pass(shape), shape_sweeps(shape), pm, max_ctas > 0 ? std::min(ctas, max_ctas) : ctas, st);
-    }
+    const int shape = cfg & 7;
+    const RotSchedule::Units * U = ((cfg & 8) && sched) ? schedule_passes(sched, kind, L, shape_pass(shape), st) : nullptr;
     if (!U) return launch_with(kind, hi2lo, shape, L, max_ctas, st);
     static thread_local RotLaunch P;
     P = L;
@@ -796,9 +751,9 @@ int tune(int kind, bool hi2lo, const RotLaunch & L, double * const * dead, int m
     // every shape, each also through the pass pipeline when the list has a schedule (it
     // spreads a task's passes over SMs: worth it when there are few tasks, not when the
     // columns would leave L2 between passes)
-    for (int cfg = 0; cfg < 8 * kPipeModes; ++cfg) {
+    for (int cfg = 0; cfg < 16; ++cfg) {
         if ((cfg & 7) > 5 || ((kind == TRI || kind == RECT) && (cfg & 7) == 1)) continue;   // tri, rect: shape 1 not built
-        if ((cfg >> 3) && !sched) continue;
+        if ((cfg & 8) && !sched) continue;
         if (launch_shape(kind, hi2lo, cfg, S, max_ctas, st, sched) != cudaSuccess) { best = -1; break; }
         if (cudaEventRecord(e0, st) != cudaSuccess) { best = -1; break; }
         if (launch_shape(kind, hi2lo, cfg, S, max_ctas, st, sched) != cudaSuccess) { best = -1; break; }

@@ -453,11 +453,13 @@ int ft_b200_execute_noalloc_dev(const ft_harmonic_plan * P, int forward, char TR
  * two transposes, its normalisation in FP64).  Relative 2-norm error against
  * the FP64 transform about 5e-7 for sph at n = 4096; the connection
  * multiplies amplify the sweeps' error by a factor that depends on the family
- * and its parameters (up to about 3e-5 for tri with generic parameters at
- * n = 2048).
+ * and its parameters (disk with generic parameters about 3e-6 at n = 2048).
+ * tri keeps its sweeps in FP64 (direct) in both split-BF16 forms and runs only
+ * its two connection multiplies on the tensor cores: its multiplies would
+ * amplify a sliced sweep's error to 3e-6 .. 3e-5; this way about 1e-7.
  * precision FT_B200_MIXED_BF16X4: four slices in the blocks (ten products)
  * and four of the input in the connection multiply: about 1.4e-7 for sph at
- * n = 2048 (up to about 9e-6 for tri with generic parameters).  The first call of either builds its slice images
+ * n = 2048.  The first call of either builds its slice images
  * of the tiles and of the connection matrices (about 1 GB at n = 4096). */
 #define FT_B200_FP64 0
 #define FT_B200_FP64_BLOCKED 1
@@ -510,18 +512,13 @@ int ft_b200_profile(int enable);
 int ft_b200_profile_read(int family, double * ms, int * launches);
 
 /* Launch configuration of the rotation kernel (no counterpart in the reference,
- * whose kernels have no launch shape).  cfg = s + 8 p forces shape s = 0 .. 5
+ * whose kernels have no launch shape).  cfg = s or s + 8 forces shape s = 0 .. 5
  * (warps x sweeps per warp x chunk: 8 x 8 x 16, 16 x 4 x 8, 8 x 4 x 8, 8 x 4 x 16,
  * 4 x 4 x 16 and 4 x 8 x 16, the last two with as many CTAs per SM as fit; tri has
- * no 16 x 4 x 8 and runs 8 x 8 x 16 for it) and pass-pipeline mode p = 0 .. 3.
- * p = 0: each CTA runs all passes (of 16 .. 64 sweeps) of the tasks it takes.
- * p > 0: a pass streams down the columns right behind the task's previous pass,
- * run by another CTA; p = 1 queues every pass as its own entry, pass-major (for
- * inputs with fewer tasks than SMs; it loses where the columns would leave L2
- * between passes); p = 2, 3 split each task into a few entries that take every
- * D-th pass and run side by side (D from the task's cost against 1/2 or 1/4 of
- * the average load of an SM), which balances the queue while the columns stay
- * in L2.
+ * no 16 x 4 x 8 and runs 8 x 8 x 16 for it); + 8 runs the pass pipeline, where
+ * each pass of 16 .. 64 sweeps of a task is its own work unit and streams down the
+ * columns on another SM right behind the previous pass (for inputs with fewer
+ * tasks than SMs; it loses where the columns would leave L2 between passes).
  * cfg = -1 (the default, or FT_B200_ROT_CFG unset) lets the autotuner choose:
  * the first out-of-place launch of each shape (family, direction, all sweeps or
  * heads only, fields, tasks, N, M) times every configuration once on its
