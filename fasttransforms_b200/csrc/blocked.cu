@@ -298,7 +298,11 @@ constexpr int MX_TMEM_COLS = 512;                     // 2 chains x 4 levels x W
 
 template <int NS> struct MxCfg {
     static constexpr int QCHAIN = NS * MX_QPIECE;     // one chain's tile image
-    static constexpr size_t SMEM = 2 * NS * (size_t) MX_PIECE + 2 * (size_t) QCHAIN + 1024;
+    // the positions entering the next window, per chain and buffer: 8 quads x MX_COLS columns
+    // (FP32), bulk-copied one tile ahead where shared memory allows (three slices)
+    static constexpr bool ROWS = NS == 3;
+    static constexpr int ROWBUF = 8 * MX_COLS * 16;
+    static constexpr size_t SMEM = 2 * NS * (size_t) MX_PIECE + 2 * (size_t) QCHAIN + (ROWS ? 4 * (size_t) ROWBUF : 0) + 1024;
     static_assert(SMEM <= 227 * 1024, "shared memory");
 };
 
@@ -384,7 +388,10 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
     unsigned char * const sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t) 1023);
     unsigned char * const Xs = sm;                        // [chain][piece]: MX_COLS rows x WIN slots
     unsigned char * const Qs = sm + 2 * NS * MX_PIECE;    // [chain]: the chain's tile image
+    float4 * const Rs = reinterpret_cast<float4 *>(Qs + 2 * QCHAIN);   // [chain][buffer][quad][column]: entering positions
+    constexpr bool ROWS = MxCfg<NS>::ROWS;
     __shared__ __align__(8) uint64_t bar_qfull[2], bar_qempty[2], bar_xready[2], bar_acc[2], bar_pmax[2], bar_block[2], bar_done;
+    __shared__ __align__(8) uint64_t bar_rows[2][2];   // [chain][buffer]: entering positions landed
     __shared__ uint32_t s_tmem;
     __shared__ int s_task;
     __shared__ volatile int s_abort;
@@ -401,6 +408,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
             tc::mbar_init(&bar_acc[i], 1);
         }
         tc::mbar_init(&bar_done, 1);
+        for (int i = 0; i < 4; ++i) tc::mbar_init(&bar_rows[i >> 1][i & 1], 1);
         s_abort = 0;
     }
     if (warp == 16) tc::tmem_alloc(&s_tmem, MX_TMEM_COLS);
@@ -420,6 +428,8 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
     unsigned pp = 0;                 // window-maximum exchanges (epilogue, own chain)
     unsigned bs = 0;                 // block boundaries passed (epilogue, own chain)
     int last_u = -1;                 // loader: last use of the chain buffers
+    unsigned rk = 0;                 // entering-position copies of the own chain so far (epilogue, finishing half)
+    unsigned rk_issued = 0;          // the same, issued (the chain's issuing thread)
 
     for (;;) {
         if (tid == 0) s_task = atomicAdd(L.counter, 1);
@@ -513,6 +523,33 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
             const uint32_t tacc = tmem + ((uint32_t) (quarter * 32) << 16) + c * NL * WIN + 32 * hf;
             float scale = 1.0f;   // slicing scale of the window the products in flight were computed from
             // 32 positions from pos0 (a multiple of 32): 8 quads, zero outside the copy
+            // entering positions: one thread of the finishing half bulk-copies the 32 positions
+            // from pos0 (a multiple of 32) for all MX_COLS columns, 8 quads x MX_COLS float4,
+            // contiguous in the task-major copy, into buffer rk & 1 of the chain (fewer quads at the
+            // end of the copy, none before its start); the half's threads read them back from there
+            const bool issuer = ROWS && hf == fh && quarter == 0 && lane == 0;
+            float4 * const Tq0 = Tq - r;                  // column 0 of this chain's quads
+            auto issue_rows = [&](int pos0, unsigned idx) {
+                const int q0 = pos0 >> 2;
+                const int nq = pos0 < 0 ? 0 : max(0, min(8, L.Lq - q0));
+                uint64_t * const bar = &bar_rows[c][idx & 1];
+                asm volatile("fence.proxy.async.global;\n" ::: "memory");   // the positions were written through the generic proxy
+                tc::mbar_arrive_expect_tx(bar, (uint32_t) (nq * MX_COLS * 16));
+                if (nq > 0) tc::bulk_g2s(Rs + ((c * 2 + (idx & 1)) * 8) * MX_COLS, Tq0 + (long long) q0 * MX_COLS,
+                                         (uint32_t) (nq * MX_COLS * 16), bar);
+                rk_issued = idx + 1;
+            };
+            auto read_rows = [&](int pos0, unsigned idx, float * v) -> bool {
+                if (!tc::mbar_wait(&bar_rows[c][idx & 1], (idx >> 1) & 1, &s_abort)) { fail(); return false; }
+                const float4 * const buf = Rs + ((c * 2 + (idx & 1)) * 8) * MX_COLS + r;
+#pragma unroll
+                for (int qd = 0; qd < TL / 4; ++qd) {
+                    const int P = pos0 + 4 * qd;
+                    const float4 x = (P >= 0 && P < Pend) ? buf[qd * MX_COLS] : make_float4(0.f, 0.f, 0.f, 0.f);
+                    v[4 * qd] = x.x; v[4 * qd + 1] = x.y; v[4 * qd + 2] = x.z; v[4 * qd + 3] = x.w;
+                }
+                return true;
+            };
             auto load32 = [&](int pos0, float * v) {
 #pragma unroll
                 for (int qd = 0; qd < TL / 4; ++qd) {
@@ -557,6 +594,9 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
                 const int kmax = L.kmax[p * L.nbeta + beta];
                 const int nk = kmax + 2;
                 float src[TL];
+                // the positions entering the second window (tile 0's), ahead of the first window
+                auto enter_pos = [&](int kk) { const int lk = kk * TL; return HI2LO ? lk - TL : lk + WIN; };
+                if (issuer && nk > 1) issue_rows(enter_pos(HI2LO ? kmax : -1), rk);
                 {   // first tile: the whole window
                     const int pos0 = (HI2LO ? kmax : -1) * TL + TL * hf;
                     load32(pos0, src);
@@ -576,8 +616,13 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
                         const int qhi = min((ppos + TL) >> 2, L.Lq);
                         if (qhi > qlo) tc::prefetch_l2(Tq - r + (long long) qlo * MX_COLS, (uint32_t) (qhi - qlo) * MX_COLS * 16);
                     }
-                    // the finishing half brings the positions entering the next tile
-                    if (!last && hf == fh) load32(npos, src);
+                    // the finishing half brings the positions entering the next tile (with ROWS,
+                    // one tile ahead into shared memory, read back before the next window is cut)
+                    if (ROWS) {
+                        if (issuer && ki + 2 < nk) issue_rows(enter_pos(HI2LO ? k - 1 : k + 1), rk + 1);
+                    } else if (!last && hf == fh) {
+                        load32(npos, src);
+                    }
                     if (!tc::mbar_wait(&bar_acc[c], ac & 1, &s_abort)) { fail(); break; }
                     ac++;
                     __syncwarp();
@@ -610,10 +655,15 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
                     }
                     // next window: the overlap stays in its slots, the entering positions take
                     // the finished ones' slots
+                    if (ROWS && !last && hf == fh) {
+                        if (!read_rows(npos, rk, src)) break;
+                        rk++;
+                    }
                     if (!last && !put32(hf == fh ? npos : lo + TL * hf, src)) break;
                 }
                 // block boundary: the next block's first window reads rows of global memory that
                 // the other half of this chain's threads wrote
+                asm volatile("fence.proxy.async.global;\n" ::: "memory");   // stores visible to the next block's bulk copies
                 tc::mbar_arrive(&bar_block[c]);
                 if (!tc::mbar_wait(&bar_block[c], bs & 1, &s_abort)) { fail(); break; }
                 bs++;
@@ -628,6 +678,11 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
     __syncthreads();
     if (warp == 17 && lane == 0 && s_abort && last_u >= 0) {
         for (int c = 0; c < 2; ++c) (void) tc::mbar_wait(&bar_qfull[c], last_u & 1, &s_never);
+    }
+    if (ROWS && s_abort && lane == 0 && warp < 16 && (warp & 7) == 4 * (HI2LO ? 1 : 0)) {
+        // a chain's issuing thread: its last two entering-position copies (one per buffer)
+        for (unsigned i = rk_issued >= 2 ? rk_issued - 2 : 0; i < rk_issued; ++i)
+            (void) tc::mbar_wait(&bar_rows[warp >> 3][i & 1], (i >> 1) & 1, &s_never);
     }
     if (warp == 16) {
         if (lane == 0) {
