@@ -387,13 +387,18 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
 #pragma unroll
                 for (int v = 0; v < PER_W; ++v) b0[soff[v]] = pre[v];
             };
+            // the pass pipeline publishes progress every kPub stored chunks (and after the last):
+            // a fence and a release per chunk cost as much as the chunk's sweeps, and a pass that
+            // trails its predecessor by a few chunks more loses nothing
+            constexpr int kPub = 4;
+            auto publishes = [&](int k) { return k % kPub == kPub - 1 || k == K - 1; };
             auto store_chunk = [&](int k) {
                 const int pmin = pmin_of(k, true);
                 const double * const bw = buf(WA, k & 1, 0, 0);
 #pragma unroll
                 for (int v = 0; v < PER_W; ++v)
                     if (row_ok(pmin, v)) __stcg(gdst[v] + (long long) ES * CH * pmin, bw[soff[v]]);
-                if (pipe) __threadfence();   // before the barrier after which they are published
+                if (pipe && publishes(k)) __threadfence();   // before the barrier after which they are published
             };
             if (pipe) {
                 if (threadIdx.x == 0) {
@@ -485,8 +490,8 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
                 if (it + 1 < K) stash_chunk(it + 1);
                 if (pipe && threadIdx.x == 0) wait_chunk(it + 2);   // loaded next iteration
                 __syncthreads();
-                // the chunk stored this iteration is final: publish it
-                if (pipe && threadIdx.x == 0 && it - WA >= 0 && it - WA < K) {
+                // the chunks stored up to this iteration are final: publish them
+                if (pipe && threadIdx.x == 0 && it - WA >= 0 && it - WA < K && publishes(it - WA)) {
                     const int pmin = pmin_of(it - WA, true);
                     publish_progress(my_prog, HI2LO ? -pmin : pmin + E - 1);
                 }

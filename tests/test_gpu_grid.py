@@ -422,3 +422,38 @@ def test_tet_grid_host_entry_points_and_errors(env):
         P.close()
     assert not ft.lib.ft_plan_tet_synthesis(8, 8, 9, 0)      # L = M = N required
     assert ft.lib.ft_b200_last_status() == 1                  # FT_B200_EINVAL
+
+
+# FFTW's r2r kind constants (fftw3.h): the values ft_plan_*_with_kind takes
+FFTW_R2HC, FFTW_HC2R, FFTW_REDFT01, FFTW_REDFT10, FFTW_RODFT01, FFTW_RODFT10 = 0, 1, 4, 5, 8, 9
+
+
+@pytest.mark.parametrize("kinds", [("REDFT01", "REDFT01"), ("RODFT01", "RODFT01"), ("REDFT10", "REDFT10"),
+                                   ("RODFT10", "REDFT10")])
+def test_sph_plan_with_kind_vs_oracle(env, kinds):
+    """ft_plan_sph_with_kind (src/fftw.c:76-102) with theta kinds other than the standard plans'
+    (classes {0, 3} and {1, 2} of one type): both sequences and both TRANS against the oracle's
+    sequences with the same kinds.  The phi kind passed (R2HC / HC2R) is accepted; the row DFT's
+    direction follows the sequence run (synthesis: half-complex to real, analysis: real to
+    half-complex)."""
+    import ctypes as C
+    ft, torch = env
+    from oracle import grid as G
+    code = {"REDFT01": FFTW_REDFT01, "REDFT10": FFTW_REDFT10, "RODFT01": FFTW_RODFT01, "RODFT10": FFTW_RODFT10}
+    N, M = 33, 65
+    X = np.random.default_rng(7).uniform(-1, 1, (N, M))
+    phi = FFTW_HC2R if kinds[0].endswith("01") else FFTW_R2HC
+    k = (C.c_int * 3)(code[kinds[0]], code[kinds[1]], phi)
+    ptr = ft.lib.ft_plan_sph_with_kind(N, M, k, 0)
+    assert ptr, ft.lib.ft_b200_last_error()
+    P = ft.SphereGridPlan(ptr, "sph_with_kind", N, M)
+    G.PLANS["with_kind_test"] = kinds
+    try:
+        for op in ("sph_synthesis", "sph_analysis"):
+            for tr in "NT":
+                got = run_dev(ft, torch, P, op, tr, X)
+                want = G.execute(op, tr, "with_kind_test", X)
+                assert rel2(got, want) <= 1e-14, (kinds, op, tr, rel2(got, want))
+    finally:
+        del G.PLANS["with_kind_test"]
+        P.close()
