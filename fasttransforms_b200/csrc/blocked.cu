@@ -367,11 +367,10 @@ __device__ __forceinline__ void slice8(const float * v, float s, uint4 * out) {
         float t0 = v[2 * q] * s, t1 = v[2 * q + 1] * s;
 #pragma unroll
         for (int a = 0; a < NS; ++a) {
-            const float i0 = rintf(t0), i1 = rintf(t1);
-            const __nv_bfloat162 b = __floats2bfloat162_rn(i0, i1);
-            w[a][q] = *reinterpret_cast<const uint32_t *>(&b);
-            t0 = (t0 - i0) * 512.0f;
-            t1 = (t1 - i1) * 512.0f;
+            const float i0 = tc::round_small(t0), i1 = tc::round_small(t1);
+            w[a][q] = tc::pack_bf16_ints(i0, i1);
+            t0 = __fmul_rn(__fsub_rn(t0, i0), 512.0f);   // exact: |t - i| <= 1/2, times a power of two
+            t1 = __fmul_rn(__fsub_rn(t1, i1), 512.0f);
         }
     }
 #pragma unroll

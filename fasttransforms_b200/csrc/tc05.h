@@ -116,6 +116,21 @@ __device__ __forceinline__ void tmem_ld8_async(uint32_t taddr, uint32_t * r) {
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
 
+// ---- integer slices at the full FP32 rate ----
+// Nearest integer, ties to even, for |t| < 2^22: adding 1.5 * 2^23 leaves a value whose unit in
+// the last place is 1, so the addition rounds t to an integer; subtracting it back is exact.
+// (rintf gives the same value, up to the sign of a zero result, through a conversion-class
+// instruction that runs at an eighth of the FP32 rate.)
+__device__ __forceinline__ float round_small(float t) {
+    return __fsub_rn(__fadd_rn(t, 12582912.0f), 12582912.0f);
+}
+// Two integer-valued floats with at most 8 significant bits (|i| <= 256) as a BF16 pair (lo in
+// the low half): their FP32 words end in 16 zero bits, so the BF16 values are the high halves
+// exactly; a byte permute instead of a conversion-class instruction.
+__device__ __forceinline__ uint32_t pack_bf16_ints(float lo, float hi) {
+    return __byte_perm(__float_as_uint(lo), __float_as_uint(hi), 0x7632);
+}
+
 // ---- mbarriers ----
 __device__ __forceinline__ void mbar_init(uint64_t * bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" :: "r"(smem_addr(bar)), "r"(count) : "memory");

@@ -95,11 +95,10 @@ __device__ __forceinline__ void slice8(const float * t_in, uint4 * out) {
         float t0 = t_in[2 * q], t1 = t_in[2 * q + 1];
 #pragma unroll
         for (int a = 0; a < NS; ++a) {
-            const float i0 = rintf(t0), i1 = rintf(t1);
-            const __nv_bfloat162 b = __floats2bfloat162_rn(i0, i1);
-            w[a][q] = *reinterpret_cast<const uint32_t *>(&b);
-            t0 = (t0 - i0) * 256.0f;
-            t1 = (t1 - i1) * 256.0f;
+            const float i0 = tc::round_small(t0), i1 = tc::round_small(t1);
+            w[a][q] = tc::pack_bf16_ints(i0, i1);
+            t0 = __fmul_rn(__fsub_rn(t0, i0), 256.0f);   // exact: |t - i| <= 1/2, times a power of two
+            t1 = __fmul_rn(__fsub_rn(t1, i1), 256.0f);
         }
     }
 #pragma unroll
