@@ -134,7 +134,7 @@ def _run_c_caller(tmp_path, src):
 
 
 @pytest.mark.skipif(has_gpu(), reason="checks the no-device path; the device run is the gpu-marked twin")
-@pytest.mark.parametrize("src", ["dropin.c", "families.c"])
+@pytest.mark.parametrize("src", ["dropin.c", "families.c", "shared_host.c"])
 def test_c_caller_compiles_links_and_runs(tmp_path, src):
     """C programs written against the reference's API (tests/c/dropin.c: sph2fourier;
     tests/c/families.c: every other family and the grids) compile, link and, without a usable
@@ -145,10 +145,11 @@ def test_c_caller_compiles_links_and_runs(tmp_path, src):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("src", ["dropin.c", "families.c"])
+@pytest.mark.parametrize("src", ["dropin.c", "families.c", "shared_host.c"])
 def test_c_caller_round_trips_on_device(tmp_path, src):
     """The same C programs on an sm_100 device: every transform they call returns its input
-    (dropin.c prints the sph2fourier round-trip error, below 1e-13; families.c prints "ok")."""
+    (dropin.c and shared_host.c print the sph round-trip error, below 1e-13; families.c prints
+    "ok")."""
     r = _run_c_caller(tmp_path, src)
     assert r.returncode == 0, r.stderr
     out = r.stdout.strip()
