@@ -41,6 +41,7 @@
 
 #include <map>
 #include <mutex>
+#include <tuple>
 #include <string>
 
 #include "ft_internal.h"
@@ -560,10 +561,11 @@ cudaError_t launch_kind(int cfg, const RotLaunch & L, int max_ctas, cudaStream_t
 
 int g_rot_cfg = -2;
 
-// A configuration is a launch shape 0 .. 5, plus 8 to run through the pass pipeline.
-// FT_B200_ROT_CFG forces one (as does ft_b200_set_rotation_config); otherwise -1 (chosen
-// per launch shape).
-bool valid_config(int cfg) { return cfg >= 0 && (cfg & 7) <= 5 && cfg < 16; }
+// A configuration is a launch shape 0 .. 5 plus 8 x a pass-pipeline mode 0 .. 2
+// (schedule_passes).  FT_B200_ROT_CFG forces one (as does ft_b200_set_rotation_config);
+// otherwise -1 (chosen per launch shape).
+constexpr int kPipeModes = 3;
+bool valid_config(int cfg) { return cfg >= 0 && (cfg & 7) <= 5 && cfg < 8 * kPipeModes; }
 
 int rotation_config() {
     if (g_rot_cfg == -2) {
@@ -579,7 +581,7 @@ void set_rotation_config(int cfg) { g_rot_cfg = valid_config(cfg) ? cfg : -1; }
 struct RotSchedule {
     std::vector<RotTask> tasks;                          // host copy of the device list (same order)
     struct Units { RotChain * d_chains = nullptr; int * d_prog = nullptr; int n = 0, nprog = 0; };
-    std::map<std::pair<int, int>, Units> lists;          // (sweeps per pass, heads only) -> queue
+    std::map<std::tuple<int, int, int>, Units> lists;    // (sweeps per pass, heads only, mode) -> queue
     std::mutex mu;
 };
 
@@ -642,10 +644,14 @@ int shape_pass(int cfg) {
 // few entries that take every D-th pass side by side, which keeps the columns in L2, measured
 // slower at every size: a CTA whose entry waits for its task's previous pass cannot take
 // other work meanwhile.)
-const RotSchedule::Units * schedule_passes(RotSchedule * S, int kind, const RotLaunch & L, int wb, cudaStream_t st) {
+// mode 2 (bounded): pass-major over only the longest tasks whose columns fit in half the L2
+// (so consecutive passes of a task still find them there), then every other task as one
+// entry running all its passes, longest first: the long tasks no longer end the launch alone,
+// and the short ones fill in at the end.
+const RotSchedule::Units * schedule_passes(RotSchedule * S, int kind, const RotLaunch & L, int wb, int mode, cudaStream_t st) {
     const int blk = L.fields[0].blk;
     std::lock_guard<std::mutex> lk(S->mu);
-    const auto key = std::make_pair(wb, blk > 0 ? 1 : 0);
+    const auto key = std::make_tuple(wb, blk > 0 ? 1 : 0, mode);
     auto it = S->lists.find(key);
     if (it != S->lists.end()) return it->second.d_chains ? &it->second : nullptr;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -663,10 +669,24 @@ const RotSchedule::Units * schedule_passes(RotSchedule * S, int kind, const RotL
         nprog += npass[t];
         maxp = std::max(maxp, npass[t]);
     }
-    std::vector<RotChain> q;   // entry: pass r of task t alone (stride npass)
+    // tasks pipelined pass by pass: all (mode 1), or the longest ones (the list is longest first)
+    // whose columns fit in half the L2 (mode 2)
+    int npipe = nt;
+    if (mode == 2) {
+        int dev = 0, l2 = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev);
+        const int seqs = (kind == TRI || kind == RECT) ? 1 : (kind == SPIN ? 4 : 2);   // doubles per order and row
+        const long long cols = (long long) Geo::task_orders(kind) * seqs;
+        const long long foot = cols * (long long) L.fields[0].N * (long long) sizeof(double);
+        npipe = (int) std::min<long long>(nt, std::max<long long>(1, (l2 / 2) / std::max<long long>(foot, 1)));
+    }
+    std::vector<RotChain> q;   // entry: pass r of task t alone (stride npass), or all of its passes
     for (int r = 0; r < maxp; ++r)
-        for (int t = 0; t < nt; ++t)
+        for (int t = 0; t < npipe; ++t)
             if (r < npass[t]) q.push_back(RotChain{t, prog0[t], r, npass[t]});
+    for (int t = npipe; t < nt; ++t)
+        if (npass[t] > 0) q.push_back(RotChain{t, prog0[t], 0, 1});
     RotSchedule::Units U;
     U.n = (int) q.size();
     U.nprog = nprog;
@@ -693,12 +713,13 @@ cudaError_t launch_with(int kind, bool hi2lo, int cfg, const RotLaunch & L, int 
     return cudaErrorInvalidValue;
 }
 
-// One launch in configuration cfg: shape cfg & 7, through the pass pipeline when cfg & 8
-// and the task list has a schedule (else each CTA runs every pass of its tasks).
+// One launch in configuration cfg: shape cfg & 7, through the pass pipeline in mode cfg >> 3
+// (schedule_passes) when the task list has a schedule (else, and in mode 0, each CTA runs
+// every pass of its tasks).
 cudaError_t launch_shape(int kind, bool hi2lo, int cfg, const RotLaunch & L, int max_ctas, cudaStream_t st,
                          RotSchedule * sched) {
-    const int shape = cfg & 7;
-    const RotSchedule::Units * U = ((cfg & 8) && sched) ? schedule_passes(sched, kind, L, shape_pass(shape), st) : nullptr;
+    const int shape = cfg & 7, mode = cfg >> 3;
+    const RotSchedule::Units * U = (mode > 0 && sched) ? schedule_passes(sched, kind, L, shape_pass(shape), mode, st) : nullptr;
     if (!U) return launch_with(kind, hi2lo, shape, L, max_ctas, st);
     static thread_local RotLaunch P;
     P = L;
@@ -756,9 +777,9 @@ int tune(int kind, bool hi2lo, const RotLaunch & L, double * const * dead, int m
     // every shape, each also through the pass pipeline when the list has a schedule (it
     // spreads a task's passes over SMs: worth it when there are few tasks, not when the
     // columns would leave L2 between passes)
-    for (int cfg = 0; cfg < 16; ++cfg) {
+    for (int cfg = 0; cfg < 8 * kPipeModes; ++cfg) {
         if ((cfg & 7) > 5 || ((kind == TRI || kind == RECT) && (cfg & 7) == 1)) continue;   // tri, rect: shape 1 not built
-        if ((cfg & 8) && !sched) continue;
+        if ((cfg >> 3) && !sched) continue;
         if (launch_shape(kind, hi2lo, cfg, S, max_ctas, st, sched) != cudaSuccess) { best = -1; break; }
         if (cudaEventRecord(e0, st) != cudaSuccess) { best = -1; break; }
         if (launch_shape(kind, hi2lo, cfg, S, max_ctas, st, sched) != cudaSuccess) { best = -1; break; }

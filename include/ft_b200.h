@@ -512,13 +512,15 @@ int ft_b200_profile(int enable);
 int ft_b200_profile_read(int family, double * ms, int * launches);
 
 /* Launch configuration of the rotation kernel (no counterpart in the reference,
- * whose kernels have no launch shape).  cfg = s or s + 8 forces shape s = 0 .. 5
+ * whose kernels have no launch shape).  cfg = s + 8 p forces shape s = 0 .. 5
  * (warps x sweeps per warp x chunk: 8 x 8 x 16, 16 x 4 x 8, 8 x 4 x 8, 8 x 4 x 16,
  * 4 x 4 x 16 and 4 x 8 x 16, the last two with as many CTAs per SM as fit; tri has
- * no 16 x 4 x 8 and runs 8 x 8 x 16 for it); + 8 runs the pass pipeline, where
- * each pass of 16 .. 64 sweeps of a task is its own work unit and streams down the
- * columns on another SM right behind the previous pass (for inputs with fewer
- * tasks than SMs; it loses where the columns would leave L2 between passes).
+ * no 16 x 4 x 8 and runs 8 x 8 x 16 for it) and pass-pipeline mode p = 0 .. 2.
+ * p = 1: each pass of 16 .. 64 sweeps of a task is its own work unit, queued
+ * pass-major, and streams down the columns on another SM right behind the previous
+ * pass (for inputs with fewer tasks than SMs; it loses where the columns would
+ * leave L2 between passes); p = 2: the same for the longest tasks whose columns
+ * fit in half the L2, every other task as one unit, after them.
  * cfg = -1 (the default, or FT_B200_ROT_CFG unset) lets the autotuner choose:
  * the first out-of-place launch of each shape (family, direction, all sweeps or
  * heads only, fields, tasks, N, M) times every configuration once on its

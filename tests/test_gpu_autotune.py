@@ -1,5 +1,5 @@
-"""The rotation kernel's launch configurations (six shapes, each with or without
-the pass pipeline) and the autotuner that picks among them
+"""The rotation kernel's launch configurations (six shapes, each without the pass
+pipeline and with its two queue modes) and the autotuner that picks among them
 (ft_b200_set_rotation_config).  Every configuration computes the same rotations
 in the same order per element, so the transforms must agree bit for bit
 whichever runs; the first out-of-place launch of a new shape times the
@@ -43,7 +43,7 @@ def test_every_shape_bit_identical(env, kind, n, params):
     try:
         ft.set_rotation_config(-1)
         ref = {(fwd, tr): transform(ft, torch, P, A, fwd, tr) for fwd in (True, False) for tr in "NT"}
-        for cfg in list(range(6)) + list(range(8, 14)):
+        for cfg in [s + 8 * p for p in range(3) for s in range(6)]:
             ft.set_rotation_config(cfg)
             for (fwd, tr), r in ref.items():
                 assert np.array_equal(transform(ft, torch, P, A, fwd, tr), r), (kind, cfg, fwd, tr)
@@ -66,8 +66,9 @@ def test_first_launch_of_a_shape_is_tuned(env):
     second = transform(ft, torch, P, A, True, "N")
     c2 = ft.kernel_launches()
     assert np.array_equal(first, second)
-    # six shapes for sph, with and without the pipeline, one untimed and one timed launch each
-    assert (c1 - c0) - (c2 - c1) == 24, (c1 - c0, c2 - c1)
+    # six shapes for sph, without the pipeline and in its two queue modes, one untimed and one
+    # timed launch each
+    assert (c1 - c0) - (c2 - c1) == 36, (c1 - c0, c2 - c1)
     P.close()
 
 
@@ -92,7 +93,7 @@ def test_pass_pipeline_rotation_stage_bitexact(env, kind, n, params):
         (O.hi2lo if hi2lo else O.lo2hi)(PO, r)
         refs[hi2lo] = r
     try:
-        for cfg in (8, 10, 12):
+        for cfg in (8, 10, 12, 16, 19):
             ft.set_rotation_config(cfg)
             for _ in range(3):
                 for hi2lo in (True, False):

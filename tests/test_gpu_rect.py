@@ -83,7 +83,7 @@ def test_rotations_bit_exact(env, n, M, beta):
     RP.close()
 
 
-@pytest.mark.parametrize("cfg", [0, 2, 3, 4, 5, 8, 10, 11, 12, 13])
+@pytest.mark.parametrize("cfg", [0, 2, 3, 4, 5, 8, 10, 11, 12, 13, 16, 19])
 def test_every_launch_shape_bit_exact(env, cfg):
     """Forced launch shapes (and the pass pipeline, cfg + 8) give the oracle's bits."""
     ft, torch, O = env
