@@ -209,7 +209,12 @@ __global__ void __launch_bounds__(256) slice_input_kernel(const __grid_constant_
 // ---------------------------------------------------------------------------
 // the multiply
 // ---------------------------------------------------------------------------
-template <int NU, int NX, int TBN>
+// F64: each chunk's level sums (exact integers in FP32) are recombined and scaled in FP64 (exactly:
+// the combined value spans about 48 bits, the scales are powers of two) and added into the
+// output, which the owning thread reads and writes once per chunk; else they are recombined in
+// FP32 into FP32 running sums and written once.  The FP64 form leaves only the slicing residuals,
+// for transforms whose multiplies cancel strongly (tri).
+template <int NU, int NX, int TBN, bool F64 = false>
 __global__ void __launch_bounds__(THREADS, 1) trmm_mixed_kernel(const __grid_constant__ MixLaunch L) {
     using C = Cfg<NU, NX, TBN>;
     constexpr int NL = C::NL;
@@ -306,6 +311,7 @@ __global__ void __launch_bounds__(THREADS, 1) trmm_mixed_kernel(const __grid_con
 #pragma unroll
             for (int j = 0; j < HALF; ++j) acc[j] = 0.0f;
             const float * xinv = L.Xinv + ((long long) (T.field * L.ncls + T.cls) * L.njt + T.jt) * nch * TBN + HALF * h;
+            bool first = true;
             for (int kt = T.k0; kt <= T.k1; ++kt) {
                 if (!chunk_end(kt, T.k1)) continue;
                 if (!tc::mbar_wait(&bar_accf, nacc & 1, &s_abort)) { fail(); break; }
@@ -321,17 +327,33 @@ __global__ void __launch_bounds__(THREADS, 1) trmm_mixed_kernel(const __grid_con
                     tc::tmem_wait_ld();
 #pragma unroll
                     for (int e = 0; e < 8; ++e) {
-                        float y = __uint_as_float(a[NL - 1][e]);
+                        if constexpr (F64) {
+                            const int row = T.it * TB + row_in;
+                            const int jj = T.jt * TBN + HALF * h + 8 * g + e;
+                            if (row < L.n && jj < class_cols(L.M, T.cls, L.ncls)) {
+                                double y = (double) __uint_as_float(a[NL - 1][e]);
 #pragma unroll
-                        for (int lv = NL - 2; lv >= 0; --lv) y = fmaf(y, 0.00390625f, __uint_as_float(a[lv][e]));
-                        acc[8 * g + e] = fmaf(y, __ldg(xi + 8 * g + e), acc[8 * g + e]);
+                                for (int lv = NL - 2; lv >= 0; --lv) y = fma(y, 0.00390625, (double) __uint_as_float(a[lv][e]));
+                                // 1 / (sX sU): powers of two
+                                y *= (double) __ldg(xi + 8 * g + e) * (double) __ldg(L.Uinv[class_matrix(T.cls, L.ncls)] + row);
+                                double * const p = L.out[T.field] + (long long) (T.cls + (long long) L.ncls * jj) * L.n + row;
+                                *p = first ? y : *p + y;
+                            }
+                        } else {
+                            float y = __uint_as_float(a[NL - 1][e]);
+#pragma unroll
+                            for (int lv = NL - 2; lv >= 0; --lv) y = fmaf(y, 0.00390625f, __uint_as_float(a[lv][e]));
+                            acc[8 * g + e] = fmaf(y, __ldg(xi + 8 * g + e), acc[8 * g + e]);
+                        }
                     }
                 }
+                first = false;
                 tc::fence_before_sync();
                 tc::mbar_arrive(&bar_acce);
             }
             if (s_abort) break;
-            // out = acc 2^-14 / sU_i
+            if (F64) continue;
+            // out = acc / sU_i (acc holds the chunks' sums divided by their sX)
             const int row = T.it * TB + row_in;
             if (row < L.n) {
                 const double sc = (double) __ldg(L.Uinv[class_matrix(T.cls, L.ncls)] + row);
@@ -546,7 +568,11 @@ cudaError_t launch_trmm_mixed(HarmonicPlan * H, void ** plan_slot, void ** work_
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int ctas = std::min(sms, X.ntiles);
     if (ctas <= 0) return cudaSuccess;
-    if (cfg) {
+    if (cfg && ncls == 1) {   // one class (tri): chunks folded into the output in FP64
+        auto kern = trmm_mixed_kernel<4, 4, 96, true>;
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) Cfg<4, 4, 96>::SMEM);
+        if (e == cudaSuccess) { kern<<<ctas, THREADS, Cfg<4, 4, 96>::SMEM, st>>>(L); e = cudaGetLastError(); }
+    } else if (cfg) {
         auto kern = trmm_mixed_kernel<4, 4, 96>;
         e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) Cfg<4, 4, 96>::SMEM);
         if (e == cudaSuccess) { kern<<<ctas, THREADS, Cfg<4, 4, 96>::SMEM, st>>>(L); e = cudaGetLastError(); }

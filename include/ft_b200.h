@@ -455,8 +455,10 @@ int ft_b200_execute_noalloc_dev(const ft_harmonic_plan * P, int forward, char TR
  * multiplies amplify the sweeps' error by a factor that depends on the family
  * and its parameters (disk with generic parameters about 3e-6 at n = 2048).
  * tri keeps its sweeps in FP64 (direct) in both split-BF16 forms and runs only
- * its two connection multiplies on the tensor cores: its multiplies would
- * amplify a sliced sweep's error to 3e-6 .. 3e-5; this way about 1e-7.
+ * its two connection multiplies on the tensor cores, with each 256-row chunk's
+ * exact sums recombined and accumulated in FP64: its multiplies amplify errors
+ * strongly (a sliced sweep's to 3e-6 .. 3e-5, an FP32 recombination's to 2e-6
+ * at n = 2048).
  * precision FT_B200_MIXED_BF16X4: four slices in the blocks (ten products)
  * and four of the input in the connection multiply: about 1.4e-7 for sph at
  * n = 2048.  The first call of either builds its slice images
