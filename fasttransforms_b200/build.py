@@ -38,7 +38,8 @@ def build(verbose: bool = False) -> str:
     for src in SOURCES:
         path = os.path.join(CSRC, src)
         obj = os.path.join(BUILD_DIR, src + ".o")
-        deps = [path, os.path.join(CSRC, "ft_internal.h"), os.path.join(HERE, os.pardir, "include", "ft_b200.h")]
+        deps = [path, os.path.join(CSRC, "ft_internal.h"), os.path.join(CSRC, "tc05.h"),
+                os.path.join(HERE, os.pardir, "include", "ft_b200.h")]
         if not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(d) for d in deps):
             cmd = [NVCC, *ARCH, *COMMON, "-c", path, "-o", obj]
             if verbose and src.endswith(".cu"):

@@ -86,15 +86,22 @@ __device__ __forceinline__ float pow2_scale(float amax) {
     return __uint_as_float((uint32_t) (260 - E) << 23);       // 2^(7 - (E - 126))
 }
 
-// 8 consecutive K values (already scaled) -> NS 16-byte chunks of integer slices
+// 8 consecutive K values (already scaled, |t| < 2^7, FP64) -> NS 16-byte chunks of integer
+// slices.  The first slice is cut in FP64; its residual times 2^8 (|r| <= 128) then rounds to
+// FP32 within 2^-17, which is 2^-32 of the scale 2^7, and the FP32 cuts that follow are exact.
+// (Rounding the input itself to FP32 first would leave 2^-24 of every entry, which the fourth
+// slice cannot recover and the multiplies of tri amplify.)
 template <int NS>
-__device__ __forceinline__ void slice8(const float * t_in, uint4 * out) {
+__device__ __forceinline__ void slice8(const double * t_in, uint4 * out) {
     uint32_t w[NS][4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-        float t0 = t_in[2 * q], t1 = t_in[2 * q + 1];
+        const double d0 = t_in[2 * q], d1 = t_in[2 * q + 1];
+        const double j0 = rint(d0), j1 = rint(d1);
+        w[0][q] = tc::pack_bf16_ints((float) j0, (float) j1);
+        float t0 = (float) ((d0 - j0) * 256.0), t1 = (float) ((d1 - j1) * 256.0);   // d - j exact
 #pragma unroll
-        for (int a = 0; a < NS; ++a) {
+        for (int a = 1; a < NS; ++a) {
             const float i0 = tc::round_small(t0), i1 = tc::round_small(t1);
             w[a][q] = tc::pack_bf16_ints(i0, i1);
             t0 = __fmul_rn(__fsub_rn(t0, i0), 256.0f);   // exact: |t - i| <= 1/2, times a power of two
@@ -163,7 +170,7 @@ struct SliceXLaunch {
 template <int NS, int TBN>
 __global__ void __launch_bounds__(256) slice_input_kernel(const __grid_constant__ SliceXLaunch L) {
     constexpr int XPIECE = TBN * KT * 2;
-    __shared__ float buf[8][256];
+    __shared__ double buf[8][256];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nch = (L.nkt + CHUNK_KT - 1) / CHUNK_KT;
     int b = blockIdx.x;
@@ -177,21 +184,23 @@ __global__ void __launch_bounds__(256) slice_input_kernel(const __grid_constant_
         const int j = jt * TBN + ci;
         const bool cok = j < ncols;
         const double * col = L.in[f] + (long long) (r + (long long) L.ncls * j) * L.n;
-        float amax = 0.0f;
+        double amax = 0.0;
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
             const int row = q * (KT * CHUNK_KT) + 32 * e + lane;
-            const float v = (cok && row < L.n) ? (float) __ldcg(col + row) : 0.0f;
+            const double v = (cok && row < L.n) ? __ldcg(col + row) : 0.0;
             buf[warp][32 * e + lane] = v;
-            amax = fmaxf(amax, fabsf(v));
+            amax = fmax(amax, fabs(v));
         }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
-        const float s = pow2_scale(amax);
+        for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+        // the FP32 image of amax keeps its binade or rounds up to the next power of two: either
+        // way |s v| < 2^7 for every v of the chunk
+        const float s = pow2_scale((float) amax);
         __syncwarp();
-        float t[8];
+        double t[8];
 #pragma unroll
-        for (int e = 0; e < 8; ++e) t[e] = buf[warp][8 * lane + e] * s;
+        for (int e = 0; e < 8; ++e) t[e] = buf[warp][8 * lane + e] * (double) s;
         __syncwarp();
         const int kt = q * CHUNK_KT + lane / 8;
         if (kt < L.nkt) {
