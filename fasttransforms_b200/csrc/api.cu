@@ -580,9 +580,11 @@ void release_batches(HarmonicPlan * H) {
     }
 }
 
-BatchCtx * get_batch(HarmonicPlan * const * H, const int * N, const int * M, int nf) {
+// lane: a second context of the same fields (its own scratch and queue), for work that may run
+// concurrently with lane 0's on another stream
+BatchCtx * get_batch(HarmonicPlan * const * H, const int * N, const int * M, int nf, int lane = 0) {
     std::lock_guard<std::mutex> lk(g_batch_mu);
-    const std::string key = batch_key(H, N, M, nf);
+    const std::string key = batch_key(H, N, M, nf) + (lane ? "#" + std::to_string(lane) : std::string());
     auto it = g_batches.find(key);
     if (it != g_batches.end()) return it->second;
     BatchCtx * B = new BatchCtx();
@@ -628,8 +630,8 @@ BatchCtx * get_batch(HarmonicPlan * const * H, const int * N, const int * M, int
 
 // one launch per stage over up to kMaxFields fields of one family
 int execute_batch_chunk(HarmonicPlan * const * H, bool forward, char TRANS, double * const * A, const int * N,
-                        const int * M, int nf, cudaStream_t st, int precision = FT_B200_FP64) {
-    BatchCtx * B = get_batch(H, N, M, nf);
+                        const int * M, int nf, cudaStream_t st, int precision = FT_B200_FP64, int lane = 0) {
+    BatchCtx * B = get_batch(H, N, M, nf, lane);
     if (!B) return t_status;
     const bool mixed = precision == FT_B200_MIXED_BF16 || precision == FT_B200_MIXED_BF16X4;
     // tri's split-BF16 forms keep the sweeps in FP64 (the direct kernel) and put only its two
@@ -825,7 +827,8 @@ bool rotation_sweeps(ft_rotation_plan * RP, bool hi2lo, const double * in, doubl
 // ---------------------------------------------------------------------------
 struct HostPipe {
     static constexpr int NBUF = 3;
-    cudaStream_t s_in = nullptr, s_comp = nullptr, s_out = nullptr;
+    static constexpr int LANES = 2;   // compute streams: consecutive groups alternate between them
+    cudaStream_t s_in = nullptr, s_comp[LANES] = {}, s_out = nullptr;
     cudaEvent_t ev_in[NBUF] = {}, ev_comp[NBUF] = {}, ev_out[NBUF] = {};
     double * buf[NBUF] = {};   // cap matrices of elems doubles each
     int cap = 0;
@@ -837,7 +840,7 @@ std::map<HarmonicPlan *, HostPipe *> g_pipes;
 
 void host_pipe_free(HostPipe * Q) {
     if (!Q) return;
-    for (cudaStream_t s : {Q->s_in, Q->s_comp, Q->s_out})
+    for (cudaStream_t s : {Q->s_in, Q->s_comp[0], Q->s_comp[1], Q->s_out})
         if (s) { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
     for (int b = 0; b < HostPipe::NBUF; b++) {
         if (Q->ev_in[b]) cudaEventDestroy(Q->ev_in[b]);
@@ -864,7 +867,8 @@ HostPipe * host_pipe(HarmonicPlan * H, int cap, size_t elems) {
     if (Q) return Q;
     Q = new HostPipe();
     bool ok = cuda_ok(cudaStreamCreateWithFlags(&Q->s_in, cudaStreamNonBlocking), "cudaStreamCreate") &&
-              cuda_ok(cudaStreamCreateWithFlags(&Q->s_comp, cudaStreamNonBlocking), "cudaStreamCreate") &&
+              cuda_ok(cudaStreamCreateWithFlags(&Q->s_comp[0], cudaStreamNonBlocking), "cudaStreamCreate") &&
+              cuda_ok(cudaStreamCreateWithFlags(&Q->s_comp[1], cudaStreamNonBlocking), "cudaStreamCreate") &&
               cuda_ok(cudaStreamCreateWithFlags(&Q->s_out, cudaStreamNonBlocking), "cudaStreamCreate");
     for (int b = 0; ok && b < HostPipe::NBUF; b++)
         ok = cuda_ok(cudaEventCreateWithFlags(&Q->ev_in[b], cudaEventDisableTiming), "cudaEventCreate") &&
@@ -916,13 +920,14 @@ int shared_prepare(HarmonicPlan * H, int precision) {
     return FT_B200_OK;
 }
 
-int shared_run(HarmonicPlan * H, bool forward, char TRANS, double * const * dA, int nfields, int precision, cudaStream_t st) {
+int shared_run(HarmonicPlan * H, bool forward, char TRANS, double * const * dA, int nfields, int precision, cudaStream_t st,
+               int lane = 0) {
     const int M = H->Mdef;
     for (int f0 = 0; f0 < nfields; f0 += kMaxFields) {
         const int nf = std::min(kMaxFields, nfields - f0);
         std::vector<HarmonicPlan *> Hs(nf, H);
         std::vector<int> Ns(nf, H->n), Ms(nf, M);
-        if (execute_batch_chunk(Hs.data(), forward, TRANS, dA + f0, Ns.data(), Ms.data(), nf, st, precision) != FT_B200_OK)
+        if (execute_batch_chunk(Hs.data(), forward, TRANS, dA + f0, Ns.data(), Ms.data(), nf, st, precision, lane) != FT_B200_OK)
             return t_status;
     }
     return FT_B200_OK;
@@ -943,7 +948,10 @@ int shared_host(HarmonicPlan * H, int nops, const int * forward, const char * TR
     bool ok = true;
     int f0 = 0;
     for (size_t g = 0; ok && g < groups.size(); g++) {
-        const int b = (int) (g % HostPipe::NBUF), nf = groups[g];
+        // group g computes on lane g mod 2 (its own stream and scratch), so that a group's kernels
+        // start on the SMs the previous group's last kernels leave idle
+        const int b = (int) (g % HostPipe::NBUF), nf = groups[g], lane = (int) (g % HostPipe::LANES);
+        cudaStream_t const sc = Q->s_comp[lane];
         std::vector<double *> d(nf);
         for (int i = 0; i < nf; i++) d[i] = Q->buf[b] + elems * (size_t) i;
         // the buffer is free once the read-back of the group that used it before has finished
@@ -951,10 +959,10 @@ int shared_host(HarmonicPlan * H, int nops, const int * forward, const char * TR
         for (int i = 0; ok && i < nf; i++)
             ok = cuda_ok(cudaMemcpyAsync(d[i], A[f0 + i], bytes, cudaMemcpyHostToDevice, Q->s_in), "cudaMemcpyAsync(H2D)");
         ok = ok && cuda_ok(cudaEventRecord(Q->ev_in[b], Q->s_in), "cudaEventRecord") &&
-             cuda_ok(cudaStreamWaitEvent(Q->s_comp, Q->ev_in[b], 0), "cudaStreamWaitEvent");
+             cuda_ok(cudaStreamWaitEvent(sc, Q->ev_in[b], 0), "cudaStreamWaitEvent");
         for (int o = 0; ok && o < nops; o++)
-            ok = shared_run(H, forward[o] != 0, TRANS[o], d.data(), nf, precision, Q->s_comp) == FT_B200_OK;
-        ok = ok && cuda_ok(cudaEventRecord(Q->ev_comp[b], Q->s_comp), "cudaEventRecord") &&
+            ok = shared_run(H, forward[o] != 0, TRANS[o], d.data(), nf, precision, sc, lane) == FT_B200_OK;
+        ok = ok && cuda_ok(cudaEventRecord(Q->ev_comp[b], sc), "cudaEventRecord") &&
              cuda_ok(cudaStreamWaitEvent(Q->s_out, Q->ev_comp[b], 0), "cudaStreamWaitEvent");
         for (int i = 0; ok && i < nf; i++)
             ok = cuda_ok(cudaMemcpyAsync(A[f0 + i], d[i], bytes, cudaMemcpyDeviceToHost, Q->s_out), "cudaMemcpyAsync(D2H)");
@@ -963,7 +971,8 @@ int shared_host(HarmonicPlan * H, int nops, const int * forward, const char * TR
     }
     // the call returns with every result in host memory (or after everything enqueued has ended)
     const bool done = cuda_ok(cudaStreamSynchronize(Q->s_in), "cudaStreamSynchronize") &
-                      cuda_ok(cudaStreamSynchronize(Q->s_comp), "cudaStreamSynchronize") &
+                      cuda_ok(cudaStreamSynchronize(Q->s_comp[0]), "cudaStreamSynchronize") &
+                      cuda_ok(cudaStreamSynchronize(Q->s_comp[1]), "cudaStreamSynchronize") &
                       cuda_ok(cudaStreamSynchronize(Q->s_out), "cudaStreamSynchronize");
     return (ok && done) ? FT_B200_OK : t_status;
 }
