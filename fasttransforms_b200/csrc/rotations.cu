@@ -104,22 +104,25 @@ __device__ int g_rot_status;
 
 // Progress word of a pipeline unit: hi2lo, -X where every position >= X of its columns is
 // final for the pass; lo2hi, X where every position <= X is final.  The launcher clears the
-// words to a value below any position; a finished unit publishes INT_MAX.
+// words to a value below any position; a finished unit publishes INT_MAX.  Thread 0 publishes
+// after a CTA barrier: the barrier orders every thread's stores of the chunk before its fence,
+// and the fence and release are cumulative, so one thread's release covers the whole CTA's
+// stores (the consumer's thread 0 acquires, then a barrier orders its CTA's loads after that).
 __device__ __forceinline__ void publish_progress(int * p, int v) {
     __threadfence();
     asm volatile("st.release.gpu.global.s32 [%0], %1;\n" :: "l"(p), "r"(v) : "memory");
 }
-// Waits until *p >= need; gives up after about 2^32 SM cycles, setting the status word, and
-// at once when the word is already set (so one failed wait costs a launch about that long,
-// not that long per unit).
-__device__ __forceinline__ void wait_progress(const int * p, int need) {
+// Waits until *p >= need and returns the value read; gives up after about 2^32 SM cycles,
+// setting the status word, and at once when the word is already set (so one failed wait costs
+// a launch about that long, not that long per unit).
+__device__ __forceinline__ int wait_progress(const int * p, int need) {
     const long long t0 = clock64();
     for (;;) {
         int v;
         asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
-        if (v >= need) return;
-        if (*(volatile int *) &g_rot_status != 0) return;
-        if (clock64() - t0 > (1LL << 32)) { atomicExch(&g_rot_status, 3); return; }
+        if (v >= need) return v;
+        if (*(volatile int *) &g_rot_status != 0) return v;
+        if (clock64() - t0 > (1LL << 32)) { atomicExch(&g_rot_status, 3); return v; }
         __nanosleep(128);
     }
 }
@@ -240,6 +243,7 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
             // pass pipeline: the previous pass's progress word and this pass's own
             const int * const prev_prog = (pipe && r > 0) ? L.prog + chain.prog0 + r - 1 : nullptr;
             int * const my_prog = pipe ? L.prog + chain.prog0 + r : nullptr;
+            int seen = -0x7fffffff - 1;   // (thread 0) the predecessor's progress as last read
 
             // ---- stage state: per column a window of 2B chain positions ----
             double win[NCOL][2 * B];
@@ -375,7 +379,10 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
                 if (!prev_prog || k >= K) return;
                 const int pmin = pmin_of(k, false), pmax = pmin + E - 1;
                 if (pmax < 0 || pmin > emax) return;                 // nothing of the chunk is loaded
-                wait_progress(prev_prog, HI2LO ? -max(pmin, 0) : min(pmax, emax));
+                // the predecessor publishes every few chunks and runs ahead: one acquire covers the
+                // chunks up to the progress it read, which the words only ever raise
+                const int need = HI2LO ? -max(pmin, 0) : min(pmax, emax);
+                if (seen < need) seen = wait_progress(prev_prog, need);
             };
             auto load_chunk = [&](int k) {
                 const int pmin = pmin_of(k, false);
@@ -388,18 +395,19 @@ rot_kernel(const __grid_constant__ RotLaunch L) {
 #pragma unroll
                 for (int v = 0; v < PER_W; ++v) b0[soff[v]] = pre[v];
             };
-            // the pass pipeline publishes progress every kPub stored chunks (and after the last):
-            // a fence and a release per chunk cost as much as the chunk's sweeps, and a pass that
-            // trails its predecessor by a few chunks more loses nothing
-            constexpr int kPub = 4;
-            auto publishes = [&](int k) { return k % kPub == kPub - 1 || k == K - 1; };
+            // the pass pipeline publishes progress every stored chunk for short columns, every
+            // fourth for long ones (and after the last): a successor trailing by a few chunks more
+            // loses little of a long pass, while a publish costs its CTA a fence and a release
+            auto publishes = [&](int k) {
+                const int m = F.N >= 2048 ? 3 : 0;
+                return (k & m) == m || k == K - 1;
+            };
             auto store_chunk = [&](int k) {
                 const int pmin = pmin_of(k, true);
                 const double * const bw = buf(WA, k & 1, 0, 0);
 #pragma unroll
                 for (int v = 0; v < PER_W; ++v)
                     if (row_ok(pmin, v)) __stcg(gdst[v] + (long long) ES * CH * pmin, bw[soff[v]]);
-                if (pipe && publishes(k)) __threadfence();   // before the barrier after which they are published
             };
             if (pipe) {
                 if (threadIdx.x == 0) {
