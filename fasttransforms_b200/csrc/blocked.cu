@@ -357,20 +357,27 @@ __device__ __forceinline__ float slice_scale(float amax) {
     return __uint_as_float((uint32_t) (261 - E) << 23);       // 2^(8 - (E - 126))
 }
 
-// eight consecutive window positions, scaled by s, -> NS 16-byte chunks of
-// integer-valued BF16 slices: s x = i_0 + i_1 2^-9 + ...
+// eight consecutive window positions, scaled by s (a power of two), -> NS 16-byte chunks of
+// integer-valued BF16 slices: s x = i_0 + i_1 2^-9 + ...  Each cut is one FMA that scales and
+// adds 1.5 * 2^23 (rounding to the nearest integer, |s x| < 2^8) and one subtraction, and each
+// residual one FMA (s x - i_0, 2^9 t - i_a: exact, |residual| <= 1/2 and a multiple of the
+// operand's last place), the values those of rounding s x, subtracting and scaling in turn.
 template <int NS>
 __device__ __forceinline__ void slice8(const float * v, float s, uint4 * out) {
+    constexpr float kMagic = 12582912.0f;         // 1.5 * 2^23
     uint32_t w[NS][4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-        float t0 = v[2 * q] * s, t1 = v[2 * q + 1] * s;
+        float t0 = v[2 * q], t1 = v[2 * q + 1], m = s;
 #pragma unroll
         for (int a = 0; a < NS; ++a) {
-            const float i0 = tc::round_small(t0), i1 = tc::round_small(t1);
+            const float i0 = __fsub_rn(__fmaf_rn(t0, m, kMagic), kMagic), i1 = __fsub_rn(__fmaf_rn(t1, m, kMagic), kMagic);
             w[a][q] = tc::pack_bf16_ints(i0, i1);
-            t0 = __fmul_rn(__fsub_rn(t0, i0), 512.0f);   // exact: |t - i| <= 1/2, times a power of two
-            t1 = __fmul_rn(__fsub_rn(t1, i1), 512.0f);
+            if (a + 1 < NS) {
+                t0 = __fmaf_rn(t0, m, -i0);
+                t1 = __fmaf_rn(t1, m, -i1);
+                m = 512.0f;
+            }
         }
     }
 #pragma unroll
@@ -557,9 +564,10 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
                     v[4 * qd] = x.x; v[4 * qd + 1] = x.y; v[4 * qd + 2] = x.z; v[4 * qd + 3] = x.w;
                 }
             };
-            // 32 positions from pos0 (a multiple of 32) into their window slots, with one
-            // scale for the whole window: the two halves exchange their largest entries
-            auto put32 = [&](int pos0, const float * v) -> bool {
+            // 32 positions from pos0 (a multiple of 32), the values v times vs (a power of two),
+            // into their window slots, with one scale for the whole window: the two halves
+            // exchange their largest entries
+            auto put32 = [&](int pos0, const float * v, float vs) -> bool {
                 float m0 = 0.0f, m1 = 0.0f, m2 = 0.0f, m3 = 0.0f;
 #pragma unroll
                 for (int e = 0; e < TL; e += 4) {
@@ -568,7 +576,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
                     m2 = fmaxf(m2, fabsf(v[e + 2]));
                     m3 = fmaxf(m3, fabsf(v[e + 3]));
                 }
-                const float pm = fmaxf(fmaxf(m0, m1), fmaxf(m2, m3));
+                const float pm = fmaxf(fmaxf(m0, m1), fmaxf(m2, m3)) * vs;
                 s_pmax[c][hf][r] = pm;
                 tc::mbar_arrive(&bar_pmax[c]);
                 if (!tc::mbar_wait(&bar_pmax[c], pp & 1, &s_abort)) { fail(); return false; }
@@ -578,7 +586,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
 #pragma unroll
                 for (int g = 0; g < TL / 8; ++g) {
                     uint4 ch[NS];
-                    slice8<NS>(v + 8 * g, sc, ch);
+                    slice8<NS>(v + 8 * g, sc * vs, ch);
                     const uint32_t off = tc::sw128_offset(r, (pos0 + 8 * g) & (WIN - 1));
 #pragma unroll
                     for (int a = 0; a < NS; ++a) *reinterpret_cast<uint4 *>(xrow + a * MX_PIECE + off) = ch[a];
@@ -599,7 +607,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
                 {   // first tile: the whole window
                     const int pos0 = (HI2LO ? kmax : -1) * TL + TL * hf;
                     load32(pos0, src);
-                    if (!put32(pos0, src)) break;
+                    if (!put32(pos0, src, 1.0f)) break;
                 }
                 for (int ki = 0; ki < nk; ++ki) {
                     const int k = HI2LO ? kmax - ki : ki - 1;
@@ -641,12 +649,14 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
                                 float y = __uint_as_float(a[NL - 1][4 * hq + e]);
 #pragma unroll
                                 for (int lv = NL - 2; lv >= 0; --lv) y = fmaf(y, 0.001953125f, __uint_as_float(a[lv][4 * hq + e]));
-                                v[e] = y * unscale;
+                                v[e] = y;
                             }
                             const int P = lo + TL * hf + 8 * g + 4 * hq;
                             if (fin) {
-                                if (P >= 0 && P < Pend) __stcg(Tq + (long long) (P >> 2) * MX_COLS, make_float4(v[0], v[1], v[2], v[3]));
-                            } else {
+                                if (P >= 0 && P < Pend)
+                                    __stcg(Tq + (long long) (P >> 2) * MX_COLS,
+                                           make_float4(v[0] * unscale, v[1] * unscale, v[2] * unscale, v[3] * unscale));
+                            } else {   // kept unscaled: the window cut below applies unscale
 #pragma unroll
                                 for (int e = 0; e < 4; ++e) src[8 * g + 4 * hq + e] = v[e];
                             }
@@ -658,7 +668,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
                         if (!read_rows(npos, rk, src)) break;
                         rk++;
                     }
-                    if (!last && !put32(hf == fh ? npos : lo + TL * hf, src)) break;
+                    if (!last && !put32(hf == fh ? npos : lo + TL * hf, src, hf == fh ? 1.0f : unscale)) break;
                 }
                 // block boundary: the next block's first window reads rows of global memory that
                 // the other half of this chain's threads wrote
