@@ -164,12 +164,21 @@ def ft_time(block, ntimes: int) -> float:
     return (time.perf_counter() - t0) / ntimes
 
 
+def quad_cols(M: int) -> list:
+    """Columns of every stride-4 class spread over all orders, where the GPU's forward transforms
+    are compared with the quad-precision oracle (the same set as the parity tests)."""
+    return sorted({0, 1, 2, 3, 4, 5, 6, M // 4 - 1, M // 4, M // 4 + 1, M // 4 + 2, M // 2 - 1, M // 2, M // 2 + 1,
+                   M // 2 + 2, 3 * M // 4, 3 * M // 4 + 1, M - 4, M - 3, M - 2, M - 1})
+
+
 def cpu_sample(n: int, ref_out: str | None = None) -> dict:
     """Reference CPU build on this host's cores with the reference's timing protocol:
     FT_TIME (two warm-ups, then NTIMES = 1 + (2048 / n)^2 timed runs in C integer arithmetic,
     test/test_drivers.c:257) of sph2fourier 'N' and of fourier2sph 'N', each repeated five times,
     the medians summed.  With ref_out, the reference's forward 'N' of the field (before any
-    timing) is saved there for the GPU's parity check."""
+    timing) is saved there for the GPU's parity check, and beside it (ref_out + ".quad.npy") the
+    __float128 oracle's forward of the same field on quad_cols(M), with the reference plan's own
+    connection matrices (oracle/ft_quad.c; a checker, run here on the host only)."""
     import numpy as np
     threads, cpu_desc = host_cpu()
     from oracle.bind import Reference, Oracle, fill
@@ -190,6 +199,12 @@ def cpu_sample(n: int, ref_out: str | None = None) -> dict:
         run(True, F)
         np.save(ref_out, F)
         del F
+        if kind == "reference":
+            from oracle.bind import Quad
+            Ps, _ = R.connection(P, n)
+            hi, _ = Quad().columns("sph", A, quad_cols(A.shape[1]), (), True, (np.triu(Ps[0]), np.triu(Ps[1])))
+            np.save(ref_out + ".quad.npy", hi)
+            del Ps
     ntimes = 1 + (2048 // n) ** 2
     B = A.copy(order="F")
     tf = statistics.median(ft_time(lambda: run(True, B), ntimes) for _ in range(5))
@@ -560,6 +575,22 @@ def run_ours(args, rank, world, local_rank, dist):
                       "plain_fp64_epsinf": float(np.abs(fp64_f0 - ref).max() / ni),
                       "mixed_bf16_eps2": float(np.linalg.norm(mixed_f0 - ref) / nr),
                       "mixed_bf16_epsinf": float(np.abs(mixed_f0 - ref).max() / ni)}
+            qpath = ref_path + ".quad.npy"
+            if os.path.exists(qpath):
+                # every form's forward of field 0 against the __float128 oracle on quad_cols(M)
+                # columns (the compiled reference's own error beside them)
+                hi = np.load(qpath)
+                os.remove(qpath)
+                cols = quad_cols(M)
+                nh, ih = np.linalg.norm(hi), np.abs(hi).max()
+                err = lambda x: {"eps2": float(np.linalg.norm(x - hi) / nh), "epsinf": float(np.abs(x - hi).max() / ih)}
+                colsof = lambda flat: flat.reshape((n, M), order="F")[:, cols]
+                pq = {"oracle": f"oracle/ft_quad.c (__float128 sweeps and connection multiply), {len(cols)} columns "
+                                f"of every class over all orders, field 0 (seed {SEED})",
+                      "reference": err(colsof(ref)), "plain_fp64": err(colsof(fp64_f0)), "mixed_bf16": err(colsof(mixed_f0))}
+                for name, x in ((extra or {}).get("_field0_cols") or {}).items():
+                    pq["shared_" + name] = err(x)
+                parity["vs_quad"] = pq
             del ref
         fam_cpu = cpu.pop("families", None) if isinstance(cpu, dict) else None
         for key, v in (fam_cpu or {}).items():
@@ -568,6 +599,8 @@ def run_ours(args, rank, world, local_rank, dist):
                 v["sample"] = "the compiled reference, one timed fwd+bwd 'N' after one warm-up, same size"
                 extra[key]["reference_cpu"] = v
                 extra[key]["gpu_over_reference_cpu"] = extra[key]["coeffs_per_s"] / v["value"]
+    if isinstance(extra, dict):
+        extra.pop("_field0_cols", None)   # host copies for the quad check, not part of the line
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -1044,16 +1077,19 @@ def extra_workloads(args, torch, ft):
     n = 4096
     Pn = ft.plan_sph2fourier(n)
     M = Pn.M
-    fields = [torch.from_numpy(ft.sphrand(n, SEED + 100 + f).ravel(order="F").copy()).cuda() for f in range(16)]
+    fields = [torch.from_numpy(ft.sphrand(n, SEED + f).ravel(order="F").copy()).cuda() for f in range(16)]
     fptr = [f.data_ptr() for f in fields]
     res = {}
     ref_out = None
+    qcols = quad_cols(M)
+    out["_field0_cols"] = {}
     field0 = fields[0].clone()   # the fields below are transformed in place; errors start from this copy
     for name, prec in (("fp64_direct", ft.FP64), ("fp64_blocked", ft.FP64_BLOCKED), ("mixed_bf16_3slices", ft.MIXED_BF16),
                        ("mixed_bf16_4slices", ft.MIXED_BF16X4)):
         x0 = field0.clone()
         ft.execute_shared_dev(Pn, True, "N", [x0.data_ptr()], prec, sp)   # builds tables outside timing
         torch.cuda.synchronize()
+        out["_field0_cols"][name] = x0.view(M, n).t()[:, qcols].cpu().numpy()
         if ref_out is None:
             ref_out = x0
             err = 0.0
@@ -1066,7 +1102,7 @@ def extra_workloads(args, torch, ft):
         step()
         ms = timed(step, 3)
         res[name] = {"coeffs_per_s": 16 * n * n / (ms * 1e-3), "ms_per_step": ms,
-                     "eps2_fwd_vs_fp64_direct": err, "fields": "seeds 20261303 + f (field 0 for the error)"}
+                     "eps2_fwd_vs_fp64_direct": err, "fields": "seeds 20261203 + f (field 0 for the error)"}
     out["shared_16_n4096"] = res
     del fields
     Pn.close()
