@@ -105,12 +105,12 @@ __device__ int g_rot_status;
 // Progress word of a pipeline unit: hi2lo, -X where every position >= X of its columns is
 // final for the pass; lo2hi, X where every position <= X is final.  The launcher clears the
 // words to a value below any position; a finished unit publishes INT_MAX.  Thread 0 publishes
-// after a CTA barrier: the barrier orders every thread's stores of the chunk before its fence,
-// and the fence and release are cumulative, so one thread's release covers the whole CTA's
-// stores (the consumer's thread 0 acquires, then a barrier orders its CTA's loads after that).
+// after a CTA barrier: the barrier orders every thread's stores of the chunk before its release,
+// and a release is cumulative, so one thread's release covers the whole CTA's stores (the
+// consumer's thread 0 acquires, then a barrier orders its CTA's loads after that).  A release
+// reduction (max: the words only rise) does not hold the thread the way a fence does.
 __device__ __forceinline__ void publish_progress(int * p, int v) {
-    __threadfence();
-    asm volatile("st.release.gpu.global.s32 [%0], %1;\n" :: "l"(p), "r"(v) : "memory");
+    asm volatile("red.release.gpu.global.max.s32 [%0], %1;\n" :: "l"(p), "r"(v) : "memory");
 }
 // Waits until *p >= need and returns the value read; gives up after about 2^32 SM cycles,
 // setting the status word, and at once when the word is already set (so one failed wait costs
