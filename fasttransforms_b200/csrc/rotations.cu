@@ -24,10 +24,14 @@
 // traffic: during each iteration every warp loads its share of the next
 // chunk's column segments into registers (latency hidden behind the sweeps)
 // and writes its share of the last stage's finished chunk back, so one pass of
-// W*B sweeps reads and writes each column once.  All lanes of a warp use the
-// same (sin, cos) pair at each rotation, read as a warp-broadcast 16-byte load.
+// W*B sweeps reads and writes each column once.  The lanes of a warp that carry
+// the same chain use the same (sin, cos) pair at each rotation, read as a
+// broadcast 16-byte shared-memory load (two pairs per warp for two-chain kinds);
+// each sweep's pairs of a chunk arrive in shared memory by one bulk copy from a
+// padded table (identity pairs outside the sweep), issued one chunk ahead.
 // With W = 8 warps every SM sub-partition holds two warps and the register
-// budget per thread is the full 255.
+// budget per thread is the full 255.  In the pipelined configurations each pass
+// of a task is a work unit of its own that streams behind the previous pass.
 //
 // Within a CTA no thread waits on another except through __syncthreads.  The
 // one spin loop is the pass pipeline's wait on another CTA's progress word
