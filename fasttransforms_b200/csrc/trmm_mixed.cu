@@ -59,6 +59,9 @@ template <int NU, int NX, int TBN> struct Cfg {
 
 struct MixTile { int field, cls, it, jt, k0, k1; };   // K-tiles k0 .. k1 inclusive
 
+// Order of the tiles (launch_trmm_mixed): blocks of row tiles x column tiles, 0 for one block
+constexpr int kRowGroup = 8, kColGroup = 18;
+
 struct MixLaunch {
     double * out[kMaxFields];
     const unsigned char * Uimg[2];      // per class matrix: [it][kt][NU slices]
@@ -532,15 +535,28 @@ cudaError_t launch_trmm_mixed(HarmonicPlan * H, void ** plan_slot, void ** work_
         if (e == cudaSuccess) e = cudaMalloc(&X.xinv, sizeof(float) * (size_t) nf * ncls * X.njt * W->nch * tbn);
         if (e != cudaSuccess) return e;
         for (int tr = 0; tr < 2; ++tr) {
-            std::vector<std::pair<int, MixTile>> v;
+            // Tiles in blocks of kRowGroup row tiles (longest K first) x kColGroup column tiles:
+            // the persistent CTAs take consecutive tiles, so the tiles in flight share a few row
+            // tiles' slices of op(U) and a few column tiles' slices of the input, which stay in
+            // L2 (longest first, the input's slices are re-read from DRAM once per row tile).
+            // Within a block, longest K first.
+            struct Key { int rg, cg, klen, col, it; };
+            std::vector<std::pair<Key, MixTile>> v;
             for (int f = 0; f < nf; ++f)
                 for (int r = 0; r < ncls; ++r)
                     for (int it = 0; it < nit; ++it)
                         for (int jt = 0; jt * tbn < class_cols(M, r, ncls); ++jt) {
                             const int k0 = tr ? 0 : 2 * it, k1 = tr ? std::min(nkt - 1, 2 * it + 1) : nkt - 1;
-                            v.push_back({k1 - k0 + 1, MixTile{f, r, it, jt, k0, k1}});
+                            const int rank = tr ? nit - 1 - it : it;            // row tiles by K length, longest first
+                            const int col = (f * ncls + r) * X.njt + jt;
+                            const Key k{kRowGroup > 0 ? rank / kRowGroup : 0, kColGroup > 0 ? col / kColGroup : 0, k1 - k0 + 1, col, it};
+                            v.push_back({k, MixTile{f, r, it, jt, k0, k1}});
                         }
-            std::stable_sort(v.begin(), v.end(), [](const auto & a, const auto & b) { return a.first > b.first; });
+            std::stable_sort(v.begin(), v.end(), [](const auto & a, const auto & b) {
+                if (a.first.rg != b.first.rg) return a.first.rg < b.first.rg;
+                if (a.first.cg != b.first.cg) return a.first.cg < b.first.cg;
+                return a.first.klen > b.first.klen;
+            });
             std::vector<MixTile> tl;
             for (auto & x : v) tl.push_back(x.second);
             X.ntiles = (int) tl.size();
