@@ -257,9 +257,10 @@ __global__ void __launch_bounds__(THREADS, 1) trmm_mixed_kernel(const __grid_con
     auto chunk_start = [&](int kt, int k0) { return kt == k0 || kt % CHUNK_KT == 0; };
     auto chunk_end = [&](int kt, int k1) { return kt == k1 || kt % CHUNK_KT == CHUNK_KT - 1; };
 
+    __shared__ unsigned s_issued;   // K-tile copies the loader issued
     if (warp == 9) {
         if (lane == 0) {
-            unsigned q = 0;
+            unsigned q = 0, issued = 0;
             for (int t = blockIdx.x; t < L.ntiles && !s_abort; t += gridDim.x) {
                 const MixTile T = L.tiles[t];
                 const unsigned char * ua = L.Uimg[class_matrix(T.cls, L.ncls)] + (long long) T.it * L.nkt * NU * PIECE;
@@ -270,8 +271,10 @@ __global__ void __launch_bounds__(THREADS, 1) trmm_mixed_kernel(const __grid_con
                     tc::mbar_arrive_expect_tx(&bar_full[st], C::STAGE);
                     tc::bulk_g2s(sm + st * C::STAGE, ua + (long long) kt * NU * PIECE, NU * PIECE, &bar_full[st]);
                     tc::bulk_g2s(sm + st * C::STAGE + NU * PIECE, xb + (long long) kt * NX * XPIECE, NX * XPIECE, &bar_full[st]);
+                    issued = q + 1;
                 }
             }
+            s_issued = issued;
         }
         __syncwarp();
     } else if (warp == 8) {
@@ -381,11 +384,19 @@ __global__ void __launch_bounds__(THREADS, 1) trmm_mixed_kernel(const __grid_con
     }
 
     __syncthreads();
+    __shared__ volatile int s_never;
+    if (tid == 0) s_never = 0;
+    __syncthreads();
+    if (warp == 9 && lane == 0 && s_abort) {
+        // after a wait ran out, copies may still be landing: the last one issued into each stage
+        // (bounded waits) before the CTA's shared memory goes
+        const unsigned issued = s_issued;
+        for (unsigned j = issued >= 2 ? issued - 2 : 0; j < issued; ++j)
+            (void) tc::mbar_wait(&bar_full[j & 1], (j >> 1) & 1, &s_never);
+    }
     if (warp == 8) {
         if (lane == 0) {
             tc::commit(&bar_done);
-            __shared__ volatile int s_never;
-            s_never = 0;
             if (!tc::mbar_wait(&bar_done, 0, &s_never)) atomicExch(L.err, 2);
         }
         __syncwarp();
