@@ -604,7 +604,7 @@ def run_ours(args, rank, world, local_rank, dist):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "bf16 slices (3 per operand) / f32 exact acc (f64 in and out)",
+        "vs_baseline": None, "dtype": "bf16 slices in the blocked sweeps, s8 digits in the connection multiply; exact f32 / s32 accumulation (f64 in and out)",
         "data": "synthetic: seeded U(-1,1) in the sph triangular layout (splitmix64, seed 20261203 + field)",
         "config": {"workload": f"batched mixed-precision sph2fourier+fourier2sph: {nf} fields of degree {n - 1} "
                                f"(n={n}, M={M}) sharing one plan, MIXED_BF16, per GPU",

@@ -38,6 +38,37 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t) (N >> 3) << 17) | ((uint32_t) (M >> 4) << 24);
 }
 
+// instruction descriptor: S8 x S8 -> S32 (exact integer accumulation), A and B K-major, M x N
+__host__ __device__ constexpr uint32_t idesc_s8(int M, int N) {
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t) (N >> 3) << 17) | ((uint32_t) (M >> 4) << 24);
+}
+
+// byte offset of byte k of row r inside a K-major tile with the 64-byte swizzle (64 one-byte
+// elements a row): the 16-byte chunk index XOR address bits 7-8, 8-row groups 512 bytes apart
+__host__ __device__ __forceinline__ uint32_t sw64_byte(int r, int k) {
+    return (uint32_t) ((r >> 3) * 512 + (r & 7) * 64 + ((((k >> 4) ^ (r >> 1)) & 3) << 4) + (k & 15));
+}
+
+// shared-memory matrix descriptor: K-major, 64-byte swizzle, 8-row groups 512 bytes apart
+__device__ __forceinline__ uint64_t desc_sw64(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t) ((saddr >> 4) & 0x3FFF);          // start address
+    d |= (uint64_t) 1 << 16;                          // leading byte offset (unused with this swizzle)
+    d |= (uint64_t) (512 >> 4) << 32;                 // stride byte offset
+    d |= (uint64_t) 1 << 46;                          // descriptor version (sm_100)
+    d |= (uint64_t) 4 << 61;                          // 64-byte swizzle
+    return d;
+}
+
+// D[tmem] (+)= A[smem] * B[smem]^T over 8-bit signed integers, 32-bit integer accumulation, one thread
+__device__ __forceinline__ void mma_s8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, bool accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n"
+        :: "r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"((uint32_t) accumulate));
+}
+
 // D[tmem] (+)= A[smem] * B[smem]^T, issued by one thread
 __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, bool accumulate) {
     asm volatile(

@@ -448,21 +448,22 @@ int ft_b200_execute_noalloc_dev(const ft_harmonic_plan * P, int forward, char TR
  * slices per operand (eight slice products, exact FP32 accumulation per order
  * level); a value is carried between tiles at FP32 accuracy, in global memory
  * the matrices stay FP64.  The connection multiply runs on the tensor cores
- * too (four 8-bit slices of the matrix, three of the input, four for tri;
- * exact chunks of 256 rows, FP32 running sums; tri's right multiply through
- * two transposes, its normalisation in FP64).  Relative 2-norm error against
- * the FP64 transform about 5e-7 for sph at n = 4096; the connection
- * multiplies amplify the sweeps' error by a factor that depends on the family
- * and its parameters (disk with generic parameters about 3e-6 at n = 2048).
- * tri keeps its sweeps in FP64 (direct) in both split-BF16 forms and runs only
- * its two connection multiplies on the tensor cores, with each 256-row chunk's
- * exact sums recombined and accumulated in FP64: its multiplies amplify errors
- * strongly (a sliced sweep's to 3e-6 .. 3e-5, an FP32 recombination's to 2e-6
- * at n = 2048).
+ * too, from 8-bit integer digits (five of each row of the matrix, four of
+ * each input column, five for tri; exact 32-bit integer accumulation over the
+ * whole column, recombined in FP64; tri's right multiply through two
+ * transposes, its normalisation in FP64).  Relative 2-norm error against the
+ * FP64 transform about 3.5e-7 for sph at n = 4096; the connection multiplies
+ * amplify the sweeps' error by a factor that depends on the family and its
+ * parameters (disk with generic parameters about 3e-6 at n = 2048).  tri
+ * keeps its sweeps in FP64 (direct) in both mixed forms and runs only its two
+ * connection multiplies on the tensor cores: its multiplies amplify errors
+ * strongly (a sliced sweep's to 3e-6 .. 3e-5 at n = 2048).
  * precision FT_B200_MIXED_BF16X4: four slices in the blocks (ten products)
- * and four of the input in the connection multiply: about 1.4e-7 for sph at
- * n = 2048.  The first call of either builds its slice images
- * of the tiles and of the connection matrices (about 1 GB at n = 4096). */
+ * and five digits of the input in the connection multiply: about 1.5e-7 for
+ * sph at n = 4096.  The first call of either builds its slice images of the
+ * tiles and of the connection matrices (about 1 GB at n = 4096).
+ * FT_B200_MULTIPLY=bf16 in the environment selects the earlier connection
+ * multiply from BF16 slices (exact FP32 sums of 256-row chunks). */
 #define FT_B200_FP64 0
 #define FT_B200_FP64_BLOCKED 1
 #define FT_B200_MIXED_BF16 2
