@@ -689,9 +689,12 @@ __global__ void __launch_bounds__(THREADS, 1) trmm_s8_kernel(const __grid_consta
 #pragma unroll
                 for (int e = 0; e < 8; ++e) {
                     const int jj = T.jt * TBN + HALF * h + 8 * g + e;
-                    double y = (double) (int) a[NL - 1][e];
+                    // a 32-bit integer as FP64 without the conversion unit: 2^52 + 2^31 + A in the
+                    // bits, then subtract 2^52 + 2^31 (exact)
+                    auto as_f64 = [](uint32_t v) { return __hiloint2double(0x43300000, (int) (v ^ 0x80000000u)) - 4503601774854144.0; };
+                    double y = as_f64(a[NL - 1][e]);
 #pragma unroll
-                    for (int lv = NL - 2; lv >= 0; --lv) y = fma(y, 0.0078125, (double) (int) a[lv][e]);   // 2^-7
+                    for (int lv = NL - 2; lv >= 0; --lv) y = fma(y, 0.0078125, as_f64(a[lv][e]));   // 2^-7
                     if (row < L.n && jj < ncols)
                         __stcg(o + (long long) (T.cls + (long long) L.ncls * jj) * L.n + row, y * su * __ldg(xinv + 8 * g + e));
                 }
