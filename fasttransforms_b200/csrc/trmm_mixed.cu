@@ -418,21 +418,25 @@ __global__ void __launch_bounds__(THREADS, 1) trmm_mixed_kernel(const __grid_con
 // (|sX_j x| < 64), both cut into balanced digits of base 2^7,
 //   t = d_0 + d_1 2^-7 + d_2 2^-14 + ...,  d_k = nearest integer of the remaining value,
 // every digit in [-64, 64] (each remainder is at most 1/2 before the factor 2^7; the cuts are
-// exact in FP64).  Products d_b e_a of one level L = a + b <= 4 are at most 2^12 and a level sums
-// at most 5 of them per row of K, so its 32-bit integer accumulator (tcgen05.mma kind::i8) is
+// exact in FP64).  Products d_b e_a of one level L = a + b <= LMAX are at most 2^12 and a level
+// sums at most 5 of them per row of K, so its 32-bit integer accumulator (tcgen05.mma kind::i8) is
 // exact for any K below 2^31 / (5 2^12) = 104857: one accumulator set per output tile, no folds
-// along K.  The epilogue recombines the five levels in FP64 (exact: integers below 2^31, powers of
-// two) and scales by 1 / (sU_i sX_j).  Digits: NU = 5 of op(U) (34 bits), NX = 4 (27 bits) or 5
-// (34) of the input; 14 or 15 products at twice the BF16 rate.  K-tiles of 64 rows are 64-byte
-// rows of one-byte digits (the 64-byte swizzle), three stages in flight.
+// along K.  The epilogue recombines the levels in FP64 (exact: integers below 2^31, powers of two)
+// and scales by 1 / (sU_i sX_j).  Digits: NU = 5 of op(U) (34 bits), NX = 4 (27 bits) or 5 (34)
+// of the input, at twice the BF16 rate.  K-tiles of 64 rows are 64-byte rows of one-byte digits
+// (the 64-byte swizzle), three stages in flight.
 constexpr int KT8 = 64;                      // K per tile (a 64-byte row of one-byte digits)
 constexpr int PIECE8 = TB * KT8;             // bytes of one digit of one K-tile of op(U) (8 KB)
-constexpr int LMAX8 = 4;                     // levels kept: 0 .. 4
 constexpr int NSTAGE8 = 3;
-constexpr int TBN8 = 96;                     // output tile columns
+// configurations (NU, NX, TBN, levels kept 0 .. LMAX): four input digits -> (5, 4, 96, 4),
+// fourteen products; five input digits (tri, MIXED_BF16X4) -> (5, 5, 96, 4), fifteen products.
+// (Levels 0 .. 3 only would let 128-column tiles fill tensor memory with ten products, 30 % less
+// time in the multiply, but the dropped level doubles the mixed forms' error.)
+constexpr int TBN8_4 = 96, LMAX8_4 = 4;
+constexpr int TBN8_5 = 96, LMAX8_5 = 4;
 
-template <int NU, int NX, int TBN> struct Cfg8 {
-    static constexpr int NL = LMAX8 + 1;                    // accumulators per tile
+template <int NU, int NX, int TBN, int LMAX> struct Cfg8 {
+    static constexpr int NL = LMAX + 1;                     // accumulators per tile
     static constexpr int XPIECE = TBN * KT8;                // bytes of one input digit of one K-tile
     static constexpr int STAGE = NU * PIECE8 + NX * XPIECE;
     static constexpr size_t SMEM = NSTAGE8 * (size_t) STAGE + 1024;
@@ -583,9 +587,9 @@ struct Mix8Launch {
     int * err;
 };
 
-template <int NU, int NX, int TBN>
+template <int NU, int NX, int TBN, int LMAX>
 __global__ void __launch_bounds__(THREADS, 1) trmm_s8_kernel(const __grid_constant__ Mix8Launch L) {
-    using C = Cfg8<NU, NX, TBN>;
+    using C = Cfg8<NU, NX, TBN, LMAX>;
     constexpr int NL = C::NL;
     constexpr int XPIECE = C::XPIECE;
     constexpr int HALF = TBN / 2;                     // columns per epilogue thread
@@ -880,7 +884,7 @@ cudaError_t launch_trmm_s8(HarmonicPlan * H, MixedTrmmPlan * T, MixedTrmmWork * 
                            double * const * in, double * const * out, int nf, int M, cudaStream_t st, int ncls, int which) {
     const int n = H->n;
     const int nkt = (n + KT8 - 1) / KT8, nit = (n + TB - 1) / TB;
-    const int cfg = nx8 == 5 ? 1 : 0, tbn = TBN8;
+    const int cfg = nx8 == 5 ? 1 : 0, tbn = cfg ? TBN8_5 : TBN8_4;
     const int ii = inverse ? 1 : 0, ti = trans ? 1 : 0;
     for (int u = 0; u < 2; ++u) {
         if (T->img8[ii][ti][u] || (ncls == 1 && u != which)) continue;
@@ -918,8 +922,8 @@ cudaError_t launch_trmm_s8(HarmonicPlan * H, MixedTrmmPlan * T, MixedTrmmWork * 
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const int sgrid = nf * ncls * X.njt * ((nkt + 3) / 4);
-    if (cfg) slice_input_s8_kernel<5, TBN8><<<sgrid, 256, 0, st>>>(SX);
-    else     slice_input_s8_kernel<4, TBN8><<<sgrid, 256, 0, st>>>(SX);
+    if (cfg) slice_input_s8_kernel<5, TBN8_5><<<sgrid, 256, 0, st>>>(SX);
+    else     slice_input_s8_kernel<4, TBN8_4><<<sgrid, 256, 0, st>>>(SX);
     count_launch();
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -940,13 +944,13 @@ cudaError_t launch_trmm_s8(HarmonicPlan * H, MixedTrmmPlan * T, MixedTrmmWork * 
     const int ctas = std::min(sms, X.ntiles);
     if (ctas <= 0) return cudaSuccess;
     if (cfg) {
-        using C = Cfg8<5, 5, TBN8>;
-        auto kern = trmm_s8_kernel<5, 5, TBN8>;
+        using C = Cfg8<5, 5, TBN8_5, LMAX8_5>;
+        auto kern = trmm_s8_kernel<5, 5, TBN8_5, LMAX8_5>;
         e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) C::SMEM);
         if (e == cudaSuccess) { kern<<<ctas, THREADS, C::SMEM, st>>>(L); e = cudaGetLastError(); }
     } else {
-        using C = Cfg8<5, 4, TBN8>;
-        auto kern = trmm_s8_kernel<5, 4, TBN8>;
+        using C = Cfg8<5, 4, TBN8_4, LMAX8_4>;
+        auto kern = trmm_s8_kernel<5, 4, TBN8_4, LMAX8_4>;
         e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) C::SMEM);
         if (e == cudaSuccess) { kern<<<ctas, THREADS, C::SMEM, st>>>(L); e = cudaGetLastError(); }
     }
