@@ -339,12 +339,13 @@ __global__ void build_img_kernel(const double * __restrict__ Q, long long qb, in
     unsigned char * out = reinterpret_cast<unsigned char *>(img) + (qb + (long long) k1 * nch + c) * (long long) MxCfg<NS>::QCHAIN;
     for (int e = threadIdx.x; e < WIN * WIN; e += blockDim.x) {
         const int o = e / WIN, w = e % WIN;
-        // 256 q = j_0 + j_1 2^-9 + ..., integers |j| <= 2^8
+        // 256 q = j_0 + j_1 2^-9 + ..., integers |j| <= 2^8, stored negated (-j_b; a zero as +0)
+        // because the window's slices are -i_a: the products (-i_a)(-j_b) are those of the slices
         double t = (transpose ? q[(long long) w * WIN + o] : q[e]) * 256.0;
         const uint32_t off = tc::sw128_offset(o, w);
         for (int b = 0; b < NS; ++b) {
             const double j = rint(t);
-            *reinterpret_cast<__nv_bfloat16 *>(out + b * MX_QPIECE + off) = __float2bfloat16_rn((float) j);
+            *reinterpret_cast<__nv_bfloat16 *>(out + b * MX_QPIECE + off) = __float2bfloat16_rn(j == 0.0 ? 0.0f : (float) -j);
             t = (t - j) * 512.0;
         }
     }
@@ -357,26 +358,58 @@ __device__ __forceinline__ float slice_scale(float amax) {
     return __uint_as_float((uint32_t) (261 - E) << 23);       // 2^(8 - (E - 126))
 }
 
+// Pairs of FP32 values in one 64-bit register, with sm_100's packed `.f32x2` arithmetic: each
+// half is rounded exactly as the scalar instruction rounds it (round to nearest, subnormals kept),
+// so a pair costs one instruction where two scalar ones gave the same bits.
+__device__ __forceinline__ uint64_t f2_pack(float lo, float hi) {
+    uint64_t d;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(lo), "f"(hi));
+    return d;
+}
+__device__ __forceinline__ void f2_unpack(uint64_t d, float & lo, float & hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(d));
+}
+__device__ __forceinline__ uint64_t f2_fma(uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ uint64_t f2_sub(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t f2_mul(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
 // eight consecutive window positions, scaled by s (a power of two), -> NS 16-byte chunks of
-// integer-valued BF16 slices: s x = i_0 + i_1 2^-9 + ...  Each cut is one FMA that scales and
-// adds 1.5 * 2^23 (rounding to the nearest integer, |s x| < 2^8) and one subtraction, and each
-// residual one FMA (s x - i_0, 2^9 t - i_a: exact, |residual| <= 1/2 and a multiple of the
-// operand's last place), the values those of rounding s x, subtracting and scaling in turn.
+// integer-valued BF16 slices, negated: s x = i_0 + i_1 2^-9 + ..., stored -i_a (the tile images
+// hold -j_b, so every product keeps its sign).  Each cut is one FMA that scales and adds
+// 1.5 * 2^23 (rounding to the nearest integer, |s x| < 2^8) and one subtraction from 1.5 * 2^23,
+// which gives -i_a exactly; the residual is one FMA with that same -i_a (s x - i_0, 2^9 t - i_a:
+// exact, |residual| <= 1/2 and a multiple of the operand's last place), the values those of
+// rounding s x, subtracting and scaling in turn.  Two positions go through each instruction.
 template <int NS>
 __device__ __forceinline__ void slice8(const float * v, float s, uint4 * out) {
     constexpr float kMagic = 12582912.0f;         // 1.5 * 2^23
+    const uint64_t magic = f2_pack(kMagic, kMagic), c512 = f2_pack(512.0f, 512.0f);
     uint32_t w[NS][4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-        float t0 = v[2 * q], t1 = v[2 * q + 1], m = s;
+        uint64_t t = f2_pack(v[2 * q], v[2 * q + 1]), m = f2_pack(s, s);
 #pragma unroll
         for (int a = 0; a < NS; ++a) {
-            const float i0 = __fsub_rn(__fmaf_rn(t0, m, kMagic), kMagic), i1 = __fsub_rn(__fmaf_rn(t1, m, kMagic), kMagic);
+            const uint64_t u = f2_fma(t, m, magic);
+            const uint64_t ni = f2_sub(magic, u);
+            float i0, i1;
+            f2_unpack(ni, i0, i1);
             w[a][q] = tc::pack_bf16_ints(i0, i1);
             if (a + 1 < NS) {
-                t0 = __fmaf_rn(t0, m, -i0);
-                t1 = __fmaf_rn(t1, m, -i1);
-                m = 512.0f;
+                t = f2_fma(t, m, ni);
+                m = c512;
             }
         }
     }
@@ -635,6 +668,7 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
                     __syncwarp();
                     tc::fence_after_sync();
                     const float unscale = 0.00390625f / scale;    // 2^-8 / s, a power of two
+                    const uint64_t c2m9 = f2_pack(0.001953125f, 0.001953125f), unscale2 = f2_pack(unscale, unscale);
 #pragma unroll
                     for (int g = 0; g < TL / 8; ++g) {             // 8 window positions at a time
                         uint32_t a[NL][8];
@@ -643,20 +677,26 @@ __global__ void __launch_bounds__(MX_THREADS, 1) blocked_mixed_kernel(const __gr
                         tc::tmem_wait_ld();
 #pragma unroll
                         for (int hq = 0; hq < 2; ++hq) {           // one quad of positions at a time
-                            float v[4];
+                            // levels recombined highest first, y = 2^-9 y + A_lv, two positions a step
+                            uint64_t y[2];
 #pragma unroll
-                            for (int e = 0; e < 4; ++e) {
-                                float y = __uint_as_float(a[NL - 1][4 * hq + e]);
+                            for (int e2 = 0; e2 < 2; ++e2) {
+                                const int e = 4 * hq + 2 * e2;
+                                y[e2] = f2_pack(__uint_as_float(a[NL - 1][e]), __uint_as_float(a[NL - 1][e + 1]));
 #pragma unroll
-                                for (int lv = NL - 2; lv >= 0; --lv) y = fmaf(y, 0.001953125f, __uint_as_float(a[lv][4 * hq + e]));
-                                v[e] = y;
+                                for (int lv = NL - 2; lv >= 0; --lv)
+                                    y[e2] = f2_fma(y[e2], c2m9, f2_pack(__uint_as_float(a[lv][e]), __uint_as_float(a[lv][e + 1])));
                             }
                             const int P = lo + TL * hf + 8 * g + 4 * hq;
                             if (fin) {
-                                if (P >= 0 && P < Pend)
-                                    __stcg(Tq + (long long) (P >> 2) * MX_COLS,
-                                           make_float4(v[0] * unscale, v[1] * unscale, v[2] * unscale, v[3] * unscale));
+                                float4 o;
+                                f2_unpack(f2_mul(y[0], unscale2), o.x, o.y);
+                                f2_unpack(f2_mul(y[1], unscale2), o.z, o.w);
+                                if (P >= 0 && P < Pend) __stcg(Tq + (long long) (P >> 2) * MX_COLS, o);
                             } else {   // kept unscaled: the window cut below applies unscale
+                                float v[4];
+                                f2_unpack(y[0], v[0], v[1]);
+                                f2_unpack(y[1], v[2], v[3]);
 #pragma unroll
                                 for (int e = 0; e < 4; ++e) src[8 * g + 4 * hq + e] = v[e];
                             }
