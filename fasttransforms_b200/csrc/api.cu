@@ -162,7 +162,19 @@ bool get_tasks(ft_rotation_plan * RP, int M, RotTask ** d_tasks, int * ntasks) {
 // stage runs out of place.
 int untouched_cols(int kind, int M) { return std::min(M, kind == TRI ? 1 : (kind == RECT ? 2 : 3)); }
 
-bool rotations(ft_rotation_plan * RP, bool hi2lo, const double * in, double * out, int M, long long lda, cudaStream_t st) {
+// Device memory of one execute call (call_scratch): the out-of-place matrix S, the rotation
+// kernel's work counter and the pass pipeline's progress words, so that calls on one plan share
+// none of them.
+struct CallScratch {
+    void * base = nullptr;     // the one pool allocation holding the rest
+    double * S = nullptr;
+    int * counter = nullptr;
+    int * prog = nullptr;
+    int prog_cap = 0;
+};
+
+bool rotations(ft_rotation_plan * RP, bool hi2lo, const double * in, double * out, int M, long long lda, cudaStream_t st,
+               const CallScratch * cs = nullptr) {
     RotTask * d_tasks = nullptr;
     int ntasks = 0;
     if (!get_tasks(RP, M, &d_tasks, &ntasks)) return false;
@@ -177,7 +189,7 @@ bool rotations(ft_rotation_plan * RP, bool hi2lo, const double * in, double * ou
     L.fields[0] = RotField{in, out, RP->d_scp, RP->n, M, RP->kind, lda, 0};
     L.tasks = d_tasks;
     L.ntasks = ntasks;
-    L.counter = RP->d_counter;
+    L.counter = cs ? cs->counter : RP->d_counter;
     // out of place, the destination holds nothing live yet: the autotuner may time there
     double * const dead[1] = {out};
     prof_begin(FAM_ROT, st);
@@ -187,7 +199,8 @@ bool rotations(ft_rotation_plan * RP, bool hi2lo, const double * in, double * ou
         auto it = RP->sched->find(M);
         if (it != RP->sched->end()) sched = it->second;
     }
-    const cudaError_t e = launch_rotations(RP->kind, hi2lo, L, 0, st, in != out ? dead : nullptr, sched);
+    const cudaError_t e = launch_rotations(RP->kind, hi2lo, L, 0, st, in != out ? dead : nullptr, sched,
+                                           cs ? cs->prog : nullptr, cs ? cs->prog_cap : 0);
     prof_end(st);
     return cuda_ok(e, "rotation kernel");
 }
@@ -196,12 +209,12 @@ bool rotations(ft_rotation_plan * RP, bool hi2lo, const double * in, double * ou
 // 2m + 2 for m = 2 .. M/2 - 1, i.e. the sph sweeps of the matrix that starts two columns
 // later and has M - 2 columns; columns 0 and 1 are left alone.
 bool rotations_sphv(ft_rotation_plan * RP, bool hi2lo, const double * in, double * out, int M, long long lda,
-                    cudaStream_t st) {
+                    cudaStream_t st, const CallScratch * cs = nullptr) {
     const int lead = std::min(M, 2);
     if (in != out && !cuda_ok(cudaMemcpy2DAsync(out, lda * sizeof(double), in, lda * sizeof(double), RP->n * sizeof(double),
                                                 lead, cudaMemcpyDeviceToDevice, st), "cudaMemcpy2DAsync")) return false;
     if (M <= 2) return true;
-    return rotations(RP, hi2lo, in + 2 * lda, out + 2 * lda, M - 2, lda, st);
+    return rotations(RP, hi2lo, in + 2 * lda, out + 2 * lda, M - 2, lda, st, cs);
 }
 
 // sph and disk: order m occupies the column pair (2m - 1, 2m) for m = 2 .. M/2
@@ -277,15 +290,58 @@ bool normalize(double * A, int N, int M, long long lda, bool transposed, cudaStr
     return cuda_ok(e, "normalize");
 }
 
-bool ensure_scratch(HarmonicPlan * H, size_t elems) {
-    if (elems <= H->scratch_elems) return true;
-    if (H->d_scratch) cudaFree(H->d_scratch);
-    H->d_scratch = nullptr;
-    H->scratch_elems = 0;
-    if (!cuda_ok(cudaMalloc(&H->d_scratch, elems * sizeof(double)), "cudaMalloc(scratch)")) return false;
-    H->scratch_elems = elems;
-    H->pub.B = H->d_scratch;
+// The library's stream-ordered memory pool on device dev (created on first use, kept until the
+// process exits).  Its release threshold is unlimited: memory a call frees goes back to the
+// pool once the call's stream reaches the free and serves the next call, without returning to
+// the driver in between.
+cudaMemPool_t call_pool(int dev) {
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = pools.find(dev);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (!cuda_ok(cudaMemPoolCreate(&pool, &props), "cudaMemPoolCreate")) return nullptr;
+    uint64_t keep = UINT64_MAX;
+    if (!cuda_ok(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "cudaMemPoolSetAttribute")) {
+        cudaMemPoolDestroy(pool);
+        return nullptr;
+    }
+    pools[dev] = pool;
+    return pool;
+}
+
+// Scratch of one execute call, allocated on its stream from the pool: elems doubles, the work
+// counter and prog_cap progress words.  call_scratch_free returns it on the same stream, after
+// the work enqueued before it.
+bool call_scratch(int dev, size_t elems, int prog_cap, cudaStream_t st, CallScratch * cs) {
+    cudaMemPool_t pool = call_pool(dev);
+    if (!pool) return false;
+    const size_t s_bytes = (elems * sizeof(double) + 255) & ~(size_t) 255;
+    const size_t bytes = s_bytes + 256 + sizeof(int) * (size_t) std::max(prog_cap, 1);
+    void * p = nullptr;
+    const cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, pool, st);
+    if (e != cudaSuccess) {
+        set_error(e == cudaErrorMemoryAllocation ? FT_B200_ENOMEM : FT_B200_ECUDA,
+                  std::string("cudaMallocFromPoolAsync(call scratch): ") + cudaGetErrorString(e));
+        return false;
+    }
+    char * b = static_cast<char *>(p);
+    cs->base = p;
+    cs->S = reinterpret_cast<double *>(b);
+    cs->counter = reinterpret_cast<int *>(b + s_bytes);
+    cs->prog = reinterpret_cast<int *>(b + s_bytes + 256);
+    cs->prog_cap = prog_cap;
     return true;
+}
+
+void call_scratch_free(CallScratch & cs, cudaStream_t st) {
+    if (cs.base) cudaFreeAsync(cs.base, st);
+    cs = CallScratch{};
 }
 
 int execute_dev_impl(HarmonicPlan * H, bool forward, char TRANS, double * A, int N, int M, cudaStream_t st,
@@ -294,16 +350,28 @@ int execute_dev_impl(HarmonicPlan * H, bool forward, char TRANS, double * A, int
     if (!A) { set_error(FT_B200_EINVAL, "NULL matrix"); return t_status; }
     if (vector && H->kind != SPH) { set_error(FT_B200_EINVAL, "vector-field transforms take a sph plan"); return t_status; }
     if (!valid_MN(H->kind, H->n, N, M)) return t_status;
-    if (!ensure_scratch(H, (size_t) N * M)) return t_status;
-    double * S = H->d_scratch;
     ft_rotation_plan * RP = H->rp_arr[0];
+    // Everything this call writes besides A comes from the pool, on st: two calls on one plan
+    // (from two threads, on two streams) share no device memory.  The pass pipeline needs a
+    // progress word per pass of every task, at most ceil(sweeps / 16) <= n / 16 + 1 per task.
+    RotTask * d_tasks = nullptr;
+    int ntasks = 0;
+    if (!get_tasks(RP, vector ? std::max(M - 2, 1) : M, &d_tasks, &ntasks)) return t_status;
+    struct Guard {
+        CallScratch cs;
+        cudaStream_t st;
+        ~Guard() { call_scratch_free(cs, st); }
+    } guard{CallScratch{}, st};
+    if (!call_scratch(H->device, (size_t) N * M, ntasks * (N / 16 + 2), st, &guard.cs)) return t_status;
+    const CallScratch * const cs = &guard.cs;
+    double * S = guard.cs.S;
     const bool tN = TRANS == 'N';
     const long long lda = N;
     if (H->kind != TRI) {
         // rotations (out of place) then trmm back, or trmm out then rotations back
         // (sph vector fields: the shifted sweeps and the swapped matrices, src/drivers.c:867-899)
         auto rot = [&](bool hi2lo, const double * in, double * out) {
-            return vector ? rotations_sphv(RP, hi2lo, in, out, M, lda, st) : rotations(RP, hi2lo, in, out, M, lda, st);
+            return vector ? rotations_sphv(RP, hi2lo, in, out, M, lda, st, cs) : rotations(RP, hi2lo, in, out, M, lda, st, cs);
         };
         if (forward && tN) {            // hi2lo, P
             if (!rot(true, A, S)) return t_status;
@@ -334,7 +402,7 @@ int execute_dev_impl(HarmonicPlan * H, bool forward, char TRANS, double * A, int
     if (rot_hi2lo_first) {
         // rotation, then left / right, then normalisation; the rotation goes out of place iff k is odd
         double * rot_out = (k % 2) ? S : A;
-        if (!rotations(RP, true, A, rot_out, M, lda, st)) return t_status;
+        if (!rotations(RP, true, A, rot_out, M, lda, st, cs)) return t_status;
         cur = rot_out; oth = (rot_out == A) ? S : A;
         if (forward) {   // tri2cheb 'N': left N P0, right T P1
             if (left) { if (!trmm_left1(H, U0, false, cur, oth, M, st)) return t_status; flip(); }
@@ -355,7 +423,7 @@ int execute_dev_impl(HarmonicPlan * H, bool forward, char TRANS, double * A, int
             if (right) { if (!trmm_right(U1, cur, oth, N, lda, true, st)) return t_status; flip(); }
             if (left) { if (!trmm_left1(H, U0, false, cur, oth, M, st)) return t_status; flip(); }
         }
-        if (!rotations(RP, false, cur, A, M, lda, st)) return t_status;
+        if (!rotations(RP, false, cur, A, M, lda, st, cs)) return t_status;
     }
     return FT_B200_OK;
 }
@@ -427,19 +495,25 @@ HarmonicPlan * make_harmonic_plan(int kind, int n, double alpha, double beta, do
             !cuda_ok(cudaMemcpy(H->dPinv[i], H->hostPinv[i], nn, cudaMemcpyHostToDevice), "cudaMemcpy(Pinv)"))
             return fail();
     }
-    if (!ensure_scratch(H, (size_t) n * H->Mdef)) return fail();
     if (!cuda_ok(cudaStreamCreateWithFlags(&H->stream, cudaStreamNonBlocking), "cudaStreamCreate")) return fail();
     // build the default task list now, outside any later stream capture
     RotTask * dt; int nt;
     if (!get_tasks(H->rp_arr[0], H->Mdef, &dt, &nt)) return fail();
+    // the pool keeps what one call at the default size takes, ready for the first call
+    CallScratch warm;
+    if (!call_scratch(dev, (size_t) n * H->Mdef, nt * (n / 16 + 2), H->stream, &warm)) return fail();
+    call_scratch_free(warm, H->stream);
+    if (!cuda_ok(cudaStreamSynchronize(H->stream), "cudaStreamSynchronize")) return fail();
     return H;
 }
 
-// host-pointer execution: stage A on the device, run, copy back, wait
+// host-pointer execution: stage A on the device, run, copy back, wait (one call per plan at a
+// time: concurrent calls from other threads wait for the plan's staging buffer and stream)
 void execute_host(const ft_harmonic_plan * P, bool forward, char TRANS, double * A, int N, int M, bool vector = false) {
     clear_error();
     HarmonicPlan * H = as_plan(P);
     if (!H) { set_error(FT_B200_EINVAL, "not a plan created by this library"); return; }
+    std::lock_guard<std::mutex> lk(H->host_mu);
     if (TRANS != 'N' && TRANS != 'T') { set_error(FT_B200_EINVAL, "TRANS must be 'N' or 'T'"); return; }
     if (!A) { set_error(FT_B200_EINVAL, "NULL matrix"); return; }
     if (!valid_MN(H->kind, H->n, N, M)) return;
@@ -1042,7 +1116,6 @@ void ft_destroy_harmonic_plan(ft_harmonic_plan * P) {
         if (H->dP[i]) cudaFree(H->dP[i]);
         if (H->dPinv[i]) cudaFree(H->dPinv[i]);
     }
-    if (H->d_scratch) cudaFree(H->d_scratch);
     if (H->d_stage) cudaFree(H->d_stage);
     if (H->blocked) blocked_plan_free(H->blocked);
     if (H->mixed_trmm) mixed_trmm_plan_free(H->mixed_trmm);

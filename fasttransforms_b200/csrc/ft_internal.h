@@ -171,9 +171,13 @@ int rotation_device_error();   // reads and clears the rotation kernel's status 
 // dead: per field, memory the caller has no live data in (N x M at the field's leading
 // dimension), or null.  With it, the first launch of a shape times every configuration
 // there and keeps the fastest for the shape (the autotuner; FT_B200_AUTOTUNE=0 turns it off).
-// sched: the task list's schedule (null: no pass pipeline).
+// sched: the task list's schedule (null: no pass pipeline).  prog_call: progress words of the
+// calling execute (prog_cap of them) for the pass pipeline instead of the schedule's own, so
+// that concurrent calls on one plan do not share them; a queue needing more runs without the
+// pipeline.
 cudaError_t launch_rotations(int kind, bool hi2lo, const RotLaunch & L, int max_ctas, cudaStream_t st,
-                             double * const * dead = nullptr, RotSchedule * sched = nullptr);
+                             double * const * dead = nullptr, RotSchedule * sched = nullptr,
+                             int * prog_call = nullptr, int prog_cap = 0);
 void set_rotation_config(int cfg);   // 0 .. 3 forces a configuration, -1 chooses per shape
 // (Re)builds RP->d_scp from RP->d_sc (call after every change of d_sc; synchronous)
 bool rotation_plan_pad(ft_rotation_plan * RP);
@@ -242,8 +246,7 @@ struct HarmonicPlan {
     double * hostPinv[2];
     double * dP[2];
     double * dPinv[2];
-    double * d_scratch;
-    size_t scratch_elems;
+    std::mutex host_mu;         // one host-pointer call at a time (they share d_stage and stream)
     double * d_stage;           // device copy of A for host-pointer calls
     size_t stage_elems;
     cudaStream_t stream;

@@ -727,18 +727,21 @@ cudaError_t launch_with(int kind, bool hi2lo, int cfg, const RotLaunch & L, int 
 
 // One launch in configuration cfg: shape cfg & 7, through the pass pipeline in mode cfg >> 3
 // (schedule_passes) when the task list has a schedule (else, and in mode 0, each CTA runs
-// every pass of its tasks).
+// every pass of its tasks).  The progress words are the call's own (prog_call) when it has
+// them, else the schedule's.
 cudaError_t launch_shape(int kind, bool hi2lo, int cfg, const RotLaunch & L, int max_ctas, cudaStream_t st,
-                         RotSchedule * sched) {
+                         RotSchedule * sched, int * prog_call = nullptr, int prog_cap = 0) {
     const int shape = cfg & 7, mode = cfg >> 3;
     const RotSchedule::Units * U = (mode > 0 && sched) ? schedule_passes(sched, kind, L, shape_pass(shape), mode, st) : nullptr;
-    if (!U) return launch_with(kind, hi2lo, shape, L, max_ctas, st);
+    // a call with words of its own too few for this queue runs whole tasks per CTA instead
+    if (!U || (prog_call && U->nprog > prog_cap)) return launch_with(kind, hi2lo, shape, L, max_ctas, st);
+    int * const prog = prog_call ? prog_call : U->d_prog;
     static thread_local RotLaunch P;
     P = L;
     P.chains = U->d_chains;
     P.nchains = U->n;
-    P.prog = U->d_prog;
-    const cudaError_t e = cudaMemsetAsync(U->d_prog, 0x80, sizeof(int) * U->nprog, st);   // below any position
+    P.prog = prog;
+    const cudaError_t e = cudaMemsetAsync(prog, 0x80, sizeof(int) * U->nprog, st);   // below any position
     if (e != cudaSuccess) return e;
     return launch_with(kind, hi2lo, shape, P, max_ctas, st);
 }
@@ -775,7 +778,7 @@ bool autotune_enabled() {
 // kernel's cost does not depend on the values, and every configuration computes the same
 // results bit for bit (each element meets its rotations in the same order).
 int tune(int kind, bool hi2lo, const RotLaunch & L, double * const * dead, int max_ctas, cudaStream_t st,
-         RotSchedule * sched) {
+         RotSchedule * sched, int * prog_call, int prog_cap) {
     static thread_local RotLaunch S;
     S = L;
     for (int f = 0; f < L.nfields; ++f) { S.fields[f].in = dead[f]; S.fields[f].out = dead[f]; }
@@ -792,9 +795,9 @@ int tune(int kind, bool hi2lo, const RotLaunch & L, double * const * dead, int m
     for (int cfg = 0; cfg < 8 * kPipeModes; ++cfg) {
         if ((cfg & 7) > 5 || ((kind == TRI || kind == RECT) && (cfg & 7) == 1)) continue;   // tri, rect: shape 1 not built
         if ((cfg >> 3) && !sched) continue;
-        if (launch_shape(kind, hi2lo, cfg, S, max_ctas, st, sched) != cudaSuccess) { best = -1; break; }
+        if (launch_shape(kind, hi2lo, cfg, S, max_ctas, st, sched, prog_call, prog_cap) != cudaSuccess) { best = -1; break; }
         if (cudaEventRecord(e0, st) != cudaSuccess) { best = -1; break; }
-        if (launch_shape(kind, hi2lo, cfg, S, max_ctas, st, sched) != cudaSuccess) { best = -1; break; }
+        if (launch_shape(kind, hi2lo, cfg, S, max_ctas, st, sched, prog_call, prog_cap) != cudaSuccess) { best = -1; break; }
         float ms = 0.0f;
         if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
             cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) { best = -1; break; }
@@ -808,7 +811,7 @@ int tune(int kind, bool hi2lo, const RotLaunch & L, double * const * dead, int m
 }  // namespace
 
 cudaError_t launch_rotations(int kind, bool hi2lo, const RotLaunch & L, int max_ctas, cudaStream_t st,
-                             double * const * dead, RotSchedule * sched) {
+                             double * const * dead, RotSchedule * sched, int * prog_call, int prog_cap) {
     if (L.ntasks <= 0) return cudaSuccess;
     int cfg = rotation_config();
     if (cfg < 0) {
@@ -825,7 +828,7 @@ cudaError_t launch_rotations(int kind, bool hi2lo, const RotLaunch & L, int max_
             if (known >= 0) {
                 cfg = known;
             } else if (dead && cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) {
-                const int t = tune(kind, hi2lo, L, dead, max_ctas, st, sched);
+                const int t = tune(kind, hi2lo, L, dead, max_ctas, st, sched, prog_call, prog_cap);
                 if (t >= 0) {
                     std::lock_guard<std::mutex> lk(g_tune_mu);
                     g_tuned[key] = t;
@@ -834,7 +837,7 @@ cudaError_t launch_rotations(int kind, bool hi2lo, const RotLaunch & L, int max_
             }
         }
     }
-    return launch_shape(kind, hi2lo, cfg, L, max_ctas, st, sched);
+    return launch_shape(kind, hi2lo, cfg, L, max_ctas, st, sched, prog_call, prog_cap);
 }
 
 

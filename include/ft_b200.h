@@ -17,9 +17,16 @@
  *   - TRANS 'N' applies the operator, 'T' its transpose; any other character
  *     is a no-op (the reference silently ignores it; here the status is
  *     FT_B200_EINVAL and A is left untouched).
- *   - In place on A.  The plan owns its device scratch, so two concurrent
- *     executes on ONE plan are not reentrant (as in the reference, whose plan
- *     owns P->B).  Different plans may run concurrently on different streams.
+ *   - In place on A.  ft_b200_execute_dev and ft_b200_execute_sphv_dev on sph,
+ *     tri and disk plans are reentrant: each call takes its scratch matrix,
+ *     work counter and progress words from the library's stream-ordered memory
+ *     pool on its own stream (freed there after its work), so calls on ONE plan
+ *     may run concurrently from several threads on several streams.  The
+ *     host-pointer calls (ft_execute_*) on one plan share its staging buffer
+ *     and stream and run one at a time (a call from another thread waits).
+ *     Every other entry point keeps plan-owned scratch, as the reference's plan
+ *     owns P->B: concurrent calls on one such plan are not reentrant.  Different
+ *     plans may run concurrently on different streams.
  *
  * Everything runs on the current CUDA device.  There is no CPU fallback: if no
  * sm_100 device is present, plan creation fails (NULL) and the status says why.
@@ -361,7 +368,9 @@ void ft_kernel_tet_lo2hi(const ft_rotation_plan * RP, const int L, const int m, 
 enum { FT_B200_SPH = 0, FT_B200_TRI = 1, FT_B200_DISK = 2 };
 
 /* Full transform.  forward = 1: sph2fourier / tri2cheb / disk2cxf / rectdisk2cheb / ann2cxf;
- * forward = 0: fourier2sph / cheb2tri / cxf2disk / cheb2rectdisk / cxf2ann. */
+ * forward = 0: fourier2sph / cheb2tri / cxf2disk / cheb2rectdisk / cxf2ann.  Reentrant per
+ * plan for sph, tri and disk plans (per-call scratch from a stream-ordered pool: N x M doubles
+ * and a few hundred KB per call while it runs); rectdisk and annulus plans are not. */
 int ft_b200_execute_dev(const ft_harmonic_plan * P, int forward, char TRANS, double * dA, int N, int M, void * stream);
 /* Grid synthesis / analysis on device memory: op 0 sph synthesis, 1 sph analysis,
  * 2 sphv synthesis, 3 sphv analysis (the sequences of the ft_execute_* above, with
