@@ -30,11 +30,11 @@ def slice_scale(amax):
 
 
 def cut(v, s, ns):
-    """The kernel's cut of float32 values v at scale s: the stored (negated) slices and, for the
-    check, the residuals of the former positive form."""
+    """The kernel's cut of float32 values v at scale s: the stored (negated) slices and the
+    residuals, each checked against the former positive form's on the way."""
     v = np.asarray(v, dtype=np.float32)
     t, m = v.copy(), np.float32(s)
-    stored, resid_pos, resid_neg = [], [], []
+    stored, resid_neg = [], []
     for a in range(ns):
         u = (t * m) + MAGIC                      # fma(t, m, magic): t * m is exact
         neg_i = MAGIC - u                        # -i_a, exact
