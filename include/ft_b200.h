@@ -21,7 +21,9 @@
  *     tri and disk plans are reentrant: each call takes its scratch matrix,
  *     work counter and progress words from the library's stream-ordered memory
  *     pool on its own stream (freed there after its work), so calls on ONE plan
- *     may run concurrently from several threads on several streams.  The
+ *     may run concurrently from several threads on several streams.  The pool
+ *     keeps what it has handed out (at most the peak of concurrent calls) for
+ *     reuse until the process exits.  The
  *     host-pointer calls (ft_execute_*) on one plan share its staging buffer
  *     and stream and run one at a time (a call from another thread waits).
  *     Every other entry point keeps plan-owned scratch, as the reference's plan
